@@ -1,0 +1,232 @@
+/*
+ * rq.h -- C ABI of librq, the B200-native RealQM real-space solver step.
+ *
+ * One context (rq_ctx) owns every device buffer of one grid: the density field psi
+ * (double-buffered), the int32 domain label per voxel (double-buffered), the nuclear
+ * potential K, the Hartree half-potential P, the level-set field W and the FP64
+ * per-domain sums.  All entry points return RQ_OK (0) or a negative RQ_E* status;
+ * nothing throws or aborts across this boundary.  Host buffers belong to the caller
+ * and are copied; device memory belongs to the context.
+ *
+ * Grid convention (both reference hosts): S = NN+1 points per axis, linear index
+ * id = i*S*S + j*S + k (k fastest), the outer planes are Dirichlet boundary
+ * (cloud/solver.py:20-30, molecule.js:268-276).  Atom positions are in grid units
+ * (x = i*h), like the reference's {i, j, k} atom records.
+ *
+ * Threading: a context is used by one host thread at a time and issues its work on
+ * one CUDA stream (rq_set_stream).  Different contexts are independent.
+ *
+ * Each entry point cites the reference interface it replaces.
+ */
+#ifndef RQ_H
+#define RQ_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RQ_API __attribute__((visibility("default")))
+#else
+#define RQ_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------- */
+#define RQ_OK 0
+#define RQ_EINVAL (-1)      /* bad argument (null pointer, size, out-of-range label) */
+#define RQ_ENOMEM (-2)      /* device or host allocation failed */
+#define RQ_ECUDA (-3)       /* a CUDA runtime call failed (message in rq_last_error) */
+#define RQ_ENONFINITE (-4)  /* NaN/Inf detected in an energy or norm (molecule.js:3198-3201) */
+#define RQ_ETIMEOUT (-5)    /* a bounded device wait gave up (batched work queue) */
+#define RQ_ENOTSUP (-6)     /* option not supported by this flavour */
+#define RQ_ENODEV (-7)      /* no CUDA device */
+
+/* ---- flavours and precision ---------------------------------------------------------- */
+typedef enum {
+  RQ_FLAVOR_MOLECULE_JS = 0, /* molecule.js WGSL step (r_c exclusion, W level set, weighted Jacobi) */
+  RQ_FLAVOR_SOLVER_PY = 1,   /* cloud/solver.py CUDA-C step (Jacobi every 2, labels every 100) */
+  RQ_FLAVOR_NEW = 2          /* Gaussian nuclei, red-black multigrid, FP64 domain sums */
+} rq_flavor;
+
+typedef enum {
+  RQ_PREC_MIXED = 0, /* fp32 fields and stencils, FP64 domain sums / energies / coarsest solve */
+  RQ_PREC_FP64 = 1   /* every field FP64 (the plain path the mixed path is compared against) */
+} rq_precision;
+
+/* ---- configuration (mirrors window.USER_* of molecule.js:4-152 and the config dict of
+ *      cloud/solver.py:321-362).  Zero / negative numeric fields take the flavour default. ---- */
+typedef struct rq_config {
+  int32_t NN;               /* grid intervals per axis (USER_NN / gridN); S = NN+1 */
+  int32_t flavor;           /* rq_flavor */
+  int32_t precision;        /* rq_precision (RQ_PREC_FP64 only with RQ_FLAVOR_NEW) */
+  int32_t norm_interval;    /* normalise every n steps (solver.py 20, molecule.js NORM_INTERVAL 20) */
+  double screen;            /* box edge in bohr (USER_SCREEN / screen); h = screen/NN */
+  double dv;                /* dt = dv*h^2; <=0 -> flavour table (molecule.js:78, solver.py:342-351) */
+  int32_t poisson_interval; /* solver.py: Poisson step every 2; new: V-cycle every n steps */
+  int32_t label_interval;   /* solver.py: 5*norm_interval (100); new: level-set step period */
+  int32_t jacobi_per_step;  /* Jacobi sweeps per Poisson step (2 in both references) */
+  int32_t steps_per_frame;  /* molecule.js STEPS_PER_FRAME (frame = steps + energy + labels) */
+  int32_t vcycle_interval;  /* molecule.js POISSON_INTERVAL (50) */
+  int32_t mg_levels;        /* new: multigrid levels (<=0: as deep as NN allows, coarsest >= 4) */
+  int32_t mg_pre, mg_post;  /* new: red-black sweeps before / after the coarse correction (2, 2) */
+  int32_t mg_coarse_sweeps; /* new: FP64 red-black sweeps on the coarsest level (64) */
+  int32_t sic;              /* molecule.js SIC (:3009-3076): 0 off (only value supported here) */
+  double boundary_speed;    /* molecule.js dt_w (0.5, :135) */
+  double curv_reg;          /* molecule.js curvReg (0.15, :34) */
+  double sigma;             /* new: Gaussian nucleus width in bohr (<=0: h) */
+  int32_t reserved[8];
+} rq_config;
+
+/* One entry of the reference atom list: a nucleus and/or one electron domain. */
+typedef struct rq_atom {
+  double i, j, k;    /* position in grid units; molecule.js stores them as u32 (:1882-1884) */
+  double Z;          /* charge of this entry's electron domain (Z_eff); 0 = no domain */
+  double Z_nuc;      /* nuclear charge placed here (molecule.js Z_nuc; the Python host sets Z) */
+  double rc;         /* pseudopotential core radius in bohr (0 = bare Coulomb) */
+  double init_zeff;  /* molecule.js initZeff for the trial psi (<=0: Z) */
+  double init_rcut;  /* molecule.js initRcut (<=0: 1e6) */
+} rq_atom;
+
+typedef struct rq_ctx rq_ctx;
+
+/* Read-only facts about a context (sizes, chosen defaults, device pointers for zero-copy). */
+typedef struct rq_info {
+  int32_t NN, S, n_atoms, flavor, precision, steps_done, mg_levels, _pad;
+  double h, dv, dt, sigma;
+  int64_t S3;
+  void* psi;   /* current psi (float* or double* by precision) */
+  void* label; /* current int32 labels */
+  void* K;     /* nuclear potential (same type as psi) */
+  void* P;     /* Hartree half-potential (same type as psi) */
+  void* W;     /* level-set field (float*) */
+  int64_t kernel_launches; /* librq kernels launched by this context so far (graph replays included) */
+} rq_info;
+
+/* Kernel classes for the per-kernel profile (CUDA events around each launch). */
+#define RQ_KC_UPDATE 0    /* fused ITP update (+ FP64 domain norms on normalisation steps) */
+#define RQ_KC_POISSON 1   /* Jacobi / red-black smoother sweeps on the fine grid */
+#define RQ_KC_LABELS 2    /* label / level-set update */
+#define RQ_KC_NORMALIZE 3 /* norm scale + apply */
+#define RQ_KC_ENERGY 4    /* per-domain energy sums */
+#define RQ_KC_FORCES 5    /* force gathers */
+#define RQ_KC_MG 6        /* multigrid transfer and coarse levels */
+#define RQ_KC_OTHER 7     /* init, potential, copies */
+#define RQ_KC_COUNT 8
+
+typedef struct rq_profile {
+  int64_t launches[RQ_KC_COUNT];  /* launches per class between begin and end */
+  double ms[RQ_KC_COUNT];         /* summed CUDA-event durations (ms) */
+  double bytes[RQ_KC_COUNT];      /* summed algorithmic bytes (reads + writes the kernel must do) */
+} rq_profile;
+
+/* Energy vector returned by rq_energy (molecule.js:3124-3195, cloud/solver.py:446-476). */
+#define RQ_E_TOTAL 0
+#define RQ_E_T 1
+#define RQ_E_EK 2
+#define RQ_E_EE 3
+#define RQ_E_KK 4
+#define RQ_E_DIPX 5
+#define RQ_E_DIPY 6
+#define RQ_E_DIPZ 7
+#define RQ_ENERGY_LEN 8
+
+/* Per-domain columns of rq_energy's per_domain (n_atoms x 5); atom.js:259-283, :340-342. */
+#define RQ_D_NORM 0
+#define RQ_D_T 1
+#define RQ_D_EK 2
+#define RQ_D_EE 3
+#define RQ_D_EIG 4
+#define RQ_DOMAIN_LEN 5
+
+/* Force methods for rq_forces. */
+#define RQ_FORCE_HF 0      /* Hellmann-Feynman integral: cloud/solver.py:282-315, molecule.js:1271-1330 */
+#define RQ_FORCE_GRADP 1   /* molecule.js gradPtotal (:1200-1269) */
+#define RQ_FORCE_ADJOINT 2 /* dE/dR of the converged energy (labels frozen); new flavour: Gaussian nuclei */
+
+/* ---- lifecycle ---------------------------------------------------------------------- */
+/* Replaces RealQMSolver.__init__ (cloud/solver.py:321-400) and molecule.js initGPU buffer
+ * set-up (:2263-2347).  Allocates every device buffer of the grid. */
+RQ_API int rq_create(const rq_config* cfg, const rq_atom* atoms, int32_t n_atoms, rq_ctx** out);
+RQ_API void rq_destroy(rq_ctx* ctx);
+/* Binds the context to a CUDA stream (cudaStream_t passed as void*; NULL = the stream the
+ * context created for itself).  Pending work on the previous stream is finished first. */
+RQ_API int rq_set_stream(rq_ctx* ctx, void* stream);
+RQ_API int rq_get_info(const rq_ctx* ctx, rq_info* info);
+RQ_API const char* rq_last_error(const rq_ctx* ctx);
+RQ_API const char* rq_status_string(int status);
+
+/* ---- state -------------------------------------------------------------------------- */
+/* RealQMSolver.initialize (cloud/solver.py:402-419): trial psi, labels, K, normalise, then
+ * 100 Poisson bootstrap steps; molecule.js uploadInitialData (:1905-2101) for that flavour;
+ * new flavour: nearest-seed labels, psi ~ exp(-|x-seed|) normalised per domain, one MG solve. */
+RQ_API int rq_initialize(rq_ctx* ctx);
+/* Move nuclei and rebuild K (cloud/solver.py:538-548, molecule.js:4563-4582 without relabel). */
+RQ_API int rq_set_atoms(rq_ctx* ctx, const rq_atom* atoms, int32_t n_atoms);
+/* Copy a full state in / out (host arrays of S^3 elements; any pointer may be NULL to skip).
+ * Labels must lie in [0, n_atoms).  Replaces window.restartWithPositions re-uploads
+ * (molecule.js:2127-2147) and direct access to RealQMSolver.U / .label. */
+RQ_API int rq_upload_state(rq_ctx* ctx, const float* psi, const int32_t* label, const float* W, const float* P);
+RQ_API int rq_download_state(rq_ctx* ctx, float* psi, int32_t* label, float* W, float* P);
+RQ_API int rq_upload_state_f64(rq_ctx* ctx, const double* psi, const double* P);
+RQ_API int rq_download_state_f64(rq_ctx* ctx, double* psi, double* P, double* K);
+RQ_API int rq_download_K(rq_ctx* ctx, float* K);
+
+/* ---- the solver step ------------------------------------------------------------------- */
+/* n solver steps on the flavour schedule: the loop body of RealQMSolver.run
+ * (cloud/solver.py:561-591) or the s-loop of molecule.js doSteps (:2829-3006) with the
+ * frame tail (:3009-3104) every steps_per_frame steps.  Asynchronous on the stream. */
+RQ_API int rq_step(rq_ctx* ctx, int32_t n_steps);
+/* Energies (FP64 sums).  out[RQ_ENERGY_LEN]; per_domain may be NULL or n_atoms*RQ_DOMAIN_LEN.
+ * Synchronises the stream.  Returns RQ_ENONFINITE if any component is NaN/Inf. */
+RQ_API int rq_energy(rq_ctx* ctx, double* out, double* per_domain);
+/* Electronic forces on every atom entry (n_atoms x 3, FP64), without nuclear-nuclear terms.
+ * cloud/solver.py _compute_forces (:478-502); molecule.js gradPtotal / HF (:1200-1330). */
+RQ_API int rq_forces(rq_ctx* ctx, int32_t method, double* F);
+/* Nuclear-nuclear energy and forces with the flavour's softening (host-side terms of
+ * cloud/solver.py:462-474, :504-520 and molecule.js:3170-3185, :3218-3242). */
+RQ_API int rq_nuclear_terms(rq_ctx* ctx, double* E_KK, double* F /* n_atoms x 3 or NULL */);
+/* Step until |E_n - E_{n-1}| < tol_dE between checks every check_interval steps. */
+RQ_API int rq_solve(rq_ctx* ctx, double tol_dE, int32_t max_steps, int32_t check_interval, int32_t* steps_taken,
+             double* E_final);
+RQ_API int rq_synchronize(rq_ctx* ctx);
+/* Per-kernel timing (the reference only times whole frames, molecule.js:2823, :3168,
+ * and whole runs, cloud/solver.py:559-597): between begin and end every launch of the context
+ * is bracketed by CUDA events on its stream.  Work recorded while profiling runs eagerly
+ * (no CUDA-graph replay).  end synchronises and fills *out. */
+RQ_API int rq_profile_begin(rq_ctx* ctx);
+RQ_API int rq_profile_end(rq_ctx* ctx, rq_profile* out);
+
+/* ---- single kernels on caller-owned device memory (zero-copy PyTorch interop) ---------------
+ * Pointers are device pointers of S^3 elements; `stream` is a cudaStream_t or NULL.  These run
+ * exactly the kernels rq_step uses and exist for kernel-level parity checks and custom drivers. */
+/* cloud/solver.py:61-90 updateU (S^3 interior update, boundary written 0). */
+RQ_API int rq_kernel_update_sp(const float* U, float* Unew, const float* K, const float* P, const int32_t* label,
+                        int32_t S, float half_dv, float dtv, void* stream);
+/* cloud/solver.py:181-208 computeRho + jacobiStep fused: Pnew = (sum P + coeff*U^2*h2)/6. */
+RQ_API int rq_kernel_jacobi_sp(const float* P, float* Pnew, const float* U, int32_t S, float h2, float coeff, void* stream);
+/* cloud/solver.py:92-147 boundaryEvolve with snapshot semantics (read labelIn, write labelOut). */
+RQ_API int rq_kernel_labels_sp(const int32_t* labelIn, int32_t* labelOut, const float* atoms5, int32_t n_atoms,
+                        int32_t S, float h, float h2, void* stream);
+/* cloud/solver.py:16-59 initTrial (U, label, K, bestU). */
+RQ_API int rq_kernel_init_sp(float* U, int32_t* label, float* K, float* bestU, const float* atoms5, int32_t n_atoms,
+                      int32_t S, float h, float h2, void* stream);
+/* cloud/solver.py:149-179 recomputeK. */
+RQ_API int rq_kernel_recompute_k_sp(float* K, const float* atoms5, int32_t n_atoms, int32_t S, float h, float h2,
+                             void* stream);
+/* FP64 per-label sums of psi^2*h3 (label clipped to [0,n) like cloud/solver.py:427), then
+ * normalizeU (:210-225) with scale sqrt(Z/n).  norms_out (n doubles, device) may be NULL. */
+RQ_API int rq_kernel_normalize_sp(float* U, const int32_t* label, const float* Zeff, int32_t n_atoms, int32_t S, float h3,
+                           double* norms_out, void* stream);
+/* Per-label FP64 (norm, T, V_eK, V_ee) of cloud/solver.py:246-256 into per_domain (n x 4, device). */
+RQ_API int rq_kernel_energy_sp(const float* U, const float* K, const float* P, const int32_t* label, int32_t n_atoms,
+                        int32_t S, float h, float h3, double* per_domain, void* stream);
+/* cloud/solver.py:282-315 computeForceAll with FP64 accumulation into F (n x 3, device). */
+RQ_API int rq_kernel_forces_hf_sp(const float* U, const float* atoms5, int32_t n_atoms, int32_t S, float h, float h2,
+                           float h3, double* F, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RQ_H */

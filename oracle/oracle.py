@@ -1,0 +1,328 @@
+"""Python face of the oracle (TEST INFRASTRUCTURE ONLY).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference arm
+may import this module.  It provides
+
+* ``build()``            -- compile oracle/rq_oracle.c (and, when the reference tree is
+                            present, the reference kernels via oracle/ref_build.py);
+* ``O``                  -- numpy wrappers over the C restatement (oracle/rq_oracle.c);
+* ``RefKernels``         -- numpy wrappers over the reference's own cloud/solver.py
+                            kernels compiled for the host (oracle/_ref/libsolverpy_ref.so);
+* ``SolverPyDriver``     -- the schedule of ``RealQMSolver.run`` (cloud/solver.py:402-634)
+                            restated over either kernel set, used as the CPU baseline and
+                            as the multi-step oracle of the solver.py flavour.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SRC = os.path.join(HERE, "rq_oracle.c")
+ORACLE_LIB = os.path.join(HERE, "librq_oracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libsolverpy_ref.so")
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_i, _i64, _f, _d = C.c_int, C.c_int64, C.c_float, C.c_double
+
+
+def build(force: bool = False, with_reference: bool = True) -> None:
+    """Compile the C oracle (and the reference kernels when the reference tree exists)."""
+    if force or not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < os.path.getmtime(ORACLE_SRC):
+        subprocess.check_call(["gcc", "-O2", "-fopenmp", "-fPIC", "-shared", "-ffp-contract=off",
+                               "-fno-fast-math", ORACLE_SRC, "-o", ORACLE_LIB, "-lm"])
+    if with_reference:
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("rq_ref_build", os.path.join(HERE, "ref_build.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        try:
+            mod.build(quiet=True)
+        except FileNotFoundError:
+            pass  # no reference tree and no prebuilt library: reference-pinned tests skip
+
+
+class MjAtom(C.Structure):
+    """molecule.js atom record (molecule.js:183-191) as the oracle takes it."""
+    _fields_ = [("posI", C.c_uint32), ("posJ", C.c_uint32), ("posK", C.c_uint32), ("Z", C.c_float),
+                ("rc", C.c_float), ("Z_nuc", C.c_float), ("initZeff", C.c_float), ("initRcut", C.c_float)]
+
+
+def mj_atoms(rows):
+    """rows: iterable of dicts with i,j,k,Z[,rc,Z_nuc,initZeff,initRcut] -> ctypes array.
+
+    Positions are truncated to unsigned integers like molecule.js:1882-1884."""
+    rows = list(rows)
+    arr = (MjAtom * len(rows))()
+    for n, a in enumerate(rows):
+        arr[n].posI, arr[n].posJ, arr[n].posK = int(a["i"]), int(a["j"]), int(a["k"])
+        arr[n].Z = a["Z"]
+        arr[n].rc = a.get("rc", 0.0)
+        arr[n].Z_nuc = a.get("Z_nuc", a["Z"])
+        arr[n].initZeff = a.get("initZeff", a["Z"]) or a["Z"]
+        arr[n].initRcut = a.get("initRcut", 1e6)
+    return arr
+
+
+class _Oracle:
+    def __init__(self):
+        build(with_reference=False)
+        L = C.CDLL(ORACLE_LIB)
+        sig = {
+            "orc_sp_init_trial": [_f32p, _i32p, _f32p, _f32p, _f32p, _i, _i, _f, _f],
+            "orc_sp_recompute_K": [_f32p, _f32p, _i, _i, _f, _f],
+            "orc_sp_update": [_f32p, _f32p, _f32p, _f32p, _i32p, _i, _f, _f],
+            "orc_sp_boundary_snapshot": [_i32p, _i32p, _f32p, _i, _i, _f, _f],
+            "orc_sp_boundary_inplace_lex": [_i32p, _f32p, _i, _i, _f, _f],
+            "orc_sp_jacobi": [_f32p, _f32p, _f32p, _i, _f, _f],
+            "orc_sp_norms_f32_seq": [_f32p, _i32p, _i64, _i, _f, _f32p],
+            "orc_sp_norms_f64": [_f32p, _i32p, _i, _i, _d, _f64p],
+            "orc_sp_normalize": [_f32p, _i32p, _f32p, _f32p, _i64, _i],
+            "orc_sp_energy_blocktree": [_f32p, _f32p, _f32p, _i32p, _f32p, _i, _f, _f, _i],
+            "orc_sp_energy_f64": [_f32p, _f32p, _f32p, _i32p, _i, _d, _d, _f64p, _i, C.c_void_p],
+            "orc_sp_forces": [_f32p, _f32p, _i, _i, _f, _f, _f, _f64p],
+            "orc_mj_update": [_f32p, _f32p, _f32p, _u32p, _f32p, C.c_void_p, _i, _i, _i, _f, _f, _f],
+            "orc_mj_evolve_boundary": [_u32p, _u32p, _f32p, _f32p, _i, _f, _f],
+            "orc_mj_jacobi": [_f32p, _f32p, _f32p, _i, _f, _f],
+            "orc_mj_rho": [_f32p, _f32p, _i],
+            "orc_mj_residual": [_f32p, _f32p, _f32p, _i, _f, _f],
+            "orc_mj_restrict": [_f32p, _f32p, _i, _i],
+            "orc_mj_coarse_smooth": [_f32p, _f32p, _f32p, _i, _f],
+            "orc_mj_prolong": [_f32p, _f32p, _i, _i],
+            "orc_mj_norms_fixed": [_f32p, _u32p, _i, _f, _i, _u32p, _f32p],
+            "orc_mj_normalize": [_f32p, _f32p, _u32p, C.c_void_p, _i],
+            "orc_mj_energy": [_f32p, _f32p, _f32p, _u32p, C.c_void_p, _i, _f, _f, _f, _f64p],
+            "orc_mj_force_gradP": [_f32p, C.c_void_p, _i, _i, _f, _i, _f64p],
+            "orc_mj_force_hf": [_f32p, C.c_void_p, _i, _i, _f, _f64p],
+            "orc_mj_init": [_f32p, _f32p, _u32p, C.c_void_p, _i, _i, _f, _f],
+            "orc_nm_potential": [_f64p, _f64p, _f64p, _i, _i, _d, _d],
+            "orc_nm_update": [_f64p, _f64p, _f64p, _f64p, _i32p, _i, _d, _d],
+            "orc_nm_vcycle": [_f64p, _f64p, _i, _d, _i, _i, _i, _i],
+            "orc_nm_energy": [_f64p, _f64p, _f64p, _i32p, _i, _d, _f64p, _i, _f64p],
+            "orc_nm_normalize": [_f64p, _i32p, _i64, _i, _f64p, _f64p],
+            "orc_nm_force": [_f64p, _f64p, _f64p, _i, _i, _d, _d, _f64p],
+        }
+        for name, argt in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = argt
+            fn.restype = None
+            setattr(self, name[4:], fn)
+        self.lib = L
+
+
+_O = None
+
+
+def O() -> _Oracle:
+    """The loaded C oracle (compiled on first use)."""
+    global _O
+    if _O is None:
+        _O = _Oracle()
+    return _O
+
+
+class RefKernels:
+    """The reference's own cloud/solver.py kernels compiled for the host (oracle/_ref)."""
+
+    SIGS = {
+        "initTrial": ["p", "p", "p", "p", "p", "i", "i", "f", "f"],
+        "updateU": ["p", "p", "p", "p", "p", "i", "f", "f"],
+        "boundaryEvolve": ["p", "p", "p", "i", "i", "f", "f", "f", "f"],
+        "recomputeK": ["p", "p", "i", "i", "f", "f"],
+        "computeRho": ["p", "p", "i"],
+        "jacobiStep": ["p", "p", "p", "i", "f", "f"],
+        "normalizeU": ["p", "p", "p", "p", "i", "i", "f"],
+        "computeForceAll": ["p", "p", "p", "i", "i", "f", "f", "f"],
+    }
+
+    def __init__(self, path: str = REF_LIB):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = C.CDLL(path)
+        tmap = {"p": C.c_void_p, "i": C.c_int, "f": C.c_float}
+        for name, s in self.SIGS.items():
+            for pre in ("rqref_launch_", "rqref_launch_serial_"):
+                fn = getattr(self.lib, pre + name)
+                fn.argtypes = [C.c_int, C.c_int] + [tmap[c] for c in s]
+                fn.restype = None
+
+    def launch(self, name, grid, block, args, serial=False):
+        conv = []
+        for a in args:
+            if isinstance(a, np.ndarray):
+                assert a.flags.c_contiguous
+                conv.append(a.ctypes.data)
+            elif isinstance(a, (np.floating, float)):
+                conv.append(float(a))
+            else:
+                conv.append(int(a))
+        fn = getattr(self.lib, ("rqref_launch_serial_" if serial else "rqref_launch_") + name)
+        fn(int(grid), int(block), *conv)
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def solverpy_dv(n_elec: int) -> float:
+    """Time-step table of cloud/solver.py:342-351."""
+    if n_elec > 500:
+        return 0.005
+    if n_elec > 200:
+        return 0.01
+    if n_elec > 100:
+        return 0.02
+    if n_elec > 30:
+        return 0.03
+    return 0.12
+
+
+class SolverPyDriver:
+    """Restatement of the RealQMSolver state and schedule (cloud/solver.py:321-634).
+
+    ``kernels="reference"`` runs the reference's own kernels (oracle/_ref) with
+    numpy norms exactly as the reference host code computes them (f32 np.add.at);
+    ``kernels="oracle"`` runs the C restatement with FP64 per-domain norms, which is
+    the arithmetic the CUDA product uses.  Dynamics are not restated here.
+    """
+
+    def __init__(self, config: dict, kernels: str = "oracle", label_mode: str = "snapshot"):
+        self.label_mode = label_mode
+        self.NN = int(config["gridN"])
+        self.S = self.NN + 1
+        self.S3 = self.S ** 3
+        self.h = config["screen"] / self.NN
+        self.h2 = self.h * self.h
+        self.h3 = self.h ** 3
+        N2 = self.NN // 2
+        atoms = config["atoms"]
+        self.nAtoms = len(atoms)
+        self.Z_eff = np.array([a["Z"] for a in atoms], dtype=np.float32)
+        self.atom_pos = np.array([[a["i"], a["j"], a.get("k", N2)] for a in atoms], dtype=np.float32)
+        self.atom_rc = np.array([a.get("rc", 0) for a in atoms], dtype=np.float32)
+        self.nElec = int((self.Z_eff > 0).sum())
+        self.dv = float(config.get("dv", solverpy_dv(self.nElec)))
+        self.half_dv = 0.5 * self.dv
+        self.dtv = self.dv * self.h2
+        self.U = np.zeros(self.S3, np.float32)
+        self.U2 = np.zeros(self.S3, np.float32)
+        self.K = np.zeros(self.S3, np.float32)
+        self.P = np.zeros(self.S3, np.float32)
+        self.P2 = np.zeros(self.S3, np.float32)
+        self.rho = np.zeros(self.S3, np.float32)
+        self.label = np.zeros(self.S3, np.int32)
+        self.label2 = np.zeros(self.S3, np.int32)
+        self.bestU = np.zeros(self.S3, np.float32)
+        self.atoms5 = np.zeros((self.nAtoms, 5), np.float32)
+        for n, a in enumerate(atoms):
+            self.atoms5[n] = [a["i"], a["j"], a.get("k", N2), a["Z"], a.get("rc", 0)]
+        self.atoms5 = np.ascontiguousarray(self.atoms5.reshape(-1))
+        self.kernels = kernels
+        self.block = 256
+        self.grid = (self.S3 + self.block - 1) // self.block
+        self.R = RefKernels() if kernels == "reference" else None
+        self.E = self.E_T = self.E_eK = self.E_ee = self.E_KK = 0.0
+        self.steps_done = 0
+
+    # -- kernels ---------------------------------------------------------
+    def initialize(self, bootstrap: int = 100):
+        if self.R:
+            self.R.launch("initTrial", self.grid, self.block,
+                          (self.U, self.label, self.K, self.bestU, self.atoms5, self.nAtoms, self.S,
+                           np.float32(self.h), np.float32(self.h2)))
+        else:
+            O().sp_init_trial(self.U, self.label, self.K, self.bestU, self.atoms5, self.nAtoms, self.S,
+                              self.h, self.h2)
+        self.normalize()
+        for _ in range(bootstrap):
+            self.poisson_step()
+
+    def normalize(self):
+        if self.R:
+            norms = np.zeros(self.nAtoms, np.float32)
+            O().sp_norms_f32_seq(self.U, self.label, self.S3, self.nAtoms, np.float32(self.h3), norms)
+        else:
+            n64 = np.zeros(self.nAtoms, np.float64)
+            O().sp_norms_f64(self.U, self.label, self.S, self.nAtoms, self.h3, n64)
+            norms = n64.astype(np.float32)
+        if self.R:
+            self.R.launch("normalizeU", self.grid, self.block,
+                          (self.U, self.label, norms, self.Z_eff, self.S3, self.nAtoms, np.float32(self.h3)))
+        else:
+            O().sp_normalize(self.U, self.label, norms, self.Z_eff, self.S3, self.nAtoms)
+
+    def poisson_step(self):
+        coeff = np.float32(2.0 * np.pi)
+        if self.R:
+            self.R.launch("computeRho", self.grid, self.block, (self.rho, self.U, self.S3))
+            for _ in range(2):
+                self.R.launch("jacobiStep", self.grid, self.block,
+                              (self.P, self.P2, self.rho, self.S, np.float32(self.h2), coeff))
+                self.P, self.P2 = self.P2, self.P
+        else:
+            for _ in range(2):
+                O().sp_jacobi(self.P, self.P2, self.U, self.S, self.h2, coeff)
+                self.P, self.P2 = self.P2, self.P
+
+    def update(self):
+        if self.R:
+            self.R.launch("updateU", self.grid, self.block,
+                          (self.U, self.U2, self.K, self.P, self.label, self.S, np.float32(self.half_dv),
+                           np.float32(self.dtv)))
+        else:
+            O().sp_update(self.U, self.U2, self.K, self.P, self.label, self.S, self.half_dv, self.dtv)
+        self.U, self.U2 = self.U2, self.U
+
+    def boundary(self):
+        # snapshot semantics by default (the reference writes in place, which races on a
+        # GPU); "inplace_lex" reproduces the reference kernel run serially in index order
+        if self.label_mode == "inplace_lex":
+            O().sp_boundary_inplace_lex(self.label, self.atoms5, self.nAtoms, self.S, self.h, self.h2)
+            return
+        O().sp_boundary_snapshot(self.label, self.label2, self.atoms5, self.nAtoms, self.S, self.h, self.h2)
+        self.label, self.label2 = self.label2, self.label
+
+    def step(self, step: int, norm_interval=20, poisson_interval=2):
+        if step % poisson_interval == 0:
+            self.poisson_step()
+        self.update()
+        if step % norm_interval == 0:
+            self.normalize()
+        if step % (norm_interval * 5) == 0:
+            self.boundary()
+
+    def run(self, total_steps: int, norm_interval=20, poisson_interval=2):
+        """Continue the schedule for total_steps (the step counter persists across calls)."""
+        for _ in range(total_steps):
+            self.steps_done += 1
+            self.step(self.steps_done, norm_interval, poisson_interval)
+
+    def energy(self):
+        out = np.zeros(3, np.float64)
+        O().sp_energy_f64(self.U, self.K, self.P, self.label, self.S, self.h, self.h3, out, 0, None)
+        self.E_T, self.E_eK, self.E_ee = map(float, out)
+        self.E_KK = e_kk_solverpy(self.atom_pos, self.Z_eff, self.h)
+        self.E = self.E_T + self.E_eK + self.E_ee + self.E_KK
+        return self.E
+
+
+def e_kk_solverpy(atom_pos, Z_eff, h) -> float:
+    """cloud/solver.py:462-474: sum Za Zb / sqrt(d^2 + h^2) over active pairs (FP64)."""
+    e = 0.0
+    n = len(Z_eff)
+    for a in range(n):
+        if Z_eff[a] <= 0:
+            continue
+        for b in range(a + 1, n):
+            if Z_eff[b] <= 0:
+                continue
+            d = (np.asarray(atom_pos[a], np.float64) - np.asarray(atom_pos[b], np.float64)) * h
+            e += float(Z_eff[a]) * float(Z_eff[b]) / math.sqrt(float(d @ d) + h * h)
+    return e

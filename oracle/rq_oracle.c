@@ -1,0 +1,952 @@
+/*
+ * rq_oracle.c -- CPU restatement of the RealQM solver step (TEST INFRASTRUCTURE).
+ *
+ * This file is the oracle: tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline leg call it to check or time the CUDA product.  The product path
+ * (realmolecule_b200/) never links or calls it.
+ *
+ * Three flavours are restated, each function citing the reference lines it follows:
+ *   sp_*  cloud/solver.py   (CUDA-C strings compiled by CuPy/NVRTC)
+ *   mj_*  molecule.js       (WGSL compute shaders)
+ *   nm_*  the FP64 "new method" (Gaussian nuclei, red-black multigrid), which has no
+ *         reference counterpart; its parity is "FP64 oracle of the same method".
+ *
+ * Arithmetic rules: f32 functions use plain IEEE single operations in the order the
+ * reference writes them (built with -ffp-contract=off, no fast-math), so integer
+ * and label results are bit-exact and field updates are bit-exact whenever the
+ * CUDA kernel uses the same non-contracted order.  Reductions are FP64 with a
+ * fixed per-plane order so that results do not depend on the thread count.
+ *
+ * Grid convention (both references): S = NN+1 points per axis, linear index
+ * id = i*S*S + j*S + k with k fastest (cloud/solver.py:24-26, molecule.js:273-276);
+ * the outer planes i,j,k in {0, NN} are Dirichlet boundary.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define IDX(i, j, k, S) ((int64_t)(i) * (S) * (S) + (int64_t)(j) * (S) + (k))
+
+static inline int interior(int i, int j, int k, int NN) {
+  return i >= 1 && i < NN && j >= 1 && j < NN && k >= 1 && k < NN;
+}
+
+/* ======================================================================
+ * solver.py flavour
+ * ==================================================================== */
+
+/* cloud/solver.py:16-59 initTrial: K = sum Z/r_soft, trial u = Z^2/sqrt(pi) e^{-Zr},
+ * label = argmax (first wins ties).  atoms5 = [i,j,k,Z,rc] floats per atom. */
+void orc_sp_init_trial(float* U, int32_t* label, float* K, float* bestU, const float* atoms5,
+                       int nAtoms, int S, float h, float h2) {
+  const int NN = S - 1;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < S; ++i)
+    for (int j = 0; j < S; ++j)
+      for (int k = 0; k < S; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        if (!interior(i, j, k, NN)) { U[id] = 0.f; label[id] = 0; K[id] = 0.f; bestU[id] = 0.f; continue; }
+        float xi = (float)i * h, yj = (float)j * h, zk = (float)k * h;
+        float bU = 0.f, Kval = 0.f;
+        int bestN = 0;
+        const float inv_sqrt_pi = 0.5641895835f;
+        for (int n = 0; n < nAtoms; ++n) {
+          float Za = atoms5[n * 5 + 3];
+          if (Za <= 0.f) continue;
+          float rc = atoms5[n * 5 + 4];
+          float dx = xi - atoms5[n * 5 + 0] * h;
+          float dy = yj - atoms5[n * 5 + 1] * h;
+          float dz = zk - atoms5[n * 5 + 2] * h;
+          float r2 = dx * dx + dy * dy + dz * dz;
+          float r = (rc > 0.f) ? fmaxf(sqrtf(r2 + 0.04f * h2), rc) : sqrtf(r2 + h2);
+          Kval += Za / r;
+          float uT = Za * Za * inv_sqrt_pi * expf(-Za * r);
+          if (uT > bU) { bU = uT; bestN = n; }
+        }
+        K[id] = Kval; bestU[id] = bU; label[id] = bestN; U[id] = bU;
+      }
+}
+
+/* cloud/solver.py:149-179 recomputeK (same K as initTrial, no trial/labels). */
+void orc_sp_recompute_K(float* K, const float* atoms5, int nAtoms, int S, float h, float h2) {
+  const int NN = S - 1;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < S; ++i)
+    for (int j = 0; j < S; ++j)
+      for (int k = 0; k < S; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        if (!interior(i, j, k, NN)) { K[id] = 0.f; continue; }
+        float xi = (float)i * h, yj = (float)j * h, zk = (float)k * h, Kval = 0.f;
+        for (int n = 0; n < nAtoms; ++n) {
+          float Za = atoms5[n * 5 + 3];
+          if (Za <= 0.f) continue;
+          float rc = atoms5[n * 5 + 4];
+          float dx = xi - atoms5[n * 5 + 0] * h;
+          float dy = yj - atoms5[n * 5 + 1] * h;
+          float dz = zk - atoms5[n * 5 + 2] * h;
+          float r2 = dx * dx + dy * dy + dz * dz;
+          float r = (rc > 0.f) ? fmaxf(sqrtf(r2 + 0.04f * h2), rc) : sqrtf(r2 + h2);
+          Kval += Za / r;
+        }
+        K[id] = Kval;
+      }
+}
+
+/* cloud/solver.py:61-90 updateU: same-label Neumann 7-point Laplacian, then
+ * Unew = u + half_dv*lap + dtv*(K - 2P)*u; boundary planes written 0. */
+void orc_sp_update(const float* U, float* Unew, const float* K, const float* P, const int32_t* label,
+                   int S, float half_dv, float dtv) {
+  const int NN = S - 1;
+  const int64_t S2 = (int64_t)S * S;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < S; ++i)
+    for (int j = 0; j < S; ++j)
+      for (int k = 0; k < S; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        if (!interior(i, j, k, NN)) { Unew[id] = 0.f; continue; }
+        int32_t L = label[id];
+        float u = U[id];
+        float uip = (label[id + S2] == L) ? U[id + S2] : u;
+        float uim = (label[id - S2] == L) ? U[id - S2] : u;
+        float ujp = (label[id + S] == L) ? U[id + S] : u;
+        float ujm = (label[id - S] == L) ? U[id - S] : u;
+        float ukp = (label[id + 1] == L) ? U[id + 1] : u;
+        float ukm = (label[id - 1] == L) ? U[id - 1] : u;
+        float lap = uip + uim + ujp + ujm + ukp + ukm - 6.0f * u;
+        Unew[id] = u + half_dv * lap + dtv * (K[id] - 2.0f * P[id]) * u;
+      }
+}
+
+/* cloud/solver.py:92-147 boundaryEvolve decision for one interior cell, reading
+ * labels from `lab`.  Returns the new label (== current label when no flip). */
+static inline int32_t sp_boundary_cell(const int32_t* lab, const float* atoms5, int nAtoms, int S,
+                                       int i, int j, int k, float h, float h2) {
+  const int64_t S2 = (int64_t)S * S;
+  int64_t id = IDX(i, j, k, S);
+  float xi = (float)i * h, yj = (float)j * h, zk = (float)k * h;
+  int32_t cur = lab[id];
+  int otherCount = 0;
+  const int64_t nb[6] = {id + S2, id - S2, id + S, id - S, id + 1, id - 1};
+  for (int n = 0; n < 6; ++n)
+    if (lab[nb[n]] != cur) otherCount++;
+  if (otherCount == 0) return cur;
+  float curScore = 0.f, bestScore = 0.f;
+  int32_t bestN = cur;
+  for (int n = 0; n < nAtoms; ++n) {
+    float Za = atoms5[n * 5 + 3];
+    if (Za <= 0.f) continue;
+    float dx = xi - atoms5[n * 5 + 0] * h;
+    float dy = yj - atoms5[n * 5 + 1] * h;
+    float dz = zk - atoms5[n * 5 + 2] * h;
+    float r2 = dx * dx + dy * dy + dz * dz + h2;
+    float score = Za / sqrtf(r2);
+    if (n == cur) curScore = score;
+    if (score > bestScore) { bestScore = score; bestN = n; }
+  }
+  if (bestN != cur && bestScore > curScore * 1.1f && otherCount >= 2) return bestN;
+  return cur;
+}
+
+/* Snapshot semantics (read labelIn, write labelOut): the deterministic form of
+ * cloud/solver.py:92-147, whose in-place write (:143-145) races on a GPU. */
+void orc_sp_boundary_snapshot(const int32_t* labelIn, int32_t* labelOut, const float* atoms5, int nAtoms,
+                              int S, float h, float h2) {
+  const int NN = S - 1;
+  const int64_t S3 = (int64_t)S * S * S;
+  memcpy(labelOut, labelIn, (size_t)S3 * sizeof(int32_t));
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k)
+        labelOut[IDX(i, j, k, S)] = sp_boundary_cell(labelIn, atoms5, nAtoms, S, i, j, k, h, h2);
+}
+
+/* In-place, lexicographic order: what the reference kernel produces when its
+ * threads run one after another in index order.  Used only to pin the decision
+ * rule against the reference kernel run serially on the host. */
+void orc_sp_boundary_inplace_lex(int32_t* label, const float* atoms5, int nAtoms, int S, float h, float h2) {
+  const int NN = S - 1;
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k)
+        label[IDX(i, j, k, S)] = sp_boundary_cell(label, atoms5, nAtoms, S, i, j, k, h, h2);
+}
+
+/* cloud/solver.py:181-208 computeRho + jacobiStep: Pnew = (sum_6 P + coeff*rho*h2)/6. */
+void orc_sp_jacobi(const float* P, float* Pnew, const float* U, int S, float h2, float coeff) {
+  const int NN = S - 1;
+  const int64_t S2 = (int64_t)S * S;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < S; ++i)
+    for (int j = 0; j < S; ++j)
+      for (int k = 0; k < S; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        if (!interior(i, j, k, NN)) { Pnew[id] = 0.f; continue; }
+        float rho = U[id] * U[id];
+        float sumN = P[id + S2] + P[id - S2] + P[id + S] + P[id - S] + P[id + 1] + P[id - 1];
+        Pnew[id] = (sumN + coeff * rho * h2) / 6.0f;
+      }
+}
+
+/* cloud/solver.py:421-427 norms as numpy/cupyx computes them on the host:
+ * rho = U*U*h3 in f32, scatter_add in index order into f32 (np.add.at). */
+void orc_sp_norms_f32_seq(const float* U, const int32_t* label, int64_t S3, int nAtoms, float h3, float* norms) {
+  for (int n = 0; n < nAtoms; ++n) norms[n] = 0.f;
+  for (int64_t id = 0; id < S3; ++id) {
+    int32_t l = label[id];
+    if (l < 0) l = 0;
+    if (l > nAtoms - 1) l = nAtoms - 1;
+    norms[l] += (U[id] * U[id]) * h3;
+  }
+}
+
+/* Per-label FP64 sums of psi^2 h^3 over ALL points (the reference sums the whole
+ * array; boundary points are zero), with the label clipped like :427. */
+void orc_sp_norms_f64(const float* U, const int32_t* label, int S, int nAtoms, double h3, double* norms) {
+  const int64_t S2 = (int64_t)S * S;
+  double* part = (double*)calloc((size_t)S * nAtoms, sizeof(double));
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < S; ++i) {
+    double* pp = part + (size_t)i * nAtoms;
+    for (int64_t q = 0; q < S2; ++q) {
+      int64_t id = i * S2 + q;
+      int32_t l = label[id];
+      if (l < 0) l = 0;
+      if (l > nAtoms - 1) l = nAtoms - 1;
+      double u = (double)U[id];
+      pp[l] += u * u * h3;
+    }
+  }
+  for (int n = 0; n < nAtoms; ++n) norms[n] = 0.0;
+  for (int i = 0; i < S; ++i)
+    for (int n = 0; n < nAtoms; ++n) norms[n] += part[(size_t)i * nAtoms + n];
+  free(part);
+}
+
+/* cloud/solver.py:210-225 normalizeU: U *= sqrt(Z/n) for labels in range with Z>0, n>1e-20. */
+void orc_sp_normalize(float* U, const int32_t* label, const float* norms, const float* Zeff, int64_t S3, int nAtoms) {
+#pragma omp parallel for schedule(static)
+  for (int64_t id = 0; id < S3; ++id) {
+    int32_t l = label[id];
+    if (l < 0 || l >= nAtoms) continue;
+    float z = Zeff[l];
+    if (z <= 0.f) continue;
+    float n = norms[l];
+    if (n > 1e-20f) U[id] *= sqrtf(z / n);
+  }
+}
+
+/* cloud/solver.py:227-280 computeEnergy, restated: per thread T/VeK/Vee terms in f32,
+ * a shared-memory tree per block of `block` threads, then block partials added in
+ * block order (the reference adds them with float atomics in arbitrary order). */
+void orc_sp_energy_blocktree(const float* U, const float* K, const float* P, const int32_t* label, float* out,
+                             int S, float h, float h3, int block) {
+  const int NN = S - 1;
+  const int64_t S2 = (int64_t)S * S, S3 = S2 * S;
+  const int64_t nblk = (S3 + block - 1) / block;
+  float* bp = (float*)malloc(sizeof(float) * 3 * (size_t)nblk);
+#pragma omp parallel
+  {
+    float* sd = (float*)malloc(sizeof(float) * 3 * (size_t)block);
+#pragma omp for schedule(static)
+    for (int64_t b = 0; b < nblk; ++b) {
+      for (int t = 0; t < block; ++t) {
+        int64_t id = b * block + t;
+        float lT = 0.f, lK = 0.f, lE = 0.f;
+        if (id < S3) {
+          int i = (int)(id / S2), j = (int)((id / S) % S), k = (int)(id % S);
+          if (interior(i, j, k, NN)) {
+            float u = U[id], rho = u * u;
+            int32_t L = label[id];
+            float dui = (label[id + S2] == L) ? U[id + S2] - u : 0.f;
+            float duj = (label[id + S] == L) ? U[id + S] - u : 0.f;
+            float duk = (label[id + 1] == L) ? U[id + 1] - u : 0.f;
+            lT = 0.5f * (dui * dui + duj * duj + duk * duk) * h;
+            lK = -K[id] * rho * h3;
+            lE = P[id] * rho * h3;
+          }
+        }
+        sd[t] = lT; sd[t + block] = lK; sd[t + 2 * block] = lE;
+      }
+      for (int s = block / 2; s > 0; s >>= 1)
+        for (int t = 0; t < s; ++t) {
+          sd[t] += sd[t + s]; sd[t + block] += sd[t + block + s]; sd[t + 2 * block] += sd[t + 2 * block + s];
+        }
+      bp[3 * b] = sd[0]; bp[3 * b + 1] = sd[block]; bp[3 * b + 2] = sd[2 * block];
+    }
+    free(sd);
+  }
+  out[0] = out[1] = out[2] = 0.f;
+  for (int64_t b = 0; b < nblk; ++b) { out[0] += bp[3 * b]; out[1] += bp[3 * b + 1]; out[2] += bp[3 * b + 2]; }
+  free(bp);
+}
+
+/* Same energy terms (cloud/solver.py:246-256) accumulated in FP64, total and per
+ * label: out[0..2] = T, V_eK, V_ee; per_domain (nDom x 4, may be NULL) = norm, T,
+ * V_eK, V_ee of each label (labels outside [0,nDom) are skipped there). */
+void orc_sp_energy_f64(const float* U, const float* K, const float* P, const int32_t* label, int S, double h,
+                       double h3, double* out, int nDom, double* per_domain) {
+  const int NN = S - 1;
+  const int64_t S2 = (int64_t)S * S;
+  double* part = (double*)calloc((size_t)S * 3, sizeof(double));
+  double* pd = per_domain ? (double*)calloc((size_t)S * nDom * 4, sizeof(double)) : NULL;
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i) {
+    double t = 0, vk = 0, ve = 0;
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        double u = U[id], rho = u * u;
+        int32_t L = label[id];
+        double dui = (label[id + S2] == L) ? (double)U[id + S2] - u : 0.0;
+        double duj = (label[id + S] == L) ? (double)U[id + S] - u : 0.0;
+        double duk = (label[id + 1] == L) ? (double)U[id + 1] - u : 0.0;
+        double lt = 0.5 * (dui * dui + duj * duj + duk * duk) * h;
+        double lk = -(double)K[id] * rho * h3, le = (double)P[id] * rho * h3;
+        t += lt; vk += lk; ve += le;
+        if (pd && L >= 0 && L < nDom) {
+          double* q = pd + ((size_t)i * nDom + L) * 4;
+          q[0] += rho * h3; q[1] += lt; q[2] += lk; q[3] += le;
+        }
+      }
+    part[3 * i] = t; part[3 * i + 1] = vk; part[3 * i + 2] = ve;
+  }
+  out[0] = out[1] = out[2] = 0;
+  for (int i = 0; i < S; ++i) { out[0] += part[3 * i]; out[1] += part[3 * i + 1]; out[2] += part[3 * i + 2]; }
+  if (pd) {
+    memset(per_domain, 0, sizeof(double) * nDom * 4);
+    for (int i = 0; i < S; ++i)
+      for (int q = 0; q < nDom * 4; ++q) per_domain[q] += pd[(size_t)i * nDom * 4 + q];
+    free(pd);
+  }
+  free(part);
+}
+
+/* cloud/solver.py:282-315 computeForceAll (Hellmann-Feynman), FP64 accumulation:
+ * F_n += Z_n rho h^3 (x - R_n) / (|x-R_n|^2 + h^2)^{3/2} over interior points with rho >= 1e-20.
+ * Per-voxel terms are evaluated in f32 as the reference does. */
+void orc_sp_forces(const float* U, const float* atoms5, int nAtoms, int S, float h, float h2, float h3, double* F) {
+  const int NN = S - 1;
+  double* part = (double*)calloc((size_t)S * nAtoms * 3, sizeof(double));
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i) {
+    double* pp = part + (size_t)i * nAtoms * 3;
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        float rho = U[id] * U[id];
+        if (rho < 1e-20f) continue;
+        float xi = (float)i * h, yj = (float)j * h, zk = (float)k * h;
+        for (int n = 0; n < nAtoms; ++n) {
+          float Za = atoms5[n * 5 + 3];
+          if (Za <= 0.f) continue;
+          float dx = xi - atoms5[n * 5 + 0] * h;
+          float dy = yj - atoms5[n * 5 + 1] * h;
+          float dz = zk - atoms5[n * 5 + 2] * h;
+          float r2 = dx * dx + dy * dy + dz * dz + h2;
+          float inv_r3 = 1.0f / (r2 * sqrtf(r2));
+          float w = Za * rho * inv_r3 * h3;
+          pp[n * 3 + 0] += (double)(w * dx);
+          pp[n * 3 + 1] += (double)(w * dy);
+          pp[n * 3 + 2] += (double)(w * dz);
+        }
+      }
+  }
+  memset(F, 0, sizeof(double) * nAtoms * 3);
+  for (int i = 0; i < S; ++i)
+    for (int q = 0; q < nAtoms * 3; ++q) F[q] += part[(size_t)i * nAtoms * 3 + q];
+  free(part);
+}
+
+/* ======================================================================
+ * molecule.js flavour
+ * ==================================================================== */
+
+/* Atom record as molecule.js packs it (molecule.js:183-191, :1875-1903): positions are
+ * stored in a Uint32Array, so fractional grid positions are truncated. */
+typedef struct {
+  uint32_t posI, posJ, posK;
+  float Z, rc, Z_nuc, initZeff, initRcut;
+} orc_mj_atom;
+
+static inline float mj_dist(int ci, int cj, int ck, const orc_mj_atom* a, float h) {
+  float dx = ((float)ci - (float)a->posI) * h;
+  float dy = ((float)cj - (float)a->posJ) * h;
+  float dz = ((float)ck - (float)a->posK) * h;
+  return sqrtf(dx * dx + dy * dy + dz * dz);
+}
+
+/* molecule.js:246-259 isInsideRc (own r_c sphere; bare nuclei when present). */
+static inline int mj_inside_rc(int ci, int cj, int ck, uint32_t lbl, const orc_mj_atom* atoms, int nElec,
+                               int hasBare, float h) {
+  float rc = atoms[lbl].rc;
+  if (rc > 0.f && mj_dist(ci, cj, ck, &atoms[lbl], h) < rc) return 1;
+  if (hasBare)
+    for (int n = 0; n < nElec; ++n)
+      if (atoms[n].Z <= 0.f && atoms[n].Z_nuc > 0.f && atoms[n].rc > 0.f)
+        if (mj_dist(ci, cj, ck, &atoms[n], h) < atoms[n].rc) return 1;
+  return 0;
+}
+
+/* molecule.js:263-343 updateU with W_CUTOFF = 0 (the default, :83): Dirichlet 0
+ * inside the own r_c sphere; a neighbour of another label or inside its label's
+ * r_c sphere is replaced by the centre value.  Interior cells only are written. */
+void orc_mj_update(const float* U, float* Uo, const float* K, const uint32_t* label, const float* Pother,
+                   const orc_mj_atom* atoms, int nElec, int hasBare, int S, float h, float half_d, float dt) {
+  const int NN = S - 1;
+  const int64_t S2 = (int64_t)S * S;
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        uint32_t L = label[id];
+        if (mj_inside_rc(i, j, k, L, atoms, nElec, hasBare, h)) { Uo[id] = 0.f; continue; }
+        float uc = U[id];
+        uint32_t lip = label[id + S2], lim = label[id - S2], ljp = label[id + S], ljm = label[id - S];
+        uint32_t lkp = label[id + 1], lkm = label[id - 1];
+        int eip = mj_inside_rc(i + 1, j, k, lip, atoms, nElec, hasBare, h);
+        int eim = mj_inside_rc(i - 1, j, k, lim, atoms, nElec, hasBare, h);
+        int ejp = mj_inside_rc(i, j + 1, k, ljp, atoms, nElec, hasBare, h);
+        int ejm = mj_inside_rc(i, j - 1, k, ljm, atoms, nElec, hasBare, h);
+        int ekp = mj_inside_rc(i, j, k + 1, lkp, atoms, nElec, hasBare, h);
+        int ekm = mj_inside_rc(i, j, k - 1, lkm, atoms, nElec, hasBare, h);
+        float uip = (lip == L && !eip) ? U[id + S2] : uc;
+        float uim = (lim == L && !eim) ? U[id - S2] : uc;
+        float ujp = (ljp == L && !ejp) ? U[id + S] : uc;
+        float ujm = (ljm == L && !ejm) ? U[id - S] : uc;
+        float ukp = (lkp == L && !ekp) ? U[id + 1] : uc;
+        float ukm = (lkm == L && !ekm) ? U[id - 1] : uc;
+        float lap = uip + uim + ujp + ujm + ukp + ukm - 6.0f * uc;
+        Uo[id] = uc + half_d * lap + dt * (K[id] - 2.0f * Pother[id]) * uc;
+      }
+}
+
+/* molecule.js:426-540 evolveBoundary without locked groups or shell splits
+ * (both off unless a page sets them, :490-503): snapshot read labelIn, write labelOut and W. */
+void orc_mj_evolve_boundary(const uint32_t* labelIn, uint32_t* labelOut, const float* U, float* W, int S,
+                            float dt_w, float curvReg) {
+  const int NN = S - 1;
+  const int64_t S2 = (int64_t)S * S;
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        uint32_t myL = labelIn[id];
+        float myRho = U[id] * U[id];
+        const int64_t nb[6] = {id + S2, id - S2, id + S, id - S, id + 1, id - 1};
+        uint32_t bestL = myL;
+        float bestRho = 0.f, myCnt = 0.f;
+        for (int q = 0; q < 6; ++q) {
+          uint32_t l = labelIn[nb[q]];
+          if (l == myL) myCnt += 1.0f;
+          else {
+            float r = U[nb[q]] * U[nb[q]];
+            if (r > bestRho) { bestRho = r; bestL = l; }
+          }
+        }
+        float w = W[id];
+        if (myCnt >= 6.0f) { w = fmaxf(w, 1.0f); W[id] = w; labelOut[id] = myL; continue; }
+        float denom = myRho + bestRho;
+        float vel = (denom < 1e-20f) ? 0.0f : (myRho - bestRho) / denom;
+        w += dt_w * vel;
+        float curv = (myCnt - 3.0f) / 3.0f;
+        w += curvReg * curv;
+        uint32_t newL = myL;
+        if (w < 0.0f) { newL = bestL; w = 0.1f; }
+        W[id] = w;
+        labelOut[id] = newL;
+      }
+}
+
+/* molecule.js:723-749 weighted Jacobi: Pout = 0.3333*Pc + (sum_6 + h2*2pi*rho)/9. */
+void orc_mj_jacobi(const float* Pin, float* Pout, const float* rho, int S, float h2, float two_pi) {
+  const int NN = S - 1;
+  const int64_t S2 = (int64_t)S * S;
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        float Pc = Pin[id];
+        float sn = Pin[id + S2] + Pin[id - S2] + Pin[id + S] + Pin[id - S] + Pin[id + 1] + Pin[id - 1];
+        float rhs = h2 * two_pi * rho[id];
+        Pout[id] = 0.3333f * Pc + (sn + rhs) / 9.0f;
+      }
+}
+
+/* molecule.js:754-774 computeRho (interior only). */
+void orc_mj_rho(const float* U, float* rho, int S) {
+  const int NN = S - 1;
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) { int64_t id = IDX(i, j, k, S); float u = U[id]; rho[id] = u * u; }
+}
+
+/* molecule.js:777-803 residual r = -2pi*rho - lap(P)/h^2 (sign as written). */
+void orc_mj_residual(const float* Pin, float* R, const float* rho, int S, float inv_h2, float two_pi) {
+  const int NN = S - 1;
+  const int64_t S2 = (int64_t)S * S;
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        float Pc = Pin[id];
+        float lap = (Pin[id + S2] + Pin[id - S2] + Pin[id + S] + Pin[id - S] + Pin[id + 1] + Pin[id - 1] - 6.0f * Pc) *
+                    inv_h2;
+        R[id] = -two_pi * rho[id] - lap;
+      }
+}
+
+/* molecule.js:806-839 27-point full weighting (8/4/2/1)/64 onto SC = NN/2+1. */
+void orc_mj_restrict(const float* fine, float* coarse, int S, int SC) {
+  const int NC = SC - 1;
+  const int64_t S2 = (int64_t)S * S;
+#pragma omp parallel for schedule(static)
+  for (int I = 1; I < NC; ++I)
+    for (int J = 1; J < NC; ++J)
+      for (int K2 = 1; K2 < NC; ++K2) {
+        int fi = 2 * I, fj = 2 * J, fk = 2 * K2;
+#define F(a, b, c) fine[(int64_t)(a) * S2 + (int64_t)(b) * S + (c)]
+        float val = 8.0f * F(fi, fj, fk);
+        val += 4.0f * (F(fi + 1, fj, fk) + F(fi - 1, fj, fk) + F(fi, fj + 1, fk) + F(fi, fj - 1, fk) +
+                       F(fi, fj, fk + 1) + F(fi, fj, fk - 1));
+        val += 2.0f * (F(fi + 1, fj + 1, fk) + F(fi + 1, fj - 1, fk) + F(fi - 1, fj + 1, fk) + F(fi - 1, fj - 1, fk) +
+                       F(fi + 1, fj, fk + 1) + F(fi + 1, fj, fk - 1) + F(fi - 1, fj, fk + 1) + F(fi - 1, fj, fk - 1) +
+                       F(fi, fj + 1, fk + 1) + F(fi, fj + 1, fk - 1) + F(fi, fj - 1, fk + 1) + F(fi, fj - 1, fk - 1));
+        val += F(fi + 1, fj + 1, fk + 1) + F(fi + 1, fj + 1, fk - 1) + F(fi + 1, fj - 1, fk + 1) +
+               F(fi + 1, fj - 1, fk - 1) + F(fi - 1, fj + 1, fk + 1) + F(fi - 1, fj + 1, fk - 1) +
+               F(fi - 1, fj - 1, fk + 1) + F(fi - 1, fj - 1, fk - 1);
+#undef F
+        coarse[IDX(I, J, K2, SC)] = val * 0.015625f;
+      }
+}
+
+/* molecule.js:842-867 coarse weighted Jacobi with hc^2 = 4 h^2. */
+void orc_mj_coarse_smooth(const float* Ein, float* Eout, const float* f, int SC, float h2) {
+  const int NC = SC - 1;
+  const int64_t SC2 = (int64_t)SC * SC;
+#pragma omp parallel for schedule(static)
+  for (int I = 1; I < NC; ++I)
+    for (int J = 1; J < NC; ++J)
+      for (int K2 = 1; K2 < NC; ++K2) {
+        int64_t c = IDX(I, J, K2, SC);
+        float ec = Ein[c];
+        float sn = Ein[c + SC2] + Ein[c - SC2] + Ein[c + SC] + Ein[c - SC] + Ein[c + 1] + Ein[c - 1];
+        float hc2 = 4.0f * h2;
+        Eout[c] = 0.3333f * ec + (sn + hc2 * f[c]) / 9.0f;
+      }
+}
+
+/* molecule.js:870-909 trilinear prolongation, Pf += 0.5*corr (sign/damping as written). */
+void orc_mj_prolong(const float* Ec, float* Pf, int S, int SC) {
+  const int NN = S - 1, NC = SC - 1;
+  const int64_t S2 = (int64_t)S * S, SC2 = (int64_t)SC * SC;
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int ci = i / 2, cj = j / 2, ck = k / 2;
+        int ci1 = ci + (i & 1); if (ci1 > NC) ci1 = NC;
+        int cj1 = cj + (j & 1); if (cj1 > NC) cj1 = NC;
+        int ck1 = ck + (k & 1); if (ck1 > NC) ck1 = NC;
+        float wi = (i & 1) ? 0.5f : 1.0f, wj = (j & 1) ? 0.5f : 1.0f, wk = (k & 1) ? 0.5f : 1.0f;
+        float wi1 = 1.0f - wi, wj1 = 1.0f - wj, wk1 = 1.0f - wk;
+#define E(a, b, c) Ec[(int64_t)(a) * SC2 + (int64_t)(b) * SC + (c)]
+        float corr = 0.0f;
+        corr += wi * wj * wk * E(ci, cj, ck);
+        corr += wi * wj * wk1 * E(ci, cj, ck1);
+        corr += wi * wj1 * wk * E(ci, cj1, ck);
+        corr += wi * wj1 * wk1 * E(ci, cj1, ck1);
+        corr += wi1 * wj * wk * E(ci1, cj, ck);
+        corr += wi1 * wj * wk1 * E(ci1, cj, ck1);
+        corr += wi1 * wj1 * wk * E(ci1, cj1, ck);
+        corr += wi1 * wj1 * wk1 * E(ci1, cj1, ck1);
+#undef E
+        Pf[(int64_t)i * S2 + (int64_t)j * S + k] += 0.5f * corr;
+      }
+}
+
+/* molecule.js:912-946 fixed-point norms: norm[l] += u32(u*u*h3*2^24) (truncation),
+ * decoded as f32(sum) * 2^-24.  The u32 sum wraps modulo 2^32 like WGSL atomics. */
+void orc_mj_norms_fixed(const float* U, const uint32_t* label, int S, float h3, int nDom, uint32_t* acc,
+                        float* normFloat) {
+  const int NN = S - 1;
+  for (int n = 0; n < nDom; ++n) acc[n] = 0u;
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        float v = U[id];
+        uint32_t c = (uint32_t)(v * v * h3 * 16777216.0f);
+        acc[label[id]] += c;
+      }
+  for (int n = 0; n < nDom; ++n) normFloat[n] = (float)acc[n] * (1.0f / 16777216.0f);
+}
+
+/* molecule.js:1077-1105 normalize: U *= sqrt(Z/n) when n > 0 and Z > 0 (interior only). */
+void orc_mj_normalize(float* U, const float* normFloat, const uint32_t* label, const orc_mj_atom* atoms, int S) {
+  const int NN = S - 1;
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        uint32_t l = label[id];
+        float n = normFloat[l], Z = atoms[l].Z;
+        if (n > 0.f && Z > 0.f) U[id] *= sqrtf(Z / n);
+      }
+}
+
+/* molecule.js:950-1075 reduceEnergy terms accumulated in FP64 (the reference sums in f32):
+ * out = {T, V_eK, V_ee, dipX, dipY, dipZ}; exclusion sphere radius max(rc, R_SING). */
+void orc_mj_energy(const float* U, const float* Pv, const float* K, const uint32_t* label, const orc_mj_atom* atoms,
+                   int S, float h, float h3, float Rsing, double* out) {
+  const int NN = S - 1;
+  const int64_t S2 = (int64_t)S * S;
+  double* part = (double*)calloc((size_t)S * 6, sizeof(double));
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i) {
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        float v = U[id], rho = v * v;
+        uint32_t L = label[id];
+        const orc_mj_atom* a = &atoms[L];
+        float rcx = fmaxf(a->rc, Rsing);
+#define EXCL(ci, cj, ck) (mj_dist((ci), (cj), (ck), a, h) < rcx)
+        if (EXCL(i, j, k)) continue;
+        int sip = label[id + S2] == L && !EXCL(i + 1, j, k);
+        int sjp = label[id + S] == L && !EXCL(i, j + 1, k);
+        int skp = label[id + 1] == L && !EXCL(i, j, k + 1);
+#undef EXCL
+        float da = sip ? U[id + S2] - v : 0.f;
+        float db = sjp ? U[id + S] - v : 0.f;
+        float dc = skp ? U[id + 1] - v : 0.f;
+        acc[0] += 0.5 * ((double)da * da + (double)db * db + (double)dc * dc) * h;
+        acc[1] += -(double)K[id] * rho * h3;
+        acc[2] += (double)Pv[id] * rho * h3;
+        acc[3] += (double)rho * ((float)i * h) * h3;
+        acc[4] += (double)rho * ((float)j * h) * h3;
+        acc[5] += (double)rho * ((float)k * h) * h3;
+      }
+    for (int q = 0; q < 6; ++q) part[6 * i + q] = acc[q];
+  }
+  for (int q = 0; q < 6; ++q) out[q] = 0;
+  for (int i = 0; i < S; ++i)
+    for (int q = 0; q < 6; ++q) out[q] += part[6 * i + q];
+  free(part);
+}
+
+/* molecule.js:1200-1269 gradPtotal: F = 2 Z <grad P> over the integer ball |d|^2 <= R^2
+ * around the (integer) nucleus, central differences; FP64 accumulation of the f32 terms. */
+void orc_mj_force_gradP(const float* Pt, const orc_mj_atom* atoms, int nElec, int S, float inv_h, int R, double* F) {
+  const int64_t S2 = (int64_t)S * S;
+  for (int a = 0; a < nElec; ++a) {
+    float ZA = (atoms[a].Z <= 0.f) ? atoms[a].Z_nuc : atoms[a].Z;
+    if (ZA <= 0.f) { F[3 * a] = F[3 * a + 1] = F[3 * a + 2] = 0; continue; }
+    int ci = (int)atoms[a].posI, cj = (int)atoms[a].posJ, ck = (int)atoms[a].posK;
+    float inv2h = 0.5f * inv_h;
+    double sx = 0, sy = 0, sz = 0, cnt = 0;
+    for (int di = -R; di <= R; ++di) {
+      int ii = ci + di;
+      if (ii < 1 || ii >= S - 1) continue;
+      for (int dj = -R; dj <= R; ++dj) {
+        int jj = cj + dj;
+        if (jj < 1 || jj >= S - 1) continue;
+        for (int dk = -R; dk <= R; ++dk) {
+          int kk = ck + dk;
+          if (kk < 1 || kk >= S - 1) continue;
+          if (di * di + dj * dj + dk * dk > R * R) continue;
+          int64_t id = (int64_t)ii * S2 + (int64_t)jj * S + kk;
+          sx += (double)((Pt[id + S2] - Pt[id - S2]) * inv2h);
+          sy += (double)((Pt[id + S] - Pt[id - S]) * inv2h);
+          sz += (double)((Pt[id + 1] - Pt[id - 1]) * inv2h);
+          cnt += 1;
+        }
+      }
+    }
+    if (cnt > 0) { sx /= cnt; sy /= cnt; sz /= cnt; }
+    F[3 * a] = 2.0 * ZA * sx; F[3 * a + 1] = 2.0 * ZA * sy; F[3 * a + 2] = 2.0 * ZA * sz;
+  }
+}
+
+/* molecule.js:1271-1330 direct HF force with h^2 softening over the interior. */
+void orc_mj_force_hf(const float* U, const orc_mj_atom* atoms, int nElec, int S, float h, double* F) {
+  const int NN = S - 1;
+  const float h2 = h * h, h3 = h * h * h;
+  for (int a = 0; a < nElec; ++a) {
+    float ZA = (atoms[a].Z <= 0.f) ? atoms[a].Z_nuc : atoms[a].Z;
+    F[3 * a] = F[3 * a + 1] = F[3 * a + 2] = 0;
+    if (ZA <= 0.f) continue;
+    float Ri = (float)atoms[a].posI * h, Rj = (float)atoms[a].posJ * h, Rk = (float)atoms[a].posK * h;
+    double fx = 0, fy = 0, fz = 0;
+#pragma omp parallel for reduction(+ : fx, fy, fz) schedule(static)
+    for (int i = 1; i < NN; ++i)
+      for (int j = 1; j < NN; ++j)
+        for (int k = 1; k < NN; ++k) {
+          float di = (float)i * h - Ri, dj = (float)j * h - Rj, dk = (float)k * h - Rk;
+          float r2 = di * di + dj * dj + dk * dk + h2;
+          float r = sqrtf(r2);
+          float inv_r3 = 1.0f / (r * r2);
+          int64_t id = IDX(i, j, k, S);
+          float rho = U[id] * U[id];
+          float w = rho * inv_r3 * h3;
+          fx += (double)(di * w); fy += (double)(dj * w); fz += (double)(dk * w);
+        }
+    F[3 * a] = ZA * fx; F[3 * a + 1] = ZA * fy; F[3 * a + 2] = ZA * fz;
+  }
+}
+
+/* molecule.js:1377-1426 gpuInitAccum over all atoms in one pass plus :1437-1449 final copy:
+ * K = sum Zn/r_eff, trial u = Ze^2/sqrt(pi) e^{-Ze r} (0 beyond initRcut or for bare nuclei),
+ * label = argmax (strict >, first wins).  K/bestU/label start from 0/0/0 over ALL S^3 points. */
+void orc_mj_init(float* K, float* U, uint32_t* label, const orc_mj_atom* atoms, int nElec, int S, float h,
+                 float Rsing) {
+  const float h2 = h * h;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < S; ++i)
+    for (int j = 0; j < S; ++j)
+      for (int kk = 0; kk < S; ++kk) {
+        int64_t id = IDX(i, j, kk, S);
+        float xi = (float)i * h, yj = (float)j * h, zk = (float)kk * h;
+        float Kval = 0.f, bU = 0.f;
+        uint32_t bestN = 0;
+        for (int n = 0; n < nElec; ++n) {
+          float Za = atoms[n].Z;
+          float Zn = (atoms[n].Z_nuc > 0.f) ? atoms[n].Z_nuc : Za;
+          if (Za <= 0.f && Zn <= 0.f) continue;
+          float dx = xi - (float)atoms[n].posI * h;
+          float dy = yj - (float)atoms[n].posJ * h;
+          float dz = zk - (float)atoms[n].posK * h;
+          float r2 = dx * dx + dy * dy + dz * dz;
+          float r = (atoms[n].rc > 0.f) ? fmaxf(sqrtf(r2 + 0.04f * h2), atoms[n].rc) : fmaxf(sqrtf(r2), Rsing);
+          Kval += Zn / r;
+          float Ze = atoms[n].initZeff;
+          float rReal = sqrtf(r2);
+          float uT = (rReal > atoms[n].initRcut || Za <= 0.f) ? 0.f : Ze * Ze * 0.5641895835f * expf(-Ze * r);
+          if (uT > bU) { bU = uT; bestN = (uint32_t)n; }
+        }
+        K[id] = Kval; U[id] = bU; label[id] = bestN;
+      }
+}
+
+/* ======================================================================
+ * FP64 new method (Gaussian nuclei, red-black multigrid).  No reference counterpart.
+ * ==================================================================== */
+
+/* Gaussian-smeared nucleus of charge Z and width sigma: K(r) = Z erf(r/(sqrt2 sigma))/r,
+ * K(0) = Z sqrt(2/pi)/sigma.  xyz are atom centres in bohr relative to grid point (0,0,0). */
+void orc_nm_potential(double* K, const double* xyz, const double* Z, int nAt, int S, double h, double sigma) {
+  const int NN = S - 1;
+  const double c0 = sqrt(2.0 / M_PI) / sigma, inv = 1.0 / (sqrt(2.0) * sigma);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < S; ++i)
+    for (int j = 0; j < S; ++j)
+      for (int k = 0; k < S; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        if (!interior(i, j, k, NN)) { K[id] = 0; continue; }
+        double v = 0;
+        for (int a = 0; a < nAt; ++a) {
+          double dx = i * h - xyz[3 * a], dy = j * h - xyz[3 * a + 1], dz = k * h - xyz[3 * a + 2];
+          double r = sqrt(dx * dx + dy * dy + dz * dz);
+          v += (r < 1e-12) ? Z[a] * c0 : Z[a] * erf(r * inv) / r;
+        }
+        K[id] = v;
+      }
+}
+
+/* FP64 ITP update of the new method: same-label Neumann Laplacian, psi' = psi +
+ * half_dv*lap + dt*(K - 2P)*psi (the solver.py update with FP64 fields). */
+void orc_nm_update(const double* U, double* Unew, const double* K, const double* P, const int32_t* label, int S,
+                   double half_dv, double dt) {
+  const int NN = S - 1;
+  const int64_t S2 = (int64_t)S * S;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < S; ++i)
+    for (int j = 0; j < S; ++j)
+      for (int k = 0; k < S; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        if (!interior(i, j, k, NN)) { Unew[id] = 0; continue; }
+        int32_t L = label[id];
+        double u = U[id];
+        double s = ((label[id + S2] == L) ? U[id + S2] : u) + ((label[id - S2] == L) ? U[id - S2] : u) +
+                   ((label[id + S] == L) ? U[id + S] : u) + ((label[id - S] == L) ? U[id - S] : u) +
+                   ((label[id + 1] == L) ? U[id + 1] : u) + ((label[id - 1] == L) ? U[id - 1] : u);
+        Unew[id] = u + half_dv * (s - 6.0 * u) + dt * (K[id] - 2.0 * P[id]) * u;
+      }
+}
+
+/* One red-black Gauss-Seidel sweep (red = (i+j+k) even first) for -lap(P)/h^2 = f,
+ * i.e. P = (sum_6 P + h^2 f)/6, on a level with S points per axis. */
+static void nm_rbgs(double* P, const double* f, int S, double h2) {
+  const int NN = S - 1;
+  const int64_t S2 = (int64_t)S * S;
+  for (int color = 0; color < 2; ++color) {
+#pragma omp parallel for schedule(static)
+    for (int i = 1; i < NN; ++i)
+      for (int j = 1; j < NN; ++j)
+        for (int k = 1 + ((i + j + 1 + color) & 1); k < NN; k += 2) {
+          int64_t id = IDX(i, j, k, S);
+          P[id] = (P[id + S2] + P[id - S2] + P[id + S] + P[id - S] + P[id + 1] + P[id - 1] + h2 * f[id]) / 6.0;
+        }
+  }
+}
+
+static void nm_residual(const double* P, const double* f, double* r, int S, double inv_h2) {
+  const int NN = S - 1;
+  const int64_t S2 = (int64_t)S * S;
+  memset(r, 0, sizeof(double) * (size_t)S * S * S);
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        r[id] = f[id] + (P[id + S2] + P[id - S2] + P[id + S] + P[id - S] + P[id + 1] + P[id - 1] - 6.0 * P[id]) *
+                            inv_h2;
+      }
+}
+
+/* full weighting (1/64)(8,4,2,1) onto the next coarser vertex-centred level */
+static void nm_restrict(const double* fine, double* coarse, int S, int SC) {
+  const int NC = SC - 1;
+  const int64_t S2 = (int64_t)S * S;
+  memset(coarse, 0, sizeof(double) * (size_t)SC * SC * SC);
+#pragma omp parallel for schedule(static)
+  for (int I = 1; I < NC; ++I)
+    for (int J = 1; J < NC; ++J)
+      for (int K2 = 1; K2 < NC; ++K2) {
+        double v = 0;
+        for (int a = -1; a <= 1; ++a)
+          for (int b = -1; b <= 1; ++b)
+            for (int c = -1; c <= 1; ++c) {
+              double w = (a == 0 ? 2.0 : 1.0) * (b == 0 ? 2.0 : 1.0) * (c == 0 ? 2.0 : 1.0);
+              v += w * fine[(int64_t)(2 * I + a) * S2 + (int64_t)(2 * J + b) * S + (2 * K2 + c)];
+            }
+        coarse[IDX(I, J, K2, SC)] = v / 64.0;
+      }
+}
+
+/* trilinear prolongation of the coarse correction, added to the fine solution */
+static void nm_prolong_add(const double* Ec, double* P, int S, int SC) {
+  const int NN = S - 1;
+  const int64_t SC2 = (int64_t)SC * SC;
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int ci = i >> 1, cj = j >> 1, ck = k >> 1;
+        int oi = i & 1, oj = j & 1, ok = k & 1;
+        double v = 0;
+        for (int a = 0; a <= oi; ++a)
+          for (int b = 0; b <= oj; ++b)
+            for (int c = 0; c <= ok; ++c) v += Ec[(int64_t)(ci + a) * SC2 + (int64_t)(cj + b) * SC + (ck + c)];
+        v /= (double)((1 + oi) * (1 + oj) * (1 + ok));
+        P[IDX(i, j, k, S)] += v;
+      }
+}
+
+/* V(pre,post) cycle on -lap P = f with `levels` levels (NN divisible by 2^(levels-1)),
+ * coarsest level solved by `coarse_sweeps` RBGS sweeps.  FP64 throughout. */
+static void nm_vcycle_rec(double* P, const double* f, int S, double h, int levels, int pre, int post,
+                          int coarse_sweeps) {
+  double h2 = h * h;
+  if (levels <= 1) {
+    for (int s = 0; s < coarse_sweeps; ++s) nm_rbgs(P, f, S, h2);
+    return;
+  }
+  for (int s = 0; s < pre; ++s) nm_rbgs(P, f, S, h2);
+  int SC = (S - 1) / 2 + 1;
+  size_t nf = (size_t)S * S * S, nc = (size_t)SC * SC * SC;
+  double* r = (double*)malloc(sizeof(double) * nf);
+  double* rc = (double*)malloc(sizeof(double) * nc);
+  double* ec = (double*)calloc(nc, sizeof(double));
+  nm_residual(P, f, r, S, 1.0 / h2);
+  nm_restrict(r, rc, S, SC);
+  nm_vcycle_rec(ec, rc, SC, 2 * h, levels - 1, pre, post, coarse_sweeps);
+  nm_prolong_add(ec, P, S, SC);
+  for (int s = 0; s < post; ++s) nm_rbgs(P, f, S, h2);
+  free(r); free(rc); free(ec);
+}
+
+/* Poisson for the Hartree half-potential: lap P = -2 pi rho  <=>  -lap P = 2 pi psi^2. */
+void orc_nm_vcycle(double* P, const double* U, int S, double h, int levels, int pre, int post, int coarse_sweeps) {
+  size_t n = (size_t)S * S * S;
+  double* f = (double*)malloc(sizeof(double) * n);
+  for (size_t q = 0; q < n; ++q) f[q] = 2.0 * M_PI * U[q] * U[q];
+  nm_vcycle_rec(P, f, S, h, levels, pre, post, coarse_sweeps);
+  free(f);
+}
+
+/* Per-label FP64 norm / T / V_eK / V_ee (same terms as orc_sp_energy_f64) for FP64 fields. */
+void orc_nm_energy(const double* U, const double* K, const double* P, const int32_t* label, int S, double h,
+                   double* out, int nDom, double* per_domain) {
+  const int NN = S - 1;
+  const int64_t S2 = (int64_t)S * S;
+  const double h3 = h * h * h;
+  double* pd = (double*)calloc((size_t)S * nDom * 4, sizeof(double));
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        double u = U[id], rho = u * u;
+        int32_t L = label[id];
+        if (L < 0 || L >= nDom) continue;
+        double a = (label[id + S2] == L) ? U[id + S2] - u : 0.0;
+        double b = (label[id + S] == L) ? U[id + S] - u : 0.0;
+        double c = (label[id + 1] == L) ? U[id + 1] - u : 0.0;
+        double* q = pd + ((size_t)i * nDom + L) * 4;
+        q[0] += rho * h3; q[1] += 0.5 * (a * a + b * b + c * c) * h; q[2] += -K[id] * rho * h3;
+        q[3] += P[id] * rho * h3;
+      }
+  memset(per_domain, 0, sizeof(double) * nDom * 4);
+  for (int i = 0; i < S; ++i)
+    for (int q = 0; q < nDom * 4; ++q) per_domain[q] += pd[(size_t)i * nDom * 4 + q];
+  out[0] = out[1] = out[2] = 0;
+  for (int d = 0; d < nDom; ++d) { out[0] += per_domain[4 * d + 1]; out[1] += per_domain[4 * d + 2]; out[2] += per_domain[4 * d + 3]; }
+  free(pd);
+}
+
+/* Normalise FP64 psi to charge Zdom[l] per label from the per_domain norms (column 0). */
+void orc_nm_normalize(double* U, const int32_t* label, int64_t S3, int nDom, const double* Zdom, const double* norms) {
+#pragma omp parallel for schedule(static)
+  for (int64_t id = 0; id < S3; ++id) {
+    int32_t l = label[id];
+    if (l < 0 || l >= nDom) continue;
+    double n = norms[l];
+    if (n > 1e-300 && Zdom[l] > 0) U[id] *= sqrt(Zdom[l] / n);
+  }
+}
+
+/* Hellmann-Feynman / stationary-point gradient of E_eK = -h^3 sum K rho with Gaussian
+ * nuclei: dE/dR_a = -h^3 sum rho dK_a/dR_a, where dK_a/dR_a = -dK_a/dr * (x-R)/|x-R|.
+ * Returns the FORCE -dE/dR (without the nuclear-nuclear part). */
+void orc_nm_force(const double* U, const double* xyz, const double* Z, int nAt, int S, double h, double sigma,
+                  double* F) {
+  const int NN = S - 1;
+  const double h3 = h * h * h, inv = 1.0 / (sqrt(2.0) * sigma), g = sqrt(2.0 / M_PI) / sigma;
+  for (int a = 0; a < nAt; ++a) {
+    double fx = 0, fy = 0, fz = 0;
+#pragma omp parallel for reduction(+ : fx, fy, fz) schedule(static)
+    for (int i = 1; i < NN; ++i)
+      for (int j = 1; j < NN; ++j)
+        for (int k = 1; k < NN; ++k) {
+          double dx = i * h - xyz[3 * a], dy = j * h - xyz[3 * a + 1], dz = k * h - xyz[3 * a + 2];
+          double r2 = dx * dx + dy * dy + dz * dz, r = sqrt(r2);
+          if (r < 1e-12) continue;
+          double u = U[IDX(i, j, k, S)], rho = u * u;
+          /* d/dr [erf(r*inv)/r] = (g e^{-r^2 inv^2})/r - erf(r inv)/r^2 */
+          double dKdr = Z[a] * (g * exp(-r2 * inv * inv) / r - erf(r * inv) / r2);
+          /* F = -dE/dR = -(h^3 sum rho dK/dr (x-R)/r)  since dK/dR = -dK/dr (x-R)/r and E=-sum K rho h3 */
+          double w = -h3 * rho * dKdr / r;
+          fx += w * dx; fy += w * dy; fz += w * dz;
+        }
+    F[3 * a] = fx; F[3 * a + 1] = fy; F[3 * a + 2] = fz;
+  }
+}

@@ -1,0 +1,132 @@
+"""ctypes binding of librq (include/rq.h).
+
+The library is built in-tree by ``python -m realmolecule_b200.build`` and loaded from the
+package directory.  There is no fallback: if librq.so is missing or no CUDA device is
+visible, the calls fail with an exception naming the reason.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "librq.so")
+HEADER = os.path.join(os.path.dirname(PKG), "include", "rq.h")
+
+RQ_OK, RQ_EINVAL, RQ_ENOMEM, RQ_ECUDA, RQ_ENONFINITE, RQ_ETIMEOUT, RQ_ENOTSUP, RQ_ENODEV = 0, -1, -2, -3, -4, -5, -6, -7
+FLAVOR_MOLECULE_JS, FLAVOR_SOLVER_PY, FLAVOR_NEW = 0, 1, 2
+PREC_MIXED, PREC_FP64 = 0, 1
+FORCE_HF, FORCE_GRADP, FORCE_ADJOINT = 0, 1, 2
+E_TOTAL, E_T, E_EK, E_EE, E_KK, E_DIPX, E_DIPY, E_DIPZ = range(8)
+ENERGY_LEN, DOMAIN_LEN = 8, 5
+
+
+class RqError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str = ""):
+        self.status = status
+        super().__init__(f"{where}: status {status} ({status_string(status)}){': ' + detail if detail else ''}")
+
+
+class Config(C.Structure):
+    _fields_ = [("NN", C.c_int32), ("flavor", C.c_int32), ("precision", C.c_int32), ("norm_interval", C.c_int32),
+                ("screen", C.c_double), ("dv", C.c_double), ("poisson_interval", C.c_int32),
+                ("label_interval", C.c_int32), ("jacobi_per_step", C.c_int32), ("steps_per_frame", C.c_int32),
+                ("vcycle_interval", C.c_int32), ("mg_levels", C.c_int32), ("mg_pre", C.c_int32),
+                ("mg_post", C.c_int32), ("mg_coarse_sweeps", C.c_int32), ("sic", C.c_int32),
+                ("boundary_speed", C.c_double), ("curv_reg", C.c_double), ("sigma", C.c_double),
+                ("reserved", C.c_int32 * 8)]
+
+
+class Atom(C.Structure):
+    _fields_ = [("i", C.c_double), ("j", C.c_double), ("k", C.c_double), ("Z", C.c_double), ("Z_nuc", C.c_double),
+                ("rc", C.c_double), ("init_zeff", C.c_double), ("init_rcut", C.c_double)]
+
+
+class Info(C.Structure):
+    _fields_ = [("NN", C.c_int32), ("S", C.c_int32), ("n_atoms", C.c_int32), ("flavor", C.c_int32),
+                ("precision", C.c_int32), ("steps_done", C.c_int32), ("mg_levels", C.c_int32), ("_pad", C.c_int32),
+                ("h", C.c_double), ("dv", C.c_double), ("dt", C.c_double), ("sigma", C.c_double),
+                ("S3", C.c_int64), ("psi", C.c_void_p), ("label", C.c_void_p), ("K", C.c_void_p),
+                ("P", C.c_void_p), ("W", C.c_void_p), ("kernel_launches", C.c_int64)]
+
+
+KC_UPDATE, KC_POISSON, KC_LABELS, KC_NORMALIZE, KC_ENERGY, KC_FORCES, KC_MG, KC_OTHER = range(8)
+KC_NAMES = ["update", "poisson", "labels", "normalize", "energy", "forces", "multigrid", "other"]
+
+
+class Profile(C.Structure):
+    _fields_ = [("launches", C.c_int64 * 8), ("ms", C.c_double * 8), ("bytes", C.c_double * 8)]
+
+
+_V, _P, _I, _F, _D = C.c_void_p, C.c_void_p, C.c_int32, C.c_float, C.c_double
+_DP = C.POINTER(C.c_double)
+
+# name -> (restype, argtypes); every symbol include/rq.h declares
+SIGNATURES = {
+    "rq_create": (C.c_int, [C.POINTER(Config), C.POINTER(Atom), _I, C.POINTER(C.c_void_p)]),
+    "rq_destroy": (None, [_V]),
+    "rq_set_stream": (C.c_int, [_V, _V]),
+    "rq_get_info": (C.c_int, [_V, C.POINTER(Info)]),
+    "rq_last_error": (C.c_char_p, [_V]),
+    "rq_status_string": (C.c_char_p, [C.c_int]),
+    "rq_initialize": (C.c_int, [_V]),
+    "rq_set_atoms": (C.c_int, [_V, C.POINTER(Atom), _I]),
+    "rq_upload_state": (C.c_int, [_V, _P, _P, _P, _P]),
+    "rq_download_state": (C.c_int, [_V, _P, _P, _P, _P]),
+    "rq_upload_state_f64": (C.c_int, [_V, _P, _P]),
+    "rq_download_state_f64": (C.c_int, [_V, _P, _P, _P]),
+    "rq_download_K": (C.c_int, [_V, _P]),
+    "rq_step": (C.c_int, [_V, _I]),
+    "rq_energy": (C.c_int, [_V, _P, _P]),
+    "rq_forces": (C.c_int, [_V, _I, _P]),
+    "rq_nuclear_terms": (C.c_int, [_V, _DP, _P]),
+    "rq_solve": (C.c_int, [_V, _D, _I, _I, C.POINTER(C.c_int32), _DP]),
+    "rq_synchronize": (C.c_int, [_V]),
+    "rq_profile_begin": (C.c_int, [_V]),
+    "rq_profile_end": (C.c_int, [_V, C.POINTER(Profile)]),
+    "rq_kernel_update_sp": (C.c_int, [_P, _P, _P, _P, _P, _I, _F, _F, _V]),
+    "rq_kernel_jacobi_sp": (C.c_int, [_P, _P, _P, _I, _F, _F, _V]),
+    "rq_kernel_labels_sp": (C.c_int, [_P, _P, _P, _I, _I, _F, _F, _V]),
+    "rq_kernel_init_sp": (C.c_int, [_P, _P, _P, _P, _P, _I, _I, _F, _F, _V]),
+    "rq_kernel_recompute_k_sp": (C.c_int, [_P, _P, _I, _I, _F, _F, _V]),
+    "rq_kernel_normalize_sp": (C.c_int, [_P, _P, _P, _I, _I, _F, _P, _V]),
+    "rq_kernel_energy_sp": (C.c_int, [_P, _P, _P, _P, _I, _I, _F, _F, _P, _V]),
+    "rq_kernel_forces_hf_sp": (C.c_int, [_P, _P, _I, _I, _F, _F, _F, _P, _V]),
+}
+
+_lib = None
+
+
+def load():
+    """Load librq.so (built in-tree).  Raises if it is missing -- there is no fallback."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"librq.so not built at {LIB_PATH}; run `python -m realmolecule_b200.build`")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def status_string(status: int) -> str:
+    try:
+        return load().rq_status_string(status).decode()
+    except Exception:  # pragma: no cover - only when the library itself is missing
+        return "?"
+
+
+def check(status: int, where: str, ctx=None):
+    if status != RQ_OK:
+        detail = ""
+        if ctx is not None:
+            try:
+                detail = load().rq_last_error(ctx).decode()
+            except Exception:
+                pass
+        raise RqError(status, where, detail)
+    return status

@@ -1,0 +1,203 @@
+"""Thin object wrapper over one librq context (include/rq.h).
+
+``Context`` owns an ``rq_ctx``: it creates it from a flavour, grid and atom list, and
+exposes the step, energies, forces and state transfer with numpy arrays on the host.
+Device pointers of the live fields are available through ``info()`` for zero-copy use
+(e.g. wrapping them as torch tensors).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Iterable, Optional, Sequence
+
+import numpy as np
+
+from . import _lib as L
+
+FLAVORS = {"molecule.js": L.FLAVOR_MOLECULE_JS, "molecule": L.FLAVOR_MOLECULE_JS, "solver.py": L.FLAVOR_SOLVER_PY,
+           "solverpy": L.FLAVOR_SOLVER_PY, "new": L.FLAVOR_NEW}
+PRECISIONS = {"mixed": L.PREC_MIXED, "fp32": L.PREC_MIXED, "fp64": L.PREC_FP64}
+
+
+def make_atoms(rows: Iterable[dict], default_k: Optional[float] = None):
+    """Reference atom dicts ({i, j, k, Z, rc, Z_nuc, initZeff, initRcut}) -> ctypes array."""
+    rows = list(rows)
+    arr = (L.Atom * len(rows))()
+    for n, a in enumerate(rows):
+        arr[n].i = float(a["i"])
+        arr[n].j = float(a["j"])
+        arr[n].k = float(a.get("k", default_k if default_k is not None else 0.0))
+        arr[n].Z = float(a.get("Z", 0.0))
+        arr[n].Z_nuc = float(a["Z_nuc"]) if a.get("Z_nuc") is not None else float(a.get("Z", 0.0))
+        arr[n].rc = float(a.get("rc", 0.0) or 0.0)
+        arr[n].init_zeff = float(a.get("initZeff", 0.0) or 0.0)
+        arr[n].init_rcut = float(a.get("initRcut", 0.0) or 0.0)
+    return arr
+
+
+def _ptr(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    assert a.flags.c_contiguous
+    return a.ctypes.data
+
+
+class Context:
+    """One solver grid on the current CUDA device."""
+
+    def __init__(self, NN: int, screen: float, atoms: Sequence[dict], flavor: str = "solver.py",
+                 precision: str = "mixed", **opts):
+        self.lib = L.load()
+        cfg = L.Config()
+        cfg.NN = int(NN)
+        cfg.screen = float(screen)
+        cfg.flavor = FLAVORS[flavor] if isinstance(flavor, str) else int(flavor)
+        cfg.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        for k, v in opts.items():
+            if v is None:
+                continue
+            if not hasattr(cfg, k):
+                raise TypeError(f"unknown option {k}")
+            setattr(cfg, k, v)
+        self.cfg = cfg
+        self._atoms = make_atoms(atoms, default_k=NN // 2)
+        self.n_atoms = len(self._atoms)
+        h = C.c_void_p()
+        st = self.lib.rq_create(C.byref(cfg), self._atoms, self.n_atoms, C.byref(h))
+        L.check(st, "rq_create")
+        self.ctx = h
+        inf = self.info()
+        self.S, self.NN, self.S3 = inf.S, inf.NN, inf.S3
+        self.h, self.dv, self.dt = inf.h, inf.dv, inf.dt
+        self.fp64 = inf.precision == L.PREC_FP64
+
+    # -- lifecycle ------------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.rq_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, st, where):
+        return L.check(st, where, self.ctx)
+
+    def info(self) -> L.Info:
+        inf = L.Info()
+        self._chk(self.lib.rq_get_info(self.ctx, C.byref(inf)), "rq_get_info")
+        return inf
+
+    def set_stream(self, stream_handle: int | None):
+        self._chk(self.lib.rq_set_stream(self.ctx, stream_handle), "rq_set_stream")
+
+    # -- solver ---------------------------------------------------------------------------
+    def initialize(self):
+        self._chk(self.lib.rq_initialize(self.ctx), "rq_initialize")
+
+    def step(self, n: int = 1):
+        self._chk(self.lib.rq_step(self.ctx, int(n)), "rq_step")
+
+    def synchronize(self):
+        self._chk(self.lib.rq_synchronize(self.ctx), "rq_synchronize")
+
+    def energy(self, per_domain: bool = False):
+        out = np.zeros(L.ENERGY_LEN, np.float64)
+        pd = np.zeros((self.n_atoms, L.DOMAIN_LEN), np.float64) if per_domain else None
+        self._chk(self.lib.rq_energy(self.ctx, _ptr(out), _ptr(pd)), "rq_energy")
+        return (out, pd) if per_domain else out
+
+    def forces(self, method: int = L.FORCE_HF) -> np.ndarray:
+        F = np.zeros((self.n_atoms, 3), np.float64)
+        self._chk(self.lib.rq_forces(self.ctx, int(method), _ptr(F)), "rq_forces")
+        return F
+
+    def nuclear_terms(self):
+        e = C.c_double()
+        F = np.zeros((self.n_atoms, 3), np.float64)
+        self._chk(self.lib.rq_nuclear_terms(self.ctx, C.byref(e), _ptr(F)), "rq_nuclear_terms")
+        return e.value, F
+
+    def set_atoms(self, atoms: Sequence[dict]):
+        arr = make_atoms(atoms, default_k=self.NN // 2)
+        self._chk(self.lib.rq_set_atoms(self.ctx, arr, len(arr)), "rq_set_atoms")
+        self._atoms = arr
+
+    def solve(self, tol_dE: float, max_steps: int, check_interval: int = 100):
+        taken = C.c_int32()
+        e = C.c_double()
+        self._chk(self.lib.rq_solve(self.ctx, float(tol_dE), int(max_steps), int(check_interval), C.byref(taken),
+                                    C.byref(e)), "rq_solve")
+        return taken.value, e.value
+
+    def profile_begin(self):
+        self._chk(self.lib.rq_profile_begin(self.ctx), "rq_profile_begin")
+
+    def profile_end(self) -> dict:
+        """{kernel class: {launches, ms, bytes, gbs}} since profile_begin (CUDA events)."""
+        p = L.Profile()
+        self._chk(self.lib.rq_profile_end(self.ctx, C.byref(p)), "rq_profile_end")
+        out = {}
+        for q, name in enumerate(L.KC_NAMES):
+            if p.launches[q]:
+                out[name] = {"launches": int(p.launches[q]), "ms": float(p.ms[q]), "bytes": float(p.bytes[q]),
+                             "gbs": float(p.bytes[q]) / (float(p.ms[q]) * 1e6) if p.ms[q] > 0 else 0.0}
+        return out
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self.info().kernel_launches)
+
+    # -- state ----------------------------------------------------------------------------
+    def download(self, psi=True, label=True, W=False, P=False):
+        S3 = self.S3
+        if self.fp64:
+            out = {}
+            if psi or P:
+                u = np.empty(S3, np.float64) if psi else None
+                p = np.empty(S3, np.float64) if P else None
+                self._chk(self.lib.rq_download_state_f64(self.ctx, _ptr(u), _ptr(p), None), "rq_download_state_f64")
+                if psi:
+                    out["psi"] = u
+                if P:
+                    out["P"] = p
+            if label or W:
+                lab = np.empty(S3, np.int32) if label else None
+                w = np.empty(S3, np.float32) if W else None
+                self._chk(self.lib.rq_download_state(self.ctx, None, _ptr(lab), _ptr(w), None), "rq_download_state")
+                if label:
+                    out["label"] = lab
+                if W:
+                    out["W"] = w
+            return out
+        u = np.empty(S3, np.float32) if psi else None
+        lab = np.empty(S3, np.int32) if label else None
+        w = np.empty(S3, np.float32) if W else None
+        p = np.empty(S3, np.float32) if P else None
+        self._chk(self.lib.rq_download_state(self.ctx, _ptr(u), _ptr(lab), _ptr(w), _ptr(p)), "rq_download_state")
+        return {k: v for k, v in (("psi", u), ("label", lab), ("W", w), ("P", p)) if v is not None}
+
+    def download_K(self) -> np.ndarray:
+        if self.fp64:
+            k = np.empty(self.S3, np.float64)
+            self._chk(self.lib.rq_download_state_f64(self.ctx, None, None, _ptr(k)), "rq_download_state_f64")
+            return k
+        k = np.empty(self.S3, np.float32)
+        self._chk(self.lib.rq_download_K(self.ctx, _ptr(k)), "rq_download_K")
+        return k
+
+    def upload(self, psi=None, label=None, W=None, P=None):
+        cv = lambda a, t: None if a is None else np.ascontiguousarray(np.asarray(a).reshape(-1), dtype=t)
+        if self.fp64:
+            psi64, P64 = cv(psi, np.float64), cv(P, np.float64)
+            if psi64 is not None or P64 is not None:
+                self._chk(self.lib.rq_upload_state_f64(self.ctx, _ptr(psi64), _ptr(P64)), "rq_upload_state_f64")
+            lab, w = cv(label, np.int32), cv(W, np.float32)
+            if lab is not None or w is not None:
+                self._chk(self.lib.rq_upload_state(self.ctx, None, _ptr(lab), _ptr(w), None), "rq_upload_state")
+            return
+        u, lab, w, p = cv(psi, np.float32), cv(label, np.int32), cv(W, np.float32), cv(P, np.float32)
+        self._chk(self.lib.rq_upload_state(self.ctx, _ptr(u), _ptr(lab), _ptr(w), _ptr(p)), "rq_upload_state")

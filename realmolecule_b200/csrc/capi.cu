@@ -1,0 +1,758 @@
+// capi.cu -- the C ABI of librq (include/rq.h): context lifecycle, state transfer, the
+// per-flavour step schedule (captured as CUDA graphs), energies and forces.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+
+#include "rq_ctx.h"
+#include "rq_flavors.h"
+
+using namespace rq;
+
+int rq_fail(rq_ctx* c, int code, const std::string& msg) {
+  if (c) c->last_error = msg;
+  return code;
+}
+
+int rq_cuda(rq_ctx* c, cudaError_t e, const char* where) {
+  if (e == cudaSuccess) return RQ_OK;
+  if (c) c->last_error = std::string(where) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) return RQ_ENOMEM;
+  return RQ_ECUDA;
+}
+
+#define CK(call)                                        \
+  do {                                                  \
+    int _rc = rq_cuda(c, (call), #call);                \
+    if (_rc != RQ_OK) return _rc;                       \
+  } while (0)
+
+static const char* kStatus[] = {"ok", "invalid argument", "out of memory", "CUDA error",
+                                "non-finite value", "device wait timed out", "not supported", "no CUDA device"};
+
+extern "C" const char* rq_status_string(int s) {
+  if (s > 0 || s < -7) return "unknown status";
+  return kStatus[-s];
+}
+
+extern "C" const char* rq_last_error(const rq_ctx* c) { return c ? c->last_error.c_str() : "null context"; }
+
+// ----------------------------------------------------------------------------------------
+// defaults per flavour
+// ----------------------------------------------------------------------------------------
+static int count_domains(const std::vector<rq_atom>& a) {
+  int n = 0;
+  for (auto& x : a) n += (x.Z > 0);
+  return n;
+}
+
+static double default_dv(const rq_ctx* c) {
+  const int ne = count_domains(c->atoms);
+  switch (c->cfg.flavor) {
+    case RQ_FLAVOR_SOLVER_PY:  // cloud/solver.py:342-351
+      return ne > 500 ? 0.005 : ne > 200 ? 0.01 : ne > 100 ? 0.02 : ne > 30 ? 0.03 : 0.12;
+    case RQ_FLAVOR_MOLECULE_JS: {  // molecule.js:12-17 NELEC counts Z>0 or Z_nuc>0 entries, :78
+      int nel = 0;
+      for (auto& x : c->atoms) nel += (x.Z > 0 || x.Z_nuc > 0);
+      return nel > 500 ? 0.01 : nel > 100 ? 0.03 : 0.12;
+    }
+    default:
+      return 0.2;  // dt = 0.2 h^2
+  }
+}
+
+static void fill_defaults(rq_ctx* c) {
+  rq_config& f = c->cfg;
+  const bool sp = f.flavor == RQ_FLAVOR_SOLVER_PY, mj = f.flavor == RQ_FLAVOR_MOLECULE_JS;
+  if (f.norm_interval <= 0) f.norm_interval = 20;
+  if (f.poisson_interval <= 0) f.poisson_interval = sp ? 2 : 1;
+  if (f.label_interval <= 0) f.label_interval = sp ? 5 * f.norm_interval : 20;
+  if (f.jacobi_per_step <= 0) f.jacobi_per_step = 2;
+  if (f.steps_per_frame <= 0) {  // molecule.js:106
+    int nel = 0;
+    for (auto& x : c->atoms) nel += (x.Z > 0 || x.Z_nuc > 0);
+    f.steps_per_frame = nel <= 30 ? 50 : nel <= 100 ? 5 : 2;
+  }
+  if (f.vcycle_interval <= 0) f.vcycle_interval = 50;
+  if (f.mg_pre <= 0) f.mg_pre = 2;
+  if (f.mg_post <= 0) f.mg_post = 2;
+  if (f.mg_coarse_sweeps <= 0) f.mg_coarse_sweeps = 64;
+  if (f.boundary_speed <= 0) f.boundary_speed = 0.5;
+  if (f.curv_reg < 0 || (mj && f.curv_reg == 0)) f.curv_reg = 0.15;
+  c->dv = f.dv > 0 ? f.dv : default_dv(c);
+  c->half_dv = 0.5 * c->dv;
+  c->dt = c->dv * c->h2;
+  c->sigma = f.sigma > 0 ? f.sigma : c->h;
+}
+
+// ----------------------------------------------------------------------------------------
+// atoms -> device tables
+// ----------------------------------------------------------------------------------------
+static int upload_atoms(rq_ctx* c) {
+  const int n = c->n_atoms;
+  std::vector<float> a5((size_t)n * 5), zd(n);
+  std::vector<double> zd64(n), nm((size_t)n * 4);
+  std::vector<MjAtom> mj(n);
+  for (int q = 0; q < n; ++q) {
+    const rq_atom& a = c->atoms[q];
+    a5[q * 5 + 0] = (float)a.i; a5[q * 5 + 1] = (float)a.j; a5[q * 5 + 2] = (float)a.k;
+    a5[q * 5 + 3] = (float)a.Z; a5[q * 5 + 4] = (float)a.rc;
+    zd[q] = (float)a.Z; zd64[q] = a.Z;
+    // molecule.js:1882-1884 stores positions in a Uint32Array: truncation toward zero
+    mj[q].posI = (uint32_t)(a.i < 0 ? 0 : a.i); mj[q].posJ = (uint32_t)(a.j < 0 ? 0 : a.j);
+    mj[q].posK = (uint32_t)(a.k < 0 ? 0 : a.k);
+    mj[q].Z = (float)a.Z; mj[q].rc = (float)a.rc; mj[q].Z_nuc = (float)a.Z_nuc;
+    mj[q].initZeff = (float)(a.init_zeff > 0 ? a.init_zeff : a.Z);
+    mj[q].initRcut = (float)(a.init_rcut > 0 ? a.init_rcut : 1e6);
+    nm[q * 4 + 0] = a.i * c->h; nm[q * 4 + 1] = a.j * c->h; nm[q * 4 + 2] = a.k * c->h; nm[q * 4 + 3] = a.Z_nuc;
+  }
+  CK(cudaMemcpyAsync(c->atoms5, a5.data(), sizeof(float) * a5.size(), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->Zdom, zd.data(), sizeof(float) * n, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->Zdom64, zd64.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->atoms_mj, mj.data(), sizeof(MjAtom) * n, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->atoms_nm, nm.data(), sizeof(double) * nm.size(), cudaMemcpyHostToDevice, c->st));
+  return cudaStreamSynchronize(c->st) == cudaSuccess ? RQ_OK : rq_cuda(c, cudaGetLastError(), "upload_atoms");
+}
+
+static void free_ctx(rq_ctx* c) {
+  for (auto e : c->evpool) cudaEventDestroy(e);
+  for (auto& gx : c->graph)
+    if (gx) cudaGraphExecDestroy(gx);
+  void* ptrs[] = {c->U[0], c->U[1], c->P[0], c->P[1], c->K, c->W, c->bestU, c->rho, c->Pother, c->lab[0], c->lab[1],
+                  c->Ec[0], c->Ec[1], c->fc, c->atoms5, c->atoms_mj, c->atoms_nm, c->Zdom, c->Zdom64, c->dnorm,
+                  c->dpd, c->dF, c->dsum, c->unorm, c->scale, c->err};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  for (auto& L : c->mg) {
+    if (L.P) cudaFree(L.P);
+    if (L.f) cudaFree(L.f);
+    if (L.r) cudaFree(L.r);
+  }
+  if (c->own_st) cudaStreamDestroy(c->own_st);
+}
+
+static int dalloc(rq_ctx* c, void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) return rq_cuda(c, e, "cudaMalloc");
+  e = cudaMemsetAsync(*p, 0, bytes, c->st);
+  return rq_cuda(c, e, "cudaMemsetAsync");
+}
+#define DALLOC(ptr, bytes)                                        \
+  do {                                                            \
+    int _r = dalloc(c, (void**)&(ptr), (bytes));                  \
+    if (_r != RQ_OK) return _r;                                   \
+  } while (0)
+
+static int alloc_all(rq_ctx* c) {
+  const size_t S3 = (size_t)c->g.S3;
+  const size_t es = c->fp64 ? sizeof(double) : sizeof(float);
+  const int n = c->n_atoms;
+  for (int b = 0; b < 2; ++b) {
+    DALLOC(c->U[b], S3 * es);
+    DALLOC(c->P[b], S3 * es);
+    DALLOC(c->lab[b], S3 * sizeof(int));
+  }
+  DALLOC(c->K, S3 * es);
+  DALLOC(c->W, S3 * sizeof(float));
+  if (c->cfg.flavor == RQ_FLAVOR_SOLVER_PY || c->cfg.flavor == RQ_FLAVOR_MOLECULE_JS) DALLOC(c->bestU, S3 * sizeof(float));
+  if (c->cfg.flavor == RQ_FLAVOR_MOLECULE_JS) {
+    DALLOC(c->rho, S3 * sizeof(float));
+    DALLOC(c->Pother, S3 * sizeof(float));
+    const int SC = c->g.NN / 2 + 1;
+    c->gc = make_geo(SC);
+    const size_t SC3 = (size_t)c->gc.S3;
+    DALLOC(c->Ec[0], SC3 * sizeof(float));
+    DALLOC(c->Ec[1], SC3 * sizeof(float));
+    DALLOC(c->fc, SC3 * sizeof(float));
+  }
+  DALLOC(c->atoms5, sizeof(float) * 5 * n);
+  DALLOC(c->atoms_mj, sizeof(MjAtom) * n);
+  DALLOC(c->atoms_nm, sizeof(double) * 4 * n);
+  DALLOC(c->Zdom, sizeof(float) * n);
+  DALLOC(c->Zdom64, sizeof(double) * n);
+  DALLOC(c->dnorm, sizeof(double) * n);
+  DALLOC(c->dpd, sizeof(double) * 4 * n);
+  DALLOC(c->dF, sizeof(double) * 3 * n);
+  DALLOC(c->dsum, sizeof(double) * 8);
+  DALLOC(c->unorm, sizeof(unsigned) * n);
+  DALLOC(c->scale, sizeof(float) * n);
+  DALLOC(c->err, sizeof(int) * 4);
+  if (c->cfg.flavor == RQ_FLAVOR_NEW) {
+    int r = nm_alloc_levels(c);
+    if (r != RQ_OK) return r;
+  }
+  return RQ_OK;
+}
+
+extern "C" int rq_create(const rq_config* cfg, const rq_atom* atoms, int32_t n_atoms, rq_ctx** out) {
+  if (!cfg || !out || (n_atoms > 0 && !atoms) || n_atoms < 1) return RQ_EINVAL;
+  *out = nullptr;
+  if (cfg->NN < 4 || cfg->NN % 2 != 0 || cfg->screen <= 0) return RQ_EINVAL;  // molecule.js:155 needs even NN
+  if (cfg->flavor < 0 || cfg->flavor > 2 || cfg->precision < 0 || cfg->precision > 1) return RQ_EINVAL;
+  if (cfg->precision == RQ_PREC_FP64 && cfg->flavor != RQ_FLAVOR_NEW) return RQ_ENOTSUP;
+  if (cfg->sic != 0) return RQ_ENOTSUP;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return RQ_ENODEV;
+  rq_ctx* c = new (std::nothrow) rq_ctx();
+  if (!c) return RQ_ENOMEM;
+  c->cfg = *cfg;
+  c->g = make_geo(cfg->NN + 1);
+  c->h = cfg->screen / cfg->NN;
+  c->h2 = c->h * c->h;
+  c->h3 = c->h2 * c->h;
+  c->n_atoms = n_atoms;
+  c->atoms.assign(atoms, atoms + n_atoms);
+  c->fp64 = cfg->precision == RQ_PREC_FP64;
+  cudaGetDevice(&c->device);
+  fill_defaults(c);
+  int rc = rq_cuda(c, cudaStreamCreateWithFlags(&c->own_st, cudaStreamNonBlocking), "cudaStreamCreate");
+  c->st = c->own_st;
+  if (rc == RQ_OK) rc = alloc_all(c);
+  if (rc == RQ_OK) rc = upload_atoms(c);
+  if (rc == RQ_OK) rc = rq_cuda(c, cudaStreamSynchronize(c->st), "create sync");
+  if (rc != RQ_OK) {
+    std::fprintf(stderr, "rq_create: %s\n", c->last_error.c_str());
+    free_ctx(c);
+    delete c;
+    return rc;
+  }
+  *out = c;
+  return RQ_OK;
+}
+
+extern "C" void rq_destroy(rq_ctx* c) {
+  if (!c) return;
+  cudaStreamSynchronize(c->st);
+  free_ctx(c);
+  delete c;
+}
+
+extern "C" int rq_set_stream(rq_ctx* c, void* stream) {
+  if (!c) return RQ_EINVAL;
+  CK(cudaStreamSynchronize(c->st));
+  c->st = stream ? (cudaStream_t)stream : c->own_st;
+  return RQ_OK;
+}
+
+extern "C" int rq_get_info(const rq_ctx* c, rq_info* info) {
+  if (!c || !info) return RQ_EINVAL;
+  std::memset(info, 0, sizeof(*info));
+  info->NN = c->g.NN; info->S = c->g.S; info->n_atoms = c->n_atoms; info->flavor = c->cfg.flavor;
+  info->precision = c->cfg.precision; info->steps_done = c->steps_done; info->mg_levels = (int)c->mg.size();
+  info->h = c->h; info->dv = c->dv; info->dt = c->dt; info->sigma = c->sigma; info->S3 = c->g.S3;
+  info->psi = c->U[c->cu]; info->label = c->lab[c->cl]; info->K = c->K; info->P = c->P[c->cp]; info->W = c->W;
+  info->kernel_launches = c->launches;
+  return RQ_OK;
+}
+
+extern "C" int rq_synchronize(rq_ctx* c) {
+  if (!c) return RQ_EINVAL;
+  CK(cudaStreamSynchronize(c->st));
+  return RQ_OK;
+}
+
+// ----------------------------------------------------------------------------------------
+// solver.py flavour schedule (cloud/solver.py:402-444, :561-586)
+// ----------------------------------------------------------------------------------------
+static double interior_points(const Geo& g) {
+  const double n = g.NN - 1;
+  return n * n * n;
+}
+
+static int sp_normalize(rq_ctx* c, bool accumulate) {
+  float* U = (float*)c->U[c->cu];
+  const double S3 = (double)c->g.S3;
+  if (accumulate) {
+    CK(cudaMemsetAsync(c->dnorm, 0, sizeof(double) * c->n_atoms, c->st));
+    LAUNCH(RQ_KC_NORMALIZE, 8 * S3, launch_norms_flat(U, c->lab[c->cl], c->g, c->h3, c->n_atoms, c->dnorm, c->st));
+  }
+  LAUNCH(RQ_KC_NORMALIZE, 12.0 * c->n_atoms,
+         launch_norm_scale_sp(c->dnorm, c->Zdom, c->n_atoms, c->scale, c->err, c->st));
+  LAUNCH(RQ_KC_NORMALIZE, 12 * S3, launch_apply_scale_sp(U, c->lab[c->cl], c->scale, c->g, c->n_atoms, c->st));
+  return RQ_OK;
+}
+
+static int sp_poisson(rq_ctx* c) {
+  const float coeff = (float)(2.0 * M_PI);
+  for (int q = 0; q < c->cfg.jacobi_per_step; ++q) {
+    LAUNCH(RQ_KC_POISSON, 12 * interior_points(c->g),
+           launch_jacobi_sp((float*)c->P[c->cp], (float*)c->P[1 - c->cp], (float*)c->U[c->cu], c->g, (float)c->h2,
+                            coeff, c->st));
+    c->cp ^= 1;
+  }
+  return RQ_OK;
+}
+
+static int sp_step_one(rq_ctx* c, int s) {
+  const rq_config& f = c->cfg;
+  int rc;
+  if (s % f.poisson_interval == 0 && (rc = sp_poisson(c)) != RQ_OK) return rc;
+  const bool norm = s % f.norm_interval == 0;
+  if (norm) CK(cudaMemsetAsync(c->dnorm, 0, sizeof(double) * c->n_atoms, c->st));
+  LAUNCH(RQ_KC_UPDATE, 20 * interior_points(c->g),
+         launch_update_sp((float*)c->U[c->cu], (float*)c->U[1 - c->cu], (float*)c->K, (float*)c->P[c->cp],
+                          c->lab[c->cl], c->g, (float)c->half_dv, (float)c->dt, c->h3, c->n_atoms,
+                          norm ? c->dnorm : nullptr, c->st));
+  c->cu ^= 1;
+  if (norm && (rc = sp_normalize(c, false)) != RQ_OK) return rc;
+  if (s % f.label_interval == 0) {
+    LAUNCH(RQ_KC_LABELS, 8 * interior_points(c->g),
+           launch_labels_sp(c->lab[c->cl], c->lab[1 - c->cl], c->atoms5, c->n_atoms, c->g, (float)c->h,
+                            (float)c->h2, c->st));
+    c->cl ^= 1;
+  }
+  return RQ_OK;
+}
+
+static int sp_initialize(rq_ctx* c) {
+  for (int b = 0; b < 2; ++b) {
+    CK(cudaMemsetAsync(c->P[b], 0, sizeof(float) * c->g.S3, c->st));
+  }
+  c->cu = c->cp = c->cl = 0;
+  LAUNCH(RQ_KC_OTHER, 16.0 * c->g.S3,
+         launch_init_sp((float*)c->U[0], c->lab[0], (float*)c->K, c->bestU, c->atoms5, c->n_atoms, c->g, (float)c->h,
+                        (float)c->h2, true, c->st));
+  CK(cudaMemcpyAsync(c->lab[1], c->lab[0], sizeof(int) * c->g.S3, cudaMemcpyDeviceToDevice, c->st));
+  int rc = sp_normalize(c, true);
+  if (rc != RQ_OK) return rc;
+  for (int q = 0; q < 100; ++q)
+    if ((rc = sp_poisson(c)) != RQ_OK) return rc;
+  return RQ_OK;
+}
+
+// ----------------------------------------------------------------------------------------
+// generic step driver with CUDA-graph replay of whole schedule periods
+// ----------------------------------------------------------------------------------------
+static int step_one(rq_ctx* c, int s) {
+  switch (c->cfg.flavor) {
+    case RQ_FLAVOR_SOLVER_PY: return sp_step_one(c, s);
+    case RQ_FLAVOR_MOLECULE_JS: return mj_step_one(c, s);
+    default: return nm_step_one(c, s);
+  }
+}
+
+static int schedule_period(const rq_ctx* c) {
+  const rq_config& f = c->cfg;
+  auto lcm = [](long a, long b) { return a / std::gcd(a, b) * b; };
+  long p = 1;
+  switch (f.flavor) {
+    case RQ_FLAVOR_SOLVER_PY: p = lcm(lcm(f.poisson_interval, f.norm_interval), f.label_interval); break;
+    case RQ_FLAVOR_MOLECULE_JS: p = f.steps_per_frame; break;
+    default: p = lcm(lcm(f.poisson_interval, f.norm_interval), f.label_interval); break;
+  }
+  return p > 4096 ? 0 : (int)p;
+}
+
+static int run_steps_eager(rq_ctx* c, int n) {
+  for (int q = 0; q < n; ++q) {
+    int rc = step_one(c, c->steps_done + 1);
+    if (rc != RQ_OK) return rc;
+    c->steps_done++;
+  }
+  return RQ_OK;
+}
+
+extern "C" int rq_step(rq_ctx* c, int32_t n) {
+  if (!c || n < 0) return RQ_EINVAL;
+  const int period = schedule_period(c);
+  int left = n;
+  while (left > 0) {
+    const bool aligned = !c->prof && period > 0 && c->steps_done % period == 0 && left >= period;
+    if (!aligned) {
+      // run eagerly up to the next period boundary (or all that is left)
+      int todo = left;
+      if (period > 0 && c->steps_done % period != 0) todo = std::min(left, period - c->steps_done % period);
+      int rc = run_steps_eager(c, todo);
+      if (rc != RQ_OK) return rc;
+      left -= todo;
+      continue;
+    }
+    // one aligned period: replay its CUDA graph (captured on first use for this buffer parity)
+    const int key = c->cu | (c->cp << 1) | (c->cl << 2);
+    if (!c->graph[key]) {
+      const long long l0 = c->launches;
+      CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+      int rc = run_steps_eager(c, period);  // records the work and advances the parities
+      cudaGraph_t gr = nullptr;
+      cudaError_t e = cudaStreamEndCapture(c->st, &gr);
+      if (rc != RQ_OK) {
+        if (gr) cudaGraphDestroy(gr);
+        return rc;
+      }
+      CK(e);
+      e = cudaGraphInstantiate(&c->graph[key], gr, 0);
+      cudaGraphDestroy(gr);
+      CK(e);
+      c->graph_post[key] = c->cu | (c->cp << 1) | (c->cl << 2);
+      c->graph_launches[key] = c->launches - l0;
+      CK(cudaGraphLaunch(c->graph[key], c->st));
+    } else {
+      CK(cudaGraphLaunch(c->graph[key], c->st));
+      const int post = c->graph_post[key];
+      c->cu = post & 1; c->cp = (post >> 1) & 1; c->cl = (post >> 2) & 1;
+      c->steps_done += period;
+      c->launches += c->graph_launches[key];
+    }
+    left -= period;
+  }
+  return RQ_OK;
+}
+
+extern "C" int rq_initialize(rq_ctx* c) {
+  if (!c) return RQ_EINVAL;
+  int rc;
+  switch (c->cfg.flavor) {
+    case RQ_FLAVOR_SOLVER_PY: rc = sp_initialize(c); break;
+    case RQ_FLAVOR_MOLECULE_JS: rc = mj_initialize(c); break;
+    default: rc = nm_initialize(c); break;
+  }
+  if (rc != RQ_OK) return rc;
+  c->steps_done = 0;
+  c->frame = 0;
+  CK(cudaStreamSynchronize(c->st));
+  return RQ_OK;
+}
+
+// ----------------------------------------------------------------------------------------
+// state transfer
+// ----------------------------------------------------------------------------------------
+static int check_labels(rq_ctx* c, const int32_t* label) {
+  for (long long q = 0; q < c->g.S3; ++q)
+    if (label[q] < 0 || label[q] >= c->n_atoms)
+      return rq_fail(c, RQ_EINVAL, "label " + std::to_string(label[q]) + " at index " + std::to_string(q) +
+                                       " outside [0, n_atoms)");
+  return RQ_OK;
+}
+
+extern "C" int rq_upload_state(rq_ctx* c, const float* psi, const int32_t* label, const float* W, const float* P) {
+  if (!c) return RQ_EINVAL;
+  if (c->fp64 && (psi || P)) return rq_fail(c, RQ_EINVAL, "FP64 context: use rq_upload_state_f64 for psi/P");
+  const size_t n = (size_t)c->g.S3;
+  if (label) {
+    int rc = check_labels(c, label);
+    if (rc != RQ_OK) return rc;
+    CK(cudaMemcpyAsync(c->lab[c->cl], label, n * sizeof(int), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->lab[1 - c->cl], c->lab[c->cl], n * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+  }
+  if (psi) {
+    CK(cudaMemcpyAsync(c->U[c->cu], psi, n * sizeof(float), cudaMemcpyHostToDevice, c->st));
+    CK(launch_zero_faces((float*)c->U[c->cu], c->g, c->st));  // Dirichlet planes are 0
+  }
+  if (W) CK(cudaMemcpyAsync(c->W, W, n * sizeof(float), cudaMemcpyHostToDevice, c->st));
+  if (P) {
+    CK(cudaMemcpyAsync(c->P[c->cp], P, n * sizeof(float), cudaMemcpyHostToDevice, c->st));
+    CK(launch_zero_faces((float*)c->P[c->cp], c->g, c->st));
+    if (c->Pother) CK(cudaMemcpyAsync(c->Pother, c->P[c->cp], n * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
+  }
+  CK(cudaStreamSynchronize(c->st));
+  return RQ_OK;
+}
+
+extern "C" int rq_download_state(rq_ctx* c, float* psi, int32_t* label, float* W, float* P) {
+  if (!c) return RQ_EINVAL;
+  if (c->fp64 && (psi || P)) return rq_fail(c, RQ_EINVAL, "FP64 context: use rq_download_state_f64 for psi/P");
+  const size_t n = (size_t)c->g.S3;
+  if (psi) CK(cudaMemcpyAsync(psi, c->U[c->cu], n * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+  if (label) CK(cudaMemcpyAsync(label, c->lab[c->cl], n * sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  if (W) CK(cudaMemcpyAsync(W, c->W, n * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+  if (P) CK(cudaMemcpyAsync(P, c->P[c->cp], n * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return RQ_OK;
+}
+
+extern "C" int rq_upload_state_f64(rq_ctx* c, const double* psi, const double* P) {
+  if (!c) return RQ_EINVAL;
+  if (!c->fp64) return rq_fail(c, RQ_EINVAL, "mixed-precision context: use rq_upload_state");
+  const size_t n = (size_t)c->g.S3;
+  if (psi) {
+    CK(cudaMemcpyAsync(c->U[c->cu], psi, n * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(launch_zero_faces((double*)c->U[c->cu], c->g, c->st));
+  }
+  if (P) {
+    CK(cudaMemcpyAsync(c->P[c->cp], P, n * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(launch_zero_faces((double*)c->P[c->cp], c->g, c->st));
+  }
+  CK(cudaStreamSynchronize(c->st));
+  return RQ_OK;
+}
+
+extern "C" int rq_download_state_f64(rq_ctx* c, double* psi, double* P, double* K) {
+  if (!c) return RQ_EINVAL;
+  if (!c->fp64) return rq_fail(c, RQ_EINVAL, "mixed-precision context: use rq_download_state");
+  const size_t n = (size_t)c->g.S3;
+  if (psi) CK(cudaMemcpyAsync(psi, c->U[c->cu], n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  if (P) CK(cudaMemcpyAsync(P, c->P[c->cp], n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  if (K) CK(cudaMemcpyAsync(K, c->K, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return RQ_OK;
+}
+
+extern "C" int rq_download_K(rq_ctx* c, float* K) {
+  if (!c || !K) return RQ_EINVAL;
+  if (c->fp64) return rq_fail(c, RQ_EINVAL, "FP64 context: use rq_download_state_f64");
+  CK(cudaMemcpyAsync(K, c->K, (size_t)c->g.S3 * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return RQ_OK;
+}
+
+// ----------------------------------------------------------------------------------------
+// atoms, energies, forces
+// ----------------------------------------------------------------------------------------
+extern "C" int rq_set_atoms(rq_ctx* c, const rq_atom* atoms, int32_t n) {
+  if (!c || !atoms || n != c->n_atoms) return RQ_EINVAL;
+  c->atoms.assign(atoms, atoms + n);  // tables are rewritten in place: captured graphs stay valid
+  int rc = upload_atoms(c);
+  if (rc != RQ_OK) return rc;
+  switch (c->cfg.flavor) {
+    case RQ_FLAVOR_SOLVER_PY:  // cloud/solver.py:538-548 recomputeK
+      CK(launch_init_sp(nullptr, nullptr, (float*)c->K, nullptr, c->atoms5, c->n_atoms, c->g, (float)c->h,
+                        (float)c->h2, false, c->st));
+      break;
+    case RQ_FLAVOR_MOLECULE_JS:
+      rc = mj_set_atoms(c);
+      break;
+    default:
+      rc = nm_set_atoms(c);
+      break;
+  }
+  if (rc != RQ_OK) return rc;
+  CK(cudaStreamSynchronize(c->st));
+  return RQ_OK;
+}
+
+static void fill_domains(rq_ctx* c, const std::vector<double>& pd, double* out, double* per_domain) {
+  double T = 0, EK = 0, EE = 0;
+  for (int q = 0; q < c->n_atoms; ++q) {
+    T += pd[q * 4 + 1]; EK += pd[q * 4 + 2]; EE += pd[q * 4 + 3];
+    if (per_domain) {
+      double* d = per_domain + (size_t)q * RQ_DOMAIN_LEN;
+      d[RQ_D_NORM] = pd[q * 4]; d[RQ_D_T] = pd[q * 4 + 1]; d[RQ_D_EK] = pd[q * 4 + 2]; d[RQ_D_EE] = pd[q * 4 + 3];
+      const double nr = pd[q * 4] != 0 ? pd[q * 4] : 1.0;  // atom.js:340 eigenvalue (|| 1)
+      d[RQ_D_EIG] = (pd[q * 4 + 1] + 2 * pd[q * 4 + 3] + pd[q * 4 + 2]) / nr;
+    }
+  }
+  out[RQ_E_T] = T; out[RQ_E_EK] = EK; out[RQ_E_EE] = EE;
+}
+
+extern "C" int rq_nuclear_terms(rq_ctx* c, double* E_KK, double* F) {
+  if (!c) return RQ_EINVAL;
+  const int n = c->n_atoms;
+  const double h = c->h;
+  std::vector<double> f((size_t)n * 3, 0.0);
+  double e = 0;
+  if (c->cfg.flavor == RQ_FLAVOR_SOLVER_PY) {
+    // cloud/solver.py:462-474 energy and :504-520 forces: softening h^2, charges Z_eff
+    for (int a = 0; a < n; ++a) {
+      if (c->atoms[a].Z <= 0) continue;
+      for (int b = 0; b < n; ++b) {
+        if (b == a || c->atoms[b].Z <= 0) continue;
+        const double dx = (double)(float)c->atoms[a].i - (double)(float)c->atoms[b].i;
+        const double dy = (double)(float)c->atoms[a].j - (double)(float)c->atoms[b].j;
+        const double dz = (double)(float)c->atoms[a].k - (double)(float)c->atoms[b].k;
+        const double r2 = (dx * dx + dy * dy + dz * dz) * h * h + h * h;
+        const double zz = (double)(float)c->atoms[a].Z * (double)(float)c->atoms[b].Z;
+        if (b > a) e += zz / std::sqrt(r2);
+        const double w = zz / (r2 * std::sqrt(r2));
+        f[a * 3] += w * dx * h; f[a * 3 + 1] += w * dy * h; f[a * 3 + 2] += w * dz * h;
+      }
+    }
+  } else if (c->cfg.flavor == RQ_FLAVOR_MOLECULE_JS) {
+    mj_nuclear_terms(c, &e, f.data());
+  } else {
+    nm_nuclear_terms(c, &e, f.data());
+  }
+  if (E_KK) *E_KK = e;
+  if (F) std::memcpy(F, f.data(), sizeof(double) * f.size());
+  return RQ_OK;
+}
+
+extern "C" int rq_energy(rq_ctx* c, double* out, double* per_domain) {
+  if (!c || !out) return RQ_EINVAL;
+  for (int q = 0; q < RQ_ENERGY_LEN; ++q) out[q] = 0;
+  int rc = RQ_OK;
+  if (c->cfg.flavor == RQ_FLAVOR_SOLVER_PY) {
+    const int n = c->n_atoms;
+    CK(cudaMemsetAsync(c->dpd, 0, sizeof(double) * 4 * n, c->st));
+    CK(launch_energy_sp((float*)c->U[c->cu], (float*)c->K, (float*)c->P[c->cp], c->lab[c->cl], c->g, c->h, c->h3, n,
+                        c->dpd, c->st));
+    std::vector<double> pd((size_t)4 * n);
+    CK(cudaMemcpyAsync(pd.data(), c->dpd, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    fill_domains(c, pd, out, per_domain);
+  } else if (c->cfg.flavor == RQ_FLAVOR_MOLECULE_JS) {
+    rc = mj_energy(c, out, per_domain);
+  } else {
+    rc = nm_energy(c, out, per_domain);
+  }
+  if (rc != RQ_OK) return rc;
+  double ekk = 0;
+  rq_nuclear_terms(c, &ekk, nullptr);
+  out[RQ_E_KK] = ekk;
+  out[RQ_E_TOTAL] = out[RQ_E_T] + out[RQ_E_EK] + out[RQ_E_EE] + out[RQ_E_KK];
+  for (int q = 0; q < RQ_ENERGY_LEN; ++q)
+    if (!std::isfinite(out[q])) return rq_fail(c, RQ_ENONFINITE, "non-finite energy component");
+  return RQ_OK;
+}
+
+extern "C" int rq_forces(rq_ctx* c, int32_t method, double* F) {
+  if (!c || !F) return RQ_EINVAL;
+  const int n = c->n_atoms;
+  if (c->cfg.flavor == RQ_FLAVOR_SOLVER_PY) {
+    if (method != RQ_FORCE_HF && method != RQ_FORCE_ADJOINT) return RQ_ENOTSUP;
+    CK(cudaMemsetAsync(c->dF, 0, sizeof(double) * 3 * n, c->st));
+    CK(launch_forces_hf_sp((float*)c->U[c->cu], c->atoms5, n, c->g, (float)c->h, (float)c->h2, (float)c->h3, c->dF,
+                           c->st));
+    CK(cudaMemcpyAsync(F, c->dF, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return RQ_OK;
+  }
+  if (c->cfg.flavor == RQ_FLAVOR_MOLECULE_JS) return mj_forces(c, method, F);
+  return nm_forces(c, method, F);
+}
+
+extern "C" int rq_solve(rq_ctx* c, double tol_dE, int32_t max_steps, int32_t check_interval, int32_t* steps_taken,
+                        double* E_final) {
+  if (!c || max_steps < 0 || check_interval <= 0) return RQ_EINVAL;
+  double e[RQ_ENERGY_LEN];
+  int rc = rq_energy(c, e, nullptr);
+  if (rc != RQ_OK) return rc;
+  double prev = e[RQ_E_TOTAL];
+  int taken = 0;
+  while (taken < max_steps) {
+    const int n = std::min(check_interval, max_steps - taken);
+    if ((rc = rq_step(c, n)) != RQ_OK) return rc;
+    taken += n;
+    if ((rc = rq_energy(c, e, nullptr)) != RQ_OK) return rc;
+    const double d = std::fabs(e[RQ_E_TOTAL] - prev);
+    prev = e[RQ_E_TOTAL];
+    if (d < tol_dE) break;
+  }
+  if (steps_taken) *steps_taken = taken;
+  if (E_final) *E_final = prev;
+  return RQ_OK;
+}
+
+// ----------------------------------------------------------------------------------------
+// single kernels on caller-owned device memory
+// ----------------------------------------------------------------------------------------
+#define KCHK(call)                                   \
+  do {                                               \
+    cudaError_t _e = (call);                         \
+    if (_e != cudaSuccess) return RQ_ECUDA;          \
+  } while (0)
+
+extern "C" int rq_kernel_update_sp(const float* U, float* Unew, const float* K, const float* P, const int32_t* label,
+                                   int32_t S, float half_dv, float dtv, void* stream) {
+  if (!U || !Unew || !K || !P || !label || S < 3) return RQ_EINVAL;
+  Geo g = make_geo(S);
+  cudaStream_t st = (cudaStream_t)stream;
+  KCHK(launch_update_sp(U, Unew, K, P, label, g, half_dv, dtv, 0.0, 1, nullptr, st));
+  KCHK(launch_zero_faces(Unew, g, st));
+  return RQ_OK;
+}
+
+extern "C" int rq_kernel_jacobi_sp(const float* P, float* Pnew, const float* U, int32_t S, float h2, float coeff,
+                                   void* stream) {
+  if (!P || !Pnew || !U || S < 3) return RQ_EINVAL;
+  Geo g = make_geo(S);
+  cudaStream_t st = (cudaStream_t)stream;
+  KCHK(launch_jacobi_sp(P, Pnew, U, g, h2, coeff, st));
+  KCHK(launch_zero_faces(Pnew, g, st));
+  return RQ_OK;
+}
+
+extern "C" int rq_kernel_labels_sp(const int32_t* labelIn, int32_t* labelOut, const float* atoms5, int32_t n_atoms,
+                                   int32_t S, float h, float h2, void* stream) {
+  if (!labelIn || !labelOut || !atoms5 || n_atoms < 1 || S < 3 || labelIn == labelOut) return RQ_EINVAL;
+  Geo g = make_geo(S);
+  cudaStream_t st = (cudaStream_t)stream;
+  KCHK(cudaMemcpyAsync(labelOut, labelIn, sizeof(int) * g.S3, cudaMemcpyDeviceToDevice, st));
+  KCHK(launch_labels_sp(labelIn, labelOut, atoms5, n_atoms, g, h, h2, st));
+  return RQ_OK;
+}
+
+extern "C" int rq_kernel_init_sp(float* U, int32_t* label, float* K, float* bestU, const float* atoms5,
+                                 int32_t n_atoms, int32_t S, float h, float h2, void* stream) {
+  if (!U || !label || !K || !bestU || !atoms5 || n_atoms < 1 || S < 3) return RQ_EINVAL;
+  KCHK(launch_init_sp(U, label, K, bestU, atoms5, n_atoms, make_geo(S), h, h2, true, (cudaStream_t)stream));
+  return RQ_OK;
+}
+
+extern "C" int rq_kernel_recompute_k_sp(float* K, const float* atoms5, int32_t n_atoms, int32_t S, float h, float h2,
+                                        void* stream) {
+  if (!K || !atoms5 || n_atoms < 1 || S < 3) return RQ_EINVAL;
+  KCHK(launch_init_sp(nullptr, nullptr, K, nullptr, atoms5, n_atoms, make_geo(S), h, h2, false,
+                      (cudaStream_t)stream));
+  return RQ_OK;
+}
+
+extern "C" int rq_kernel_normalize_sp(float* U, const int32_t* label, const float* Zeff, int32_t n_atoms, int32_t S,
+                                      float h3, double* norms_out, void* stream) {
+  if (!U || !label || !Zeff || n_atoms < 1 || S < 3) return RQ_EINVAL;
+  Geo g = make_geo(S);
+  cudaStream_t st = (cudaStream_t)stream;
+  double* norms = norms_out;
+  float* scale = nullptr;
+  int* err = nullptr;
+  // scratch for the per-domain sums when the caller passes none, the scale table and the error word
+  if (!norms) KCHK(cudaMallocAsync((void**)&norms, sizeof(double) * n_atoms, st));
+  KCHK(cudaMallocAsync((void**)&scale, sizeof(float) * n_atoms, st));
+  KCHK(cudaMallocAsync((void**)&err, sizeof(int), st));
+  KCHK(cudaMemsetAsync(norms, 0, sizeof(double) * n_atoms, st));
+  KCHK(cudaMemsetAsync(err, 0, sizeof(int), st));
+  KCHK(launch_norms_flat(U, label, g, (double)h3, n_atoms, norms, st));
+  KCHK(launch_norm_scale_sp(norms, Zeff, n_atoms, scale, err, st));
+  KCHK(launch_apply_scale_sp(U, label, scale, g, n_atoms, st));
+  if (!norms_out) KCHK(cudaFreeAsync(norms, st));
+  KCHK(cudaFreeAsync(scale, st));
+  KCHK(cudaFreeAsync(err, st));
+  return RQ_OK;
+}
+
+extern "C" int rq_kernel_energy_sp(const float* U, const float* K, const float* P, const int32_t* label,
+                                   int32_t n_atoms, int32_t S, float h, float h3, double* per_domain, void* stream) {
+  if (!U || !K || !P || !label || !per_domain || n_atoms < 1 || S < 3) return RQ_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  KCHK(cudaMemsetAsync(per_domain, 0, sizeof(double) * 4 * n_atoms, st));
+  KCHK(launch_energy_sp(U, K, P, label, make_geo(S), (double)h, (double)h3, n_atoms, per_domain, st));
+  return RQ_OK;
+}
+
+extern "C" int rq_kernel_forces_hf_sp(const float* U, const float* atoms5, int32_t n_atoms, int32_t S, float h,
+                                      float h2, float h3, double* F, void* stream) {
+  if (!U || !atoms5 || !F || n_atoms < 1 || S < 3) return RQ_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  KCHK(cudaMemsetAsync(F, 0, sizeof(double) * 3 * n_atoms, st));
+  KCHK(launch_forces_hf_sp(U, atoms5, n_atoms, make_geo(S), h, h2, h3, F, st));
+  return RQ_OK;
+}
+
+// ----------------------------------------------------------------------------------------
+// per-kernel profile
+// ----------------------------------------------------------------------------------------
+extern "C" int rq_profile_begin(rq_ctx* c) {
+  if (!c) return RQ_EINVAL;
+  CK(cudaStreamSynchronize(c->st));
+  c->prec.clear();
+  c->evused = 0;
+  c->prof = true;
+  return RQ_OK;
+}
+
+extern "C" int rq_profile_end(rq_ctx* c, rq_profile* out) {
+  if (!c || !out) return RQ_EINVAL;
+  CK(cudaStreamSynchronize(c->st));
+  std::memset(out, 0, sizeof(*out));
+  for (auto& r : c->prec) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, r.a, r.b));
+    out->launches[r.cls] += 1;
+    out->ms[r.cls] += ms;
+    out->bytes[r.cls] += r.bytes;
+  }
+  c->prec.clear();
+  c->evused = 0;
+  c->prof = false;
+  return RQ_OK;
+}

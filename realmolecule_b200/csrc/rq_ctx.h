@@ -1,0 +1,112 @@
+// rq_ctx.h -- the context object behind the C ABI (internal).
+#pragma once
+#include <string>
+#include <vector>
+
+#include "../../include/rq.h"
+#include "rq_kernels.h"
+
+struct rq_ctx;
+int rq_fail(rq_ctx* c, int code, const std::string& msg);
+int rq_cuda(rq_ctx* c, cudaError_t e, const char* where);
+
+struct rq_mg_level {  // one level of the new flavour's multigrid hierarchy
+  rq::Geo g;
+  double h;
+  void* P = nullptr;  // solution / correction (T)
+  void* f = nullptr;  // right-hand side (T)
+  void* r = nullptr;  // residual (T)
+};
+
+struct rq_ctx {
+  rq_config cfg{};
+  rq::Geo g{};
+  double h = 0, h2 = 0, h3 = 0, dv = 0, dt = 0, half_dv = 0, sigma = 0;
+  int n_atoms = 0;
+  std::vector<rq_atom> atoms;
+  bool fp64 = false;
+  cudaStream_t st = nullptr;
+  cudaStream_t own_st = nullptr;
+  int device = 0;
+
+  // fields: psi, P double-buffered; labels double-buffered; T = float or double by precision
+  void* U[2] = {nullptr, nullptr};
+  void* P[2] = {nullptr, nullptr};
+  void* K = nullptr;
+  float* W = nullptr;
+  float* bestU = nullptr;
+  float* rho = nullptr;   // molecule.js rhoTotal / residual scratch (float)
+  float* Pother = nullptr;  // molecule.js PotherBuf (stale P of the previous frame)
+  int* lab[2] = {nullptr, nullptr};
+  int cu = 0, cp = 0, cl = 0;
+
+  // molecule.js coarse grid (2-level V-cycle) buffers
+  rq::Geo gc{};
+  float* Ec[2] = {nullptr, nullptr};
+  float* fc = nullptr;
+
+  // new flavour multigrid hierarchy (level 0 = fine)
+  std::vector<rq_mg_level> mg;
+
+  // atoms on the device
+  float* atoms5 = nullptr;    // [i,j,k,Z,rc] f32 (cloud/solver.py:378-382)
+  void* atoms_mj = nullptr;   // molecule.js records (u32 positions)
+  double* atoms_nm = nullptr; // new flavour: x,y,z (bohr), Z_nuc per atom
+  float* Zdom = nullptr;      // domain charge per label (f32)
+  double* Zdom64 = nullptr;
+
+  // FP64 per-domain sums and outputs
+  double* dnorm = nullptr;    // n_atoms
+  double* dpd = nullptr;      // n_atoms x 4
+  double* dF = nullptr;       // n_atoms x 3
+  double* dsum = nullptr;     // 8 global sums (energies / dipole)
+  unsigned* unorm = nullptr;  // molecule.js fixed-point norms (n_atoms)
+  float* scale = nullptr;     // n_atoms
+  int* err = nullptr;         // device error word
+
+  int steps_done = 0;
+  int frame = 0;
+  std::string last_error;
+
+  // CUDA graphs of one schedule period, keyed by buffer parity (cu, cp, cl)
+  cudaGraphExec_t graph[8] = {};
+  int graph_post[8] = {};
+  long long graph_launches[8] = {};
+
+  // launch accounting and the optional per-kernel profile
+  long long launches = 0;
+  bool prof = false;
+  struct ProfRec { cudaEvent_t a, b; int cls; double bytes; };
+  std::vector<ProfRec> prec;
+  std::vector<cudaEvent_t> evpool;
+  size_t evused = 0;
+};
+
+// Launch wrapper: counts the launch and, while profiling, brackets it with CUDA events.
+template <class F>
+inline int rq_launch(rq_ctx* c, int cls, double bytes, F&& f) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (c->prof) {
+    while (c->evpool.size() < c->evused + 2) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return rq_cuda(c, cudaGetLastError(), "cudaEventCreate");
+      c->evpool.push_back(e);
+    }
+    a = c->evpool[c->evused++];
+    b = c->evpool[c->evused++];
+    cudaEventRecord(a, c->st);
+  }
+  cudaError_t e = f();
+  if (c->prof) {
+    cudaEventRecord(b, c->st);
+    c->prec.push_back({a, b, cls, bytes});
+  }
+  c->launches++;
+  return rq_cuda(c, e, "kernel launch");
+}
+#define LAUNCH(cls, bytes, call)                                               \
+  do {                                                                         \
+    int _lr = rq_launch(c, (cls), (double)(bytes), [&]() { return (call); });  \
+    if (_lr != RQ_OK) return _lr;                                              \
+  } while (0)
+

@@ -1,0 +1,27 @@
+// rq_flavors.h -- per-flavour schedule entry points used by capi.cu (internal).
+#pragma once
+#include "rq_ctx.h"
+
+// molecule.js atom record on the device (molecule.js:183-191 without the split fields):
+// positions are unsigned integers, as the Uint32Array store of :1882-1884 leaves them.
+struct MjAtom {
+  uint32_t posI, posJ, posK;
+  float Z, rc, Z_nuc, initZeff, initRcut;
+};
+
+// molecule.js flavour (mj_flavor.cu)
+int mj_initialize(rq_ctx* c);
+int mj_step_one(rq_ctx* c, int s);
+int mj_energy(rq_ctx* c, double* out, double* per_domain);
+int mj_forces(rq_ctx* c, int method, double* F);
+int mj_set_atoms(rq_ctx* c);
+void mj_nuclear_terms(rq_ctx* c, double* E, double* F);
+
+// new flavour (nm_flavor.cu)
+int nm_alloc_levels(rq_ctx* c);
+int nm_initialize(rq_ctx* c);
+int nm_step_one(rq_ctx* c, int s);
+int nm_energy(rq_ctx* c, double* out, double* per_domain);
+int nm_forces(rq_ctx* c, int method, double* F);
+int nm_set_atoms(rq_ctx* c);
+void nm_nuclear_terms(rq_ctx* c, double* E, double* F);

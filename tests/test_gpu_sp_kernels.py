@@ -1,0 +1,157 @@
+"""solver.py-flavour kernels on the GPU against the oracle and the reference's golden vectors.
+
+Bar: bit-exact for the update, the Jacobi sweep, K and the labels (same IEEE f32 operations in
+the reference's order, no contraction); FP64 sums within 1e-12 relative; the init trial psi
+(which goes through expf) within 2 ulp, with labels equal except where the two best trial
+values are within that error.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as orc
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from realmolecule_b200 import _lib
+    return _lib.load()
+
+
+@pytest.fixture(scope="module")
+def g():
+    return dict(np.load(os.path.join(GOLD, "solverpy_kernels_nn16.npz")))
+
+
+def seeded(NN, nA, seed):
+    import sys
+    sys.path.insert(0, GOLD)
+    from make_golden import seeded_state
+    return seeded_state(NN, nA, seed)
+
+
+CASES = [("golden16", None), ("nn32", (32, 6, 1)), ("nn64", (64, 12, 2)), ("nn90", (90, 40, 3))]
+
+
+def state(case, g):
+    name, spec = case
+    if spec is None:
+        return int(g["NN"]), float(g["h"]), {k[3:]: g[k] for k in g if k.startswith("in_")}
+    NN, nA, seed = spec
+    return NN, 8.0 / NN, seeded(NN, nA, seed)
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_update_bit_exact(lib, g, case):
+    from gpu_util import dev, host, ptr, stream, bits_equal
+    NN, h, st = state(case, g)
+    S = NN + 1
+    half_dv, dtv = np.float32(0.06), np.float32(0.12 * h * h)
+    ref = np.zeros_like(st["U"])
+    orc.O().sp_update(st["U"], ref, st["K"], st["P"], st["label"], S, half_dv, dtv)
+    U, K, P, L = dev(st["U"]), dev(st["K"]), dev(st["P"]), dev(st["label"])
+    out = dev(np.full_like(st["U"], 7.0))
+    assert lib.rq_kernel_update_sp(ptr(U), ptr(out), ptr(K), ptr(P), ptr(L), S, half_dv, dtv, stream()) == 0
+    assert bits_equal(host(out), ref)
+    if case[1] is None:
+        assert bits_equal(host(out), g["out_updateU"])
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_jacobi_bit_exact(lib, g, case):
+    from gpu_util import dev, host, ptr, stream, bits_equal
+    NN, h, st = state(case, g)
+    S = NN + 1
+    ref = np.zeros_like(st["P"])
+    orc.O().sp_jacobi(st["P"], ref, st["U"], S, np.float32(h * h), np.float32(2 * np.pi))
+    P, U = dev(st["P"]), dev(st["U"])
+    out = dev(np.full_like(st["P"], 3.0))
+    assert lib.rq_kernel_jacobi_sp(ptr(P), ptr(out), ptr(U), S, np.float32(h * h), np.float32(2 * np.pi), stream()) == 0
+    assert bits_equal(host(out), ref)
+    if case[1] is None:
+        assert bits_equal(host(out), g["out_jacobiStep"])
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_labels_bit_exact(lib, g, case):
+    from gpu_util import dev, host, ptr, stream
+    NN, h, st = state(case, g)
+    S = NN + 1
+    nA = st["atoms5"].size // 5
+    ref = np.zeros_like(st["label"])
+    orc.O().sp_boundary_snapshot(st["label"], ref, st["atoms5"], nA, S, np.float32(h), np.float32(h * h))
+    assert (ref != st["label"]).sum() > 0  # the case exercises flips
+    Lin, A = dev(st["label"]), dev(st["atoms5"])
+    out = dev(np.zeros_like(st["label"]))
+    assert lib.rq_kernel_labels_sp(ptr(Lin), ptr(out), ptr(A), nA, S, np.float32(h), np.float32(h * h), stream()) == 0
+    assert np.array_equal(host(out), ref)
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_init_and_recompute_k(lib, g, case):
+    from gpu_util import dev, host, ptr, stream, bits_equal
+    NN, h, st = state(case, g)
+    S = NN + 1
+    S3 = S ** 3
+    nA = st["atoms5"].size // 5
+    U, K, B = (np.zeros(S3, np.float32) for _ in range(3))
+    lab = np.zeros(S3, np.int32)
+    orc.O().sp_init_trial(U, lab, K, B, st["atoms5"], nA, S, np.float32(h), np.float32(h * h))
+    dU, dK, dB, dL, A = dev(U * 0), dev(K * 0), dev(B * 0), dev(lab * 0), dev(st["atoms5"])
+    assert lib.rq_kernel_init_sp(ptr(dU), ptr(dL), ptr(dK), ptr(dB), ptr(A), nA, S, np.float32(h),
+                                 np.float32(h * h), stream()) == 0
+    assert bits_equal(host(dK), K)
+    gu, gl = host(dU), host(dL)
+    np.testing.assert_allclose(gu, U, rtol=3e-7, atol=0)
+    bad = np.flatnonzero(gl != lab)
+    assert bad.size <= max(3, S3 // 100000)
+    for q in bad:  # a label may differ only where two atoms' trial values are within ~2 ulp
+        assert abs(gu[q] - U[q]) <= 3e-7 * abs(U[q])
+    K2 = dev(K * 0)
+    assert lib.rq_kernel_recompute_k_sp(ptr(K2), ptr(A), nA, S, np.float32(h), np.float32(h * h), stream()) == 0
+    assert bits_equal(host(K2), K)
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_normalize_energy_forces(lib, g, case):
+    from gpu_util import dev, host, ptr, stream
+    NN, h, st = state(case, g)
+    S = NN + 1
+    nA = st["atoms5"].size // 5
+    h3 = np.float32(h ** 3)
+    Z = st["atoms5"].reshape(nA, 5)[:, 3].copy()
+    # normalise: FP64 norms, scale sqrt(Z/n) in f32 -> compare with the oracle in the same arithmetic
+    n64 = np.zeros(nA, np.float64)
+    orc.O().sp_norms_f64(st["U"], st["label"], S, nA, float(h3), n64)
+    Uref = st["U"].copy()
+    orc.O().sp_normalize(Uref, st["label"], n64.astype(np.float32), Z, S ** 3, nA)
+    dU, dL, dZ = dev(st["U"]), dev(st["label"]), dev(Z)
+    import torch
+    dn = torch.zeros(nA, dtype=torch.float64, device="cuda")
+    assert lib.rq_kernel_normalize_sp(ptr(dU), ptr(dL), ptr(dZ), nA, S, h3, ptr(dn), stream()) == 0
+    np.testing.assert_allclose(host(dn), n64, rtol=1e-12)
+    gu = host(dU)
+    assert np.max(np.abs(gu - Uref)) <= 2e-6 * np.max(np.abs(Uref))
+    # energies per domain (FP64)
+    out = np.zeros(3)
+    pd_ref = np.zeros(nA * 4)
+    orc.O().sp_energy_f64(st["U"], st["K"], st["P"], st["label"], S, h, float(h3), out, nA, pd_ref.ctypes.data)
+    dU0, dK, dP = dev(st["U"]), dev(st["K"]), dev(st["P"])
+    pd = torch.zeros(nA * 4, dtype=torch.float64, device="cuda")
+    assert lib.rq_kernel_energy_sp(ptr(dU0), ptr(dK), ptr(dP), ptr(dL), nA, S, np.float32(h), h3, ptr(pd),
+                                   stream()) == 0
+    np.testing.assert_allclose(host(pd), pd_ref, rtol=1e-10, atol=1e-14)
+    # Hellmann-Feynman forces
+    Fref = np.zeros(nA * 3)
+    orc.O().sp_forces(st["U"], st["atoms5"], nA, S, np.float32(h), np.float32(h * h), h3, Fref)
+    A = dev(st["atoms5"])
+    F = torch.zeros(nA * 3, dtype=torch.float64, device="cuda")
+    assert lib.rq_kernel_forces_hf_sp(ptr(dU0), ptr(A), nA, S, np.float32(h), np.float32(h * h), h3, ptr(F),
+                                      stream()) == 0
+    np.testing.assert_allclose(host(F), Fref, rtol=1e-4, atol=1e-6 * np.abs(Fref).max())
+    if case[1] is None:
+        np.testing.assert_allclose(host(F), g["out_computeForceAll"], rtol=1e-4, atol=1e-6)
