@@ -139,7 +139,8 @@ def test_normalize_energy_forces(lib, g, case):
     # energies per domain (FP64)
     out = np.zeros(3)
     pd_ref = np.zeros(nA * 4)
-    orc.O().sp_energy_f64(st["U"], st["K"], st["P"], st["label"], S, h, float(h3), out, nA, pd_ref.ctypes.data)
+    hf = float(np.float32(h))  # the kernel receives h as f32
+    orc.O().sp_energy_f64(st["U"], st["K"], st["P"], st["label"], S, hf, float(h3), out, nA, pd_ref.ctypes.data)
     dU0, dK, dP = dev(st["U"]), dev(st["K"]), dev(st["P"])
     pd = torch.zeros(nA * 4, dtype=torch.float64, device="cuda")
     assert lib.rq_kernel_energy_sp(ptr(dU0), ptr(dK), ptr(dP), ptr(dL), nA, S, np.float32(h), h3, ptr(pd),
