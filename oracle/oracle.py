@@ -100,8 +100,9 @@ class _Oracle:
             "orc_mj_normalize": [_f32p, _f32p, _u32p, C.c_void_p, _i],
             "orc_mj_energy": [_f32p, _f32p, _f32p, _u32p, C.c_void_p, _i, _f, _f, _f, _f64p],
             "orc_mj_force_gradP": [_f32p, C.c_void_p, _i, _i, _f, _i, _f64p],
-            "orc_mj_force_hf": [_f32p, C.c_void_p, _i, _i, _f, _f64p],
-            "orc_mj_init": [_f32p, _f32p, _u32p, C.c_void_p, _i, _i, _f, _f],
+            "orc_mj_force_hf": [_f32p, C.c_void_p, _i, _i, _f, _f, _f64p],
+            "orc_mj_init": [_f32p, _f32p, _u32p, C.c_void_p, _i, _i, _f, _f, _f],
+            "orc_mj_init_persist": [_f32p, _f32p, _u32p, C.c_void_p, _i, _i, _f, _f, _f],
             "orc_nm_potential": [_f64p, _f64p, _f64p, _i, _i, _d, _d],
             "orc_nm_update": [_f64p, _f64p, _f64p, _f64p, _i32p, _i, _d, _d],
             "orc_nm_vcycle": [_f64p, _f64p, _i, _d, _i, _i, _i, _i],
@@ -326,3 +327,118 @@ def e_kk_solverpy(atom_pos, Z_eff, h) -> float:
             d = (np.asarray(atom_pos[a], np.float64) - np.asarray(atom_pos[b], np.float64)) * h
             e += float(Z_eff[a]) * float(Z_eff[b]) / math.sqrt(float(d @ d) + h * h)
     return e
+
+
+class MoleculeJsDriver:
+    """Restatement of molecule.js's doSteps schedule (molecule.js:2822-3104) over the C oracle,
+    total-Poisson path without SIC (the reference's choice for NELEC > 30), W_CUTOFF = 0, no
+    locked groups or shell splits.  One ``step()`` is one iteration of doSteps' s-loop; every
+    ``steps_per_frame`` steps the frame tail runs (Pother <- P, then the level-set passes).
+
+    Parameters are the f32 values of the uniform buffer (molecule.js:1829-1836): h, h2 = f32(h*h
+    in double), h3, 1/h^2, dt = f32(dv*h^2), half_d = f32(dv/2).
+    """
+
+    def __init__(self, NN, screen, atoms, dv=None, steps_per_frame=None, norm_interval=20, vcycle_interval=50,
+                 jacobi_per_step=2, boundary_speed=0.5, curv_reg=0.15):
+        self.NN = NN
+        self.S = NN + 1
+        self.S3 = self.S ** 3
+        h = screen / NN
+        self.hd = h
+        self.h = np.float32(h)
+        self.h2 = np.float32(h * h)
+        self.h3 = np.float32(h * h * h)
+        self.inv_h2 = np.float32(1.0 / (h * h))
+        self.Rsing = np.float32(2 * h)
+        self.rows = [dict(a) for a in atoms]
+        for r in self.rows:
+            r.setdefault("Z_nuc", r["Z"])
+        self.atoms = mj_atoms(self.rows)
+        self.nA = len(self.rows)
+        nelec = sum(1 for a in self.rows if a["Z"] > 0 or a.get("Z_nuc", 0) > 0)
+        self.nelec = nelec
+        self.n_electrons = sum(a["Z"] for a in self.rows)
+        self.has_bare = any(a["Z"] == 0 and a.get("Z_nuc", 0) > 0 for a in self.rows)
+        self.dv = dv if dv else (0.01 if nelec > 500 else 0.03 if nelec > 100 else 0.12)
+        self.dt = np.float32(self.dv * h * h)
+        self.half_d = np.float32(0.5 * self.dv)
+        self.spf = steps_per_frame or (50 if nelec <= 30 else 5 if nelec <= 100 else 2)
+        self.norm_interval, self.vcycle_interval, self.jps = norm_interval, vcycle_interval, jacobi_per_step
+        self.dt_w, self.curv = np.float32(boundary_speed), np.float32(curv_reg)
+        S3 = self.S3
+        self.K = np.zeros(S3, np.float32)
+        self.U = np.zeros(S3, np.float32)
+        self.Unext = np.zeros(S3, np.float32)
+        self.label = np.zeros(S3, np.uint32)
+        self.label2 = np.zeros(S3, np.uint32)
+        self.bestU = np.zeros(S3, np.float32)
+        self.P = np.zeros(S3, np.float32)
+        self.P2 = np.zeros(S3, np.float32)
+        self.Pother = np.zeros(S3, np.float32)
+        self.W = np.ones(S3, np.float32)
+        self.rho = np.zeros(S3, np.float32)
+        self.steps_done = 0
+        SC = NN // 2 + 1
+        self.SC = SC
+
+    def initialize(self):
+        O().mj_init(self.K, self.U, self.label, C.addressof(self.atoms), self.nA, self.S, self.h, self.h2, self.Rsing)
+        self.bestU[:] = self.U
+        self.Unext[:] = self.U
+        self.label2[:] = self.label
+
+    def set_positions(self, rows):
+        self.rows = [dict(a) for a in rows]
+        for r in self.rows:
+            r.setdefault("Z_nuc", r["Z"])
+        self.atoms = mj_atoms(self.rows)
+        O().mj_init_persist(self.K, self.bestU, self.label, C.addressof(self.atoms), self.nA, self.S, self.h, self.h2,
+                            self.Rsing)
+        self.label2[:] = self.label
+
+    def vcycle(self):
+        S, SC = self.S, self.SC
+        R = np.zeros(self.S3, np.float32)
+        O().mj_rho(self.U, self.rho, S)
+        O().mj_residual(self.P, R, self.rho, S, self.inv_h2, np.float32(2 * np.pi))
+        fc = np.zeros(SC ** 3, np.float32)
+        O().mj_restrict(R, fc, S, SC)
+        E = [np.zeros(SC ** 3, np.float32), np.zeros(SC ** 3, np.float32)]
+        for cs in range(10):
+            O().mj_coarse_smooth(E[cs % 2], E[(cs + 1) % 2], fc, SC, self.h2)
+        O().mj_prolong(E[0], self.P, S, SC)
+
+    def step(self):
+        self.steps_done += 1
+        sf = (self.steps_done - 1) % self.spf
+        poisson = self.n_electrons > 1
+        if poisson:
+            O().mj_rho(self.U, self.rho, self.S)
+            for _ in range(self.jps):
+                O().mj_jacobi(self.P, self.P2, self.rho, self.S, self.h2, np.float32(2 * np.pi))
+                self.P, self.P2 = self.P2, self.P
+            if sf > 0 and sf % self.vcycle_interval == 0:
+                self.vcycle()
+        O().mj_update(self.U, self.Unext, self.K, self.label, self.Pother, C.addressof(self.atoms), self.nA,
+                      int(self.has_bare), self.S, self.h, self.half_d, self.dt)
+        self.U, self.Unext = self.Unext, self.U
+        if (sf + 1) % self.norm_interval == 0 or sf == self.spf - 1:
+            acc = np.zeros(self.nA, np.uint32)
+            nf = np.zeros(self.nA, np.float32)
+            O().mj_norms_fixed(self.U, self.label, self.S, self.h3, self.nA, acc, nf)
+            O().mj_normalize(self.U, nf, self.label, C.addressof(self.atoms), self.S)
+        if sf == self.spf - 1:
+            if poisson:
+                self.Pother[:] = self.P
+            else:
+                self.Pother[:] = 0
+            for _ in range(max(1, self.spf)):
+                O().mj_evolve_boundary(self.label, self.label2, self.U, self.W, self.S, self.dt_w, self.curv)
+                self.label, self.label2 = self.label2, self.label
+
+    def energy(self):
+        out = np.zeros(6)
+        O().mj_energy(self.U, self.Pother, self.K, self.label, C.addressof(self.atoms), self.S, self.h, self.h3,
+                      self.Rsing, out)
+        return out

@@ -677,9 +677,9 @@ void orc_mj_force_gradP(const float* Pt, const orc_mj_atom* atoms, int nElec, in
 }
 
 /* molecule.js:1271-1330 direct HF force with h^2 softening over the interior. */
-void orc_mj_force_hf(const float* U, const orc_mj_atom* atoms, int nElec, int S, float h, double* F) {
+void orc_mj_force_hf(const float* U, const orc_mj_atom* atoms, int nElec, int S, float h, float h2, double* F) {
   const int NN = S - 1;
-  const float h2 = h * h, h3 = h * h * h;
+  const float h3 = h * h * h;
   for (int a = 0; a < nElec; ++a) {
     float ZA = (atoms[a].Z <= 0.f) ? atoms[a].Z_nuc : atoms[a].Z;
     F[3 * a] = F[3 * a + 1] = F[3 * a + 2] = 0;
@@ -707,8 +707,7 @@ void orc_mj_force_hf(const float* U, const orc_mj_atom* atoms, int nElec, int S,
  * K = sum Zn/r_eff, trial u = Ze^2/sqrt(pi) e^{-Ze r} (0 beyond initRcut or for bare nuclei),
  * label = argmax (strict >, first wins).  K/bestU/label start from 0/0/0 over ALL S^3 points. */
 void orc_mj_init(float* K, float* U, uint32_t* label, const orc_mj_atom* atoms, int nElec, int S, float h,
-                 float Rsing) {
-  const float h2 = h * h;
+                 float h2, float Rsing) {
 #pragma omp parallel for schedule(static)
   for (int i = 0; i < S; ++i)
     for (int j = 0; j < S; ++j)
@@ -733,6 +732,38 @@ void orc_mj_init(float* K, float* U, uint32_t* label, const orc_mj_atom* atoms, 
           if (uT > bU) { bU = uT; bestN = (uint32_t)n; }
         }
         K[id] = Kval; U[id] = bU; label[id] = bestN;
+      }
+}
+
+/* molecule.js:4563-4582 + :1377-1426: moveNuclei's K rebuild -- K from 0 with the init
+ * formula, the running maximum bestU and the current labels persist (an atom may take cells
+ * over); psi is not touched. */
+void orc_mj_init_persist(float* K, float* bestU, uint32_t* label, const orc_mj_atom* atoms, int nElec, int S, float h,
+                         float h2, float Rsing) {
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < S; ++i)
+    for (int j = 0; j < S; ++j)
+      for (int kk = 0; kk < S; ++kk) {
+        int64_t id = IDX(i, j, kk, S);
+        float xi = (float)i * h, yj = (float)j * h, zk = (float)kk * h;
+        float Kval = 0.f, bU = bestU[id];
+        uint32_t bestN = label[id];
+        for (int n = 0; n < nElec; ++n) {
+          float Za = atoms[n].Z;
+          float Zn = (atoms[n].Z_nuc > 0.f) ? atoms[n].Z_nuc : Za;
+          if (Za <= 0.f && Zn <= 0.f) continue;
+          float dx = xi - (float)atoms[n].posI * h;
+          float dy = yj - (float)atoms[n].posJ * h;
+          float dz = zk - (float)atoms[n].posK * h;
+          float r2 = dx * dx + dy * dy + dz * dz;
+          float r = (atoms[n].rc > 0.f) ? fmaxf(sqrtf(r2 + 0.04f * h2), atoms[n].rc) : fmaxf(sqrtf(r2), Rsing);
+          Kval += Zn / r;
+          float Ze = atoms[n].initZeff;
+          float rReal = sqrtf(r2);
+          float uT = (rReal > atoms[n].initRcut || Za <= 0.f) ? 0.f : Ze * Ze * 0.5641895835f * expf(-Ze * r);
+          if (uT > bU) { bU = uT; bestN = (uint32_t)n; }
+        }
+        K[id] = Kval; bestU[id] = bU; label[id] = bestN;
       }
 }
 

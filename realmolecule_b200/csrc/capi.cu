@@ -120,7 +120,7 @@ static void free_ctx(rq_ctx* c) {
   for (auto& gx : c->graph)
     if (gx) cudaGraphExecDestroy(gx);
   void* ptrs[] = {c->U[0], c->U[1], c->P[0], c->P[1], c->K, c->W, c->bestU, c->rho, c->Pother, c->lab[0], c->lab[1],
-                  c->Ec[0], c->Ec[1], c->fc, c->atoms5, c->atoms_mj, c->atoms_nm, c->Zdom, c->Zdom64, c->dnorm,
+                  c->Ec[0], c->Ec[1], c->fc, c->atoms5, c->scratch_atoms5, c->atoms_mj, c->atoms_nm, c->Zdom, c->Zdom64, c->dnorm,
                   c->dpd, c->dF, c->dsum, c->unorm, c->scale, c->err};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -167,6 +167,7 @@ static int alloc_all(rq_ctx* c) {
     DALLOC(c->fc, SC3 * sizeof(float));
   }
   DALLOC(c->atoms5, sizeof(float) * 5 * n);
+  DALLOC(c->scratch_atoms5, sizeof(float) * 5 * n);
   DALLOC(c->atoms_mj, sizeof(MjAtom) * n);
   DALLOC(c->atoms_nm, sizeof(double) * 4 * n);
   DALLOC(c->Zdom, sizeof(float) * n);
@@ -203,6 +204,7 @@ extern "C" int rq_create(const rq_config* cfg, const rq_atom* atoms, int32_t n_a
   c->h3 = c->h2 * c->h;
   c->n_atoms = n_atoms;
   c->atoms.assign(atoms, atoms + n_atoms);
+  c->atoms0 = c->atoms;
   c->fp64 = cfg->precision == RQ_PREC_FP64;
   cudaGetDevice(&c->device);
   fill_defaults(c);
@@ -429,15 +431,20 @@ extern "C" int rq_upload_state(rq_ctx* c, const float* psi, const int32_t* label
   if (!c) return RQ_EINVAL;
   if (c->fp64 && (psi || P)) return rq_fail(c, RQ_EINVAL, "FP64 context: use rq_upload_state_f64 for psi/P");
   const size_t n = (size_t)c->g.S3;
+  const bool mj = c->cfg.flavor == RQ_FLAVOR_MOLECULE_JS;
   if (label) {
     int rc = check_labels(c, label);
     if (rc != RQ_OK) return rc;
     CK(cudaMemcpyAsync(c->lab[c->cl], label, n * sizeof(int), cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(c->lab[1 - c->cl], c->lab[c->cl], n * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+    if (mj && (rc = mj_refresh_flags(c)) != RQ_OK) return rc;  // r_c-exclusion bits of the new labels
   }
   if (psi) {
     CK(cudaMemcpyAsync(c->U[c->cu], psi, n * sizeof(float), cudaMemcpyHostToDevice, c->st));
-    CK(launch_zero_faces((float*)c->U[c->cu], c->g, c->st));  // Dirichlet planes are 0
+    if (mj)  // molecule.js keeps the boundary values of psi (never rewritten): both buffers hold them
+      CK(cudaMemcpyAsync(c->U[1 - c->cu], c->U[c->cu], n * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
+    else
+      CK(launch_zero_faces((float*)c->U[c->cu], c->g, c->st));  // Dirichlet planes are 0
   }
   if (W) CK(cudaMemcpyAsync(c->W, W, n * sizeof(float), cudaMemcpyHostToDevice, c->st));
   if (P) {
@@ -458,6 +465,8 @@ extern "C" int rq_download_state(rq_ctx* c, float* psi, int32_t* label, float* W
   if (W) CK(cudaMemcpyAsync(W, c->W, n * sizeof(float), cudaMemcpyDeviceToHost, c->st));
   if (P) CK(cudaMemcpyAsync(P, c->P[c->cp], n * sizeof(float), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
+  if (label && c->cfg.flavor == RQ_FLAVOR_MOLECULE_JS)
+    for (size_t q = 0; q < n; ++q) label[q] &= kMjLabelMask;  // strip the exclusion bit
   return RQ_OK;
 }
 

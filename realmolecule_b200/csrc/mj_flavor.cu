@@ -1,8 +1,273 @@
-// mj_flavor.cu -- molecule.js flavour (placeholder until its kernels land).
+// mj_flavor.cu -- the molecule.js flavour's schedule, energies and forces (host side of librq).
+//
+// One rq_step of this flavour is one iteration of the s-loop of doSteps (molecule.js:2829-3006);
+// every steps_per_frame steps the frame tail runs (Pother <- P, molecule.js:3014-3015, then
+// W_STEPS_PER_FRAME level-set passes, :3093-3104).  The self-interaction correction and the
+// direct per-electron Poisson of small systems (:2833-2858, :3016-3076) are not built: this
+// flavour always takes the total-Poisson path the reference uses for NELEC > 30.
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <tuple>
+
 #include "rq_flavors.h"
-int mj_initialize(rq_ctx* c) { return rq_fail(c, RQ_ENOTSUP, "molecule.js flavour not built yet"); }
-int mj_step_one(rq_ctx* c, int) { return rq_fail(c, RQ_ENOTSUP, "molecule.js flavour not built yet"); }
-int mj_energy(rq_ctx* c, double*, double*) { return rq_fail(c, RQ_ENOTSUP, "molecule.js flavour not built yet"); }
-int mj_forces(rq_ctx* c, int, double*) { return rq_fail(c, RQ_ENOTSUP, "molecule.js flavour not built yet"); }
-int mj_set_atoms(rq_ctx* c) { return rq_fail(c, RQ_ENOTSUP, "molecule.js flavour not built yet"); }
-void mj_nuclear_terms(rq_ctx*, double* E, double*) { *E = 0; }
+#include "rq_kernels.h"
+
+using namespace rq;
+
+#define CK(call)                                 \
+  do {                                           \
+    int _rc = rq_cuda(c, (call), #call);         \
+    if (_rc != RQ_OK) return _rc;                \
+  } while (0)
+
+namespace {
+
+struct MjParams {  // the f32 uniform P of molecule.js:175-181 (fillParamsBuf :1829-1836)
+  float h, h2, h3, inv_h, inv_h2, dt, half_d, two_pi, dt_w, curvReg, Rsing;
+  bool hasBare;
+  int nelec;
+  double n_electrons;
+};
+
+MjParams mj_params(const rq_ctx* c) {
+  MjParams p;
+  const double h = c->h;
+  p.h = (float)h;
+  p.h2 = (float)(h * h);
+  p.h3 = (float)(h * h * h);
+  p.inv_h = (float)(1.0 / h);
+  p.inv_h2 = (float)(1.0 / (h * h));
+  p.dt = (float)(c->dv * h * h);
+  p.half_d = (float)(0.5 * c->dv);
+  p.two_pi = (float)(2.0 * M_PI);
+  p.dt_w = (float)c->cfg.boundary_speed;
+  p.curvReg = (float)c->cfg.curv_reg;
+  p.Rsing = (float)(2.0 * h);  // R_SING = 2 h (molecule.js:82)
+  p.hasBare = false;
+  p.nelec = 0;
+  p.n_electrons = 0;
+  for (auto& a : c->atoms) {
+    if (a.Z == 0 && a.Z_nuc > 0) p.hasBare = true;  // molecule.js:85-91
+    if (a.Z > 0 || a.Z_nuc > 0) p.nelec++;
+    p.n_electrons += a.Z;
+  }
+  return p;
+}
+
+const MjAtom* atoms_dev(rq_ctx* c) { return (const MjAtom*)c->atoms_mj; }
+
+double interior(const Geo& g) {
+  const double n = g.NN - 1;
+  return n * n * n;
+}
+
+}  // namespace
+
+int mj_initialize(rq_ctx* c) {
+  const MjParams p = mj_params(c);
+  const size_t n = (size_t)c->g.S3;
+  c->cu = c->cp = c->cl = 0;
+  // molecule.js uploadInitialData (:1905-2101): K, trial psi and argmax labels over all S^3
+  // points; both psi buffers, both label buffers, P = Pother = 0, W = 1
+  LAUNCH(RQ_KC_OTHER, 12.0 * c->g.S3,
+         launch_mj_init((float*)c->K, (float*)c->U[0], c->bestU, c->lab[0], atoms_dev(c), c->n_atoms, c->g, p.h, p.h2,
+                        p.Rsing, p.hasBare, false, c->st));
+  CK(cudaMemcpyAsync(c->U[1], c->U[0], n * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaMemcpyAsync(c->lab[1], c->lab[0], n * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+  for (int b = 0; b < 2; ++b) CK(cudaMemsetAsync(c->P[b], 0, n * sizeof(float), c->st));
+  CK(cudaMemsetAsync(c->Pother, 0, n * sizeof(float), c->st));
+  LAUNCH(RQ_KC_OTHER, 4.0 * c->g.S3, launch_fill(c->W, 1.0f, c->g.S3, c->st));
+  return RQ_OK;
+}
+
+int mj_set_atoms(rq_ctx* c) {
+  // moveNuclei's rebuild (molecule.js:4563-4582): K from 0 with the init formula, persistent
+  // bestU / labels (a moved atom may take cells over); then the exclusion bits of every label
+  const MjParams p = mj_params(c);
+  LAUNCH(RQ_KC_OTHER, 16.0 * c->g.S3,
+         launch_mj_init((float*)c->K, nullptr, c->bestU, c->lab[c->cl], atoms_dev(c), c->n_atoms, c->g, p.h, p.h2,
+                        p.Rsing, p.hasBare, true, c->st));
+  CK(cudaMemcpyAsync(c->lab[1 - c->cl], c->lab[c->cl], (size_t)c->g.S3 * sizeof(int), cudaMemcpyDeviceToDevice,
+                     c->st));
+  return RQ_OK;
+}
+
+int mj_refresh_flags(rq_ctx* c) {
+  const MjParams p = mj_params(c);
+  for (int b = 0; b < 2; ++b)
+    LAUNCH(RQ_KC_OTHER, 8.0 * c->g.S3,
+           launch_mj_flags(c->lab[b], atoms_dev(c), c->n_atoms, c->g, p.h, p.hasBare, c->st));
+  return RQ_OK;
+}
+
+int mj_step_one(rq_ctx* c, int s) {
+  const MjParams p = mj_params(c);
+  const rq_config& f = c->cfg;
+  const int spf = f.steps_per_frame;
+  const int sf = (s - 1) % spf;  // position inside the frame (doSteps' s)
+  const bool poisson = p.n_electrons > 1.0;
+  const double ip = interior(c->g);
+  if (poisson) {
+    for (int js = 0; js < f.jacobi_per_step; ++js) {
+      LAUNCH(RQ_KC_POISSON, 12 * ip,
+             launch_mj_jacobi((float*)c->P[c->cp], (float*)c->P[1 - c->cp], (float*)c->U[c->cu], c->g, p.h2, p.two_pi,
+                              c->st));
+      c->cp ^= 1;
+    }
+    if (sf > 0 && sf % f.vcycle_interval == 0)  // molecule.js:2879
+      LAUNCH(RQ_KC_MG, 40 * ip,
+             launch_mj_vcycle((float*)c->P[c->cp], (float*)c->U[c->cu], c->rho, c->bestU, c->Ec[0], c->Ec[1], c->fc,
+                              c->g, c->gc, p.h2, p.inv_h2, p.two_pi, c->st));
+  }
+  const bool norm = ((sf + 1) % f.norm_interval == 0) || sf == spf - 1;  // molecule.js:2972
+  if (norm) CK(cudaMemsetAsync(c->unorm, 0, sizeof(unsigned) * c->n_atoms, c->st));
+  LAUNCH(RQ_KC_UPDATE, 20 * ip,
+         launch_mj_update((float*)c->U[c->cu], (float*)c->U[1 - c->cu], (float*)c->K, c->lab[c->cl], c->Pother, c->g,
+                          p.half_d, p.dt, p.h3, c->n_atoms, norm ? c->unorm : nullptr, c->st));
+  c->cu ^= 1;
+  if (norm) {
+    LAUNCH(RQ_KC_NORMALIZE, 8.0 * c->n_atoms,
+           launch_mj_norm_scale(c->unorm, atoms_dev(c), c->n_atoms, c->scale, c->st));
+    LAUNCH(RQ_KC_NORMALIZE, 12 * ip, launch_mj_apply_scale((float*)c->U[c->cu], c->lab[c->cl], c->scale, c->g, c->st));
+  }
+  if (sf == spf - 1) {
+    // frame tail: Pother <- P_buf[0] (no SIC), then the level-set passes on the same psi
+    if (poisson)
+      CK(cudaMemcpyAsync(c->Pother, c->P[c->cp], (size_t)c->g.S3 * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
+    else
+      CK(cudaMemsetAsync(c->Pother, 0, (size_t)c->g.S3 * sizeof(float), c->st));
+    const int wsteps = spf > 1 ? spf : 1;  // W_STEPS_PER_FRAME (:107)
+    for (int q = 0; q < wsteps; ++q) {
+      LAUNCH(RQ_KC_LABELS, 20 * ip,
+             launch_mj_evolve(c->lab[c->cl], c->lab[1 - c->cl], (float*)c->U[c->cu], c->W, atoms_dev(c), c->n_atoms,
+                              c->g, p.dt_w, p.curvReg, p.h, p.hasBare, c->st));
+      c->cl ^= 1;
+    }
+  }
+  return RQ_OK;
+}
+
+// Unique nuclei of molecule.js:50-67: entries with Z>0 or Z_nuc>0 grouped by their initial
+// grid position key; charge = sum of (Z_nuc || Z); the first entry's current position.
+static void mj_unique_nuclei(const rq_ctx* c, std::vector<std::vector<int>>& groups, std::vector<double>& zeff) {
+  std::map<std::tuple<double, double, double>, int> key;
+  for (int e = 0; e < c->n_atoms; ++e) {
+    const rq_atom& a = c->atoms0[e];
+    if (a.Z == 0 && a.Z_nuc == 0) continue;
+    // the reference keys on the page's atom positions ("i,j,k" strings): exact equality of the
+    // creation-time positions
+    auto k = std::make_tuple(a.i, a.j, a.k);
+    auto it = key.find(k);
+    const double z = a.Z_nuc != 0 ? a.Z_nuc : a.Z;
+    if (it == key.end()) {
+      key[k] = (int)groups.size();
+      groups.push_back({e});
+      zeff.push_back(z);
+    } else {
+      groups[it->second].push_back(e);
+      zeff[it->second] += z;
+    }
+  }
+}
+
+void mj_nuclear_terms(rq_ctx* c, double* E, double* F) {
+  // molecule.js:3170-3185 (E_KK, softening 0.04 h^2) and :3218-3242 (forces, softening h^2)
+  std::vector<std::vector<int>> groups;
+  std::vector<double> zeff;
+  mj_unique_nuclei(c, groups, zeff);
+  const double h = c->h;
+  double e = 0;
+  const size_t G = groups.size();
+  for (size_t a = 0; a < G; ++a) {
+    const rq_atom& A = c->atoms[groups[a][0]];
+    double fx = 0, fy = 0, fz = 0;
+    for (size_t b = 0; b < G; ++b) {
+      if (b == a) continue;
+      const rq_atom& B = c->atoms[groups[b][0]];
+      const double dx = (A.i - B.i) * h, dy = (A.j - B.j) * h, dz = (A.k - B.k) * h;
+      const double d2 = dx * dx + dy * dy + dz * dz;
+      if (b > a) e += zeff[a] * zeff[b] / std::sqrt(d2 + 0.04 * h * h);
+      const double r2 = d2 + h * h, r = std::sqrt(r2), inv_r3 = 1.0 / (r * r2);
+      fx += zeff[a] * zeff[b] * dx * inv_r3;
+      fy += zeff[a] * zeff[b] * dy * inv_r3;
+      fz += zeff[a] * zeff[b] * dz * inv_r3;
+    }
+    for (int q : groups[a]) {
+      F[q * 3] = fx; F[q * 3 + 1] = fy; F[q * 3 + 2] = fz;
+    }
+  }
+  *E = e;
+}
+
+int mj_energy(rq_ctx* c, double* out, double* per_domain) {
+  const MjParams p = mj_params(c);
+  const int n = c->n_atoms;
+  CK(cudaMemsetAsync(c->dpd, 0, sizeof(double) * 4 * n, c->st));
+  CK(cudaMemsetAsync(c->dsum, 0, sizeof(double) * 8, c->st));
+  LAUNCH(RQ_KC_ENERGY, 16 * interior(c->g),
+         launch_mj_energy((float*)c->U[c->cu], c->Pother, (float*)c->K, c->lab[c->cl], atoms_dev(c), c->g, p.h, p.h3,
+                          p.Rsing, n, c->dpd, c->dsum, c->st));
+  std::vector<double> pd((size_t)4 * n);
+  double dip[3];
+  CK(cudaMemcpyAsync(pd.data(), c->dpd, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(dip, c->dsum, sizeof(double) * 3, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  double T = 0, EK = 0, EE = 0;
+  for (int q = 0; q < n; ++q) {
+    T += pd[q * 4 + 1]; EK += pd[q * 4 + 2]; EE += pd[q * 4 + 3];
+    if (per_domain) {
+      double* d = per_domain + (size_t)q * RQ_DOMAIN_LEN;
+      d[RQ_D_NORM] = pd[q * 4]; d[RQ_D_T] = pd[q * 4 + 1]; d[RQ_D_EK] = pd[q * 4 + 2]; d[RQ_D_EE] = pd[q * 4 + 3];
+      const double nr = pd[q * 4] != 0 ? pd[q * 4] : 1.0;
+      d[RQ_D_EIG] = (pd[q * 4 + 1] + 2 * pd[q * 4 + 3] + pd[q * 4 + 2]) / nr;
+    }
+  }
+  // per-H exclusion-sphere correction (molecule.js:3130-3139)
+  int nH = 0;
+  for (auto& a : c->atoms)
+    if (a.Z == 1 && a.rc == 0) nH++;
+  double raw0 = 0.503, raw1 = -1.028;  // H_RAW[200], the default
+  if (c->g.NN == 100 || c->g.NN == 300) { raw0 = 0.5; raw1 = -1.0; }
+  T += nH * (0.5 - raw0);
+  EK += nH * (-1.0 - raw1);
+  out[RQ_E_T] = T; out[RQ_E_EK] = EK; out[RQ_E_EE] = EE;
+  // dipole (molecule.js:3141-3161): sum Z_a R_a h - electronic sums
+  double dx = 0, dy = 0, dz = 0;
+  for (auto& a : c->atoms) {
+    if (a.Z == 0) continue;
+    dx += a.Z * a.i * c->h; dy += a.Z * a.j * c->h; dz += a.Z * a.k * c->h;
+  }
+  out[RQ_E_DIPX] = dx - dip[0]; out[RQ_E_DIPY] = dy - dip[1]; out[RQ_E_DIPZ] = dz - dip[2];
+  return RQ_OK;
+}
+
+int mj_forces(rq_ctx* c, int method, double* F) {
+  const MjParams p = mj_params(c);
+  const int n = c->n_atoms;
+  if (method == RQ_FORCE_GRADP) {
+    const int R = std::max(5, (int)std::lround(3.0 / c->h));  // FORCE_RADIUS (molecule.js:1198)
+    LAUNCH(RQ_KC_FORCES, 4.0 * n * (2 * R + 1) * (2 * R + 1) * (2 * R + 1),
+           launch_mj_gradp((float*)c->P[c->cp], atoms_dev(c), n, c->g, p.inv_h, R, c->dF, c->st));
+  } else if (method == RQ_FORCE_HF || method == RQ_FORCE_ADJOINT) {
+    // molecule.js:1271-1330: Z_A = Z (or Z_nuc for bare nuclei), integer positions, h^2 softening
+    std::vector<float> a5((size_t)n * 5);
+    for (int q = 0; q < n; ++q) {
+      const rq_atom& a = c->atoms[q];
+      a5[q * 5 + 0] = (float)(uint32_t)(a.i < 0 ? 0 : a.i);
+      a5[q * 5 + 1] = (float)(uint32_t)(a.j < 0 ? 0 : a.j);
+      a5[q * 5 + 2] = (float)(uint32_t)(a.k < 0 ? 0 : a.k);
+      a5[q * 5 + 3] = (float)(a.Z <= 0 ? a.Z_nuc : a.Z);
+      a5[q * 5 + 4] = 0.f;
+    }
+    CK(cudaMemcpyAsync(c->scratch_atoms5, a5.data(), sizeof(float) * a5.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemsetAsync(c->dF, 0, sizeof(double) * 3 * n, c->st));
+    LAUNCH(RQ_KC_FORCES, 4 * interior(c->g),
+           launch_forces_hf_sp((float*)c->U[c->cu], c->scratch_atoms5, n, c->g, p.h, p.h2, p.h3, c->dF, c->st));
+  } else {
+    return RQ_ENOTSUP;
+  }
+  CK(cudaMemcpyAsync(F, c->dF, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return RQ_OK;
+}

@@ -1,0 +1,608 @@
+// mj_kernels.cu -- the molecule.js flavour of the solver step on sm_100a.
+//
+// Each kernel restates one WGSL compute shader of molecule.js with the same f32 operations
+// in the same order (explicitly rounded), so outputs are bit-identical to the strict-f32
+// oracle.  B200-specific changes:
+//  * the per-neighbour "inside its label's r_c sphere" tests of updateU (molecule.js:246-259,
+//    seven sqrt per cell) are precomputed once per label change into bit 30 of the label word
+//    (kMjExcl), so the update reads one int per neighbour like the solver.py flavour;
+//  * rhoTotal = psi^2 is computed inside the Jacobi sweep (no separate pass);
+//  * the u32 fixed-point norms (molecule.js:912-946) are aggregated per block in shared memory
+//    before the global atomics -- integer adds, so the result is bit-exact in any order.
+#include "rq_flavors.h"
+#include "rq_kernels.h"
+
+namespace rq {
+
+constexpr int kMjExcl = 0x40000000;  // bit 30 of a stored label: cell inside its label's r_c sphere
+constexpr int kMjMask = 0x3FFFFFFF;
+
+__device__ __forceinline__ float mj_dist(int ci, int cj, int ck, const MjAtom& a, float h) {
+  const float dx = F_MUL(F_SUB((float)ci, (float)a.posI), h);
+  const float dy = F_MUL(F_SUB((float)cj, (float)a.posJ), h);
+  const float dz = F_MUL(F_SUB((float)ck, (float)a.posK), h);
+  return F_SQRT(F_ADD(F_ADD(F_MUL(dx, dx), F_MUL(dy, dy)), F_MUL(dz, dz)));
+}
+
+// molecule.js:246-259 isInsideRc(ci, cj, ck, lbl)
+__device__ __forceinline__ bool mj_inside_rc(int ci, int cj, int ck, int lbl, const MjAtom* __restrict__ atoms,
+                                             int nAt, bool hasBare, float h) {
+  const MjAtom a = atoms[lbl];
+  if (a.rc > 0.f && mj_dist(ci, cj, ck, a, h) < a.rc) return true;
+  if (hasBare)
+    for (int n = 0; n < nAt; ++n) {
+      const MjAtom b = atoms[n];
+      if (b.Z <= 0.f && b.Z_nuc > 0.f && b.rc > 0.f && mj_dist(ci, cj, ck, b, h) < b.rc) return true;
+    }
+  return false;
+}
+
+__device__ __forceinline__ int mj_pack(int ci, int cj, int ck, int lbl, const MjAtom* atoms, int nAt, bool hasBare,
+                                       float h) {
+  return lbl | (mj_inside_rc(ci, cj, ck, lbl, atoms, nAt, hasBare, h) ? kMjExcl : 0);
+}
+
+// ---------------------------------------------------------------------------------------
+// init: molecule.js:1377-1426 gpuInitAccum over all atoms in one pass (identical to its
+// 50-atom batches: the running K / bestU / label carry over in the same order) + :1437-1449.
+// ---------------------------------------------------------------------------------------
+// With PERSIST (moveNuclei's K rebuild, molecule.js:4563-4582) K restarts from 0 but the
+// running maximum bestU and the current label persist, so a moved atom can take cells over;
+// psi is not touched.  Without PERSIST (initial upload) everything starts from 0 and psi = bestU.
+template <bool PERSIST>
+__global__ void __launch_bounds__(256) k_mj_init(float* __restrict__ K, float* __restrict__ U, float* __restrict__ bestU,
+                                                 int* __restrict__ label, const MjAtom* __restrict__ atoms, int nAt,
+                                                 Geo g, float h, float h2, float Rsing, bool hasBare) {
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= g.S3) return;
+  const int S = g.S;
+  const int i = (int)(id / g.S2), j = (int)((id / S) % S), kk = (int)(id % S);
+  const float xi = F_MUL((float)i, h), yj = F_MUL((float)j, h), zk = F_MUL((float)kk, h);
+  float Kval = 0.f, bU = PERSIST ? bestU[id] : 0.f;
+  int bestN = PERSIST ? (label[id] & kMjMask) : 0;
+  for (int n = 0; n < nAt; ++n) {
+    const MjAtom a = atoms[n];
+    const float Za = a.Z;
+    const float Zn = (a.Z_nuc > 0.f) ? a.Z_nuc : Za;
+    if (Za <= 0.f && Zn <= 0.f) continue;
+    const float dx = F_SUB(xi, F_MUL((float)a.posI, h));
+    const float dy = F_SUB(yj, F_MUL((float)a.posJ, h));
+    const float dz = F_SUB(zk, F_MUL((float)a.posK, h));
+    const float r2 = F_ADD(F_ADD(F_MUL(dx, dx), F_MUL(dy, dy)), F_MUL(dz, dz));
+    const float r = (a.rc > 0.f) ? fmaxf(F_SQRT(F_ADD(r2, F_MUL(0.04f, h2))), a.rc) : fmaxf(F_SQRT(r2), Rsing);
+    Kval = F_ADD(Kval, F_DIV(Zn, r));
+    const float rReal = F_SQRT(r2);
+    const float Ze = a.initZeff;
+    const float uT = (rReal > a.initRcut || Za <= 0.f) ? 0.f
+                                                       : F_MUL(F_MUL(F_MUL(Ze, Ze), 0.5641895835f), expf(F_MUL(-Ze, r)));
+    if (uT > bU) { bU = uT; bestN = n; }
+  }
+  K[id] = Kval;
+  bestU[id] = bU;
+  if (!PERSIST) U[id] = bU;
+  label[id] = mj_pack(i, j, kk, bestN, atoms, nAt, hasBare, h);
+}
+
+// molecule.js:1337-1370 recomputeK (all S^3 points).
+__global__ void __launch_bounds__(256) k_mj_recompute_k(float* __restrict__ K, const MjAtom* __restrict__ atoms,
+                                                        int nAt, Geo g, float h, float Rsing) {
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= g.S3) return;
+  const int S = g.S;
+  const int i = (int)(id / g.S2), j = (int)((id / S) % S), kk = (int)(id % S);
+  float Kval = 0.f;
+  for (int n = 0; n < nAt; ++n) {
+    const MjAtom a = atoms[n];
+    const float Za = a.Z;
+    const float Zn = (a.Z_nuc > 0.f) ? a.Z_nuc : Za;
+    if (Za <= 0.f && Zn <= 0.f) continue;
+    const float di = F_MUL(F_SUB((float)i, (float)a.posI), h);
+    const float dj = F_MUL(F_SUB((float)j, (float)a.posJ), h);
+    const float dk = F_MUL(F_SUB((float)kk, (float)a.posK), h);
+    const float r = F_SQRT(F_ADD(F_ADD(F_MUL(di, di), F_MUL(dj, dj)), F_MUL(dk, dk)));
+    const float reff = (a.rc > 0.f) ? fmaxf(r, a.rc) : fmaxf(r, Rsing);
+    Kval = F_ADD(Kval, F_DIV(Zn, reff));
+  }
+  K[id] = Kval;
+}
+
+// Recompute the exclusion bit of every stored label (after nuclei move or a label upload).
+__global__ void __launch_bounds__(256) k_mj_flags(int* __restrict__ label, const MjAtom* __restrict__ atoms, int nAt,
+                                                  Geo g, float h, bool hasBare) {
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= g.S3) return;
+  const int S = g.S;
+  const int i = (int)(id / g.S2), j = (int)((id / S) % S), kk = (int)(id % S);
+  label[id] = mj_pack(i, j, kk, label[id] & kMjMask, atoms, nAt, hasBare, h);
+}
+
+// ---------------------------------------------------------------------------------------
+// updateU (molecule.js:263-343, W_CUTOFF = 0): 20 B per interior point.  With ACC the new
+// psi's u32 fixed-point norm per label (molecule.js:912-933) is accumulated as well.
+// ---------------------------------------------------------------------------------------
+template <bool ACC>
+__global__ void __launch_bounds__(256) k_mj_update(const float* __restrict__ U, float* __restrict__ Uo,
+                                                   const float* __restrict__ K, const int* __restrict__ label,
+                                                   const float* __restrict__ Pother, Geo g, float half_d, float dt,
+                                                   float h3, int nDom, unsigned* __restrict__ unorm) {
+  constexpr int NSLOT = 128;
+  __shared__ int keys[NSLOT];
+  __shared__ unsigned vals[NSLOT];
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  if (ACC) {
+    for (int s = tid; s < NSLOT; s += blockDim.x * blockDim.y) { keys[s] = -1; vals[s] = 0u; }
+    __syncthreads();
+  }
+  const int k = 1 + blockIdx.x * kThreadsK + threadIdx.x;
+  const int j = 1 + blockIdx.y * kThreadsJ + threadIdx.y;
+  const int i0 = 1 + blockIdx.z * kMarch;
+  int runL = -1;
+  unsigned runV = 0u;
+  auto flush_run = [&]() {
+    if (runL < 0) return;
+    unsigned slot = ((unsigned)runL * 2654435761u) & (NSLOT - 1);
+    for (int p = 0; p < NSLOT; ++p) {
+      const int old = atomicCAS(&keys[slot], -1, runL);
+      if (old == -1 || old == runL) { atomicAdd(&vals[slot], runV); return; }
+      slot = (slot + 1) & (NSLOT - 1);
+    }
+    atomicAdd(&unorm[runL], runV);
+  };
+  if (k < g.NN && j < g.NN && i0 < g.NN) {
+    const int iend = min(i0 + kMarch, g.NN);
+    const long long S = g.S, S2 = g.S2;
+    long long id = (long long)i0 * S2 + j * S + k;
+    float u_m = __ldg(U + id - S2), u_c = __ldg(U + id);
+    int l_m = __ldg(label + id - S2), l_c = __ldg(label + id);
+    for (int i = i0; i < iend; ++i, id += S2) {
+      const float u_p = __ldg(U + id + S2);
+      const int l_p = __ldg(label + id + S2);
+      float out;
+      if (l_c & kMjExcl) {
+        out = 0.0f;  // Dirichlet inside the own r_c sphere
+      } else {
+        const float ujp = __ldg(U + id + S), ujm = __ldg(U + id - S), ukp = __ldg(U + id + 1), ukm = __ldg(U + id - 1);
+        const int ljp = __ldg(label + id + S), ljm = __ldg(label + id - S), lkp = __ldg(label + id + 1),
+                  lkm = __ldg(label + id - 1);
+        // a neighbour is used iff same label and not inside its r_c sphere: packed words equal
+        const float a = (l_p == l_c) ? u_p : u_c;
+        const float b = (l_m == l_c) ? u_m : u_c;
+        const float c = (ljp == l_c) ? ujp : u_c;
+        const float d = (ljm == l_c) ? ujm : u_c;
+        const float e = (lkp == l_c) ? ukp : u_c;
+        const float f = (lkm == l_c) ? ukm : u_c;
+        const float lap = F_SUB(F_ADD(F_ADD(F_ADD(F_ADD(F_ADD(a, b), c), d), e), f), F_MUL(6.0f, u_c));
+        out = F_ADD(F_ADD(u_c, F_MUL(half_d, lap)),
+                    F_MUL(F_MUL(dt, F_SUB(__ldg(K + id), F_MUL(2.0f, __ldg(Pother + id)))), u_c));
+      }
+      Uo[id] = out;
+      if (ACC) {
+        const unsigned contrib = __float2uint_rz(F_MUL(F_MUL(F_MUL(out, out), h3), 16777216.0f));
+        const int L = l_c & kMjMask;
+        if (L != runL) { flush_run(); runL = L; runV = contrib; } else { runV += contrib; }
+      }
+      u_m = u_c; u_c = u_p; l_m = l_c; l_c = l_p;
+    }
+  }
+  if (ACC) {
+    flush_run();
+    __syncthreads();
+    for (int s = tid; s < NSLOT; s += blockDim.x * blockDim.y)
+      if (keys[s] >= 0) atomicAdd(&unorm[keys[s]], vals[s]);
+  }
+}
+
+// decodeNorms + the scale of normalize (molecule.js:938-946, :1098-1104): n = f32(acc)*2^-24,
+// scale = sqrt(Z/n) if n > 0 and Z > 0 else 1.
+__global__ void k_mj_norm_scale(const unsigned* __restrict__ unorm, const MjAtom* __restrict__ atoms, int nDom,
+                                float* __restrict__ scale) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= nDom) return;
+  const float n = F_MUL((float)unorm[l], 5.9604644775390625e-08f);
+  const float Z = atoms[l].Z;
+  scale[l] = (n > 0.f && Z > 0.f) ? F_SQRT(F_DIV(Z, n)) : 1.0f;
+}
+
+__global__ void __launch_bounds__(256) k_mj_apply_scale(float* __restrict__ U, const int* __restrict__ label,
+                                                        const float* __restrict__ scale, Geo g) {
+  const int k = 1 + blockIdx.x * kThreadsK + threadIdx.x;
+  const int j = 1 + blockIdx.y * kThreadsJ + threadIdx.y;
+  const int i0 = 1 + blockIdx.z * kMarch;
+  if (k >= g.NN || j >= g.NN || i0 >= g.NN) return;
+  const int iend = min(i0 + kMarch, g.NN);
+  for (int i = i0; i < iend; ++i) {
+    const long long id = (long long)i * g.S2 + (long long)j * g.S + k;
+    U[id] = F_MUL(U[id], scale[label[id] & kMjMask]);
+  }
+}
+
+// Weighted Jacobi with rho = psi^2 inline (molecule.js:723-749, :754-774).  12 B per point.
+__global__ void __launch_bounds__(256) k_mj_jacobi(const float* __restrict__ Pin, float* __restrict__ Pout,
+                                                   const float* __restrict__ U, Geo g, float h2, float two_pi) {
+  const int k = 1 + blockIdx.x * kThreadsK + threadIdx.x;
+  const int j = 1 + blockIdx.y * kThreadsJ + threadIdx.y;
+  const int i0 = 1 + blockIdx.z * kMarch;
+  if (k >= g.NN || j >= g.NN || i0 >= g.NN) return;
+  const int iend = min(i0 + kMarch, g.NN);
+  const long long S = g.S, S2 = g.S2;
+  long long id = (long long)i0 * S2 + j * S + k;
+  float p_m = __ldg(Pin + id - S2), p_c = __ldg(Pin + id);
+  const float c0 = F_MUL(h2, two_pi);
+  for (int i = i0; i < iend; ++i, id += S2) {
+    const float p_p = __ldg(Pin + id + S2);
+    const float u = __ldg(U + id);
+    const float sn = F_ADD(F_ADD(F_ADD(F_ADD(F_ADD(p_p, p_m), __ldg(Pin + id + S)), __ldg(Pin + id - S)),
+                                 __ldg(Pin + id + 1)),
+                           __ldg(Pin + id - 1));
+    const float rhs = F_MUL(c0, F_MUL(u, u));
+    Pout[id] = F_ADD(F_MUL(0.3333f, p_c), F_DIV(F_ADD(sn, rhs), 9.0f));
+    p_m = p_c; p_c = p_p;
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// the 2-level V-cycle of molecule.js:777-909 (one thread per point; it runs every
+// POISSON_INTERVAL steps at most)
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ bool interior_of(long long id, const Geo& g, int& i, int& j, int& k) {
+  i = (int)(id / g.S2); j = (int)((id / g.S) % g.S); k = (int)(id % g.S);
+  return i >= 1 && i < g.NN && j >= 1 && j < g.NN && k >= 1 && k < g.NN;
+}
+
+__global__ void k_mj_rho(const float* __restrict__ U, float* __restrict__ rho, Geo g) {
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, k;
+  if (id >= g.S3 || !interior_of(id, g, i, j, k)) return;
+  const float u = U[id];
+  rho[id] = F_MUL(u, u);
+}
+
+__global__ void k_mj_residual(const float* __restrict__ Pin, float* __restrict__ R, const float* __restrict__ rho, Geo g,
+                              float inv_h2, float two_pi) {
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, k;
+  if (id >= g.S3 || !interior_of(id, g, i, j, k)) return;
+  const long long S = g.S, S2 = g.S2;
+  const float Pc = Pin[id];
+  const float sum = F_ADD(F_ADD(F_ADD(F_ADD(F_ADD(Pin[id + S2], Pin[id - S2]), Pin[id + S]), Pin[id - S]), Pin[id + 1]),
+                          Pin[id - 1]);
+  const float lap = F_MUL(F_SUB(sum, F_MUL(6.0f, Pc)), inv_h2);
+  R[id] = F_SUB(F_MUL(-two_pi, rho[id]), lap);
+}
+
+__global__ void k_mj_restrict(const float* __restrict__ fine, float* __restrict__ coarse, Geo g, Geo gc) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int NCM = gc.NN - 1;
+  if (q >= (long long)NCM * NCM * NCM) return;
+  const int K2 = (int)(q % NCM) + 1, J = (int)((q / NCM) % NCM) + 1, I = (int)(q / ((long long)NCM * NCM)) + 1;
+  const int fi = 2 * I, fj = 2 * J, fk = 2 * K2;
+  const long long S = g.S, S2 = g.S2;
+#define FN(a, b, c) fine[(long long)(a) * S2 + (long long)(b) * S + (c)]
+  float val = F_MUL(8.0f, FN(fi, fj, fk));
+  float s4 = F_ADD(F_ADD(F_ADD(F_ADD(F_ADD(FN(fi + 1, fj, fk), FN(fi - 1, fj, fk)), FN(fi, fj + 1, fk)), FN(fi, fj - 1, fk)),
+                         FN(fi, fj, fk + 1)),
+                   FN(fi, fj, fk - 1));
+  val = F_ADD(val, F_MUL(4.0f, s4));
+  float s2 = FN(fi + 1, fj + 1, fk);
+  s2 = F_ADD(s2, FN(fi + 1, fj - 1, fk)); s2 = F_ADD(s2, FN(fi - 1, fj + 1, fk)); s2 = F_ADD(s2, FN(fi - 1, fj - 1, fk));
+  s2 = F_ADD(s2, FN(fi + 1, fj, fk + 1)); s2 = F_ADD(s2, FN(fi + 1, fj, fk - 1)); s2 = F_ADD(s2, FN(fi - 1, fj, fk + 1));
+  s2 = F_ADD(s2, FN(fi - 1, fj, fk - 1)); s2 = F_ADD(s2, FN(fi, fj + 1, fk + 1)); s2 = F_ADD(s2, FN(fi, fj + 1, fk - 1));
+  s2 = F_ADD(s2, FN(fi, fj - 1, fk + 1)); s2 = F_ADD(s2, FN(fi, fj - 1, fk - 1));
+  val = F_ADD(val, F_MUL(2.0f, s2));
+  float s1 = FN(fi + 1, fj + 1, fk + 1);
+  s1 = F_ADD(s1, FN(fi + 1, fj + 1, fk - 1)); s1 = F_ADD(s1, FN(fi + 1, fj - 1, fk + 1)); s1 = F_ADD(s1, FN(fi + 1, fj - 1, fk - 1));
+  s1 = F_ADD(s1, FN(fi - 1, fj + 1, fk + 1)); s1 = F_ADD(s1, FN(fi - 1, fj + 1, fk - 1)); s1 = F_ADD(s1, FN(fi - 1, fj - 1, fk + 1));
+  s1 = F_ADD(s1, FN(fi - 1, fj - 1, fk - 1));
+  val = F_ADD(val, s1);
+#undef FN
+  coarse[(long long)I * gc.S2 + (long long)J * gc.S + K2] = F_MUL(val, 0.015625f);
+}
+
+__global__ void k_mj_coarse_smooth(const float* __restrict__ Ein, float* __restrict__ Eout, const float* __restrict__ f,
+                                   Geo gc, float h2) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int NCM = gc.NN - 1;
+  if (q >= (long long)NCM * NCM * NCM) return;
+  const int K2 = (int)(q % NCM) + 1, J = (int)((q / NCM) % NCM) + 1, I = (int)(q / ((long long)NCM * NCM)) + 1;
+  const long long c = (long long)I * gc.S2 + (long long)J * gc.S + K2, SC = gc.S, SC2 = gc.S2;
+  const float ec = Ein[c];
+  const float sn = F_ADD(F_ADD(F_ADD(F_ADD(F_ADD(Ein[c + SC2], Ein[c - SC2]), Ein[c + SC]), Ein[c - SC]), Ein[c + 1]),
+                         Ein[c - 1]);
+  const float hc2 = F_MUL(4.0f, h2);
+  Eout[c] = F_ADD(F_MUL(0.3333f, ec), F_DIV(F_ADD(sn, F_MUL(hc2, f[c])), 9.0f));
+}
+
+__global__ void k_mj_prolong(const float* __restrict__ Ec, float* __restrict__ Pf, Geo g, Geo gc) {
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, k;
+  if (id >= g.S3 || !interior_of(id, g, i, j, k)) return;
+  const int NC = gc.NN;
+  const int ci = i / 2, cj = j / 2, ck = k / 2;
+  const int ci1 = min(ci + (i & 1), NC), cj1 = min(cj + (j & 1), NC), ck1 = min(ck + (k & 1), NC);
+  const float wi = (i & 1) ? 0.5f : 1.0f, wj = (j & 1) ? 0.5f : 1.0f, wk = (k & 1) ? 0.5f : 1.0f;
+  const float wi1 = F_SUB(1.0f, wi), wj1 = F_SUB(1.0f, wj), wk1 = F_SUB(1.0f, wk);
+  const long long SC = gc.S, SC2 = gc.S2;
+#define EC(a, b, c) Ec[(long long)(a) * SC2 + (long long)(b) * SC + (c)]
+  float corr = 0.0f;
+  corr = F_ADD(corr, F_MUL(F_MUL(F_MUL(wi, wj), wk), EC(ci, cj, ck)));
+  corr = F_ADD(corr, F_MUL(F_MUL(F_MUL(wi, wj), wk1), EC(ci, cj, ck1)));
+  corr = F_ADD(corr, F_MUL(F_MUL(F_MUL(wi, wj1), wk), EC(ci, cj1, ck)));
+  corr = F_ADD(corr, F_MUL(F_MUL(F_MUL(wi, wj1), wk1), EC(ci, cj1, ck1)));
+  corr = F_ADD(corr, F_MUL(F_MUL(F_MUL(wi1, wj), wk), EC(ci1, cj, ck)));
+  corr = F_ADD(corr, F_MUL(F_MUL(F_MUL(wi1, wj), wk1), EC(ci1, cj, ck1)));
+  corr = F_ADD(corr, F_MUL(F_MUL(F_MUL(wi1, wj1), wk), EC(ci1, cj1, ck)));
+  corr = F_ADD(corr, F_MUL(F_MUL(F_MUL(wi1, wj1), wk1), EC(ci1, cj1, ck1)));
+#undef EC
+  Pf[id] = F_ADD(Pf[id], F_MUL(0.5f, corr));
+}
+
+// ---------------------------------------------------------------------------------------
+// evolveBoundary (molecule.js:426-540 without locked groups / shell splits): snapshot
+// labels in, labels + W out; the new label word carries its recomputed exclusion bit.
+// ---------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_mj_evolve(const int* __restrict__ labIn, int* __restrict__ labOut,
+                                                   const float* __restrict__ U, float* __restrict__ W,
+                                                   const MjAtom* __restrict__ atoms, int nAt, Geo g, float dt_w,
+                                                   float curvReg, float h, bool hasBare) {
+  const int k = 1 + blockIdx.x * kThreadsK + threadIdx.x;
+  const int j = 1 + blockIdx.y * kThreadsJ + threadIdx.y;
+  const int i0 = 1 + blockIdx.z * kMarch;
+  if (k >= g.NN || j >= g.NN || i0 >= g.NN) return;
+  const int iend = min(i0 + kMarch, g.NN);
+  const long long S = g.S, S2 = g.S2;
+  for (int i = i0; i < iend; ++i) {
+    const long long id = (long long)i * S2 + j * S + k;
+    const int stored = __ldg(labIn + id);
+    const int myL = stored & kMjMask;
+    const float uc = __ldg(U + id);
+    const float myRho = F_MUL(uc, uc);
+    const long long nb[6] = {id + S2, id - S2, id + S, id - S, id + 1, id - 1};
+    int bestL = myL;
+    float bestRho = 0.f, myCnt = 0.f;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      const int l = __ldg(labIn + nb[q]) & kMjMask;
+      if (l == myL) {
+        myCnt = F_ADD(myCnt, 1.0f);
+      } else {
+        const float un = __ldg(U + nb[q]);
+        const float r = F_MUL(un, un);
+        if (r > bestRho) { bestRho = r; bestL = l; }
+      }
+    }
+    float w = W[id];
+    if (myCnt >= 6.0f) {
+      W[id] = fmaxf(w, 1.0f);
+      labOut[id] = stored;
+      continue;
+    }
+    const float denom = F_ADD(myRho, bestRho);
+    const float vel = (denom < 1e-20f) ? 0.0f : F_DIV(F_SUB(myRho, bestRho), denom);
+    w = F_ADD(w, F_MUL(dt_w, vel));
+    const float curv = F_DIV(F_SUB(myCnt, 3.0f), 3.0f);
+    w = F_ADD(w, F_MUL(curvReg, curv));
+    int newL = myL;
+    if (w < 0.0f) { newL = bestL; w = 0.1f; }
+    W[id] = w;
+    labOut[id] = (newL == myL) ? stored : mj_pack(i, j, k, newL, atoms, nAt, hasBare, h);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// reduceEnergy terms (molecule.js:950-1075) in FP64: per label (norm, T, V_eK, V_ee) plus
+// the three dipole sums; exclusion radius max(rc, R_SING) with real distances.
+// ---------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_mj_energy(const float* __restrict__ U, const float* __restrict__ Pv,
+                                                   const float* __restrict__ K, const int* __restrict__ label,
+                                                   const MjAtom* __restrict__ atoms, Geo g, float h, float h3,
+                                                   float Rsing, int nDom, double* __restrict__ pd,
+                                                   double* __restrict__ dip) {
+  __shared__ DomTable<4, 128> tab;
+  __shared__ double sdip[3][8];
+  dom_table_init(tab);
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  __syncthreads();
+  RunSum<4> rs;
+  rs.reset();
+  double dx = 0, dy = 0, dz = 0;
+  const int k = 1 + blockIdx.x * kThreadsK + threadIdx.x;
+  const int j = 1 + blockIdx.y * kThreadsJ + threadIdx.y;
+  const int i0 = 1 + blockIdx.z * kMarch;
+  if (k < g.NN && j < g.NN && i0 < g.NN) {
+    const int iend = min(i0 + kMarch, g.NN);
+    const long long S = g.S, S2 = g.S2;
+    for (int i = i0; i < iend; ++i) {
+      const long long id = (long long)i * S2 + j * S + k;
+      const float v = U[id];
+      const float rho = F_MUL(v, v);
+      const int L = label[id] & kMjMask;
+      const MjAtom a = atoms[L];
+      const float rcx = fmaxf(a.rc, Rsing);
+      if (mj_dist(i, j, k, a, h) < rcx) continue;
+      const bool sip = (label[id + S2] & kMjMask) == L && !(mj_dist(i + 1, j, k, a, h) < rcx);
+      const bool sjp = (label[id + S] & kMjMask) == L && !(mj_dist(i, j + 1, k, a, h) < rcx);
+      const bool skp = (label[id + 1] & kMjMask) == L && !(mj_dist(i, j, k + 1, a, h) < rcx);
+      const double da = sip ? (double)F_SUB(U[id + S2], v) : 0.0;
+      const double db = sjp ? (double)F_SUB(U[id + S], v) : 0.0;
+      const double dc = skp ? (double)F_SUB(U[id + 1], v) : 0.0;
+      const double r3 = (double)rho * (double)h3;
+      double q[4] = {r3, 0.5 * (da * da + db * db + dc * dc) * (double)h, -(double)K[id] * r3, (double)Pv[id] * r3};
+      rs.add(min(L, nDom - 1), q, tab, pd);
+      dx += r3 * (double)F_MUL((float)i, h);
+      dy += r3 * (double)F_MUL((float)j, h);
+      dz += r3 * (double)F_MUL((float)k, h);
+    }
+  }
+  rs.finish(tab, pd);
+  // warp reduce the dipole partials
+  for (int o = 16; o > 0; o >>= 1) {
+    dx += __shfl_down_sync(0xffffffffu, dx, o);
+    dy += __shfl_down_sync(0xffffffffu, dy, o);
+    dz += __shfl_down_sync(0xffffffffu, dz, o);
+  }
+  if ((tid & 31) == 0) { sdip[0][tid >> 5] = dx; sdip[1][tid >> 5] = dy; sdip[2][tid >> 5] = dz; }
+  __syncthreads();
+  dom_table_flush(tab, pd);
+  if (tid < 3) {
+    double s = 0;
+    for (int w = 0; w < (blockDim.x * blockDim.y) / 32; ++w) s += sdip[tid][w];
+    atomicAdd(&dip[tid], s);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// gradPtotal (molecule.js:1200-1269): F = 2 Z <grad P> over the integer ball of radius R
+// around the (integer) nucleus; one block per atom, FP64 block reduction.
+// ---------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_mj_gradp(const float* __restrict__ Pt, const MjAtom* __restrict__ atoms,
+                                                  Geo g, float inv_h, int R, double* __restrict__ F) {
+  __shared__ double red[4][8];
+  const int atom = blockIdx.x;
+  const MjAtom a = atoms[atom];
+  const float ZA = (a.Z <= 0.f) ? a.Z_nuc : a.Z;
+  const int tid = threadIdx.x;
+  if (ZA <= 0.f) {
+    if (tid < 3) F[atom * 3 + tid] = 0.0;
+    return;
+  }
+  const int ci = (int)a.posI, cj = (int)a.posJ, ck = (int)a.posK;
+  const int D = 2 * R + 1;
+  const long long nball = (long long)D * D * D;
+  const float inv2h = F_MUL(0.5f, inv_h);
+  const long long S = g.S, S2 = g.S2;
+  double sx = 0, sy = 0, sz = 0, cnt = 0;
+  for (long long q = tid; q < nball; q += blockDim.x) {
+    const int di = (int)(q / ((long long)D * D)) - R, dj = (int)((q / D) % D) - R, dk = (int)(q % D) - R;
+    const int ii = ci + di, jj = cj + dj, kk = ck + dk;
+    if (ii < 1 || ii >= g.S - 1 || jj < 1 || jj >= g.S - 1 || kk < 1 || kk >= g.S - 1) continue;
+    if (di * di + dj * dj + dk * dk > R * R) continue;
+    const long long id = (long long)ii * S2 + (long long)jj * S + kk;
+    sx += (double)F_MUL(F_SUB(Pt[id + S2], Pt[id - S2]), inv2h);
+    sy += (double)F_MUL(F_SUB(Pt[id + S], Pt[id - S]), inv2h);
+    sz += (double)F_MUL(F_SUB(Pt[id + 1], Pt[id - 1]), inv2h);
+    cnt += 1.0;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sx += __shfl_down_sync(0xffffffffu, sx, o);
+    sy += __shfl_down_sync(0xffffffffu, sy, o);
+    sz += __shfl_down_sync(0xffffffffu, sz, o);
+    cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+  }
+  if ((tid & 31) == 0) { red[0][tid >> 5] = sx; red[1][tid >> 5] = sy; red[2][tid >> 5] = sz; red[3][tid >> 5] = cnt; }
+  __syncthreads();
+  if (tid == 0) {
+    double t[4] = {0, 0, 0, 0};
+    for (int w = 0; w < blockDim.x / 32; ++w)
+      for (int c = 0; c < 4; ++c) t[c] += red[c][w];
+    const double n = t[3] > 0 ? t[3] : 1.0;
+    F[atom * 3 + 0] = 2.0 * (double)ZA * (t[0] / n);
+    F[atom * 3 + 1] = 2.0 * (double)ZA * (t[1] / n);
+    F[atom * 3 + 2] = 2.0 * (double)ZA * (t[2] / n);
+  }
+}
+
+// ======================================================================================
+// host launchers
+// ======================================================================================
+static unsigned flat_blocks(long long n) { return (unsigned)((n + 255) / 256); }
+
+cudaError_t launch_mj_init(float* K, float* U, float* bestU, int* label, const MjAtom* atoms, int nAt, const Geo& g,
+                           float h, float h2, float Rsing, bool hasBare, bool persist, cudaStream_t st) {
+  if (persist)
+    k_mj_init<true><<<flat_blocks(g.S3), 256, 0, st>>>(K, U, bestU, label, atoms, nAt, g, h, h2, Rsing, hasBare);
+  else
+    k_mj_init<false><<<flat_blocks(g.S3), 256, 0, st>>>(K, U, bestU, label, atoms, nAt, g, h, h2, Rsing, hasBare);
+  return cudaGetLastError();
+}
+cudaError_t launch_mj_recompute_k(float* K, const MjAtom* atoms, int nAt, const Geo& g, float h, float Rsing,
+                                  cudaStream_t st) {
+  k_mj_recompute_k<<<flat_blocks(g.S3), 256, 0, st>>>(K, atoms, nAt, g, h, Rsing);
+  return cudaGetLastError();
+}
+cudaError_t launch_mj_flags(int* label, const MjAtom* atoms, int nAt, const Geo& g, float h, bool hasBare,
+                            cudaStream_t st) {
+  k_mj_flags<<<flat_blocks(g.S3), 256, 0, st>>>(label, atoms, nAt, g, h, hasBare);
+  return cudaGetLastError();
+}
+cudaError_t launch_mj_update(const float* U, float* Uo, const float* K, const int* label, const float* Pother,
+                             const Geo& g, float half_d, float dt, float h3, int nDom, unsigned* unorm,
+                             cudaStream_t st) {
+  if (g.NN < 2) return cudaSuccess;
+  if (unorm)
+    k_mj_update<true><<<march_grid(g), march_block(), 0, st>>>(U, Uo, K, label, Pother, g, half_d, dt, h3, nDom, unorm);
+  else
+    k_mj_update<false><<<march_grid(g), march_block(), 0, st>>>(U, Uo, K, label, Pother, g, half_d, dt, h3, nDom,
+                                                                 nullptr);
+  return cudaGetLastError();
+}
+cudaError_t launch_mj_norm_scale(const unsigned* unorm, const MjAtom* atoms, int nDom, float* scale, cudaStream_t st) {
+  k_mj_norm_scale<<<(nDom + 127) / 128, 128, 0, st>>>(unorm, atoms, nDom, scale);
+  return cudaGetLastError();
+}
+cudaError_t launch_mj_apply_scale(float* U, const int* label, const float* scale, const Geo& g, cudaStream_t st) {
+  if (g.NN < 2) return cudaSuccess;
+  k_mj_apply_scale<<<march_grid(g), march_block(), 0, st>>>(U, label, scale, g);
+  return cudaGetLastError();
+}
+cudaError_t launch_mj_jacobi(const float* Pin, float* Pout, const float* U, const Geo& g, float h2, float two_pi,
+                             cudaStream_t st) {
+  if (g.NN < 2) return cudaSuccess;
+  k_mj_jacobi<<<march_grid(g), march_block(), 0, st>>>(Pin, Pout, U, g, h2, two_pi);
+  return cudaGetLastError();
+}
+cudaError_t launch_mj_vcycle(float* P, const float* U, float* rho, float* resid, float* Ec0, float* Ec1, float* fc,
+                             const Geo& g, const Geo& gc, float h2, float inv_h2, float two_pi, cudaStream_t st) {
+  // molecule.js:2879-2907: residual of P, restrict, 10 coarse weighted-Jacobi sweeps from 0,
+  // prolongate with P += 0.5 * correction
+  k_mj_rho<<<flat_blocks(g.S3), 256, 0, st>>>(U, rho, g);
+  k_mj_residual<<<flat_blocks(g.S3), 256, 0, st>>>(P, resid, rho, g, inv_h2, two_pi);
+  const long long nc = (long long)(gc.NN - 1) * (gc.NN - 1) * (gc.NN - 1);
+  k_mj_restrict<<<flat_blocks(nc), 256, 0, st>>>(resid, fc, g, gc);
+  cudaError_t e = cudaMemsetAsync(Ec0, 0, sizeof(float) * gc.S3, st);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(Ec1, 0, sizeof(float) * gc.S3, st);
+  if (e != cudaSuccess) return e;
+  float* E[2] = {Ec0, Ec1};
+  for (int cs = 0; cs < 10; ++cs) k_mj_coarse_smooth<<<flat_blocks(nc), 256, 0, st>>>(E[cs % 2], E[(cs + 1) % 2], fc, gc, h2);
+  k_mj_prolong<<<flat_blocks(g.S3), 256, 0, st>>>(E[0], P, g, gc);
+  return cudaGetLastError();
+}
+cudaError_t launch_mj_evolve(const int* labIn, int* labOut, const float* U, float* W, const MjAtom* atoms, int nAt,
+                             const Geo& g, float dt_w, float curvReg, float h, bool hasBare, cudaStream_t st) {
+  if (g.NN < 2) return cudaSuccess;
+  k_mj_evolve<<<march_grid(g), march_block(), 0, st>>>(labIn, labOut, U, W, atoms, nAt, g, dt_w, curvReg, h, hasBare);
+  return cudaGetLastError();
+}
+cudaError_t launch_mj_energy(const float* U, const float* Pv, const float* K, const int* label, const MjAtom* atoms,
+                             const Geo& g, float h, float h3, float Rsing, int nDom, double* pd, double* dip,
+                             cudaStream_t st) {
+  if (g.NN < 2) return cudaSuccess;
+  k_mj_energy<<<march_grid(g), march_block(), 0, st>>>(U, Pv, K, label, atoms, g, h, h3, Rsing, nDom, pd, dip);
+  return cudaGetLastError();
+}
+cudaError_t launch_mj_gradp(const float* P, const MjAtom* atoms, int nAt, const Geo& g, float inv_h, int R, double* F,
+                            cudaStream_t st) {
+  k_mj_gradp<<<nAt, 256, 0, st>>>(P, atoms, g, inv_h, R, F);
+  return cudaGetLastError();
+}
+
+}  // namespace rq
+
+namespace rq {
+__global__ void k_fill(float* __restrict__ f, float v, long long n) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    f[q] = v;
+}
+__global__ void k_unpack(const int* __restrict__ in, int* __restrict__ out, long long n) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    out[q] = in[q] & kMjMask;
+}
+cudaError_t launch_fill(float* f, float v, long long n, cudaStream_t st) {
+  k_fill<<<148 * 8, 256, 0, st>>>(f, v, n);
+  return cudaGetLastError();
+}
+cudaError_t launch_unpack_labels(const int* in, int* out, long long n, cudaStream_t st) {
+  k_unpack<<<148 * 8, 256, 0, st>>>(in, out, n);
+  return cudaGetLastError();
+}
+}  // namespace rq

@@ -24,6 +24,7 @@ struct rq_ctx {
   double h = 0, h2 = 0, h3 = 0, dv = 0, dt = 0, half_dv = 0, sigma = 0;
   int n_atoms = 0;
   std::vector<rq_atom> atoms;
+  std::vector<rq_atom> atoms0;  // positions at creation (molecule.js groups nuclei by them)
   bool fp64 = false;
   cudaStream_t st = nullptr;
   cudaStream_t own_st = nullptr;
@@ -50,6 +51,7 @@ struct rq_ctx {
 
   // atoms on the device
   float* atoms5 = nullptr;    // [i,j,k,Z,rc] f32 (cloud/solver.py:378-382)
+  float* scratch_atoms5 = nullptr;  // per-call atom table for force variants
   void* atoms_mj = nullptr;   // molecule.js records (u32 positions)
   double* atoms_nm = nullptr; // new flavour: x,y,z (bohr), Z_nuc per atom
   float* Zdom = nullptr;      // domain charge per label (f32)

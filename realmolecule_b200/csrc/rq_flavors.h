@@ -15,6 +15,7 @@ int mj_step_one(rq_ctx* c, int s);
 int mj_energy(rq_ctx* c, double* out, double* per_domain);
 int mj_forces(rq_ctx* c, int method, double* F);
 int mj_set_atoms(rq_ctx* c);
+int mj_refresh_flags(rq_ctx* c);
 void mj_nuclear_terms(rq_ctx* c, double* E, double* F);
 
 // new flavour (nm_flavor.cu)

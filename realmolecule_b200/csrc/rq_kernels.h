@@ -27,4 +27,34 @@ cudaError_t launch_forces_hf_sp(const float* U, const float* atoms5, int nAtoms,
 template <typename T>
 cudaError_t launch_zero_faces(T* f, const Geo& g, cudaStream_t st);
 
+// ---- molecule.js flavour (mj_kernels.cu); labels carry the r_c-exclusion flag in bit 30 ---
+}  // namespace rq
+struct MjAtom;
+namespace rq {
+constexpr int kMjExclBit = 0x40000000;
+constexpr int kMjLabelMask = 0x3FFFFFFF;
+cudaError_t launch_mj_init(float* K, float* U, float* bestU, int* label, const MjAtom* atoms, int nAt, const Geo& g,
+                           float h, float h2, float Rsing, bool hasBare, bool persist, cudaStream_t st);
+cudaError_t launch_mj_recompute_k(float* K, const MjAtom* atoms, int nAt, const Geo& g, float h, float Rsing,
+                                  cudaStream_t st);
+cudaError_t launch_mj_flags(int* label, const MjAtom* atoms, int nAt, const Geo& g, float h, bool hasBare,
+                            cudaStream_t st);
+cudaError_t launch_mj_update(const float* U, float* Uo, const float* K, const int* label, const float* Pother,
+                             const Geo& g, float half_d, float dt, float h3, int nDom, unsigned* unorm, cudaStream_t st);
+cudaError_t launch_mj_norm_scale(const unsigned* unorm, const MjAtom* atoms, int nDom, float* scale, cudaStream_t st);
+cudaError_t launch_mj_apply_scale(float* U, const int* label, const float* scale, const Geo& g, cudaStream_t st);
+cudaError_t launch_mj_jacobi(const float* Pin, float* Pout, const float* U, const Geo& g, float h2, float two_pi,
+                             cudaStream_t st);
+cudaError_t launch_mj_vcycle(float* P, const float* U, float* rho, float* resid, float* Ec0, float* Ec1, float* fc,
+                             const Geo& g, const Geo& gc, float h2, float inv_h2, float two_pi, cudaStream_t st);
+cudaError_t launch_mj_evolve(const int* labIn, int* labOut, const float* U, float* W, const MjAtom* atoms, int nAt,
+                             const Geo& g, float dt_w, float curvReg, float h, bool hasBare, cudaStream_t st);
+cudaError_t launch_mj_energy(const float* U, const float* Pv, const float* K, const int* label, const MjAtom* atoms,
+                             const Geo& g, float h, float h3, float Rsing, int nDom, double* pd, double* dip,
+                             cudaStream_t st);
+cudaError_t launch_mj_gradp(const float* P, const MjAtom* atoms, int nAt, const Geo& g, float inv_h, int R, double* F,
+                            cudaStream_t st);
+cudaError_t launch_fill(float* f, float v, long long n, cudaStream_t st);
+cudaError_t launch_unpack_labels(const int* in, int* out, long long n, cudaStream_t st);
+
 }  // namespace rq
