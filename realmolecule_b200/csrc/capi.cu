@@ -119,7 +119,7 @@ static void free_ctx(rq_ctx* c) {
   for (auto e : c->evpool) cudaEventDestroy(e);
   for (auto& gx : c->graph)
     if (gx) cudaGraphExecDestroy(gx);
-  void* ptrs[] = {c->U[0], c->U[1], c->P[0], c->P[1], c->K, c->W, c->bestU, c->rho, c->Pother, c->lab[0], c->lab[1],
+  void* ptrs[] = {c->U[0], c->U[1], c->P[0], c->P[1], c->K, c->W, c->bestU, c->rho, c->Pother, c->resid, c->lab[0], c->lab[1],
                   c->Ec[0], c->Ec[1], c->fc, c->atoms5, c->scratch_atoms5, c->atoms_mj, c->atoms_nm, c->Zdom, c->Zdom64, c->dnorm,
                   c->dpd, c->dF, c->dsum, c->unorm, c->scale, c->err};
   for (void* p : ptrs)
@@ -159,6 +159,7 @@ static int alloc_all(rq_ctx* c) {
   if (c->cfg.flavor == RQ_FLAVOR_MOLECULE_JS) {
     DALLOC(c->rho, S3 * sizeof(float));
     DALLOC(c->Pother, S3 * sizeof(float));
+    DALLOC(c->resid, S3 * sizeof(float));
     const int SC = c->g.NN / 2 + 1;
     c->gc = make_geo(SC);
     const size_t SC3 = (size_t)c->gc.S3;

@@ -117,7 +117,7 @@ int mj_step_one(rq_ctx* c, int s) {
     }
     if (sf > 0 && sf % f.vcycle_interval == 0)  // molecule.js:2879
       LAUNCH(RQ_KC_MG, 40 * ip,
-             launch_mj_vcycle((float*)c->P[c->cp], (float*)c->U[c->cu], c->rho, c->bestU, c->Ec[0], c->Ec[1], c->fc,
+             launch_mj_vcycle((float*)c->P[c->cp], (float*)c->U[c->cu], c->rho, c->resid, c->Ec[0], c->Ec[1], c->fc,
                               c->g, c->gc, p.h2, p.inv_h2, p.two_pi, c->st));
   }
   const bool norm = ((sf + 1) % f.norm_interval == 0) || sf == spf - 1;  // molecule.js:2972

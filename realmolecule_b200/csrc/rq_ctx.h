@@ -38,6 +38,7 @@ struct rq_ctx {
   float* bestU = nullptr;
   float* rho = nullptr;   // molecule.js rhoTotal / residual scratch (float)
   float* Pother = nullptr;  // molecule.js PotherBuf (stale P of the previous frame)
+  float* resid = nullptr;   // molecule.js V-cycle residual
   int* lab[2] = {nullptr, nullptr};
   int cu = 0, cp = 0, cl = 0;
 
