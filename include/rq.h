@@ -74,9 +74,10 @@ typedef struct rq_config {
   int32_t mg_coarse_sweeps; /* new: FP64 red-black sweeps on the coarsest level (64) */
   int32_t sic;              /* molecule.js SIC (:3009-3076): 0 off (only value supported here) */
   double boundary_speed;    /* molecule.js dt_w (0.5, :135) */
-  double curv_reg;          /* molecule.js curvReg (0.15, :34) */
+  double curv_reg;          /* molecule.js curvReg (0: 0.15 as :34; < 0: off) */
   double sigma;             /* new: Gaussian nucleus width in bohr (<=0: h) */
-  int32_t reserved[8];
+  int32_t label_until;      /* labels update only while steps_done < label_until (0: always) */
+  int32_t reserved[7];
 } rq_config;
 
 /* One entry of the reference atom list: a nucleus and/or one electron domain. */

@@ -109,6 +109,8 @@ class _Oracle:
             "orc_nm_energy": [_f64p, _f64p, _f64p, _i32p, _i, _d, _f64p, _i, _f64p],
             "orc_nm_normalize": [_f64p, _i32p, _i64, _i, _f64p, _f64p],
             "orc_nm_force": [_f64p, _f64p, _f64p, _i, _i, _d, _d, _f64p],
+            "orc_nm_init": [_f64p, _i32p, _f32p, _i32p, _i, _i, _f],
+            "orc_nm_evolve": [_i32p, _i32p, _f64p, _f32p, _i, _d, _d],
         }
         for name, argt in sig.items():
             fn = getattr(L, name)
@@ -442,3 +444,111 @@ class MoleculeJsDriver:
         O().mj_energy(self.U, self.Pother, self.K, self.label, C.addressof(self.atoms), self.S, self.h, self.h3,
                       self.Rsing, out)
         return out
+
+
+class NewMethodDriver:
+    """FP64 restatement of the new flavour's schedule (Gaussian nuclei of width sigma, red-black
+    multigrid V-cycle every ``poisson_interval`` steps, ITP update, FP64 normalisation to the
+    domain charges every ``norm_interval`` steps, level-set labels every ``label_interval``).
+
+    ``rows`` use the flavour's idiom: nuclei have Z_nuc > 0, domains have Z > 0 (their position
+    is the seed of the initial state).  Positions are grid units (x = i*h)."""
+
+    def __init__(self, NN, screen, rows, dv=0.2, sigma=None, poisson_interval=2, norm_interval=1, label_interval=20,
+                 levels=None, pre=2, post=2, coarse_sweeps=64, boundary_speed=0.5, curv_reg=0.15, label_until=0):
+        self.NN, self.S = NN, NN + 1
+        self.S3 = self.S ** 3
+        self.h = screen / NN
+        self.sigma = sigma or self.h
+        self.rows = [dict(r) for r in rows]
+        self.n = len(rows)
+        self.dv = dv
+        self.half_dv, self.dt = 0.5 * dv, dv * self.h * self.h
+        self.pi_, self.ni, self.li = poisson_interval, norm_interval, label_interval
+        if levels is None:
+            levels, nn = 1, NN
+            while nn % 2 == 0 and nn // 2 >= 6:
+                nn //= 2
+                levels += 1
+        self.levels, self.pre, self.post, self.cs = levels, pre, post, coarse_sweeps
+        self.dt_w, self.curv = boundary_speed, curv_reg
+        self.label_until = label_until
+        self.Zdom = np.array([r.get("Z", 0.0) for r in rows], np.float64)
+        self.K = np.zeros(self.S3)
+        self.U = np.zeros(self.S3)
+        self.U2 = np.zeros(self.S3)
+        self.P = np.zeros(self.S3)
+        self.label = np.zeros(self.S3, np.int32)
+        self.label2 = np.zeros(self.S3, np.int32)
+        self.W = np.ones(self.S3, np.float32)
+        self.steps_done = 0
+        self.potential()
+
+    def nuclei(self):
+        xyz = np.array([[r["i"] * self.h, r["j"] * self.h, r["k"] * self.h] for r in self.rows], np.float64)
+        Z = np.array([max(r.get("Z_nuc", 0.0), 0.0) for r in self.rows], np.float64)
+        return np.ascontiguousarray(xyz.reshape(-1)), Z
+
+    def potential(self):
+        xyz, Z = self.nuclei()
+        O().nm_potential(self.K, xyz, Z, self.n, self.S, self.h, self.sigma)
+
+    def set_positions(self, rows):
+        self.rows = [dict(r) for r in rows]
+        self.potential()
+
+    def initialize(self, vcycles=10):
+        seeds = [(q, r) for q, r in enumerate(self.rows) if r.get("Z", 0) > 0]
+        hf = np.float32(self.h)
+        xyz = np.array([[np.float32(r["i"] * self.h), np.float32(r["j"] * self.h), np.float32(r["k"] * self.h)]
+                        for _, r in seeds], np.float32).reshape(-1)
+        idx = np.array([q for q, _ in seeds], np.int32)
+        O().nm_init(self.U, self.label, np.ascontiguousarray(xyz), idx, len(seeds), self.S, hf)
+        self.label2[:] = self.label
+        self.normalize()
+        for _ in range(vcycles):
+            self.vcycle()
+
+    def domain_sums(self):
+        out = np.zeros(3)
+        pd = np.zeros(self.n * 4)
+        O().nm_energy(self.U, self.K, self.P, self.label, self.S, self.h, out, self.n, pd)
+        return out, pd.reshape(self.n, 4)
+
+    def normalize(self):
+        _, pd = self.domain_sums()
+        O().nm_normalize(self.U, self.label, self.S3, self.n, self.Zdom, np.ascontiguousarray(pd[:, 0]))
+
+    def vcycle(self):
+        O().nm_vcycle(self.P, self.U, self.S, self.h, self.levels, self.pre, self.post, self.cs)
+
+    def step(self):
+        self.steps_done += 1
+        s = self.steps_done
+        if s % self.pi_ == 0:
+            self.vcycle()
+        O().nm_update(self.U, self.U2, self.K, self.P, self.label, self.S, self.half_dv, self.dt)
+        self.U, self.U2 = self.U2, self.U
+        if s % self.ni == 0:
+            self.normalize()
+        if s % self.li == 0 and (self.label_until <= 0 or s <= self.label_until):
+            O().nm_evolve(self.label, self.label2, self.U, self.W, self.S, float(np.float32(self.dt_w)),
+                          float(np.float32(self.curv)))
+            self.label, self.label2 = self.label2, self.label
+
+    def energy(self):
+        out, pd = self.domain_sums()
+        xyz, Z = self.nuclei()
+        xyz = xyz.reshape(-1, 3)
+        ekk = 0.0
+        for a in range(self.n):
+            for b in range(a + 1, self.n):
+                if Z[a] > 0 and Z[b] > 0:
+                    ekk += Z[a] * Z[b] / np.linalg.norm(xyz[a] - xyz[b])
+        return {"T": out[0], "EK": out[1], "EE": out[2], "KK": ekk, "E": out.sum() + ekk, "per_domain": pd}
+
+    def forces(self):
+        xyz, Z = self.nuclei()
+        F = np.zeros(self.n * 3)
+        O().nm_force(self.U, xyz, Z, self.n, self.S, self.h, self.sigma, F)
+        return F.reshape(-1, 3)

@@ -932,8 +932,14 @@ void orc_nm_energy(const double* U, const double* K, const double* P, const int3
         double a = (label[id + S2] == L) ? U[id + S2] - u : 0.0;
         double b = (label[id + S] == L) ? U[id + S] - u : 0.0;
         double c = (label[id + 1] == L) ? U[id + 1] - u : 0.0;
+        /* every same-label edge with an interior end point once: forward edges plus the edge
+           to the Dirichlet face below on the first interior layer (psi = 0 there) */
+        double t = a * a + b * b + c * c;
+        if (i == 1 && label[id - S2] == L) t += u * u;
+        if (j == 1 && label[id - S] == L) t += u * u;
+        if (k == 1 && label[id - 1] == L) t += u * u;
         double* q = pd + ((size_t)i * nDom + L) * 4;
-        q[0] += rho * h3; q[1] += 0.5 * (a * a + b * b + c * c) * h; q[2] += -K[id] * rho * h3;
+        q[0] += rho * h3; q[1] += 0.5 * t * h; q[2] += -K[id] * rho * h3;
         q[3] += P[id] * rho * h3;
       }
   memset(per_domain, 0, sizeof(double) * nDom * 4);
@@ -980,4 +986,65 @@ void orc_nm_force(const double* U, const double* xyz, const double* Z, int nAt, 
         }
     F[3 * a] = fx; F[3 * a + 1] = fy; F[3 * a + 2] = fz;
   }
+}
+
+/* Initial state of the new method: label = nearest domain seed by f32 squared distance
+ * (first seed wins ties), psi = exp(-sqrt(d2)) in FP64, boundary psi = 0.  seeds: x,y,z (f32,
+ * bohr) and the entry index of each domain seed. */
+void orc_nm_init(double* U, int32_t* label, const float* seeds_xyz, const int32_t* seed_idx, int nSeed, int S, float h) {
+  const int NN = S - 1;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < S; ++i)
+    for (int j = 0; j < S; ++j)
+      for (int k = 0; k < S; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        float x = (float)i * h, y = (float)j * h, z = (float)k * h;
+        float best = 3.4e38f;
+        int bl = 0;
+        for (int m = 0; m < nSeed; ++m) {
+          float dx = x - seeds_xyz[3 * m], dy = y - seeds_xyz[3 * m + 1], dz = z - seeds_xyz[3 * m + 2];
+          float d2 = dx * dx + dy * dy + dz * dz;
+          if (d2 < best) { best = d2; bl = seed_idx[m]; }
+        }
+        label[id] = bl;
+        U[id] = interior(i, j, k, NN) ? exp(-sqrt((double)best)) : 0.0;
+      }
+}
+
+/* The molecule.js level-set rule (molecule.js:426-540) on FP64 psi, snapshot labels. */
+void orc_nm_evolve(const int32_t* labelIn, int32_t* labelOut, const double* U, float* W, int S, double dt_w,
+                   double curvReg) {
+  const int NN = S - 1;
+  const int64_t S2 = (int64_t)S * S;
+  memcpy(labelOut, labelIn, sizeof(int32_t) * (size_t)S2 * S);
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        int32_t myL = labelIn[id];
+        double myRho = U[id] * U[id];
+        const int64_t nb[6] = {id + S2, id - S2, id + S, id - S, id + 1, id - 1};
+        int32_t bestL = myL;
+        double bestRho = 0, myCnt = 0;
+        for (int q = 0; q < 6; ++q) {
+          int32_t l = labelIn[nb[q]];
+          if (l == myL) myCnt += 1.0;
+          else {
+            double r = U[nb[q]] * U[nb[q]];
+            if (r > bestRho) { bestRho = r; bestL = l; }
+          }
+        }
+        double w = (double)W[id];
+        if (myCnt >= 6.0) { W[id] = (float)(w > 1.0 ? w : 1.0); labelOut[id] = myL; continue; }
+        double denom = myRho + bestRho;
+        double vel = (denom < (double)1e-20f) ? 0.0 : (myRho - bestRho) / denom;
+        w = w + dt_w * vel;
+        double curv = (myCnt - 3.0) / 3.0;
+        w = w + curvReg * curv;
+        int32_t newL = myL;
+        if (w < 0.0) { newL = bestL; w = (double)0.1f; }
+        W[id] = (float)w;
+        labelOut[id] = newL;
+      }
 }

@@ -65,8 +65,10 @@ static double default_dv(const rq_ctx* c) {
 static void fill_defaults(rq_ctx* c) {
   rq_config& f = c->cfg;
   const bool sp = f.flavor == RQ_FLAVOR_SOLVER_PY, mj = f.flavor == RQ_FLAVOR_MOLECULE_JS;
-  if (f.norm_interval <= 0) f.norm_interval = 20;
-  if (f.poisson_interval <= 0) f.poisson_interval = sp ? 2 : 1;
+  const bool nm = f.flavor == RQ_FLAVOR_NEW;
+  // the new flavour normalises every step: all-electron cores grow by e^{dt |eps|} per step
+  if (f.norm_interval <= 0) f.norm_interval = nm ? 1 : 20;
+  if (f.poisson_interval <= 0) f.poisson_interval = sp || nm ? 2 : 1;
   if (f.label_interval <= 0) f.label_interval = sp ? 5 * f.norm_interval : 20;
   if (f.jacobi_per_step <= 0) f.jacobi_per_step = 2;
   if (f.steps_per_frame <= 0) {  // molecule.js:106
@@ -79,7 +81,8 @@ static void fill_defaults(rq_ctx* c) {
   if (f.mg_post <= 0) f.mg_post = 2;
   if (f.mg_coarse_sweeps <= 0) f.mg_coarse_sweeps = 64;
   if (f.boundary_speed <= 0) f.boundary_speed = 0.5;
-  if (f.curv_reg < 0 || (mj && f.curv_reg == 0)) f.curv_reg = 0.15;
+  if (f.curv_reg == 0) f.curv_reg = 0.15;  // molecule.js:34 default; a negative value switches it off
+  if (f.curv_reg < 0) f.curv_reg = 0;
   c->dv = f.dv > 0 ? f.dv : default_dv(c);
   c->half_dv = 0.5 * c->dv;
   c->dt = c->dv * c->h2;
@@ -121,7 +124,7 @@ static void free_ctx(rq_ctx* c) {
     if (gx) cudaGraphExecDestroy(gx);
   void* ptrs[] = {c->U[0], c->U[1], c->P[0], c->P[1], c->K, c->W, c->bestU, c->rho, c->Pother, c->resid, c->lab[0], c->lab[1],
                   c->Ec[0], c->Ec[1], c->fc, c->atoms5, c->scratch_atoms5, c->atoms_mj, c->atoms_nm, c->Zdom, c->Zdom64, c->dnorm,
-                  c->dpd, c->dF, c->dsum, c->unorm, c->scale, c->err};
+                  c->dpd, c->dF, c->dsum, c->unorm, c->scale, c->err, c->seeds, c->scale64};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& L : c->mg) {
@@ -299,7 +302,7 @@ static int sp_step_one(rq_ctx* c, int s) {
                           norm ? c->dnorm : nullptr, c->st));
   c->cu ^= 1;
   if (norm && (rc = sp_normalize(c, false)) != RQ_OK) return rc;
-  if (s % f.label_interval == 0) {
+  if (s % f.label_interval == 0 && (f.label_until <= 0 || s <= f.label_until)) {
     LAUNCH(RQ_KC_LABELS, 8 * interior_points(c->g),
            launch_labels_sp(c->lab[c->cl], c->lab[1 - c->cl], c->atoms5, c->n_atoms, c->g, (float)c->h,
                             (float)c->h2, c->st));
@@ -361,7 +364,10 @@ extern "C" int rq_step(rq_ctx* c, int32_t n) {
   const int period = schedule_period(c);
   int left = n;
   while (left > 0) {
-    const bool aligned = !c->prof && period > 0 && c->steps_done % period == 0 && left >= period;
+    // a period that straddles label_until has no single captured pattern: run it eagerly
+    const int lu = c->cfg.label_until;
+    const bool straddle = lu > 0 && c->steps_done < lu && c->steps_done + period > lu;
+    const bool aligned = !c->prof && !straddle && period > 0 && c->steps_done % period == 0 && left >= period;
     if (!aligned) {
       // run eagerly up to the next period boundary (or all that is left)
       int todo = left;
@@ -372,7 +378,8 @@ extern "C" int rq_step(rq_ctx* c, int32_t n) {
       continue;
     }
     // one aligned period: replay its CUDA graph (captured on first use for this buffer parity)
-    const int key = c->cu | (c->cp << 1) | (c->cl << 2);
+    const int labels_on = (lu <= 0 || c->steps_done < lu) ? 1 : 0;
+    const int key = c->cu | (c->cp << 1) | (c->cl << 2) | (labels_on << 3);
     if (!c->graph[key]) {
       const long long l0 = c->launches;
       CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));

@@ -1,9 +1,243 @@
-// nm_flavor.cu -- new flavour (placeholder until its kernels land).
+// nm_flavor.cu -- schedule, energies and forces of the new flavour (host side of librq).
+//
+// Atom list idiom: entries with Z_nuc > 0 are nuclei (Gaussian charge of width sigma), entries
+// with Z > 0 are electron domains (their position is the seed of the initial state); labels
+// index entries.  One rq_step:
+//   every poisson_interval steps one multigrid V-cycle for  -lap P = 2 pi psi^2  (red-black
+//     Gauss-Seidel, full weighting, trilinear, coarsest level in FP64);
+//   the ITP update psi' = psi + dv/2 lap psi + dt (K - 2P) psi with same-label Neumann faces;
+//   every norm_interval steps normalisation to the domain charges (FP64 sums);
+//   every label_interval steps the level-set label update (molecule.js:426-540 rule).
+// Precision RQ_PREC_MIXED keeps fields in fp32, RQ_PREC_FP64 keeps everything in double.
+#include <cmath>
+#include <cstring>
+
 #include "rq_flavors.h"
-int nm_alloc_levels(rq_ctx*) { return RQ_OK; }
-int nm_initialize(rq_ctx* c) { return rq_fail(c, RQ_ENOTSUP, "new flavour not built yet"); }
-int nm_step_one(rq_ctx* c, int) { return rq_fail(c, RQ_ENOTSUP, "new flavour not built yet"); }
-int nm_energy(rq_ctx* c, double*, double*) { return rq_fail(c, RQ_ENOTSUP, "new flavour not built yet"); }
-int nm_forces(rq_ctx* c, int, double*) { return rq_fail(c, RQ_ENOTSUP, "new flavour not built yet"); }
-int nm_set_atoms(rq_ctx* c) { return rq_fail(c, RQ_ENOTSUP, "new flavour not built yet"); }
-void nm_nuclear_terms(rq_ctx*, double* E, double*) { *E = 0; }
+#include "rq_kernels.h"
+
+using namespace rq;
+
+#define CK(call)                                 \
+  do {                                           \
+    int _rc = rq_cuda(c, (call), #call);         \
+    if (_rc != RQ_OK) return _rc;                \
+  } while (0)
+
+namespace {
+double interior(const Geo& g) {
+  const double n = g.NN - 1;
+  return n * n * n;
+}
+size_t esize(const rq_ctx* c) { return c->fp64 ? sizeof(double) : sizeof(float); }
+}  // namespace
+
+int nm_alloc_levels(rq_ctx* c) {
+  // levels: halve NN while it stays even and the next level keeps NN >= 6, or mg_levels if set
+  int levels = 1, NN = c->g.NN;
+  const int want = c->cfg.mg_levels;
+  while (NN % 2 == 0 && (want > 0 ? levels < want : NN / 2 >= 6)) {
+    NN /= 2;
+    levels++;
+  }
+  if (want > 0 && levels != want) return rq_fail(c, RQ_EINVAL, "NN cannot be halved mg_levels-1 times");
+  if (levels < 2) return rq_fail(c, RQ_EINVAL, "multigrid needs NN divisible by 2");
+  if ((long long)(NN + 1) * (NN + 1) * (NN + 1) * 16 > 200 * 1024)
+    return rq_fail(c, RQ_EINVAL, "coarsest multigrid level too large for the FP64 shared-memory solve (NN/2^k > 28)");
+  c->mg.assign(levels, rq_mg_level());
+  const size_t es = esize(c);
+  double h = c->h;
+  int nn = c->g.NN;
+  for (int l = 0; l < levels; ++l) {
+    rq_mg_level& L = c->mg[l];
+    L.g = make_geo(nn + 1);
+    L.h = h;
+    const size_t n = (size_t)L.g.S3 * es;
+    if (l > 0) {
+      if (cudaMalloc(&L.P, n) != cudaSuccess || cudaMalloc(&L.f, n) != cudaSuccess)
+        return rq_cuda(c, cudaErrorMemoryAllocation, "multigrid levels");
+      cudaMemsetAsync(L.P, 0, n, c->st);
+      cudaMemsetAsync(L.f, 0, n, c->st);
+    }
+    if (l < levels - 1) {
+      if (cudaMalloc(&L.r, n) != cudaSuccess) return rq_cuda(c, cudaErrorMemoryAllocation, "multigrid residual");
+      cudaMemsetAsync(L.r, 0, n, c->st);
+    }
+    h *= 2;
+    nn /= 2;
+  }
+  if (cudaMalloc(&c->seeds, sizeof(float4) * c->n_atoms) != cudaSuccess ||
+      cudaMalloc(&c->scale64, sizeof(double) * c->n_atoms) != cudaSuccess)
+    return rq_cuda(c, cudaErrorMemoryAllocation, "seed table");
+  return RQ_OK;
+}
+
+template <typename T>
+static int vcycle_level(rq_ctx* c, int l) {
+  rq_mg_level& L = c->mg[l];
+  const bool fine = l == 0;
+  T* P = fine ? (T*)c->P[c->cp] : (T*)L.P;
+  const T* f = fine ? (const T*)c->U[c->cu] : (const T*)L.f;
+  const double h2 = L.h * L.h;
+  const double ip = interior(L.g);
+  const int last = (int)c->mg.size() - 1;
+  if (l == last) {
+    LAUNCH(RQ_KC_MG, 2.0 * sizeof(T) * L.g.S3, nm_coarsest<T>(P, f, L.g, h2, c->cfg.mg_coarse_sweeps, c->st));
+    return RQ_OK;
+  }
+  const int kc = fine ? RQ_KC_POISSON : RQ_KC_MG;
+  for (int s = 0; s < c->cfg.mg_pre; ++s)
+    for (int color = 0; color < 2; ++color)
+      LAUNCH(kc, sizeof(T) * 2.5 * ip, nm_rbgs<T>(P, f, fine, L.g, h2, color, c->st));
+  LAUNCH(kc, sizeof(T) * 3.0 * ip, nm_residual<T>(P, f, fine, (T*)L.r, L.g, 1.0 / h2, c->st));
+  rq_mg_level& C = c->mg[l + 1];
+  LAUNCH(RQ_KC_MG, sizeof(T) * (ip + interior(C.g)), nm_restrict<T>((const T*)L.r, (T*)C.f, L.g, C.g, c->st));
+  CK(cudaMemsetAsync(C.P, 0, sizeof(T) * C.g.S3, c->st));
+  int rc = vcycle_level<T>(c, l + 1);
+  if (rc != RQ_OK) return rc;
+  LAUNCH(RQ_KC_MG, sizeof(T) * (2.0 * ip + interior(C.g)), nm_prolong<T>((const T*)C.P, P, L.g, C.g, c->st));
+  for (int s = 0; s < c->cfg.mg_post; ++s)
+    for (int color = 0; color < 2; ++color)
+      LAUNCH(kc, sizeof(T) * 2.5 * ip, nm_rbgs<T>(P, f, fine, L.g, h2, color, c->st));
+  return RQ_OK;
+}
+
+static int nm_vcycle(rq_ctx* c) { return c->fp64 ? vcycle_level<double>(c, 0) : vcycle_level<float>(c, 0); }
+
+template <typename T>
+static int nm_normalize_t(rq_ctx* c, bool accumulate) {
+  T* U = (T*)c->U[c->cu];
+  if (accumulate) {
+    CK(cudaMemsetAsync(c->dnorm, 0, sizeof(double) * c->n_atoms, c->st));
+    LAUNCH(RQ_KC_NORMALIZE, (sizeof(T) + 4.0) * c->g.S3, nm_norms<T>(U, c->lab[c->cl], c->g, c->h3, c->n_atoms, c->dnorm, c->st));
+  }
+  LAUNCH(RQ_KC_NORMALIZE, (2.0 * sizeof(T) + 4.0) * c->g.S3,
+         nm_normalize<T>(U, c->lab[c->cl], c->dnorm, c->Zdom64, c->n_atoms, (T*)c->scale64, c->err, c->g, c->st));
+  return RQ_OK;
+}
+
+template <typename T>
+static int nm_step_t(rq_ctx* c, int s) {
+  const rq_config& f = c->cfg;
+  int rc;
+  if (s % f.poisson_interval == 0 && (rc = nm_vcycle(c)) != RQ_OK) return rc;
+  const bool norm = s % f.norm_interval == 0;
+  if (norm) CK(cudaMemsetAsync(c->dnorm, 0, sizeof(double) * c->n_atoms, c->st));
+  LAUNCH(RQ_KC_UPDATE, (4.0 * sizeof(T) + 4.0) * interior(c->g),
+         nm_update<T>((const T*)c->U[c->cu], (T*)c->U[1 - c->cu], (const T*)c->K, (const T*)c->P[c->cp], c->lab[c->cl],
+                      c->g, (T)c->half_dv, (T)c->dt, c->h3, c->n_atoms, norm ? c->dnorm : nullptr, c->st));
+  c->cu ^= 1;
+  if (norm && (rc = nm_normalize_t<T>(c, false)) != RQ_OK) return rc;
+  if (s % f.label_interval == 0 && (f.label_until <= 0 || s <= f.label_until)) {
+    LAUNCH(RQ_KC_LABELS, (sizeof(T) + 12.0) * interior(c->g),
+           nm_evolve<T>(c->lab[c->cl], c->lab[1 - c->cl], (const T*)c->U[c->cu], c->W, c->g, f.boundary_speed, f.curv_reg,
+                        c->st));
+    c->cl ^= 1;
+  }
+  return RQ_OK;
+}
+
+int nm_step_one(rq_ctx* c, int s) { return c->fp64 ? nm_step_t<double>(c, s) : nm_step_t<float>(c, s); }
+
+template <typename T>
+static int nm_potential_t(rq_ctx* c) {
+  LAUNCH(RQ_KC_OTHER, sizeof(T) * c->g.S3,
+         nm_potential<T>((T*)c->K, c->atoms_nm, c->n_atoms, c->g, c->h, c->sigma, c->st));
+  return RQ_OK;
+}
+
+int nm_set_atoms(rq_ctx* c) { return c->fp64 ? nm_potential_t<double>(c) : nm_potential_t<float>(c); }
+
+template <typename T>
+static int nm_init_t(rq_ctx* c) {
+  const size_t n = (size_t)c->g.S3;
+  c->cu = c->cp = c->cl = 0;
+  int rc = nm_potential_t<T>(c);
+  if (rc != RQ_OK) return rc;
+  std::vector<float4> seeds;
+  for (int q = 0; q < c->n_atoms; ++q) {
+    const rq_atom& a = c->atoms[q];
+    if (a.Z <= 0) continue;
+    float4 s;
+    s.x = (float)(a.i * c->h); s.y = (float)(a.j * c->h); s.z = (float)(a.k * c->h);
+    int idx = q;
+    std::memcpy(&s.w, &idx, sizeof(int));
+    seeds.push_back(s);
+  }
+  if (seeds.empty()) return rq_fail(c, RQ_EINVAL, "the new flavour needs at least one entry with Z > 0 (a domain)");
+  CK(cudaMemcpyAsync(c->seeds, seeds.data(), sizeof(float4) * seeds.size(), cudaMemcpyHostToDevice, c->st));
+  LAUNCH(RQ_KC_OTHER, (sizeof(T) + 4.0) * n,
+         nm_init<T>((T*)c->U[0], c->lab[0], (const float4*)c->seeds, (int)seeds.size(), c->g, (float)c->h, c->st));
+  CK(cudaMemcpyAsync(c->lab[1], c->lab[0], n * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaMemsetAsync(c->U[1], 0, n * sizeof(T), c->st));
+  for (int b = 0; b < 2; ++b) CK(cudaMemsetAsync(c->P[b], 0, n * sizeof(T), c->st));
+  LAUNCH(RQ_KC_OTHER, 4.0 * n, launch_fill(c->W, 1.0f, c->g.S3, c->st));
+  if ((rc = nm_normalize_t<T>(c, true)) != RQ_OK) return rc;
+  for (int v = 0; v < 10; ++v)  // converge the initial Hartree potential
+    if ((rc = nm_vcycle(c)) != RQ_OK) return rc;
+  return RQ_OK;
+}
+
+int nm_initialize(rq_ctx* c) { return c->fp64 ? nm_init_t<double>(c) : nm_init_t<float>(c); }
+
+void nm_nuclear_terms(rq_ctx* c, double* E, double* F) {
+  // point-charge nuclear repulsion between entries with Z_nuc > 0 (bohr)
+  double e = 0;
+  const double h = c->h;
+  for (int a = 0; a < c->n_atoms; ++a) {
+    const rq_atom& A = c->atoms[a];
+    if (A.Z_nuc <= 0) continue;
+    for (int b = 0; b < c->n_atoms; ++b) {
+      const rq_atom& B = c->atoms[b];
+      if (b == a || B.Z_nuc <= 0) continue;
+      const double dx = (A.i - B.i) * h, dy = (A.j - B.j) * h, dz = (A.k - B.k) * h;
+      const double r2 = dx * dx + dy * dy + dz * dz, r = std::sqrt(r2);
+      if (b > a) e += A.Z_nuc * B.Z_nuc / r;
+      const double w = A.Z_nuc * B.Z_nuc / (r2 * r);
+      F[a * 3] += w * dx; F[a * 3 + 1] += w * dy; F[a * 3 + 2] += w * dz;
+    }
+  }
+  *E = e;
+}
+
+int nm_energy(rq_ctx* c, double* out, double* per_domain) {
+  const int n = c->n_atoms;
+  CK(cudaMemsetAsync(c->dpd, 0, sizeof(double) * 4 * n, c->st));
+  if (c->fp64)
+    LAUNCH(RQ_KC_ENERGY, 36 * interior(c->g),
+           nm_energy<double>((const double*)c->U[c->cu], (const double*)c->K, (const double*)c->P[c->cp], c->lab[c->cl],
+                             c->g, c->h, n, c->dpd, c->st));
+  else
+    LAUNCH(RQ_KC_ENERGY, 16 * interior(c->g),
+           nm_energy<float>((const float*)c->U[c->cu], (const float*)c->K, (const float*)c->P[c->cp], c->lab[c->cl],
+                            c->g, c->h, n, c->dpd, c->st));
+  std::vector<double> pd((size_t)4 * n);
+  CK(cudaMemcpyAsync(pd.data(), c->dpd, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  double T = 0, EK = 0, EE = 0;
+  for (int q = 0; q < n; ++q) {
+    T += pd[q * 4 + 1]; EK += pd[q * 4 + 2]; EE += pd[q * 4 + 3];
+    if (per_domain) {
+      double* d = per_domain + (size_t)q * RQ_DOMAIN_LEN;
+      d[RQ_D_NORM] = pd[q * 4]; d[RQ_D_T] = pd[q * 4 + 1]; d[RQ_D_EK] = pd[q * 4 + 2]; d[RQ_D_EE] = pd[q * 4 + 3];
+      const double nr = pd[q * 4] != 0 ? pd[q * 4] : 1.0;
+      d[RQ_D_EIG] = (pd[q * 4 + 1] + 2 * pd[q * 4 + 3] + pd[q * 4 + 2]) / nr;
+    }
+  }
+  out[RQ_E_T] = T; out[RQ_E_EK] = EK; out[RQ_E_EE] = EE;
+  return RQ_OK;
+}
+
+int nm_forces(rq_ctx* c, int method, double* F) {
+  if (method != RQ_FORCE_HF && method != RQ_FORCE_ADJOINT) return RQ_ENOTSUP;
+  const int n = c->n_atoms;
+  CK(cudaMemsetAsync(c->dF, 0, sizeof(double) * 3 * n, c->st));
+  if (c->fp64)
+    LAUNCH(RQ_KC_FORCES, 8 * interior(c->g),
+           nm_force<double>((const double*)c->U[c->cu], c->atoms_nm, n, c->g, c->h, c->sigma, c->dF, c->st));
+  else
+    LAUNCH(RQ_KC_FORCES, 4 * interior(c->g),
+           nm_force<float>((const float*)c->U[c->cu], c->atoms_nm, n, c->g, c->h, c->sigma, c->dF, c->st));
+  CK(cudaMemcpyAsync(F, c->dF, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return RQ_OK;
+}

@@ -55,6 +55,8 @@ struct rq_ctx {
   float* scratch_atoms5 = nullptr;  // per-call atom table for force variants
   void* atoms_mj = nullptr;   // molecule.js records (u32 positions)
   double* atoms_nm = nullptr; // new flavour: x,y,z (bohr), Z_nuc per atom
+  void* seeds = nullptr;      // new flavour: float4 (x, y, z, entry) per domain seed
+  void* scale64 = nullptr;    // new flavour: per-domain scale (T)
   float* Zdom = nullptr;      // domain charge per label (f32)
   double* Zdom64 = nullptr;
 
@@ -71,10 +73,11 @@ struct rq_ctx {
   int frame = 0;
   std::string last_error;
 
-  // CUDA graphs of one schedule period, keyed by buffer parity (cu, cp, cl)
-  cudaGraphExec_t graph[8] = {};
-  int graph_post[8] = {};
-  long long graph_launches[8] = {};
+  // CUDA graphs of one schedule period, keyed by buffer parity (cu, cp, cl) and whether the
+  // label updates of the period are active (label_until)
+  cudaGraphExec_t graph[16] = {};
+  int graph_post[16] = {};
+  long long graph_launches[16] = {};
 
   // launch accounting and the optional per-kernel profile
   long long launches = 0;

@@ -55,6 +55,39 @@ cudaError_t launch_mj_energy(const float* U, const float* Pv, const float* K, co
 cudaError_t launch_mj_gradp(const float* P, const MjAtom* atoms, int nAt, const Geo& g, float inv_h, int R, double* F,
                             cudaStream_t st);
 cudaError_t launch_fill(float* f, float v, long long n, cudaStream_t st);
+
+// ---- new flavour (nm_kernels.cu), T = float (mixed) or double (FP64) --------------------
+template <typename T>
+cudaError_t nm_potential(T* K, const double* at, int nAt, const Geo& g, double h, double sigma, cudaStream_t st);
+template <typename T>
+cudaError_t nm_init(T* U, int* label, const float4* seeds, int nSeed, const Geo& g, float h, cudaStream_t st);
+template <typename T>
+cudaError_t nm_update(const T* U, T* Unew, const T* K, const T* P, const int* label, const Geo& g, T half_dv, T dt,
+                      double h3, int nDom, double* norms, cudaStream_t st);
+template <typename T>
+cudaError_t nm_normalize(T* U, const int* label, const double* norms, const double* Zdom, int nDom, T* scale, int* err,
+                         const Geo& g, cudaStream_t st);
+template <typename T>
+cudaError_t nm_norms(const T* U, const int* label, const Geo& g, double h3, int nDom, double* norms, cudaStream_t st);
+template <typename T>
+cudaError_t nm_rbgs(T* P, const T* f, bool fine, const Geo& g, double h2, int color, cudaStream_t st);
+template <typename T>
+cudaError_t nm_residual(const T* P, const T* f, bool fine, T* r, const Geo& g, double inv_h2, cudaStream_t st);
+template <typename T>
+cudaError_t nm_restrict(const T* fine, T* coarse, const Geo& g, const Geo& gc, cudaStream_t st);
+template <typename T>
+cudaError_t nm_prolong(const T* Ec, T* P, const Geo& g, const Geo& gc, cudaStream_t st);
+template <typename T>
+cudaError_t nm_coarsest(T* P, const T* f, const Geo& g, double h2, int sweeps, cudaStream_t st);
+template <typename T>
+cudaError_t nm_energy(const T* U, const T* K, const T* P, const int* label, const Geo& g, double h, int nDom, double* pd,
+                      cudaStream_t st);
+template <typename T>
+cudaError_t nm_evolve(const int* labIn, int* labOut, const T* U, float* W, const Geo& g, double dt_w, double curvReg,
+                      cudaStream_t st);
+template <typename T>
+cudaError_t nm_force(const T* U, const double* at, int nAt, const Geo& g, double h, double sigma, double* F,
+                     cudaStream_t st);
 cudaError_t launch_unpack_labels(const int* in, int* out, long long n, cudaStream_t st);
 
 }  // namespace rq
