@@ -220,6 +220,19 @@ RQ_API int rq_kernel_recompute_k_sp(float* K, const float* atoms5, int32_t n_ato
  * normalizeU (:210-225) with scale sqrt(Z/n).  norms_out (n doubles, device) may be NULL. */
 RQ_API int rq_kernel_normalize_sp(float* U, const int32_t* label, const float* Zeff, int32_t n_atoms, int32_t S, float h3,
                            double* norms_out, void* stream);
+/* No counterpart in the reference.  The same normalisation as rq_kernel_normalize_sp, for
+ * callers that cannot allocate device memory (for example a host framework whose own caching
+ * allocator owns the GPU memory, or a solver loop that must not allocate once it runs): its
+ * scratch -- the per-domain FP64 sums, the scale table and an error word -- lives in one fixed
+ * device array inside the library, so the call allocates and frees nothing.
+ * Limit: n_atoms <= RQ_NOALLOC_MAX_DOMAINS, otherwise RQ_EINVAL and nothing runs.
+ * The array is shared by every call on a device and keeps the last call's contents (each call
+ * clears what it sums into first); calls that overlap on the GPU race on it, so order them on
+ * one stream.  The first call on each device looks up the array's device address; make it
+ * before starting any stream capture on that device.  The per-domain sums are not returned. */
+#define RQ_NOALLOC_MAX_DOMAINS 16384
+RQ_API int rq_kernel_normalize_sp_noalloc(float* U, const int32_t* label, const float* Zeff, int32_t n_atoms, int32_t S,
+                                          float h3, void* stream);
 /* Per-label FP64 (norm, T, V_eK, V_ee) of cloud/solver.py:246-256 into per_domain (n x 4, device). */
 RQ_API int rq_kernel_energy_sp(const float* U, const float* K, const float* P, const int32_t* label, int32_t n_atoms,
                         int32_t S, float h, float h3, double* per_domain, void* stream);

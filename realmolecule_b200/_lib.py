@@ -19,6 +19,7 @@ PREC_MIXED, PREC_FP64 = 0, 1
 FORCE_HF, FORCE_GRADP, FORCE_ADJOINT = 0, 1, 2
 E_TOTAL, E_T, E_EK, E_EE, E_KK, E_DIPX, E_DIPY, E_DIPZ = range(8)
 ENERGY_LEN, DOMAIN_LEN = 8, 5
+NOALLOC_MAX_DOMAINS = 16384
 
 
 class RqError(RuntimeError):
@@ -90,6 +91,7 @@ SIGNATURES = {
     "rq_kernel_init_sp": (C.c_int, [_P, _P, _P, _P, _P, _I, _I, _F, _F, _V]),
     "rq_kernel_recompute_k_sp": (C.c_int, [_P, _P, _I, _I, _F, _F, _V]),
     "rq_kernel_normalize_sp": (C.c_int, [_P, _P, _P, _I, _I, _F, _P, _V]),
+    "rq_kernel_normalize_sp_noalloc": (C.c_int, [_P, _P, _P, _I, _I, _F, _V]),
     "rq_kernel_energy_sp": (C.c_int, [_P, _P, _P, _P, _I, _I, _F, _F, _P, _V]),
     "rq_kernel_forces_hf_sp": (C.c_int, [_P, _P, _I, _I, _F, _F, _F, _P, _V]),
 }
