@@ -165,6 +165,10 @@ RQ_API const char* rq_status_string(int status);
 RQ_API int rq_initialize(rq_ctx* ctx);
 /* Move nuclei and rebuild K (cloud/solver.py:538-548, molecule.js:4563-4582 without relabel). */
 RQ_API int rq_set_atoms(rq_ctx* ctx, const rq_atom* atoms, int32_t n_atoms);
+/* External potential v (host array of S^3 doubles, Ha) added to the nuclear potential K of the
+ * new flavour: the update uses K + v and E_eK = -h^3 sum (K + v) rho.  NULL removes it.  No
+ * reference counterpart: the handle through which dE/dv = -h^3 rho is exposed to autograd. */
+RQ_API int rq_set_external_potential(rq_ctx* ctx, const double* v);
 /* Copy a full state in / out (host arrays of S^3 elements; any pointer may be NULL to skip).
  * Labels must lie in [0, n_atoms).  Replaces window.restartWithPositions re-uploads
  * (molecule.js:2127-2147) and direct access to RealQMSolver.U / .label. */

@@ -72,6 +72,7 @@ SIGNATURES = {
     "rq_status_string": (C.c_char_p, [C.c_int]),
     "rq_initialize": (C.c_int, [_V]),
     "rq_set_atoms": (C.c_int, [_V, C.POINTER(Atom), _I]),
+    "rq_set_external_potential": (C.c_int, [_V, _P]),
     "rq_upload_state": (C.c_int, [_V, _P, _P, _P, _P]),
     "rq_download_state": (C.c_int, [_V, _P, _P, _P, _P]),
     "rq_upload_state_f64": (C.c_int, [_V, _P, _P]),

@@ -126,6 +126,11 @@ class Context:
         self._chk(self.lib.rq_set_atoms(self.ctx, arr, len(arr)), "rq_set_atoms")
         self._atoms = arr
 
+    def set_external_potential(self, v):
+        """Add an external potential v (S^3 values, Ha) to K (new flavour); None removes it."""
+        arr = None if v is None else np.ascontiguousarray(np.asarray(v, np.float64).reshape(-1))
+        self._chk(self.lib.rq_set_external_potential(self.ctx, _ptr(arr)), "rq_set_external_potential")
+
     def solve(self, tol_dE: float, max_steps: int, check_interval: int = 100):
         taken = C.c_int32()
         e = C.c_double()

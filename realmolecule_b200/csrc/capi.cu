@@ -124,7 +124,7 @@ static void free_ctx(rq_ctx* c) {
     if (gx) cudaGraphExecDestroy(gx);
   void* ptrs[] = {c->U[0], c->U[1], c->P[0], c->P[1], c->K, c->W, c->bestU, c->rho, c->Pother, c->resid, c->lab[0], c->lab[1],
                   c->Ec[0], c->Ec[1], c->fc, c->atoms5, c->scratch_atoms5, c->atoms_mj, c->atoms_nm, c->Zdom, c->Zdom64, c->dnorm,
-                  c->dpd, c->dF, c->dsum, c->unorm, c->scale, c->err, c->seeds, c->scale64};
+                  c->dpd, c->dF, c->dsum, c->unorm, c->scale, c->err, c->seeds, c->scale64, c->Kext};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& L : c->mg) {
@@ -533,6 +533,15 @@ extern "C" int rq_set_atoms(rq_ctx* c, const rq_atom* atoms, int32_t n) {
       rc = nm_set_atoms(c);
       break;
   }
+  if (rc != RQ_OK) return rc;
+  CK(cudaStreamSynchronize(c->st));
+  return RQ_OK;
+}
+
+extern "C" int rq_set_external_potential(rq_ctx* c, const double* v) {
+  if (!c) return RQ_EINVAL;
+  if (c->cfg.flavor != RQ_FLAVOR_NEW) return rq_fail(c, RQ_ENOTSUP, "external potential: new flavour only");
+  int rc = nm_set_external(c, v);
   if (rc != RQ_OK) return rc;
   CK(cudaStreamSynchronize(c->st));
   return RQ_OK;

@@ -142,7 +142,27 @@ template <typename T>
 static int nm_potential_t(rq_ctx* c) {
   LAUNCH(RQ_KC_OTHER, sizeof(T) * c->g.S3,
          nm_potential<T>((T*)c->K, c->atoms_nm, c->n_atoms, c->g, c->h, c->sigma, c->st));
+  if (c->Kext) LAUNCH(RQ_KC_OTHER, 3.0 * sizeof(T) * c->g.S3, nm_add<T>((T*)c->K, (const T*)c->Kext, c->g.S3, c->st));
   return RQ_OK;
+}
+
+int nm_set_external(rq_ctx* c, const double* v) {
+  const size_t n = (size_t)c->g.S3;
+  if (!v) {
+    if (c->Kext) { cudaFree(c->Kext); c->Kext = nullptr; }
+  } else {
+    if (!c->Kext && cudaMalloc(&c->Kext, n * esize(c)) != cudaSuccess)
+      return rq_cuda(c, cudaErrorMemoryAllocation, "external potential");
+    if (c->fp64) {
+      CK(cudaMemcpyAsync(c->Kext, v, n * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    } else {
+      std::vector<float> f(n);
+      for (size_t q = 0; q < n; ++q) f[q] = (float)v[q];
+      CK(cudaMemcpyAsync(c->Kext, f.data(), n * sizeof(float), cudaMemcpyHostToDevice, c->st));
+      CK(cudaStreamSynchronize(c->st));
+    }
+  }
+  return nm_set_atoms(c);  // K = K_nuclei (+ v)
 }
 
 int nm_set_atoms(rq_ctx* c) { return c->fp64 ? nm_potential_t<double>(c) : nm_potential_t<float>(c); }

@@ -451,6 +451,12 @@ __global__ void __launch_bounds__(256) k_nm_force(const T* __restrict__ U, const
   }
 }
 
+template <typename T>
+__global__ void k_nm_add(T* __restrict__ K, const T* __restrict__ v, long long n) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    K[q] = Ar<T>::add(K[q], v[q]);
+}
+
 // ======================================================================================
 // host launchers (T = float or double)
 // ======================================================================================
@@ -558,7 +564,16 @@ cudaError_t nm_force(const T* U, const double* at, int nAt, const Geo& g, double
   return cudaGetLastError();
 }
 
+template <typename T>
+cudaError_t nm_add(T* K, const T* v, long long n, cudaStream_t st) {
+  k_nm_add<T><<<148 * 8, 256, 0, st>>>(K, v, n);
+  return cudaGetLastError();
+}
+
 #define RQ_NM_INSTANTIATE(T)                                                                                          \
+  template cudaError_t nm_add<T>(T*, const T*, long long, cudaStream_t);                                           \
+  RQ_NM_INSTANTIATE2(T)
+#define RQ_NM_INSTANTIATE2(T)                                                                                          \
   template cudaError_t nm_potential<T>(T*, const double*, int, const Geo&, double, double, cudaStream_t);           \
   template cudaError_t nm_init<T>(T*, int*, const float4*, int, const Geo&, float, cudaStream_t);                   \
   template cudaError_t nm_update<T>(const T*, T*, const T*, const T*, const int*, const Geo&, T, T, double, int,     \

@@ -57,6 +57,7 @@ struct rq_ctx {
   double* atoms_nm = nullptr; // new flavour: x,y,z (bohr), Z_nuc per atom
   void* seeds = nullptr;      // new flavour: float4 (x, y, z, entry) per domain seed
   void* scale64 = nullptr;    // new flavour: per-domain scale (T)
+  void* Kext = nullptr;       // new flavour: external potential added to K (T), or null
   float* Zdom = nullptr;      // domain charge per label (f32)
   double* Zdom64 = nullptr;
 

@@ -25,4 +25,5 @@ int nm_step_one(rq_ctx* c, int s);
 int nm_energy(rq_ctx* c, double* out, double* per_domain);
 int nm_forces(rq_ctx* c, int method, double* F);
 int nm_set_atoms(rq_ctx* c);
+int nm_set_external(rq_ctx* c, const double* v);
 void nm_nuclear_terms(rq_ctx* c, double* E, double* F);

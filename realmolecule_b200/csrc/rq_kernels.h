@@ -86,6 +86,8 @@ template <typename T>
 cudaError_t nm_evolve(const int* labIn, int* labOut, const T* U, float* W, const Geo& g, double dt_w, double curvReg,
                       cudaStream_t st);
 template <typename T>
+cudaError_t nm_add(T* K, const T* v, long long n, cudaStream_t st);
+template <typename T>
 cudaError_t nm_force(const T* U, const double* at, int nAt, const Geo& g, double h, double sigma, double* F,
                      cudaStream_t st);
 cudaError_t launch_unpack_labels(const int* in, int* out, long long n, cudaStream_t st);
