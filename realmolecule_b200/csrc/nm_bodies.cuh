@@ -1,0 +1,411 @@
+// nm_bodies.cuh -- device bodies of the new flavour's kernels.
+//
+// Each body takes its block coordinates explicitly, so the same code runs in two shapes:
+// one grid per instance (nm_kernels.cu: the coordinates are blockIdx) and one launch over the
+// (instance, tile) work list of a batch of uneven grids (batch_kernels.cu: the coordinates come
+// from the work item).  Templated on the field type T (float: mixed path, double: FP64 path);
+// point-wise arithmetic is explicitly rounded in the FP64 oracle's operation order
+// (oracle/rq_oracle.c, orc_nm_*).
+#pragma once
+#include "rq_internal.cuh"
+
+namespace rq {
+
+template <typename T> struct Ar;
+template <> struct Ar<float> {
+  static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+  static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+  static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+  static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+};
+template <> struct Ar<double> {
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+};
+
+constexpr int kNmFlatChunk = 16;     // points per thread of the flat (all S^3) bodies
+constexpr int kNmForceTile = 512;    // interior points staged per force tile
+
+// ---------------------------------------------------------------------------------------
+// K = sum Z erf(r/(sqrt2 sigma))/r in FP64 (K(0) = Z sqrt(2/pi)/sigma); boundary planes 0.
+// One block of 256 threads covers points [blk*256, blk*256+256); sa: 512 doubles of smem.
+// ---------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void nm_potential_body(T* __restrict__ K, const double* __restrict__ at, int nAt,
+                                                  const Geo& g, double h, double sigma, long long blk, double* sa) {
+  const long long id = blk * blockDim.x + threadIdx.x;
+  const bool inside = id < g.S3;
+  int i = 0, j = 0, k = 0;
+  if (inside) { i = (int)(id / g.S2); j = (int)((id / g.S) % g.S); k = (int)(id % g.S); }
+  const bool interior = inside && i >= 1 && i < g.NN && j >= 1 && j < g.NN && k >= 1 && k < g.NN;
+  const double x = i * h, y = j * h, z = k * h;
+  const double inv = 1.0 / (1.4142135623730951 * sigma), c0 = 0.7978845608028654 / sigma;  // sqrt(2/pi)
+  double v = 0.0;
+  for (int base = 0; base < nAt; base += 128) {
+    const int cnt = min(128, nAt - base);
+    __syncthreads();
+    for (int q = threadIdx.x; q < cnt * 4; q += blockDim.x) sa[q] = at[base * 4 + q];
+    __syncthreads();
+    if (!interior) continue;
+    for (int m = 0; m < cnt; ++m) {
+      const double Z = sa[m * 4 + 3];
+      if (Z <= 0.0) continue;
+      const double dx = x - sa[m * 4 + 0], dy = y - sa[m * 4 + 1], dz = z - sa[m * 4 + 2];
+      const double r = sqrt(dx * dx + dy * dy + dz * dz);
+      v += (r < 1e-12) ? Z * c0 : Z * erf(r * inv) / r;
+    }
+  }
+  if (inside) K[id] = interior ? (T)v : T(0);
+}
+
+// initial state: nearest domain seed (f32 squared distances, first wins ties), psi = exp(-d)
+template <typename T>
+__device__ __forceinline__ void nm_init_body(T* __restrict__ U, int* __restrict__ label,
+                                             const float4* __restrict__ seeds, int nSeed, const Geo& g, float h,
+                                             long long blk, float4* ss) {
+  const long long id = blk * blockDim.x + threadIdx.x;
+  const bool inside = id < g.S3;
+  int i = 0, j = 0, k = 0;
+  if (inside) { i = (int)(id / g.S2); j = (int)((id / g.S) % g.S); k = (int)(id % g.S); }
+  const float x = F_MUL((float)i, h), y = F_MUL((float)j, h), z = F_MUL((float)k, h);
+  float best = 3.4e38f;
+  int bl = 0;
+  for (int base = 0; base < nSeed; base += 256) {
+    const int cnt = min(256, nSeed - base);
+    __syncthreads();
+    if (threadIdx.x < cnt) ss[threadIdx.x] = seeds[base + threadIdx.x];
+    __syncthreads();
+    for (int m = 0; m < cnt; ++m) {
+      const float4 s = ss[m];
+      const float dx = F_SUB(x, s.x), dy = F_SUB(y, s.y), dz = F_SUB(z, s.z);
+      const float d2 = F_ADD(F_ADD(F_MUL(dx, dx), F_MUL(dy, dy)), F_MUL(dz, dz));
+      if (d2 < best) { best = d2; bl = __float_as_int(s.w); }
+    }
+  }
+  if (!inside) return;
+  const bool interior = i >= 1 && i < g.NN && j >= 1 && j < g.NN && k >= 1 && k < g.NN;
+  label[id] = bl;
+  U[id] = interior ? (T)exp(-sqrt((double)best)) : T(0);
+}
+
+// ITP update (same-label Neumann Laplacian) on the march tile (bx, by, bz); with ACC the FP64
+// norm of the new psi per label goes through the block table (caller inits and flushes it).
+template <typename T, bool ACC>
+__device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __restrict__ Unew, const T* __restrict__ K,
+                                               const T* __restrict__ P, const int* __restrict__ label, const Geo& g,
+                                               T half_dv, T dt, double h3, int nDom, double* __restrict__ norms,
+                                               DomTable<1, 128>& tab, int bx, int by, int bz) {
+  using A = Ar<T>;
+  RunSum<1> rs;
+  rs.reset();
+  const int k = 1 + bx * kThreadsK + threadIdx.x;
+  const int j = 1 + by * kThreadsJ + threadIdx.y;
+  const int i0 = 1 + bz * kMarch;
+  if (k < g.NN && j < g.NN && i0 < g.NN) {
+    const int iend = min(i0 + kMarch, g.NN);
+    const long long S = g.S, S2 = g.S2;
+    long long id = (long long)i0 * S2 + j * S + k;
+    T u_m = U[id - S2], u_c = U[id];
+    int l_m = label[id - S2], l_c = label[id];
+    for (int i = i0; i < iend; ++i, id += S2) {
+      const T u_p = U[id + S2];
+      const int l_p = label[id + S2];
+      const T a = (l_p == l_c) ? u_p : u_c;
+      const T b = (l_m == l_c) ? u_m : u_c;
+      const T c = (label[id + S] == l_c) ? U[id + S] : u_c;
+      const T d = (label[id - S] == l_c) ? U[id - S] : u_c;
+      const T e = (label[id + 1] == l_c) ? U[id + 1] : u_c;
+      const T f = (label[id - 1] == l_c) ? U[id - 1] : u_c;
+      const T lap = A::sub(A::add(A::add(A::add(A::add(A::add(a, b), c), d), e), f), A::mul(T(6), u_c));
+      const T out = A::add(A::add(u_c, A::mul(half_dv, lap)), A::mul(A::mul(dt, A::sub(K[id], A::mul(T(2), P[id]))), u_c));
+      Unew[id] = out;
+      if (ACC) {
+        const double r = (double)out * (double)out * h3;
+        rs.add(min(max(l_c, 0), nDom - 1), &r, tab, norms);
+      }
+      u_m = u_c; u_c = u_p; l_m = l_c; l_c = l_p;
+    }
+  }
+  if (ACC) rs.finish(tab, norms);
+}
+
+// U *= scale[label] for labels in [0, nDom) over kNmFlatChunk*256 points from blk
+template <typename T>
+__device__ __forceinline__ void nm_apply_scale_body(T* __restrict__ U, const int* __restrict__ label,
+                                                    const T* __restrict__ scale, long long S3, int nDom, long long blk) {
+  const long long base = blk * blockDim.x * kNmFlatChunk;
+  for (int q = 0; q < kNmFlatChunk; ++q) {
+    const long long id = base + (long long)q * blockDim.x + threadIdx.x;
+    if (id >= S3) break;
+    const int l = label[id];
+    if (l < 0 || l >= nDom) continue;
+    U[id] = Ar<T>::mul(U[id], scale[l]);
+  }
+}
+
+// FP64 per-label psi^2 h^3 over kNmFlatChunk*256 points from blk (label clipped to [0, nDom))
+template <typename T>
+__device__ __forceinline__ void nm_norms_body(const T* __restrict__ U, const int* __restrict__ label, long long S3,
+                                              double h3, int nDom, double* __restrict__ norms, DomTable<1, 128>& tab,
+                                              long long blk) {
+  RunSum<1> rs;
+  rs.reset();
+  const long long base = blk * blockDim.x * kNmFlatChunk;
+  for (int q = 0; q < kNmFlatChunk; ++q) {
+    const long long id = base + (long long)q * blockDim.x + threadIdx.x;
+    if (id >= S3) break;
+    const double u = (double)U[id];
+    const double r = u * u * h3;
+    rs.add(min(max(label[id], 0), nDom - 1), &r, tab, norms);
+  }
+  rs.finish(tab, norms);
+}
+
+// fine-level right-hand side f = (2 pi psi) psi formed from psi on the fly
+template <typename T, bool FINE>
+__device__ __forceinline__ T rhs_at(const T* __restrict__ f, long long id) {
+  if (FINE) {
+    const T u = f[id];
+    return Ar<T>::mul(Ar<T>::mul((T)6.283185307179586, u), u);
+  }
+  return f[id];
+}
+
+// one colour of a red-black sweep for A P = f, A P = (6P - sum_6 P)/h^2; block (32, 8): each
+// thread owns the pair (k0, k0+1) of plane i = 1+bz, one of which has the colour
+template <typename T, bool FINE>
+__device__ __forceinline__ void nm_rbgs_body(T* __restrict__ P, const T* __restrict__ f, const Geo& g, T h2, int color,
+                                             int bx, int by, int bz) {
+  using A = Ar<T>;
+  const int k0 = 1 + bx * 64 + 2 * threadIdx.x;
+  const int j = 1 + by * blockDim.y + threadIdx.y;
+  const int i = 1 + bz;
+  if (j >= g.NN || i >= g.NN) return;
+  const int k = k0 + ((i + j + k0 + color) & 1);
+  if (k >= g.NN) return;
+  const long long S = g.S, S2 = g.S2;
+  const long long id = (long long)i * S2 + (long long)j * S + k;
+  const T s = A::add(A::add(A::add(A::add(A::add(P[id + S2], P[id - S2]), P[id + S]), P[id - S]), P[id + 1]), P[id - 1]);
+  P[id] = A::div(A::add(s, A::mul(h2, rhs_at<T, FINE>(f, id))), T(6));
+}
+
+template <typename T, bool FINE>
+__device__ __forceinline__ void nm_residual_body(const T* __restrict__ P, const T* __restrict__ f, T* __restrict__ r,
+                                                 const Geo& g, T inv_h2, int bx, int by, int bz) {
+  using A = Ar<T>;
+  const int k = 1 + bx * kThreadsK + threadIdx.x;
+  const int j = 1 + by * kThreadsJ + threadIdx.y;
+  const int i0 = 1 + bz * kMarch;
+  if (k >= g.NN || j >= g.NN || i0 >= g.NN) return;
+  const int iend = min(i0 + kMarch, g.NN);
+  const long long S = g.S, S2 = g.S2;
+  for (int i = i0; i < iend; ++i) {
+    const long long id = (long long)i * S2 + (long long)j * S + k;
+    const T s = A::add(A::add(A::add(A::add(A::add(P[id + S2], P[id - S2]), P[id + S]), P[id - S]), P[id + 1]), P[id - 1]);
+    r[id] = A::add(rhs_at<T, FINE>(f, id), A::mul(A::sub(s, A::mul(T(6), P[id])), inv_h2));
+  }
+}
+
+// full weighting (1/64)(8,4,2,1) at coarse interior point number q; loop order a, b, c
+template <typename T>
+__device__ __forceinline__ void nm_restrict_body(const T* __restrict__ fine, T* __restrict__ coarse, const Geo& g,
+                                                 const Geo& gc, long long q) {
+  using A = Ar<T>;
+  const int n = gc.NN - 1;
+  if (q >= (long long)n * n * n) return;
+  const int K2 = 1 + (int)(q % n), J = 1 + (int)((q / n) % n), I = 1 + (int)(q / ((long long)n * n));
+  T v = T(0);
+  for (int a = -1; a <= 1; ++a)
+    for (int b = -1; b <= 1; ++b)
+      for (int c = -1; c <= 1; ++c) {
+        const T w = (T)((a == 0 ? 2 : 1) * (b == 0 ? 2 : 1) * (c == 0 ? 2 : 1));
+        v = A::add(v, A::mul(w, fine[(long long)(2 * I + a) * g.S2 + (long long)(2 * J + b) * g.S + (2 * K2 + c)]));
+      }
+  coarse[(long long)I * gc.S2 + (long long)J * gc.S + K2] = A::div(v, T(64));
+}
+
+// trilinear prolongation of the coarse correction, added on the march tile (bx, by, bz)
+template <typename T>
+__device__ __forceinline__ void nm_prolong_body(const T* __restrict__ Ec, T* __restrict__ P, const Geo& g,
+                                                const Geo& gc, int bx, int by, int bz) {
+  using A = Ar<T>;
+  const int k = 1 + bx * kThreadsK + threadIdx.x;
+  const int j = 1 + by * kThreadsJ + threadIdx.y;
+  const int i0 = 1 + bz * kMarch;
+  if (k >= g.NN || j >= g.NN || i0 >= g.NN) return;
+  const int iend = min(i0 + kMarch, g.NN);
+  for (int i = i0; i < iend; ++i) {
+    const int ci = i >> 1, cj = j >> 1, ck = k >> 1, oi = i & 1, oj = j & 1, ok = k & 1;
+    T v = T(0);
+    for (int a = 0; a <= oi; ++a)
+      for (int b = 0; b <= oj; ++b)
+        for (int c = 0; c <= ok; ++c) v = A::add(v, Ec[(long long)(ci + a) * gc.S2 + (long long)(cj + b) * gc.S + (ck + c)]);
+    v = A::div(v, (T)((1 + oi) * (1 + oj) * (1 + ok)));
+    const long long id = (long long)i * g.S2 + (long long)j * g.S + k;
+    P[id] = A::add(P[id], v);
+  }
+}
+
+// coarsest level: `sweeps` red-black sweeps in FP64 by one block; sm: 2*S^3 doubles of smem
+template <typename T>
+__device__ __forceinline__ void nm_coarsest_body(T* __restrict__ P, const T* __restrict__ f, const Geo& g, double h2,
+                                                 int sweeps, double* sm) {
+  double* sP = sm;
+  double* sf = sm + g.S3;
+  for (long long q = threadIdx.x; q < g.S3; q += blockDim.x) { sP[q] = (double)P[q]; sf[q] = (double)f[q]; }
+  __syncthreads();
+  const int n = g.NN - 1;
+  const long long nint = (long long)n * n * n;
+  for (int s = 0; s < sweeps; ++s)
+    for (int color = 0; color < 2; ++color) {
+      for (long long q = threadIdx.x; q < nint; q += blockDim.x) {
+        const int k = 1 + (int)(q % n), j = 1 + (int)((q / n) % n), i = 1 + (int)(q / ((long long)n * n));
+        if (((i + j + k) & 1) != color) continue;
+        const long long id = (long long)i * g.S2 + (long long)j * g.S + k;
+        const double sum = __dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(sP[id + g.S2], sP[id - g.S2]), sP[id + g.S]),
+                                                        sP[id - g.S]), sP[id + 1]), sP[id - 1]);
+        sP[id] = __ddiv_rn(__dadd_rn(sum, __dmul_rn(h2, sf[id])), 6.0);
+      }
+      __syncthreads();
+    }
+  for (long long q = threadIdx.x; q < g.S3; q += blockDim.x) P[q] = (T)sP[q];
+}
+
+// per-domain (norm, T, V_eK, V_ee) on the march tile; T counts every same-label edge with an
+// interior end point once (forward edges + the edge to the Dirichlet face on the first layer)
+template <typename T>
+__device__ __forceinline__ void nm_energy_body(const T* __restrict__ U, const T* __restrict__ K, const T* __restrict__ P,
+                                               const int* __restrict__ label, const Geo& g, double h, int nDom,
+                                               double* __restrict__ pd, DomTable<4, 128>& tab, int bx, int by, int bz) {
+  RunSum<4> rs;
+  rs.reset();
+  const double h3 = h * h * h;
+  const int k = 1 + bx * kThreadsK + threadIdx.x;
+  const int j = 1 + by * kThreadsJ + threadIdx.y;
+  const int i0 = 1 + bz * kMarch;
+  if (k < g.NN && j < g.NN && i0 < g.NN) {
+    const int iend = min(i0 + kMarch, g.NN);
+    const long long S = g.S, S2 = g.S2;
+    for (int i = i0; i < iend; ++i) {
+      const long long id = (long long)i * S2 + j * S + k;
+      const double u = U[id], rho = u * u;
+      const int L = label[id];
+      if (L < 0 || L >= nDom) continue;
+      const double a = (label[id + S2] == L) ? (double)U[id + S2] - u : 0.0;
+      const double b = (label[id + S] == L) ? (double)U[id + S] - u : 0.0;
+      const double c = (label[id + 1] == L) ? (double)U[id + 1] - u : 0.0;
+      double t = a * a + b * b + c * c;
+      if (i == 1 && label[id - S2] == L) t += u * u;
+      if (j == 1 && label[id - S] == L) t += u * u;
+      if (k == 1 && label[id - 1] == L) t += u * u;
+      double v[4] = {rho * h3, 0.5 * t * h, -(double)K[id] * rho * h3, (double)P[id] * rho * h3};
+      rs.add(L, v, tab, pd);
+    }
+  }
+  rs.finish(tab, pd);
+}
+
+// level-set label update (molecule.js:426-540 rule) on psi of type T, march tile
+template <typename T>
+__device__ __forceinline__ void nm_evolve_body(const int* __restrict__ labIn, int* __restrict__ labOut,
+                                               const T* __restrict__ U, float* __restrict__ W, const Geo& g, T dt_w,
+                                               T curvReg, int bx, int by, int bz) {
+  using A = Ar<T>;
+  const int k = 1 + bx * kThreadsK + threadIdx.x;
+  const int j = 1 + by * kThreadsJ + threadIdx.y;
+  const int i0 = 1 + bz * kMarch;
+  if (k >= g.NN || j >= g.NN || i0 >= g.NN) return;
+  const int iend = min(i0 + kMarch, g.NN);
+  const long long S = g.S, S2 = g.S2;
+  for (int i = i0; i < iend; ++i) {
+    const long long id = (long long)i * S2 + j * S + k;
+    const int myL = labIn[id];
+    const T uc = U[id];
+    const T myRho = A::mul(uc, uc);
+    const long long nb[6] = {id + S2, id - S2, id + S, id - S, id + 1, id - 1};
+    int bestL = myL;
+    T bestRho = T(0), myCnt = T(0);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      const int l = labIn[nb[q]];
+      if (l == myL) {
+        myCnt = A::add(myCnt, T(1));
+      } else {
+        const T un = U[nb[q]];
+        const T r = A::mul(un, un);
+        if (r > bestRho) { bestRho = r; bestL = l; }
+      }
+    }
+    T w = (T)W[id];
+    if (myCnt >= T(6)) {
+      W[id] = (float)(w > T(1) ? w : T(1));
+      labOut[id] = myL;
+      continue;
+    }
+    const T denom = A::add(myRho, bestRho);
+    const T vel = (denom < (T)1e-20f) ? T(0) : A::div(A::sub(myRho, bestRho), denom);
+    w = A::add(w, A::mul(dt_w, vel));
+    const T curv = A::div(A::sub(myCnt, T(3)), T(3));
+    w = A::add(w, A::mul(curvReg, curv));
+    int newL = myL;
+    if (w < T(0)) { newL = bestL; w = (T)0.1f; }
+    W[id] = (float)w;
+    labOut[id] = newL;
+  }
+}
+
+// Gaussian-nucleus force: tiles t = t0, t0+stride, ... of interior points staged in smem (in
+// the field type), thread = nucleus a of chunk `chunk`; F_a = -h^3 sum rho dK/dr (x-R)/r.
+template <typename T>
+__device__ __forceinline__ void nm_force_body(const T* __restrict__ U, const double* __restrict__ at, int nAt,
+                                              const Geo& g, double h, double sigma, double* __restrict__ F,
+                                              long long t0, long long tstride, int chunk, T* sx, T* sy, T* sz, T* sr) {
+  const int a = chunk * blockDim.x + threadIdx.x;
+  const bool valid = a < nAt && at[a * 4 + 3] > 0.0;
+  const double Z = valid ? at[a * 4 + 3] : 0.0;
+  const double ax = valid ? at[a * 4 + 0] : 0.0, ay = valid ? at[a * 4 + 1] : 0.0, az = valid ? at[a * 4 + 2] : 0.0;
+  const double inv = 1.0 / (1.4142135623730951 * sigma), gs = 0.7978845608028654 / sigma;
+  const double h3 = h * h * h;
+  const long long n1 = g.NN - 1, nInt = n1 * n1 * n1;
+  const long long ntiles = (nInt + kNmForceTile - 1) / kNmForceTile;
+  double fx = 0, fy = 0, fz = 0;
+  for (long long t = t0; t < ntiles; t += tstride) {
+    __syncthreads();
+    for (int q = threadIdx.x; q < kNmForceTile; q += blockDim.x) {
+      const long long v = t * kNmForceTile + q;
+      T rho = T(0), x = T(0), y = T(0), z = T(0);
+      if (v < nInt) {
+        const int i = 1 + (int)(v / (n1 * n1)), j = 1 + (int)((v / n1) % n1), k = 1 + (int)(v % n1);
+        const double u = (double)U[(long long)i * g.S2 + (long long)j * g.S + k];
+        rho = (T)(u * u);
+        x = (T)(i * h); y = (T)(j * h); z = (T)(k * h);
+      }
+      sx[q] = x; sy[q] = y; sz[q] = z; sr[q] = rho;
+    }
+    __syncthreads();
+    if (valid) {
+      double lx = 0, ly = 0, lz = 0;
+      for (int q = 0; q < kNmForceTile; ++q) {
+        const double rho = sr[q];
+        if (rho == 0.0) continue;
+        const double dx = (double)sx[q] - ax, dy = (double)sy[q] - ay, dz = (double)sz[q] - az;
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 < 1e-24) continue;
+        const double r = sqrt(r2);
+        const double dKdr = (r * inv < 6.0) ? Z * (gs * exp(-r2 * inv * inv) / r - erf(r * inv) / r2) : -Z / r2;
+        const double w = -h3 * rho * dKdr / r;
+        lx += w * dx; ly += w * dy; lz += w * dz;
+      }
+      fx += lx; fy += ly; fz += lz;
+    }
+  }
+  if (valid) {
+    atomicAdd(&F[a * 3 + 0], fx);
+    atomicAdd(&F[a * 3 + 1], fy);
+    atomicAdd(&F[a * 3 + 2], fz);
+  }
+}
+
+}  // namespace rq

@@ -68,6 +68,8 @@ template <typename T>
 cudaError_t nm_normalize(T* U, const int* label, const double* norms, const double* Zdom, int nDom, T* scale, int* err,
                          const Geo& g, cudaStream_t st);
 template <typename T>
+cudaError_t nm_norm_scale(const double* norms, const double* Zdom, int nDom, T* scale, int* err, cudaStream_t st);
+template <typename T>
 cudaError_t nm_norms(const T* U, const int* label, const Geo& g, double h3, int nDom, double* norms, cudaStream_t st);
 template <typename T>
 cudaError_t nm_rbgs(T* P, const T* f, bool fine, const Geo& g, double h2, int color, cudaStream_t st);
