@@ -203,6 +203,33 @@ RQ_API int rq_synchronize(rq_ctx* ctx);
 RQ_API int rq_profile_begin(rq_ctx* ctx);
 RQ_API int rq_profile_end(rq_ctx* ctx, rq_profile* out);
 
+/* ---- batches of independent new-flavour instances with uneven grids ----------------------
+ * No single reference call site: the reference runs one molecule per process (cloud/app.py:70-87
+ * loops jobs serially).  A batch steps n_inst instances in lockstep; every kernel of the
+ * schedule is one launch over an (instance, tile) work list, and a schedule period is one CUDA
+ * graph.  cfgs[q] gives each instance's NN and screen (one flavour RQ_FLAVOR_NEW, one precision
+ * and one grid spacing h for the batch; the intervals of cfgs[0] apply to all).  atoms holds the
+ * entries of instance 0, then instance 1, ... (n_atoms[q] each). */
+typedef struct rq_batch rq_batch;
+RQ_API int rq_batch_create(const rq_config* cfgs, const rq_atom* atoms, const int32_t* n_atoms, int32_t n_inst,
+                           rq_batch** out);
+RQ_API void rq_batch_destroy(rq_batch* b);
+RQ_API const char* rq_batch_last_error(const rq_batch* b);
+RQ_API int rq_batch_set_stream(rq_batch* b, void* stream);
+RQ_API int rq_batch_initialize(rq_batch* b);
+RQ_API int rq_batch_step(rq_batch* b, int32_t n_steps);
+/* out: n_inst x RQ_ENERGY_LEN (dipole entries 0).  Synchronises. */
+RQ_API int rq_batch_energy(rq_batch* b, double* out);
+/* Forces on every entry (sum of n_atoms x 3, instance-major), electronic + nuclear repulsion. */
+RQ_API int rq_batch_forces(rq_batch* b, double* F);
+/* Steps until every instance's |dE| between checks is below tol_dE; converged_at[q] = step count
+ * at which instance q converged (-1 if not within max_steps); E_final[q] its last energy. */
+RQ_API int rq_batch_solve(rq_batch* b, double tol_dE, int32_t max_steps, int32_t check_interval, int32_t* converged_at,
+                          double* E_final);
+RQ_API int rq_batch_info(const rq_batch* b, int32_t* n_inst, int64_t* total_points, int64_t* interior_points,
+                         int64_t* kernel_launches);
+RQ_API int rq_batch_synchronize(rq_batch* b);
+
 /* ---- single kernels on caller-owned device memory (zero-copy PyTorch interop) ---------------
  * Pointers are device pointers of S^3 elements; `stream` is a cudaStream_t or NULL.  These run
  * exactly the kernels rq_step uses and exist for kernel-level parity checks and custom drivers. */

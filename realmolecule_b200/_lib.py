@@ -86,6 +86,19 @@ SIGNATURES = {
     "rq_synchronize": (C.c_int, [_V]),
     "rq_profile_begin": (C.c_int, [_V]),
     "rq_profile_end": (C.c_int, [_V, C.POINTER(Profile)]),
+    "rq_batch_create": (C.c_int, [C.POINTER(Config), C.POINTER(Atom), C.POINTER(C.c_int32), _I,
+                                  C.POINTER(C.c_void_p)]),
+    "rq_batch_destroy": (None, [_V]),
+    "rq_batch_last_error": (C.c_char_p, [_V]),
+    "rq_batch_set_stream": (C.c_int, [_V, _V]),
+    "rq_batch_initialize": (C.c_int, [_V]),
+    "rq_batch_step": (C.c_int, [_V, _I]),
+    "rq_batch_energy": (C.c_int, [_V, _P]),
+    "rq_batch_forces": (C.c_int, [_V, _P]),
+    "rq_batch_solve": (C.c_int, [_V, _D, _I, _I, _P, _P]),
+    "rq_batch_info": (C.c_int, [_V, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                C.POINTER(C.c_int64)]),
+    "rq_batch_synchronize": (C.c_int, [_V]),
     "rq_kernel_update_sp": (C.c_int, [_P, _P, _P, _P, _P, _I, _F, _F, _V]),
     "rq_kernel_jacobi_sp": (C.c_int, [_P, _P, _P, _I, _F, _F, _V]),
     "rq_kernel_labels_sp": (C.c_int, [_P, _P, _P, _I, _I, _F, _F, _V]),

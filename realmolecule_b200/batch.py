@@ -1,0 +1,88 @@
+"""Batches of independent new-flavour instances with uneven grids (rq_batch_* of include/rq.h).
+
+All instances step in lockstep; every kernel of the schedule is one launch over an
+(instance, tile) work list, and a schedule period of the whole batch is one CUDA-graph replay.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Sequence
+
+import numpy as np
+
+from . import _lib as L
+from .context import FLAVORS, PRECISIONS, make_atoms
+
+
+class Batch:
+    def __init__(self, instances: Sequence[dict], precision: str = "mixed", **opts):
+        """instances: [{"NN": int, "screen": float, "atoms": [rows]}]; one grid spacing for all."""
+        self.lib = L.load()
+        n = len(instances)
+        cfgs = (L.Config * n)()
+        rows: List[dict] = []
+        counts = (C.c_int32 * n)()
+        for q, inst in enumerate(instances):
+            c = cfgs[q]
+            c.NN, c.screen = int(inst["NN"]), float(inst["screen"])
+            c.flavor, c.precision = FLAVORS["new"], PRECISIONS[precision]
+            for k, v in opts.items():
+                if v is not None:
+                    setattr(c, k, v)
+            rows.extend(dict(r, k=r.get("k", inst["NN"] // 2)) for r in inst["atoms"])
+            counts[q] = len(inst["atoms"])
+        self.counts = list(counts)
+        self._atoms = make_atoms(rows)
+        h = C.c_void_p()
+        L.check(self.lib.rq_batch_create(cfgs, self._atoms, counts, n, C.byref(h)), "rq_batch_create")
+        self.b = h
+        self.n = n
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.lib.rq_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, st, where):
+        if st != L.RQ_OK:
+            raise L.RqError(st, where, self.lib.rq_batch_last_error(self.b).decode())
+
+    def set_stream(self, handle):
+        self._chk(self.lib.rq_batch_set_stream(self.b, handle), "rq_batch_set_stream")
+
+    def initialize(self):
+        self._chk(self.lib.rq_batch_initialize(self.b), "rq_batch_initialize")
+
+    def step(self, n: int = 1):
+        self._chk(self.lib.rq_batch_step(self.b, int(n)), "rq_batch_step")
+
+    def synchronize(self):
+        self._chk(self.lib.rq_batch_synchronize(self.b), "rq_batch_synchronize")
+
+    def energy(self) -> np.ndarray:
+        out = np.zeros((self.n, L.ENERGY_LEN))
+        self._chk(self.lib.rq_batch_energy(self.b, out.ctypes.data), "rq_batch_energy")
+        return out
+
+    def forces(self) -> List[np.ndarray]:
+        F = np.zeros((sum(self.counts), 3))
+        self._chk(self.lib.rq_batch_forces(self.b, F.ctypes.data), "rq_batch_forces")
+        return np.split(F, np.cumsum(self.counts)[:-1])
+
+    def solve(self, tol_dE: float, max_steps: int, check_interval: int = 100):
+        conv = np.zeros(self.n, np.int32)
+        E = np.zeros(self.n)
+        self._chk(self.lib.rq_batch_solve(self.b, float(tol_dE), int(max_steps), int(check_interval),
+                                          conv.ctypes.data, E.ctypes.data), "rq_batch_solve")
+        return conv, E
+
+    def info(self):
+        n, tp, ip, kl = C.c_int32(), C.c_int64(), C.c_int64(), C.c_int64()
+        self._chk(self.lib.rq_batch_info(self.b, C.byref(n), C.byref(tp), C.byref(ip), C.byref(kl)), "rq_batch_info")
+        return {"instances": n.value, "points": tp.value, "interior_points": ip.value, "kernel_launches": kl.value}

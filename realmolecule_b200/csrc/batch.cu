@@ -1,0 +1,809 @@
+// batch.cu -- many new-flavour instances with uneven grids stepped together (rq_batch_*).
+//
+// Every kernel of the schedule is ONE launch over a work list of (instance, tile) items built
+// once at creation: block b reads item b, looks up its instance's geometry and buffers, and
+// runs the same device body as the single-grid kernel (nm_bodies.cuh) on that tile.  Small
+// instances therefore share the GPU instead of each launching a mostly idle grid, and a whole
+// schedule period of the batch is one CUDA-graph replay.  The multigrid V-cycle descends level
+// by level over the instances that still have a coarser level, solves each instance's coarsest
+// level (one block per instance, FP64) when it is reached, and ascends again.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/rq.h"
+#include "nm_bodies.cuh"
+#include "rq_kernels.h"
+
+namespace rq {
+
+constexpr int kMaxLev = 10;
+
+struct BInst {
+  Geo g;
+  double h;
+  void* U[2];
+  void* P[2];
+  void* K;
+  int* lab[2];
+  float* W;
+  int nDom, dom0;  // domains of this instance and their offset in the batch-wide arrays
+  int nlev;
+  Geo lg[kMaxLev];
+  double lh[kMaxLev];
+  void* lP[kMaxLev];
+  void* lf[kMaxLev];
+  void* lr[kMaxLev];
+  const double* at;  // (x, y, z, Z_nuc) per entry of this instance
+  int nAt, at0;      // entries and their offset in the batch-wide force array
+  const float4* seeds;
+  int nSeed;
+};
+
+struct BItem {
+  int inst, bx, by, bz;
+};
+
+// ---------------------------------------------------------------------------------------
+// batched kernels: block b works on items[b]
+// ---------------------------------------------------------------------------------------
+template <typename T, bool ACC>
+__global__ void __launch_bounds__(256) kb_update(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cu,
+                                                 int cp, int cl, T half_dv, T dt, double* __restrict__ norms) {
+  __shared__ DomTable<1, 128> tab;
+  const BItem it = items[blockIdx.x];
+  const BInst& I = ins[it.inst];
+  double* nrm = norms ? norms + I.dom0 : nullptr;
+  if (ACC) {
+    dom_table_init(tab);
+    __syncthreads();
+  }
+  nm_update_body<T, ACC>((const T*)I.U[cu], (T*)I.U[1 - cu], (const T*)I.K, (const T*)I.P[cp], I.lab[cl], I.g, half_dv,
+                         dt, I.h * I.h * I.h, I.nDom, nrm, tab, it.bx, it.by, it.bz);
+  if (ACC) {
+    __syncthreads();
+    dom_table_flush(tab, nrm);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) kb_apply_scale(const BInst* __restrict__ ins, const BItem* __restrict__ items,
+                                                      int cu, int cl, const T* __restrict__ scale) {
+  const BItem it = items[blockIdx.x];
+  const BInst& I = ins[it.inst];
+  nm_apply_scale_body<T>((T*)I.U[cu], I.lab[cl], scale + I.dom0, I.g.S3, I.nDom, it.bx);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) kb_norms(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cu,
+                                                int cl, double* __restrict__ norms) {
+  __shared__ DomTable<1, 128> tab;
+  const BItem it = items[blockIdx.x];
+  const BInst& I = ins[it.inst];
+  dom_table_init(tab);
+  __syncthreads();
+  nm_norms_body<T>((const T*)I.U[cu], I.lab[cl], I.g.S3, I.h * I.h * I.h, I.nDom, norms + I.dom0, tab, it.bx);
+  __syncthreads();
+  dom_table_flush(tab, norms + I.dom0);
+}
+
+template <typename T, bool FINE>
+__global__ void __launch_bounds__(256) kb_rbgs(const BInst* __restrict__ ins, const BItem* __restrict__ items, int lev,
+                                               int cu, int cp, int color) {
+  const BItem it = items[blockIdx.x];
+  const BInst& I = ins[it.inst];
+  T* P = FINE ? (T*)I.P[cp] : (T*)I.lP[lev];
+  const T* f = FINE ? (const T*)I.U[cu] : (const T*)I.lf[lev];
+  nm_rbgs_body<T, FINE>(P, f, I.lg[lev], (T)(I.lh[lev] * I.lh[lev]), color, it.bx, it.by, it.bz);
+}
+
+template <typename T, bool FINE>
+__global__ void __launch_bounds__(256) kb_residual(const BInst* __restrict__ ins, const BItem* __restrict__ items, int lev,
+                                                   int cu, int cp) {
+  const BItem it = items[blockIdx.x];
+  const BInst& I = ins[it.inst];
+  const T* P = FINE ? (const T*)I.P[cp] : (const T*)I.lP[lev];
+  const T* f = FINE ? (const T*)I.U[cu] : (const T*)I.lf[lev];
+  nm_residual_body<T, FINE>(P, f, (T*)I.lr[lev], I.lg[lev], (T)(1.0 / (I.lh[lev] * I.lh[lev])), it.bx, it.by, it.bz);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) kb_restrict(const BInst* __restrict__ ins, const BItem* __restrict__ items,
+                                                   int lev) {
+  const BItem it = items[blockIdx.x];
+  const BInst& I = ins[it.inst];
+  nm_restrict_body<T>((const T*)I.lr[lev], (T*)I.lf[lev + 1], I.lg[lev], I.lg[lev + 1],
+                      (long long)it.bx * blockDim.x + threadIdx.x);
+}
+
+// zero the correction of level lev (flat blocks of 256 points)
+template <typename T>
+__global__ void __launch_bounds__(256) kb_zero(const BInst* __restrict__ ins, const BItem* __restrict__ items, int lev) {
+  const BItem it = items[blockIdx.x];
+  const BInst& I = ins[it.inst];
+  const long long id = (long long)it.bx * blockDim.x + threadIdx.x;
+  if (id < I.lg[lev].S3) ((T*)I.lP[lev])[id] = T(0);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) kb_prolong(const BInst* __restrict__ ins, const BItem* __restrict__ items, int lev,
+                                                  int cp) {
+  const BItem it = items[blockIdx.x];
+  const BInst& I = ins[it.inst];
+  T* P = lev == 0 ? (T*)I.P[cp] : (T*)I.lP[lev];
+  nm_prolong_body<T>((const T*)I.lP[lev + 1], P, I.lg[lev], I.lg[lev + 1], it.bx, it.by, it.bz);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024) kb_coarsest(const BInst* __restrict__ ins, const BItem* __restrict__ items,
+                                                    int lev, int sweeps) {
+  extern __shared__ double sm[];
+  const BItem it = items[blockIdx.x];
+  const BInst& I = ins[it.inst];
+  nm_coarsest_body<T>((T*)I.lP[lev], (const T*)I.lf[lev], I.lg[lev], I.lh[lev] * I.lh[lev], sweeps, sm);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) kb_energy(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cu,
+                                                 int cp, int cl, double* __restrict__ pd) {
+  __shared__ DomTable<4, 128> tab;
+  const BItem it = items[blockIdx.x];
+  const BInst& I = ins[it.inst];
+  dom_table_init(tab);
+  __syncthreads();
+  nm_energy_body<T>((const T*)I.U[cu], (const T*)I.K, (const T*)I.P[cp], I.lab[cl], I.g, I.h, I.nDom, pd + 4 * I.dom0,
+                    tab, it.bx, it.by, it.bz);
+  __syncthreads();
+  dom_table_flush(tab, pd + 4 * I.dom0);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) kb_evolve(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cu,
+                                                 int cl, T dt_w, T curv) {
+  const BItem it = items[blockIdx.x];
+  const BInst& I = ins[it.inst];
+  nm_evolve_body<T>(I.lab[cl], I.lab[1 - cl], (const T*)I.U[cu], I.W, I.g, dt_w, curv, it.bx, it.by, it.bz);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) kb_potential(const BInst* __restrict__ ins, const BItem* __restrict__ items,
+                                                    double sigma_scale) {
+  __shared__ double sa[128 * 4];
+  const BItem it = items[blockIdx.x];
+  const BInst& I = ins[it.inst];
+  nm_potential_body<T>((T*)I.K, I.at, I.nAt, I.g, I.h, sigma_scale > 0 ? sigma_scale : I.h, it.bx, sa);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) kb_init(const BInst* __restrict__ ins, const BItem* __restrict__ items) {
+  __shared__ float4 ss[256];
+  const BItem it = items[blockIdx.x];
+  const BInst& I = ins[it.inst];
+  nm_init_body<T>((T*)I.U[0], I.lab[0], I.seeds, I.nSeed, I.g, (float)I.h, it.bx, ss);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) kb_force(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cu,
+                                                double sigma_scale, double* __restrict__ F) {
+  __shared__ T sx[kNmForceTile], sy[kNmForceTile], sz[kNmForceTile], sr[kNmForceTile];
+  const BItem it = items[blockIdx.x];
+  const BInst& I = ins[it.inst];
+  nm_force_body<T>((const T*)I.U[cu], I.at, I.nAt, I.g, I.h, sigma_scale > 0 ? sigma_scale : I.h, F + 3 * I.at0, it.bx,
+                   it.by, it.bz, sx, sy, sz, sr);
+}
+
+}  // namespace rq
+
+// =========================================================================================
+// host side
+// =========================================================================================
+using namespace rq;
+
+struct rq_batch {
+  int n = 0;
+  bool fp64 = false;
+  rq_config cfg{};
+  double dv = 0.2;
+  std::vector<BInst> hin;         // host copy of the instance table
+  BInst* din = nullptr;           // device copy
+  std::vector<std::vector<rq_atom>> atoms;
+  std::vector<void*> allocs;
+  int D = 0, A = 0;               // total domains / entries
+  double *dnorm = nullptr, *dpd = nullptr, *dF = nullptr, *Zdom = nullptr, *at_all = nullptr;
+  void* scale = nullptr;
+  int* err = nullptr;
+  float4* seeds_all = nullptr;
+  int maxlev = 0;
+  // work lists
+  struct Plan { BItem* d = nullptr; int n = 0; };
+  Plan march[kMaxLev], rbgs[kMaxLev], restr[kMaxLev], zero[kMaxLev], coarse[kMaxLev], prol[kMaxLev];
+  size_t coarse_smem[kMaxLev] = {};
+  Plan flat16, flat1, force;
+  cudaStream_t st = nullptr, own = nullptr;
+  int cu = 0, cp = 0, cl = 0, steps_done = 0;
+  long long launches = 0;
+  cudaGraphExec_t graph[16] = {};
+  int graph_post[16] = {};
+  long long graph_launches[16] = {};
+  std::string last_error;
+};
+
+#define BCK(call)                                                                  \
+  do {                                                                             \
+    cudaError_t _e = (call);                                                       \
+    if (_e != cudaSuccess) {                                                       \
+      b->last_error = std::string(#call) + ": " + cudaGetErrorString(_e);          \
+      return _e == cudaErrorMemoryAllocation ? RQ_ENOMEM : RQ_ECUDA;               \
+    }                                                                              \
+  } while (0)
+
+static int balloc(rq_batch* b, void** p, size_t bytes) {
+  BCK(cudaMalloc(p, bytes));
+  b->allocs.push_back(*p);
+  BCK(cudaMemsetAsync(*p, 0, bytes, b->st));
+  return RQ_OK;
+}
+#define BALLOC(ptr, bytes)                                     \
+  do {                                                         \
+    int _r = balloc(b, (void**)&(ptr), (bytes));               \
+    if (_r != RQ_OK) return _r;                                \
+  } while (0)
+
+static int upload_plan(rq_batch* b, rq_batch::Plan& p, const std::vector<BItem>& v) {
+  p.n = (int)v.size();
+  if (!p.n) return RQ_OK;
+  BALLOC(p.d, sizeof(BItem) * v.size());
+  BCK(cudaMemcpyAsync(p.d, v.data(), sizeof(BItem) * v.size(), cudaMemcpyHostToDevice, b->st));
+  return RQ_OK;
+}
+
+static void march_items(std::vector<BItem>& v, int inst, const Geo& g) {
+  const dim3 gr = march_grid(g);
+  for (unsigned z = 0; z < gr.z; ++z)
+    for (unsigned y = 0; y < gr.y; ++y)
+      for (unsigned x = 0; x < gr.x; ++x) v.push_back({inst, (int)x, (int)y, (int)z});
+}
+
+static int build(rq_batch* b) {
+  const int n = b->n;
+  const size_t es = b->fp64 ? sizeof(double) : sizeof(float);
+  // per-instance buffers and level hierarchy
+  for (int q = 0; q < n; ++q) {
+    BInst& I = b->hin[q];
+    const size_t S3 = (size_t)I.g.S3;
+    for (int k = 0; k < 2; ++k) {
+      BALLOC(I.U[k], S3 * es);
+      BALLOC(I.P[k], S3 * es);
+      BALLOC(I.lab[k], S3 * sizeof(int));
+    }
+    BALLOC(I.K, S3 * es);
+    BALLOC(I.W, S3 * sizeof(float));
+    for (int l = 0; l < I.nlev; ++l) {
+      const size_t s3 = (size_t)I.lg[l].S3;
+      I.lP[l] = I.lf[l] = I.lr[l] = nullptr;
+      if (l > 0) {
+        BALLOC(I.lP[l], s3 * es);
+        BALLOC(I.lf[l], s3 * es);
+      }
+      if (l < I.nlev - 1) BALLOC(I.lr[l], s3 * es);
+    }
+  }
+  // batch-wide per-domain arrays and atom tables
+  BALLOC(b->dnorm, sizeof(double) * b->D);
+  BALLOC(b->dpd, sizeof(double) * 4 * b->D);
+  BALLOC(b->Zdom, sizeof(double) * b->D);
+  BALLOC(b->scale, es * b->D);
+  BALLOC(b->dF, sizeof(double) * 3 * b->A);
+  BALLOC(b->at_all, sizeof(double) * 4 * b->A);
+  BALLOC(b->seeds_all, sizeof(float4) * b->A);
+  BALLOC(b->err, sizeof(int) * 4);
+  std::vector<double> zd(b->D), at(4 * (size_t)b->A);
+  std::vector<float4> seeds;
+  seeds.reserve(b->A);
+  for (int q = 0; q < n; ++q) {
+    BInst& I = b->hin[q];
+    I.at = b->at_all + 4 * (size_t)I.at0;
+    I.seeds = b->seeds_all + seeds.size();
+    int ns = 0;
+    for (int e = 0; e < I.nAt; ++e) {
+      const rq_atom& a = b->atoms[q][e];
+      zd[I.dom0 + e] = a.Z;
+      double* r = &at[4 * ((size_t)I.at0 + e)];
+      r[0] = a.i * I.h; r[1] = a.j * I.h; r[2] = a.k * I.h; r[3] = a.Z_nuc;
+      if (a.Z > 0) {
+        float4 s;
+        s.x = (float)(a.i * I.h); s.y = (float)(a.j * I.h); s.z = (float)(a.k * I.h);
+        int idx = e;
+        std::memcpy(&s.w, &idx, sizeof(int));
+        seeds.push_back(s);
+        ns++;
+      }
+    }
+    I.nSeed = ns;
+  }
+  BCK(cudaMemcpyAsync(b->Zdom, zd.data(), sizeof(double) * b->D, cudaMemcpyHostToDevice, b->st));
+  BCK(cudaMemcpyAsync(b->at_all, at.data(), sizeof(double) * at.size(), cudaMemcpyHostToDevice, b->st));
+  if (!seeds.empty())
+    BCK(cudaMemcpyAsync(b->seeds_all, seeds.data(), sizeof(float4) * seeds.size(), cudaMemcpyHostToDevice, b->st));
+  BALLOC(b->din, sizeof(BInst) * n);
+  BCK(cudaMemcpyAsync(b->din, b->hin.data(), sizeof(BInst) * n, cudaMemcpyHostToDevice, b->st));
+  // work lists
+  for (int l = 0; l < b->maxlev; ++l) {
+    std::vector<BItem> m, r, rs, z, c, p;
+    for (int q = 0; q < n; ++q) {
+      const BInst& I = b->hin[q];
+      if (l >= I.nlev) continue;
+      march_items(m, q, I.lg[l]);
+      if (l == I.nlev - 1) {
+        c.push_back({q, 0, 0, 0});
+        b->coarse_smem[l] = std::max(b->coarse_smem[l], sizeof(double) * 2 * (size_t)I.lg[l].S3);
+        continue;
+      }
+      const int nn = I.lg[l].NN - 1;
+      for (int zz = 0; zz < nn; ++zz)
+        for (int y = 0; y < (nn + 7) / 8; ++y)
+          for (int x = 0; x < (nn + 63) / 64; ++x) r.push_back({q, x, y, zz});
+      const long long nc = (long long)(I.lg[l + 1].NN - 1) * (I.lg[l + 1].NN - 1) * (I.lg[l + 1].NN - 1);
+      for (long long x = 0; x < (nc + 255) / 256; ++x) rs.push_back({q, (int)x, 0, 0});
+      for (long long x = 0; x < (I.lg[l + 1].S3 + 255) / 256; ++x) z.push_back({q, (int)x, 0, 0});
+      march_items(p, q, I.lg[l]);
+    }
+    int rc;
+    if ((rc = upload_plan(b, b->march[l], m)) || (rc = upload_plan(b, b->rbgs[l], r)) ||
+        (rc = upload_plan(b, b->restr[l], rs)) || (rc = upload_plan(b, b->zero[l], z)) ||
+        (rc = upload_plan(b, b->coarse[l], c)) || (rc = upload_plan(b, b->prol[l], p)))
+      return rc;
+  }
+  std::vector<BItem> f16, f1, fo;
+  for (int q = 0; q < n; ++q) {
+    const BInst& I = b->hin[q];
+    for (long long x = 0; x < (I.g.S3 + 256 * kNmFlatChunk - 1) / (256 * kNmFlatChunk); ++x) f16.push_back({q, (int)x, 0, 0});
+    for (long long x = 0; x < (I.g.S3 + 255) / 256; ++x) f1.push_back({q, (int)x, 0, 0});
+    const long long n1 = I.g.NN - 1, ntiles = (n1 * n1 * n1 + kNmForceTile - 1) / kNmForceTile;
+    const int groups = (int)std::min<long long>(ntiles, 32);
+    for (int ch = 0; ch < (I.nAt + 255) / 256; ++ch)
+      for (int t = 0; t < groups; ++t) fo.push_back({q, t, groups, ch});
+  }
+  int rc;
+  if ((rc = upload_plan(b, b->flat16, f16)) || (rc = upload_plan(b, b->flat1, f1)) || (rc = upload_plan(b, b->force, fo)))
+    return rc;
+  size_t smax = 0;
+  for (int l = 0; l < b->maxlev; ++l) smax = std::max(smax, b->coarse_smem[l]);
+  if (smax > 200 * 1024) {
+    b->last_error = "coarsest multigrid level too large for the shared-memory FP64 solve";
+    return RQ_EINVAL;
+  }
+  if (b->fp64)
+    BCK(cudaFuncSetAttribute(kb_coarsest<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
+  else
+    BCK(cudaFuncSetAttribute(kb_coarsest<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
+  BCK(cudaStreamSynchronize(b->st));
+  return RQ_OK;
+}
+
+template <typename T>
+static int b_launch_err(rq_batch* b, const char* what) {
+  cudaError_t e = cudaGetLastError();
+  b->launches++;
+  if (e != cudaSuccess) {
+    b->last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return RQ_ECUDA;
+  }
+  return RQ_OK;
+}
+#define BL(what)                                              \
+  do {                                                        \
+    int _r = b_launch_err<T>(b, what);                        \
+    if (_r != RQ_OK) return _r;                               \
+  } while (0)
+
+template <typename T>
+static int b_vcycle(rq_batch* b) {
+  const int pre = b->cfg.mg_pre, post = b->cfg.mg_post;
+  for (int l = 0; l < b->maxlev; ++l) {
+    if (b->coarse[l].n) {
+      kb_coarsest<T><<<b->coarse[l].n, 1024, b->coarse_smem[l], b->st>>>(b->din, b->coarse[l].d, l,
+                                                                           b->cfg.mg_coarse_sweeps);
+      BL("coarsest");
+    }
+    if (!b->rbgs[l].n) continue;
+    for (int s = 0; s < pre; ++s)
+      for (int color = 0; color < 2; ++color) {
+        if (l == 0)
+          kb_rbgs<T, true><<<b->rbgs[l].n, dim3(32, 8), 0, b->st>>>(b->din, b->rbgs[l].d, l, b->cu, b->cp, color);
+        else
+          kb_rbgs<T, false><<<b->rbgs[l].n, dim3(32, 8), 0, b->st>>>(b->din, b->rbgs[l].d, l, b->cu, b->cp, color);
+        BL("rbgs");
+      }
+    if (l == 0)
+      kb_residual<T, true><<<b->prol[l].n, march_block(), 0, b->st>>>(b->din, b->prol[l].d, l, b->cu, b->cp);
+    else
+      kb_residual<T, false><<<b->prol[l].n, march_block(), 0, b->st>>>(b->din, b->prol[l].d, l, b->cu, b->cp);
+    BL("residual");
+    kb_restrict<T><<<b->restr[l].n, 256, 0, b->st>>>(b->din, b->restr[l].d, l);
+    BL("restrict");
+    kb_zero<T><<<b->zero[l].n, 256, 0, b->st>>>(b->din, b->zero[l].d, l + 1);
+    BL("zero");
+  }
+  for (int l = b->maxlev - 2; l >= 0; --l) {
+    if (!b->rbgs[l].n) continue;
+    kb_prolong<T><<<b->prol[l].n, march_block(), 0, b->st>>>(b->din, b->prol[l].d, l, b->cp);
+    BL("prolong");
+    for (int s = 0; s < post; ++s)
+      for (int color = 0; color < 2; ++color) {
+        if (l == 0)
+          kb_rbgs<T, true><<<b->rbgs[l].n, dim3(32, 8), 0, b->st>>>(b->din, b->rbgs[l].d, l, b->cu, b->cp, color);
+        else
+          kb_rbgs<T, false><<<b->rbgs[l].n, dim3(32, 8), 0, b->st>>>(b->din, b->rbgs[l].d, l, b->cu, b->cp, color);
+        BL("rbgs");
+      }
+  }
+  return RQ_OK;
+}
+
+template <typename T>
+static int b_normalize(rq_batch* b, bool accumulate) {
+  if (accumulate) {
+    BCK(cudaMemsetAsync(b->dnorm, 0, sizeof(double) * b->D, b->st));
+    kb_norms<T><<<b->flat16.n, 256, 0, b->st>>>(b->din, b->flat16.d, b->cu, b->cl, b->dnorm);
+    BL("norms");
+  }
+  BCK(nm_norm_scale<T>(b->dnorm, b->Zdom, b->D, (T*)b->scale, b->err, b->st));
+  b->launches++;
+  kb_apply_scale<T><<<b->flat16.n, 256, 0, b->st>>>(b->din, b->flat16.d, b->cu, b->cl, (const T*)b->scale);
+  BL("apply_scale");
+  return RQ_OK;
+}
+
+template <typename T>
+static int b_step(rq_batch* b, int s) {
+  const rq_config& f = b->cfg;
+  int rc;
+  if (s % f.poisson_interval == 0 && (rc = b_vcycle<T>(b)) != RQ_OK) return rc;
+  const bool norm = s % f.norm_interval == 0;
+  const T hd = (T)(0.5 * b->dv);
+  // dt = dv h^2 differs per instance only through h: every instance of a batch shares h
+  const T dt = (T)(b->dv * b->hin[0].h * b->hin[0].h);
+  if (norm) {
+    BCK(cudaMemsetAsync(b->dnorm, 0, sizeof(double) * b->D, b->st));
+    kb_update<T, true><<<b->march[0].n, march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cp, b->cl, hd, dt,
+                                                                    b->dnorm);
+  } else {
+    kb_update<T, false><<<b->march[0].n, march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cp, b->cl, hd, dt,
+                                                                     nullptr);
+  }
+  BL("update");
+  b->cu ^= 1;
+  if (norm && (rc = b_normalize<T>(b, false)) != RQ_OK) return rc;
+  if (s % f.label_interval == 0 && (f.label_until <= 0 || s <= f.label_until)) {
+    kb_evolve<T><<<b->march[0].n, march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cl,
+                                                              (T)(float)f.boundary_speed, (T)(float)f.curv_reg);
+    BL("evolve");
+    b->cl ^= 1;
+  }
+  return RQ_OK;
+}
+
+template <typename T>
+static int b_initialize(rq_batch* b) {
+  b->cu = b->cp = b->cl = 0;
+  const double sig = b->cfg.sigma;
+  kb_potential<T><<<b->flat1.n, 256, 0, b->st>>>(b->din, b->flat1.d, sig);
+  BL("potential");
+  kb_init<T><<<b->flat1.n, 256, 0, b->st>>>(b->din, b->flat1.d);
+  BL("init");
+  const size_t es = sizeof(T);
+  for (int q = 0; q < b->n; ++q) {
+    const BInst& I = b->hin[q];
+    BCK(cudaMemcpyAsync(I.lab[1], I.lab[0], sizeof(int) * I.g.S3, cudaMemcpyDeviceToDevice, b->st));
+    BCK(cudaMemsetAsync(I.U[1], 0, es * I.g.S3, b->st));
+    for (int k = 0; k < 2; ++k) BCK(cudaMemsetAsync(I.P[k], 0, es * I.g.S3, b->st));
+    BCK(launch_fill(I.W, 1.0f, I.g.S3, b->st));
+  }
+  int rc = b_normalize<T>(b, true);
+  if (rc != RQ_OK) return rc;
+  for (int v = 0; v < 10; ++v)
+    if ((rc = b_vcycle<T>(b)) != RQ_OK) return rc;
+  b->steps_done = 0;
+  BCK(cudaStreamSynchronize(b->st));
+  return RQ_OK;
+}
+
+// -----------------------------------------------------------------------------------------
+// C ABI
+// -----------------------------------------------------------------------------------------
+extern "C" int rq_batch_create(const rq_config* cfgs, const rq_atom* atoms, const int32_t* n_atoms, int32_t n_inst,
+                               rq_batch** out) {
+  if (!cfgs || !atoms || !n_atoms || !out || n_inst < 1) return RQ_EINVAL;
+  *out = nullptr;
+  const rq_config& c0 = cfgs[0];
+  if (c0.flavor != RQ_FLAVOR_NEW) return RQ_ENOTSUP;
+  for (int q = 0; q < n_inst; ++q) {
+    const rq_config& c = cfgs[q];
+    if (c.flavor != c0.flavor || c.precision != c0.precision || c.NN < 4 || c.NN % 2 || c.screen <= 0 ||
+        std::fabs(c.screen / c.NN - c0.screen / c0.NN) > 1e-12 * (c0.screen / c0.NN) || n_atoms[q] < 1)
+      return RQ_EINVAL;  // one flavour/precision and one grid spacing h for the whole batch
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return RQ_ENODEV;
+  rq_batch* b = new (std::nothrow) rq_batch();
+  if (!b) return RQ_ENOMEM;
+  b->n = n_inst;
+  b->cfg = c0;
+  b->fp64 = c0.precision == RQ_PREC_FP64;
+  rq_config& f = b->cfg;  // the new flavour's defaults (capi.cu fill_defaults)
+  if (f.norm_interval <= 0) f.norm_interval = 1;
+  if (f.poisson_interval <= 0) f.poisson_interval = 2;
+  if (f.label_interval <= 0) f.label_interval = 20;
+  if (f.mg_pre <= 0) f.mg_pre = 2;
+  if (f.mg_post <= 0) f.mg_post = 2;
+  if (f.mg_coarse_sweeps <= 0) f.mg_coarse_sweeps = 64;
+  if (f.boundary_speed <= 0) f.boundary_speed = 0.5;
+  if (f.curv_reg == 0) f.curv_reg = 0.15;
+  if (f.curv_reg < 0) f.curv_reg = 0;
+  b->dv = f.dv > 0 ? f.dv : 0.2;
+  if (cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking) != cudaSuccess) {
+    delete b;
+    return RQ_ECUDA;
+  }
+  b->st = b->own;
+  b->hin.resize(n_inst);
+  b->atoms.resize(n_inst);
+  const rq_atom* a = atoms;
+  for (int q = 0; q < n_inst; ++q) {
+    BInst& I = b->hin[q];
+    std::memset(&I, 0, sizeof(I));
+    const rq_config& c = cfgs[q];
+    I.g = make_geo(c.NN + 1);
+    I.h = c.screen / c.NN;
+    I.nAt = I.nDom = n_atoms[q];
+    I.dom0 = I.at0 = b->A;
+    b->atoms[q].assign(a, a + n_atoms[q]);
+    a += n_atoms[q];
+    b->A += n_atoms[q];
+    int nl = 1, nn = c.NN;
+    const int want = c.mg_levels;
+    while (nn % 2 == 0 && (want > 0 ? nl < want : nn / 2 >= 6) && nl < kMaxLev) {
+      nn /= 2;
+      nl++;
+    }
+    I.nlev = nl;
+    double h = I.h;
+    int m = c.NN;
+    for (int l = 0; l < nl; ++l) {
+      I.lg[l] = make_geo(m + 1);
+      I.lh[l] = h;
+      h *= 2;
+      m /= 2;
+    }
+    b->maxlev = std::max(b->maxlev, nl);
+  }
+  b->D = b->A;
+  int rc = build(b);
+  if (rc != RQ_OK) {
+    std::fprintf(stderr, "rq_batch_create: %s\n", b->last_error.c_str());
+    rq_batch_destroy(b);
+    return rc;
+  }
+  *out = b;
+  return RQ_OK;
+}
+
+extern "C" void rq_batch_destroy(rq_batch* b) {
+  if (!b) return;
+  cudaStreamSynchronize(b->st);
+  for (auto& g : b->graph)
+    if (g) cudaGraphExecDestroy(g);
+  for (void* p : b->allocs) cudaFree(p);
+  if (b->own) cudaStreamDestroy(b->own);
+  delete b;
+}
+
+extern "C" const char* rq_batch_last_error(const rq_batch* b) { return b ? b->last_error.c_str() : "null batch"; }
+
+extern "C" int rq_batch_set_stream(rq_batch* b, void* stream) {
+  if (!b) return RQ_EINVAL;
+  BCK(cudaStreamSynchronize(b->st));
+  b->st = stream ? (cudaStream_t)stream : b->own;
+  return RQ_OK;
+}
+
+extern "C" int rq_batch_initialize(rq_batch* b) {
+  if (!b) return RQ_EINVAL;
+  return b->fp64 ? b_initialize<double>(b) : b_initialize<float>(b);
+}
+
+static int b_period(const rq_batch* b) {
+  auto lcm = [](long x, long y) {
+    long a = x, c = y;
+    while (c) { long t = a % c; a = c; c = t; }
+    return x / a * y;
+  };
+  const rq_config& f = b->cfg;
+  return (int)lcm(lcm(f.poisson_interval, f.norm_interval), f.label_interval);
+}
+
+static int b_eager(rq_batch* b, int n) {
+  for (int q = 0; q < n; ++q) {
+    const int s = b->steps_done + 1;
+    const int rc = b->fp64 ? b_step<double>(b, s) : b_step<float>(b, s);
+    if (rc != RQ_OK) return rc;
+    b->steps_done = s;
+  }
+  return RQ_OK;
+}
+
+extern "C" int rq_batch_step(rq_batch* b, int32_t n) {
+  if (!b || n < 0) return RQ_EINVAL;
+  const int period = b_period(b);
+  int left = n;
+  while (left > 0) {
+    const int lu = b->cfg.label_until;
+    const bool straddle = lu > 0 && b->steps_done < lu && b->steps_done + period > lu;
+    const bool aligned = !straddle && period > 0 && period <= 4096 && b->steps_done % period == 0 && left >= period;
+    if (!aligned) {
+      int todo = left;
+      if (period > 0 && b->steps_done % period != 0) todo = std::min(left, period - b->steps_done % period);
+      else if (period > 0 && straddle) todo = std::min(left, period);
+      int rc = b_eager(b, todo);
+      if (rc != RQ_OK) return rc;
+      left -= todo;
+      continue;
+    }
+    const int on = (lu <= 0 || b->steps_done < lu) ? 1 : 0;
+    const int key = b->cu | (b->cp << 1) | (b->cl << 2) | (on << 3);
+    if (!b->graph[key]) {
+      const long long l0 = b->launches;
+      BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+      int rc = b_eager(b, period);
+      cudaGraph_t gr = nullptr;
+      cudaError_t e = cudaStreamEndCapture(b->st, &gr);
+      if (rc != RQ_OK) {
+        if (gr) cudaGraphDestroy(gr);
+        return rc;
+      }
+      BCK(e);
+      e = cudaGraphInstantiate(&b->graph[key], gr, 0);
+      cudaGraphDestroy(gr);
+      BCK(e);
+      b->graph_post[key] = b->cu | (b->cp << 1) | (b->cl << 2);
+      b->graph_launches[key] = b->launches - l0;
+      BCK(cudaGraphLaunch(b->graph[key], b->st));
+    } else {
+      BCK(cudaGraphLaunch(b->graph[key], b->st));
+      const int post = b->graph_post[key];
+      b->cu = post & 1; b->cp = (post >> 1) & 1; b->cl = (post >> 2) & 1;
+      b->steps_done += period;
+      b->launches += b->graph_launches[key];
+    }
+    left -= period;
+  }
+  return RQ_OK;
+}
+
+extern "C" int rq_batch_energy(rq_batch* b, double* out) {
+  if (!b || !out) return RQ_EINVAL;
+  BCK(cudaMemsetAsync(b->dpd, 0, sizeof(double) * 4 * b->D, b->st));
+  if (b->fp64) {
+    using T = double;
+    kb_energy<T><<<b->march[0].n, march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cp, b->cl, b->dpd);
+    BL("energy");
+  } else {
+    using T = float;
+    kb_energy<T><<<b->march[0].n, march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cp, b->cl, b->dpd);
+    BL("energy");
+  }
+  std::vector<double> pd((size_t)4 * b->D);
+  BCK(cudaMemcpyAsync(pd.data(), b->dpd, sizeof(double) * pd.size(), cudaMemcpyDeviceToHost, b->st));
+  BCK(cudaStreamSynchronize(b->st));
+  for (int q = 0; q < b->n; ++q) {
+    const BInst& I = b->hin[q];
+    double* o = out + (size_t)q * RQ_ENERGY_LEN;
+    std::memset(o, 0, sizeof(double) * RQ_ENERGY_LEN);
+    for (int d = 0; d < I.nDom; ++d) {
+      o[RQ_E_T] += pd[4 * (I.dom0 + d) + 1];
+      o[RQ_E_EK] += pd[4 * (I.dom0 + d) + 2];
+      o[RQ_E_EE] += pd[4 * (I.dom0 + d) + 3];
+    }
+    double ekk = 0;  // point-charge nuclear repulsion (bohr)
+    const auto& at = b->atoms[q];
+    for (size_t x = 0; x < at.size(); ++x)
+      for (size_t y = x + 1; y < at.size(); ++y) {
+        if (at[x].Z_nuc <= 0 || at[y].Z_nuc <= 0) continue;
+        const double dx = (at[x].i - at[y].i) * I.h, dy = (at[x].j - at[y].j) * I.h, dz = (at[x].k - at[y].k) * I.h;
+        ekk += at[x].Z_nuc * at[y].Z_nuc / std::sqrt(dx * dx + dy * dy + dz * dz);
+      }
+    o[RQ_E_KK] = ekk;
+    o[RQ_E_TOTAL] = o[RQ_E_T] + o[RQ_E_EK] + o[RQ_E_EE] + ekk;
+    if (!std::isfinite(o[RQ_E_TOTAL])) {
+      b->last_error = "non-finite energy in instance " + std::to_string(q);
+      return RQ_ENONFINITE;
+    }
+  }
+  return RQ_OK;
+}
+
+extern "C" int rq_batch_forces(rq_batch* b, double* F) {
+  if (!b || !F) return RQ_EINVAL;
+  BCK(cudaMemsetAsync(b->dF, 0, sizeof(double) * 3 * b->A, b->st));
+  if (b->fp64) {
+    using T = double;
+    kb_force<T><<<b->force.n, 256, 0, b->st>>>(b->din, b->force.d, b->cu, b->cfg.sigma, b->dF);
+    BL("force");
+  } else {
+    using T = float;
+    kb_force<T><<<b->force.n, 256, 0, b->st>>>(b->din, b->force.d, b->cu, b->cfg.sigma, b->dF);
+    BL("force");
+  }
+  BCK(cudaMemcpyAsync(F, b->dF, sizeof(double) * 3 * b->A, cudaMemcpyDeviceToHost, b->st));
+  BCK(cudaStreamSynchronize(b->st));
+  // add the point-charge nuclear repulsion forces
+  for (int q = 0; q < b->n; ++q) {
+    const BInst& I = b->hin[q];
+    const auto& at = b->atoms[q];
+    for (size_t x = 0; x < at.size(); ++x) {
+      if (at[x].Z_nuc <= 0) continue;
+      for (size_t y = 0; y < at.size(); ++y) {
+        if (y == x || at[y].Z_nuc <= 0) continue;
+        const double dx = (at[x].i - at[y].i) * I.h, dy = (at[x].j - at[y].j) * I.h, dz = (at[x].k - at[y].k) * I.h;
+        const double r2 = dx * dx + dy * dy + dz * dz, w = at[x].Z_nuc * at[y].Z_nuc / (r2 * std::sqrt(r2));
+        double* f = F + 3 * ((size_t)I.at0 + x);
+        f[0] += w * dx; f[1] += w * dy; f[2] += w * dz;
+      }
+    }
+  }
+  return RQ_OK;
+}
+
+extern "C" int rq_batch_solve(rq_batch* b, double tol_dE, int32_t max_steps, int32_t check_interval,
+                              int32_t* converged_at, double* E_final) {
+  if (!b || max_steps < 0 || check_interval <= 0) return RQ_EINVAL;
+  std::vector<double> e((size_t)b->n * RQ_ENERGY_LEN), prev(b->n);
+  int rc = rq_batch_energy(b, e.data());
+  if (rc != RQ_OK) return rc;
+  std::vector<int> conv(b->n, -1);
+  for (int q = 0; q < b->n; ++q) prev[q] = e[(size_t)q * RQ_ENERGY_LEN];
+  int taken = 0, left = b->n;
+  while (taken < max_steps && left > 0) {
+    const int n = std::min(check_interval, max_steps - taken);
+    if ((rc = rq_batch_step(b, n)) != RQ_OK) return rc;
+    taken += n;
+    if ((rc = rq_batch_energy(b, e.data())) != RQ_OK) return rc;
+    for (int q = 0; q < b->n; ++q) {
+      const double E = e[(size_t)q * RQ_ENERGY_LEN];
+      if (conv[q] < 0 && std::fabs(E - prev[q]) < tol_dE) {
+        conv[q] = taken;
+        left--;
+      }
+      prev[q] = E;
+    }
+  }
+  for (int q = 0; q < b->n; ++q) {
+    if (converged_at) converged_at[q] = conv[q];
+    if (E_final) E_final[q] = prev[q];
+  }
+  return RQ_OK;
+}
+
+extern "C" int rq_batch_info(const rq_batch* b, int32_t* n_inst, int64_t* total_points, int64_t* interior_points,
+                             int64_t* kernel_launches) {
+  if (!b) return RQ_EINVAL;
+  long long tp = 0, ip = 0;
+  for (const auto& I : b->hin) {
+    tp += I.g.S3;
+    ip += (long long)(I.g.NN - 1) * (I.g.NN - 1) * (I.g.NN - 1);
+  }
+  if (n_inst) *n_inst = b->n;
+  if (total_points) *total_points = tp;
+  if (interior_points) *interior_points = ip;
+  if (kernel_launches) *kernel_launches = b->launches;
+  return RQ_OK;
+}
+
+extern "C" int rq_batch_synchronize(rq_batch* b) {
+  if (!b) return RQ_EINVAL;
+  BCK(cudaStreamSynchronize(b->st));
+  return RQ_OK;
+}
