@@ -64,14 +64,14 @@ typedef struct rq_config {
   int32_t norm_interval;    /* normalise every n steps (solver.py 20, molecule.js NORM_INTERVAL 20) */
   double screen;            /* box edge in bohr (USER_SCREEN / screen); h = screen/NN */
   double dv;                /* dt = dv*h^2; <=0 -> flavour table (molecule.js:78, solver.py:342-351) */
-  int32_t poisson_interval; /* solver.py: Poisson step every 2; new: V-cycle every n steps */
+  int32_t poisson_interval; /* solver.py: Poisson step every 2; new: one V-cycle every n steps (4) */
   int32_t label_interval;   /* solver.py: 5*norm_interval (100); new: level-set step period */
   int32_t jacobi_per_step;  /* Jacobi sweeps per Poisson step (2 in both references) */
   int32_t steps_per_frame;  /* molecule.js STEPS_PER_FRAME (frame = steps + energy + labels) */
   int32_t vcycle_interval;  /* molecule.js POISSON_INTERVAL (50) */
   int32_t mg_levels;        /* new: multigrid levels (<=0: as deep as NN allows, coarsest >= 4) */
-  int32_t mg_pre, mg_post;  /* new: red-black sweeps before / after the coarse correction (2, 2) */
-  int32_t mg_coarse_sweeps; /* new: FP64 red-black sweeps on the coarsest level (64) */
+  int32_t mg_pre, mg_post;  /* new: red-black sweeps before / after the coarse correction (1, 1) */
+  int32_t mg_coarse_sweeps; /* new: FP64 red-black sweeps on the coarsest level (16) */
   int32_t sic;              /* molecule.js SIC (:3009-3076): 0 off (only value supported here) */
   double boundary_speed;    /* molecule.js dt_w (0.5, :135) */
   double curv_reg;          /* molecule.js curvReg (0: 0.15 as :34; < 0: off) */
@@ -154,6 +154,8 @@ RQ_API void rq_destroy(rq_ctx* ctx);
 /* Binds the context to a CUDA stream (cudaStream_t passed as void*; NULL = the stream the
  * context created for itself).  Pending work on the previous stream is finished first. */
 RQ_API int rq_set_stream(rq_ctx* ctx, void* stream);
+/* Device pointers in info are the live fields; for the new flavour call rq_synchronize first
+ * (it materialises a per-domain normalisation that the next update would otherwise apply). */
 RQ_API int rq_get_info(const rq_ctx* ctx, rq_info* info);
 RQ_API const char* rq_last_error(const rq_ctx* ctx);
 RQ_API const char* rq_status_string(int status);

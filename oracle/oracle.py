@@ -454,8 +454,8 @@ class NewMethodDriver:
     ``rows`` use the flavour's idiom: nuclei have Z_nuc > 0, domains have Z > 0 (their position
     is the seed of the initial state).  Positions are grid units (x = i*h)."""
 
-    def __init__(self, NN, screen, rows, dv=0.2, sigma=None, poisson_interval=2, norm_interval=1, label_interval=20,
-                 levels=None, pre=2, post=2, coarse_sweeps=64, boundary_speed=0.5, curv_reg=0.15, label_until=0):
+    def __init__(self, NN, screen, rows, dv=0.2, sigma=None, poisson_interval=4, norm_interval=1, label_interval=20,
+                 levels=None, pre=1, post=1, coarse_sweeps=16, boundary_speed=0.5, curv_reg=0.15, label_until=0):
         self.NN, self.S = NN, NN + 1
         self.S3 = self.S ** 3
         self.h = screen / NN

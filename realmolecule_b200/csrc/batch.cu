@@ -51,7 +51,8 @@ struct BItem {
 // ---------------------------------------------------------------------------------------
 template <typename T, bool ACC>
 __global__ void __launch_bounds__(256) kb_update(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cu,
-                                                 int cp, int cl, T half_dv, T dt, double* __restrict__ norms) {
+                                                 int cp, int cl, T half_dv, T dt, double* __restrict__ norms,
+                                                 const T* __restrict__ scale) {
   __shared__ DomTable<1, 128> tab;
   const BItem it = items[blockIdx.x];
   const BInst& I = ins[it.inst];
@@ -61,7 +62,7 @@ __global__ void __launch_bounds__(256) kb_update(const BInst* __restrict__ ins, 
     __syncthreads();
   }
   nm_update_body<T, ACC>((const T*)I.U[cu], (T*)I.U[1 - cu], (const T*)I.K, (const T*)I.P[cp], I.lab[cl], I.g, half_dv,
-                         dt, I.h * I.h * I.h, I.nDom, nrm, tab, it.bx, it.by, it.bz);
+                         dt, I.h * I.h * I.h, I.nDom, nrm, tab, it.bx, it.by, it.bz, scale ? scale + I.dom0 : nullptr);
   if (ACC) {
     __syncthreads();
     dom_table_flush(tab, nrm);
@@ -106,7 +107,8 @@ __global__ void __launch_bounds__(256) kb_residual(const BInst* __restrict__ ins
   const BInst& I = ins[it.inst];
   const T* P = FINE ? (const T*)I.P[cp] : (const T*)I.lP[lev];
   const T* f = FINE ? (const T*)I.U[cu] : (const T*)I.lf[lev];
-  nm_residual_body<T, FINE>(P, f, (T*)I.lr[lev], I.lg[lev], (T)(1.0 / (I.lh[lev] * I.lh[lev])), it.bx, it.by, it.bz);
+  nm_residual_flat_body<T, FINE>(P, f, (T*)I.lr[lev], I.lg[lev], (T)(1.0 / (I.lh[lev] * I.lh[lev])),
+                                 (long long)it.bx * blockDim.x + threadIdx.x);
 }
 
 template <typename T>
@@ -133,7 +135,8 @@ __global__ void __launch_bounds__(256) kb_prolong(const BInst* __restrict__ ins,
   const BItem it = items[blockIdx.x];
   const BInst& I = ins[it.inst];
   T* P = lev == 0 ? (T*)I.P[cp] : (T*)I.lP[lev];
-  nm_prolong_body<T>((const T*)I.lP[lev + 1], P, I.lg[lev], I.lg[lev + 1], it.bx, it.by, it.bz);
+  nm_prolong_flat_body<T>((const T*)I.lP[lev + 1], P, I.lg[lev], I.lg[lev + 1],
+                          (long long)it.bx * blockDim.x + threadIdx.x);
 }
 
 template <typename T>
@@ -217,16 +220,20 @@ struct rq_batch {
   float4* seeds_all = nullptr;
   int maxlev = 0;
   // work lists
-  struct Plan { BItem* d = nullptr; int n = 0; };
+  struct Plan { BItem* d = nullptr; int n = 0, cap = 0; };
   Plan march[kMaxLev], rbgs[kMaxLev], restr[kMaxLev], zero[kMaxLev], coarse[kMaxLev], prol[kMaxLev];
   size_t coarse_smem[kMaxLev] = {};
   Plan flat16, flat1, force;
   cudaStream_t st = nullptr, own = nullptr;
   int cu = 0, cp = 0, cl = 0, steps_done = 0;
   long long launches = 0;
-  cudaGraphExec_t graph[16] = {};
-  int graph_post[16] = {};
-  long long graph_launches[16] = {};
+  cudaGraphExec_t graph[32] = {};
+  int graph_post[32] = {};
+  long long graph_launches[32] = {};
+  std::vector<char> active;       // instances still being stepped (solve drops converged ones)
+  std::vector<double> lastE;      // last energies per instance (n x RQ_ENERGY_LEN)
+  bool pending = false;           // psi awaits the per-domain scale (applied by the next update or a flush)
+  bool promoted = false;          // a mixed batch switched to FP64 for its final refinement
   std::string last_error;
 };
 
@@ -254,7 +261,10 @@ static int balloc(rq_batch* b, void** p, size_t bytes) {
 static int upload_plan(rq_batch* b, rq_batch::Plan& p, const std::vector<BItem>& v) {
   p.n = (int)v.size();
   if (!p.n) return RQ_OK;
-  BALLOC(p.d, sizeof(BItem) * v.size());
+  if (p.n > p.cap) {  // first build allocates the full size; later builds (fewer instances) reuse it
+    BALLOC(p.d, sizeof(BItem) * v.size());
+    p.cap = p.n;
+  }
   BCK(cudaMemcpyAsync(p.d, v.data(), sizeof(BItem) * v.size(), cudaMemcpyHostToDevice, b->st));
   return RQ_OK;
 }
@@ -264,6 +274,56 @@ static void march_items(std::vector<BItem>& v, int inst, const Geo& g) {
   for (unsigned z = 0; z < gr.z; ++z)
     for (unsigned y = 0; y < gr.y; ++y)
       for (unsigned x = 0; x < gr.x; ++x) v.push_back({inst, (int)x, (int)y, (int)z});
+}
+
+// Work lists over the active instances (all of them at creation; solve drops converged ones).
+static int build_plans(rq_batch* b) {
+  const int n = b->n;
+  // work lists
+  for (int l = 0; l < b->maxlev; ++l) {
+    std::vector<BItem> m, r, rs, z, c, p;
+    for (int q = 0; q < n; ++q) {
+      const BInst& I = b->hin[q];
+      if (l >= I.nlev || !b->active[q]) continue;
+      march_items(m, q, I.lg[l]);
+      if (l == I.nlev - 1) {
+        c.push_back({q, 0, 0, 0});
+        b->coarse_smem[l] = std::max(b->coarse_smem[l], sizeof(double) * 2 * (size_t)I.lg[l].S3);
+        continue;
+      }
+      const int nn = I.lg[l].NN - 1;
+      for (int zz = 0; zz < nn; ++zz)
+        for (int y = 0; y < (nn + 7) / 8; ++y)
+          for (int x = 0; x < (nn + 63) / 64; ++x) r.push_back({q, x, y, zz});
+      const long long nc = (long long)(I.lg[l + 1].NN - 1) * (I.lg[l + 1].NN - 1) * (I.lg[l + 1].NN - 1);
+      for (long long x = 0; x < (nc + 255) / 256; ++x) rs.push_back({q, (int)x, 0, 0});
+      for (long long x = 0; x < (I.lg[l + 1].S3 + 255) / 256; ++x) z.push_back({q, (int)x, 0, 0});
+      const long long ni = (long long)nn * nn * nn;
+      for (long long x = 0; x < (ni + 255) / 256; ++x) p.push_back({q, (int)x, 0, 0});
+    }
+    int rc;
+    if ((rc = upload_plan(b, b->march[l], m)) || (rc = upload_plan(b, b->rbgs[l], r)) ||
+        (rc = upload_plan(b, b->restr[l], rs)) || (rc = upload_plan(b, b->zero[l], z)) ||
+        (rc = upload_plan(b, b->coarse[l], c)) || (rc = upload_plan(b, b->prol[l], p)))
+      return rc;
+  }
+  std::vector<BItem> f16, f1, fo;
+  for (int q = 0; q < n; ++q) {
+    if (!b->active[q]) continue;
+    const BInst& I = b->hin[q];
+    for (long long x = 0; x < (I.g.S3 + 256 * kNmFlatChunk - 1) / (256 * kNmFlatChunk); ++x) f16.push_back({q, (int)x, 0, 0});
+    for (long long x = 0; x < (I.g.S3 + 255) / 256; ++x) f1.push_back({q, (int)x, 0, 0});
+    const long long n1 = I.g.NN - 1, ntiles = (n1 * n1 * n1 + kNmForceTile - 1) / kNmForceTile;
+    const int groups = (int)std::min<long long>(ntiles, 32);
+    for (int ch = 0; ch < (I.nAt + 255) / 256; ++ch)
+      for (int t = 0; t < groups; ++t) fo.push_back({q, t, groups, ch});
+  }
+  int rc;
+  if ((rc = upload_plan(b, b->flat16, f16)) || (rc = upload_plan(b, b->flat1, f1)) || (rc = upload_plan(b, b->force, fo)))
+    return rc;
+  for (auto& g : b->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  return RQ_OK;
 }
 
 static int build(rq_batch* b) {
@@ -329,59 +389,21 @@ static int build(rq_batch* b) {
     BCK(cudaMemcpyAsync(b->seeds_all, seeds.data(), sizeof(float4) * seeds.size(), cudaMemcpyHostToDevice, b->st));
   BALLOC(b->din, sizeof(BInst) * n);
   BCK(cudaMemcpyAsync(b->din, b->hin.data(), sizeof(BInst) * n, cudaMemcpyHostToDevice, b->st));
-  // work lists
-  for (int l = 0; l < b->maxlev; ++l) {
-    std::vector<BItem> m, r, rs, z, c, p;
-    for (int q = 0; q < n; ++q) {
-      const BInst& I = b->hin[q];
-      if (l >= I.nlev) continue;
-      march_items(m, q, I.lg[l]);
-      if (l == I.nlev - 1) {
-        c.push_back({q, 0, 0, 0});
-        b->coarse_smem[l] = std::max(b->coarse_smem[l], sizeof(double) * 2 * (size_t)I.lg[l].S3);
-        continue;
-      }
-      const int nn = I.lg[l].NN - 1;
-      for (int zz = 0; zz < nn; ++zz)
-        for (int y = 0; y < (nn + 7) / 8; ++y)
-          for (int x = 0; x < (nn + 63) / 64; ++x) r.push_back({q, x, y, zz});
-      const long long nc = (long long)(I.lg[l + 1].NN - 1) * (I.lg[l + 1].NN - 1) * (I.lg[l + 1].NN - 1);
-      for (long long x = 0; x < (nc + 255) / 256; ++x) rs.push_back({q, (int)x, 0, 0});
-      for (long long x = 0; x < (I.lg[l + 1].S3 + 255) / 256; ++x) z.push_back({q, (int)x, 0, 0});
-      march_items(p, q, I.lg[l]);
-    }
-    int rc;
-    if ((rc = upload_plan(b, b->march[l], m)) || (rc = upload_plan(b, b->rbgs[l], r)) ||
-        (rc = upload_plan(b, b->restr[l], rs)) || (rc = upload_plan(b, b->zero[l], z)) ||
-        (rc = upload_plan(b, b->coarse[l], c)) || (rc = upload_plan(b, b->prol[l], p)))
-      return rc;
-  }
-  std::vector<BItem> f16, f1, fo;
-  for (int q = 0; q < n; ++q) {
-    const BInst& I = b->hin[q];
-    for (long long x = 0; x < (I.g.S3 + 256 * kNmFlatChunk - 1) / (256 * kNmFlatChunk); ++x) f16.push_back({q, (int)x, 0, 0});
-    for (long long x = 0; x < (I.g.S3 + 255) / 256; ++x) f1.push_back({q, (int)x, 0, 0});
-    const long long n1 = I.g.NN - 1, ntiles = (n1 * n1 * n1 + kNmForceTile - 1) / kNmForceTile;
-    const int groups = (int)std::min<long long>(ntiles, 32);
-    for (int ch = 0; ch < (I.nAt + 255) / 256; ++ch)
-      for (int t = 0; t < groups; ++t) fo.push_back({q, t, groups, ch});
-  }
-  int rc;
-  if ((rc = upload_plan(b, b->flat16, f16)) || (rc = upload_plan(b, b->flat1, f1)) || (rc = upload_plan(b, b->force, fo)))
-    return rc;
+  int rc = build_plans(b);
+  if (rc != RQ_OK) return rc;
   size_t smax = 0;
   for (int l = 0; l < b->maxlev; ++l) smax = std::max(smax, b->coarse_smem[l]);
   if (smax > 200 * 1024) {
     b->last_error = "coarsest multigrid level too large for the shared-memory FP64 solve";
     return RQ_EINVAL;
   }
-  if (b->fp64)
-    BCK(cudaFuncSetAttribute(kb_coarsest<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
-  else
-    BCK(cudaFuncSetAttribute(kb_coarsest<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
+  BCK(cudaFuncSetAttribute(kb_coarsest<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
+  BCK(cudaFuncSetAttribute(kb_coarsest<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
   BCK(cudaStreamSynchronize(b->st));
   return RQ_OK;
 }
+
+int rq_batch_set_active_all(rq_batch* b);
 
 template <typename T>
 static int b_launch_err(rq_batch* b, const char* what) {
@@ -404,7 +426,7 @@ static int b_vcycle(rq_batch* b) {
   const int pre = b->cfg.mg_pre, post = b->cfg.mg_post;
   for (int l = 0; l < b->maxlev; ++l) {
     if (b->coarse[l].n) {
-      kb_coarsest<T><<<b->coarse[l].n, 1024, b->coarse_smem[l], b->st>>>(b->din, b->coarse[l].d, l,
+      kb_coarsest<T><<<b->coarse[l].n, kCoarsestThreads, b->coarse_smem[l], b->st>>>(b->din, b->coarse[l].d, l,
                                                                            b->cfg.mg_coarse_sweeps);
       BL("coarsest");
     }
@@ -418,9 +440,9 @@ static int b_vcycle(rq_batch* b) {
         BL("rbgs");
       }
     if (l == 0)
-      kb_residual<T, true><<<b->prol[l].n, march_block(), 0, b->st>>>(b->din, b->prol[l].d, l, b->cu, b->cp);
+      kb_residual<T, true><<<b->prol[l].n, 256, 0, b->st>>>(b->din, b->prol[l].d, l, b->cu, b->cp);
     else
-      kb_residual<T, false><<<b->prol[l].n, march_block(), 0, b->st>>>(b->din, b->prol[l].d, l, b->cu, b->cp);
+      kb_residual<T, false><<<b->prol[l].n, 256, 0, b->st>>>(b->din, b->prol[l].d, l, b->cu, b->cp);
     BL("residual");
     kb_restrict<T><<<b->restr[l].n, 256, 0, b->st>>>(b->din, b->restr[l].d, l);
     BL("restrict");
@@ -429,7 +451,7 @@ static int b_vcycle(rq_batch* b) {
   }
   for (int l = b->maxlev - 2; l >= 0; --l) {
     if (!b->rbgs[l].n) continue;
-    kb_prolong<T><<<b->prol[l].n, march_block(), 0, b->st>>>(b->din, b->prol[l].d, l, b->cp);
+    kb_prolong<T><<<b->prol[l].n, 256, 0, b->st>>>(b->din, b->prol[l].d, l, b->cp);
     BL("prolong");
     for (int s = 0; s < post; ++s)
       for (int color = 0; color < 2; ++color) {
@@ -445,6 +467,7 @@ static int b_vcycle(rq_batch* b) {
 
 template <typename T>
 static int b_normalize(rq_batch* b, bool accumulate) {
+  if (b->flat16.n == 0) return RQ_OK;
   if (accumulate) {
     BCK(cudaMemsetAsync(b->dnorm, 0, sizeof(double) * b->D, b->st));
     kb_norms<T><<<b->flat16.n, 256, 0, b->st>>>(b->din, b->flat16.d, b->cu, b->cl, b->dnorm);
@@ -454,30 +477,53 @@ static int b_normalize(rq_batch* b, bool accumulate) {
   b->launches++;
   kb_apply_scale<T><<<b->flat16.n, 256, 0, b->st>>>(b->din, b->flat16.d, b->cu, b->cl, (const T*)b->scale);
   BL("apply_scale");
+  b->pending = false;
   return RQ_OK;
 }
+
+// materialise a pending per-domain normalisation (needed by the multigrid, labels and readouts)
+template <typename T>
+static int b_flush(rq_batch* b) {
+  if (!b->pending || b->flat16.n == 0) return RQ_OK;
+  kb_apply_scale<T><<<b->flat16.n, 256, 0, b->st>>>(b->din, b->flat16.d, b->cu, b->cl, (const T*)b->scale);
+  BL("apply_scale");
+  b->pending = false;
+  return RQ_OK;
+}
+static int b_flush_any(rq_batch* b) { return b->fp64 ? b_flush<double>(b) : b_flush<float>(b); }
 
 template <typename T>
 static int b_step(rq_batch* b, int s) {
   const rq_config& f = b->cfg;
   int rc;
-  if (s % f.poisson_interval == 0 && (rc = b_vcycle<T>(b)) != RQ_OK) return rc;
+  if (b->march[0].n == 0) return RQ_OK;  // no active instance
+  if (s % f.poisson_interval == 0) {
+    if ((rc = b_flush<T>(b)) != RQ_OK) return rc;
+    if ((rc = b_vcycle<T>(b)) != RQ_OK) return rc;
+  }
   const bool norm = s % f.norm_interval == 0;
   const T hd = (T)(0.5 * b->dv);
   // dt = dv h^2 differs per instance only through h: every instance of a batch shares h
   const T dt = (T)(b->dv * b->hin[0].h * b->hin[0].h);
+  const T* sc = b->pending ? (const T*)b->scale : nullptr;
   if (norm) {
     BCK(cudaMemsetAsync(b->dnorm, 0, sizeof(double) * b->D, b->st));
     kb_update<T, true><<<b->march[0].n, march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cp, b->cl, hd, dt,
-                                                                    b->dnorm);
+                                                                    b->dnorm, sc);
   } else {
     kb_update<T, false><<<b->march[0].n, march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cp, b->cl, hd, dt,
-                                                                     nullptr);
+                                                                     nullptr, sc);
   }
   BL("update");
   b->cu ^= 1;
-  if (norm && (rc = b_normalize<T>(b, false)) != RQ_OK) return rc;
+  b->pending = false;
+  if (norm) {  // applied by the next update (or a flush)
+    BCK(nm_norm_scale<T>(b->dnorm, b->Zdom, b->D, (T*)b->scale, b->err, b->st));
+    b->launches++;
+    b->pending = true;
+  }
   if (s % f.label_interval == 0 && (f.label_until <= 0 || s <= f.label_until)) {
+    if ((rc = b_flush<T>(b)) != RQ_OK) return rc;
     kb_evolve<T><<<b->march[0].n, march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cl,
                                                               (T)(float)f.boundary_speed, (T)(float)f.curv_reg);
     BL("evolve");
@@ -535,11 +581,11 @@ extern "C" int rq_batch_create(const rq_config* cfgs, const rq_atom* atoms, cons
   b->fp64 = c0.precision == RQ_PREC_FP64;
   rq_config& f = b->cfg;  // the new flavour's defaults (capi.cu fill_defaults)
   if (f.norm_interval <= 0) f.norm_interval = 1;
-  if (f.poisson_interval <= 0) f.poisson_interval = 2;
+  if (f.poisson_interval <= 0) f.poisson_interval = 4;
   if (f.label_interval <= 0) f.label_interval = 20;
-  if (f.mg_pre <= 0) f.mg_pre = 2;
-  if (f.mg_post <= 0) f.mg_post = 2;
-  if (f.mg_coarse_sweeps <= 0) f.mg_coarse_sweeps = 64;
+  if (f.mg_pre <= 0) f.mg_pre = 1;
+  if (f.mg_post <= 0) f.mg_post = 1;
+  if (f.mg_coarse_sweeps <= 0) f.mg_coarse_sweeps = 16;
   if (f.boundary_speed <= 0) f.boundary_speed = 0.5;
   if (f.curv_reg == 0) f.curv_reg = 0.15;
   if (f.curv_reg < 0) f.curv_reg = 0;
@@ -581,6 +627,7 @@ extern "C" int rq_batch_create(const rq_config* cfgs, const rq_atom* atoms, cons
     b->maxlev = std::max(b->maxlev, nl);
   }
   b->D = b->A;
+  b->active.assign(n_inst, 1);
   int rc = build(b);
   if (rc != RQ_OK) {
     std::fprintf(stderr, "rq_batch_create: %s\n", b->last_error.c_str());
@@ -653,7 +700,7 @@ extern "C" int rq_batch_step(rq_batch* b, int32_t n) {
       continue;
     }
     const int on = (lu <= 0 || b->steps_done < lu) ? 1 : 0;
-    const int key = b->cu | (b->cp << 1) | (b->cl << 2) | (on << 3);
+    const int key = b->cu | (b->cp << 1) | (b->cl << 2) | (on << 3) | ((b->pending ? 1 : 0) << 4);
     if (!b->graph[key]) {
       const long long l0 = b->launches;
       BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
@@ -668,13 +715,14 @@ extern "C" int rq_batch_step(rq_batch* b, int32_t n) {
       e = cudaGraphInstantiate(&b->graph[key], gr, 0);
       cudaGraphDestroy(gr);
       BCK(e);
-      b->graph_post[key] = b->cu | (b->cp << 1) | (b->cl << 2);
+      b->graph_post[key] = b->cu | (b->cp << 1) | (b->cl << 2) | ((b->pending ? 1 : 0) << 4);
       b->graph_launches[key] = b->launches - l0;
       BCK(cudaGraphLaunch(b->graph[key], b->st));
     } else {
       BCK(cudaGraphLaunch(b->graph[key], b->st));
       const int post = b->graph_post[key];
       b->cu = post & 1; b->cp = (post >> 1) & 1; b->cl = (post >> 2) & 1;
+      b->pending = (post >> 4) & 1;
       b->steps_done += period;
       b->launches += b->graph_launches[key];
     }
@@ -685,6 +733,13 @@ extern "C" int rq_batch_step(rq_batch* b, int32_t n) {
 
 extern "C" int rq_batch_energy(rq_batch* b, double* out) {
   if (!b || !out) return RQ_EINVAL;
+  if (b->lastE.size() != (size_t)b->n * RQ_ENERGY_LEN) b->lastE.assign((size_t)b->n * RQ_ENERGY_LEN, 0.0);
+  if (b->march[0].n == 0) {  // nothing active: the cached energies are current
+    std::memcpy(out, b->lastE.data(), sizeof(double) * b->lastE.size());
+    return RQ_OK;
+  }
+  int frc = b_flush_any(b);
+  if (frc != RQ_OK) return frc;
   BCK(cudaMemsetAsync(b->dpd, 0, sizeof(double) * 4 * b->D, b->st));
   if (b->fp64) {
     using T = double;
@@ -701,6 +756,10 @@ extern "C" int rq_batch_energy(rq_batch* b, double* out) {
   for (int q = 0; q < b->n; ++q) {
     const BInst& I = b->hin[q];
     double* o = out + (size_t)q * RQ_ENERGY_LEN;
+    if (!b->active[q]) {  // instances dropped by solve keep their last energies
+      std::memcpy(o, &b->lastE[(size_t)q * RQ_ENERGY_LEN], sizeof(double) * RQ_ENERGY_LEN);
+      continue;
+    }
     std::memset(o, 0, sizeof(double) * RQ_ENERGY_LEN);
     for (int d = 0; d < I.nDom; ++d) {
       o[RQ_E_T] += pd[4 * (I.dom0 + d) + 1];
@@ -717,6 +776,7 @@ extern "C" int rq_batch_energy(rq_batch* b, double* out) {
       }
     o[RQ_E_KK] = ekk;
     o[RQ_E_TOTAL] = o[RQ_E_T] + o[RQ_E_EK] + o[RQ_E_EE] + ekk;
+    std::memcpy(&b->lastE[(size_t)q * RQ_ENERGY_LEN], o, sizeof(double) * RQ_ENERGY_LEN);
     if (!std::isfinite(o[RQ_E_TOTAL])) {
       b->last_error = "non-finite energy in instance " + std::to_string(q);
       return RQ_ENONFINITE;
@@ -727,6 +787,10 @@ extern "C" int rq_batch_energy(rq_batch* b, double* out) {
 
 extern "C" int rq_batch_forces(rq_batch* b, double* F) {
   if (!b || !F) return RQ_EINVAL;
+  for (char a : b->active)
+    if (!a) return rq_batch_set_active_all(b) != RQ_OK ? RQ_ECUDA : rq_batch_forces(b, F);
+  int frc = b_flush_any(b);
+  if (frc != RQ_OK) return frc;
   BCK(cudaMemsetAsync(b->dF, 0, sizeof(double) * 3 * b->A, b->st));
   if (b->fp64) {
     using T = double;
@@ -757,34 +821,122 @@ extern "C" int rq_batch_forces(rq_batch* b, double* F) {
   return RQ_OK;
 }
 
-extern "C" int rq_batch_solve(rq_batch* b, double tol_dE, int32_t max_steps, int32_t check_interval,
-                              int32_t* converged_at, double* E_final) {
-  if (!b || max_steps < 0 || check_interval <= 0) return RQ_EINVAL;
+__global__ void kb_widen(const float* __restrict__ a, double* __restrict__ d, long long n) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    d[q] = (double)a[q];
+}
+
+// A mixed batch switches every instance to FP64 fields for its final refinement: psi and P are
+// widened, K is recomputed in FP64, labels and W carry over.  The fp32 buffers stay allocated
+// until the batch is destroyed.
+static int b_promote(rq_batch* b) {
+  if (b->fp64) return RQ_OK;
+  int frc = b_flush_any(b);
+  if (frc != RQ_OK) return frc;
+  const size_t es = sizeof(double);
+  for (int q = 0; q < b->n; ++q) {
+    BInst& I = b->hin[q];
+    const size_t S3 = (size_t)I.g.S3;
+    void *U[2], *P[2], *K;
+    for (int k = 0; k < 2; ++k) {
+      BALLOC(U[k], S3 * es);
+      BALLOC(P[k], S3 * es);
+    }
+    BALLOC(K, S3 * es);
+    kb_widen<<<148 * 4, 256, 0, b->st>>>((const float*)I.U[b->cu], (double*)U[b->cu], (long long)S3);
+    kb_widen<<<148 * 4, 256, 0, b->st>>>((const float*)I.P[b->cp], (double*)P[b->cp], (long long)S3);
+    BCK(cudaGetLastError());
+    for (int k = 0; k < 2; ++k) { I.U[k] = U[k]; I.P[k] = P[k]; }
+    I.K = K;
+    for (int l = 0; l < I.nlev; ++l) {
+      const size_t s3 = (size_t)I.lg[l].S3;
+      if (l > 0) {
+        BALLOC(I.lP[l], s3 * es);
+        BALLOC(I.lf[l], s3 * es);
+      }
+      if (l < I.nlev - 1) BALLOC(I.lr[l], s3 * es);
+    }
+  }
+  BALLOC(b->scale, es * b->D);
+  BCK(cudaMemcpyAsync(b->din, b->hin.data(), sizeof(BInst) * b->n, cudaMemcpyHostToDevice, b->st));
+  b->fp64 = true;
+  b->promoted = true;
+  std::vector<char> keep = b->active;
+  b->active.assign(b->n, 1);  // K of every instance in FP64
+  int rc = build_plans(b);
+  if (rc != RQ_OK) return rc;
+  kb_potential<double><<<b->flat1.n, 256, 0, b->st>>>(b->din, b->flat1.d, b->cfg.sigma);
+  BCK(cudaGetLastError());
+  b->active = keep;
+  rc = build_plans(b);
+  if (rc != RQ_OK) return rc;
+  BCK(cudaStreamSynchronize(b->st));
+  return RQ_OK;
+}
+
+int rq_batch_set_active_all(rq_batch* b) {
+  b->active.assign(b->n, 1);
+  return build_plans(b);
+}
+
+// One converge-to-tol loop over the active instances; instances are dropped from the work lists
+// as they converge.  conv[q] receives the total step count at convergence.
+static int b_converge(rq_batch* b, std::vector<double> tol, int max_steps, int check, std::vector<int>& conv,
+                      int& taken) {
   std::vector<double> e((size_t)b->n * RQ_ENERGY_LEN), prev(b->n);
   int rc = rq_batch_energy(b, e.data());
   if (rc != RQ_OK) return rc;
-  std::vector<int> conv(b->n, -1);
   for (int q = 0; q < b->n; ++q) prev[q] = e[(size_t)q * RQ_ENERGY_LEN];
-  int taken = 0, left = b->n;
+  int left = 0;
+  for (int q = 0; q < b->n; ++q) left += b->active[q] ? 1 : 0;
   while (taken < max_steps && left > 0) {
-    const int n = std::min(check_interval, max_steps - taken);
+    const int n = std::min(check, max_steps - taken);
     if ((rc = rq_batch_step(b, n)) != RQ_OK) return rc;
     taken += n;
     if ((rc = rq_batch_energy(b, e.data())) != RQ_OK) return rc;
+    bool dropped = false;
     for (int q = 0; q < b->n; ++q) {
+      if (!b->active[q]) continue;
       const double E = e[(size_t)q * RQ_ENERGY_LEN];
-      if (conv[q] < 0 && std::fabs(E - prev[q]) < tol_dE) {
+      if (std::fabs(E - prev[q]) < tol[q]) {
         conv[q] = taken;
+        b->active[q] = 0;
+        dropped = true;
         left--;
       }
       prev[q] = E;
     }
-  }
-  for (int q = 0; q < b->n; ++q) {
-    if (converged_at) converged_at[q] = conv[q];
-    if (E_final) E_final[q] = prev[q];
+    if (dropped && (rc = build_plans(b)) != RQ_OK) return rc;
   }
   return RQ_OK;
+}
+
+extern "C" int rq_batch_solve(rq_batch* b, double tol_dE, int32_t max_steps, int32_t check_interval,
+                              int32_t* converged_at, double* E_final) {
+  if (!b || max_steps < 0 || check_interval <= 0) return RQ_EINVAL;
+  int rc, taken = 0;
+  std::vector<int> conv(b->n, -1);
+  if ((rc = rq_batch_set_active_all(b)) != RQ_OK) return rc;
+  if (!b->fp64) {
+    // fp32 fields stop improving near |dE| ~ 1e-8 |E|: converge to that floor in fp32 first ...
+    std::vector<double> e((size_t)b->n * RQ_ENERGY_LEN), tol(b->n);
+    if ((rc = rq_batch_energy(b, e.data())) != RQ_OK) return rc;
+    for (int q = 0; q < b->n; ++q) tol[q] = std::max(tol_dE, 3e-8 * std::fabs(e[(size_t)q * RQ_ENERGY_LEN]));
+    std::vector<int> c32(b->n, -1);
+    if ((rc = b_converge(b, tol, max_steps, check_interval, c32, taken)) != RQ_OK) return rc;
+    // ... then widen the batch to FP64 and refine to tol_dE (iterative refinement)
+    if ((rc = b_promote(b)) != RQ_OK) return rc;
+    if ((rc = rq_batch_set_active_all(b)) != RQ_OK) return rc;
+  }
+  std::vector<double> tol(b->n, tol_dE);
+  if ((rc = b_converge(b, tol, max_steps, check_interval, conv, taken)) != RQ_OK) return rc;
+  std::vector<double> e((size_t)b->n * RQ_ENERGY_LEN);
+  if ((rc = rq_batch_energy(b, e.data())) != RQ_OK) return rc;
+  for (int q = 0; q < b->n; ++q) {
+    if (converged_at) converged_at[q] = conv[q];
+    if (E_final) E_final[q] = e[(size_t)q * RQ_ENERGY_LEN];
+  }
+  return rq_batch_set_active_all(b);
 }
 
 extern "C" int rq_batch_info(const rq_batch* b, int32_t* n_inst, int64_t* total_points, int64_t* interior_points,

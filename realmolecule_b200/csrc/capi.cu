@@ -68,7 +68,9 @@ static void fill_defaults(rq_ctx* c) {
   const bool nm = f.flavor == RQ_FLAVOR_NEW;
   // the new flavour normalises every step: all-electron cores grow by e^{dt |eps|} per step
   if (f.norm_interval <= 0) f.norm_interval = nm ? 1 : 20;
-  if (f.poisson_interval <= 0) f.poisson_interval = sp || nm ? 2 : 1;
+  // new flavour: one V(1,1) every 4 steps (the Hartree potential changes slowly; measured to
+  // leave the iteration count and the converged energy unchanged against V(2,2) every 2 steps)
+  if (f.poisson_interval <= 0) f.poisson_interval = nm ? 4 : sp ? 2 : 1;
   if (f.label_interval <= 0) f.label_interval = sp ? 5 * f.norm_interval : 20;
   if (f.jacobi_per_step <= 0) f.jacobi_per_step = 2;
   if (f.steps_per_frame <= 0) {  // molecule.js:106
@@ -77,9 +79,9 @@ static void fill_defaults(rq_ctx* c) {
     f.steps_per_frame = nel <= 30 ? 50 : nel <= 100 ? 5 : 2;
   }
   if (f.vcycle_interval <= 0) f.vcycle_interval = 50;
-  if (f.mg_pre <= 0) f.mg_pre = 2;
-  if (f.mg_post <= 0) f.mg_post = 2;
-  if (f.mg_coarse_sweeps <= 0) f.mg_coarse_sweeps = 64;
+  if (f.mg_pre <= 0) f.mg_pre = nm ? 1 : 2;
+  if (f.mg_post <= 0) f.mg_post = nm ? 1 : 2;
+  if (f.mg_coarse_sweeps <= 0) f.mg_coarse_sweeps = 16;
   if (f.boundary_speed <= 0) f.boundary_speed = 0.5;
   if (f.curv_reg == 0) f.curv_reg = 0.15;  // molecule.js:34 default; a negative value switches it off
   if (f.curv_reg < 0) f.curv_reg = 0;
@@ -254,6 +256,10 @@ extern "C" int rq_get_info(const rq_ctx* c, rq_info* info) {
 
 extern "C" int rq_synchronize(rq_ctx* c) {
   if (!c) return RQ_EINVAL;
+  if (c->cfg.flavor == RQ_FLAVOR_NEW) {
+    int rc = nm_flush(c);  // device pointers from rq_get_info then hold the normalised psi
+    if (rc != RQ_OK) return rc;
+  }
   CK(cudaStreamSynchronize(c->st));
   return RQ_OK;
 }
@@ -379,7 +385,7 @@ extern "C" int rq_step(rq_ctx* c, int32_t n) {
     }
     // one aligned period: replay its CUDA graph (captured on first use for this buffer parity)
     const int labels_on = (lu <= 0 || c->steps_done < lu) ? 1 : 0;
-    const int key = c->cu | (c->cp << 1) | (c->cl << 2) | (labels_on << 3);
+    const int key = c->cu | (c->cp << 1) | (c->cl << 2) | (labels_on << 3) | ((c->nm_pending ? 1 : 0) << 4);
     if (!c->graph[key]) {
       const long long l0 = c->launches;
       CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
@@ -394,13 +400,14 @@ extern "C" int rq_step(rq_ctx* c, int32_t n) {
       e = cudaGraphInstantiate(&c->graph[key], gr, 0);
       cudaGraphDestroy(gr);
       CK(e);
-      c->graph_post[key] = c->cu | (c->cp << 1) | (c->cl << 2);
+      c->graph_post[key] = c->cu | (c->cp << 1) | (c->cl << 2) | ((c->nm_pending ? 1 : 0) << 4);
       c->graph_launches[key] = c->launches - l0;
       CK(cudaGraphLaunch(c->graph[key], c->st));
     } else {
       CK(cudaGraphLaunch(c->graph[key], c->st));
       const int post = c->graph_post[key];
       c->cu = post & 1; c->cp = (post >> 1) & 1; c->cl = (post >> 2) & 1;
+      c->nm_pending = (post >> 4) & 1;
       c->steps_done += period;
       c->launches += c->graph_launches[key];
     }
@@ -448,6 +455,7 @@ extern "C" int rq_upload_state(rq_ctx* c, const float* psi, const int32_t* label
     if (mj && (rc = mj_refresh_flags(c)) != RQ_OK) return rc;  // r_c-exclusion bits of the new labels
   }
   if (psi) {
+    c->nm_pending = false;
     CK(cudaMemcpyAsync(c->U[c->cu], psi, n * sizeof(float), cudaMemcpyHostToDevice, c->st));
     if (mj)  // molecule.js keeps the boundary values of psi (never rewritten): both buffers hold them
       CK(cudaMemcpyAsync(c->U[1 - c->cu], c->U[c->cu], n * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
@@ -466,6 +474,10 @@ extern "C" int rq_upload_state(rq_ctx* c, const float* psi, const int32_t* label
 
 extern "C" int rq_download_state(rq_ctx* c, float* psi, int32_t* label, float* W, float* P) {
   if (!c) return RQ_EINVAL;
+  if (c->cfg.flavor == RQ_FLAVOR_NEW && psi) {
+    int rc = nm_flush(c);
+    if (rc != RQ_OK) return rc;
+  }
   if (c->fp64 && (psi || P)) return rq_fail(c, RQ_EINVAL, "FP64 context: use rq_download_state_f64 for psi/P");
   const size_t n = (size_t)c->g.S3;
   if (psi) CK(cudaMemcpyAsync(psi, c->U[c->cu], n * sizeof(float), cudaMemcpyDeviceToHost, c->st));
@@ -483,6 +495,7 @@ extern "C" int rq_upload_state_f64(rq_ctx* c, const double* psi, const double* P
   if (!c->fp64) return rq_fail(c, RQ_EINVAL, "mixed-precision context: use rq_upload_state");
   const size_t n = (size_t)c->g.S3;
   if (psi) {
+    c->nm_pending = false;
     CK(cudaMemcpyAsync(c->U[c->cu], psi, n * sizeof(double), cudaMemcpyHostToDevice, c->st));
     CK(launch_zero_faces((double*)c->U[c->cu], c->g, c->st));
   }
@@ -496,6 +509,10 @@ extern "C" int rq_upload_state_f64(rq_ctx* c, const double* psi, const double* P
 
 extern "C" int rq_download_state_f64(rq_ctx* c, double* psi, double* P, double* K) {
   if (!c) return RQ_EINVAL;
+  if (psi) {
+    int rc = nm_flush(c);
+    if (rc != RQ_OK) return rc;
+  }
   if (!c->fp64) return rq_fail(c, RQ_EINVAL, "mixed-precision context: use rq_download_state");
   const size_t n = (size_t)c->g.S3;
   if (psi) CK(cudaMemcpyAsync(psi, c->U[c->cu], n * sizeof(double), cudaMemcpyDeviceToHost, c->st));

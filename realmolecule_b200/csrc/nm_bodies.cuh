@@ -27,6 +27,7 @@ template <> struct Ar<double> {
 
 constexpr int kNmFlatChunk = 16;     // points per thread of the flat (all S^3) bodies
 constexpr int kNmForceTile = 512;    // interior points staged per force tile
+constexpr int kCoarsestThreads = 256; // one block solves the coarsest level (<= 29^3 points)
 
 // ---------------------------------------------------------------------------------------
 // K = sum Z erf(r/(sqrt2 sigma))/r in FP64 (K(0) = Z sqrt(2/pi)/sigma); boundary planes 0.
@@ -92,11 +93,16 @@ __device__ __forceinline__ void nm_init_body(T* __restrict__ U, int* __restrict_
 
 // ITP update (same-label Neumann Laplacian) on the march tile (bx, by, bz); with ACC the FP64
 // norm of the new psi per label goes through the block table (caller inits and flushes it).
+// With a non-null `scale` the stored psi is one normalisation behind: every value read is first
+// multiplied by scale[label of the centre] (the same for every neighbour that is used, since only
+// same-label neighbours enter), which reproduces "normalise, then update" bit for bit without a
+// separate pass over psi.
 template <typename T, bool ACC>
 __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __restrict__ Unew, const T* __restrict__ K,
                                                const T* __restrict__ P, const int* __restrict__ label, const Geo& g,
                                                T half_dv, T dt, double h3, int nDom, double* __restrict__ norms,
-                                               DomTable<1, 128>& tab, int bx, int by, int bz) {
+                                               DomTable<1, 128>& tab, int bx, int by, int bz,
+                                               const T* __restrict__ scale = nullptr) {
   using A = Ar<T>;
   RunSum<1> rs;
   rs.reset();
@@ -112,14 +118,17 @@ __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __res
     for (int i = i0; i < iend; ++i, id += S2) {
       const T u_p = U[id + S2];
       const int l_p = label[id + S2];
-      const T a = (l_p == l_c) ? u_p : u_c;
-      const T b = (l_m == l_c) ? u_m : u_c;
-      const T c = (label[id + S] == l_c) ? U[id + S] : u_c;
-      const T d = (label[id - S] == l_c) ? U[id - S] : u_c;
-      const T e = (label[id + 1] == l_c) ? U[id + 1] : u_c;
-      const T f = (label[id - 1] == l_c) ? U[id - 1] : u_c;
-      const T lap = A::sub(A::add(A::add(A::add(A::add(A::add(a, b), c), d), e), f), A::mul(T(6), u_c));
-      const T out = A::add(A::add(u_c, A::mul(half_dv, lap)), A::mul(A::mul(dt, A::sub(K[id], A::mul(T(2), P[id]))), u_c));
+      const T sc = scale ? scale[min(max(l_c, 0), nDom - 1)] : T(1);
+      auto sv = [&](T v) { return scale ? A::mul(v, sc) : v; };
+      const T uc = sv(u_c);
+      const T a = (l_p == l_c) ? sv(u_p) : uc;
+      const T b = (l_m == l_c) ? sv(u_m) : uc;
+      const T c = (label[id + S] == l_c) ? sv(U[id + S]) : uc;
+      const T d = (label[id - S] == l_c) ? sv(U[id - S]) : uc;
+      const T e = (label[id + 1] == l_c) ? sv(U[id + 1]) : uc;
+      const T f = (label[id - 1] == l_c) ? sv(U[id - 1]) : uc;
+      const T lap = A::sub(A::add(A::add(A::add(A::add(A::add(a, b), c), d), e), f), A::mul(T(6), uc));
+      const T out = A::add(A::add(uc, A::mul(half_dv, lap)), A::mul(A::mul(dt, A::sub(K[id], A::mul(T(2), P[id]))), uc));
       Unew[id] = out;
       if (ACC) {
         const double r = (double)out * (double)out * h3;
@@ -128,7 +137,7 @@ __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __res
       u_m = u_c; u_c = u_p; l_m = l_c; l_c = l_p;
     }
   }
-  if (ACC) rs.finish(tab, norms);
+  if (ACC) rs.finish_warp(tab, norms);  // every lane of the (32 x 8) block reaches this point
 }
 
 // U *= scale[label] for labels in [0, nDom) over kNmFlatChunk*256 points from blk
@@ -203,9 +212,59 @@ __device__ __forceinline__ void nm_residual_body(const T* __restrict__ P, const 
   const long long S = g.S, S2 = g.S2;
   for (int i = i0; i < iend; ++i) {
     const long long id = (long long)i * S2 + (long long)j * S + k;
+    if (sizeof(T) == sizeof(float)) {
+      // fp32 fields: sum_6 P - 6 P cancels most of its digits (P is smooth), so the residual is
+      // formed in FP64 from the fp32 values and rounded once -- this is what lets the fp32
+      // multigrid reach the fp32 resolution of P instead of stalling at ~1e-4 relative
+      const double sd = (double)P[id + S2] + (double)P[id - S2] + (double)P[id + S] + (double)P[id - S] +
+                        (double)P[id + 1] + (double)P[id - 1];
+      r[id] = (T)((double)rhs_at<T, FINE>(f, id) + (sd - 6.0 * (double)P[id]) * (double)inv_h2);
+    } else {
+      const T s = A::add(A::add(A::add(A::add(A::add(P[id + S2], P[id - S2]), P[id + S]), P[id - S]), P[id + 1]), P[id - 1]);
+      r[id] = A::add(rhs_at<T, FINE>(f, id), A::mul(A::sub(s, A::mul(T(6), P[id])), inv_h2));
+    }
+  }
+}
+
+// the same residual at interior point number q (one point per thread: the level is small or
+// the march's per-plane latency chain would dominate)
+template <typename T, bool FINE>
+__device__ __forceinline__ void nm_residual_flat_body(const T* __restrict__ P, const T* __restrict__ f,
+                                                      T* __restrict__ r, const Geo& g, T inv_h2, long long q) {
+  using A = Ar<T>;
+  const int n = g.NN - 1;
+  if (q >= (long long)n * n * n) return;
+  const int qi = (int)q;
+  const int k = 1 + qi % n, j = 1 + (qi / n) % n, i = 1 + qi / (n * n);
+  const long long S = g.S, S2 = g.S2;
+  const long long id = (long long)i * S2 + (long long)j * S + k;
+  if (sizeof(T) == sizeof(float)) {
+    const double sd = (double)P[id + S2] + (double)P[id - S2] + (double)P[id + S] + (double)P[id - S] +
+                      (double)P[id + 1] + (double)P[id - 1];
+    r[id] = (T)((double)rhs_at<T, FINE>(f, id) + (sd - 6.0 * (double)P[id]) * (double)inv_h2);
+  } else {
     const T s = A::add(A::add(A::add(A::add(A::add(P[id + S2], P[id - S2]), P[id + S]), P[id - S]), P[id + 1]), P[id - 1]);
     r[id] = A::add(rhs_at<T, FINE>(f, id), A::mul(A::sub(s, A::mul(T(6), P[id])), inv_h2));
   }
+}
+
+// trilinear prolongation + correction at fine interior point number q
+template <typename T>
+__device__ __forceinline__ void nm_prolong_flat_body(const T* __restrict__ Ec, T* __restrict__ P, const Geo& g,
+                                                     const Geo& gc, long long q) {
+  using A = Ar<T>;
+  const int n = g.NN - 1;
+  if (q >= (long long)n * n * n) return;
+  const int qi = (int)q;
+  const int k = 1 + qi % n, j = 1 + (qi / n) % n, i = 1 + qi / (n * n);
+  const int ci = i >> 1, cj = j >> 1, ck = k >> 1, oi = i & 1, oj = j & 1, ok = k & 1;
+  T v = T(0);
+  for (int a = 0; a <= oi; ++a)
+    for (int b = 0; b <= oj; ++b)
+      for (int c = 0; c <= ok; ++c) v = A::add(v, Ec[(long long)(ci + a) * gc.S2 + (long long)(cj + b) * gc.S + (ck + c)]);
+  v = A::div(v, (T)((1 + oi) * (1 + oj) * (1 + ok)));
+  const long long id = (long long)i * g.S2 + (long long)j * g.S + k;
+  P[id] = A::add(P[id], v);
 }
 
 // full weighting (1/64)(8,4,2,1) at coarse interior point number q; loop order a, b, c
@@ -256,16 +315,16 @@ __device__ __forceinline__ void nm_coarsest_body(T* __restrict__ P, const T* __r
   double* sf = sm + g.S3;
   for (long long q = threadIdx.x; q < g.S3; q += blockDim.x) { sP[q] = (double)P[q]; sf[q] = (double)f[q]; }
   __syncthreads();
-  const int n = g.NN - 1;
-  const long long nint = (long long)n * n * n;
+  const int n = g.NN - 1, S = g.S, S2 = (int)g.S2;  // the coarsest level is at most 29^3 points
+  const int nint = n * n * n;
   for (int s = 0; s < sweeps; ++s)
     for (int color = 0; color < 2; ++color) {
-      for (long long q = threadIdx.x; q < nint; q += blockDim.x) {
-        const int k = 1 + (int)(q % n), j = 1 + (int)((q / n) % n), i = 1 + (int)(q / ((long long)n * n));
+      for (int q = threadIdx.x; q < nint; q += blockDim.x) {
+        const int k = 1 + q % n, j = 1 + (q / n) % n, i = 1 + q / (n * n);
         if (((i + j + k) & 1) != color) continue;
-        const long long id = (long long)i * g.S2 + (long long)j * g.S + k;
-        const double sum = __dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(sP[id + g.S2], sP[id - g.S2]), sP[id + g.S]),
-                                                        sP[id - g.S]), sP[id + 1]), sP[id - 1]);
+        const int id = i * S2 + j * S + k;
+        const double sum = __dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(sP[id + S2], sP[id - S2]), sP[id + S]),
+                                                        sP[id - S]), sP[id + 1]), sP[id - 1]);
         sP[id] = __ddiv_rn(__dadd_rn(sum, __dmul_rn(h2, sf[id])), 6.0);
       }
       __syncthreads();
@@ -304,7 +363,7 @@ __device__ __forceinline__ void nm_energy_body(const T* __restrict__ U, const T*
       rs.add(L, v, tab, pd);
     }
   }
-  rs.finish(tab, pd);
+  rs.finish_warp(tab, pd);
 }
 
 // level-set label update (molecule.js:426-540 rule) on psi of type T, march tile

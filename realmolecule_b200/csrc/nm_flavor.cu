@@ -112,22 +112,46 @@ static int nm_normalize_t(rq_ctx* c, bool accumulate) {
   }
   LAUNCH(RQ_KC_NORMALIZE, (2.0 * sizeof(T) + 4.0) * c->g.S3,
          nm_normalize<T>(U, c->lab[c->cl], c->dnorm, c->Zdom64, c->n_atoms, (T*)c->scale64, c->err, c->g, c->st));
+  c->nm_pending = false;
   return RQ_OK;
 }
+
+// Apply a pending per-domain normalisation to the stored psi (the update applies it on the
+// fly; the multigrid, the label pass and every readout need it materialised).
+template <typename T>
+static int nm_flush_t(rq_ctx* c) {
+  if (!c->nm_pending) return RQ_OK;
+  LAUNCH(RQ_KC_NORMALIZE, (2.0 * sizeof(T) + 4.0) * c->g.S3,
+         nm_apply<T>((T*)c->U[c->cu], c->lab[c->cl], (const T*)c->scale64, c->n_atoms, c->g, c->st));
+  c->nm_pending = false;
+  return RQ_OK;
+}
+
+int nm_flush(rq_ctx* c) { return c->fp64 ? nm_flush_t<double>(c) : nm_flush_t<float>(c); }
 
 template <typename T>
 static int nm_step_t(rq_ctx* c, int s) {
   const rq_config& f = c->cfg;
   int rc;
-  if (s % f.poisson_interval == 0 && (rc = nm_vcycle(c)) != RQ_OK) return rc;
+  if (s % f.poisson_interval == 0) {
+    if ((rc = nm_flush_t<T>(c)) != RQ_OK) return rc;
+    if ((rc = nm_vcycle(c)) != RQ_OK) return rc;
+  }
   const bool norm = s % f.norm_interval == 0;
   if (norm) CK(cudaMemsetAsync(c->dnorm, 0, sizeof(double) * c->n_atoms, c->st));
   LAUNCH(RQ_KC_UPDATE, (4.0 * sizeof(T) + 4.0) * interior(c->g),
          nm_update<T>((const T*)c->U[c->cu], (T*)c->U[1 - c->cu], (const T*)c->K, (const T*)c->P[c->cp], c->lab[c->cl],
-                      c->g, (T)c->half_dv, (T)c->dt, c->h3, c->n_atoms, norm ? c->dnorm : nullptr, c->st));
+                      c->g, (T)c->half_dv, (T)c->dt, c->h3, c->n_atoms, norm ? c->dnorm : nullptr, c->st,
+                      c->nm_pending ? (const T*)c->scale64 : nullptr));
   c->cu ^= 1;
-  if (norm && (rc = nm_normalize_t<T>(c, false)) != RQ_OK) return rc;
+  c->nm_pending = false;  // the update consumed the pending scale
+  if (norm) {  // the scale of this step is applied by the next update (or a flush)
+    LAUNCH(RQ_KC_NORMALIZE, 12.0 * c->n_atoms,
+           nm_norm_scale<T>(c->dnorm, c->Zdom64, c->n_atoms, (T*)c->scale64, c->err, c->st));
+    c->nm_pending = true;
+  }
   if (s % f.label_interval == 0 && (f.label_until <= 0 || s <= f.label_until)) {
+    if ((rc = nm_flush_t<T>(c)) != RQ_OK) return rc;
     LAUNCH(RQ_KC_LABELS, (sizeof(T) + 12.0) * interior(c->g),
            nm_evolve<T>(c->lab[c->cl], c->lab[1 - c->cl], (const T*)c->U[c->cu], c->W, c->g, f.boundary_speed, f.curv_reg,
                         c->st));
@@ -221,6 +245,8 @@ void nm_nuclear_terms(rq_ctx* c, double* E, double* F) {
 
 int nm_energy(rq_ctx* c, double* out, double* per_domain) {
   const int n = c->n_atoms;
+  int frc = nm_flush(c);
+  if (frc != RQ_OK) return frc;
   CK(cudaMemsetAsync(c->dpd, 0, sizeof(double) * 4 * n, c->st));
   if (c->fp64)
     LAUNCH(RQ_KC_ENERGY, 36 * interior(c->g),
@@ -250,6 +276,8 @@ int nm_energy(rq_ctx* c, double* out, double* per_domain) {
 int nm_forces(rq_ctx* c, int method, double* F) {
   if (method != RQ_FORCE_HF && method != RQ_FORCE_ADJOINT) return RQ_ENOTSUP;
   const int n = c->n_atoms;
+  int frc = nm_flush(c);
+  if (frc != RQ_OK) return frc;
   CK(cudaMemsetAsync(c->dF, 0, sizeof(double) * 3 * n, c->st));
   if (c->fp64)
     LAUNCH(RQ_KC_FORCES, 8 * interior(c->g),

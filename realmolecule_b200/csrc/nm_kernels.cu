@@ -22,14 +22,14 @@ __global__ void __launch_bounds__(256) k_nm_init(T* U, int* label, const float4*
 
 template <typename T, bool ACC>
 __global__ void __launch_bounds__(256) k_nm_update(const T* U, T* Unew, const T* K, const T* P, const int* label, Geo g,
-                                                   T half_dv, T dt, double h3, int nDom, double* norms) {
+                                                   T half_dv, T dt, double h3, int nDom, double* norms, const T* scale) {
   __shared__ DomTable<1, 128> tab;
   if (ACC) {
     dom_table_init(tab);
     __syncthreads();
   }
   nm_update_body<T, ACC>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, norms, tab, blockIdx.x, blockIdx.y,
-                         blockIdx.z);
+                         blockIdx.z, scale);
   if (ACC) {
     __syncthreads();
     dom_table_flush(tab, norms);
@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(256) k_nm_rbgs(T* P, const T* f, Geo g, T h2, 
 
 template <typename T, bool FINE>
 __global__ void __launch_bounds__(256) k_nm_residual(const T* P, const T* f, T* r, Geo g, T inv_h2) {
-  nm_residual_body<T, FINE>(P, f, r, g, inv_h2, blockIdx.x, blockIdx.y, blockIdx.z);
+  nm_residual_flat_body<T, FINE>(P, f, r, g, inv_h2, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 template <typename T>
@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(256) k_nm_restrict(const T* fine, T* coarse, G
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_nm_prolong(const T* Ec, T* P, Geo g, Geo gc) {
-  nm_prolong_body<T>(Ec, P, g, gc, blockIdx.x, blockIdx.y, blockIdx.z);
+  nm_prolong_flat_body<T>(Ec, P, g, gc, (long long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 template <typename T>
@@ -136,13 +136,19 @@ cudaError_t nm_init(T* U, int* label, const float4* seeds, int nSeed, const Geo&
 }
 template <typename T>
 cudaError_t nm_update(const T* U, T* Unew, const T* K, const T* P, const int* label, const Geo& g, T half_dv, T dt,
-                      double h3, int nDom, double* norms, cudaStream_t st) {
+                      double h3, int nDom, double* norms, cudaStream_t st, const T* scale) {
   if (g.NN < 2) return cudaSuccess;
   if (norms)
-    k_nm_update<T, true><<<march_grid(g), march_block(), 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, norms);
+    k_nm_update<T, true><<<march_grid(g), march_block(), 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, norms,
+                                                                   scale);
   else
     k_nm_update<T, false><<<march_grid(g), march_block(), 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom,
-                                                                    nullptr);
+                                                                    nullptr, scale);
+  return cudaGetLastError();
+}
+template <typename T>
+cudaError_t nm_apply(T* U, const int* label, const T* scale, int nDom, const Geo& g, cudaStream_t st) {
+  k_nm_apply_scale<T><<<nblk(g.S3, 256 * kNmFlatChunk), 256, 0, st>>>(U, label, scale, g.S3, nDom);
   return cudaGetLastError();
 }
 template <typename T>
@@ -175,10 +181,11 @@ cudaError_t nm_rbgs(T* P, const T* f, bool fine, const Geo& g, double h2, int co
 }
 template <typename T>
 cudaError_t nm_residual(const T* P, const T* f, bool fine, T* r, const Geo& g, double inv_h2, cudaStream_t st) {
+  const long long n = g.NN - 1;
   if (fine)
-    k_nm_residual<T, true><<<march_grid(g), march_block(), 0, st>>>(P, f, r, g, (T)inv_h2);
+    k_nm_residual<T, true><<<nblk(n * n * n), 256, 0, st>>>(P, f, r, g, (T)inv_h2);
   else
-    k_nm_residual<T, false><<<march_grid(g), march_block(), 0, st>>>(P, f, r, g, (T)inv_h2);
+    k_nm_residual<T, false><<<nblk(n * n * n), 256, 0, st>>>(P, f, r, g, (T)inv_h2);
   return cudaGetLastError();
 }
 template <typename T>
@@ -189,7 +196,8 @@ cudaError_t nm_restrict(const T* fine, T* coarse, const Geo& g, const Geo& gc, c
 }
 template <typename T>
 cudaError_t nm_prolong(const T* Ec, T* P, const Geo& g, const Geo& gc, cudaStream_t st) {
-  k_nm_prolong<T><<<march_grid(g), march_block(), 0, st>>>(Ec, P, g, gc);
+  const long long n = g.NN - 1;
+  k_nm_prolong<T><<<nblk(n * n * n), 256, 0, st>>>(Ec, P, g, gc);
   return cudaGetLastError();
 }
 template <typename T>
@@ -198,7 +206,7 @@ cudaError_t nm_coarsest(T* P, const T* f, const Geo& g, double h2, int sweeps, c
   if (smem > 200 * 1024) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(k_nm_coarsest<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  k_nm_coarsest<T><<<1, 1024, smem, st>>>(P, f, g, h2, sweeps);
+  k_nm_coarsest<T><<<1, kCoarsestThreads, smem, st>>>(P, f, g, h2, sweeps);
   return cudaGetLastError();
 }
 template <typename T>
@@ -239,7 +247,8 @@ cudaError_t nm_add(T* K, const T* v, long long n, cudaStream_t st) {
   template cudaError_t nm_potential<T>(T*, const double*, int, const Geo&, double, double, cudaStream_t);           \
   template cudaError_t nm_init<T>(T*, int*, const float4*, int, const Geo&, float, cudaStream_t);                   \
   template cudaError_t nm_update<T>(const T*, T*, const T*, const T*, const int*, const Geo&, T, T, double, int,     \
-                                    double*, cudaStream_t);                                                          \
+                                    double*, cudaStream_t, const T*);                                                \
+  template cudaError_t nm_apply<T>(T*, const int*, const T*, int, const Geo&, cudaStream_t);                        \
   template cudaError_t nm_normalize<T>(T*, const int*, const double*, const double*, int, T*, int*, const Geo&,     \
                                        cudaStream_t);                                                                \
   template cudaError_t nm_norm_scale<T>(const double*, const double*, int, T*, int*, cudaStream_t);                 \

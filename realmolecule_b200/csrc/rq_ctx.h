@@ -58,6 +58,7 @@ struct rq_ctx {
   void* seeds = nullptr;      // new flavour: float4 (x, y, z, entry) per domain seed
   void* scale64 = nullptr;    // new flavour: per-domain scale (T)
   void* Kext = nullptr;       // new flavour: external potential added to K (T), or null
+  bool nm_pending = false;    // new flavour: psi awaits scale64 (applied by the next update or a flush)
   float* Zdom = nullptr;      // domain charge per label (f32)
   double* Zdom64 = nullptr;
 
@@ -76,9 +77,9 @@ struct rq_ctx {
 
   // CUDA graphs of one schedule period, keyed by buffer parity (cu, cp, cl) and whether the
   // label updates of the period are active (label_until)
-  cudaGraphExec_t graph[16] = {};
-  int graph_post[16] = {};
-  long long graph_launches[16] = {};
+  cudaGraphExec_t graph[32] = {};
+  int graph_post[32] = {};
+  long long graph_launches[32] = {};
 
   // launch accounting and the optional per-kernel profile
   long long launches = 0;

@@ -26,4 +26,5 @@ int nm_energy(rq_ctx* c, double* out, double* per_domain);
 int nm_forces(rq_ctx* c, int method, double* F);
 int nm_set_atoms(rq_ctx* c);
 int nm_set_external(rq_ctx* c, const double* v);
+int nm_flush(rq_ctx* c);  // materialise a pending per-domain normalisation of psi
 void nm_nuclear_terms(rq_ctx* c, double* E, double* F);

@@ -122,6 +122,25 @@ struct RunSum {
   __device__ __forceinline__ void finish(DomTable<NQ, NSLOT>& t, double* global) {
     if (label >= 0) dom_table_add(t, label, v, global);
   }
+  // Same as finish, but must be called by every lane of the warp together: lanes holding the
+  // same label first combine their sums with shuffles, so one lane per distinct label touches
+  // the shared table (neighbouring k values almost always share a label).
+  template <int NSLOT>
+  __device__ __forceinline__ void finish_warp(DomTable<NQ, NSLOT>& t, double* global) {
+    const unsigned peers = __match_any_sync(0xffffffffu, label);
+    const int lane = threadIdx.x & 31;
+    double s[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) s[q] = 0.0;
+    for (int l = 0; l < 32; ++l) {
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        const double x = __shfl_sync(0xffffffffu, v[q], l);
+        if ((peers >> l) & 1u) s[q] += x;
+      }
+    }
+    if (label >= 0 && lane == __ffs(peers) - 1) dom_table_add(t, label, s, global);
+  }
 };
 
 }  // namespace rq

@@ -44,12 +44,17 @@ def test_batch_matches_single_contexts(precision):
         np.testing.assert_allclose(Fb[q], F, rtol=1e-6, atol=1e-8)
 
 
-def test_batch_solve_reports_convergence_per_instance():
+def test_mixed_solve_matches_fp64_solve_to_1e6_ha():
+    """The mixed solve (fp32 to its noise floor, then FP64 refinement of the same batch) reaches the
+    FP64 solve's converged energies within 1e-6 Ha, instance by instance."""
     from realmolecule_b200.batch import Batch
-    b = Batch(instances(), precision="mixed", label_until=200)
-    b.initialize()
-    conv, E = b.solve(1e-6, 20000, 100)
-    assert (conv > 0).all(), conv
-    assert np.isfinite(E).all()
-    info = b.info()
-    assert info["instances"] == 4 and info["kernel_launches"] > 0
+    E = {}
+    for p in ("mixed", "fp64"):
+        b = Batch(instances(), precision=p, label_until=200)
+        b.initialize()
+        b.step(200)
+        conv, E[p] = b.solve(1e-8, 40000, 100)
+        assert (conv > 0).all(), (p, conv)
+        info = b.info()
+        assert info["instances"] == 4 and info["kernel_launches"] > 0
+    assert np.max(np.abs(E["mixed"] - E["fp64"])) < 1e-6, (E["mixed"], E["fp64"])
