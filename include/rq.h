@@ -61,7 +61,9 @@ typedef struct rq_config {
   int32_t NN;               /* grid intervals per axis (USER_NN / gridN); S = NN+1 */
   int32_t flavor;           /* rq_flavor */
   int32_t precision;        /* rq_precision (RQ_PREC_FP64 only with RQ_FLAVOR_NEW) */
-  int32_t norm_interval;    /* normalise every n steps (solver.py 20, molecule.js NORM_INTERVAL 20) */
+  int32_t norm_interval;    /* normalise every n steps (solver.py 20, molecule.js NORM_INTERVAL 20); new
+                               flavour: also always before each V-cycle and label pass (default
+                               poisson_interval) */
   double screen;            /* box edge in bohr (USER_SCREEN / screen); h = screen/NN */
   double dv;                /* dt = dv*h^2; <=0 -> flavour table (molecule.js:78, solver.py:342-351) */
   int32_t poisson_interval; /* solver.py: Poisson step every 2; new: one V-cycle every n steps (4) */

@@ -449,12 +449,14 @@ class MoleculeJsDriver:
 class NewMethodDriver:
     """FP64 restatement of the new flavour's schedule (Gaussian nuclei of width sigma, red-black
     multigrid V-cycle every ``poisson_interval`` steps, ITP update, FP64 normalisation to the
-    domain charges every ``norm_interval`` steps, level-set labels every ``label_interval``).
+    domain charges after every ``norm_interval``-th update and after each update that precedes a
+    V-cycle or a label pass, level-set labels every ``label_interval``).  Readouts (energy,
+    forces, ``state``) first normalise psi when updates ran since the last normalisation.
 
     ``rows`` use the flavour's idiom: nuclei have Z_nuc > 0, domains have Z > 0 (their position
     is the seed of the initial state).  Positions are grid units (x = i*h)."""
 
-    def __init__(self, NN, screen, rows, dv=0.2, sigma=None, poisson_interval=4, norm_interval=1, label_interval=20,
+    def __init__(self, NN, screen, rows, dv=0.2, sigma=None, poisson_interval=4, norm_interval=None, label_interval=20,
                  levels=None, pre=1, post=1, coarse_sweeps=16, boundary_speed=0.5, curv_reg=0.15, label_until=0):
         self.NN, self.S = NN, NN + 1
         self.S3 = self.S ** 3
@@ -464,7 +466,8 @@ class NewMethodDriver:
         self.n = len(rows)
         self.dv = dv
         self.half_dv, self.dt = 0.5 * dv, dv * self.h * self.h
-        self.pi_, self.ni, self.li = poisson_interval, norm_interval, label_interval
+        self.pi_, self.ni, self.li = poisson_interval, norm_interval or poisson_interval, label_interval
+        self.age = 0  # updates since the last normalisation
         if levels is None:
             levels, nn = 1, NN
             while nn % 2 == 0 and nn // 2 >= 6:
@@ -518,6 +521,16 @@ class NewMethodDriver:
     def normalize(self):
         _, pd = self.domain_sums()
         O().nm_normalize(self.U, self.label, self.S3, self.n, self.Zdom, np.ascontiguousarray(pd[:, 0]))
+        self.age = 0
+
+    def ready(self):
+        if self.age:
+            self.normalize()
+
+    def state(self):
+        """(psi, label, P) as readouts see them (psi normalised)."""
+        self.ready()
+        return self.U, self.label, self.P
 
     def vcycle(self):
         O().nm_vcycle(self.P, self.U, self.S, self.h, self.levels, self.pre, self.post, self.cs)
@@ -529,15 +542,22 @@ class NewMethodDriver:
             self.vcycle()
         O().nm_update(self.U, self.U2, self.K, self.P, self.label, self.S, self.half_dv, self.dt)
         self.U, self.U2 = self.U2, self.U
-        if s % self.ni == 0:
+        label_step = s % self.li == 0 and (self.label_until <= 0 or s <= self.label_until)
+        if (s + 1) % self.ni == 0 or (s + 1) % self.pi_ == 0 or label_step:
             self.normalize()
-        if s % self.li == 0 and (self.label_until <= 0 or s <= self.label_until):
+        else:
+            self.age += 1
+        if label_step:
             O().nm_evolve(self.label, self.label2, self.U, self.W, self.S, float(np.float32(self.dt_w)),
                           float(np.float32(self.curv)))
             self.label, self.label2 = self.label2, self.label
 
     def energy(self):
+        self.ready()
         out, pd = self.domain_sums()
+        # partials of the exactly normalised domains (each is linear in its density for this P)
+        w = np.where((self.Zdom > 0) & (pd[:, 0] > 0), self.Zdom / np.where(pd[:, 0] > 0, pd[:, 0], 1.0), 1.0)
+        out = np.array([(w * pd[:, 1]).sum(), (w * pd[:, 2]).sum(), (w * pd[:, 3]).sum()])
         xyz, Z = self.nuclei()
         xyz = xyz.reshape(-1, 3)
         ekk = 0.0
@@ -548,6 +568,7 @@ class NewMethodDriver:
         return {"T": out[0], "EK": out[1], "EE": out[2], "KK": ekk, "E": out.sum() + ekk, "per_domain": pd}
 
     def forces(self):
+        self.ready()
         xyz, Z = self.nuclei()
         F = np.zeros(self.n * 3)
         O().nm_force(self.U, xyz, Z, self.n, self.S, self.h, self.sigma, F)

@@ -47,12 +47,14 @@ struct BItem {
 };
 
 // ---------------------------------------------------------------------------------------
-// batched kernels: block b works on items[b]
+// batched kernels: block b works on items[b].  Each copies its instance's geometry into
+// registers first: through a reference into the instance table the compiler would re-read it
+// after every store, as it cannot prove the field pointers do not alias the table.
 // ---------------------------------------------------------------------------------------
 template <typename T, bool ACC>
 __global__ void __launch_bounds__(256) kb_update(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cu,
                                                  int cp, int cl, T half_dv, T dt, double* __restrict__ norms,
-                                                 const T* __restrict__ scale) {
+                                                 const double* __restrict__ scale) {
   __shared__ DomTable<1, 128> tab;
   const BItem it = items[blockIdx.x];
   const BInst& I = ins[it.inst];
@@ -61,7 +63,8 @@ __global__ void __launch_bounds__(256) kb_update(const BInst* __restrict__ ins, 
     dom_table_init(tab);
     __syncthreads();
   }
-  nm_update_body<T, ACC>((const T*)I.U[cu], (T*)I.U[1 - cu], (const T*)I.K, (const T*)I.P[cp], I.lab[cl], I.g, half_dv,
+  const Geo g = I.g;
+  nm_update_body<T, ACC>((const T*)I.U[cu], (T*)I.U[1 - cu], (const T*)I.K, (const T*)I.P[cp], I.lab[cl], g, half_dv,
                          dt, I.h * I.h * I.h, I.nDom, nrm, tab, it.bx, it.by, it.bz, scale ? scale + I.dom0 : nullptr);
   if (ACC) {
     __syncthreads();
@@ -71,7 +74,7 @@ __global__ void __launch_bounds__(256) kb_update(const BInst* __restrict__ ins, 
 
 template <typename T>
 __global__ void __launch_bounds__(256) kb_apply_scale(const BInst* __restrict__ ins, const BItem* __restrict__ items,
-                                                      int cu, int cl, const T* __restrict__ scale) {
+                                                      int cu, int cl, const double* __restrict__ scale) {
   const BItem it = items[blockIdx.x];
   const BInst& I = ins[it.inst];
   nm_apply_scale_body<T>((T*)I.U[cu], I.lab[cl], scale + I.dom0, I.g.S3, I.nDom, it.bx);
@@ -97,7 +100,8 @@ __global__ void __launch_bounds__(256) kb_rbgs(const BInst* __restrict__ ins, co
   const BInst& I = ins[it.inst];
   T* P = FINE ? (T*)I.P[cp] : (T*)I.lP[lev];
   const T* f = FINE ? (const T*)I.U[cu] : (const T*)I.lf[lev];
-  nm_rbgs_body<T, FINE>(P, f, I.lg[lev], (T)(I.lh[lev] * I.lh[lev]), color, it.bx, it.by, it.bz);
+  const Geo g = I.lg[lev];
+  nm_rbgs_body<T, FINE>(P, f, g, (T)(I.lh[lev] * I.lh[lev]), color, it.bx, it.by, it.bz);
 }
 
 template <typename T, bool FINE>
@@ -107,8 +111,8 @@ __global__ void __launch_bounds__(256) kb_residual(const BInst* __restrict__ ins
   const BInst& I = ins[it.inst];
   const T* P = FINE ? (const T*)I.P[cp] : (const T*)I.lP[lev];
   const T* f = FINE ? (const T*)I.U[cu] : (const T*)I.lf[lev];
-  nm_residual_flat_body<T, FINE>(P, f, (T*)I.lr[lev], I.lg[lev], (T)(1.0 / (I.lh[lev] * I.lh[lev])),
-                                 (long long)it.bx * blockDim.x + threadIdx.x);
+  const Geo g = I.lg[lev];
+  nm_residual_rows_body<T, FINE>(P, f, (T*)I.lr[lev], g, (T)(1.0 / (I.lh[lev] * I.lh[lev])), it.bx, it.by, it.bz);
 }
 
 template <typename T>
@@ -116,17 +120,21 @@ __global__ void __launch_bounds__(256) kb_restrict(const BInst* __restrict__ ins
                                                    int lev) {
   const BItem it = items[blockIdx.x];
   const BInst& I = ins[it.inst];
-  nm_restrict_body<T>((const T*)I.lr[lev], (T*)I.lf[lev + 1], I.lg[lev], I.lg[lev + 1],
-                      (long long)it.bx * blockDim.x + threadIdx.x);
+  const Geo g = I.lg[lev], gc = I.lg[lev + 1];
+  nm_restrict_body<T>((const T*)I.lr[lev], (T*)I.lf[lev + 1], g, gc, (long long)it.bx * blockDim.x + threadIdx.x);
 }
 
-// zero the correction of level lev (flat blocks of 256 points)
+// zero the correction of level lev (flat blocks of 256 * kNmFlatChunk points)
 template <typename T>
 __global__ void __launch_bounds__(256) kb_zero(const BInst* __restrict__ ins, const BItem* __restrict__ items, int lev) {
   const BItem it = items[blockIdx.x];
   const BInst& I = ins[it.inst];
-  const long long id = (long long)it.bx * blockDim.x + threadIdx.x;
-  if (id < I.lg[lev].S3) ((T*)I.lP[lev])[id] = T(0);
+  const long long S3 = I.lg[lev].S3, base = (long long)it.bx * blockDim.x * kNmFlatChunk;
+  T* p = (T*)I.lP[lev];
+  for (int q = 0; q < kNmFlatChunk; ++q) {
+    const long long id = base + (long long)q * blockDim.x + threadIdx.x;
+    if (id < S3) p[id] = T(0);
+  }
 }
 
 template <typename T>
@@ -135,8 +143,8 @@ __global__ void __launch_bounds__(256) kb_prolong(const BInst* __restrict__ ins,
   const BItem it = items[blockIdx.x];
   const BInst& I = ins[it.inst];
   T* P = lev == 0 ? (T*)I.P[cp] : (T*)I.lP[lev];
-  nm_prolong_flat_body<T>((const T*)I.lP[lev + 1], P, I.lg[lev], I.lg[lev + 1],
-                          (long long)it.bx * blockDim.x + threadIdx.x);
+  const Geo g = I.lg[lev], gc = I.lg[lev + 1];
+  nm_prolong_rows_body<T>((const T*)I.lP[lev + 1], P, g, gc, it.bx, it.by, it.bz);
 }
 
 template <typename T>
@@ -156,8 +164,9 @@ __global__ void __launch_bounds__(256) kb_energy(const BInst* __restrict__ ins, 
   const BInst& I = ins[it.inst];
   dom_table_init(tab);
   __syncthreads();
-  nm_energy_body<T>((const T*)I.U[cu], (const T*)I.K, (const T*)I.P[cp], I.lab[cl], I.g, I.h, I.nDom, pd + 4 * I.dom0,
-                    tab, it.bx, it.by, it.bz);
+  const Geo g = I.g;
+  nm_energy_body<T>((const T*)I.U[cu], (const T*)I.K, (const T*)I.P[cp], I.lab[cl], g, I.h, I.nDom, pd + 4 * I.dom0, tab,
+                    it.bx, it.by, it.bz);
   __syncthreads();
   dom_table_flush(tab, pd + 4 * I.dom0);
 }
@@ -167,7 +176,8 @@ __global__ void __launch_bounds__(256) kb_evolve(const BInst* __restrict__ ins, 
                                                  int cl, T dt_w, T curv) {
   const BItem it = items[blockIdx.x];
   const BInst& I = ins[it.inst];
-  nm_evolve_body<T>(I.lab[cl], I.lab[1 - cl], (const T*)I.U[cu], I.W, I.g, dt_w, curv, it.bx, it.by, it.bz);
+  const Geo g = I.g;
+  nm_evolve_body<T>(I.lab[cl], I.lab[1 - cl], (const T*)I.U[cu], I.W, g, dt_w, curv, it.bx, it.by, it.bz);
 }
 
 template <typename T>
@@ -221,7 +231,7 @@ struct rq_batch {
   int maxlev = 0;
   // work lists
   struct Plan { BItem* d = nullptr; int n = 0, cap = 0; };
-  Plan march[kMaxLev], rbgs[kMaxLev], restr[kMaxLev], zero[kMaxLev], coarse[kMaxLev], prol[kMaxLev];
+  Plan march[kMaxLev], rbgs[kMaxLev], restr[kMaxLev], zero[kMaxLev], coarse[kMaxLev];
   size_t coarse_smem[kMaxLev] = {};
   Plan flat16, flat1, force;
   cudaStream_t st = nullptr, own = nullptr;
@@ -233,6 +243,7 @@ struct rq_batch {
   std::vector<char> active;       // instances still being stepped (solve drops converged ones)
   std::vector<double> lastE;      // last energies per instance (n x RQ_ENERGY_LEN)
   bool pending = false;           // psi awaits the per-domain scale (applied by the next update or a flush)
+  int age = 0;                    // updates since psi was last normalised (0: normalised or pending)
   bool promoted = false;          // a mixed batch switched to FP64 for its final refinement
   std::string last_error;
 };
@@ -281,7 +292,7 @@ static int build_plans(rq_batch* b) {
   const int n = b->n;
   // work lists
   for (int l = 0; l < b->maxlev; ++l) {
-    std::vector<BItem> m, r, rs, z, c, p;
+    std::vector<BItem> m, r, rs, z, c;
     for (int q = 0; q < n; ++q) {
       const BInst& I = b->hin[q];
       if (l >= I.nlev || !b->active[q]) continue;
@@ -292,19 +303,18 @@ static int build_plans(rq_batch* b) {
         continue;
       }
       const int nn = I.lg[l].NN - 1;
-      for (int zz = 0; zz < nn; ++zz)
+      for (int zz = 0; zz < (nn + kNmRowPlanes - 1) / kNmRowPlanes; ++zz)
         for (int y = 0; y < (nn + 7) / 8; ++y)
           for (int x = 0; x < (nn + 63) / 64; ++x) r.push_back({q, x, y, zz});
       const long long nc = (long long)(I.lg[l + 1].NN - 1) * (I.lg[l + 1].NN - 1) * (I.lg[l + 1].NN - 1);
       for (long long x = 0; x < (nc + 255) / 256; ++x) rs.push_back({q, (int)x, 0, 0});
-      for (long long x = 0; x < (I.lg[l + 1].S3 + 255) / 256; ++x) z.push_back({q, (int)x, 0, 0});
-      const long long ni = (long long)nn * nn * nn;
-      for (long long x = 0; x < (ni + 255) / 256; ++x) p.push_back({q, (int)x, 0, 0});
+      for (long long x = 0; x < (I.lg[l + 1].S3 + 256 * kNmFlatChunk - 1) / (256 * kNmFlatChunk); ++x)
+        z.push_back({q, (int)x, 0, 0});
     }
     int rc;
     if ((rc = upload_plan(b, b->march[l], m)) || (rc = upload_plan(b, b->rbgs[l], r)) ||
         (rc = upload_plan(b, b->restr[l], rs)) || (rc = upload_plan(b, b->zero[l], z)) ||
-        (rc = upload_plan(b, b->coarse[l], c)) || (rc = upload_plan(b, b->prol[l], p)))
+        (rc = upload_plan(b, b->coarse[l], c)))
       return rc;
   }
   std::vector<BItem> f16, f1, fo;
@@ -354,7 +364,7 @@ static int build(rq_batch* b) {
   BALLOC(b->dnorm, sizeof(double) * b->D);
   BALLOC(b->dpd, sizeof(double) * 4 * b->D);
   BALLOC(b->Zdom, sizeof(double) * b->D);
-  BALLOC(b->scale, es * b->D);
+  BALLOC(b->scale, sizeof(double) * b->D);
   BALLOC(b->dF, sizeof(double) * 3 * b->A);
   BALLOC(b->at_all, sizeof(double) * 4 * b->A);
   BALLOC(b->seeds_all, sizeof(float4) * b->A);
@@ -440,9 +450,9 @@ static int b_vcycle(rq_batch* b) {
         BL("rbgs");
       }
     if (l == 0)
-      kb_residual<T, true><<<b->prol[l].n, 256, 0, b->st>>>(b->din, b->prol[l].d, l, b->cu, b->cp);
+      kb_residual<T, true><<<b->rbgs[l].n, dim3(32, 8), 0, b->st>>>(b->din, b->rbgs[l].d, l, b->cu, b->cp);
     else
-      kb_residual<T, false><<<b->prol[l].n, 256, 0, b->st>>>(b->din, b->prol[l].d, l, b->cu, b->cp);
+      kb_residual<T, false><<<b->rbgs[l].n, dim3(32, 8), 0, b->st>>>(b->din, b->rbgs[l].d, l, b->cu, b->cp);
     BL("residual");
     kb_restrict<T><<<b->restr[l].n, 256, 0, b->st>>>(b->din, b->restr[l].d, l);
     BL("restrict");
@@ -451,7 +461,7 @@ static int b_vcycle(rq_batch* b) {
   }
   for (int l = b->maxlev - 2; l >= 0; --l) {
     if (!b->rbgs[l].n) continue;
-    kb_prolong<T><<<b->prol[l].n, 256, 0, b->st>>>(b->din, b->prol[l].d, l, b->cp);
+    kb_prolong<T><<<b->rbgs[l].n, dim3(32, 8), 0, b->st>>>(b->din, b->rbgs[l].d, l, b->cp);
     BL("prolong");
     for (int s = 0; s < post; ++s)
       for (int color = 0; color < 2; ++color) {
@@ -473,11 +483,12 @@ static int b_normalize(rq_batch* b, bool accumulate) {
     kb_norms<T><<<b->flat16.n, 256, 0, b->st>>>(b->din, b->flat16.d, b->cu, b->cl, b->dnorm);
     BL("norms");
   }
-  BCK(nm_norm_scale<T>(b->dnorm, b->Zdom, b->D, (T*)b->scale, b->err, b->st));
+  BCK(nm_norm_scale<T>(b->dnorm, b->Zdom, b->D, (double*)b->scale, b->err, b->st));
   b->launches++;
-  kb_apply_scale<T><<<b->flat16.n, 256, 0, b->st>>>(b->din, b->flat16.d, b->cu, b->cl, (const T*)b->scale);
+  kb_apply_scale<T><<<b->flat16.n, 256, 0, b->st>>>(b->din, b->flat16.d, b->cu, b->cl, (const double*)b->scale);
   BL("apply_scale");
   b->pending = false;
+  b->age = 0;
   return RQ_OK;
 }
 
@@ -485,12 +496,23 @@ static int b_normalize(rq_batch* b, bool accumulate) {
 template <typename T>
 static int b_flush(rq_batch* b) {
   if (!b->pending || b->flat16.n == 0) return RQ_OK;
-  kb_apply_scale<T><<<b->flat16.n, 256, 0, b->st>>>(b->din, b->flat16.d, b->cu, b->cl, (const T*)b->scale);
+  kb_apply_scale<T><<<b->flat16.n, 256, 0, b->st>>>(b->din, b->flat16.d, b->cu, b->cl, (const double*)b->scale);
   BL("apply_scale");
   b->pending = false;
   return RQ_OK;
 }
 static int b_flush_any(rq_batch* b) { return b->fp64 ? b_flush<double>(b) : b_flush<float>(b); }
+
+// the normalised state every readout reports: flush a pending scale, or normalise now when
+// updates ran since the last normalisation
+template <typename T>
+static int b_ready(rq_batch* b) {
+  if (b->age == 0) return b_flush<T>(b);
+  const int rc = b_normalize<T>(b, true);
+  b->age = 0;
+  return rc;
+}
+static int b_ready_any(rq_batch* b) { return b->fp64 ? b_ready<double>(b) : b_ready<float>(b); }
 
 template <typename T>
 static int b_step(rq_batch* b, int s) {
@@ -501,11 +523,14 @@ static int b_step(rq_batch* b, int s) {
     if ((rc = b_flush<T>(b)) != RQ_OK) return rc;
     if ((rc = b_vcycle<T>(b)) != RQ_OK) return rc;
   }
-  const bool norm = s % f.norm_interval == 0;
+  // normalised after every norm_interval-th update and always after the update that precedes a
+  // V-cycle or a label pass (the update commutes with per-domain scales between Poisson solves)
+  const bool label_step = s % f.label_interval == 0 && (f.label_until <= 0 || s <= f.label_until);
+  const bool norm = (s + 1) % f.norm_interval == 0 || (s + 1) % f.poisson_interval == 0 || label_step;
   const T hd = (T)(0.5 * b->dv);
   // dt = dv h^2 differs per instance only through h: every instance of a batch shares h
   const T dt = (T)(b->dv * b->hin[0].h * b->hin[0].h);
-  const T* sc = b->pending ? (const T*)b->scale : nullptr;
+  const double* sc = b->pending ? (const double*)b->scale : nullptr;
   if (norm) {
     BCK(cudaMemsetAsync(b->dnorm, 0, sizeof(double) * b->D, b->st));
     kb_update<T, true><<<b->march[0].n, march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cp, b->cl, hd, dt,
@@ -518,11 +543,12 @@ static int b_step(rq_batch* b, int s) {
   b->cu ^= 1;
   b->pending = false;
   if (norm) {  // applied by the next update (or a flush)
-    BCK(nm_norm_scale<T>(b->dnorm, b->Zdom, b->D, (T*)b->scale, b->err, b->st));
+    BCK(nm_norm_scale<T>(b->dnorm, b->Zdom, b->D, (double*)b->scale, b->err, b->st));
     b->launches++;
     b->pending = true;
   }
-  if (s % f.label_interval == 0 && (f.label_until <= 0 || s <= f.label_until)) {
+  b->age = norm ? 0 : b->age + 1;
+  if (label_step) {
     if ((rc = b_flush<T>(b)) != RQ_OK) return rc;
     kb_evolve<T><<<b->march[0].n, march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cl,
                                                               (T)(float)f.boundary_speed, (T)(float)f.curv_reg);
@@ -580,8 +606,8 @@ extern "C" int rq_batch_create(const rq_config* cfgs, const rq_atom* atoms, cons
   b->cfg = c0;
   b->fp64 = c0.precision == RQ_PREC_FP64;
   rq_config& f = b->cfg;  // the new flavour's defaults (capi.cu fill_defaults)
-  if (f.norm_interval <= 0) f.norm_interval = 1;
   if (f.poisson_interval <= 0) f.poisson_interval = 4;
+  if (f.norm_interval <= 0) f.norm_interval = f.poisson_interval;
   if (f.label_interval <= 0) f.label_interval = 20;
   if (f.mg_pre <= 0) f.mg_pre = 1;
   if (f.mg_post <= 0) f.mg_post = 1;
@@ -715,7 +741,7 @@ extern "C" int rq_batch_step(rq_batch* b, int32_t n) {
       e = cudaGraphInstantiate(&b->graph[key], gr, 0);
       cudaGraphDestroy(gr);
       BCK(e);
-      b->graph_post[key] = b->cu | (b->cp << 1) | (b->cl << 2) | ((b->pending ? 1 : 0) << 4);
+      b->graph_post[key] = b->cu | (b->cp << 1) | (b->cl << 2) | ((b->pending ? 1 : 0) << 4) | (b->age << 5);
       b->graph_launches[key] = b->launches - l0;
       BCK(cudaGraphLaunch(b->graph[key], b->st));
     } else {
@@ -723,6 +749,7 @@ extern "C" int rq_batch_step(rq_batch* b, int32_t n) {
       const int post = b->graph_post[key];
       b->cu = post & 1; b->cp = (post >> 1) & 1; b->cl = (post >> 2) & 1;
       b->pending = (post >> 4) & 1;
+      b->age = post >> 5;
       b->steps_done += period;
       b->launches += b->graph_launches[key];
     }
@@ -738,7 +765,7 @@ extern "C" int rq_batch_energy(rq_batch* b, double* out) {
     std::memcpy(out, b->lastE.data(), sizeof(double) * b->lastE.size());
     return RQ_OK;
   }
-  int frc = b_flush_any(b);
+  int frc = b_ready_any(b);
   if (frc != RQ_OK) return frc;
   BCK(cudaMemsetAsync(b->dpd, 0, sizeof(double) * 4 * b->D, b->st));
   if (b->fp64) {
@@ -761,10 +788,12 @@ extern "C" int rq_batch_energy(rq_batch* b, double* out) {
       continue;
     }
     std::memset(o, 0, sizeof(double) * RQ_ENERGY_LEN);
-    for (int d = 0; d < I.nDom; ++d) {
-      o[RQ_E_T] += pd[4 * (I.dom0 + d) + 1];
-      o[RQ_E_EK] += pd[4 * (I.dom0 + d) + 2];
-      o[RQ_E_EE] += pd[4 * (I.dom0 + d) + 3];
+    for (int d = 0; d < I.nDom; ++d) {  // partials of the exactly normalised domains
+      const double* x = &pd[4 * ((size_t)I.dom0 + d)];
+      const double w = domain_norm_weight(b->atoms[q][d].Z, x[0]);
+      o[RQ_E_T] += w * x[1];
+      o[RQ_E_EK] += w * x[2];
+      o[RQ_E_EE] += w * x[3];
     }
     double ekk = 0;  // point-charge nuclear repulsion (bohr)
     const auto& at = b->atoms[q];
@@ -789,7 +818,7 @@ extern "C" int rq_batch_forces(rq_batch* b, double* F) {
   if (!b || !F) return RQ_EINVAL;
   for (char a : b->active)
     if (!a) return rq_batch_set_active_all(b) != RQ_OK ? RQ_ECUDA : rq_batch_forces(b, F);
-  int frc = b_flush_any(b);
+  int frc = b_ready_any(b);
   if (frc != RQ_OK) return frc;
   BCK(cudaMemsetAsync(b->dF, 0, sizeof(double) * 3 * b->A, b->st));
   if (b->fp64) {
@@ -831,7 +860,7 @@ __global__ void kb_widen(const float* __restrict__ a, double* __restrict__ d, lo
 // until the batch is destroyed.
 static int b_promote(rq_batch* b) {
   if (b->fp64) return RQ_OK;
-  int frc = b_flush_any(b);
+  int frc = b_ready_any(b);
   if (frc != RQ_OK) return frc;
   const size_t es = sizeof(double);
   for (int q = 0; q < b->n; ++q) {
@@ -857,7 +886,6 @@ static int b_promote(rq_batch* b) {
       if (l < I.nlev - 1) BALLOC(I.lr[l], s3 * es);
     }
   }
-  BALLOC(b->scale, es * b->D);
   BCK(cudaMemcpyAsync(b->din, b->hin.data(), sizeof(BInst) * b->n, cudaMemcpyHostToDevice, b->st));
   b->fp64 = true;
   b->promoted = true;

@@ -67,7 +67,7 @@ static void fill_defaults(rq_ctx* c) {
   const bool sp = f.flavor == RQ_FLAVOR_SOLVER_PY, mj = f.flavor == RQ_FLAVOR_MOLECULE_JS;
   const bool nm = f.flavor == RQ_FLAVOR_NEW;
   // the new flavour normalises every step: all-electron cores grow by e^{dt |eps|} per step
-  if (f.norm_interval <= 0) f.norm_interval = nm ? 1 : 20;
+  if (f.norm_interval <= 0) f.norm_interval = nm ? (f.poisson_interval > 0 ? f.poisson_interval : 4) : 20;
   // new flavour: one V(1,1) every 4 steps (the Hartree potential changes slowly; measured to
   // leave the iteration count and the converged energy unchanged against V(2,2) every 2 steps)
   if (f.poisson_interval <= 0) f.poisson_interval = nm ? 4 : sp ? 2 : 1;
@@ -257,7 +257,7 @@ extern "C" int rq_get_info(const rq_ctx* c, rq_info* info) {
 extern "C" int rq_synchronize(rq_ctx* c) {
   if (!c) return RQ_EINVAL;
   if (c->cfg.flavor == RQ_FLAVOR_NEW) {
-    int rc = nm_flush(c);  // device pointers from rq_get_info then hold the normalised psi
+    int rc = nm_ready(c);  // device pointers from rq_get_info then hold the normalised psi
     if (rc != RQ_OK) return rc;
   }
   CK(cudaStreamSynchronize(c->st));
@@ -400,7 +400,7 @@ extern "C" int rq_step(rq_ctx* c, int32_t n) {
       e = cudaGraphInstantiate(&c->graph[key], gr, 0);
       cudaGraphDestroy(gr);
       CK(e);
-      c->graph_post[key] = c->cu | (c->cp << 1) | (c->cl << 2) | ((c->nm_pending ? 1 : 0) << 4);
+      c->graph_post[key] = c->cu | (c->cp << 1) | (c->cl << 2) | ((c->nm_pending ? 1 : 0) << 4) | (c->nm_age << 5);
       c->graph_launches[key] = c->launches - l0;
       CK(cudaGraphLaunch(c->graph[key], c->st));
     } else {
@@ -408,6 +408,7 @@ extern "C" int rq_step(rq_ctx* c, int32_t n) {
       const int post = c->graph_post[key];
       c->cu = post & 1; c->cp = (post >> 1) & 1; c->cl = (post >> 2) & 1;
       c->nm_pending = (post >> 4) & 1;
+      c->nm_age = post >> 5;
       c->steps_done += period;
       c->launches += c->graph_launches[key];
     }
@@ -456,6 +457,7 @@ extern "C" int rq_upload_state(rq_ctx* c, const float* psi, const int32_t* label
   }
   if (psi) {
     c->nm_pending = false;
+    c->nm_age = 0;
     CK(cudaMemcpyAsync(c->U[c->cu], psi, n * sizeof(float), cudaMemcpyHostToDevice, c->st));
     if (mj)  // molecule.js keeps the boundary values of psi (never rewritten): both buffers hold them
       CK(cudaMemcpyAsync(c->U[1 - c->cu], c->U[c->cu], n * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
@@ -475,7 +477,7 @@ extern "C" int rq_upload_state(rq_ctx* c, const float* psi, const int32_t* label
 extern "C" int rq_download_state(rq_ctx* c, float* psi, int32_t* label, float* W, float* P) {
   if (!c) return RQ_EINVAL;
   if (c->cfg.flavor == RQ_FLAVOR_NEW && psi) {
-    int rc = nm_flush(c);
+    int rc = nm_ready(c);
     if (rc != RQ_OK) return rc;
   }
   if (c->fp64 && (psi || P)) return rq_fail(c, RQ_EINVAL, "FP64 context: use rq_download_state_f64 for psi/P");
@@ -496,6 +498,7 @@ extern "C" int rq_upload_state_f64(rq_ctx* c, const double* psi, const double* P
   const size_t n = (size_t)c->g.S3;
   if (psi) {
     c->nm_pending = false;
+    c->nm_age = 0;
     CK(cudaMemcpyAsync(c->U[c->cu], psi, n * sizeof(double), cudaMemcpyHostToDevice, c->st));
     CK(launch_zero_faces((double*)c->U[c->cu], c->g, c->st));
   }
@@ -510,7 +513,7 @@ extern "C" int rq_upload_state_f64(rq_ctx* c, const double* psi, const double* P
 extern "C" int rq_download_state_f64(rq_ctx* c, double* psi, double* P, double* K) {
   if (!c) return RQ_EINVAL;
   if (psi) {
-    int rc = nm_flush(c);
+    int rc = nm_ready(c);
     if (rc != RQ_OK) return rc;
   }
   if (!c->fp64) return rq_fail(c, RQ_EINVAL, "mixed-precision context: use rq_download_state");

@@ -27,6 +27,7 @@ template <> struct Ar<double> {
 
 constexpr int kNmFlatChunk = 16;     // points per thread of the flat (all S^3) bodies
 constexpr int kNmForceTile = 512;    // interior points staged per force tile
+constexpr int kNmRowPlanes = 4;      // planes i per block of the row-tiled multigrid bodies
 constexpr int kCoarsestThreads = 256; // one block solves the coarsest level (<= 29^3 points)
 
 // ---------------------------------------------------------------------------------------
@@ -102,7 +103,7 @@ __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __res
                                                const T* __restrict__ P, const int* __restrict__ label, const Geo& g,
                                                T half_dv, T dt, double h3, int nDom, double* __restrict__ norms,
                                                DomTable<1, 128>& tab, int bx, int by, int bz,
-                                               const T* __restrict__ scale = nullptr) {
+                                               const double* __restrict__ scale = nullptr) {
   using A = Ar<T>;
   RunSum<1> rs;
   rs.reset();
@@ -118,8 +119,10 @@ __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __res
     for (int i = i0; i < iend; ++i, id += S2) {
       const T u_p = U[id + S2];
       const int l_p = label[id + S2];
-      const T sc = scale ? scale[min(max(l_c, 0), nDom - 1)] : T(1);
-      auto sv = [&](T v) { return scale ? A::mul(v, sc) : v; };
+      // a pending normalisation: each value is scaled in FP64 and rounded once, so fp32 fields
+      // carry no per-domain bias from rounding the scale itself
+      const double sc = scale ? scale[min(max(l_c, 0), nDom - 1)] : 1.0;
+      auto sv = [&](T v) { return scale ? (T)((double)v * sc) : v; };
       const T uc = sv(u_c);
       const T a = (l_p == l_c) ? sv(u_p) : uc;
       const T b = (l_m == l_c) ? sv(u_m) : uc;
@@ -140,17 +143,19 @@ __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __res
   if (ACC) rs.finish_warp(tab, norms);  // every lane of the (32 x 8) block reaches this point
 }
 
-// U *= scale[label] for labels in [0, nDom) over kNmFlatChunk*256 points from blk
+// U *= scale[label] (FP64 product, rounded once) for labels in [0, nDom) over kNmFlatChunk*256
+// points from blk
 template <typename T>
 __device__ __forceinline__ void nm_apply_scale_body(T* __restrict__ U, const int* __restrict__ label,
-                                                    const T* __restrict__ scale, long long S3, int nDom, long long blk) {
+                                                    const double* __restrict__ scale, long long S3, int nDom,
+                                                    long long blk) {
   const long long base = blk * blockDim.x * kNmFlatChunk;
   for (int q = 0; q < kNmFlatChunk; ++q) {
     const long long id = base + (long long)q * blockDim.x + threadIdx.x;
     if (id >= S3) break;
     const int l = label[id];
     if (l < 0 || l >= nDom) continue;
-    U[id] = Ar<T>::mul(U[id], scale[l]);
+    U[id] = (T)((double)U[id] * scale[l]);
   }
 }
 
@@ -183,62 +188,38 @@ __device__ __forceinline__ T rhs_at(const T* __restrict__ f, long long id) {
 }
 
 // one colour of a red-black sweep for A P = f, A P = (6P - sum_6 P)/h^2; block (32, 8): each
-// thread owns the pair (k0, k0+1) of plane i = 1+bz, one of which has the colour
+// thread owns the pair (k0, k0+1) of row j on the kNmRowPlanes planes i from 1 + bz*kNmRowPlanes,
+// and on each plane updates the one of the pair that has the colour
 template <typename T, bool FINE>
 __device__ __forceinline__ void nm_rbgs_body(T* __restrict__ P, const T* __restrict__ f, const Geo& g, T h2, int color,
                                              int bx, int by, int bz) {
   using A = Ar<T>;
   const int k0 = 1 + bx * 64 + 2 * threadIdx.x;
   const int j = 1 + by * blockDim.y + threadIdx.y;
-  const int i = 1 + bz;
-  if (j >= g.NN || i >= g.NN) return;
-  const int k = k0 + ((i + j + k0 + color) & 1);
-  if (k >= g.NN) return;
+  const int i0 = 1 + bz * kNmRowPlanes;
+  if (j >= g.NN || k0 >= g.NN) return;
+  const int iend = min(i0 + kNmRowPlanes, g.NN);
   const long long S = g.S, S2 = g.S2;
-  const long long id = (long long)i * S2 + (long long)j * S + k;
-  const T s = A::add(A::add(A::add(A::add(A::add(P[id + S2], P[id - S2]), P[id + S]), P[id - S]), P[id + 1]), P[id - 1]);
-  P[id] = A::div(A::add(s, A::mul(h2, rhs_at<T, FINE>(f, id))), T(6));
-}
-
-template <typename T, bool FINE>
-__device__ __forceinline__ void nm_residual_body(const T* __restrict__ P, const T* __restrict__ f, T* __restrict__ r,
-                                                 const Geo& g, T inv_h2, int bx, int by, int bz) {
-  using A = Ar<T>;
-  const int k = 1 + bx * kThreadsK + threadIdx.x;
-  const int j = 1 + by * kThreadsJ + threadIdx.y;
-  const int i0 = 1 + bz * kMarch;
-  if (k >= g.NN || j >= g.NN || i0 >= g.NN) return;
-  const int iend = min(i0 + kMarch, g.NN);
-  const long long S = g.S, S2 = g.S2;
-  for (int i = i0; i < iend; ++i) {
+#pragma unroll
+  for (int q = 0; q < kNmRowPlanes; ++q) {
+    const int i = i0 + q;
+    const int k = k0 + ((i + j + k0 + color) & 1);
+    if (i >= iend || k >= g.NN) continue;
     const long long id = (long long)i * S2 + (long long)j * S + k;
-    if (sizeof(T) == sizeof(float)) {
-      // fp32 fields: sum_6 P - 6 P cancels most of its digits (P is smooth), so the residual is
-      // formed in FP64 from the fp32 values and rounded once -- this is what lets the fp32
-      // multigrid reach the fp32 resolution of P instead of stalling at ~1e-4 relative
-      const double sd = (double)P[id + S2] + (double)P[id - S2] + (double)P[id + S] + (double)P[id - S] +
-                        (double)P[id + 1] + (double)P[id - 1];
-      r[id] = (T)((double)rhs_at<T, FINE>(f, id) + (sd - 6.0 * (double)P[id]) * (double)inv_h2);
-    } else {
-      const T s = A::add(A::add(A::add(A::add(A::add(P[id + S2], P[id - S2]), P[id + S]), P[id - S]), P[id + 1]), P[id - 1]);
-      r[id] = A::add(rhs_at<T, FINE>(f, id), A::mul(A::sub(s, A::mul(T(6), P[id])), inv_h2));
-    }
+    const T s = A::add(A::add(A::add(A::add(A::add(P[id + S2], P[id - S2]), P[id + S]), P[id - S]), P[id + 1]), P[id - 1]);
+    P[id] = A::div(A::add(s, A::mul(h2, rhs_at<T, FINE>(f, id))), T(6));
   }
 }
 
-// the same residual at interior point number q (one point per thread: the level is small or
-// the march's per-plane latency chain would dominate)
+// residual r = f - A P at one interior point
 template <typename T, bool FINE>
-__device__ __forceinline__ void nm_residual_flat_body(const T* __restrict__ P, const T* __restrict__ f,
-                                                      T* __restrict__ r, const Geo& g, T inv_h2, long long q) {
+__device__ __forceinline__ void nm_residual_point(const T* __restrict__ P, const T* __restrict__ f, T* __restrict__ r,
+                                                  long long id, long long S, long long S2, T inv_h2) {
   using A = Ar<T>;
-  const int n = g.NN - 1;
-  if (q >= (long long)n * n * n) return;
-  const int qi = (int)q;
-  const int k = 1 + qi % n, j = 1 + (qi / n) % n, i = 1 + qi / (n * n);
-  const long long S = g.S, S2 = g.S2;
-  const long long id = (long long)i * S2 + (long long)j * S + k;
   if (sizeof(T) == sizeof(float)) {
+    // fp32 fields: sum_6 P - 6 P cancels most of its digits (P is smooth), so the residual is
+    // formed in FP64 from the fp32 values and rounded once -- this is what lets the fp32
+    // multigrid reach the fp32 resolution of P instead of stalling at ~1e-4 relative
     const double sd = (double)P[id + S2] + (double)P[id - S2] + (double)P[id + S] + (double)P[id - S] +
                       (double)P[id + 1] + (double)P[id - 1];
     r[id] = (T)((double)rhs_at<T, FINE>(f, id) + (sd - 6.0 * (double)P[id]) * (double)inv_h2);
@@ -248,24 +229,70 @@ __device__ __forceinline__ void nm_residual_flat_body(const T* __restrict__ P, c
   }
 }
 
-// trilinear prolongation + correction at fine interior point number q
-template <typename T>
-__device__ __forceinline__ void nm_prolong_flat_body(const T* __restrict__ Ec, T* __restrict__ P, const Geo& g,
-                                                     const Geo& gc, long long q) {
-  using A = Ar<T>;
-  const int n = g.NN - 1;
-  if (q >= (long long)n * n * n) return;
-  const int qi = (int)q;
-  const int k = 1 + qi % n, j = 1 + (qi / n) % n, i = 1 + qi / (n * n);
-  const int ci = i >> 1, cj = j >> 1, ck = k >> 1, oi = i & 1, oj = j & 1, ok = k & 1;
-  T v = T(0);
-  for (int a = 0; a <= oi; ++a)
-    for (int b = 0; b <= oj; ++b)
-      for (int c = 0; c <= ok; ++c) v = A::add(v, Ec[(long long)(ci + a) * gc.S2 + (long long)(cj + b) * gc.S + (ck + c)]);
-  v = A::div(v, (T)((1 + oi) * (1 + oj) * (1 + ok)));
-  const long long id = (long long)i * g.S2 + (long long)j * g.S + k;
-  P[id] = A::add(P[id], v);
+// Row tiling shared by the residual and the prolongation: block (32, 8) covers 64 points of k
+// on 8 rows j of the kNmRowPlanes planes from i = 1 + bz*kNmRowPlanes; thread x takes
+// k = 1 + 64 bx + x and k + 32 on each plane.  Every point is independent (no dependent chain
+// along i), so levels of every size fill the SMs, and each warp load is one contiguous run of 32
+// values.
+#define NM_ROWS_PROLOGUE                                  \
+  const int j = 1 + by * blockDim.y + threadIdx.y;        \
+  const int i0 = 1 + bz * kNmRowPlanes;                   \
+  if (j >= g.NN) return;                                  \
+  const int iend = min(i0 + kNmRowPlanes, g.NN);          \
+  const long long S = g.S, S2 = g.S2;
+
+template <typename T, bool FINE>
+__device__ __forceinline__ void nm_residual_rows_body(const T* __restrict__ P, const T* __restrict__ f,
+                                                      T* __restrict__ r, const Geo& g, T inv_h2, int bx, int by,
+                                                      int bz) {
+  NM_ROWS_PROLOGUE
+#pragma unroll
+  for (int q = 0; q < kNmRowPlanes; ++q) {
+    const int i = i0 + q;
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const int k = 1 + bx * 64 + threadIdx.x + 32 * t;
+      if (i < iend && k < g.NN)
+        nm_residual_point<T, FINE>(P, f, r, (long long)i * S2 + (long long)j * S + k, S, S2, inv_h2);
+    }
+  }
 }
+
+// Trilinear prolongation + correction, P += I E_c, on the row tiling.  A fine point averages the
+// 1, 2, 4 or 8 coarse values around it, summed in the order (a, b, c) = (i, j, k) offsets with
+// k fastest, then divided by their count.  The i and j parities are uniform over a warp's row;
+// only the k parity alternates between lanes, and it selects whether a second value is added.
+template <typename T>
+__device__ __forceinline__ void nm_prolong_rows_body(const T* __restrict__ Ec, T* __restrict__ P, const Geo& g,
+                                                     const Geo& gc, int bx, int by, int bz) {
+  using A = Ar<T>;
+  NM_ROWS_PROLOGUE
+  const int oj = j & 1;
+#pragma unroll
+  for (int q = 0; q < kNmRowPlanes * 2; ++q) {
+    const int i = i0 + (q >> 1);
+    const int k = 1 + bx * 64 + threadIdx.x + 32 * (q & 1);
+    if (i >= iend || k >= g.NN) continue;
+    const int oi = i & 1;
+    const long long row0 = (long long)(i >> 1) * gc.S2 + (long long)(j >> 1) * gc.S;
+    const int ck = k >> 1, ok = k & 1;
+    T v = T(0);
+    auto add_row = [&](long long row) {
+      v = A::add(v, Ec[row + ck]);
+      if (ok) v = A::add(v, Ec[row + ck + 1]);
+    };
+    add_row(row0);
+    if (oj) add_row(row0 + gc.S);
+    if (oi) {
+      add_row(row0 + gc.S2);
+      if (oj) add_row(row0 + gc.S2 + gc.S);
+    }
+    v = A::div(v, (T)((1 + oi) * (1 + oj) * (1 + ok)));
+    const long long id = (long long)i * S2 + (long long)j * S + k;
+    P[id] = A::add(P[id], v);
+  }
+}
+#undef NM_ROWS_PROLOGUE
 
 // full weighting (1/64)(8,4,2,1) at coarse interior point number q; loop order a, b, c
 template <typename T>
@@ -283,28 +310,6 @@ __device__ __forceinline__ void nm_restrict_body(const T* __restrict__ fine, T* 
         v = A::add(v, A::mul(w, fine[(long long)(2 * I + a) * g.S2 + (long long)(2 * J + b) * g.S + (2 * K2 + c)]));
       }
   coarse[(long long)I * gc.S2 + (long long)J * gc.S + K2] = A::div(v, T(64));
-}
-
-// trilinear prolongation of the coarse correction, added on the march tile (bx, by, bz)
-template <typename T>
-__device__ __forceinline__ void nm_prolong_body(const T* __restrict__ Ec, T* __restrict__ P, const Geo& g,
-                                                const Geo& gc, int bx, int by, int bz) {
-  using A = Ar<T>;
-  const int k = 1 + bx * kThreadsK + threadIdx.x;
-  const int j = 1 + by * kThreadsJ + threadIdx.y;
-  const int i0 = 1 + bz * kMarch;
-  if (k >= g.NN || j >= g.NN || i0 >= g.NN) return;
-  const int iend = min(i0 + kMarch, g.NN);
-  for (int i = i0; i < iend; ++i) {
-    const int ci = i >> 1, cj = j >> 1, ck = k >> 1, oi = i & 1, oj = j & 1, ok = k & 1;
-    T v = T(0);
-    for (int a = 0; a <= oi; ++a)
-      for (int b = 0; b <= oj; ++b)
-        for (int c = 0; c <= ok; ++c) v = A::add(v, Ec[(long long)(ci + a) * gc.S2 + (long long)(cj + b) * gc.S + (ck + c)]);
-    v = A::div(v, (T)((1 + oi) * (1 + oj) * (1 + ok)));
-    const long long id = (long long)i * g.S2 + (long long)j * g.S + k;
-    P[id] = A::add(P[id], v);
-  }
 }
 
 // coarsest level: `sweeps` red-black sweeps in FP64 by one block; sm: 2*S^3 doubles of smem

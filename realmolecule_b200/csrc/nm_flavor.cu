@@ -111,8 +111,9 @@ static int nm_normalize_t(rq_ctx* c, bool accumulate) {
     LAUNCH(RQ_KC_NORMALIZE, (sizeof(T) + 4.0) * c->g.S3, nm_norms<T>(U, c->lab[c->cl], c->g, c->h3, c->n_atoms, c->dnorm, c->st));
   }
   LAUNCH(RQ_KC_NORMALIZE, (2.0 * sizeof(T) + 4.0) * c->g.S3,
-         nm_normalize<T>(U, c->lab[c->cl], c->dnorm, c->Zdom64, c->n_atoms, (T*)c->scale64, c->err, c->g, c->st));
+         nm_normalize<T>(U, c->lab[c->cl], c->dnorm, c->Zdom64, c->n_atoms, (double*)c->scale64, c->err, c->g, c->st));
   c->nm_pending = false;
+  c->nm_age = 0;
   return RQ_OK;
 }
 
@@ -122,12 +123,24 @@ template <typename T>
 static int nm_flush_t(rq_ctx* c) {
   if (!c->nm_pending) return RQ_OK;
   LAUNCH(RQ_KC_NORMALIZE, (2.0 * sizeof(T) + 4.0) * c->g.S3,
-         nm_apply<T>((T*)c->U[c->cu], c->lab[c->cl], (const T*)c->scale64, c->n_atoms, c->g, c->st));
+         nm_apply<T>((T*)c->U[c->cu], c->lab[c->cl], (const double*)c->scale64, c->n_atoms, c->g, c->st));
   c->nm_pending = false;
   return RQ_OK;
 }
 
 int nm_flush(rq_ctx* c) { return c->fp64 ? nm_flush_t<double>(c) : nm_flush_t<float>(c); }
+
+// Bring psi to the normalised state that every readout reports: apply a pending scale, or, when
+// updates ran since the last normalisation, normalise now.
+template <typename T>
+static int nm_ready_t(rq_ctx* c) {
+  if (c->nm_age == 0) return nm_flush_t<T>(c);
+  const int rc = nm_normalize_t<T>(c, true);
+  c->nm_age = 0;
+  return rc;
+}
+
+int nm_ready(rq_ctx* c) { return c->fp64 ? nm_ready_t<double>(c) : nm_ready_t<float>(c); }
 
 template <typename T>
 static int nm_step_t(rq_ctx* c, int s) {
@@ -137,20 +150,26 @@ static int nm_step_t(rq_ctx* c, int s) {
     if ((rc = nm_flush_t<T>(c)) != RQ_OK) return rc;
     if ((rc = nm_vcycle(c)) != RQ_OK) return rc;
   }
-  const bool norm = s % f.norm_interval == 0;
+  // The update is linear in psi and couples only points of one domain, so between two Poisson
+  // solves a per-domain scale commutes with it: normalising every step or once before the next
+  // V-cycle / label pass gives the same psi there.  Normalise after every norm_interval-th update
+  // and always after the update that precedes a V-cycle or ends with a label pass.
+  const bool label_step = s % f.label_interval == 0 && (f.label_until <= 0 || s <= f.label_until);
+  const bool norm = (s + 1) % f.norm_interval == 0 || (s + 1) % f.poisson_interval == 0 || label_step;
   if (norm) CK(cudaMemsetAsync(c->dnorm, 0, sizeof(double) * c->n_atoms, c->st));
   LAUNCH(RQ_KC_UPDATE, (4.0 * sizeof(T) + 4.0) * interior(c->g),
          nm_update<T>((const T*)c->U[c->cu], (T*)c->U[1 - c->cu], (const T*)c->K, (const T*)c->P[c->cp], c->lab[c->cl],
                       c->g, (T)c->half_dv, (T)c->dt, c->h3, c->n_atoms, norm ? c->dnorm : nullptr, c->st,
-                      c->nm_pending ? (const T*)c->scale64 : nullptr));
+                      c->nm_pending ? (const double*)c->scale64 : nullptr));
   c->cu ^= 1;
   c->nm_pending = false;  // the update consumed the pending scale
   if (norm) {  // the scale of this step is applied by the next update (or a flush)
     LAUNCH(RQ_KC_NORMALIZE, 12.0 * c->n_atoms,
-           nm_norm_scale<T>(c->dnorm, c->Zdom64, c->n_atoms, (T*)c->scale64, c->err, c->st));
+           nm_norm_scale<T>(c->dnorm, c->Zdom64, c->n_atoms, (double*)c->scale64, c->err, c->st));
     c->nm_pending = true;
   }
-  if (s % f.label_interval == 0 && (f.label_until <= 0 || s <= f.label_until)) {
+  c->nm_age = norm ? 0 : c->nm_age + 1;
+  if (label_step) {
     if ((rc = nm_flush_t<T>(c)) != RQ_OK) return rc;
     LAUNCH(RQ_KC_LABELS, (sizeof(T) + 12.0) * interior(c->g),
            nm_evolve<T>(c->lab[c->cl], c->lab[1 - c->cl], (const T*)c->U[c->cu], c->W, c->g, f.boundary_speed, f.curv_reg,
@@ -245,7 +264,7 @@ void nm_nuclear_terms(rq_ctx* c, double* E, double* F) {
 
 int nm_energy(rq_ctx* c, double* out, double* per_domain) {
   const int n = c->n_atoms;
-  int frc = nm_flush(c);
+  int frc = nm_ready(c);
   if (frc != RQ_OK) return frc;
   CK(cudaMemsetAsync(c->dpd, 0, sizeof(double) * 4 * n, c->st));
   if (c->fp64)
@@ -261,12 +280,17 @@ int nm_energy(rq_ctx* c, double* out, double* per_domain) {
   CK(cudaStreamSynchronize(c->st));
   double T = 0, EK = 0, EE = 0;
   for (int q = 0; q < n; ++q) {
-    T += pd[q * 4 + 1]; EK += pd[q * 4 + 2]; EE += pd[q * 4 + 3];
+    // Every term is linear in the domain's density for the current P, so the energy of the
+    // exactly normalised state is the partial times Z/N: this removes the rounding of the stored
+    // scale (fp32 fields) from the reported energy.
+    const double w = domain_norm_weight(c->atoms[q].Z, pd[q * 4]);
+    const double t = w * pd[q * 4 + 1], ek = w * pd[q * 4 + 2], ee = w * pd[q * 4 + 3];
+    T += t; EK += ek; EE += ee;
     if (per_domain) {
       double* d = per_domain + (size_t)q * RQ_DOMAIN_LEN;
-      d[RQ_D_NORM] = pd[q * 4]; d[RQ_D_T] = pd[q * 4 + 1]; d[RQ_D_EK] = pd[q * 4 + 2]; d[RQ_D_EE] = pd[q * 4 + 3];
-      const double nr = pd[q * 4] != 0 ? pd[q * 4] : 1.0;
-      d[RQ_D_EIG] = (pd[q * 4 + 1] + 2 * pd[q * 4 + 3] + pd[q * 4 + 2]) / nr;
+      d[RQ_D_NORM] = pd[q * 4]; d[RQ_D_T] = t; d[RQ_D_EK] = ek; d[RQ_D_EE] = ee;
+      const double nr = c->atoms[q].Z > 0 ? c->atoms[q].Z : (pd[q * 4] != 0 ? pd[q * 4] : 1.0);
+      d[RQ_D_EIG] = (t + 2 * ee + ek) / nr;
     }
   }
   out[RQ_E_T] = T; out[RQ_E_EK] = EK; out[RQ_E_EE] = EE;
@@ -276,7 +300,7 @@ int nm_energy(rq_ctx* c, double* out, double* per_domain) {
 int nm_forces(rq_ctx* c, int method, double* F) {
   if (method != RQ_FORCE_HF && method != RQ_FORCE_ADJOINT) return RQ_ENOTSUP;
   const int n = c->n_atoms;
-  int frc = nm_flush(c);
+  int frc = nm_ready(c);
   if (frc != RQ_OK) return frc;
   CK(cudaMemsetAsync(c->dF, 0, sizeof(double) * 3 * n, c->st));
   if (c->fp64)

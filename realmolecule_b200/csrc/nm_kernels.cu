@@ -22,7 +22,7 @@ __global__ void __launch_bounds__(256) k_nm_init(T* U, int* label, const float4*
 
 template <typename T, bool ACC>
 __global__ void __launch_bounds__(256) k_nm_update(const T* U, T* Unew, const T* K, const T* P, const int* label, Geo g,
-                                                   T half_dv, T dt, double h3, int nDom, double* norms, const T* scale) {
+                                                   T half_dv, T dt, double h3, int nDom, double* norms, const double* scale) {
   __shared__ DomTable<1, 128> tab;
   if (ACC) {
     dom_table_init(tab);
@@ -39,16 +39,16 @@ __global__ void __launch_bounds__(256) k_nm_update(const T* U, T* Unew, const T*
 // scale[l] = sqrt(Zdom_l / n_l) (FP64) for every domain of the (concatenated) arrays
 template <typename T>
 __global__ void k_nm_norm_scale(const double* __restrict__ norms, const double* __restrict__ Zdom, int nDom,
-                                T* __restrict__ scale, int* __restrict__ err) {
+                                double* __restrict__ scale, int* __restrict__ err) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= nDom) return;
   const double n = norms[l];
   if (!isfinite(n)) atomicOr(err, 1);
-  scale[l] = (Zdom[l] > 0.0 && n > 1e-300) ? (T)sqrt(Zdom[l] / n) : T(1);
+  scale[l] = (Zdom[l] > 0.0 && n > 1e-300) ? sqrt(Zdom[l] / n) : 1.0;
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_nm_apply_scale(T* U, const int* label, const T* scale, long long S3, int nDom) {
+__global__ void __launch_bounds__(256) k_nm_apply_scale(T* U, const int* label, const double* scale, long long S3, int nDom) {
   nm_apply_scale_body<T>(U, label, scale, S3, nDom, blockIdx.x);
 }
 
@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(256) k_nm_rbgs(T* P, const T* f, Geo g, T h2, 
 
 template <typename T, bool FINE>
 __global__ void __launch_bounds__(256) k_nm_residual(const T* P, const T* f, T* r, Geo g, T inv_h2) {
-  nm_residual_flat_body<T, FINE>(P, f, r, g, inv_h2, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+  nm_residual_rows_body<T, FINE>(P, f, r, g, inv_h2, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 template <typename T>
@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(256) k_nm_restrict(const T* fine, T* coarse, G
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_nm_prolong(const T* Ec, T* P, Geo g, Geo gc) {
-  nm_prolong_flat_body<T>(Ec, P, g, gc, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+  nm_prolong_rows_body<T>(Ec, P, g, gc, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 template <typename T>
@@ -136,7 +136,7 @@ cudaError_t nm_init(T* U, int* label, const float4* seeds, int nSeed, const Geo&
 }
 template <typename T>
 cudaError_t nm_update(const T* U, T* Unew, const T* K, const T* P, const int* label, const Geo& g, T half_dv, T dt,
-                      double h3, int nDom, double* norms, cudaStream_t st, const T* scale) {
+                      double h3, int nDom, double* norms, cudaStream_t st, const double* scale) {
   if (g.NN < 2) return cudaSuccess;
   if (norms)
     k_nm_update<T, true><<<march_grid(g), march_block(), 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, norms,
@@ -147,19 +147,19 @@ cudaError_t nm_update(const T* U, T* Unew, const T* K, const T* P, const int* la
   return cudaGetLastError();
 }
 template <typename T>
-cudaError_t nm_apply(T* U, const int* label, const T* scale, int nDom, const Geo& g, cudaStream_t st) {
+cudaError_t nm_apply(T* U, const int* label, const double* scale, int nDom, const Geo& g, cudaStream_t st) {
   k_nm_apply_scale<T><<<nblk(g.S3, 256 * kNmFlatChunk), 256, 0, st>>>(U, label, scale, g.S3, nDom);
   return cudaGetLastError();
 }
 template <typename T>
-cudaError_t nm_normalize(T* U, const int* label, const double* norms, const double* Zdom, int nDom, T* scale, int* err,
+cudaError_t nm_normalize(T* U, const int* label, const double* norms, const double* Zdom, int nDom, double* scale, int* err,
                          const Geo& g, cudaStream_t st) {
   k_nm_norm_scale<T><<<nblk(nDom, 128), 128, 0, st>>>(norms, Zdom, nDom, scale, err);
   k_nm_apply_scale<T><<<nblk(g.S3, 256 * kNmFlatChunk), 256, 0, st>>>(U, label, scale, g.S3, nDom);
   return cudaGetLastError();
 }
 template <typename T>
-cudaError_t nm_norm_scale(const double* norms, const double* Zdom, int nDom, T* scale, int* err, cudaStream_t st) {
+cudaError_t nm_norm_scale(const double* norms, const double* Zdom, int nDom, double* scale, int* err, cudaStream_t st) {
   k_nm_norm_scale<T><<<nblk(nDom, 128), 128, 0, st>>>(norms, Zdom, nDom, scale, err);
   return cudaGetLastError();
 }
@@ -172,7 +172,7 @@ template <typename T>
 cudaError_t nm_rbgs(T* P, const T* f, bool fine, const Geo& g, double h2, int color, cudaStream_t st) {
   const int n = g.NN - 1;
   const dim3 blk(32, 8);
-  const dim3 grd((n + 63) / 64, (n + 7) / 8, n);
+  const dim3 grd((n + 63) / 64, (n + 7) / 8, (n + kNmRowPlanes - 1) / kNmRowPlanes);
   if (fine)
     k_nm_rbgs<T, true><<<grd, blk, 0, st>>>(P, f, g, (T)h2, color);
   else
@@ -181,11 +181,12 @@ cudaError_t nm_rbgs(T* P, const T* f, bool fine, const Geo& g, double h2, int co
 }
 template <typename T>
 cudaError_t nm_residual(const T* P, const T* f, bool fine, T* r, const Geo& g, double inv_h2, cudaStream_t st) {
-  const long long n = g.NN - 1;
+  const int n = g.NN - 1;
+  const dim3 blk(32, 8), grd((n + 63) / 64, (n + 7) / 8, (n + kNmRowPlanes - 1) / kNmRowPlanes);
   if (fine)
-    k_nm_residual<T, true><<<nblk(n * n * n), 256, 0, st>>>(P, f, r, g, (T)inv_h2);
+    k_nm_residual<T, true><<<grd, blk, 0, st>>>(P, f, r, g, (T)inv_h2);
   else
-    k_nm_residual<T, false><<<nblk(n * n * n), 256, 0, st>>>(P, f, r, g, (T)inv_h2);
+    k_nm_residual<T, false><<<grd, blk, 0, st>>>(P, f, r, g, (T)inv_h2);
   return cudaGetLastError();
 }
 template <typename T>
@@ -196,8 +197,9 @@ cudaError_t nm_restrict(const T* fine, T* coarse, const Geo& g, const Geo& gc, c
 }
 template <typename T>
 cudaError_t nm_prolong(const T* Ec, T* P, const Geo& g, const Geo& gc, cudaStream_t st) {
-  const long long n = g.NN - 1;
-  k_nm_prolong<T><<<nblk(n * n * n), 256, 0, st>>>(Ec, P, g, gc);
+  const int n = g.NN - 1;
+  const dim3 blk(32, 8), grd((n + 63) / 64, (n + 7) / 8, (n + kNmRowPlanes - 1) / kNmRowPlanes);
+  k_nm_prolong<T><<<grd, blk, 0, st>>>(Ec, P, g, gc);
   return cudaGetLastError();
 }
 template <typename T>
@@ -247,11 +249,11 @@ cudaError_t nm_add(T* K, const T* v, long long n, cudaStream_t st) {
   template cudaError_t nm_potential<T>(T*, const double*, int, const Geo&, double, double, cudaStream_t);           \
   template cudaError_t nm_init<T>(T*, int*, const float4*, int, const Geo&, float, cudaStream_t);                   \
   template cudaError_t nm_update<T>(const T*, T*, const T*, const T*, const int*, const Geo&, T, T, double, int,     \
-                                    double*, cudaStream_t, const T*);                                                \
-  template cudaError_t nm_apply<T>(T*, const int*, const T*, int, const Geo&, cudaStream_t);                        \
-  template cudaError_t nm_normalize<T>(T*, const int*, const double*, const double*, int, T*, int*, const Geo&,     \
+                                    double*, cudaStream_t, const double*);                                           \
+  template cudaError_t nm_apply<T>(T*, const int*, const double*, int, const Geo&, cudaStream_t);                   \
+  template cudaError_t nm_normalize<T>(T*, const int*, const double*, const double*, int, double*, int*, const Geo&, \
                                        cudaStream_t);                                                                \
-  template cudaError_t nm_norm_scale<T>(const double*, const double*, int, T*, int*, cudaStream_t);                 \
+  template cudaError_t nm_norm_scale<T>(const double*, const double*, int, double*, int*, cudaStream_t);            \
   template cudaError_t nm_norms<T>(const T*, const int*, const Geo&, double, int, double*, cudaStream_t);           \
   template cudaError_t nm_rbgs<T>(T*, const T*, bool, const Geo&, double, int, cudaStream_t);                       \
   template cudaError_t nm_residual<T>(const T*, const T*, bool, T*, const Geo&, double, cudaStream_t);              \

@@ -56,9 +56,10 @@ struct rq_ctx {
   void* atoms_mj = nullptr;   // molecule.js records (u32 positions)
   double* atoms_nm = nullptr; // new flavour: x,y,z (bohr), Z_nuc per atom
   void* seeds = nullptr;      // new flavour: float4 (x, y, z, entry) per domain seed
-  void* scale64 = nullptr;    // new flavour: per-domain scale (T)
+  void* scale64 = nullptr;    // new flavour: per-domain scale (FP64 for both precisions)
   void* Kext = nullptr;       // new flavour: external potential added to K (T), or null
   bool nm_pending = false;    // new flavour: psi awaits scale64 (applied by the next update or a flush)
+  int nm_age = 0;             // new flavour: updates since psi was last normalised (0: normalised or pending)
   float* Zdom = nullptr;      // domain charge per label (f32)
   double* Zdom64 = nullptr;
 

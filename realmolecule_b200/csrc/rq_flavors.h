@@ -27,4 +27,5 @@ int nm_forces(rq_ctx* c, int method, double* F);
 int nm_set_atoms(rq_ctx* c);
 int nm_set_external(rq_ctx* c, const double* v);
 int nm_flush(rq_ctx* c);  // materialise a pending per-domain normalisation of psi
+int nm_ready(rq_ctx* c);  // nm_flush, or normalise now when updates ran since the last normalisation
 void nm_nuclear_terms(rq_ctx* c, double* E, double* F);

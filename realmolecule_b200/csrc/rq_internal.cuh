@@ -143,4 +143,8 @@ struct RunSum {
   }
 };
 
+// Weight Z/N that turns a domain's energy partials (each linear in its density for a fixed P)
+// into those of the exactly normalised domain; 1 when Z or the measured norm N is not positive.
+inline double domain_norm_weight(double Z, double N) { return (Z > 0.0 && N > 0.0) ? Z / N : 1.0; }
+
 }  // namespace rq

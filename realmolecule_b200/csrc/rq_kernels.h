@@ -63,14 +63,14 @@ template <typename T>
 cudaError_t nm_init(T* U, int* label, const float4* seeds, int nSeed, const Geo& g, float h, cudaStream_t st);
 template <typename T>
 cudaError_t nm_update(const T* U, T* Unew, const T* K, const T* P, const int* label, const Geo& g, T half_dv, T dt,
-                      double h3, int nDom, double* norms, cudaStream_t st, const T* scale = nullptr);
+                      double h3, int nDom, double* norms, cudaStream_t st, const double* scale = nullptr);
 template <typename T>
-cudaError_t nm_apply(T* U, const int* label, const T* scale, int nDom, const Geo& g, cudaStream_t st);
+cudaError_t nm_apply(T* U, const int* label, const double* scale, int nDom, const Geo& g, cudaStream_t st);
 template <typename T>
-cudaError_t nm_normalize(T* U, const int* label, const double* norms, const double* Zdom, int nDom, T* scale, int* err,
+cudaError_t nm_normalize(T* U, const int* label, const double* norms, const double* Zdom, int nDom, double* scale, int* err,
                          const Geo& g, cudaStream_t st);
 template <typename T>
-cudaError_t nm_norm_scale(const double* norms, const double* Zdom, int nDom, T* scale, int* err, cudaStream_t st);
+cudaError_t nm_norm_scale(const double* norms, const double* Zdom, int nDom, double* scale, int* err, cudaStream_t st);
 template <typename T>
 cudaError_t nm_norms(const T* U, const int* label, const Geo& g, double h3, int nDom, double* norms, cudaStream_t st);
 template <typename T>

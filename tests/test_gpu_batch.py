@@ -41,7 +41,9 @@ def test_batch_matches_single_contexts(precision):
         for k in (L.E_T, L.E_EK, L.E_EE, L.E_KK, L.E_TOTAL):
             assert abs(Eb[q, k] - e[k]) <= tol * max(1.0, abs(e[k])), (q, k, Eb[q, k], e[k])
         F = c.forces(L.FORCE_ADJOINT) + c.nuclear_terms()[1]
-        np.testing.assert_allclose(Fb[q], F, rtol=1e-6, atol=1e-8)
+        # fp32 fields: the two runs round psi differently wherever their FP64 domain sums (atomics in
+        # a different order) differ in the last bit, ~1e-7 of the largest force
+        np.testing.assert_allclose(Fb[q], F, rtol=1e-6, atol=1e-8 if precision == "fp64" else 1e-6)
 
 
 def test_mixed_solve_matches_fp64_solve_to_1e6_ha():
