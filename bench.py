@@ -23,10 +23,18 @@ period with the flush before EVERY solver step (every kernel reads HBM cold).
 ``cpu_baseline`` the reference's own cloud/solver.py kernels compiled for the host
            (oracle/_ref, OpenMP over all host cores) on a bounded sample of the same workload.
 
+``converge`` the second half of the metric, seconds to converge (|dE| < 1e-6 Ha between checks
+           100 steps apart) with the new flavour: glycine (40 electrons, 128^3) as one context in
+           mixed precision and in FP64, and the 96 water clusters (1-12 waters, 48^3-128^3) as one
+           mixed-precision batch against the plain FP64 path (one FP64 context per instance, one
+           after another).  Times are CUDA events around initialise + solve on the solver stream.
+
 ``--impl reference`` times that reference CPU implementation alone (the reference has no
 GPU path that can run here: its kernels need CuPy, which is not installed).
-Multi-GPU (torchrun): every rank runs an independent replica (the solve does not shard);
-value = all ranks' updates / max-over-ranks time; scaling "weak".
+Multi-GPU (torchrun): every rank runs an independent replica of the period (one grid does not
+shard); value = all ranks' updates / max-over-ranks time; scaling "weak".  The cluster batch of
+``converge`` is partitioned over the ranks by cost (realmolecule_b200.shard), max over ranks:
+strong scaling of a fixed set of 96 solves.
 """
 from __future__ import annotations
 
@@ -50,11 +58,12 @@ PERIOD = 100
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="glycine128")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-converge", action="store_true")
     return ap.parse_args()
 
 
@@ -95,13 +104,13 @@ def run_reference_arm(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    # each bench step is a bounded sample: 20 solver steps (a 1/5 period) of the same workload
-    per = 20
+    # each bench step is one schedule period (100 solver steps) of the same workload
+    per = PERIOD
     rate, threads, dt = cpu_reference_rate(cfg, per * a.steps, per * a.warmup)
     line = {"metric": METRIC, "value": rate, "unit": "Gpt/s", "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": dt / a.steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": desc, "step": f"{per} solver steps (bounded sample of the period)"},
+            "config": {"workload": desc, "step": f"one schedule period = {per} solver steps"},
             "cpu_baseline": {"value": rate, "unit": "Gpt/s", "cores": threads, "kind": "reference",
                              "sample": f"{per * a.steps} solver steps after {per * a.warmup} warm-up"},
             "e2e": {"value": rate, "unit": "Gpt/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -123,8 +132,9 @@ class Clocks:
     def __enter__(self):
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                       "--format=csv,noheader,nounits", "-lms", "20"],
                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            time.sleep(0.5)  # nvidia-smi is sampling before the timed region starts
         except Exception:
             self.p = None
         return self
@@ -282,6 +292,9 @@ def run_ours(a):
     h2d = S3 * 12
     d2h = ctx.n_atoms * L.DOMAIN_LEN * 8
 
+    ctx.close()
+    conv = None if a.no_converge else converge_leg(stream, dist, rank, world)
+
     if rank == 0:
         peak, peak_kind = measured_peak()
         up = prof.get("update", {"ms": 0, "bytes": 0, "launches": 1})
@@ -291,9 +304,10 @@ def run_ours(a):
         cpu = None
         if world == 1 and not a.no_cpu_baseline:
             try:
-                rate, threads, dt = cpu_reference_rate(cfg, 40, 2)
+                nsteps = 40 * PERIOD
+                rate, threads, dt = cpu_reference_rate(cfg, nsteps, 2)
                 cpu = {"value": rate, "unit": "Gpt/s", "cores": threads, "kind": "reference",
-                       "sample": f"40 solver steps of {a.workload} after 2 warm-up ({dt:.1f} s)"}
+                       "sample": f"{nsteps} solver steps of {a.workload} after 2 warm-up ({dt:.1f} s)"}
             except Exception as e:  # the reference build is missing: say so
                 cpu = {"value": None, "unit": "Gpt/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
         line = {
@@ -313,13 +327,99 @@ def run_ours(a):
             "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 4), "GB/s": round(v["gbs"], 1)}
                         for k, v in prof.items()},
             "cpu_baseline": cpu,
+            "converge": conv,
             "clocks": clk.summary(),
             "gpu_launches": launches,
         }
         print(json.dumps(line), flush=True)
-    ctx.close()
     if dist:
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------
+# seconds to converge: mixed / batched against plain FP64 (new flavour)
+# ---------------------------------------------------------------------------------------
+TOL, CHECK, MAX_STEPS = 1e-6, 100, 40000
+
+
+def _timed(stream, fn):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    out = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return out, e0.elapsed_time(e1) * 1e-3
+
+
+def _max_over_ranks(dist, x):
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def converge_leg(stream, dist, rank, world):
+    from realmolecule_b200 import Context, configs
+    from realmolecule_b200.batch import Batch
+    from realmolecule_b200 import shard
+    out = {"criterion": f"|dE| < {TOL:g} Ha between checks {CHECK} steps apart (labels frozen after step 1)",
+           "timing": "CUDA events around initialise + solve on the solver stream (allocation excluded)"}
+
+    # glycine 128^3, one context per precision (every rank solves it; rank 0 reports)
+    g = configs.glycine128()
+    rows = configs.to_domain_atoms(g)
+    gly = {}
+    for prec in ("mixed", "fp64"):
+        c = Context(g.NN, g.screen, rows, flavor="new", precision=prec, label_until=1)
+        c.set_stream(stream.cuda_stream)
+        (steps, E), t = _timed(stream, lambda: (c.initialize(), c.solve(TOL, MAX_STEPS, CHECK))[1])
+        c.close()
+        gly[prec] = (_max_over_ranks(dist, t), int(steps), float(E))
+    out["glycine128"] = {"electrons": int(g.charges.sum()), "grid": f"{g.NN}^3 h={g.h}",
+                         "mixed_s": gly["mixed"][0], "fp64_s": gly["fp64"][0],
+                         "steps_mixed": gly["mixed"][1], "steps_fp64": gly["fp64"][1],
+                         "E_mixed": gly["mixed"][2], "E_fp64": gly["fp64"][2],
+                         "abs_dE_Ha": abs(gly["mixed"][2] - gly["fp64"][2])}
+
+    # 96 water clusters: this rank's cost share, mixed batch vs one FP64 context per instance
+    geoms = configs.clusters96()
+    inst = [{"NN": x.NN, "screen": x.screen, "atoms": configs.to_domain_atoms(x)} for x in geoms]
+    share = [inst[q] for q in shard.my_share(inst, rank, world)]
+    b = Batch(share, precision="mixed", label_until=1)
+    b.set_stream(stream.cuda_stream)
+    (cb, Eb), tb = _timed(stream, lambda: (b.initialize(), b.solve(TOL, MAX_STEPS, CHECK))[1])
+    if len(share) and (cb <= 0).any():
+        raise RuntimeError(f"mixed batch: {(cb <= 0).sum()} instances did not converge in {MAX_STEPS} steps")
+    pts = b.info()["interior_points"]
+    b.close()
+
+    def plain():
+        E, steps = [], []
+        for it in share:
+            c = Context(it["NN"], it["screen"], it["atoms"], flavor="new", precision="fp64", label_until=1)
+            c.set_stream(stream.cuda_stream)
+            c.initialize()
+            n, e = c.solve(TOL, MAX_STEPS, CHECK)
+            c.close()
+            E.append(e)
+            steps.append(n)
+        return np.array(E), np.array(steps)
+    (Ep, sp), tp = _timed(stream, plain)
+    tb, tp = _max_over_ranks(dist, tb), _max_over_ranks(dist, tp)
+    dE = _max_over_ranks(dist, float(np.max(np.abs(Eb - Ep))) if len(share) else 0.0)
+    out["clusters96"] = {"instances": len(inst), "ranks": world, "scaling": "strong",
+                         "interior_points_rank0": pts,
+                         "mixed_batched_s": tb, "fp64_plain_s": tp,
+                         "solves_per_s_mixed_batched": len(inst) / tb, "solves_per_s_fp64_plain": len(inst) / tp,
+                         "speedup_vs_fp64_plain": tp / tb, "max_abs_dE_Ha": dE,
+                         "steps_rank0": {"mixed_batched_max": int(cb.max()) if len(share) else 0,
+                                         "fp64_plain_max": int(sp.max()) if len(share) else 0,
+                                         "fp64_plain_sum": int(sp.sum()) if len(share) else 0}}
+    return out
 
 
 def main():

@@ -281,7 +281,7 @@ static int upload_plan(rq_batch* b, rq_batch::Plan& p, const std::vector<BItem>&
 }
 
 static void march_items(std::vector<BItem>& v, int inst, const Geo& g) {
-  const dim3 gr = march_grid(g);
+  const dim3 gr = nm_march_grid(g);
   for (unsigned z = 0; z < gr.z; ++z)
     for (unsigned y = 0; y < gr.y; ++y)
       for (unsigned x = 0; x < gr.x; ++x) v.push_back({inst, (int)x, (int)y, (int)z});
@@ -533,10 +533,10 @@ static int b_step(rq_batch* b, int s) {
   const double* sc = b->pending ? (const double*)b->scale : nullptr;
   if (norm) {
     BCK(cudaMemsetAsync(b->dnorm, 0, sizeof(double) * b->D, b->st));
-    kb_update<T, true><<<b->march[0].n, march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cp, b->cl, hd, dt,
+    kb_update<T, true><<<b->march[0].n, nm_march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cp, b->cl, hd, dt,
                                                                     b->dnorm, sc);
   } else {
-    kb_update<T, false><<<b->march[0].n, march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cp, b->cl, hd, dt,
+    kb_update<T, false><<<b->march[0].n, nm_march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cp, b->cl, hd, dt,
                                                                      nullptr, sc);
   }
   BL("update");
@@ -550,7 +550,7 @@ static int b_step(rq_batch* b, int s) {
   b->age = norm ? 0 : b->age + 1;
   if (label_step) {
     if ((rc = b_flush<T>(b)) != RQ_OK) return rc;
-    kb_evolve<T><<<b->march[0].n, march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cl,
+    kb_evolve<T><<<b->march[0].n, nm_march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cl,
                                                               (T)(float)f.boundary_speed, (T)(float)f.curv_reg);
     BL("evolve");
     b->cl ^= 1;
@@ -770,11 +770,11 @@ extern "C" int rq_batch_energy(rq_batch* b, double* out) {
   BCK(cudaMemsetAsync(b->dpd, 0, sizeof(double) * 4 * b->D, b->st));
   if (b->fp64) {
     using T = double;
-    kb_energy<T><<<b->march[0].n, march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cp, b->cl, b->dpd);
+    kb_energy<T><<<b->march[0].n, nm_march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cp, b->cl, b->dpd);
     BL("energy");
   } else {
     using T = float;
-    kb_energy<T><<<b->march[0].n, march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cp, b->cl, b->dpd);
+    kb_energy<T><<<b->march[0].n, nm_march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cp, b->cl, b->dpd);
     BL("energy");
   }
   std::vector<double> pd((size_t)4 * b->D);
@@ -909,6 +909,8 @@ int rq_batch_set_active_all(rq_batch* b) {
 
 // One converge-to-tol loop over the active instances; instances are dropped from the work lists
 // as they converge.  conv[q] receives the total step count at convergence.
+constexpr double kMixedFloor = 3e-9;  // relative |dE| a mixed-precision batch is asked to reach
+
 static int b_converge(rq_batch* b, std::vector<double> tol, int max_steps, int check, std::vector<int>& conv,
                       int& taken) {
   std::vector<double> e((size_t)b->n * RQ_ENERGY_LEN), prev(b->n);
@@ -946,10 +948,11 @@ extern "C" int rq_batch_solve(rq_batch* b, double tol_dE, int32_t max_steps, int
   std::vector<int> conv(b->n, -1);
   if ((rc = rq_batch_set_active_all(b)) != RQ_OK) return rc;
   if (!b->fp64) {
-    // fp32 fields stop improving near |dE| ~ 1e-8 |E|: converge to that floor in fp32 first ...
+    // fp32 fields: |dE| between checks has a noise floor of ~1e-9 |E| (round-off of psi and P),
+    // so converge to max(tol, kMixedFloor |E|) in fp32 first ...
     std::vector<double> e((size_t)b->n * RQ_ENERGY_LEN), tol(b->n);
     if ((rc = rq_batch_energy(b, e.data())) != RQ_OK) return rc;
-    for (int q = 0; q < b->n; ++q) tol[q] = std::max(tol_dE, 3e-8 * std::fabs(e[(size_t)q * RQ_ENERGY_LEN]));
+    for (int q = 0; q < b->n; ++q) tol[q] = std::max(tol_dE, kMixedFloor * std::fabs(e[(size_t)q * RQ_ENERGY_LEN]));
     std::vector<int> c32(b->n, -1);
     if ((rc = b_converge(b, tol, max_steps, check_interval, c32, taken)) != RQ_OK) return rc;
     // ... then widen the batch to FP64 and refine to tol_dE (iterative refinement)

@@ -28,6 +28,15 @@ template <> struct Ar<double> {
 constexpr int kNmFlatChunk = 16;     // points per thread of the flat (all S^3) bodies
 constexpr int kNmForceTile = 512;    // interior points staged per force tile
 constexpr int kNmRowPlanes = 4;      // planes i per block of the row-tiled multigrid bodies
+// March tile of the new flavour's stencil bodies: 16 (k) x 16 (j) threads, each walking kMarch
+// planes of i.  16 wide rows waste fewer lanes than 32 on the 47..127-point interiors of the
+// cluster grids (a warp still reads two contiguous 64-byte runs).
+constexpr int kNmTK = 16, kNmTJ = 16;
+inline dim3 nm_march_grid(const Geo& g) {
+  const int n = g.NN - 1;
+  return dim3((n + kNmTK - 1) / kNmTK, (n + kNmTJ - 1) / kNmTJ, (n + kMarch - 1) / kMarch);
+}
+inline dim3 nm_march_block() { return dim3(kNmTK, kNmTJ, 1); }
 constexpr int kCoarsestThreads = 256; // one block solves the coarsest level (<= 29^3 points)
 
 // ---------------------------------------------------------------------------------------
@@ -94,10 +103,11 @@ __device__ __forceinline__ void nm_init_body(T* __restrict__ U, int* __restrict_
 
 // ITP update (same-label Neumann Laplacian) on the march tile (bx, by, bz); with ACC the FP64
 // norm of the new psi per label goes through the block table (caller inits and flushes it).
-// With a non-null `scale` the stored psi is one normalisation behind: every value read is first
-// multiplied by scale[label of the centre] (the same for every neighbour that is used, since only
-// same-label neighbours enter), which reproduces "normalise, then update" bit for bit without a
-// separate pass over psi.
+// With a non-null `scale` the stored psi is one normalisation behind.  The update is linear in
+// psi and reads only neighbours of the centre's label (a neighbour of another label is replaced
+// by the centre value), so the pending per-domain scale multiplies the result once: psi' =
+// scale[label] * update(psi), formed in FP64 and rounded once -- normalise-then-update up to
+// rounding, without a separate pass over psi.
 template <typename T, bool ACC>
 __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __restrict__ Unew, const T* __restrict__ K,
                                                const T* __restrict__ P, const int* __restrict__ label, const Geo& g,
@@ -107,31 +117,31 @@ __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __res
   using A = Ar<T>;
   RunSum<1> rs;
   rs.reset();
-  const int k = 1 + bx * kThreadsK + threadIdx.x;
-  const int j = 1 + by * kThreadsJ + threadIdx.y;
+  const int k = 1 + bx * kNmTK + threadIdx.x;
+  const int j = 1 + by * kNmTJ + threadIdx.y;
   const int i0 = 1 + bz * kMarch;
   if (k < g.NN && j < g.NN && i0 < g.NN) {
     const int iend = min(i0 + kMarch, g.NN);
     const long long S = g.S, S2 = g.S2;
     long long id = (long long)i0 * S2 + j * S + k;
-    T u_m = U[id - S2], u_c = U[id];
-    int l_m = label[id - S2], l_c = label[id];
+    T u_m = __ldg(U + id - S2), u_c = __ldg(U + id);
+    int l_m = __ldg(label + id - S2), l_c = __ldg(label + id);
     for (int i = i0; i < iend; ++i, id += S2) {
-      const T u_p = U[id + S2];
-      const int l_p = label[id + S2];
-      // a pending normalisation: each value is scaled in FP64 and rounded once, so fp32 fields
-      // carry no per-domain bias from rounding the scale itself
-      const double sc = scale ? scale[min(max(l_c, 0), nDom - 1)] : 1.0;
-      auto sv = [&](T v) { return scale ? (T)((double)v * sc) : v; };
-      const T uc = sv(u_c);
-      const T a = (l_p == l_c) ? sv(u_p) : uc;
-      const T b = (l_m == l_c) ? sv(u_m) : uc;
-      const T c = (label[id + S] == l_c) ? sv(U[id + S]) : uc;
-      const T d = (label[id - S] == l_c) ? sv(U[id - S]) : uc;
-      const T e = (label[id + 1] == l_c) ? sv(U[id + 1]) : uc;
-      const T f = (label[id - 1] == l_c) ? sv(U[id - 1]) : uc;
-      const T lap = A::sub(A::add(A::add(A::add(A::add(A::add(a, b), c), d), e), f), A::mul(T(6), uc));
-      const T out = A::add(A::add(uc, A::mul(half_dv, lap)), A::mul(A::mul(dt, A::sub(K[id], A::mul(T(2), P[id]))), uc));
+      const T u_p = __ldg(U + id + S2);
+      const int l_p = __ldg(label + id + S2);
+      const T ujp = __ldg(U + id + S), ujm = __ldg(U + id - S), ukp = __ldg(U + id + 1), ukm = __ldg(U + id - 1);
+      const int ljp = __ldg(label + id + S), ljm = __ldg(label + id - S), lkp = __ldg(label + id + 1),
+                lkm = __ldg(label + id - 1);
+      const T kv = __ldg(K + id), pv = __ldg(P + id);
+      const T a = (l_p == l_c) ? u_p : u_c;
+      const T b = (l_m == l_c) ? u_m : u_c;
+      const T c = (ljp == l_c) ? ujp : u_c;
+      const T d = (ljm == l_c) ? ujm : u_c;
+      const T e = (lkp == l_c) ? ukp : u_c;
+      const T f = (lkm == l_c) ? ukm : u_c;
+      const T lap = A::sub(A::add(A::add(A::add(A::add(A::add(a, b), c), d), e), f), A::mul(T(6), u_c));
+      T out = A::add(A::add(u_c, A::mul(half_dv, lap)), A::mul(A::mul(dt, A::sub(kv, A::mul(T(2), pv))), u_c));
+      if (scale) out = (T)((double)out * __ldg(scale + min(max(l_c, 0), nDom - 1)));
       Unew[id] = out;
       if (ACC) {
         const double r = (double)out * (double)out * h3;
@@ -140,7 +150,7 @@ __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __res
       u_m = u_c; u_c = u_p; l_m = l_c; l_c = l_p;
     }
   }
-  if (ACC) rs.finish_warp(tab, norms);  // every lane of the (32 x 8) block reaches this point
+  if (ACC) rs.finish_warp(tab, norms);  // every lane of the block reaches this point
 }
 
 // U *= scale[label] (FP64 product, rounded once) for labels in [0, nDom) over kNmFlatChunk*256
@@ -346,8 +356,8 @@ __device__ __forceinline__ void nm_energy_body(const T* __restrict__ U, const T*
   RunSum<4> rs;
   rs.reset();
   const double h3 = h * h * h;
-  const int k = 1 + bx * kThreadsK + threadIdx.x;
-  const int j = 1 + by * kThreadsJ + threadIdx.y;
+  const int k = 1 + bx * kNmTK + threadIdx.x;
+  const int j = 1 + by * kNmTJ + threadIdx.y;
   const int i0 = 1 + bz * kMarch;
   if (k < g.NN && j < g.NN && i0 < g.NN) {
     const int iend = min(i0 + kMarch, g.NN);
@@ -377,8 +387,8 @@ __device__ __forceinline__ void nm_evolve_body(const int* __restrict__ labIn, in
                                                const T* __restrict__ U, float* __restrict__ W, const Geo& g, T dt_w,
                                                T curvReg, int bx, int by, int bz) {
   using A = Ar<T>;
-  const int k = 1 + bx * kThreadsK + threadIdx.x;
-  const int j = 1 + by * kThreadsJ + threadIdx.y;
+  const int k = 1 + bx * kNmTK + threadIdx.x;
+  const int j = 1 + by * kNmTJ + threadIdx.y;
   const int i0 = 1 + bz * kMarch;
   if (k >= g.NN || j >= g.NN || i0 >= g.NN) return;
   const int iend = min(i0 + kMarch, g.NN);

@@ -139,10 +139,10 @@ cudaError_t nm_update(const T* U, T* Unew, const T* K, const T* P, const int* la
                       double h3, int nDom, double* norms, cudaStream_t st, const double* scale) {
   if (g.NN < 2) return cudaSuccess;
   if (norms)
-    k_nm_update<T, true><<<march_grid(g), march_block(), 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, norms,
+    k_nm_update<T, true><<<nm_march_grid(g), nm_march_block(), 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, norms,
                                                                    scale);
   else
-    k_nm_update<T, false><<<march_grid(g), march_block(), 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom,
+    k_nm_update<T, false><<<nm_march_grid(g), nm_march_block(), 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom,
                                                                     nullptr, scale);
   return cudaGetLastError();
 }
@@ -215,14 +215,14 @@ template <typename T>
 cudaError_t nm_energy(const T* U, const T* K, const T* P, const int* label, const Geo& g, double h, int nDom, double* pd,
                       cudaStream_t st) {
   if (g.NN < 2) return cudaSuccess;
-  k_nm_energy<T><<<march_grid(g), march_block(), 0, st>>>(U, K, P, label, g, h, nDom, pd);
+  k_nm_energy<T><<<nm_march_grid(g), nm_march_block(), 0, st>>>(U, K, P, label, g, h, nDom, pd);
   return cudaGetLastError();
 }
 template <typename T>
 cudaError_t nm_evolve(const int* labIn, int* labOut, const T* U, float* W, const Geo& g, double dt_w, double curvReg,
                       cudaStream_t st) {
   if (g.NN < 2) return cudaSuccess;
-  k_nm_evolve<T><<<march_grid(g), march_block(), 0, st>>>(labIn, labOut, U, W, g, (T)(float)dt_w, (T)(float)curvReg);
+  k_nm_evolve<T><<<nm_march_grid(g), nm_march_block(), 0, st>>>(labIn, labOut, U, W, g, (T)(float)dt_w, (T)(float)curvReg);
   return cudaGetLastError();
 }
 template <typename T>

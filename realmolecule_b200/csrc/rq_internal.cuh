@@ -96,6 +96,13 @@ __device__ __forceinline__ void dom_table_flush(DomTable<NQ, NSLOT>& t, double* 
   }
 }
 
+// lane of the calling thread in its warp (blocks of any shape)
+__device__ __forceinline__ int lane_id() {
+  int l;
+  asm("mov.u32 %0, %%laneid;" : "=r"(l));
+  return l;
+}
+
 // Per-thread running sum keyed by label; flushes into the block table on label change.
 template <int NQ>
 struct RunSum {
@@ -128,7 +135,7 @@ struct RunSum {
   template <int NSLOT>
   __device__ __forceinline__ void finish_warp(DomTable<NQ, NSLOT>& t, double* global) {
     const unsigned peers = __match_any_sync(0xffffffffu, label);
-    const int lane = threadIdx.x & 31;
+    const int lane = lane_id();
     double s[NQ];
 #pragma unroll
     for (int q = 0; q < NQ; ++q) s[q] = 0.0;
