@@ -214,9 +214,23 @@ __global__ void __launch_bounds__(256) kb_force(const BInst* __restrict__ ins, c
 // =========================================================================================
 using namespace rq;
 
+namespace {
+// The two precision sets of a batch: every instance holds its fields either in fp32 (kF32) or
+// in FP64 (kF64).  A mixed-precision batch starts all-fp32 and moves instances to FP64 one by
+// one as they reach the fp32 resolution of their energy; each kernel of a step is then one
+// launch per non-empty set.
+constexpr int kF32 = 0, kF64 = 1;
+constexpr double kMixedFloor = 3e-9;  // relative |dE| between checks that fp32 fields resolve
+}  // namespace
+
+// Work items of one instance for every list; built once at creation, concatenated by build_plans.
+struct InstItems {
+  std::vector<BItem> march[kMaxLev], rbgs[kMaxLev], restr[kMaxLev], zero[kMaxLev], coarse[kMaxLev];
+  std::vector<BItem> flat16, flat1, force;
+};
+
 struct rq_batch {
   int n = 0;
-  bool fp64 = false;
   rq_config cfg{};
   double dv = 0.2;
   std::vector<BInst> hin;         // host copy of the instance table
@@ -224,16 +238,19 @@ struct rq_batch {
   std::vector<std::vector<rq_atom>> atoms;
   std::vector<void*> allocs;
   int D = 0, A = 0;               // total domains / entries
-  double *dnorm = nullptr, *dpd = nullptr, *dF = nullptr, *Zdom = nullptr, *at_all = nullptr;
-  void* scale = nullptr;
+  double *dnorm = nullptr, *dpd = nullptr, *dF = nullptr, *Zdom = nullptr, *at_all = nullptr, *scale = nullptr;
   int* err = nullptr;
   float4* seeds_all = nullptr;
   int maxlev = 0;
-  // work lists
+  // work lists, one set per precision
   struct Plan { BItem* d = nullptr; int n = 0, cap = 0; };
-  Plan march[kMaxLev], rbgs[kMaxLev], restr[kMaxLev], zero[kMaxLev], coarse[kMaxLev];
+  struct Plans {
+    Plan march[kMaxLev], rbgs[kMaxLev], restr[kMaxLev], zero[kMaxLev], coarse[kMaxLev];
+    Plan flat16, flat1, force;
+  };
+  Plans pl[2];
+  Plan one;                       // scratch list: one instance's flat items
   size_t coarse_smem[kMaxLev] = {};
-  Plan flat16, flat1, force;
   cudaStream_t st = nullptr, own = nullptr;
   int cu = 0, cp = 0, cl = 0, steps_done = 0;
   long long launches = 0;
@@ -241,10 +258,11 @@ struct rq_batch {
   int graph_post[32] = {};
   long long graph_launches[32] = {};
   std::vector<char> active;       // instances still being stepped (solve drops converged ones)
+  std::vector<char> f64;          // instances whose fields are FP64 (created so, or promoted)
+  std::vector<InstItems> items;   // per-instance work items (built once)
   std::vector<double> lastE;      // last energies per instance (n x RQ_ENERGY_LEN)
   bool pending = false;           // psi awaits the per-domain scale (applied by the next update or a flush)
   int age = 0;                    // updates since psi was last normalised (0: normalised or pending)
-  bool promoted = false;          // a mixed batch switched to FP64 for its final refinement
   std::string last_error;
 };
 
@@ -256,6 +274,11 @@ struct rq_batch {
       return _e == cudaErrorMemoryAllocation ? RQ_ENOMEM : RQ_ECUDA;               \
     }                                                                              \
   } while (0)
+#define BRC(call)                        \
+  do {                                   \
+    const int _r = (call);               \
+    if (_r != RQ_OK) return _r;          \
+  } while (0)
 
 static int balloc(rq_batch* b, void** p, size_t bytes) {
   BCK(cudaMalloc(p, bytes));
@@ -263,16 +286,12 @@ static int balloc(rq_batch* b, void** p, size_t bytes) {
   BCK(cudaMemsetAsync(*p, 0, bytes, b->st));
   return RQ_OK;
 }
-#define BALLOC(ptr, bytes)                                     \
-  do {                                                         \
-    int _r = balloc(b, (void**)&(ptr), (bytes));               \
-    if (_r != RQ_OK) return _r;                                \
-  } while (0)
+#define BALLOC(ptr, bytes) BRC(balloc(b, (void**)&(ptr), (bytes)))
 
 static int upload_plan(rq_batch* b, rq_batch::Plan& p, const std::vector<BItem>& v) {
   p.n = (int)v.size();
   if (!p.n) return RQ_OK;
-  if (p.n > p.cap) {  // first build allocates the full size; later builds (fewer instances) reuse it
+  if (p.n > p.cap) {  // the first build allocates the full size; later builds (fewer instances) reuse it
     BALLOC(p.d, sizeof(BItem) * v.size());
     p.cap = p.n;
   }
@@ -287,78 +306,98 @@ static void march_items(std::vector<BItem>& v, int inst, const Geo& g) {
       for (unsigned x = 0; x < gr.x; ++x) v.push_back({inst, (int)x, (int)y, (int)z});
 }
 
-// Work lists over the active instances (all of them at creation; solve drops converged ones).
-static int build_plans(rq_batch* b) {
-  const int n = b->n;
-  // work lists
-  for (int l = 0; l < b->maxlev; ++l) {
-    std::vector<BItem> m, r, rs, z, c;
-    for (int q = 0; q < n; ++q) {
-      const BInst& I = b->hin[q];
-      if (l >= I.nlev || !b->active[q]) continue;
-      march_items(m, q, I.lg[l]);
-      if (l == I.nlev - 1) {
-        c.push_back({q, 0, 0, 0});
-        b->coarse_smem[l] = std::max(b->coarse_smem[l], sizeof(double) * 2 * (size_t)I.lg[l].S3);
-        continue;
-      }
-      const int nn = I.lg[l].NN - 1;
-      for (int zz = 0; zz < (nn + kNmRowPlanes - 1) / kNmRowPlanes; ++zz)
-        for (int y = 0; y < (nn + 7) / 8; ++y)
-          for (int x = 0; x < (nn + 63) / 64; ++x) r.push_back({q, x, y, zz});
-      const long long nc = (long long)(I.lg[l + 1].NN - 1) * (I.lg[l + 1].NN - 1) * (I.lg[l + 1].NN - 1);
-      for (long long x = 0; x < (nc + 255) / 256; ++x) rs.push_back({q, (int)x, 0, 0});
-      for (long long x = 0; x < (I.lg[l + 1].S3 + 256 * kNmFlatChunk - 1) / (256 * kNmFlatChunk); ++x)
-        z.push_back({q, (int)x, 0, 0});
+static void flat_items(std::vector<BItem>& v, int inst, long long npts, long long per_block) {
+  for (long long x = 0; x < (npts + per_block - 1) / per_block; ++x) v.push_back({inst, (int)x, 0, 0});
+}
+
+static void make_items(const BInst& I, int q, InstItems& it) {
+  for (int l = 0; l < I.nlev; ++l) {
+    march_items(it.march[l], q, I.lg[l]);
+    if (l == I.nlev - 1) {
+      it.coarse[l].push_back({q, 0, 0, 0});
+      continue;
     }
-    int rc;
-    if ((rc = upload_plan(b, b->march[l], m)) || (rc = upload_plan(b, b->rbgs[l], r)) ||
-        (rc = upload_plan(b, b->restr[l], rs)) || (rc = upload_plan(b, b->zero[l], z)) ||
-        (rc = upload_plan(b, b->coarse[l], c)))
-      return rc;
+    const int nn = I.lg[l].NN - 1;
+    for (int zz = 0; zz < (nn + kNmRowPlanes - 1) / kNmRowPlanes; ++zz)
+      for (int y = 0; y < (nn + 7) / 8; ++y)
+        for (int x = 0; x < (nn + 63) / 64; ++x) it.rbgs[l].push_back({q, x, y, zz});
+    const long long nc = (long long)(I.lg[l + 1].NN - 1) * (I.lg[l + 1].NN - 1) * (I.lg[l + 1].NN - 1);
+    flat_items(it.restr[l], q, nc, 256);
+    flat_items(it.zero[l], q, I.lg[l + 1].S3, 256 * kNmFlatChunk);
   }
-  std::vector<BItem> f16, f1, fo;
-  for (int q = 0; q < n; ++q) {
-    if (!b->active[q]) continue;
-    const BInst& I = b->hin[q];
-    for (long long x = 0; x < (I.g.S3 + 256 * kNmFlatChunk - 1) / (256 * kNmFlatChunk); ++x) f16.push_back({q, (int)x, 0, 0});
-    for (long long x = 0; x < (I.g.S3 + 255) / 256; ++x) f1.push_back({q, (int)x, 0, 0});
-    const long long n1 = I.g.NN - 1, ntiles = (n1 * n1 * n1 + kNmForceTile - 1) / kNmForceTile;
-    const int groups = (int)std::min<long long>(ntiles, 32);
-    for (int ch = 0; ch < (I.nAt + 255) / 256; ++ch)
-      for (int t = 0; t < groups; ++t) fo.push_back({q, t, groups, ch});
+  flat_items(it.flat16, q, I.g.S3, 256 * kNmFlatChunk);
+  flat_items(it.flat1, q, I.g.S3, 256);
+  const long long n1 = I.g.NN - 1, ntiles = (n1 * n1 * n1 + kNmForceTile - 1) / kNmForceTile;
+  const int groups = (int)std::min<long long>(ntiles, 32);
+  for (int ch = 0; ch < (I.nAt + 255) / 256; ++ch)
+    for (int t = 0; t < groups; ++t) it.force.push_back({q, t, groups, ch});
+}
+
+// Work lists of each precision set over the active instances (all of them at creation; solve
+// drops converged ones and moves promoted ones to the FP64 set): concatenations of the
+// instances' cached items.  Captured graphs hold the old lists, so they are dropped.
+static int build_plans(rq_batch* b) {
+  using Items = std::vector<BItem>;
+  for (int p = 0; p < 2; ++p) {
+    rq_batch::Plans& P = b->pl[p];
+    std::vector<int> mine;
+    for (int q = 0; q < b->n; ++q)
+      if (b->active[q] && (b->f64[q] ? kF64 : kF32) == p) mine.push_back(q);
+    auto gather = [&](rq_batch::Plan& plan, auto member) -> int {
+      Items v;
+      for (int q : mine) {
+        const Items& src = member(b->items[q]);
+        v.insert(v.end(), src.begin(), src.end());
+      }
+      return upload_plan(b, plan, v);
+    };
+    for (int l = 0; l < b->maxlev; ++l) {
+      BRC(gather(P.march[l], [l](const InstItems& it) -> const Items& { return it.march[l]; }));
+      BRC(gather(P.rbgs[l], [l](const InstItems& it) -> const Items& { return it.rbgs[l]; }));
+      BRC(gather(P.restr[l], [l](const InstItems& it) -> const Items& { return it.restr[l]; }));
+      BRC(gather(P.zero[l], [l](const InstItems& it) -> const Items& { return it.zero[l]; }));
+      BRC(gather(P.coarse[l], [l](const InstItems& it) -> const Items& { return it.coarse[l]; }));
+    }
+    BRC(gather(P.flat16, [](const InstItems& it) -> const Items& { return it.flat16; }));
+    BRC(gather(P.flat1, [](const InstItems& it) -> const Items& { return it.flat1; }));
+    BRC(gather(P.force, [](const InstItems& it) -> const Items& { return it.force; }));
   }
-  int rc;
-  if ((rc = upload_plan(b, b->flat16, f16)) || (rc = upload_plan(b, b->flat1, f1)) || (rc = upload_plan(b, b->force, fo)))
-    return rc;
   for (auto& g : b->graph)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   return RQ_OK;
 }
 
+// field buffers of instance q in its current precision (level 0 fields and the multigrid levels)
+static int alloc_fields(rq_batch* b, int q) {
+  BInst& I = b->hin[q];
+  const size_t es = b->f64[q] ? sizeof(double) : sizeof(float);
+  const size_t S3 = (size_t)I.g.S3;
+  for (int k = 0; k < 2; ++k) {
+    BALLOC(I.U[k], S3 * es);
+    BALLOC(I.P[k], S3 * es);
+  }
+  BALLOC(I.K, S3 * es);
+  for (int l = 0; l < I.nlev; ++l) {
+    const size_t s3 = (size_t)I.lg[l].S3;
+    I.lP[l] = I.lf[l] = I.lr[l] = nullptr;
+    if (l > 0) {
+      BALLOC(I.lP[l], s3 * es);
+      BALLOC(I.lf[l], s3 * es);
+    }
+    if (l < I.nlev - 1) BALLOC(I.lr[l], s3 * es);
+  }
+  return RQ_OK;
+}
+
 static int build(rq_batch* b) {
   const int n = b->n;
-  const size_t es = b->fp64 ? sizeof(double) : sizeof(float);
-  // per-instance buffers and level hierarchy
   for (int q = 0; q < n; ++q) {
     BInst& I = b->hin[q];
-    const size_t S3 = (size_t)I.g.S3;
-    for (int k = 0; k < 2; ++k) {
-      BALLOC(I.U[k], S3 * es);
-      BALLOC(I.P[k], S3 * es);
-      BALLOC(I.lab[k], S3 * sizeof(int));
-    }
-    BALLOC(I.K, S3 * es);
-    BALLOC(I.W, S3 * sizeof(float));
-    for (int l = 0; l < I.nlev; ++l) {
-      const size_t s3 = (size_t)I.lg[l].S3;
-      I.lP[l] = I.lf[l] = I.lr[l] = nullptr;
-      if (l > 0) {
-        BALLOC(I.lP[l], s3 * es);
-        BALLOC(I.lf[l], s3 * es);
-      }
-      if (l < I.nlev - 1) BALLOC(I.lr[l], s3 * es);
-    }
+    BRC(alloc_fields(b, q));
+    for (int k = 0; k < 2; ++k) BALLOC(I.lab[k], (size_t)I.g.S3 * sizeof(int));
+    BALLOC(I.W, (size_t)I.g.S3 * sizeof(float));
+    const int lc = I.nlev - 1;
+    b->coarse_smem[lc] = std::max(b->coarse_smem[lc], sizeof(double) * 2 * (size_t)I.lg[lc].S3);
   }
   // batch-wide per-domain arrays and atom tables
   BALLOC(b->dnorm, sizeof(double) * b->D);
@@ -399,8 +438,9 @@ static int build(rq_batch* b) {
     BCK(cudaMemcpyAsync(b->seeds_all, seeds.data(), sizeof(float4) * seeds.size(), cudaMemcpyHostToDevice, b->st));
   BALLOC(b->din, sizeof(BInst) * n);
   BCK(cudaMemcpyAsync(b->din, b->hin.data(), sizeof(BInst) * n, cudaMemcpyHostToDevice, b->st));
-  int rc = build_plans(b);
-  if (rc != RQ_OK) return rc;
+  b->items.resize(n);
+  for (int q = 0; q < n; ++q) make_items(b->hin[q], q, b->items[q]);
+  BRC(build_plans(b));
   size_t smax = 0;
   for (int l = 0; l < b->maxlev; ++l) smax = std::max(smax, b->coarse_smem[l]);
   if (smax > 200 * 1024) {
@@ -415,7 +455,6 @@ static int build(rq_batch* b) {
 
 int rq_batch_set_active_all(rq_batch* b);
 
-template <typename T>
 static int b_launch_err(rq_batch* b, const char* what) {
   cudaError_t e = cudaGetLastError();
   b->launches++;
@@ -425,159 +464,172 @@ static int b_launch_err(rq_batch* b, const char* what) {
   }
   return RQ_OK;
 }
-#define BL(what)                                              \
-  do {                                                        \
-    int _r = b_launch_err<T>(b, what);                        \
-    if (_r != RQ_OK) return _r;                               \
-  } while (0)
+#define BL(what) BRC(b_launch_err(b, what))
+
+// f(T(), set) for the fp32 and the FP64 set, in that order
+template <class F>
+static int each_set(F&& f) {
+  const int r = f(float(0), kF32);
+  return r != RQ_OK ? r : f(double(0), kF64);
+}
 
 template <typename T>
-static int b_vcycle(rq_batch* b) {
+static int b_vcycle(rq_batch* b, int p) {
+  const rq_batch::Plans& P = b->pl[p];
   const int pre = b->cfg.mg_pre, post = b->cfg.mg_post;
+  const dim3 rb(32, 8);
+  auto smooth = [&](int l) -> int {
+    for (int color = 0; color < 2; ++color) {
+      if (l == 0)
+        kb_rbgs<T, true><<<P.rbgs[l].n, rb, 0, b->st>>>(b->din, P.rbgs[l].d, l, b->cu, b->cp, color);
+      else
+        kb_rbgs<T, false><<<P.rbgs[l].n, rb, 0, b->st>>>(b->din, P.rbgs[l].d, l, b->cu, b->cp, color);
+      BL("rbgs");
+    }
+    return RQ_OK;
+  };
   for (int l = 0; l < b->maxlev; ++l) {
-    if (b->coarse[l].n) {
-      kb_coarsest<T><<<b->coarse[l].n, kCoarsestThreads, b->coarse_smem[l], b->st>>>(b->din, b->coarse[l].d, l,
-                                                                           b->cfg.mg_coarse_sweeps);
+    if (P.coarse[l].n) {
+      kb_coarsest<T><<<P.coarse[l].n, kCoarsestThreads, b->coarse_smem[l], b->st>>>(b->din, P.coarse[l].d, l,
+                                                                                   b->cfg.mg_coarse_sweeps);
       BL("coarsest");
     }
-    if (!b->rbgs[l].n) continue;
-    for (int s = 0; s < pre; ++s)
-      for (int color = 0; color < 2; ++color) {
-        if (l == 0)
-          kb_rbgs<T, true><<<b->rbgs[l].n, dim3(32, 8), 0, b->st>>>(b->din, b->rbgs[l].d, l, b->cu, b->cp, color);
-        else
-          kb_rbgs<T, false><<<b->rbgs[l].n, dim3(32, 8), 0, b->st>>>(b->din, b->rbgs[l].d, l, b->cu, b->cp, color);
-        BL("rbgs");
-      }
+    if (!P.rbgs[l].n) continue;
+    for (int s = 0; s < pre; ++s) BRC(smooth(l));
     if (l == 0)
-      kb_residual<T, true><<<b->rbgs[l].n, dim3(32, 8), 0, b->st>>>(b->din, b->rbgs[l].d, l, b->cu, b->cp);
+      kb_residual<T, true><<<P.rbgs[l].n, rb, 0, b->st>>>(b->din, P.rbgs[l].d, l, b->cu, b->cp);
     else
-      kb_residual<T, false><<<b->rbgs[l].n, dim3(32, 8), 0, b->st>>>(b->din, b->rbgs[l].d, l, b->cu, b->cp);
+      kb_residual<T, false><<<P.rbgs[l].n, rb, 0, b->st>>>(b->din, P.rbgs[l].d, l, b->cu, b->cp);
     BL("residual");
-    kb_restrict<T><<<b->restr[l].n, 256, 0, b->st>>>(b->din, b->restr[l].d, l);
+    kb_restrict<T><<<P.restr[l].n, 256, 0, b->st>>>(b->din, P.restr[l].d, l);
     BL("restrict");
-    kb_zero<T><<<b->zero[l].n, 256, 0, b->st>>>(b->din, b->zero[l].d, l + 1);
+    kb_zero<T><<<P.zero[l].n, 256, 0, b->st>>>(b->din, P.zero[l].d, l + 1);
     BL("zero");
   }
   for (int l = b->maxlev - 2; l >= 0; --l) {
-    if (!b->rbgs[l].n) continue;
-    kb_prolong<T><<<b->rbgs[l].n, dim3(32, 8), 0, b->st>>>(b->din, b->rbgs[l].d, l, b->cp);
+    if (!P.rbgs[l].n) continue;
+    kb_prolong<T><<<P.rbgs[l].n, rb, 0, b->st>>>(b->din, P.rbgs[l].d, l, b->cp);
     BL("prolong");
-    for (int s = 0; s < post; ++s)
-      for (int color = 0; color < 2; ++color) {
-        if (l == 0)
-          kb_rbgs<T, true><<<b->rbgs[l].n, dim3(32, 8), 0, b->st>>>(b->din, b->rbgs[l].d, l, b->cu, b->cp, color);
-        else
-          kb_rbgs<T, false><<<b->rbgs[l].n, dim3(32, 8), 0, b->st>>>(b->din, b->rbgs[l].d, l, b->cu, b->cp, color);
-        BL("rbgs");
-      }
+    for (int s = 0; s < post; ++s) BRC(smooth(l));
   }
   return RQ_OK;
 }
 
 template <typename T>
-static int b_normalize(rq_batch* b, bool accumulate) {
-  if (b->flat16.n == 0) return RQ_OK;
-  if (accumulate) {
-    BCK(cudaMemsetAsync(b->dnorm, 0, sizeof(double) * b->D, b->st));
-    kb_norms<T><<<b->flat16.n, 256, 0, b->st>>>(b->din, b->flat16.d, b->cu, b->cl, b->dnorm);
-    BL("norms");
-  }
-  BCK(nm_norm_scale<T>(b->dnorm, b->Zdom, b->D, (double*)b->scale, b->err, b->st));
-  b->launches++;
-  kb_apply_scale<T><<<b->flat16.n, 256, 0, b->st>>>(b->din, b->flat16.d, b->cu, b->cl, (const double*)b->scale);
+static int b_apply(rq_batch* b, int p) {
+  const rq_batch::Plan& f = b->pl[p].flat16;
+  if (!f.n) return RQ_OK;
+  kb_apply_scale<T><<<f.n, 256, 0, b->st>>>(b->din, f.d, b->cu, b->cl, b->scale);
   BL("apply_scale");
+  return RQ_OK;
+}
+
+static int b_normalize(rq_batch* b) {
+  BCK(cudaMemsetAsync(b->dnorm, 0, sizeof(double) * b->D, b->st));
+  BRC(each_set([&](auto tag, int p) -> int {
+    using T = decltype(tag);
+    const rq_batch::Plan& f = b->pl[p].flat16;
+    if (!f.n) return RQ_OK;
+    kb_norms<T><<<f.n, 256, 0, b->st>>>(b->din, f.d, b->cu, b->cl, b->dnorm);
+    BL("norms");
+    return RQ_OK;
+  }));
+  BCK(nm_norm_scale<double>(b->dnorm, b->Zdom, b->D, b->scale, b->err, b->st));
+  b->launches++;
+  BRC(each_set([&](auto tag, int p) { return b_apply<decltype(tag)>(b, p); }));
   b->pending = false;
   b->age = 0;
   return RQ_OK;
 }
 
 // materialise a pending per-domain normalisation (needed by the multigrid, labels and readouts)
-template <typename T>
 static int b_flush(rq_batch* b) {
-  if (!b->pending || b->flat16.n == 0) return RQ_OK;
-  kb_apply_scale<T><<<b->flat16.n, 256, 0, b->st>>>(b->din, b->flat16.d, b->cu, b->cl, (const double*)b->scale);
-  BL("apply_scale");
+  if (!b->pending) return RQ_OK;
+  BRC(each_set([&](auto tag, int p) { return b_apply<decltype(tag)>(b, p); }));
   b->pending = false;
   return RQ_OK;
 }
-static int b_flush_any(rq_batch* b) { return b->fp64 ? b_flush<double>(b) : b_flush<float>(b); }
 
 // the normalised state every readout reports: flush a pending scale, or normalise now when
 // updates ran since the last normalisation
-template <typename T>
-static int b_ready(rq_batch* b) {
-  if (b->age == 0) return b_flush<T>(b);
-  const int rc = b_normalize<T>(b, true);
-  b->age = 0;
-  return rc;
-}
-static int b_ready_any(rq_batch* b) { return b->fp64 ? b_ready<double>(b) : b_ready<float>(b); }
+static int b_ready(rq_batch* b) { return b->age == 0 ? b_flush(b) : b_normalize(b); }
 
-template <typename T>
+static bool any_active(const rq_batch* b) { return b->pl[kF32].march[0].n + b->pl[kF64].march[0].n > 0; }
+
 static int b_step(rq_batch* b, int s) {
   const rq_config& f = b->cfg;
-  int rc;
-  if (b->march[0].n == 0) return RQ_OK;  // no active instance
+  if (!any_active(b)) return RQ_OK;
   if (s % f.poisson_interval == 0) {
-    if ((rc = b_flush<T>(b)) != RQ_OK) return rc;
-    if ((rc = b_vcycle<T>(b)) != RQ_OK) return rc;
+    BRC(b_flush(b));
+    BRC(each_set([&](auto tag, int p) { return b_vcycle<decltype(tag)>(b, p); }));
   }
   // normalised after every norm_interval-th update and always after the update that precedes a
   // V-cycle or a label pass (the update commutes with per-domain scales between Poisson solves)
   const bool label_step = s % f.label_interval == 0 && (f.label_until <= 0 || s <= f.label_until);
   const bool norm = (s + 1) % f.norm_interval == 0 || (s + 1) % f.poisson_interval == 0 || label_step;
-  const T hd = (T)(0.5 * b->dv);
   // dt = dv h^2 differs per instance only through h: every instance of a batch shares h
-  const T dt = (T)(b->dv * b->hin[0].h * b->hin[0].h);
-  const double* sc = b->pending ? (const double*)b->scale : nullptr;
-  if (norm) {
-    BCK(cudaMemsetAsync(b->dnorm, 0, sizeof(double) * b->D, b->st));
-    kb_update<T, true><<<b->march[0].n, nm_march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cp, b->cl, hd, dt,
-                                                                    b->dnorm, sc);
-  } else {
-    kb_update<T, false><<<b->march[0].n, nm_march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cp, b->cl, hd, dt,
-                                                                     nullptr, sc);
-  }
-  BL("update");
+  const double hd = 0.5 * b->dv, dt = b->dv * b->hin[0].h * b->hin[0].h;
+  const double* sc = b->pending ? b->scale : nullptr;
+  if (norm) BCK(cudaMemsetAsync(b->dnorm, 0, sizeof(double) * b->D, b->st));
+  BRC(each_set([&](auto tag, int p) -> int {
+    using T = decltype(tag);
+    const rq_batch::Plan& m = b->pl[p].march[0];
+    if (!m.n) return RQ_OK;
+    if (norm)
+      kb_update<T, true><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cp, b->cl, (T)hd, (T)dt, b->dnorm,
+                                                             sc);
+    else
+      kb_update<T, false><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cp, b->cl, (T)hd, (T)dt, nullptr,
+                                                              sc);
+    BL("update");
+    return RQ_OK;
+  }));
   b->cu ^= 1;
   b->pending = false;
   if (norm) {  // applied by the next update (or a flush)
-    BCK(nm_norm_scale<T>(b->dnorm, b->Zdom, b->D, (double*)b->scale, b->err, b->st));
+    BCK(nm_norm_scale<double>(b->dnorm, b->Zdom, b->D, b->scale, b->err, b->st));
     b->launches++;
     b->pending = true;
   }
   b->age = norm ? 0 : b->age + 1;
   if (label_step) {
-    if ((rc = b_flush<T>(b)) != RQ_OK) return rc;
-    kb_evolve<T><<<b->march[0].n, nm_march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cl,
-                                                              (T)(float)f.boundary_speed, (T)(float)f.curv_reg);
-    BL("evolve");
+    BRC(b_flush(b));
+    BRC(each_set([&](auto tag, int p) -> int {
+      using T = decltype(tag);
+      const rq_batch::Plan& m = b->pl[p].march[0];
+      if (!m.n) return RQ_OK;
+      kb_evolve<T><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cl, (T)(float)f.boundary_speed,
+                                                       (T)(float)f.curv_reg);
+      BL("evolve");
+      return RQ_OK;
+    }));
     b->cl ^= 1;
   }
   return RQ_OK;
 }
 
-template <typename T>
 static int b_initialize(rq_batch* b) {
   b->cu = b->cp = b->cl = 0;
-  const double sig = b->cfg.sigma;
-  kb_potential<T><<<b->flat1.n, 256, 0, b->st>>>(b->din, b->flat1.d, sig);
-  BL("potential");
-  kb_init<T><<<b->flat1.n, 256, 0, b->st>>>(b->din, b->flat1.d);
-  BL("init");
-  const size_t es = sizeof(T);
+  BRC(each_set([&](auto tag, int p) -> int {
+    using T = decltype(tag);
+    const rq_batch::Plan& f = b->pl[p].flat1;
+    if (!f.n) return RQ_OK;
+    kb_potential<T><<<f.n, 256, 0, b->st>>>(b->din, f.d, b->cfg.sigma);
+    BL("potential");
+    kb_init<T><<<f.n, 256, 0, b->st>>>(b->din, f.d);
+    BL("init");
+    return RQ_OK;
+  }));
   for (int q = 0; q < b->n; ++q) {
     const BInst& I = b->hin[q];
+    const size_t es = b->f64[q] ? sizeof(double) : sizeof(float);
     BCK(cudaMemcpyAsync(I.lab[1], I.lab[0], sizeof(int) * I.g.S3, cudaMemcpyDeviceToDevice, b->st));
     BCK(cudaMemsetAsync(I.U[1], 0, es * I.g.S3, b->st));
     for (int k = 0; k < 2; ++k) BCK(cudaMemsetAsync(I.P[k], 0, es * I.g.S3, b->st));
     BCK(launch_fill(I.W, 1.0f, I.g.S3, b->st));
   }
-  int rc = b_normalize<T>(b, true);
-  if (rc != RQ_OK) return rc;
-  for (int v = 0; v < 10; ++v)
-    if ((rc = b_vcycle<T>(b)) != RQ_OK) return rc;
+  BRC(b_normalize(b));
+  for (int v = 0; v < 10; ++v) BRC(each_set([&](auto tag, int p) { return b_vcycle<decltype(tag)>(b, p); }));
   b->steps_done = 0;
   BCK(cudaStreamSynchronize(b->st));
   return RQ_OK;
@@ -604,7 +656,7 @@ extern "C" int rq_batch_create(const rq_config* cfgs, const rq_atom* atoms, cons
   if (!b) return RQ_ENOMEM;
   b->n = n_inst;
   b->cfg = c0;
-  b->fp64 = c0.precision == RQ_PREC_FP64;
+  b->f64.assign(n_inst, c0.precision == RQ_PREC_FP64 ? 1 : 0);
   rq_config& f = b->cfg;  // the new flavour's defaults (capi.cu fill_defaults)
   if (f.poisson_interval <= 0) f.poisson_interval = 4;
   if (f.norm_interval <= 0) f.norm_interval = f.poisson_interval;
@@ -685,7 +737,7 @@ extern "C" int rq_batch_set_stream(rq_batch* b, void* stream) {
 
 extern "C" int rq_batch_initialize(rq_batch* b) {
   if (!b) return RQ_EINVAL;
-  return b->fp64 ? b_initialize<double>(b) : b_initialize<float>(b);
+  return b_initialize(b);
 }
 
 static int b_period(const rq_batch* b) {
@@ -701,8 +753,7 @@ static int b_period(const rq_batch* b) {
 static int b_eager(rq_batch* b, int n) {
   for (int q = 0; q < n; ++q) {
     const int s = b->steps_done + 1;
-    const int rc = b->fp64 ? b_step<double>(b, s) : b_step<float>(b, s);
-    if (rc != RQ_OK) return rc;
+    BRC(b_step(b, s));
     b->steps_done = s;
   }
   return RQ_OK;
@@ -761,22 +812,20 @@ extern "C" int rq_batch_step(rq_batch* b, int32_t n) {
 extern "C" int rq_batch_energy(rq_batch* b, double* out) {
   if (!b || !out) return RQ_EINVAL;
   if (b->lastE.size() != (size_t)b->n * RQ_ENERGY_LEN) b->lastE.assign((size_t)b->n * RQ_ENERGY_LEN, 0.0);
-  if (b->march[0].n == 0) {  // nothing active: the cached energies are current
+  if (!any_active(b)) {  // nothing active: the cached energies are current
     std::memcpy(out, b->lastE.data(), sizeof(double) * b->lastE.size());
     return RQ_OK;
   }
-  int frc = b_ready_any(b);
-  if (frc != RQ_OK) return frc;
+  BRC(b_ready(b));
   BCK(cudaMemsetAsync(b->dpd, 0, sizeof(double) * 4 * b->D, b->st));
-  if (b->fp64) {
-    using T = double;
-    kb_energy<T><<<b->march[0].n, nm_march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cp, b->cl, b->dpd);
+  BRC(each_set([&](auto tag, int p) -> int {
+    using T = decltype(tag);
+    const rq_batch::Plan& m = b->pl[p].march[0];
+    if (!m.n) return RQ_OK;
+    kb_energy<T><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cp, b->cl, b->dpd);
     BL("energy");
-  } else {
-    using T = float;
-    kb_energy<T><<<b->march[0].n, nm_march_block(), 0, b->st>>>(b->din, b->march[0].d, b->cu, b->cp, b->cl, b->dpd);
-    BL("energy");
-  }
+    return RQ_OK;
+  }));
   std::vector<double> pd((size_t)4 * b->D);
   BCK(cudaMemcpyAsync(pd.data(), b->dpd, sizeof(double) * pd.size(), cudaMemcpyDeviceToHost, b->st));
   BCK(cudaStreamSynchronize(b->st));
@@ -817,19 +866,20 @@ extern "C" int rq_batch_energy(rq_batch* b, double* out) {
 extern "C" int rq_batch_forces(rq_batch* b, double* F) {
   if (!b || !F) return RQ_EINVAL;
   for (char a : b->active)
-    if (!a) return rq_batch_set_active_all(b) != RQ_OK ? RQ_ECUDA : rq_batch_forces(b, F);
-  int frc = b_ready_any(b);
-  if (frc != RQ_OK) return frc;
+    if (!a) {
+      BRC(rq_batch_set_active_all(b));
+      break;
+    }
+  BRC(b_ready(b));
   BCK(cudaMemsetAsync(b->dF, 0, sizeof(double) * 3 * b->A, b->st));
-  if (b->fp64) {
-    using T = double;
-    kb_force<T><<<b->force.n, 256, 0, b->st>>>(b->din, b->force.d, b->cu, b->cfg.sigma, b->dF);
+  BRC(each_set([&](auto tag, int p) -> int {
+    using T = decltype(tag);
+    const rq_batch::Plan& f = b->pl[p].force;
+    if (!f.n) return RQ_OK;
+    kb_force<T><<<f.n, 256, 0, b->st>>>(b->din, f.d, b->cu, b->cfg.sigma, b->dF);
     BL("force");
-  } else {
-    using T = float;
-    kb_force<T><<<b->force.n, 256, 0, b->st>>>(b->din, b->force.d, b->cu, b->cfg.sigma, b->dF);
-    BL("force");
-  }
+    return RQ_OK;
+  }));
   BCK(cudaMemcpyAsync(F, b->dF, sizeof(double) * 3 * b->A, cudaMemcpyDeviceToHost, b->st));
   BCK(cudaStreamSynchronize(b->st));
   // add the point-charge nuclear repulsion forces
@@ -855,49 +905,27 @@ __global__ void kb_widen(const float* __restrict__ a, double* __restrict__ d, lo
     d[q] = (double)a[q];
 }
 
-// A mixed batch switches every instance to FP64 fields for its final refinement: psi and P are
-// widened, K is recomputed in FP64, labels and W carry over.  The fp32 buffers stay allocated
-// until the batch is destroyed.
-static int b_promote(rq_batch* b) {
-  if (b->fp64) return RQ_OK;
-  int frc = b_ready_any(b);
-  if (frc != RQ_OK) return frc;
-  const size_t es = sizeof(double);
-  for (int q = 0; q < b->n; ++q) {
-    BInst& I = b->hin[q];
-    const size_t S3 = (size_t)I.g.S3;
-    void *U[2], *P[2], *K;
-    for (int k = 0; k < 2; ++k) {
-      BALLOC(U[k], S3 * es);
-      BALLOC(P[k], S3 * es);
-    }
-    BALLOC(K, S3 * es);
-    kb_widen<<<148 * 4, 256, 0, b->st>>>((const float*)I.U[b->cu], (double*)U[b->cu], (long long)S3);
-    kb_widen<<<148 * 4, 256, 0, b->st>>>((const float*)I.P[b->cp], (double*)P[b->cp], (long long)S3);
-    BCK(cudaGetLastError());
-    for (int k = 0; k < 2; ++k) { I.U[k] = U[k]; I.P[k] = P[k]; }
-    I.K = K;
-    for (int l = 0; l < I.nlev; ++l) {
-      const size_t s3 = (size_t)I.lg[l].S3;
-      if (l > 0) {
-        BALLOC(I.lP[l], s3 * es);
-        BALLOC(I.lf[l], s3 * es);
-      }
-      if (l < I.nlev - 1) BALLOC(I.lr[l], s3 * es);
-    }
-  }
-  BCK(cudaMemcpyAsync(b->din, b->hin.data(), sizeof(BInst) * b->n, cudaMemcpyHostToDevice, b->st));
-  b->fp64 = true;
-  b->promoted = true;
-  std::vector<char> keep = b->active;
-  b->active.assign(b->n, 1);  // K of every instance in FP64
-  int rc = build_plans(b);
-  if (rc != RQ_OK) return rc;
-  kb_potential<double><<<b->flat1.n, 256, 0, b->st>>>(b->din, b->flat1.d, b->cfg.sigma);
+// Move instance q of a mixed batch to FP64 fields for its final refinement (psi must be in its
+// normalised state): psi and P are widened, K is recomputed in FP64, the multigrid levels get
+// FP64 buffers, labels and W carry over.  The fp32 buffers stay allocated until the batch is
+// destroyed.  The caller rebuilds the work lists.
+static int b_promote(rq_batch* b, int q) {
+  if (b->f64[q]) return RQ_OK;
+  BInst& I = b->hin[q];
+  const BInst old = I;
+  b->f64[q] = 1;
+  BRC(alloc_fields(b, q));
+  const long long S3 = I.g.S3;
+  kb_widen<<<148 * 4, 256, 0, b->st>>>((const float*)old.U[b->cu], (double*)I.U[b->cu], S3);
+  kb_widen<<<148 * 4, 256, 0, b->st>>>((const float*)old.P[b->cp], (double*)I.P[b->cp], S3);
   BCK(cudaGetLastError());
-  b->active = keep;
-  rc = build_plans(b);
-  if (rc != RQ_OK) return rc;
+  BCK(cudaMemcpyAsync(b->din + q, &I, sizeof(BInst), cudaMemcpyHostToDevice, b->st));
+  std::vector<BItem> f1;
+  flat_items(f1, q, S3, 256);
+  BRC(upload_plan(b, b->one, f1));
+  kb_potential<double><<<b->one.n, 256, 0, b->st>>>(b->din, b->one.d, b->cfg.sigma);
+  BCK(cudaGetLastError());
+  // the host copies above (table entry, item list) must outlive the asynchronous copies
   BCK(cudaStreamSynchronize(b->st));
   return RQ_OK;
 }
@@ -907,62 +935,47 @@ int rq_batch_set_active_all(rq_batch* b) {
   return build_plans(b);
 }
 
-// One converge-to-tol loop over the active instances; instances are dropped from the work lists
-// as they converge.  conv[q] receives the total step count at convergence.
-constexpr double kMixedFloor = 3e-9;  // relative |dE| a mixed-precision batch is asked to reach
-
-static int b_converge(rq_batch* b, std::vector<double> tol, int max_steps, int check, std::vector<int>& conv,
-                      int& taken) {
-  std::vector<double> e((size_t)b->n * RQ_ENERGY_LEN), prev(b->n);
-  int rc = rq_batch_energy(b, e.data());
-  if (rc != RQ_OK) return rc;
-  for (int q = 0; q < b->n; ++q) prev[q] = e[(size_t)q * RQ_ENERGY_LEN];
-  int left = 0;
-  for (int q = 0; q < b->n; ++q) left += b->active[q] ? 1 : 0;
-  while (taken < max_steps && left > 0) {
-    const int n = std::min(check, max_steps - taken);
-    if ((rc = rq_batch_step(b, n)) != RQ_OK) return rc;
-    taken += n;
-    if ((rc = rq_batch_energy(b, e.data())) != RQ_OK) return rc;
-    bool dropped = false;
-    for (int q = 0; q < b->n; ++q) {
-      if (!b->active[q]) continue;
-      const double E = e[(size_t)q * RQ_ENERGY_LEN];
-      if (std::fabs(E - prev[q]) < tol[q]) {
-        conv[q] = taken;
-        b->active[q] = 0;
-        dropped = true;
-        left--;
-      }
-      prev[q] = E;
-    }
-    if (dropped && (rc = build_plans(b)) != RQ_OK) return rc;
-  }
-  return RQ_OK;
-}
-
+// Converge every instance to |dE| < tol_dE between checks `check_interval` steps apart.  An
+// fp32 instance first converges to max(tol_dE, kMixedFloor |E|), the change its fields
+// resolve; if that is looser than tol_dE it moves to FP64 right there and refines to tol_dE
+// (iterative refinement) while the other instances keep stepping.  Converged instances leave
+// the work lists; converged_at[q] is the total step count at convergence (-1: not converged).
 extern "C" int rq_batch_solve(rq_batch* b, double tol_dE, int32_t max_steps, int32_t check_interval,
                               int32_t* converged_at, double* E_final) {
   if (!b || max_steps < 0 || check_interval <= 0) return RQ_EINVAL;
-  int rc, taken = 0;
-  std::vector<int> conv(b->n, -1);
-  if ((rc = rq_batch_set_active_all(b)) != RQ_OK) return rc;
-  if (!b->fp64) {
-    // fp32 fields: |dE| between checks has a noise floor of ~1e-9 |E| (round-off of psi and P),
-    // so converge to max(tol, kMixedFloor |E|) in fp32 first ...
-    std::vector<double> e((size_t)b->n * RQ_ENERGY_LEN), tol(b->n);
-    if ((rc = rq_batch_energy(b, e.data())) != RQ_OK) return rc;
-    for (int q = 0; q < b->n; ++q) tol[q] = std::max(tol_dE, kMixedFloor * std::fabs(e[(size_t)q * RQ_ENERGY_LEN]));
-    std::vector<int> c32(b->n, -1);
-    if ((rc = b_converge(b, tol, max_steps, check_interval, c32, taken)) != RQ_OK) return rc;
-    // ... then widen the batch to FP64 and refine to tol_dE (iterative refinement)
-    if ((rc = b_promote(b)) != RQ_OK) return rc;
-    if ((rc = rq_batch_set_active_all(b)) != RQ_OK) return rc;
+  BRC(rq_batch_set_active_all(b));
+  std::vector<double> e((size_t)b->n * RQ_ENERGY_LEN), prev(b->n), tol(b->n);
+  BRC(rq_batch_energy(b, e.data()));
+  for (int q = 0; q < b->n; ++q) {
+    prev[q] = e[(size_t)q * RQ_ENERGY_LEN];
+    tol[q] = b->f64[q] ? tol_dE : std::max(tol_dE, kMixedFloor * std::fabs(prev[q]));
   }
-  std::vector<double> tol(b->n, tol_dE);
-  if ((rc = b_converge(b, tol, max_steps, check_interval, conv, taken)) != RQ_OK) return rc;
-  std::vector<double> e((size_t)b->n * RQ_ENERGY_LEN);
-  if ((rc = rq_batch_energy(b, e.data())) != RQ_OK) return rc;
+  std::vector<int> conv(b->n, -1);
+  int taken = 0, left = b->n;
+  while (taken < max_steps && left > 0) {
+    const int n = std::min(check_interval, max_steps - taken);
+    BRC(rq_batch_step(b, n));
+    taken += n;
+    BRC(rq_batch_energy(b, e.data()));  // psi is now in its normalised state
+    bool changed = false;
+    for (int q = 0; q < b->n; ++q) {
+      if (!b->active[q]) continue;
+      const double E = e[(size_t)q * RQ_ENERGY_LEN], d = std::fabs(E - prev[q]);
+      prev[q] = E;
+      if (d >= tol[q]) continue;
+      changed = true;
+      if (!b->f64[q] && tol[q] > tol_dE) {
+        BRC(b_promote(b, q));
+        tol[q] = tol_dE;
+      } else {
+        conv[q] = taken;
+        b->active[q] = 0;
+        left--;
+      }
+    }
+    if (changed) BRC(build_plans(b));
+  }
+  BRC(rq_batch_energy(b, e.data()));
   for (int q = 0; q < b->n; ++q) {
     if (converged_at) converged_at[q] = conv[q];
     if (E_final) E_final[q] = e[(size_t)q * RQ_ENERGY_LEN];
