@@ -18,8 +18,8 @@ period with the flush before EVERY solver step (every kernel reads HBM cold).
 ``e2e``    the public API call a user makes per frame: upload the state (psi, labels, P)
            from pinned host memory, run one period (CUDA-graph replay), read the energies
            back -- copies inside the timed region;
-``roofline`` the dominant kernel (fused ITP update, 20 algorithmic B per interior point)
-           against the measured HBM copy bandwidth;
+``roofline`` the dominant kernel (k_step_sp: the ITP update and one Jacobi sweep in one pass,
+           24 algorithmic B per interior point) against the measured HBM copy bandwidth;
 ``cpu_baseline`` the reference's own cloud/solver.py kernels compiled for the host
            (oracle/_ref, OpenMP over all host cores) on a bounded sample of the same workload.
 
@@ -174,13 +174,15 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """DRAM bytes per launch of the update kernel from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "update_sp_glycine128.md")
+def ncu_traffic(workload):
+    """DRAM bytes per launch of the fused step kernel on this workload, from the committed ncu
+    summary (line "traffic_bytes_per_launch <workload>: <bytes>"), or None."""
+    p = os.path.join(ROOT, "profiles", "step_sp_glycine128.md")
+    key = f"traffic_bytes_per_launch {workload}:"
     try:
         with open(p) as f:
             for ln in f:
-                if ln.startswith("traffic_bytes_per_launch:"):
+                if ln.startswith(key):
                     return float(ln.split(":")[1])
     except Exception:
         pass
@@ -321,8 +323,8 @@ def run_ours(a):
             "value_l2_flushed_every_solver_step": value_cold,
             "e2e": {"value": e2e, "unit": "Gpt/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak if achieved else None, "traffic": ncu_traffic(),
-                         "kernel": "k_update_sp (fused ITP update)", "bytes_per_launch": upd_bytes,
+                         "frac": achieved / peak if achieved else None, "traffic": ncu_traffic(a.workload),
+                         "kernel": "k_step_sp (ITP update fused with a Jacobi sweep)", "bytes_per_launch": upd_bytes,
                          "peak_kind": peak_kind},
             "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 4), "GB/s": round(v["gbs"], 1)}
                         for k, v in prof.items()},

@@ -86,3 +86,33 @@ class Batch:
         n, tp, ip, kl = C.c_int32(), C.c_int64(), C.c_int64(), C.c_int64()
         self._chk(self.lib.rq_batch_info(self.b, C.byref(n), C.byref(tp), C.byref(ip), C.byref(kl)), "rq_batch_info")
         return {"instances": n.value, "points": tp.value, "interior_points": ip.value, "kernel_launches": kl.value}
+
+
+def _main(argv=None):
+    """Step the seeded 96-water-cluster batch (realmolecule_b200.configs.clusters96) on cuda:0.
+
+    python -m realmolecule_b200.batch [--instances N] [--steps K] [--precision mixed|fp64]
+    Prints the batch size and the wall time of the K steps (after initialisation)."""
+    import argparse
+    import time
+
+    from . import configs
+    ap = argparse.ArgumentParser(description=_main.__doc__)
+    ap.add_argument("--instances", type=int, default=96)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--precision", default="mixed", choices=sorted(PRECISIONS))
+    a = ap.parse_args(argv)
+    geoms = configs.clusters96()[:a.instances]
+    b = Batch([{"NN": g.NN, "screen": g.screen, "atoms": configs.to_domain_atoms(g)} for g in geoms],
+              precision=a.precision, label_until=1)
+    b.initialize()
+    t0 = time.perf_counter()
+    b.step(a.steps)
+    b.synchronize()
+    dt = time.perf_counter() - t0
+    print({**b.info(), "steps": a.steps, "ms_per_step": dt / max(1, a.steps) * 1e3}, flush=True)
+    b.close()
+
+
+if __name__ == "__main__":
+    _main()

@@ -296,17 +296,59 @@ static int sp_poisson(rq_ctx* c) {
   return RQ_OK;
 }
 
+// One solver.py step (cloud/solver.py:561-586): Poisson every poisson_interval steps (2 Jacobi
+// sweeps), the update, normalisation every norm_interval, labels every label_interval.  An update
+// and a Jacobi sweep share one pass (k_step_sp): the last sweep of a Poisson step runs fused with
+// that step's update, and the first sweep of the NEXT Poisson step runs fused with the update of
+// the step before it whenever that step does not normalise (so psi does not change in between).
+// That early sweep writes P[1-cp] and leaves cp alone (sp_jdone = 1): every readout still sees
+// the P of the last completed Poisson step, and the next Poisson step adopts the buffer.
 static int sp_step_one(rq_ctx* c, int s) {
   const rq_config& f = c->cfg;
+  const bool poisson = s % f.poisson_interval == 0, norm = s % f.norm_interval == 0;
+  const int jps = f.jacobi_per_step;
+  const float coeff = (float)(2.0 * M_PI);
   int rc;
-  if (s % f.poisson_interval == 0 && (rc = sp_poisson(c)) != RQ_OK) return rc;
-  const bool norm = s % f.norm_interval == 0;
   if (norm) CK(cudaMemsetAsync(c->dnorm, 0, sizeof(double) * c->n_atoms, c->st));
-  LAUNCH(RQ_KC_UPDATE, 20 * interior_points(c->g),
-         launch_update_sp((float*)c->U[c->cu], (float*)c->U[1 - c->cu], (float*)c->K, (float*)c->P[c->cp],
-                          c->lab[c->cl], c->g, (float)c->half_dv, (float)c->dt, c->h3, c->n_atoms,
-                          norm ? c->dnorm : nullptr, c->st));
-  c->cu ^= 1;
+  double* nrm = norm ? c->dnorm : nullptr;
+  auto fused = [&](bool first) -> int {
+    LAUNCH(RQ_KC_UPDATE, 24 * interior_points(c->g),
+           launch_step_sp(first, (float*)c->U[c->cu], (float*)c->U[1 - c->cu], (float*)c->K, (float*)c->P[c->cp],
+                          (float*)c->P[1 - c->cp], c->lab[c->cl], c->g, (float)c->half_dv, (float)c->dt,
+                          (float)c->h2, coeff, c->h3, c->n_atoms, nrm, c->st));
+    c->cu ^= 1;
+    return RQ_OK;
+  };
+  bool updated = false;
+  if (poisson) {
+    int todo = jps;
+    if (c->sp_jdone && todo > 0) {  // the first sweep already ran with the previous update
+      c->cp ^= 1;
+      todo--;
+    }
+    c->sp_jdone = 0;
+    for (int q = 0; q + 1 < todo; ++q) {
+      LAUNCH(RQ_KC_POISSON, 12 * interior_points(c->g),
+             launch_jacobi_sp((float*)c->P[c->cp], (float*)c->P[1 - c->cp], (float*)c->U[c->cu], c->g, (float)c->h2,
+                              coeff, c->st));
+      c->cp ^= 1;
+    }
+    if (todo >= 1) {
+      if ((rc = fused(false)) != RQ_OK) return rc;
+      c->cp ^= 1;
+      updated = true;
+    }
+  } else if ((s + 1) % f.poisson_interval == 0 && jps >= 1 && !norm) {
+    if ((rc = fused(true)) != RQ_OK) return rc;
+    c->sp_jdone = 1;
+    updated = true;
+  }
+  if (!updated) {
+    LAUNCH(RQ_KC_UPDATE, 20 * interior_points(c->g),
+           launch_update_sp((float*)c->U[c->cu], (float*)c->U[1 - c->cu], (float*)c->K, (float*)c->P[c->cp],
+                            c->lab[c->cl], c->g, (float)c->half_dv, (float)c->dt, c->h3, c->n_atoms, nrm, c->st));
+    c->cu ^= 1;
+  }
   if (norm && (rc = sp_normalize(c, false)) != RQ_OK) return rc;
   if (s % f.label_interval == 0 && (f.label_until <= 0 || s <= f.label_until)) {
     LAUNCH(RQ_KC_LABELS, 8 * interior_points(c->g),
@@ -322,6 +364,7 @@ static int sp_initialize(rq_ctx* c) {
     CK(cudaMemsetAsync(c->P[b], 0, sizeof(float) * c->g.S3, c->st));
   }
   c->cu = c->cp = c->cl = 0;
+  c->sp_jdone = 0;
   LAUNCH(RQ_KC_OTHER, 16.0 * c->g.S3,
          launch_init_sp((float*)c->U[0], c->lab[0], (float*)c->K, c->bestU, c->atoms5, c->n_atoms, c->g, (float)c->h,
                         (float)c->h2, true, c->st));
@@ -373,7 +416,10 @@ extern "C" int rq_step(rq_ctx* c, int32_t n) {
     // a period that straddles label_until has no single captured pattern: run it eagerly
     const int lu = c->cfg.label_until;
     const bool straddle = lu > 0 && c->steps_done < lu && c->steps_done + period > lu;
-    const bool aligned = !c->prof && !straddle && period > 0 && c->steps_done % period == 0 && left >= period;
+    // (a period boundary never leaves an early Jacobi sweep pending: the step before a Poisson step
+    // is never the last of a period, as the period is a multiple of poisson_interval)
+    const bool aligned = !c->prof && !straddle && period > 0 && c->steps_done % period == 0 && left >= period &&
+                         c->sp_jdone == 0;
     if (!aligned) {
       // run eagerly up to the next period boundary (or all that is left)
       int todo = left;
@@ -455,6 +501,7 @@ extern "C" int rq_upload_state(rq_ctx* c, const float* psi, const int32_t* label
     CK(cudaMemcpyAsync(c->lab[1 - c->cl], c->lab[c->cl], n * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
     if (mj && (rc = mj_refresh_flags(c)) != RQ_OK) return rc;  // r_c-exclusion bits of the new labels
   }
+  if (psi || P) c->sp_jdone = 0;  // an early Jacobi sweep used the old psi and P: redo it
   if (psi) {
     c->nm_pending = false;
     c->nm_age = 0;

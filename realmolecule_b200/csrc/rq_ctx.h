@@ -59,6 +59,7 @@ struct rq_ctx {
   void* scale64 = nullptr;    // new flavour: per-domain scale (FP64 for both precisions)
   void* Kext = nullptr;       // new flavour: external potential added to K (T), or null
   bool nm_pending = false;    // new flavour: psi awaits scale64 (applied by the next update or a flush)
+  int sp_jdone = 0;           // solver.py flavour: the next Poisson step's first sweep is done (in P[1-cp])
   int nm_age = 0;             // new flavour: updates since psi was last normalised (0: normalised or pending)
   float* Zdom = nullptr;      // domain charge per label (f32)
   double* Zdom64 = nullptr;

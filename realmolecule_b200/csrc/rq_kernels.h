@@ -8,6 +8,11 @@ namespace rq {
 cudaError_t launch_update_sp(const float* U, float* Unew, const float* K, const float* P, const int* label,
                              const Geo& g, float half_dv, float dtv, double h3, int nDom, double* norms,
                              cudaStream_t st);
+// update and Jacobi sweep in one pass (first: update then the sweep on the new psi; else the
+// sweep then the update with the new P)
+cudaError_t launch_step_sp(bool first, const float* U, float* Unew, const float* K, const float* P, float* Pnew,
+                           const int* label, const Geo& g, float half_dv, float dtv, float h2, float coeff, double h3,
+                           int nDom, double* norms, cudaStream_t st);
 cudaError_t launch_jacobi_sp(const float* P, float* Pnew, const float* U, const Geo& g, float h2, float coeff,
                              cudaStream_t st);
 cudaError_t launch_labels_sp(const int* labIn, int* labOut, const float* atoms5, int nAtoms, const Geo& g, float h,

@@ -94,6 +94,79 @@ __global__ void __launch_bounds__(256) k_jacobi_sp(const float* __restrict__ P, 
 }
 
 // ---------------------------------------------------------------------------------------
+// One pass that does an ITP update and a Jacobi sweep together.  The update reads P only at
+// the centre and the sweep reads psi only at the centre, so on a march both are local:
+//   FIRST = false: Pnew = jacobi(P, rho = psi^2), then psi' = update(psi, Pnew)   (the last sweep
+//                  of a Poisson step, then that step's update);
+//   FIRST = true:  psi' = update(psi, P), then Pnew = jacobi(P, rho = psi'^2)     (a step's update,
+//                  then the first sweep of the next step's Poisson solve).
+// The per-point arithmetic is that of k_update_sp and k_jacobi_sp, so both outputs are
+// bit-identical to the two separate kernels.  Traffic: read psi, label, K, P; write psi', P' =
+// 24 B per interior point instead of 20 + 12.
+// ---------------------------------------------------------------------------------------
+template <bool FIRST, bool ACC>
+__global__ void __launch_bounds__(256) k_step_sp(const float* __restrict__ U, float* __restrict__ Unew,
+                                                 const float* __restrict__ K, const float* __restrict__ P,
+                                                 float* __restrict__ Pnew, const int* __restrict__ label, Geo g,
+                                                 float half_dv, float dtv, float h2, float coeff, double h3, int nDom,
+                                                 double* __restrict__ norms) {
+  __shared__ DomTable<1, 128> tab;
+  if (ACC) dom_table_init(tab);
+  if (ACC) __syncthreads();
+  RunSum<1> rs;
+  rs.reset();
+  const int k = 1 + blockIdx.x * kThreadsK + threadIdx.x;
+  const int j = 1 + blockIdx.y * kThreadsJ + threadIdx.y;
+  const int i0 = 1 + blockIdx.z * kMarch;
+  if (k < g.NN && j < g.NN && i0 < g.NN) {
+    const int iend = min(i0 + kMarch, g.NN);
+    const long long S = g.S, S2 = g.S2;
+    long long id = (long long)i0 * S2 + j * S + k;
+    float u_m = __ldg(U + id - S2), u_c = __ldg(U + id);
+    int l_m = __ldg(label + id - S2), l_c = __ldg(label + id);
+    float p_m = __ldg(P + id - S2), p_c = __ldg(P + id);
+    for (int i = i0; i < iend; ++i, id += S2) {
+      const float u_p = __ldg(U + id + S2), p_p = __ldg(P + id + S2);
+      const int l_p = __ldg(label + id + S2);
+      const float ujp = __ldg(U + id + S), ujm = __ldg(U + id - S), ukp = __ldg(U + id + 1), ukm = __ldg(U + id - 1);
+      const int ljp = __ldg(label + id + S), ljm = __ldg(label + id - S), lkp = __ldg(label + id + 1),
+                lkm = __ldg(label + id - 1);
+      const float sumN = F_ADD(F_ADD(F_ADD(F_ADD(F_ADD(p_p, p_m), __ldg(P + id + S)), __ldg(P + id - S)),
+                                     __ldg(P + id + 1)),
+                               __ldg(P + id - 1));
+      const float kv = __ldg(K + id);
+      const float a = (l_p == l_c) ? u_p : u_c;
+      const float b = (l_m == l_c) ? u_m : u_c;
+      const float c = (ljp == l_c) ? ujp : u_c;
+      const float d = (ljm == l_c) ? ujm : u_c;
+      const float e = (lkp == l_c) ? ukp : u_c;
+      const float f = (lkm == l_c) ? ukm : u_c;
+      const float lap = F_SUB(F_ADD(F_ADD(F_ADD(F_ADD(F_ADD(a, b), c), d), e), f), F_MUL(6.0f, u_c));
+      float pv = p_c;
+      if (!FIRST) {
+        pv = F_DIV(F_ADD(sumN, F_MUL(F_MUL(coeff, F_MUL(u_c, u_c)), h2)), 6.0f);
+        Pnew[id] = pv;
+      }
+      const float out =
+          F_ADD(F_ADD(u_c, F_MUL(half_dv, lap)), F_MUL(F_MUL(dtv, F_SUB(kv, F_MUL(2.0f, pv))), u_c));
+      Unew[id] = out;
+      if (FIRST) Pnew[id] = F_DIV(F_ADD(sumN, F_MUL(F_MUL(coeff, F_MUL(out, out)), h2)), 6.0f);
+      if (ACC) {
+        double r = (double)out * (double)out * h3;
+        int lc = min(max(l_c, 0), nDom - 1);
+        rs.add(lc, &r, tab, norms);
+      }
+      u_m = u_c; u_c = u_p; l_m = l_c; l_c = l_p; p_m = p_c; p_c = p_p;
+    }
+  }
+  if (ACC) {
+    rs.finish(tab, norms);
+    __syncthreads();
+    dom_table_flush(tab, norms);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
 // Label step (cloud/solver.py:92-147) with snapshot semantics: reads labelIn, writes
 // labelOut for interior points.  A boundary cell (>= 1 foreign neighbour) flips to the
 // atom of largest Z/sqrt(r^2+h^2) when that beats the current atom's score by 10 % and
@@ -365,6 +438,25 @@ cudaError_t launch_jacobi_sp(const float* P, float* Pnew, const float* U, const 
                              cudaStream_t st) {
   if (g.NN < 2) return cudaSuccess;
   k_jacobi_sp<<<march_grid(g), march_block(), 0, st>>>(P, Pnew, U, g, h2, coeff);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_step_sp(bool first, const float* U, float* Unew, const float* K, const float* P, float* Pnew,
+                           const int* label, const Geo& g, float half_dv, float dtv, float h2, float coeff, double h3,
+                           int nDom, double* norms, cudaStream_t st) {
+  if (g.NN < 2) return cudaSuccess;
+  const dim3 grd = march_grid(g), blk = march_block();
+  if (first && norms)
+    k_step_sp<true, true><<<grd, blk, 0, st>>>(U, Unew, K, P, Pnew, label, g, half_dv, dtv, h2, coeff, h3, nDom, norms);
+  else if (first)
+    k_step_sp<true, false><<<grd, blk, 0, st>>>(U, Unew, K, P, Pnew, label, g, half_dv, dtv, h2, coeff, h3, nDom,
+                                                nullptr);
+  else if (norms)
+    k_step_sp<false, true><<<grd, blk, 0, st>>>(U, Unew, K, P, Pnew, label, g, half_dv, dtv, h2, coeff, h3, nDom,
+                                                norms);
+  else
+    k_step_sp<false, false><<<grd, blk, 0, st>>>(U, Unew, K, P, Pnew, label, g, half_dv, dtv, h2, coeff, h3, nDom,
+                                                 nullptr);
   return cudaGetLastError();
 }
 
