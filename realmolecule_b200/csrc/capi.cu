@@ -1,5 +1,6 @@
 // capi.cu -- the C ABI of librq (include/rq.h): context lifecycle, state transfer, the
 // per-flavour step schedule (captured as CUDA graphs), energies and forces.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -117,6 +118,15 @@ static int upload_atoms(rq_ctx* c) {
   CK(cudaMemcpyAsync(c->Zdom64, zd64.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(c->atoms_mj, mj.data(), sizeof(MjAtom) * n, cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(c->atoms_nm, nm.data(), sizeof(double) * nm.size(), cudaMemcpyHostToDevice, c->st));
+  std::vector<int> bstart, bidx, bfar;
+  float zmax = 0.f;
+  if (c->bin_start) {
+    build_atom_bins(a5.data(), n, c->bins_nb, c->bins_bin, bstart, bidx, bfar, zmax);
+    CK(cudaMemcpyAsync(c->bin_start, bstart.data(), sizeof(int) * bstart.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->bin_idx, bidx.data(), sizeof(int) * bidx.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->bin_far, bfar.data(), sizeof(int) * bfar.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->bin_zmax, &zmax, sizeof(float), cudaMemcpyHostToDevice, c->st));
+  }
   return cudaStreamSynchronize(c->st) == cudaSuccess ? RQ_OK : rq_cuda(c, cudaGetLastError(), "upload_atoms");
 }
 
@@ -125,7 +135,7 @@ static void free_ctx(rq_ctx* c) {
   for (auto& gx : c->graph)
     if (gx) cudaGraphExecDestroy(gx);
   void* ptrs[] = {c->U[0], c->U[1], c->P[0], c->P[1], c->K, c->W, c->bestU, c->rho, c->Pother, c->resid, c->lab[0], c->lab[1],
-                  c->Ec[0], c->Ec[1], c->fc, c->atoms5, c->scratch_atoms5, c->atoms_mj, c->atoms_nm, c->Zdom, c->Zdom64, c->dnorm,
+                  c->Ec[0], c->Ec[1], c->fc, c->atoms5, c->scratch_atoms5, c->bin_start, c->bin_idx, c->bin_far, c->bin_zmax, c->atoms_mj, c->atoms_nm, c->Zdom, c->Zdom64, c->dnorm,
                   c->dpd, c->dF, c->dsum, c->unorm, c->scale, c->err, c->seeds, c->scale64, c->Kext};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -174,6 +184,17 @@ static int alloc_all(rq_ctx* c) {
   }
   DALLOC(c->atoms5, sizeof(float) * 5 * n);
   DALLOC(c->scratch_atoms5, sizeof(float) * 5 * n);
+  if (c->cfg.flavor == RQ_FLAVOR_SOLVER_PY) {  // bins of ~1 atom each, at most 64 per axis
+    const int S = c->g.S;
+    int bin = (int)std::lround(std::cbrt((double)c->g.S3 / std::max(1, n)));
+    bin = std::max({bin, 4, (S + 63) / 64});
+    c->bins_bin = bin;
+    c->bins_nb = (S + bin - 1) / bin;
+    DALLOC(c->bin_start, sizeof(int) * ((size_t)c->bins_nb * c->bins_nb * c->bins_nb + 1));
+    DALLOC(c->bin_idx, sizeof(int) * n);
+    DALLOC(c->bin_far, sizeof(int) * (n + 1));
+    DALLOC(c->bin_zmax, sizeof(float));
+  }
   DALLOC(c->atoms_mj, sizeof(MjAtom) * n);
   DALLOC(c->atoms_nm, sizeof(double) * 4 * n);
   DALLOC(c->Zdom, sizeof(float) * n);
@@ -352,8 +373,9 @@ static int sp_step_one(rq_ctx* c, int s) {
   if (norm && (rc = sp_normalize(c, false)) != RQ_OK) return rc;
   if (s % f.label_interval == 0 && (f.label_until <= 0 || s <= f.label_until)) {
     LAUNCH(RQ_KC_LABELS, 8 * interior_points(c->g),
-           launch_labels_sp(c->lab[c->cl], c->lab[1 - c->cl], c->atoms5, c->n_atoms, c->g, (float)c->h,
-                            (float)c->h2, c->st));
+           launch_labels_binned_sp(c->lab[c->cl], c->lab[1 - c->cl], c->atoms5, c->n_atoms,
+                                   AtomBins{c->bins_nb, c->bins_bin, c->bin_start, c->bin_idx, c->bin_far, c->bin_zmax},
+                                   c->g, (float)c->h, (float)c->h2, c->st));
     c->cl ^= 1;
   }
   return RQ_OK;

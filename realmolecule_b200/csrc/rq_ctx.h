@@ -53,6 +53,10 @@ struct rq_ctx {
   // atoms on the device
   float* atoms5 = nullptr;    // [i,j,k,Z,rc] f32 (cloud/solver.py:378-382)
   float* scratch_atoms5 = nullptr;  // per-call atom table for force variants
+  // solver.py flavour: atom bins of the label step's argmax (rebuilt whenever atoms change)
+  int bins_nb = 0, bins_bin = 0;
+  int *bin_start = nullptr, *bin_idx = nullptr, *bin_far = nullptr;
+  float* bin_zmax = nullptr;
   void* atoms_mj = nullptr;   // molecule.js records (u32 positions)
   double* atoms_nm = nullptr; // new flavour: x,y,z (bohr), Z_nuc per atom
   void* seeds = nullptr;      // new flavour: float4 (x, y, z, entry) per domain seed

@@ -1,5 +1,6 @@
 // rq_kernels.h -- host launchers of the librq kernels (internal to the library).
 #pragma once
+#include <vector>
 #include "rq_internal.cuh"
 
 namespace rq {
@@ -17,6 +18,21 @@ cudaError_t launch_jacobi_sp(const float* P, float* Pnew, const float* U, const 
                              cudaStream_t st);
 cudaError_t launch_labels_sp(const int* labIn, int* labOut, const float* atoms5, int nAtoms, const Geo& g, float h,
                              float h2, cudaStream_t st);
+// Atoms with Z > 0 sorted into cubic bins of `bin` grid units over [0, nb*bin)^3 (the grid box);
+// atoms outside it are on a far list.  Built on the host by build_atom_bins.
+struct AtomBins {
+  int nb, bin;
+  const int* start;   // nb^3 + 1 offsets into idx
+  const int* idx;     // atom indices, bin by bin
+  const int* far;     // far[0] = count, far[1..count] = atom indices
+  const float* zmax;  // largest Z of any atom (device value, so captured graphs see updates)
+};
+// host: fill start/idx/far (sizes nb^3+1, n, n+1) and zmax for atoms5 (n x 5, grid units)
+void build_atom_bins(const float* atoms5, int n, int nb, int bin, std::vector<int>& start, std::vector<int>& idx,
+                     std::vector<int>& far, float& zmax);
+// the label step with the argmax over atoms found through the bins (same result as launch_labels_sp)
+cudaError_t launch_labels_binned_sp(const int* labIn, int* labOut, const float* atoms5, int nAtoms, AtomBins bins,
+                                    const Geo& g, float h, float h2, cudaStream_t st);
 cudaError_t launch_init_sp(float* U, int* label, float* K, float* bestU, const float* atoms5, int nAtoms,
                            const Geo& g, float h, float h2, bool trial, cudaStream_t st);
 cudaError_t launch_norms_flat(const float* U, const int* label, const Geo& g, double h3, int nDom, double* norms,

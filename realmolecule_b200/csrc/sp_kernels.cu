@@ -7,6 +7,8 @@
 // that march 16 planes along i keeping the i-1/i/i+1 column in registers, rho = psi^2
 // computed inside the Jacobi sweep instead of a separate pass, and FP64 per-domain sums
 // aggregated per block instead of f32 scatter_add / atomics.
+#include <algorithm>
+
 #include "rq_kernels.h"
 
 namespace rq {
@@ -188,7 +190,7 @@ __global__ void __launch_bounds__(256) k_labels_sp(const int* __restrict__ labIn
     int other = (__ldg(labIn + id + S2) != cur) + (__ldg(labIn + id - S2) != cur) + (__ldg(labIn + id + S) != cur) +
                 (__ldg(labIn + id - S) != cur) + (__ldg(labIn + id + 1) != cur) + (__ldg(labIn + id - 1) != cur);
     int out = cur;
-    if (other > 0) {
+    if (other >= 2) {  // a cell with one foreign neighbour never flips: its argmax is not needed
       const float xi = F_MUL((float)i, h);
       float curScore = 0.f, bestScore = 0.f;
       int bestN = cur;
@@ -207,6 +209,118 @@ __global__ void __launch_bounds__(256) k_labels_sp(const int* __restrict__ labIn
     }
     labOut[id] = out;
   }
+}
+
+// The same label step with the argmax over atoms found through atom bins instead of a scan of
+// every atom.  Candidate atoms are visited bin ring by bin ring around the cell (far list
+// first); after ring r every unvisited atom is at least d_min away, so its score is at most
+// zmax / sqrt(d_min^2 + h^2).  The search stops once that bound -- taken with an absolute
+// 1e-3 bohr margin on d_min and a 1e-5 relative margin on the score, far above f32 rounding of
+// the per-atom score -- is below the best score found.  Each candidate's score is the scan's
+// expression, and ties go to the lower atom index (the scan keeps the first maximum), so the
+// winner and its score are those of the scan.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ float sp_atom_score(const float* __restrict__ atoms5, int n, float xi, float yj, float zk,
+                                               float h, float h2) {
+  const float Za = __ldg(atoms5 + n * 5 + 3);
+  const float dx = F_SUB(xi, F_MUL(__ldg(atoms5 + n * 5 + 0), h));
+  const float dy = F_SUB(yj, F_MUL(__ldg(atoms5 + n * 5 + 1), h));
+  const float dz = F_SUB(zk, F_MUL(__ldg(atoms5 + n * 5 + 2), h));
+  const float r2 = F_ADD(F_ADD(F_ADD(F_MUL(dx, dx), F_MUL(dy, dy)), F_MUL(dz, dz)), h2);
+  return F_DIV(Za, F_SQRT(r2));
+}
+
+__global__ void __launch_bounds__(256) k_labels_binned_sp(const int* __restrict__ labIn, int* __restrict__ labOut,
+                                                          const float* __restrict__ atoms5, int nAtoms, AtomBins B,
+                                                          Geo g, float h, float h2) {
+  const int k = 1 + blockIdx.x * kThreadsK + threadIdx.x;
+  const int j = 1 + blockIdx.y * kThreadsJ + threadIdx.y;
+  const int i0 = 1 + blockIdx.z * kMarch;
+  if (k >= g.NN || j >= g.NN || i0 >= g.NN) return;
+  const int iend = min(i0 + kMarch, g.NN);
+  const long long S = g.S, S2 = g.S2;
+  const float yj = F_MUL((float)j, h), zk = F_MUL((float)k, h);
+  const double zmax = (double)__ldg(B.zmax);
+  for (int i = i0; i < iend; ++i) {
+    const long long id = (long long)i * S2 + j * S + k;
+    const int cur = __ldg(labIn + id);
+    int other = (__ldg(labIn + id + S2) != cur) + (__ldg(labIn + id - S2) != cur) + (__ldg(labIn + id + S) != cur) +
+                (__ldg(labIn + id - S) != cur) + (__ldg(labIn + id + 1) != cur) + (__ldg(labIn + id - 1) != cur);
+    int out = cur;
+    if (other >= 2) {
+      const float xi = F_MUL((float)i, h);
+      float curScore = 0.f;
+      if (cur >= 0 && cur < nAtoms && __ldg(atoms5 + cur * 5 + 3) > 0.f)
+        curScore = sp_atom_score(atoms5, cur, xi, yj, zk, h, h2);
+      bool found = false;
+      float bs = 0.f;
+      int bn = cur;
+      auto visit = [&](int n) {
+        const float sc = sp_atom_score(atoms5, n, xi, yj, zk, h, h2);
+        if (!found || sc > bs || (sc == bs && n < bn)) { bs = sc; bn = n; found = true; }
+      };
+      const int nfar = __ldg(B.far);
+      for (int q = 0; q < nfar; ++q) visit(__ldg(B.far + 1 + q));
+      const int c0[3] = {min(i / B.bin, B.nb - 1), min(j / B.bin, B.nb - 1), min(k / B.bin, B.nb - 1)};
+      const int p[3] = {i, j, k};
+      for (int r = 0; r < B.nb; ++r) {
+        for (int a = max(c0[0] - r, 0); a <= min(c0[0] + r, B.nb - 1); ++a)
+          for (int b = max(c0[1] - r, 0); b <= min(c0[1] + r, B.nb - 1); ++b) {
+            const bool edge_ab = abs(a - c0[0]) == r || abs(b - c0[1]) == r;
+            for (int c = max(c0[2] - r, 0); c <= min(c0[2] + r, B.nb - 1); ++c) {
+              if (!edge_ab && abs(c - c0[2]) != r) continue;  // ring r only
+              const int bin = (a * B.nb + b) * B.nb + c;
+              for (int q = __ldg(B.start + bin); q < __ldg(B.start + bin + 1); ++q) visit(__ldg(B.idx + q));
+            }
+          }
+        // distance (grid units) from the cell to the nearest unvisited bin
+        double dmin = 1e30;
+        for (int ax = 0; ax < 3; ++ax) {
+          if (c0[ax] - r > 0) dmin = fmin(dmin, (double)(p[ax] - (c0[ax] - r) * B.bin));
+          if (c0[ax] + r < B.nb - 1) dmin = fmin(dmin, (double)((c0[ax] + r + 1) * B.bin - p[ax]));
+        }
+        if (dmin >= 1e29) break;  // every bin visited
+        const double d = fmax(dmin * (double)h - 1e-3, 0.0);
+        if (found && zmax / sqrt(d * d + (double)h2) * (1.0 + 1e-5) < (double)bs) break;
+      }
+      if (found && bn != cur && bs > F_MUL(curScore, 1.1f)) out = bn;
+    }
+    labOut[id] = out;
+  }
+}
+
+void build_atom_bins(const float* atoms5, int n, int nb, int bin, std::vector<int>& start, std::vector<int>& idx,
+                     std::vector<int>& far, float& zmax) {
+  const long long nbins = (long long)nb * nb * nb;
+  start.assign(nbins + 1, 0);
+  idx.assign(n, 0);
+  far.assign(n + 1, 0);
+  zmax = 0.f;
+  std::vector<long long> where(n, -1);
+  const double lim = (double)nb * bin;
+  for (int q = 0; q < n; ++q) {
+    const float* a = atoms5 + 5 * q;
+    if (!(a[3] > 0.f)) continue;  // the scan skips atoms without charge
+    zmax = std::max(zmax, a[3]);
+    const double x = a[0], y = a[1], z = a[2];
+    if (x >= 0 && y >= 0 && z >= 0 && x < lim && y < lim && z < lim) {
+      where[q] = ((long long)(x / bin) * nb + (long long)(y / bin)) * nb + (long long)(z / bin);
+      start[where[q] + 1]++;
+    } else {
+      far[1 + far[0]++] = q;
+    }
+  }
+  for (long long b = 0; b < nbins; ++b) start[b + 1] += start[b];
+  std::vector<int> fill(start.begin(), start.end() - 1);
+  for (int q = 0; q < n; ++q)
+    if (where[q] >= 0) idx[fill[where[q]]++] = q;
+}
+
+cudaError_t launch_labels_binned_sp(const int* labIn, int* labOut, const float* atoms5, int nAtoms, AtomBins bins,
+                                    const Geo& g, float h, float h2, cudaStream_t st) {
+  if (g.NN < 2) return cudaSuccess;
+  k_labels_binned_sp<<<march_grid(g), march_block(), 0, st>>>(labIn, labOut, atoms5, nAtoms, bins, g, h, h2);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------------------

@@ -156,3 +156,33 @@ def test_normalize_energy_forces(lib, g, case):
     np.testing.assert_allclose(host(F), Fref, rtol=1e-4, atol=1e-6 * np.abs(Fref).max())
     if case[1] is None:
         np.testing.assert_allclose(host(F), g["out_computeForceAll"], rtol=1e-4, atol=1e-6)
+
+
+def test_binned_label_step_matches_the_atom_scan():
+    """The context's label step finds each boundary cell's best atom through atom bins; on 400
+    atoms (some outside the grid box, some without charge) and a blocky label field it must
+    give the oracle's full-scan result bit for bit."""
+    from realmolecule_b200 import Context
+    NN, h = 72, 0.25
+    S = NN + 1
+    rng = np.random.default_rng(7)
+    n = 400
+    pos = rng.uniform(-6, NN + 6, size=(n, 3))           # some atoms lie outside [0, NN]
+    Z = rng.integers(1, 9, size=n).astype(float)
+    Z[rng.choice(n, 20, replace=False)] = 0.0               # charge-free entries are skipped
+    rows = [{"i": float(p[0]), "j": float(p[1]), "k": float(p[2]), "Z": float(z), "rc": 0.0}
+            for p, z in zip(pos, Z)]
+    ctx = Context(NN, NN * h, rows, flavor="solver.py", label_interval=1)
+    ctx.initialize()
+    ii, jj, kk = np.meshgrid(np.arange(S), np.arange(S), np.arange(S), indexing="ij")
+    blocks = (ii // 3) * 10007 + (jj // 3) * 101 + (kk // 3)
+    lab = (blocks * 2654435761 % n).astype(np.int32).reshape(-1)
+    ctx.upload(label=lab)
+    ctx.step(1)                                              # step 1: update, then the label step
+    got = ctx.download(psi=False, label=True)["label"]
+    a5 = np.array([[r["i"], r["j"], r["k"], r["Z"], r["rc"]] for r in rows], np.float32).reshape(-1)
+    ref = np.zeros_like(lab)
+    orc.O().sp_boundary_snapshot(lab, ref, a5, n, S, np.float32(h), np.float32(h * h))
+    assert (ref != lab).sum() > 100  # the case exercises flips
+    assert np.array_equal(got, ref)
+    ctx.close()
