@@ -503,11 +503,35 @@ extern "C" int rq_initialize(rq_ctx* c) {
 // ----------------------------------------------------------------------------------------
 // state transfer
 // ----------------------------------------------------------------------------------------
-static int check_labels(rq_ctx* c, const int32_t* label) {
-  for (long long q = 0; q < c->g.S3; ++q)
-    if (label[q] < 0 || label[q] >= c->n_atoms)
-      return rq_fail(c, RQ_EINVAL, "label " + std::to_string(label[q]) + " at index " + std::to_string(q) +
-                                       " outside [0, n_atoms)");
+// first index of a label outside [0, nAtoms) (atomicMin into *first, which starts above any index)
+__global__ void k_check_labels(const int* __restrict__ lab, long long n, int nAtoms, int* first) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    const int l = lab[q];
+    if (l < 0 || l >= nAtoms) atomicMin(first, (int)q);
+  }
+}
+
+// Upload host labels: copied into the spare label buffer and checked there on the device, so a
+// rejected upload leaves the state as it was; accepted labels become current and are copied to
+// the other buffer (the label pass writes interior points only).
+static int upload_labels(rq_ctx* c, const int32_t* label) {
+  const size_t n = (size_t)c->g.S3;
+  int* spare = c->lab[1 - c->cl];
+  CK(cudaMemcpyAsync(spare, label, n * sizeof(int), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemsetAsync(c->err + 2, 0x7f, sizeof(int), c->st));
+  k_check_labels<<<148 * 8, 256, 0, c->st>>>(spare, (long long)n, c->n_atoms, c->err + 2);
+  CK(cudaGetLastError());
+  int first = 0;
+  CK(cudaMemcpyAsync(&first, c->err + 2, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (first != 0x7f7f7f7f) {
+    CK(cudaMemcpyAsync(spare, c->lab[c->cl], n * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return rq_fail(c, RQ_EINVAL, "label " + std::to_string(label[first]) + " at index " + std::to_string(first) +
+                                     " outside [0, n_atoms)");
+  }
+  c->cl ^= 1;
+  CK(cudaMemcpyAsync(c->lab[1 - c->cl], c->lab[c->cl], n * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
   return RQ_OK;
 }
 
@@ -517,10 +541,8 @@ extern "C" int rq_upload_state(rq_ctx* c, const float* psi, const int32_t* label
   const size_t n = (size_t)c->g.S3;
   const bool mj = c->cfg.flavor == RQ_FLAVOR_MOLECULE_JS;
   if (label) {
-    int rc = check_labels(c, label);
+    int rc = upload_labels(c, label);
     if (rc != RQ_OK) return rc;
-    CK(cudaMemcpyAsync(c->lab[c->cl], label, n * sizeof(int), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->lab[1 - c->cl], c->lab[c->cl], n * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
     if (mj && (rc = mj_refresh_flags(c)) != RQ_OK) return rc;  // r_c-exclusion bits of the new labels
   }
   if (psi || P) c->sp_jdone = 0;  // an early Jacobi sweep used the old psi and P: redo it

@@ -136,3 +136,31 @@ def move(ref, F, vel, cfg):
     a5[:, :3] = ref.atom_pos
     ref.atoms5 = np.ascontiguousarray(a5.reshape(-1))
     orc.O().sp_recompute_K(ref.K, ref.atoms5, ref.nAtoms, ref.S, np.float32(ref.h), np.float32(ref.h2))
+
+
+def test_rejected_label_upload_leaves_the_state_unchanged():
+    """Labels are checked on the device after the copy; a label outside [0, n_atoms) is reported
+    (status RQ_EINVAL, index and value in the message) and the context keeps its state: the next
+    steps give the same fields as on a twin context that never saw the upload."""
+    from realmolecule_b200 import Context, _lib as L
+    cfg = h2o_cfg()
+    ctxs = [Context(cfg["gridN"], cfg["screen"], cfg["atoms"], flavor="solver.py") for _ in range(2)]
+    for c in ctxs:
+        c.initialize()
+        c.step(30)
+    st = ctxs[0].download(psi=True, label=True)
+    bad = st["label"].copy()
+    bad[1234] = len(cfg["atoms"]) + 5
+    with pytest.raises(L.RqError) as e:
+        ctxs[0].upload(label=bad)
+    assert e.value.status == L.RQ_EINVAL and "index 1234" in str(e.value)
+    assert np.array_equal(ctxs[0].download(psi=False, label=True)["label"], st["label"])
+    ctxs[0].upload(label=st["label"])  # an accepted upload of the same labels changes nothing either
+    for c in ctxs:
+        c.step(130)  # crosses a label step
+    a, b = (c.download(psi=True, label=True) for c in ctxs)
+    assert np.array_equal(a["label"], b["label"])
+    # psi: the FP64 domain sums of the normalisation are atomics in any order
+    np.testing.assert_allclose(a["psi"], b["psi"], rtol=1e-6, atol=1e-9)
+    for c in ctxs:
+        c.close()
