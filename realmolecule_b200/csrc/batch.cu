@@ -234,6 +234,8 @@ struct rq_batch {
   rq_config cfg{};
   double dv = 0.2;
   std::vector<BInst> hin;         // host copy of the instance table
+  std::vector<BInst> hin64;       // mixed batches: each instance's FP64 field set, taken over on promotion
+  BInst* din64 = nullptr;         // device copy of hin64 (to compute the FP64 K at initialisation)
   BInst* din = nullptr;           // device copy
   std::vector<std::vector<rq_atom>> atoms;
   std::vector<void*> allocs;
@@ -367,10 +369,8 @@ static int build_plans(rq_batch* b) {
   return RQ_OK;
 }
 
-// field buffers of instance q in its current precision (level 0 fields and the multigrid levels)
-static int alloc_fields(rq_batch* b, int q) {
-  BInst& I = b->hin[q];
-  const size_t es = b->f64[q] ? sizeof(double) : sizeof(float);
+// field buffers of one instance with elements of es bytes (level 0 fields and the multigrid levels)
+static int alloc_fields(rq_batch* b, BInst& I, size_t es) {
   const size_t S3 = (size_t)I.g.S3;
   for (int k = 0; k < 2; ++k) {
     BALLOC(I.U[k], S3 * es);
@@ -393,7 +393,7 @@ static int build(rq_batch* b) {
   const int n = b->n;
   for (int q = 0; q < n; ++q) {
     BInst& I = b->hin[q];
-    BRC(alloc_fields(b, q));
+    BRC(alloc_fields(b, I, b->f64[q] ? sizeof(double) : sizeof(float)));
     for (int k = 0; k < 2; ++k) BALLOC(I.lab[k], (size_t)I.g.S3 * sizeof(int));
     BALLOC(I.W, (size_t)I.g.S3 * sizeof(float));
     const int lc = I.nlev - 1;
@@ -438,6 +438,14 @@ static int build(rq_batch* b) {
     BCK(cudaMemcpyAsync(b->seeds_all, seeds.data(), sizeof(float4) * seeds.size(), cudaMemcpyHostToDevice, b->st));
   BALLOC(b->din, sizeof(BInst) * n);
   BCK(cudaMemcpyAsync(b->din, b->hin.data(), sizeof(BInst) * n, cudaMemcpyHostToDevice, b->st));
+  bool mixed = false;
+  for (int q = 0; q < n; ++q) mixed |= !b->f64[q];
+  if (mixed) {  // allocated up front, so a promotion during a solve allocates and synchronises nothing
+    b->hin64 = b->hin;
+    for (int q = 0; q < n; ++q) BRC(alloc_fields(b, b->hin64[q], sizeof(double)));
+    BALLOC(b->din64, sizeof(BInst) * n);
+    BCK(cudaMemcpyAsync(b->din64, b->hin64.data(), sizeof(BInst) * n, cudaMemcpyHostToDevice, b->st));
+  }
   b->items.resize(n);
   for (int q = 0; q < n; ++q) make_items(b->hin[q], q, b->items[q]);
   BRC(build_plans(b));
@@ -627,6 +635,14 @@ static int b_initialize(rq_batch* b) {
     BCK(cudaMemsetAsync(I.U[1], 0, es * I.g.S3, b->st));
     for (int k = 0; k < 2; ++k) BCK(cudaMemsetAsync(I.P[k], 0, es * I.g.S3, b->st));
     BCK(launch_fill(I.W, 1.0f, I.g.S3, b->st));
+  }
+  if (b->din64) {  // the FP64 K that promoted instances use
+    std::vector<BItem> f1;
+    for (int q = 0; q < b->n; ++q) f1.insert(f1.end(), b->items[q].flat1.begin(), b->items[q].flat1.end());
+    BRC(upload_plan(b, b->one, f1));
+    kb_potential<double><<<b->one.n, 256, 0, b->st>>>(b->din64, b->one.d, b->cfg.sigma);
+    BL("potential");
+    BCK(cudaStreamSynchronize(b->st));  // f1 is the source of an asynchronous copy
   }
   BRC(b_normalize(b));
   for (int v = 0; v < 10; ++v) BRC(each_set([&](auto tag, int p) { return b_vcycle<decltype(tag)>(b, p); }));
@@ -905,28 +921,26 @@ __global__ void kb_widen(const float* __restrict__ a, double* __restrict__ d, lo
     d[q] = (double)a[q];
 }
 
-// Move instance q of a mixed batch to FP64 fields for its final refinement (psi must be in its
-// normalised state): psi and P are widened, K is recomputed in FP64, the multigrid levels get
-// FP64 buffers, labels and W carry over.  The fp32 buffers stay allocated until the batch is
-// destroyed.  The caller rebuilds the work lists.
+// Move instance q of a mixed batch to its FP64 field set for the final refinement (psi must be
+// in its normalised state): psi and P are widened into it; its K was computed in FP64 at
+// initialisation, its multigrid levels are rebuilt by the next V-cycle, labels and W carry over.
+// Nothing is allocated and the host does not wait.  The caller rebuilds the work lists.
 static int b_promote(rq_batch* b, int q) {
   if (b->f64[q]) return RQ_OK;
+  if (b->hin64.empty()) {
+    b->last_error = "no FP64 field set for promotion";
+    return RQ_EINVAL;
+  }
   BInst& I = b->hin[q];
-  const BInst old = I;
-  b->f64[q] = 1;
-  BRC(alloc_fields(b, q));
+  const BInst& D = b->hin64[q];
   const long long S3 = I.g.S3;
-  kb_widen<<<148 * 4, 256, 0, b->st>>>((const float*)old.U[b->cu], (double*)I.U[b->cu], S3);
-  kb_widen<<<148 * 4, 256, 0, b->st>>>((const float*)old.P[b->cp], (double*)I.P[b->cp], S3);
+  kb_widen<<<148 * 4, 256, 0, b->st>>>((const float*)I.U[b->cu], (double*)D.U[b->cu], S3);
+  kb_widen<<<148 * 4, 256, 0, b->st>>>((const float*)I.P[b->cp], (double*)D.P[b->cp], S3);
   BCK(cudaGetLastError());
+  I = D;
+  b->f64[q] = 1;
+  // from pageable host memory: the copy has read I when the call returns
   BCK(cudaMemcpyAsync(b->din + q, &I, sizeof(BInst), cudaMemcpyHostToDevice, b->st));
-  std::vector<BItem> f1;
-  flat_items(f1, q, S3, 256);
-  BRC(upload_plan(b, b->one, f1));
-  kb_potential<double><<<b->one.n, 256, 0, b->st>>>(b->din, b->one.d, b->cfg.sigma);
-  BCK(cudaGetLastError());
-  // the host copies above (table entry, item list) must outlive the asynchronous copies
-  BCK(cudaStreamSynchronize(b->st));
   return RQ_OK;
 }
 
