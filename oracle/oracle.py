@@ -92,6 +92,8 @@ class _Oracle:
             "orc_mj_evolve_boundary": [_u32p, _u32p, _f32p, _f32p, _i, _f, _f],
             "orc_mj_jacobi": [_f32p, _f32p, _f32p, _i, _f, _f],
             "orc_mj_rho": [_f32p, _f32p, _i],
+            "orc_mj_rho_self": [_f32p, _u32p, C.c_uint32, _f32p, _i],
+            "orc_mj_sub_self": [_f32p, _f32p, _u32p, C.c_uint32, _f, _i],
             "orc_mj_residual": [_f32p, _f32p, _f32p, _i, _f, _f],
             "orc_mj_restrict": [_f32p, _f32p, _i, _i],
             "orc_mj_coarse_smooth": [_f32p, _f32p, _f32p, _i, _f],
@@ -342,7 +344,7 @@ class MoleculeJsDriver:
     """
 
     def __init__(self, NN, screen, atoms, dv=None, steps_per_frame=None, norm_interval=20, vcycle_interval=50,
-                 jacobi_per_step=2, boundary_speed=0.5, curv_reg=0.15):
+                 jacobi_per_step=2, boundary_speed=0.5, curv_reg=0.15, sic=False):
         self.NN = NN
         self.S = NN + 1
         self.S3 = self.S ** 3
@@ -381,6 +383,10 @@ class MoleculeJsDriver:
         self.W = np.ones(S3, np.float32)
         self.rho = np.zeros(S3, np.float32)
         self.steps_done = 0
+        self.frame = 0  # molecule.js frameCount
+        # SIC_INTERVAL (molecule.js:112); 0 = off
+        nel = nelec or 3
+        self.sic_interval = (1 if nel <= 15 else 5 if nel <= 30 else 0) if sic else 0
         SC = NN // 2 + 1
         self.SC = SC
 
@@ -400,16 +406,37 @@ class MoleculeJsDriver:
         self.label2[:] = self.label
 
     def vcycle(self):
+        O().mj_rho(self.U, self.rho, self.S)
+        self._vcycle_core(self.P, self.rho)
+
+    def _vcycle_core(self, P, rho):
+        """molecule.js:2879-2907: residual, restriction, 10 coarse sweeps from 0, damped prolongation."""
         S, SC = self.S, self.SC
         R = np.zeros(self.S3, np.float32)
-        O().mj_rho(self.U, self.rho, S)
-        O().mj_residual(self.P, R, self.rho, S, self.inv_h2, np.float32(2 * np.pi))
+        O().mj_residual(P, R, rho, S, self.inv_h2, np.float32(2 * np.pi))
         fc = np.zeros(SC ** 3, np.float32)
         O().mj_restrict(R, fc, S, SC)
         E = [np.zeros(SC ** 3, np.float32), np.zeros(SC ** 3, np.float32)]
         for cs in range(10):
             O().mj_coarse_smooth(E[cs % 2], E[(cs + 1) % 2], fc, SC, self.h2)
-        O().mj_prolong(E[0], self.P, S, SC)
+        O().mj_prolong(E[0], P, S, SC)
+
+    def sic_pass(self):
+        """molecule.js:3018-3075: per domain, solve for its own potential (4 sweeps from 0, the
+        coarse correction, 4 sweeps) and subtract P_m / Z_m from Pother on the domain."""
+        two_pi = np.float32(2 * np.pi)
+        for m, r in enumerate(self.rows):
+            Zm = np.float32(r["Z"])
+            if Zm == 0:
+                continue
+            O().mj_rho_self(self.U, self.label, m, self.rho, self.S)
+            a, b = np.zeros(self.S3, np.float32), np.zeros(self.S3, np.float32)
+            for js in range(4):
+                O().mj_jacobi(*((a, b) if js % 2 == 0 else (b, a)), self.rho, self.S, self.h2, two_pi)
+            self._vcycle_core(a, self.rho)
+            for js in range(4):
+                O().mj_jacobi(*((a, b) if js % 2 == 0 else (b, a)), self.rho, self.S, self.h2, two_pi)
+            O().mj_sub_self(a, self.Pother, self.label, m, Zm, self.S)
 
     def step(self):
         self.steps_done += 1
@@ -435,6 +462,9 @@ class MoleculeJsDriver:
                 self.Pother[:] = self.P
             else:
                 self.Pother[:] = 0
+            if poisson and self.sic_interval and self.frame > 0 and self.frame % self.sic_interval == 0:
+                self.sic_pass()
+            self.frame += 1
             for _ in range(max(1, self.spf)):
                 O().mj_evolve_boundary(self.label, self.label2, self.U, self.W, self.S, self.dt_w, self.curv)
                 self.label, self.label2 = self.label2, self.label

@@ -486,6 +486,33 @@ void orc_mj_rho(const float* U, float* rho, int S) {
       for (int k = 1; k < NN; ++k) { int64_t id = IDX(i, j, k, S); float u = U[id]; rho[id] = u * u; }
 }
 
+/* molecule.js:572-590 computeRhoSelf: rho = psi^2 where label == m, 0 elsewhere (interior only). */
+void orc_mj_rho_self(const float* U, const uint32_t* label, uint32_t m, float* rho, int S) {
+  const int NN = S - 1;
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        float u = U[id];
+        rho[id] = label[id] == m ? u * u : 0.0f;
+      }
+}
+
+/* molecule.js:694-721 subtractPself: Pother -= Pm * frac where label == m, with frac = 1/Z_m when
+   Z_m > 1 and 1 otherwise (f32). */
+void orc_mj_sub_self(const float* Pm, float* Pother, const uint32_t* label, uint32_t m, float Zm, int S) {
+  const int NN = S - 1;
+  const float frac = Zm > 1.0f ? 1.0f / Zm : 1.0f;
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        if (label[id] == m) Pother[id] = Pother[id] - Pm[id] * frac;
+      }
+}
+
 /* molecule.js:777-803 residual r = -2pi*rho - lap(P)/h^2 (sign as written). */
 void orc_mj_residual(const float* Pin, float* R, const float* rho, int S, float inv_h2, float two_pi) {
   const int NN = S - 1;

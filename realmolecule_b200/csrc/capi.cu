@@ -135,7 +135,7 @@ static void free_ctx(rq_ctx* c) {
   for (auto& gx : c->graph)
     if (gx) cudaGraphExecDestroy(gx);
   void* ptrs[] = {c->U[0], c->U[1], c->P[0], c->P[1], c->K, c->W, c->bestU, c->rho, c->Pother, c->resid, c->lab[0], c->lab[1],
-                  c->Ec[0], c->Ec[1], c->fc, c->atoms5, c->scratch_atoms5, c->bin_start, c->bin_idx, c->bin_far, c->bin_zmax, c->atoms_mj, c->atoms_nm, c->Zdom, c->Zdom64, c->dnorm,
+                  c->Ec[0], c->Ec[1], c->fc, c->atoms5, c->scratch_atoms5, c->sic, c->sic2, c->bin_start, c->bin_idx, c->bin_far, c->bin_zmax, c->atoms_mj, c->atoms_nm, c->Zdom, c->Zdom64, c->dnorm,
                   c->dpd, c->dF, c->dsum, c->unorm, c->scale, c->err, c->seeds, c->scale64, c->Kext};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -175,6 +175,10 @@ static int alloc_all(rq_ctx* c) {
     DALLOC(c->rho, S3 * sizeof(float));
     DALLOC(c->Pother, S3 * sizeof(float));
     DALLOC(c->resid, S3 * sizeof(float));
+    if (c->cfg.sic) {
+      DALLOC(c->sic, S3 * sizeof(float));
+      DALLOC(c->sic2, S3 * sizeof(float));
+    }
     const int SC = c->g.NN / 2 + 1;
     c->gc = make_geo(SC);
     const size_t SC3 = (size_t)c->gc.S3;
@@ -219,7 +223,16 @@ extern "C" int rq_create(const rq_config* cfg, const rq_atom* atoms, int32_t n_a
   if (cfg->NN < 4 || cfg->NN % 2 != 0 || cfg->screen <= 0) return RQ_EINVAL;  // molecule.js:155 needs even NN
   if (cfg->flavor < 0 || cfg->flavor > 2 || cfg->precision < 0 || cfg->precision > 1) return RQ_EINVAL;
   if (cfg->precision == RQ_PREC_FP64 && cfg->flavor != RQ_FLAVOR_NEW) return RQ_ENOTSUP;
-  if (cfg->sic != 0) return RQ_ENOTSUP;
+  if (cfg->sic != 0 && cfg->flavor != RQ_FLAVOR_MOLECULE_JS) return RQ_ENOTSUP;  // SIC is molecule.js's
+  if (cfg->sic != 0) {  // molecule.js:111: NELEC <= 5 takes the direct per-electron Poisson, not built here
+    int nelec = 0;
+    for (int q = 0; q < n_atoms; ++q) nelec += (atoms[q].Z > 0 || atoms[q].Z_nuc > 0) ? 1 : 0;
+    if (nelec <= 5) {
+      std::fprintf(stderr, "rq_create: sic with %d electron domains needs the direct per-electron Poisson of "
+                           "molecule.js (NELEC <= 5), which is not built\n", nelec);
+      return RQ_ENOTSUP;
+    }
+  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return RQ_ENODEV;
   rq_ctx* c = new (std::nothrow) rq_ctx();
@@ -415,7 +428,7 @@ static int schedule_period(const rq_ctx* c) {
   long p = 1;
   switch (f.flavor) {
     case RQ_FLAVOR_SOLVER_PY: p = lcm(lcm(f.poisson_interval, f.norm_interval), f.label_interval); break;
-    case RQ_FLAVOR_MOLECULE_JS: p = f.steps_per_frame; break;
+    case RQ_FLAVOR_MOLECULE_JS: p = (long)f.steps_per_frame * std::max(1, mj_sic_interval(c)); break;
     default: p = lcm(lcm(f.poisson_interval, f.norm_interval), f.label_interval); break;
   }
   return p > 4096 ? 0 : (int)p;
@@ -440,8 +453,9 @@ extern "C" int rq_step(rq_ctx* c, int32_t n) {
     const bool straddle = lu > 0 && c->steps_done < lu && c->steps_done + period > lu;
     // (a period boundary never leaves an early Jacobi sweep pending: the step before a Poisson step
     // is never the last of a period, as the period is a multiple of poisson_interval)
+    // (with SIC, frame 0 never corrects: the first period runs eagerly, the later ones repeat)
     const bool aligned = !c->prof && !straddle && period > 0 && c->steps_done % period == 0 && left >= period &&
-                         c->sp_jdone == 0;
+                         c->sp_jdone == 0 && !(mj_sic_interval(c) > 0 && c->frame == 0);
     if (!aligned) {
       // run eagerly up to the next period boundary (or all that is left)
       int todo = left;
@@ -478,6 +492,7 @@ extern "C" int rq_step(rq_ctx* c, int32_t n) {
       c->nm_pending = (post >> 4) & 1;
       c->nm_age = post >> 5;
       c->steps_done += period;
+      if (c->cfg.flavor == RQ_FLAVOR_MOLECULE_JS) c->frame += period / c->cfg.steps_per_frame;
       c->launches += c->graph_launches[key];
     }
     left -= period;

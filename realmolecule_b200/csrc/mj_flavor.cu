@@ -2,9 +2,11 @@
 //
 // One rq_step of this flavour is one iteration of the s-loop of doSteps (molecule.js:2829-3006);
 // every steps_per_frame steps the frame tail runs (Pother <- P, molecule.js:3014-3015, then
-// W_STEPS_PER_FRAME level-set passes, :3093-3104).  The self-interaction correction and the
-// direct per-electron Poisson of small systems (:2833-2858, :3016-3076) are not built: this
-// flavour always takes the total-Poisson path the reference uses for NELEC > 30.
+// W_STEPS_PER_FRAME level-set passes, :3093-3104).  With cfg.sic the frame tail also runs the
+// self-interaction correction of the total-Poisson path (:3016-3076) on the reference's frames:
+// every frame for NELEC <= 15, every 5th for NELEC <= 30, never above.  The direct per-electron
+// Poisson the reference uses for NELEC <= 5 (:2833-2858) is not built; such systems are
+// rejected when cfg.sic asks for the reference's behaviour.
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -56,6 +58,20 @@ MjParams mj_params(const rq_ctx* c) {
 }
 
 const MjAtom* atoms_dev(rq_ctx* c) { return (const MjAtom*)c->atoms_mj; }
+
+}  // namespace
+
+// Frames between self-interaction corrections (SIC_INTERVAL, molecule.js:112), 0 when off.
+int mj_sic_interval(const rq_ctx* c) {
+  if (c->cfg.flavor != RQ_FLAVOR_MOLECULE_JS || !c->cfg.sic) return 0;
+  int nelec = 0;
+  for (auto& a : c->atoms)
+    if (a.Z > 0 || a.Z_nuc > 0) nelec++;
+  if (nelec == 0) nelec = 3;  // molecule.js:16
+  return nelec <= 15 ? 1 : nelec <= 30 ? 5 : 0;
+}
+
+namespace {
 
 double interior(const Geo& g) {
   const double n = g.NN - 1;
@@ -132,11 +148,26 @@ int mj_step_one(rq_ctx* c, int s) {
     LAUNCH(RQ_KC_NORMALIZE, 12 * ip, launch_mj_apply_scale((float*)c->U[c->cu], c->lab[c->cl], c->scale, c->g, c->st));
   }
   if (sf == spf - 1) {
-    // frame tail: Pother <- P_buf[0] (no SIC), then the level-set passes on the same psi
+    // frame tail: Pother <- P_buf[0], the self-interaction correction on its frames (the frame
+    // counter is the reference's frameCount, incremented before the level-set passes), then the
+    // level-set passes on the same psi
     if (poisson)
       CK(cudaMemcpyAsync(c->Pother, c->P[c->cp], (size_t)c->g.S3 * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
     else
       CK(cudaMemsetAsync(c->Pother, 0, (size_t)c->g.S3 * sizeof(float), c->st));
+    const int sic = mj_sic_interval(c);
+    if (poisson && sic > 0 && c->frame > 0 && c->frame % sic == 0) {
+      for (int m = 0; m < c->n_atoms; ++m) {
+        const float Zm = (float)c->atoms[m].Z;
+        if (Zm == 0.f) continue;
+        const float frac = Zm > 1.f ? 1.0f / Zm : 1.0f;
+        LAUNCH(RQ_KC_MG, 120 * ip,
+               launch_mj_sic_domain((float*)c->U[c->cu], c->lab[c->cl], c->Pother, m, frac, c->rho, c->sic, c->sic2,
+                                    c->resid, c->Ec[0], c->Ec[1], c->fc, c->g, c->gc, p.h2, p.inv_h2, p.two_pi,
+                                    c->st));
+      }
+    }
+    c->frame++;
     const int wsteps = spf > 1 ? spf : 1;  // W_STEPS_PER_FRAME (:107)
     for (int q = 0; q < wsteps; ++q) {
       LAUNCH(RQ_KC_LABELS, 20 * ip,

@@ -240,6 +240,31 @@ __global__ void __launch_bounds__(256) k_mj_jacobi(const float* __restrict__ Pin
   }
 }
 
+// The same weighted Jacobi sweep with the right-hand side read from a density buffer: the
+// self-potential solve of the self-interaction correction (jacobiSmooth with rhoTotal bound to
+// the single-domain density, molecule.js:723-749, :3024-3030).
+__global__ void __launch_bounds__(256) k_mj_jacobi_rho(const float* __restrict__ Pin, float* __restrict__ Pout,
+                                                       const float* __restrict__ rho, Geo g, float h2, float two_pi) {
+  const int k = 1 + blockIdx.x * kThreadsK + threadIdx.x;
+  const int j = 1 + blockIdx.y * kThreadsJ + threadIdx.y;
+  const int i0 = 1 + blockIdx.z * kMarch;
+  if (k >= g.NN || j >= g.NN || i0 >= g.NN) return;
+  const int iend = min(i0 + kMarch, g.NN);
+  const long long S = g.S, S2 = g.S2;
+  long long id = (long long)i0 * S2 + j * S + k;
+  float p_m = __ldg(Pin + id - S2), p_c = __ldg(Pin + id);
+  const float c0 = F_MUL(h2, two_pi);
+  for (int i = i0; i < iend; ++i, id += S2) {
+    const float p_p = __ldg(Pin + id + S2);
+    const float sn = F_ADD(F_ADD(F_ADD(F_ADD(F_ADD(p_p, p_m), __ldg(Pin + id + S)), __ldg(Pin + id - S)),
+                                 __ldg(Pin + id + 1)),
+                           __ldg(Pin + id - 1));
+    const float rhs = F_MUL(c0, __ldg(rho + id));
+    Pout[id] = F_ADD(F_MUL(0.3333f, p_c), F_DIV(F_ADD(sn, rhs), 9.0f));
+    p_m = p_c; p_c = p_p;
+  }
+}
+
 // ---------------------------------------------------------------------------------------
 // the 2-level V-cycle of molecule.js:777-909 (one thread per point; it runs every
 // POISSON_INTERVAL steps at most)
@@ -255,6 +280,25 @@ __global__ void k_mj_rho(const float* __restrict__ U, float* __restrict__ rho, G
   if (id >= g.S3 || !interior_of(id, g, i, j, k)) return;
   const float u = U[id];
   rho[id] = F_MUL(u, u);
+}
+
+// computeRhoSelf (molecule.js:572-590): psi^2 where the label is m, 0 elsewhere (interior points)
+__global__ void k_mj_rho_self(const float* __restrict__ U, const int* __restrict__ label, int m,
+                              float* __restrict__ rho, Geo g) {
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, k;
+  if (id >= g.S3 || !interior_of(id, g, i, j, k)) return;
+  const float u = U[id];
+  rho[id] = ((label[id] & kMjMask) == m) ? F_MUL(u, u) : 0.0f;
+}
+
+// subtractPself (molecule.js:694-721): Pother -= Pm * frac where the label is m
+__global__ void k_mj_sub_self(const float* __restrict__ Pm, float* __restrict__ Pother, const int* __restrict__ label,
+                              int m, float frac, Geo g) {
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, k;
+  if (id >= g.S3 || !interior_of(id, g, i, j, k)) return;
+  if ((label[id] & kMjMask) == m) Pother[id] = F_SUB(Pother[id], F_MUL(Pm[id], frac));
 }
 
 __global__ void k_mj_residual(const float* __restrict__ Pin, float* __restrict__ R, const float* __restrict__ rho, Geo g,
@@ -550,11 +594,10 @@ cudaError_t launch_mj_jacobi(const float* Pin, float* Pout, const float* U, cons
   k_mj_jacobi<<<march_grid(g), march_block(), 0, st>>>(Pin, Pout, U, g, h2, two_pi);
   return cudaGetLastError();
 }
-cudaError_t launch_mj_vcycle(float* P, const float* U, float* rho, float* resid, float* Ec0, float* Ec1, float* fc,
-                             const Geo& g, const Geo& gc, float h2, float inv_h2, float two_pi, cudaStream_t st) {
-  // molecule.js:2879-2907: residual of P, restrict, 10 coarse weighted-Jacobi sweeps from 0,
-  // prolongate with P += 0.5 * correction
-  k_mj_rho<<<flat_blocks(g.S3), 256, 0, st>>>(U, rho, g);
+// molecule.js:2879-2907 (and :3031-3061 for the self-potential): residual of P for the density
+// rho, restrict, 10 coarse weighted-Jacobi sweeps from 0, prolongate with P += 0.5 * correction
+static cudaError_t mj_vcycle_core(float* P, const float* rho, float* resid, float* Ec0, float* Ec1, float* fc,
+                                  const Geo& g, const Geo& gc, float h2, float inv_h2, float two_pi, cudaStream_t st) {
   k_mj_residual<<<flat_blocks(g.S3), 256, 0, st>>>(P, resid, rho, g, inv_h2, two_pi);
   const long long nc = (long long)(gc.NN - 1) * (gc.NN - 1) * (gc.NN - 1);
   k_mj_restrict<<<flat_blocks(nc), 256, 0, st>>>(resid, fc, g, gc);
@@ -565,6 +608,32 @@ cudaError_t launch_mj_vcycle(float* P, const float* U, float* rho, float* resid,
   float* E[2] = {Ec0, Ec1};
   for (int cs = 0; cs < 10; ++cs) k_mj_coarse_smooth<<<flat_blocks(nc), 256, 0, st>>>(E[cs % 2], E[(cs + 1) % 2], fc, gc, h2);
   k_mj_prolong<<<flat_blocks(g.S3), 256, 0, st>>>(E[0], P, g, gc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mj_vcycle(float* P, const float* U, float* rho, float* resid, float* Ec0, float* Ec1, float* fc,
+                             const Geo& g, const Geo& gc, float h2, float inv_h2, float two_pi, cudaStream_t st) {
+  k_mj_rho<<<flat_blocks(g.S3), 256, 0, st>>>(U, rho, g);
+  return mj_vcycle_core(P, rho, resid, Ec0, Ec1, fc, g, gc, h2, inv_h2, two_pi, st);
+}
+
+cudaError_t launch_mj_sic_domain(const float* U, const int* label, float* Pother, int m, float frac, float* rho,
+                                 float* sic, float* sic2, float* resid, float* Ec0, float* Ec1, float* fc, const Geo& g,
+                                 const Geo& gc, float h2, float inv_h2, float two_pi, cudaStream_t st) {
+  // molecule.js:3018-3075 for one domain: its density, 4 Jacobi sweeps from 0 (sic <-> sic2),
+  // the coarse correction, 4 more sweeps, then Pother -= P_m / Z_m on the domain
+  if (g.NN < 2) return cudaSuccess;
+  k_mj_rho_self<<<flat_blocks(g.S3), 256, 0, st>>>(U, label, m, rho, g);
+  cudaError_t e = cudaMemsetAsync(sic, 0, sizeof(float) * g.S3, st);
+  if (e != cudaSuccess) return e;
+  for (int js = 0; js < 4; ++js)
+    k_mj_jacobi_rho<<<march_grid(g), march_block(), 0, st>>>(js % 2 ? sic2 : sic, js % 2 ? sic : sic2, rho, g, h2,
+                                                             two_pi);
+  if ((e = mj_vcycle_core(sic, rho, resid, Ec0, Ec1, fc, g, gc, h2, inv_h2, two_pi, st)) != cudaSuccess) return e;
+  for (int js = 0; js < 4; ++js)
+    k_mj_jacobi_rho<<<march_grid(g), march_block(), 0, st>>>(js % 2 ? sic2 : sic, js % 2 ? sic : sic2, rho, g, h2,
+                                                             two_pi);
+  k_mj_sub_self<<<flat_blocks(g.S3), 256, 0, st>>>(sic, Pother, label, m, frac, g);
   return cudaGetLastError();
 }
 cudaError_t launch_mj_evolve(const int* labIn, int* labOut, const float* U, float* W, const MjAtom* atoms, int nAt,

@@ -53,6 +53,7 @@ struct rq_ctx {
   // atoms on the device
   float* atoms5 = nullptr;    // [i,j,k,Z,rc] f32 (cloud/solver.py:378-382)
   float* scratch_atoms5 = nullptr;  // per-call atom table for force variants
+  float *sic = nullptr, *sic2 = nullptr;  // molecule.js flavour with SIC: self-potential ping-pong
   // solver.py flavour: atom bins of the label step's argmax (rebuilt whenever atoms change)
   int bins_nb = 0, bins_bin = 0;
   int *bin_start = nullptr, *bin_idx = nullptr, *bin_far = nullptr;

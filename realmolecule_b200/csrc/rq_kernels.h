@@ -68,6 +68,11 @@ cudaError_t launch_mj_jacobi(const float* Pin, float* Pout, const float* U, cons
                              cudaStream_t st);
 cudaError_t launch_mj_vcycle(float* P, const float* U, float* rho, float* resid, float* Ec0, float* Ec1, float* fc,
                              const Geo& g, const Geo& gc, float h2, float inv_h2, float two_pi, cudaStream_t st);
+// the self-interaction correction of one domain m (molecule.js:3018-3075); rho, sic, sic2, resid,
+// Ec0, Ec1 and fc are scratch
+cudaError_t launch_mj_sic_domain(const float* U, const int* label, float* Pother, int m, float frac, float* rho,
+                                 float* sic, float* sic2, float* resid, float* Ec0, float* Ec1, float* fc, const Geo& g,
+                                 const Geo& gc, float h2, float inv_h2, float two_pi, cudaStream_t st);
 cudaError_t launch_mj_evolve(const int* labIn, int* labOut, const float* U, float* W, const MjAtom* atoms, int nAt,
                              const Geo& g, float dt_w, float curvReg, float h, bool hasBare, cudaStream_t st);
 cudaError_t launch_mj_energy(const float* U, const float* Pv, const float* K, const int* label, const MjAtom* atoms,

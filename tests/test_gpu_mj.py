@@ -24,6 +24,15 @@ def atoms_case(kind):
                          {"i": 19, "j": 16, "k": 16, "Z": 1, "Z_nuc": 1, "rc": 0.0},
                          {"i": 16, "j": 20, "k": 16, "Z": 0, "Z_nuc": 1, "rc": 0.3},
                          {"i": 16, "j": 12, "k": 14, "Z": 1, "Z_nuc": 1, "rc": 0.0}]
+    if kind == "ten":  # 10 domains: the self-interaction correction runs every frame (NELEC <= 15)
+        rng = np.random.default_rng(11)
+        rows = []
+        for n in range(10):
+            p = rng.integers(12, 28, 3)
+            z = float(rng.integers(1, 3))
+            rows.append({"i": int(p[0]), "j": int(p[1]), "k": int(p[2]), "Z": z, "Z_nuc": z,
+                         "rc": float(rng.choice([0.0, 0.35]))})
+        return 40, 10.0, rows
     rng = np.random.default_rng(3)  # many domains
     rows = []
     for n in range(24):
@@ -123,3 +132,44 @@ def test_set_atoms_persistent_relabel():
     lab = ctx.download(psi=False, label=True)["label"]
     # bestU came from each side's own init (expf), so allow a handful of near-tie cells
     assert (lab != ref.label.astype(np.int32)).sum() <= 5
+
+
+@pytest.mark.parametrize("kind,frames", [("ten", 3), ("many", 6)])
+def test_frames_with_self_interaction_correction_bit_exact(kind, frames):
+    """cfg.sic: on the reference's frames (every frame for NELEC <= 15, every 5th for <= 30, never
+    on frame 0) each domain's own potential is solved (4 sweeps, the coarse correction, 4 sweeps)
+    and P_m / Z_m leaves Pother on the domain -- bit for bit with the oracle, through the graphs
+    of whole SIC periods."""
+    opts = dict(steps_per_frame=7, norm_interval=5, vcycle_interval=3)
+    from realmolecule_b200 import Context
+    NN, screen, rows = atoms_case(kind)
+    ref = orc.MoleculeJsDriver(NN, screen, rows, sic=True, **opts)
+    ref.initialize()
+    ctx = Context(NN, screen, rows, flavor="molecule.js", sic=1, **opts)
+    ctx.initialize()
+    ctx.upload(psi=ref.U, label=ref.label.astype(np.int32))
+    nsteps = frames * 7 + 2
+    plain = orc.MoleculeJsDriver(NN, screen, rows, **opts)  # the same run without the correction
+    plain.initialize()
+    plain.U[:] = ref.U
+    for _ in range(nsteps):
+        ref.step()
+        plain.step()
+    ctx.step(nsteps)
+    st = ctx.download(psi=True, label=True, W=True, P=True)
+    assert not np.array_equal(ref.Pother, plain.Pother)  # the correction did run
+    assert np.array_equal(st["label"], ref.label.astype(np.int32))
+    assert np.array_equal(st["W"].view(np.uint32), ref.W.view(np.uint32))
+    assert np.array_equal(st["P"].view(np.uint32), ref.P.view(np.uint32))
+    assert np.array_equal(st["psi"].view(np.uint32), ref.U.view(np.uint32))
+    from realmolecule_b200 import _lib as L
+    e = ctx.energy()
+    np.testing.assert_allclose(e[L.E_EE], ref.energy()[2], rtol=1e-9)  # V_ee reads the corrected Pother
+
+
+def test_self_interaction_correction_needs_more_than_five_domains():
+    from realmolecule_b200 import Context, _lib as L
+    NN, screen, rows = atoms_case("water")
+    with pytest.raises(L.RqError) as e:
+        Context(NN, screen, rows, flavor="molecule.js", sic=1)
+    assert e.value.status == L.RQ_ENOTSUP
