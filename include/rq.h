@@ -74,10 +74,10 @@ typedef struct rq_config {
   int32_t mg_levels;        /* new: multigrid levels (<=0: as deep as NN allows, coarsest >= 4) */
   int32_t mg_pre, mg_post;  /* new: red-black sweeps before / after the coarse correction (1, 1) */
   int32_t mg_coarse_sweeps; /* new: FP64 red-black sweeps on the coarsest level (16) */
-  int32_t sic;              /* molecule.js flavour: 1 = the reference's self-interaction correction
-                               (:3009-3076) on its frames (every frame for <= 15 domains, every
-                               5th for <= 30, never above); <= 5 domains -> RQ_ENOTSUP (the direct
-                               per-electron Poisson of :2833-2858 is not built); 0 off */
+  int32_t sic;              /* molecule.js flavour: 1 = the reference's own Pother path (:111-112):
+                               <= 5 domains the direct per-electron Poisson (:2833-2858), else the
+                               self-interaction correction (:3009-3076) every frame (<= 15 domains)
+                               or every 5th (<= 30), none above; 0 = total Poisson, no correction */
   double boundary_speed;    /* molecule.js dt_w (0.5, :135) */
   double curv_reg;          /* molecule.js curvReg (0: 0.15 as :34; < 0: off) */
   double sigma;             /* new: Gaussian nucleus width in bohr (<=0: h) */

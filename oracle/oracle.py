@@ -93,6 +93,9 @@ class _Oracle:
             "orc_mj_jacobi": [_f32p, _f32p, _f32p, _i, _f, _f],
             "orc_mj_rho": [_f32p, _f32p, _i],
             "orc_mj_rho_self": [_f32p, _u32p, C.c_uint32, _f32p, _i],
+            "orc_mj_rho_other": [_f32p, _u32p, C.c_uint32, _f32p, _i],
+            "orc_mj_copy_for_label": [_f32p, _f32p, _u32p, C.c_uint32, _i],
+            "orc_mj_init_pdirect": [C.c_void_p, _i, C.c_uint32, _f32p, _f32p, _i, _f, _f],
             "orc_mj_sub_self": [_f32p, _f32p, _u32p, C.c_uint32, _f, _i],
             "orc_mj_residual": [_f32p, _f32p, _f32p, _i, _f, _f],
             "orc_mj_restrict": [_f32p, _f32p, _i, _i],
@@ -386,7 +389,11 @@ class MoleculeJsDriver:
         self.frame = 0  # molecule.js frameCount
         # SIC_INTERVAL (molecule.js:112); 0 = off
         nel = nelec or 3
-        self.sic_interval = (1 if nel <= 15 else 5 if nel <= 30 else 0) if sic else 0
+        # sic=True takes the reference's own Pother path: the direct per-electron Poisson for
+        # NELEC <= 5 (USE_DIRECT_POTHER, molecule.js:111), else the SIC every SIC_INTERVAL frames
+        self.direct = bool(sic) and nel <= 5
+        self.sic_interval = (1 if nel <= 15 else 5 if nel <= 30 else 0) if sic and not self.direct else 0
+        self.Pdirect = {}
         SC = NN // 2 + 1
         self.SC = SC
 
@@ -395,6 +402,14 @@ class MoleculeJsDriver:
         self.bestU[:] = self.U
         self.Unext[:] = self.U
         self.label2[:] = self.label
+        if self.direct and self.n_electrons > 1:  # molecule.js:2678-2693
+            self.Pother[:] = 0
+            for m, r in enumerate(self.rows):
+                if np.float32(r["Z"]) == 0:
+                    continue
+                self.Pdirect[m] = np.zeros(self.S3, np.float32)
+                O().mj_init_pdirect(C.addressof(self.atoms), self.nA, m, self.Pdirect[m], self.Pother, self.S, self.h,
+                                    self.h2)
 
     def set_positions(self, rows):
         self.rows = [dict(a) for a in rows]
@@ -442,7 +457,15 @@ class MoleculeJsDriver:
         self.steps_done += 1
         sf = (self.steps_done - 1) % self.spf
         poisson = self.n_electrons > 1
-        if poisson:
+        if poisson and self.direct:  # molecule.js:2833-2858
+            two_pi = np.float32(2 * np.pi)
+            for m, Pm in self.Pdirect.items():
+                O().mj_rho_other(self.U, self.label, m, self.rho, self.S)
+                scratch = np.zeros(self.S3, np.float32)
+                for js in range(10):
+                    O().mj_jacobi(*((Pm, scratch) if js % 2 == 0 else (scratch, Pm)), self.rho, self.S, self.h2, two_pi)
+                O().mj_copy_for_label(Pm, self.Pother, self.label, m, self.S)
+        elif poisson:
             O().mj_rho(self.U, self.rho, self.S)
             for _ in range(self.jps):
                 O().mj_jacobi(self.P, self.P2, self.rho, self.S, self.h2, np.float32(2 * np.pi))
@@ -458,10 +481,10 @@ class MoleculeJsDriver:
             O().mj_norms_fixed(self.U, self.label, self.S, self.h3, self.nA, acc, nf)
             O().mj_normalize(self.U, nf, self.label, C.addressof(self.atoms), self.S)
         if sf == self.spf - 1:
-            if poisson:
-                self.Pother[:] = self.P
-            else:
+            if not poisson:
                 self.Pother[:] = 0
+            elif not self.direct:  # the direct path builds Pother every step
+                self.Pother[:] = self.P
             if poisson and self.sic_interval and self.frame > 0 and self.frame % self.sic_interval == 0:
                 self.sic_pass()
             self.frame += 1

@@ -513,6 +513,53 @@ void orc_mj_sub_self(const float* Pm, float* Pother, const uint32_t* label, uint
       }
 }
 
+/* molecule.js:593-612 computeRhoOther: rho = psi^2 except where label == m (interior only). */
+void orc_mj_rho_other(const float* U, const uint32_t* label, uint32_t m, float* rho, int S) {
+  const int NN = S - 1;
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        float u = U[id];
+        rho[id] = label[id] == m ? 0.0f : u * u;
+      }
+}
+
+/* molecule.js:651-671 copyPotherForLabel: Pother = Psrc where label == m. */
+void orc_mj_copy_for_label(const float* Psrc, float* Pother, const uint32_t* label, uint32_t m, int S) {
+  const int NN = S - 1;
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        if (label[id] == m) Pother[id] = Psrc[id];
+      }
+}
+
+/* molecule.js:614-649 initPdirect: Pm = sum over n != m with Z_n > 0 of 0.5/sqrt(r^2 + h^2) at the
+   truncated positions (f32, atoms in index order); Pother += Pm. */
+void orc_mj_init_pdirect(const orc_mj_atom* atoms, int nAt, uint32_t m, float* Pm, float* Pother, int S, float h,
+                         float h2) {
+  const int NN = S - 1;
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        float xi = (float)i * h, yj = (float)j * h, zk = (float)k * h, val = 0.0f;
+        for (int n = 0; n < nAt; ++n) {
+          if (atoms[n].Z <= 0.0f || (uint32_t)n == m) continue;
+          float dx = xi - (float)atoms[n].posI * h, dy = yj - (float)atoms[n].posJ * h, dz = zk - (float)atoms[n].posK * h;
+          float r = sqrtf(dx * dx + dy * dy + dz * dz + h2);
+          val += 0.5f / r;
+        }
+        Pm[id] = val;
+        Pother[id] += val;
+      }
+}
+
 /* molecule.js:777-803 residual r = -2pi*rho - lap(P)/h^2 (sign as written). */
 void orc_mj_residual(const float* Pin, float* R, const float* rho, int S, float inv_h2, float two_pi) {
   const int NN = S - 1;

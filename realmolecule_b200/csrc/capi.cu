@@ -135,7 +135,7 @@ static void free_ctx(rq_ctx* c) {
   for (auto& gx : c->graph)
     if (gx) cudaGraphExecDestroy(gx);
   void* ptrs[] = {c->U[0], c->U[1], c->P[0], c->P[1], c->K, c->W, c->bestU, c->rho, c->Pother, c->resid, c->lab[0], c->lab[1],
-                  c->Ec[0], c->Ec[1], c->fc, c->atoms5, c->scratch_atoms5, c->sic, c->sic2, c->bin_start, c->bin_idx, c->bin_far, c->bin_zmax, c->atoms_mj, c->atoms_nm, c->Zdom, c->Zdom64, c->dnorm,
+                  c->Ec[0], c->Ec[1], c->fc, c->atoms5, c->scratch_atoms5, c->sic, c->sic2, c->pdirect, c->bin_start, c->bin_idx, c->bin_far, c->bin_zmax, c->atoms_mj, c->atoms_nm, c->Zdom, c->Zdom64, c->dnorm,
                   c->dpd, c->dF, c->dsum, c->unorm, c->scale, c->err, c->seeds, c->scale64, c->Kext};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -178,6 +178,7 @@ static int alloc_all(rq_ctx* c) {
     if (c->cfg.sic) {
       DALLOC(c->sic, S3 * sizeof(float));
       DALLOC(c->sic2, S3 * sizeof(float));
+      if (mj_direct(c)) DALLOC(c->pdirect, S3 * sizeof(float) * n);
     }
     const int SC = c->g.NN / 2 + 1;
     c->gc = make_geo(SC);
@@ -224,15 +225,6 @@ extern "C" int rq_create(const rq_config* cfg, const rq_atom* atoms, int32_t n_a
   if (cfg->flavor < 0 || cfg->flavor > 2 || cfg->precision < 0 || cfg->precision > 1) return RQ_EINVAL;
   if (cfg->precision == RQ_PREC_FP64 && cfg->flavor != RQ_FLAVOR_NEW) return RQ_ENOTSUP;
   if (cfg->sic != 0 && cfg->flavor != RQ_FLAVOR_MOLECULE_JS) return RQ_ENOTSUP;  // SIC is molecule.js's
-  if (cfg->sic != 0) {  // molecule.js:111: NELEC <= 5 takes the direct per-electron Poisson, not built here
-    int nelec = 0;
-    for (int q = 0; q < n_atoms; ++q) nelec += (atoms[q].Z > 0 || atoms[q].Z_nuc > 0) ? 1 : 0;
-    if (nelec <= 5) {
-      std::fprintf(stderr, "rq_create: sic with %d electron domains needs the direct per-electron Poisson of "
-                           "molecule.js (NELEC <= 5), which is not built\n", nelec);
-      return RQ_ENOTSUP;
-    }
-  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return RQ_ENODEV;
   rq_ctx* c = new (std::nothrow) rq_ctx();

@@ -2,11 +2,11 @@
 //
 // One rq_step of this flavour is one iteration of the s-loop of doSteps (molecule.js:2829-3006);
 // every steps_per_frame steps the frame tail runs (Pother <- P, molecule.js:3014-3015, then
-// W_STEPS_PER_FRAME level-set passes, :3093-3104).  With cfg.sic the frame tail also runs the
-// self-interaction correction of the total-Poisson path (:3016-3076) on the reference's frames:
-// every frame for NELEC <= 15, every 5th for NELEC <= 30, never above.  The direct per-electron
-// Poisson the reference uses for NELEC <= 5 (:2833-2858) is not built; such systems are
-// rejected when cfg.sic asks for the reference's behaviour.
+// W_STEPS_PER_FRAME level-set passes, :3093-3104).  cfg.sic = 1 takes the reference's own choice
+// of Pother: for NELEC <= 5 the direct per-electron Poisson (:2833-2858; persistent P_m solved
+// every step, Pother = P_m on domain m), above it the total Poisson with the self-interaction
+// correction in the frame tail (:3016-3076) every frame for NELEC <= 15, every 5th for NELEC <=
+// 30, never above.  cfg.sic = 0 always takes the total Poisson without the correction.
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -61,13 +61,22 @@ const MjAtom* atoms_dev(rq_ctx* c) { return (const MjAtom*)c->atoms_mj; }
 
 }  // namespace
 
-// Frames between self-interaction corrections (SIC_INTERVAL, molecule.js:112), 0 when off.
-int mj_sic_interval(const rq_ctx* c) {
-  if (c->cfg.flavor != RQ_FLAVOR_MOLECULE_JS || !c->cfg.sic) return 0;
+static int mj_nelec(const rq_ctx* c) {  // NELEC (molecule.js:12-17)
   int nelec = 0;
   for (auto& a : c->atoms)
     if (a.Z > 0 || a.Z_nuc > 0) nelec++;
-  if (nelec == 0) nelec = 3;  // molecule.js:16
+  return nelec ? nelec : 3;
+}
+
+// The direct per-electron Poisson path (USE_DIRECT_POTHER, molecule.js:111).
+bool mj_direct(const rq_ctx* c) {
+  return c->cfg.flavor == RQ_FLAVOR_MOLECULE_JS && c->cfg.sic && mj_nelec(c) <= 5;
+}
+
+// Frames between self-interaction corrections (SIC_INTERVAL, molecule.js:112), 0 when off.
+int mj_sic_interval(const rq_ctx* c) {
+  if (c->cfg.flavor != RQ_FLAVOR_MOLECULE_JS || !c->cfg.sic || mj_direct(c)) return 0;
+  const int nelec = mj_nelec(c);
   return nelec <= 15 ? 1 : nelec <= 30 ? 5 : 0;
 }
 
@@ -94,6 +103,13 @@ int mj_initialize(rq_ctx* c) {
   for (int b = 0; b < 2; ++b) CK(cudaMemsetAsync(c->P[b], 0, n * sizeof(float), c->st));
   CK(cudaMemsetAsync(c->Pother, 0, n * sizeof(float), c->st));
   LAUNCH(RQ_KC_OTHER, 4.0 * c->g.S3, launch_fill(c->W, 1.0f, c->g.S3, c->st));
+  if (mj_direct(c) && p.n_electrons > 1) {  // P_m = sum_{n != m} 0.5/r, Pother = sum_m P_m (:2678-2693)
+    for (int m = 0; m < c->n_atoms; ++m)
+      if (c->atoms[m].Z != 0)
+        LAUNCH(RQ_KC_OTHER, 8.0 * c->g.S3,
+               launch_mj_direct_init(atoms_dev(c), c->n_atoms, m, c->pdirect + (size_t)m * n, c->Pother, c->g, p.h,
+                                     p.h2, c->st));
+  }
   return RQ_OK;
 }
 
@@ -124,7 +140,15 @@ int mj_step_one(rq_ctx* c, int s) {
   const int sf = (s - 1) % spf;  // position inside the frame (doSteps' s)
   const bool poisson = p.n_electrons > 1.0;
   const double ip = interior(c->g);
-  if (poisson) {
+  const bool direct = mj_direct(c);
+  if (poisson && direct) {
+    for (int m = 0; m < c->n_atoms; ++m) {
+      if ((float)c->atoms[m].Z == 0.f) continue;
+      LAUNCH(RQ_KC_POISSON, 128 * ip,
+             launch_mj_direct_domain((float*)c->U[c->cu], c->lab[c->cl], c->Pother, m,
+                                     c->pdirect + (size_t)m * c->g.S3, c->sic, c->rho, c->g, p.h2, p.two_pi, c->st));
+    }
+  } else if (poisson) {
     for (int js = 0; js < f.jacobi_per_step; ++js) {
       LAUNCH(RQ_KC_POISSON, 12 * ip,
              launch_mj_jacobi((float*)c->P[c->cp], (float*)c->P[1 - c->cp], (float*)c->U[c->cu], c->g, p.h2, p.two_pi,
@@ -151,10 +175,10 @@ int mj_step_one(rq_ctx* c, int s) {
     // frame tail: Pother <- P_buf[0], the self-interaction correction on its frames (the frame
     // counter is the reference's frameCount, incremented before the level-set passes), then the
     // level-set passes on the same psi
-    if (poisson)
-      CK(cudaMemcpyAsync(c->Pother, c->P[c->cp], (size_t)c->g.S3 * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
-    else
+    if (!poisson)
       CK(cudaMemsetAsync(c->Pother, 0, (size_t)c->g.S3 * sizeof(float), c->st));
+    else if (!direct)  // the direct path builds Pother every step
+      CK(cudaMemcpyAsync(c->Pother, c->P[c->cp], (size_t)c->g.S3 * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
     const int sic = mj_sic_interval(c);
     if (poisson && sic > 0 && c->frame > 0 && c->frame % sic == 0) {
       for (int m = 0; m < c->n_atoms; ++m) {
@@ -279,7 +303,8 @@ int mj_forces(rq_ctx* c, int method, double* F) {
   if (method == RQ_FORCE_GRADP) {
     const int R = std::max(5, (int)std::lround(3.0 / c->h));  // FORCE_RADIUS (molecule.js:1198)
     LAUNCH(RQ_KC_FORCES, 4.0 * n * (2 * R + 1) * (2 * R + 1) * (2 * R + 1),
-           launch_mj_gradp((float*)c->P[c->cp], atoms_dev(c), n, c->g, p.inv_h, R, c->dF, c->st));
+           launch_mj_gradp(mj_direct(c) ? c->Pother : (float*)c->P[c->cp], atoms_dev(c), n, c->g, p.inv_h, R, c->dF,
+                           c->st));  // molecule.js:2703: Pother on the direct path
   } else if (method == RQ_FORCE_HF || method == RQ_FORCE_ADJOINT) {
     // molecule.js:1271-1330: Z_A = Z (or Z_nuc for bare nuclei), integer positions, h^2 softening
     std::vector<float> a5((size_t)n * 5);

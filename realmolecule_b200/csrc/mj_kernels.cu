@@ -301,6 +301,47 @@ __global__ void k_mj_sub_self(const float* __restrict__ Pm, float* __restrict__ 
   if ((label[id] & kMjMask) == m) Pother[id] = F_SUB(Pother[id], F_MUL(Pm[id], frac));
 }
 
+// computeRhoOther (molecule.js:593-612): psi^2 except where the label is m (interior points)
+__global__ void k_mj_rho_other(const float* __restrict__ U, const int* __restrict__ label, int m,
+                               float* __restrict__ rho, Geo g) {
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, k;
+  if (id >= g.S3 || !interior_of(id, g, i, j, k)) return;
+  const float u = U[id];
+  rho[id] = ((label[id] & kMjMask) == m) ? 0.0f : F_MUL(u, u);
+}
+
+// copyPotherForLabel (molecule.js:651-671): Pother = Psrc where the label is m
+__global__ void k_mj_copy_for_label(const float* __restrict__ Psrc, float* __restrict__ Pother,
+                                    const int* __restrict__ label, int m, Geo g) {
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, k;
+  if (id >= g.S3 || !interior_of(id, g, i, j, k)) return;
+  if ((label[id] & kMjMask) == m) Pother[id] = Psrc[id];
+}
+
+// initPdirect (molecule.js:614-649): P_m = sum over charged n != m of 0.5 / sqrt(r^2 + h^2) (f32,
+// truncated integer positions), and Pother += P_m, on interior points
+__global__ void k_mj_init_pdirect(const MjAtom* __restrict__ atoms, int nAt, int m, float* __restrict__ Pm,
+                                  float* __restrict__ Pother, Geo g, float h, float h2) {
+  const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, k;
+  if (id >= g.S3 || !interior_of(id, g, i, j, k)) return;
+  const float xi = F_MUL((float)i, h), yj = F_MUL((float)j, h), zk = F_MUL((float)k, h);
+  float val = 0.0f;
+  for (int n = 0; n < nAt; ++n) {
+    const MjAtom a = atoms[n];
+    if (a.Z <= 0.0f || n == m) continue;
+    const float dx = F_SUB(xi, F_MUL((float)a.posI, h));
+    const float dy = F_SUB(yj, F_MUL((float)a.posJ, h));
+    const float dz = F_SUB(zk, F_MUL((float)a.posK, h));
+    const float r = F_SQRT(F_ADD(F_ADD(F_ADD(F_MUL(dx, dx), F_MUL(dy, dy)), F_MUL(dz, dz)), h2));
+    val = F_ADD(val, F_DIV(0.5f, r));
+  }
+  Pm[id] = val;
+  Pother[id] = F_ADD(Pother[id], val);
+}
+
 __global__ void k_mj_residual(const float* __restrict__ Pin, float* __restrict__ R, const float* __restrict__ rho, Geo g,
                               float inv_h2, float two_pi) {
   const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -615,6 +656,25 @@ cudaError_t launch_mj_vcycle(float* P, const float* U, float* rho, float* resid,
                              const Geo& g, const Geo& gc, float h2, float inv_h2, float two_pi, cudaStream_t st) {
   k_mj_rho<<<flat_blocks(g.S3), 256, 0, st>>>(U, rho, g);
   return mj_vcycle_core(P, rho, resid, Ec0, Ec1, fc, g, gc, h2, inv_h2, two_pi, st);
+}
+
+cudaError_t launch_mj_direct_init(const MjAtom* atoms, int nAt, int m, float* Pm, float* Pother, const Geo& g, float h,
+                                  float h2, cudaStream_t st) {
+  k_mj_init_pdirect<<<flat_blocks(g.S3), 256, 0, st>>>(atoms, nAt, m, Pm, Pother, g, h, h2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mj_direct_domain(const float* U, const int* label, float* Pother, int m, float* Pm, float* scratch,
+                                    float* rho, const Geo& g, float h2, float two_pi, cudaStream_t st) {
+  // molecule.js:2835-2857 for one domain: the density of every other domain, 10 Jacobi sweeps of
+  // the persistent P_m (P_m <-> scratch, ending in P_m), then Pother = P_m on the domain
+  if (g.NN < 2) return cudaSuccess;
+  k_mj_rho_other<<<flat_blocks(g.S3), 256, 0, st>>>(U, label, m, rho, g);
+  for (int js = 0; js < 10; ++js)
+    k_mj_jacobi_rho<<<march_grid(g), march_block(), 0, st>>>(js % 2 ? scratch : Pm, js % 2 ? Pm : scratch, rho, g, h2,
+                                                             two_pi);
+  k_mj_copy_for_label<<<flat_blocks(g.S3), 256, 0, st>>>(Pm, Pother, label, m, g);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_mj_sic_domain(const float* U, const int* label, float* Pother, int m, float frac, float* rho,

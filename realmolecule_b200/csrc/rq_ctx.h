@@ -54,6 +54,7 @@ struct rq_ctx {
   float* atoms5 = nullptr;    // [i,j,k,Z,rc] f32 (cloud/solver.py:378-382)
   float* scratch_atoms5 = nullptr;  // per-call atom table for force variants
   float *sic = nullptr, *sic2 = nullptr;  // molecule.js flavour with SIC: self-potential ping-pong
+  float* pdirect = nullptr;   // molecule.js direct path: persistent P_m of every domain (n_atoms x S^3)
   // solver.py flavour: atom bins of the label step's argmax (rebuilt whenever atoms change)
   int bins_nb = 0, bins_bin = 0;
   int *bin_start = nullptr, *bin_idx = nullptr, *bin_far = nullptr;

@@ -26,6 +26,7 @@ int nm_energy(rq_ctx* c, double* out, double* per_domain);
 int nm_forces(rq_ctx* c, int method, double* F);
 int nm_set_atoms(rq_ctx* c);
 int nm_set_external(rq_ctx* c, const double* v);
+bool mj_direct(const rq_ctx* c);      // molecule.js flavour on the direct per-electron Poisson path
 int mj_sic_interval(const rq_ctx* c);  // frames between SIC passes of the molecule.js flavour (0: off)
 int nm_flush(rq_ctx* c);  // materialise a pending per-domain normalisation of psi
 int nm_ready(rq_ctx* c);  // nm_flush, or normalise now when updates ran since the last normalisation

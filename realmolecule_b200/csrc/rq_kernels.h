@@ -68,6 +68,12 @@ cudaError_t launch_mj_jacobi(const float* Pin, float* Pout, const float* U, cons
                              cudaStream_t st);
 cudaError_t launch_mj_vcycle(float* P, const float* U, float* rho, float* resid, float* Ec0, float* Ec1, float* fc,
                              const Geo& g, const Geo& gc, float h2, float inv_h2, float two_pi, cudaStream_t st);
+// the direct per-electron Poisson of small systems (molecule.js:2833-2858, :614-671): P_m init and
+// one step's solve for domain m (Pm persistent; rho, scratch are scratch)
+cudaError_t launch_mj_direct_init(const MjAtom* atoms, int nAt, int m, float* Pm, float* Pother, const Geo& g, float h,
+                                  float h2, cudaStream_t st);
+cudaError_t launch_mj_direct_domain(const float* U, const int* label, float* Pother, int m, float* Pm, float* scratch,
+                                    float* rho, const Geo& g, float h2, float two_pi, cudaStream_t st);
 // the self-interaction correction of one domain m (molecule.js:3018-3075); rho, sic, sic2, resid,
 // Ec0, Ec1 and fc are scratch
 cudaError_t launch_mj_sic_domain(const float* U, const int* label, float* Pother, int m, float frac, float* rho,

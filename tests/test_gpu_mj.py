@@ -167,9 +167,31 @@ def test_frames_with_self_interaction_correction_bit_exact(kind, frames):
     np.testing.assert_allclose(e[L.E_EE], ref.energy()[2], rtol=1e-9)  # V_ee reads the corrected Pother
 
 
-def test_self_interaction_correction_needs_more_than_five_domains():
+@pytest.mark.parametrize("kind", ["water", "bare"])
+def test_direct_per_electron_poisson_bit_exact(kind):
+    """cfg.sic with NELEC <= 5: the reference's direct path -- a persistent P_m per domain,
+    initialised to sum_{n != m} 0.5/r and relaxed by 10 Jacobi sweeps on the density of the other
+    domains every step, copied into Pother on domain m -- bit for bit with the oracle, and the
+    gradP force reads that Pother."""
     from realmolecule_b200 import Context, _lib as L
-    NN, screen, rows = atoms_case("water")
-    with pytest.raises(L.RqError) as e:
-        Context(NN, screen, rows, flavor="molecule.js", sic=1)
-    assert e.value.status == L.RQ_ENOTSUP
+    opts = dict(steps_per_frame=7, norm_interval=5, vcycle_interval=3)
+    NN, screen, rows = atoms_case(kind)
+    ref = orc.MoleculeJsDriver(NN, screen, rows, sic=True, **opts)
+    ref.initialize()
+    assert ref.direct
+    ctx = Context(NN, screen, rows, flavor="molecule.js", sic=1, **opts)
+    ctx.initialize()
+    ctx.upload(psi=ref.U, label=ref.label.astype(np.int32))
+    nsteps = 2 * 7 + 3
+    for _ in range(nsteps):
+        ref.step()
+    ctx.step(nsteps)
+    st = ctx.download(psi=True, label=True, W=True)
+    assert np.array_equal(st["label"], ref.label.astype(np.int32))
+    assert np.array_equal(st["W"].view(np.uint32), ref.W.view(np.uint32))
+    assert np.array_equal(st["psi"].view(np.uint32), ref.U.view(np.uint32))
+    np.testing.assert_allclose(ctx.energy()[L.E_EE], ref.energy()[2], rtol=1e-9)
+    R = max(5, round(3.0 / ref.hd))
+    Fo = np.zeros(ref.nA * 3)
+    orc.O().mj_force_gradP(ref.Pother, orc.C.addressof(ref.atoms), ref.nA, ref.S, np.float32(1 / ref.hd), R, Fo)
+    np.testing.assert_allclose(ctx.forces(L.FORCE_GRADP).reshape(-1), Fo, rtol=1e-9, atol=1e-12)
