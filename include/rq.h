@@ -237,6 +237,39 @@ RQ_API int rq_batch_info(const rq_batch* b, int32_t* n_inst, int64_t* total_poin
                          int64_t* kernel_launches);
 RQ_API int rq_batch_synchronize(rq_batch* b);
 
+/* ---- atom.js per-shell solver (atom.js:1-346) ----------------------------------------------
+ * Replaces atom.js's module state and physicsStep(): one U (density amplitude), W (front) and P
+ * (Hartree potential of the other shells) field per electron shell on an S^3 grid (S = NN+1)
+ * centred on one nucleus of charge Z_kernel.  The in-place lexicographic sweep of the reference
+ * runs as a hyperplane wavefront, so every f32 store is the reference's; only the FP64 sums of
+ * the normalisation and the energies are summed in another order. */
+typedef struct rq_shells rq_shells;
+typedef struct rq_shells_config {
+  int32_t NN;       /* USER_NN (even) */
+  int32_t poisson;  /* USER_POISSON: 0 'multigrid' (default), 1 'simultaneous' */
+  double screen;    /* USER_SCREEN, box edge in bohr */
+  double Z_kernel;  /* USER_Z_KERNEL */
+  double d;         /* USER_D: dt = d h^2 */
+  int32_t reserved[4];
+} rq_shells_config;
+typedef struct rq_shell {  /* one entry of USER_SHELLS */
+  double ne, Rmax, Zeff;   /* Rmax 0: screen/2 for shells after the first */
+  int32_t split;           /* 1: split 'halfspace' */
+  int32_t half_index;      /* halfIndex of a half-space shell */
+  int32_t outer_half;      /* outerHalf */
+  int32_t fixed_w;         /* fixedW: the front of this shell does not move */
+} rq_shell;
+/* at most 8 shells; the initial state (atom.js:55-125) is built at creation */
+RQ_API int rq_shells_create(const rq_shells_config* cfg, const rq_shell* shells, int32_t n_shells, rq_shells** out);
+RQ_API void rq_shells_destroy(rq_shells* s);
+RQ_API const char* rq_shells_last_error(const rq_shells* s);
+/* n physicsStep() calls (atom.js:212-343).  E (4 or NULL) = {E, E_T, E_eK, E_ee} of the last one;
+ * per_shell (n_shells x 5 or NULL) = {ET_m, Eee_m, EeK_m, nrm_m, eig_m}.  Synchronises. */
+RQ_API int rq_shells_step(rq_shells* s, int32_t n, double* E, double* per_shell);
+RQ_API int rq_shells_download(rq_shells* s, int32_t shell, float* U, float* W, float* P);
+RQ_API int rq_shells_upload(rq_shells* s, int32_t shell, const float* U, const float* W, const float* P);
+RQ_API int rq_shells_info(const rq_shells* s, int64_t* kernel_launches);
+
 /* ---- single kernels on caller-owned device memory (zero-copy PyTorch interop) ---------------
  * Pointers are device pointers of S^3 elements; `stream` is a cudaStream_t or NULL.  These run
  * exactly the kernels rq_step uses and exist for kernel-level parity checks and custom drivers. */

@@ -116,6 +116,8 @@ class _Oracle:
             "orc_nm_force": [_f64p, _f64p, _f64p, _i, _i, _d, _d, _f64p],
             "orc_nm_init": [_f64p, _i32p, _f32p, _i32p, _i, _i, _f],
             "orc_nm_evolve": [_i32p, _i32p, _f64p, _f32p, _i, _d, _d],
+            "orc_at_init": [_f32p, _f32p, _f32p, _f32p, C.c_void_p, _i, _i, _d, _d],
+            "orc_at_step": [_f32p, _f32p, _f32p, _f32p, C.c_void_p, _i, _i, _d, _d, _i, _f64p, _f64p],
         }
         for name, argt in sig.items():
             fn = getattr(L, name)
@@ -626,3 +628,50 @@ class NewMethodDriver:
         F = np.zeros(self.n * 3)
         O().nm_force(self.U, xyz, Z, self.n, self.S, self.h, self.sigma, F)
         return F.reshape(-1, 3)
+
+
+class Shell(C.Structure):
+    _fields_ = [("ne", C.c_double), ("Rmax", C.c_double), ("Zeff", C.c_double), ("split", C.c_int32),
+                ("half_index", C.c_int32), ("outer_half", C.c_int32), ("fixed_w", C.c_int32)]
+
+
+def shell_array(shells):
+    """shells: dicts in atom.js's USER_SHELLS idiom (ne, Rmax, Zeff[, split='halfspace', halfIndex,
+    outerHalf, fixedW])."""
+    arr = (Shell * len(shells))()
+    for q, sh in enumerate(shells):
+        arr[q].ne = sh.get("ne", 1)
+        arr[q].Rmax = sh.get("Rmax", 0.0) or 0.0
+        arr[q].Zeff = sh["Zeff"]
+        arr[q].split = 1 if sh.get("split") == "halfspace" else 0
+        arr[q].half_index = int(sh.get("halfIndex", 0))
+        arr[q].outer_half = int(bool(sh.get("outerHalf", False)))
+        arr[q].fixed_w = int(bool(sh.get("fixedW", False)))
+    return arr
+
+
+class AtomShellsDriver:
+    """Sequential restatement of atom.js (init :55-125, physicsStep :212-343, the multigrid
+    Poisson :127-210) with JS semantics: f64 arithmetic, f32 array stores, lexicographic
+    in-place loops."""
+
+    def __init__(self, NN, screen, Z_kernel, shells, d=0.1, poisson="multigrid"):
+        self.NN, self.S = NN, NN + 1
+        self.S3 = self.S ** 3
+        self.screen, self.Zk, self.d = float(screen), float(Z_kernel), float(d)
+        self.shells = shell_array(shells)
+        self.nS = len(shells)
+        self.simultaneous = 1 if poisson == "simultaneous" else 0
+        n = self.nS * self.S3
+        self.U, self.W, self.P = (np.zeros(n, np.float32) for _ in range(3))
+        self.K = np.zeros(self.S3, np.float32)
+
+    def initialize(self):
+        O().at_init(self.U, self.W, self.P, self.K, C.addressof(self.shells), self.nS, self.NN, self.screen, self.Zk)
+
+    def step(self):
+        E4 = np.zeros(4)
+        ps = np.zeros(4 * self.nS)
+        O().at_step(self.U, self.W, self.P, self.K, C.addressof(self.shells), self.nS, self.NN, self.screen, self.d,
+                    self.simultaneous, E4, ps)
+        return E4, ps.reshape(self.nS, 4)

@@ -1122,3 +1122,221 @@ void orc_nm_evolve(const int32_t* labelIn, int32_t* labelOut, const double* U, f
         labelOut[id] = newL;
       }
 }
+
+/* ====================================================================
+ * atom.js flavour: per-shell fields U[m], W[m], P[m] (atom.js:1-346).  JS numbers are f64 and
+ * every Float32Array store rounds to f32; loops run in the reference's lexicographic in-place
+ * order.  Fields are nShells consecutive S^3 blocks.
+ * ==================================================================== */
+
+typedef struct {
+  double ne, Rmax, Zeff;                    /* shellConfig[m].ne / .Rmax / .Zeff */
+  int32_t split, half_index, outer_half, fixed_w;  /* 'halfspace', .halfIndex, .outerHalf, .fixedW */
+} orc_shell;
+
+/* atom.js:55-125: K, U, W, P on all S^3 points, then each U normalised over all points. */
+void orc_at_init(float* U, float* W, float* P, float* K, const orc_shell* sh, int nS, int NN, double scr,
+                 double Zk) {
+  const int S = NN + 1;
+  const int64_t S3 = (int64_t)S * S * S;
+  const double h = scr / NN, h2 = h * h, h3 = h * h * h;
+  const int N2 = NN / 2;
+  double Rmin[16], Rmax[16];
+  Rmin[0] = 0; Rmax[0] = sh[0].Rmax;
+  for (int m = 1; m < nS; ++m) { Rmin[m] = sh[m - 1].Rmax; Rmax[m] = sh[m].Rmax ? sh[m].Rmax : scr / 2; }
+  memset(U, 0, sizeof(float) * S3 * nS);
+  memset(W, 0, sizeof(float) * S3 * nS);
+  for (int i = 0; i <= NN; ++i)
+    for (int j = 0; j <= NN; ++j)
+      for (int k = 0; k <= NN; ++k) {
+        const int64_t id = IDX(i, j, k, S);
+        const double r2 = (double)((i - N2) * (i - N2)) * h2 + (double)((j - N2) * (j - N2)) * h2 +
+                          (double)((k - N2) * (k - N2)) * h2 + 0.12 * h2;
+        const double r = sqrt(r2);
+        K[id] = (float)(Zk / r);
+        for (int m = 0; m < nS; ++m) {
+          float* Um = U + m * S3; float* Wm = W + m * S3;
+          int in;
+          if (sh[m].split) {
+            if (i == N2) { in = 1; Wm[id] = 0.5f; }
+            else in = sh[m].half_index == 0 ? (i < N2) : (i > N2);
+          } else if (sh[m].outer_half) {
+            in = r >= Rmin[m] && r < Rmax[m] && i > N2;
+          } else {
+            in = r >= Rmin[m] && r < Rmax[m];
+          }
+          if (in) {
+            Um[id] = (float)exp(-sh[m].Zeff * r);
+            double w = 1.0;
+            const double smoothW = 2 * h;
+            if (!sh[m].split) {
+              if (Rmin[m] > 0) { const double din = r - Rmin[m]; if (din < smoothW) w = fmin(w, din / smoothW); }
+              const double dout = Rmax[m] - r;
+              if (dout < smoothW) w = fmin(w, dout / smoothW);
+            }
+            w = fmax(0.01, w);
+            if (Wm[id] == 0) Wm[id] = (float)w;
+          }
+        }
+        for (int m = 0; m < nS; ++m) P[m * S3 + id] = (float)(0.5 / r);
+      }
+  for (int m = 0; m < nS; ++m) {
+    float* Um = U + m * S3;
+    double n2 = 0;
+    for (int64_t id = 0; id < S3; ++id) n2 += (double)Um[id] * Um[id] * h3;
+    const double sc = 1 / sqrt(n2);
+    for (int64_t id = 0; id < S3; ++id) Um[id] = (float)(Um[id] * sc);
+  }
+}
+
+/* atom.js:127-138 in-place lexicographic Jacobi-labelled (Gauss-Seidel) sweeps */
+static void at_gs(float* P, const float* rhs, int N, double h2, int nIter) {
+  const int S = N + 1;
+  const int64_t S2 = (int64_t)S * S;
+  for (int it = 0; it < nIter; ++it)
+    for (int i = 1; i < N; ++i)
+      for (int j = 1; j < N; ++j)
+        for (int k = 1; k < N; ++k) {
+          const int64_t id = i * S2 + (int64_t)j * S + k;
+          P[id] = (float)(((double)P[id + S2] + P[id - S2] + P[id + S] + P[id - S] + P[id + 1] + P[id - 1] +
+                           h2 * rhs[id]) / 6);
+        }
+}
+
+/* atom.js:186-210 poissonVcycle: 4 sweeps, residual, injection to N/2, 20 coarse sweeps from 0,
+   injection-add prolongation, 4 sweeps. */
+void orc_at_vcycle(float* P, const float* rhs, int N, double h) {
+  const int S = N + 1, Nc = N / 2, Sc = Nc + 1;
+  const int64_t S2 = (int64_t)S * S, S3 = S2 * S, Sc2 = (int64_t)Sc * Sc;
+  const double h2 = h * h;
+  at_gs(P, rhs, N, h2, 4);
+  float* res = (float*)calloc(S3, sizeof(float));
+  for (int i = 1; i < N; ++i)
+    for (int j = 1; j < N; ++j)
+      for (int k = 1; k < N; ++k) {
+        const int64_t id = i * S2 + (int64_t)j * S + k;
+        const double lap = ((double)P[id + S2] + P[id - S2] + P[id + S] + P[id - S] + P[id + 1] + P[id - 1] -
+                            6 * (double)P[id]) / h2;
+        res[id] = (float)(rhs[id] + lap);
+      }
+  float* cd = (float*)calloc(Sc2 * Sc, sizeof(float));
+  for (int i = 1; i < Nc; ++i)
+    for (int j = 1; j < Nc; ++j)
+      for (int k = 1; k < Nc; ++k) cd[i * Sc2 + (int64_t)j * Sc + k] = res[(2 * i) * S2 + (int64_t)(2 * j) * S + 2 * k];
+  const double hc = h * 2, hc2 = hc * hc;
+  float* Pc = (float*)calloc(Sc2 * Sc, sizeof(float));
+  at_gs(Pc, cd, Nc, hc2, 20);
+  for (int i = 1; i < Nc; ++i)
+    for (int j = 1; j < Nc; ++j)
+      for (int k = 1; k < Nc; ++k) {
+        const double val = Pc[i * Sc2 + (int64_t)j * Sc + k];
+        for (int di = 0; di <= 1; ++di)
+          for (int dj = 0; dj <= 1; ++dj)
+            for (int dk = 0; dk <= 1; ++dk) {
+              const int fi = 2 * i + di, fj = 2 * j + dj, fk = 2 * k + dk;
+              if (fi > 0 && fi < N && fj > 0 && fj < N && fk > 0 && fk < N) {
+                const int64_t f = fi * S2 + (int64_t)fj * S + fk;
+                P[f] = (float)(P[f] + val);
+              }
+            }
+      }
+  at_gs(P, rhs, N, h2, 4);
+  free(res); free(cd); free(Pc);
+}
+
+/* atom.js:212-343 physicsStep.  E4 = {E, E_T, E_eK, E_ee}; per_shell (nS x 4) = {ET, Eee, EeK, nrm}. */
+void orc_at_step(float* U, float* W, float* P, const float* K, const orc_shell* sh, int nS, int NN, double scr,
+                 double d, int simultaneous, double* E4, double* per_shell) {
+  const int S = NN + 1;
+  const int64_t S2 = (int64_t)S * S, S3 = S2 * S;
+  const double h = scr / NN, h2 = h * h, h3 = h * h * h, dt = d * h2, PI = 3.141592653589793;
+  float c[16];
+  double ET = 0, Eee = 0, EeK = 0;
+  for (int q = 0; q < 4 * nS; ++q) per_shell[q] = 0;
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        const int64_t id = i * S2 + (int64_t)j * S + k;
+        for (int m = 0; m < nS; ++m) {
+          c[m] = 0;
+          for (int n = 0; n < nS; ++n) {
+            if (n != m) c[m] = (float)((double)c[m] - U[n * S3 + id]);
+            c[m] = (float)(0.5 * ((double)c[m] + U[m * S3 + id]));
+          }
+        }
+        const int64_t ip = id + S2, im = id - S2, jp = id + S, jm = id - S, kp = id + 1, km = id - 1;
+        for (int m = 0; m < nS; ++m) {
+          float* Um = U + m * S3; float* Wm = W + m * S3; float* Pm = P + m * S3;
+          if (!sh[m].fixed_w) {
+            const double lapW = ((double)Wm[ip] + Wm[im] + Wm[jp] + Wm[jm] + Wm[kp] + Wm[km] - 6 * (double)Wm[id]) / h2;
+            const double gwx = ((double)Wm[ip] - Wm[im]) / h, gwy = ((double)Wm[jp] - Wm[jm]) / h,
+                         gwz = ((double)Wm[kp] - Wm[km]) / h;
+            const double gradW = sqrt(gwx * gwx + gwy * gwy + gwz * gwz);
+            Wm[id] = (float)(Wm[id] + (2 * dt * fabs((double)c[m]) * lapW + 9 * dt * (double)c[m] * gradW));
+          }
+          const double wlap =
+              0.5 * d * (((double)Um[ip] - Um[id]) * ((double)Wm[ip] + Wm[id]) * 0.5 -
+                         ((double)Um[id] - Um[im]) * ((double)Wm[id] + Wm[im]) * 0.5) +
+              0.5 * d * (((double)Um[jp] - Um[id]) * ((double)Wm[jp] + Wm[id]) * 0.5 -
+                         ((double)Um[id] - Um[jm]) * ((double)Wm[id] + Wm[jm]) * 0.5) +
+              0.5 * d * (((double)Um[kp] - Um[id]) * ((double)Wm[kp] + Wm[id]) * 0.5 -
+                         ((double)Um[id] - Um[km]) * ((double)Wm[id] + Wm[km]) * 0.5);
+          Um[id] = (float)(Um[id] + (wlap + dt * ((double)K[id] - 2 * (double)Pm[id]) * Um[id] * Wm[id]));
+          int dominated = 1;
+          for (int n = 0; n < nS; ++n)
+            if (n != m && W[n * S3 + id] >= Wm[id]) { dominated = 0; break; }
+          if (dominated && Wm[id] > 0.01) {
+            int dip = 1, djp = 1, dkp = 1;
+            for (int n = 0; n < nS; ++n)
+              if (n != m) {
+                if (W[n * S3 + ip] >= Wm[ip]) dip = 0;
+                if (W[n * S3 + jp] >= Wm[jp]) djp = 0;
+                if (W[n * S3 + kp] >= Wm[kp]) dkp = 0;
+              }
+            const double gx = dip ? (double)Um[ip] - Um[id] : 0, gy = djp ? (double)Um[jp] - Um[id] : 0,
+                         gz = dkp ? (double)Um[kp] - Um[id] : 0;
+            const double tm = 0.5 * (gx * gx + gy * gy + gz * gz) * h;
+            const double eem = (double)Pm[id] * Um[id] * Um[id] * h3;
+            const double ekm = -(double)K[id] * Um[id] * Um[id] * h3;
+            ET += tm; Eee += eem; EeK += ekm;
+            per_shell[4 * m] += tm; per_shell[4 * m + 1] += eem; per_shell[4 * m + 2] += ekm;
+            per_shell[4 * m + 3] += (double)Um[id] * Um[id] * h3;
+          }
+          if (simultaneous) {
+            double rhoOther = 0;
+            for (int n = 0; n < nS; ++n)
+              if (n != m) rhoOther += (double)U[n * S3 + id] * U[n * S3 + id] * W[n * S3 + id];
+            const double lapP = ((double)Pm[ip] + Pm[im] + Pm[jp] + Pm[jm] + Pm[kp] + Pm[km] - 6 * (double)Pm[id]) / h2;
+            Pm[id] = (float)(Pm[id] + (dt * lapP + 2 * PI * dt * rhoOther));
+          }
+        }
+      }
+  if (!simultaneous) {
+    float* rhs = (float*)calloc(S3, sizeof(float));
+    for (int m = 0; m < nS; ++m) {
+      for (int i = 1; i < NN; ++i)
+        for (int j = 1; j < NN; ++j)
+          for (int k = 1; k < NN; ++k) {
+            const int64_t id = i * S2 + (int64_t)j * S + k;
+            double rhoOther = 0;
+            for (int n = 0; n < nS; ++n)
+              if (n != m) rhoOther += (double)U[n * S3 + id] * U[n * S3 + id] * W[n * S3 + id];
+            rhs[id] = (float)(2 * PI * rhoOther);
+          }
+      orc_at_vcycle(P + m * S3, rhs, NN, h);
+    }
+    free(rhs);
+  }
+  for (int m = 0; m < nS; ++m) {
+    float* Um = U + m * S3;
+    double n2 = 0;
+    for (int i = 1; i < NN; ++i)
+      for (int j = 1; j < NN; ++j)
+        for (int k = 1; k < NN; ++k) { const double u = Um[IDX(i, j, k, S)]; n2 += u * u * h3; }
+    const double sc = 1 / sqrt(n2);
+    for (int i = 1; i < NN; ++i)
+      for (int j = 1; j < NN; ++j)
+        for (int k = 1; k < NN; ++k) { const int64_t id = IDX(i, j, k, S); Um[id] = (float)(Um[id] * sc); }
+  }
+  E4[0] = ET + EeK + Eee; E4[1] = ET; E4[2] = EeK; E4[3] = Eee;
+}

@@ -28,6 +28,16 @@ class RqError(RuntimeError):
         super().__init__(f"{where}: status {status} ({status_string(status)}){': ' + detail if detail else ''}")
 
 
+class ShellsConfig(C.Structure):
+    _fields_ = [("NN", C.c_int32), ("poisson", C.c_int32), ("screen", C.c_double), ("Z_kernel", C.c_double),
+                ("d", C.c_double), ("reserved", C.c_int32 * 4)]
+
+
+class Shell(C.Structure):
+    _fields_ = [("ne", C.c_double), ("Rmax", C.c_double), ("Zeff", C.c_double), ("split", C.c_int32),
+                ("half_index", C.c_int32), ("outer_half", C.c_int32), ("fixed_w", C.c_int32)]
+
+
 class Config(C.Structure):
     _fields_ = [("NN", C.c_int32), ("flavor", C.c_int32), ("precision", C.c_int32), ("norm_interval", C.c_int32),
                 ("screen", C.c_double), ("dv", C.c_double), ("poisson_interval", C.c_int32),
@@ -99,6 +109,13 @@ SIGNATURES = {
     "rq_batch_info": (C.c_int, [_V, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                 C.POINTER(C.c_int64)]),
     "rq_batch_synchronize": (C.c_int, [_V]),
+    "rq_shells_create": (C.c_int, [_P, _P, _I, _P]),
+    "rq_shells_destroy": (None, [_V]),
+    "rq_shells_last_error": (C.c_char_p, [_V]),
+    "rq_shells_step": (C.c_int, [_V, _I, _P, _P]),
+    "rq_shells_download": (C.c_int, [_V, _I, _P, _P, _P]),
+    "rq_shells_upload": (C.c_int, [_V, _I, _P, _P, _P]),
+    "rq_shells_info": (C.c_int, [_V, _P]),
     "rq_kernel_update_sp": (C.c_int, [_P, _P, _P, _P, _P, _I, _F, _F, _V]),
     "rq_kernel_jacobi_sp": (C.c_int, [_P, _P, _P, _I, _F, _F, _V]),
     "rq_kernel_labels_sp": (C.c_int, [_P, _P, _P, _I, _I, _F, _F, _V]),

@@ -329,6 +329,8 @@ static int sp_poisson(rq_ctx* c) {
 // the step before it whenever that step does not normalise (so psi does not change in between).
 // That early sweep writes P[1-cp] and leaves cp alone (sp_jdone = 1): every readout still sees
 // the P of the last completed Poisson step, and the next Poisson step adopts the buffer.
+constexpr int kLabelScanAtoms = 64;  // up to this many atoms the label step scans them all
+
 static int sp_step_one(rq_ctx* c, int s) {
   const rq_config& f = c->cfg;
   const bool poisson = s % f.poisson_interval == 0, norm = s % f.norm_interval == 0;
@@ -377,10 +379,16 @@ static int sp_step_one(rq_ctx* c, int s) {
   }
   if (norm && (rc = sp_normalize(c, false)) != RQ_OK) return rc;
   if (s % f.label_interval == 0 && (f.label_until <= 0 || s <= f.label_until)) {
-    LAUNCH(RQ_KC_LABELS, 8 * interior_points(c->g),
-           launch_labels_binned_sp(c->lab[c->cl], c->lab[1 - c->cl], c->atoms5, c->n_atoms,
-                                   AtomBins{c->bins_nb, c->bins_bin, c->bin_start, c->bin_idx, c->bin_far, c->bin_zmax},
-                                   c->g, (float)c->h, (float)c->h2, c->st));
+    // a few atoms: the scan is cheaper than the bin search (same result)
+    if (c->n_atoms <= kLabelScanAtoms)
+      LAUNCH(RQ_KC_LABELS, 8 * interior_points(c->g),
+             launch_labels_sp(c->lab[c->cl], c->lab[1 - c->cl], c->atoms5, c->n_atoms, c->g, (float)c->h,
+                              (float)c->h2, c->st));
+    else
+      LAUNCH(RQ_KC_LABELS, 8 * interior_points(c->g),
+             launch_labels_binned_sp(c->lab[c->cl], c->lab[1 - c->cl], c->atoms5, c->n_atoms,
+                                     AtomBins{c->bins_nb, c->bins_bin, c->bin_start, c->bin_idx, c->bin_far, c->bin_zmax},
+                                     c->g, (float)c->h, (float)c->h2, c->st));
     c->cl ^= 1;
   }
   return RQ_OK;
