@@ -166,12 +166,16 @@ __global__ void k_at_rhs(const float* __restrict__ U, const float* __restrict__ 
 }
 
 // launch tau of `iters` pipelined in-place Gauss-Seidel sweeps (atom.js:127-138): sweep s works
-// on plane tau - 2 s
+// on plane tau - 2 s; thread (s, i, j) takes that sweep's cell of its (i, j) column
 __global__ void __launch_bounds__(256) k_at_gs(float* __restrict__ P, const float* __restrict__ rhs, AtGeo g, double h2,
                                                int tau, int iters) {
-  for (int s = 0; s < iters; ++s) {
-    int i, j, k;
-    if (!at_plane_cell(g, tau - 2 * s, i, j, k)) continue;
+  const int n = g.N - 1;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n * n * iters) return;
+  const int s = q / (n * n), c = q % (n * n);
+  const int i = 1 + c / n, j = 1 + c % n, k = tau - 2 * s - i - j;
+  if (k < 1 || k >= g.N) return;
+  {
     const long long id = (long long)i * g.S2 + (long long)j * g.S + k;
     const double s6 = __dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn((double)P[id + g.S2], (double)P[id - g.S2]),
                                                                 (double)P[id + g.S]), (double)P[id - g.S]),
@@ -280,7 +284,7 @@ static unsigned blocks_for(long long n) { return (unsigned)((n + 255) / 256); }
 
 // pipelined Gauss-Seidel: `iters` in-place sweeps of P on grid g in one wavefront
 static int at_smooth(rq_shells* s, float* P, const float* rhs, const AtGeo& g, double h2, int iters) {
-  const unsigned b = blocks_for((long long)(g.N - 1) * (g.N - 1));
+  const unsigned b = blocks_for((long long)(g.N - 1) * (g.N - 1) * iters);
   for (int tau = 3; tau <= 3 * (g.N - 1) + 2 * (iters - 1); ++tau) {
     k_at_gs<<<b, 256, 0, s->st>>>(P, rhs, g, h2, tau, iters);
     SLAUNCH();
