@@ -296,6 +296,7 @@ def run_ours(a):
 
     ctx.close()
     conv = None if a.no_converge else converge_leg(stream, dist, rank, world)
+    callers = None if a.no_converge or rank != 0 else caller_legs(a)
 
     if rank == 0:
         peak, peak_kind = measured_peak()
@@ -335,6 +336,7 @@ def run_ours(a):
                         for k, v in prof.items()},
             "cpu_baseline": cpu,
             "converge": conv,
+            "callers": callers,
             "clocks": clk.summary(),
             "gpu_launches": launches,
         }
@@ -367,6 +369,55 @@ def _max_over_ranks(dist, x):
     t = torch.tensor([x], device="cuda", dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def caller_legs(a):
+    """The other reference callers of the step, timed through their drop-ins (rank 0, context only):
+    the recorded hairpin job of cloud/run_hairpin.py through RealQMSolver (its A100 time per step is
+    in cloud/hairpin_results.json) and atom.js's physicsStep on the He page (atom_He.html) against
+    the sequential restatement on one host core."""
+    import torch
+    from realmolecule_b200 import RealQMSolver
+    from realmolecule_b200.shells import AtomShells
+    out = {}
+    with open(os.path.join(ROOT, "tests", "golden", "hairpin_config.json")) as f:
+        cfg = json.load(f)
+    with open(os.path.join(ROOT, "tests", "golden", "hairpin_golden.json")) as f:
+        gold = json.load(f)
+    s = RealQMSolver(cfg)
+    s.set_fold_atoms(cfg["fold_atoms"])
+    s.initialize()
+    s.run(total_steps=100, report_interval=100)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.run(total_steps=1000, report_interval=1000)
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) / 1000 * 1e3
+    out["hairpin"] = {"atoms": len(cfg["atoms"]), "grid": f"{cfg['gridN']}^3", "steps": 1000,
+                      "ms_per_step": ms, "recorded_a100_ms_per_step": gold["snapshots"][-1]["ms_per_step"],
+                      "timing": "host wall clock around RealQMSolver.run (dynamics on, forces every 500 steps)"}
+    he = [{"ne": 1, "Rmax": 5.0, "Zeff": 2, "split": "halfspace", "halfIndex": 0, "fixedW": True},
+          {"ne": 1, "Rmax": 5.0, "Zeff": 2, "split": "halfspace", "halfIndex": 1, "fixedW": True}]
+    sh = AtomShells(100, 5.0, 2, he, d=0.15)
+    sh.step(2)
+    t0 = time.perf_counter()
+    sh.step(100)
+    gpu_ms = (time.perf_counter() - t0) / 100 * 1e3
+    sh.close()
+    cpu_ms = None
+    if not a.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        o = orc.AtomShellsDriver(100, 5.0, 2, he, d=0.15)
+        o.initialize()
+        t0 = time.perf_counter()
+        o.step()
+        o.step()
+        cpu_ms = (time.perf_counter() - t0) / 2 * 1e3
+    out["atom_js_he"] = {"grid": "100^3", "shells": 2, "ms_per_step": gpu_ms,
+                         "cpu_sequential_ms_per_step": cpu_ms, "cpu_cores": 1,
+                         "cpu": "the oracle's sequential restatement of atom.js (2 steps)"}
+    return out
 
 
 def converge_leg(stream, dist, rank, world):
