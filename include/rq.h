@@ -270,6 +270,66 @@ RQ_API int rq_shells_download(rq_shells* s, int32_t shell, float* U, float* W, f
 RQ_API int rq_shells_upload(rq_shells* s, int32_t shell, const float* U, const float* W, const float* P);
 RQ_API int rq_shells_info(const rq_shells* s, int64_t* kernel_launches);
 
+/* ---- mol_fast.js multi-field solver (mol_fast.js:1-1651) ------------------------------------
+ * Replaces mol_fast.js's GPU state and doSteps()/computeForces(): one U (density amplitude),
+ * W (front) and P (Hartree potential of its own density) field per electron, one electron per
+ * nucleus (at most 16), all electrons advanced by one fused pass per step (competition front,
+ * weighted Laplacian, Hartree of the others, Poisson), the reference's f32 tree reductions for
+ * the norms and energies, normalisation every 20 steps and at the end of a frame, and the
+ * two-level Poisson correction of every electron every vcycle_interval steps of a frame.  The
+ * f32 arithmetic follows the shaders' operation order (no contraction). */
+typedef struct rq_mf rq_mf;
+typedef struct rq_mf_config {
+  int32_t NN;                 /* USER_NN (even) */
+  int32_t shell_mode;         /* USER_SHELL_MODE: rc / r_out / angular split per orbital */
+  int32_t vcycle;             /* USER_VCYCLE !== false */
+  int32_t vcycle_interval;    /* USER_VCYCLE_INTERVAL (50) */
+  int32_t coarse_iters;       /* USER_COARSE_ITERS (10) */
+  int32_t r_out_release_step; /* USER_R_OUT_RELEASE_STEP; < 0: never */
+  int32_t full_self;          /* USER_FULL_SELF */
+  int32_t reserved0;
+  double screen;              /* USER_SCREEN, box edge in bohr (15) */
+  double kinetic_coeff;       /* USER_KINETIC_COEFF (0.5) */
+  double kc_multi;            /* USER_KC_MULTI (1) */
+  double beta_pauli;          /* USER_BETA_PAULI (0) */
+  double field_x;             /* USER_FIELD_X (0) */
+  double alpha_tf;            /* USER_ALPHA_TF (0) */
+  double line_j_offset;       /* USER_LINE_J_OFFSET (0) */
+  int32_t reserved[8];
+} rq_mf_config;
+typedef struct rq_mf_nucleus {  /* one entry of USER_NUCLEI plus its USER_NORM_TARGETS value */
+  double i, j, k;               /* grid coordinates */
+  double Z, rc, r_out, tilt_y, tilt_x, hs;
+  double z_init;                /* initial decay rate (the page's default: Z > 0 ? Z : 1) */
+  double norm_target;           /* occupation (1) */
+  double split_axis[3];         /* raw axis, normalised by the library */
+  int32_t split;                /* 0 sphere, 2 hemi, 3 third, 4 tetra, 5 hemi_third */
+  int32_t split_idx;
+  int32_t split_fix;            /* 1: enforce the split every step */
+  int32_t reserved;
+} rq_mf_nucleus;
+/* the initial state of uploadInitialData (mol_fast.js:941-1046) is built at creation */
+RQ_API int rq_mf_create(const rq_mf_config* cfg, const rq_mf_nucleus* nuclei, int32_t n, rq_mf** out);
+RQ_API void rq_mf_destroy(rq_mf* s);
+RQ_API const char* rq_mf_last_error(const rq_mf* s);
+/* doSteps(n) (mol_fast.js:1237-1322) without its host epilogue: the f32 sums of the frame's last
+ * reduction into sums (n_electrons + 6 or NULL: norm^2 per electron, T, V_eK, V_ee, dipole x,y,z).
+ * Synchronises. */
+RQ_API int rq_mf_step(rq_mf* s, int32_t n, float* sums);
+/* the force shader (mol_fast.js:500-563): 2 Z <grad sum_m P_m> per nucleus into F (3n, f32). */
+RQ_API int rq_mf_forces(rq_mf* s, float* F);
+/* moved nuclei (stepNuclei, mol_fast.js:1375-1410): grid positions (3n doubles), the f32 copy in
+ * the parameters and K rebuilt on the device (recomputeK_WGSL, :565-587). */
+RQ_API int rq_mf_set_positions(rq_mf* s, const double* ijk);
+/* the slice of extractWGSL (mol_fast.js:595-640) as a headless buffer of 3 n S^2 floats. */
+RQ_API int rq_mf_extract(rq_mf* s, float* out);
+/* fields of electron m (S^3 each, NULL = skip); an upload writes both buffer sets, as
+ * uploadInitialData (:1039-1044) does, so the next frame reads the uploaded boundary too */
+RQ_API int rq_mf_download(rq_mf* s, int32_t m, float* U, float* W, float* P);
+RQ_API int rq_mf_upload(rq_mf* s, int32_t m, const float* U, const float* W, const float* P);
+RQ_API int rq_mf_download_K(rq_mf* s, float* K);
+RQ_API int rq_mf_info(const rq_mf* s, int64_t* kernel_launches, int64_t* steps_done);
+
 /* ---- single kernels on caller-owned device memory (zero-copy PyTorch interop) ---------------
  * Pointers are device pointers of S^3 elements; `stream` is a cudaStream_t or NULL.  These run
  * exactly the kernels rq_step uses and exist for kernel-level parity checks and custom drivers. */

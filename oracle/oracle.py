@@ -118,6 +118,14 @@ class _Oracle:
             "orc_nm_evolve": [_i32p, _i32p, _f64p, _f32p, _i, _d, _d],
             "orc_at_init": [_f32p, _f32p, _f32p, _f32p, C.c_void_p, _i, _i, _d, _d],
             "orc_at_step": [_f32p, _f32p, _f32p, _f32p, C.c_void_p, _i, _i, _d, _d, _i, _f64p, _f64p],
+            "orc_mf_update": [C.c_void_p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p],
+            "orc_mf_reduce": [C.c_void_p, _f32p, _f32p, _f32p, _f32p, _f32p],
+            "orc_mf_normalize": [C.c_void_p, _f32p, _f32p],
+            "orc_mf_vcycle": [C.c_void_p, _f32p, _f32p, _i, _i],
+            "orc_mf_force": [C.c_void_p, _f32p, _f32p],
+            "orc_mf_recompute_k": [C.c_void_p, _f32p],
+            "orc_mf_extract": [C.c_void_p, _f32p, _f32p, _f32p, _f32p],
+            "orc_mf_init": [_i, _d, _i, _f64p, _f32p, _f32p, _f32p, _f32p],
         }
         for name, argt in sig.items():
             fn = getattr(L, name)
@@ -675,3 +683,209 @@ class AtomShellsDriver:
         O().at_step(self.U, self.W, self.P, self.K, C.addressof(self.shells), self.nS, self.NN, self.screen, self.d,
                     self.simultaneous, E4, ps)
         return E4, ps.reshape(self.nS, 4)
+
+
+# ---- mol_fast.js (mol_fast.js:1-1651) ----------------------------------------------------------
+
+class MfParams(C.Structure):
+    """The uniform P of mol_fast.js (writeParams, :838-874) plus its templated shader constants."""
+    _fields_ = [("NN", C.c_int32), ("S", C.c_int32), ("N2", C.c_int32), ("n", C.c_int32), ("shell_mode", C.c_int32),
+                ("pad0", C.c_int32), ("h", C.c_float), ("h2", C.c_float), ("inv_h", C.c_float), ("inv_h2", C.c_float),
+                ("dt", C.c_float), ("half_d", C.c_float), ("h3", C.c_float), ("two_pi", C.c_float),
+                ("R_out", C.c_float), ("field_x", C.c_float), ("alpha_tf", C.c_float), ("full_self", C.c_float),
+                ("kc", C.c_float), ("kc_multi", C.c_float), ("beta", C.c_float), ("pad1", C.c_float),
+                ("atoms", (C.c_float * 4) * 16), ("rcs", (C.c_float * 4) * 16), ("r_out", C.c_float * 16),
+                ("split_type", C.c_int32 * 16), ("split_idx", C.c_int32 * 16), ("split_fix", C.c_int32 * 16),
+                ("split_group", C.c_int32 * 16), ("ax", (C.c_float * 4) * 16)]
+
+
+_MF_SPLIT = {"sphere": 0, "hemi": 2, "third": 3, "tetra": 4, "hemi_third": 5}
+
+
+def _fixed6(v: float) -> float:
+    """A number as the shader text carries it (toFixed(6)), then the literal's f32 value."""
+    return float(np.float32(float(f"{v:.6f}")))
+
+
+class MolFastDriver:
+    """mol_fast.js restated on the CPU: the page's nucleus defaults (:28-40), the templated
+    constants (:108-132), writeParams (:838-874), uploadInitialData (:941-1046), doSteps
+    (:1237-1322), computeEKK (:1326-1337), computeForces (:1339-1373) and stepNuclei
+    (:1375-1410), over the C restatement of the shaders (orc_mf_*)."""
+
+    def __init__(self, nuclei, NN=200, screen=15.0, norm_targets=None, shell_mode=False, vcycle=True,
+                 vcycle_interval=50, coarse_iters=10, kinetic_coeff=0.5, kc_multi=1.0, beta_pauli=0.0,
+                 field_x=0.0, alpha_tf=0.0, full_self=False, r_out_release_step=None, line_j_offset=0.0,
+                 dt_nuc=2.0, nuc_damping=0.9, force_scale=1.0, mass=None):
+        self.nuclei = []
+        for n in nuclei:
+            Z = n["Z"]
+            self.nuclei.append({
+                "i": n["i"], "j": n["j"], "k": n["k"], "Z": Z, "rc": n.get("rc") or 0, "r_out": n.get("r_out") or 0,
+                "tilt_y": n.get("tilt_y") or 0, "tilt_x": n.get("tilt_x") or 0, "hs": n.get("hs") or 0,
+                "fixed": n.get("fixed") is True,
+                "z_init": n["z_init"] if n.get("z_init") is not None else (Z if Z > 0 else 1),
+                "split": n.get("split") or "sphere", "split_idx": n.get("split_idx") or 0,
+                "split_axis": list(n.get("split_axis") or [1, 0, 0]),
+                "split_fix": n["split_fix"] if n.get("split_fix") is not None else True})
+        self.n = len(self.nuclei)
+        self.NN, self.S = NN, NN + 1
+        self.S3 = self.S ** 3
+        self.N2 = round(NN / 2)
+        self.hv = screen / NN
+        self.h2v = self.hv * self.hv
+        self.h3v = self.hv * self.hv * self.hv
+        self.screen = screen
+        self.tg = list(norm_targets) if norm_targets is not None else [1] * self.n
+        self.vcycle, self.vi, self.ci = vcycle, vcycle_interval, coarse_iters
+        self.release = r_out_release_step
+        self.r_out_enforce = True
+        self.dt_nuc, self.damp, self.fscale = dt_nuc, nuc_damping, force_scale
+        self.mass = list(mass) if mass is not None else [max(1, a["Z"]) * 1836 for a in self.nuclei]
+        self.vel = [[0.0, 0.0, 0.0] for _ in range(self.n)]
+        self.force = [[0.0, 0.0, 0.0] for _ in range(self.n)]
+        self.tStep = 0
+        p = self.p = MfParams()
+        p.NN, p.S, p.N2, p.n, p.shell_mode = NN, self.S, self.N2, self.n, 1 if shell_mode else 0
+        f = lambda v: float(np.float32(v))
+        p.h, p.h2, p.inv_h, p.inv_h2 = f(self.hv), f(self.h2v), f(1 / self.hv), f(1 / self.h2v)
+        p.dt, p.half_d, p.h3, p.two_pi = f(0.12 * self.h2v), f(kinetic_coeff * 0.12), f(self.h3v), f(2 * math.pi)
+        p.field_x, p.alpha_tf, p.full_self = f(field_x), f(alpha_tf), 1.0 if full_self else 0.0
+        p.kc, p.kc_multi, p.beta = _fixed6(kinetic_coeff), _fixed6(kc_multi), _fixed6(beta_pauli)
+        for a, nu in enumerate(self.nuclei):
+            p.rcs[a][0], p.rcs[a][1], p.rcs[a][2], p.rcs[a][3] = nu["rc"], self.tg[a], nu["tilt_x"], nu["tilt_y"]
+            p.r_out[a] = _fixed6(nu["r_out"])
+            p.split_type[a] = _MF_SPLIT.get(nu["split"], 0)
+            p.split_idx[a] = int(nu["split_idx"])
+            p.split_fix[a] = 1 if nu["split_fix"] else 0
+            v = nu["split_axis"]
+            Lv = math.hypot(v[0], v[1], v[2]) or 1
+            p.ax[a][0], p.ax[a][1], p.ax[a][2] = (_fixed6(v[0] / Lv), _fixed6(v[1] / Lv), _fixed6(v[2] / Lv))
+            g = a
+            if nu["split"] and nu["split"] != "sphere":
+                for b in range(a):
+                    o = self.nuclei[b]
+                    if (o["split"] == nu["split"] and o["i"] == nu["i"] and o["j"] == nu["j"]
+                            and o["k"] == nu["k"]):
+                        g = b
+                        break
+            p.split_group[a] = g
+        p.rcs[15][2] = line_j_offset
+        self._write_atoms()
+        nS = self.n * self.S3
+        self.U = [np.zeros(nS, np.float32) for _ in range(2)]
+        self.W = [np.zeros(nS, np.float32) for _ in range(2)]
+        self.P = [np.zeros(nS, np.float32) for _ in range(2)]
+        self.K = np.zeros(self.S3, np.float32)
+        self.cur = 0
+        self.sums = np.zeros(self.n + 6, np.float32)
+        self.computeEKK()
+
+    def _write_atoms(self):
+        p = self.p
+        p.R_out = 1.0 if self.r_out_enforce else 0.0
+        for a, nu in enumerate(self.nuclei):
+            p.atoms[a][0], p.atoms[a][1], p.atoms[a][2], p.atoms[a][3] = nu["i"], nu["j"], nu["k"], nu["Z"]
+
+    @property
+    def pp(self):
+        return C.addressof(self.p)
+
+    def initialize(self):
+        rec = np.zeros((self.n, 16))
+        for a, nu in enumerate(self.nuclei):
+            ax = nu["split_axis"]
+            rec[a, :14] = [nu["i"], nu["j"], nu["k"], nu["Z"], nu["rc"], nu["r_out"], nu["hs"], nu["z_init"],
+                           self.tg[a], _MF_SPLIT.get(nu["split"], 0), nu["split_idx"], ax[0], ax[1], ax[2]]
+        O().mf_init(self.NN, self.screen, self.n, np.ascontiguousarray(rec.reshape(-1)), self.K, self.U[0], self.W[0],
+                    self.P[0])
+        for X in (self.U, self.W, self.P):
+            X[1][:] = X[0]
+        self.cur = 0
+
+    def computeEKK(self):
+        E = 0.0
+        nu = self.nuclei
+        for a in range(self.n):
+            for b in range(a + 1, self.n):
+                dx, dy, dz = ((nu[a][c] - nu[b][c]) * self.hv for c in "ijk")
+                r = math.sqrt(dx * dx + dy * dy + dz * dz)
+                if r > 0:
+                    E += nu[a]["Z"] * nu[b]["Z"] / r
+        self.E_KK = E
+
+    def do_steps(self, n):
+        if self.release is not None and self.r_out_enforce and self.tStep >= self.release:
+            self.r_out_enforce = False
+            self._write_atoms()
+        o = O()
+        for s in range(n):
+            c, nx = self.cur, 1 - self.cur
+            o.mf_update(self.pp, self.U[c], self.W[c], self.P[c], self.K, self.U[nx], self.W[nx], self.P[nx])
+            if (s + 1) % 20 == 0 or s == n - 1:
+                o.mf_reduce(self.pp, self.U[nx], self.W[nx], self.P[nx], self.K, self.sums)
+                o.mf_normalize(self.pp, self.U[nx], self.sums)
+            if self.vcycle and (s + 1) % self.vi == 0:
+                for m in range(self.n):
+                    o.mf_vcycle(self.pp, self.U[nx], self.P[nx], m, self.ci)
+            self.cur = nx
+        ne, sm = self.n, self.sums
+        self.E_T, self.E_eK, self.E_ee = float(sm[ne]), float(sm[ne + 1]), float(sm[ne + 2])
+        self.E = self.E_T + self.E_eK + self.E_ee + self.E_KK
+        dn = [0.0, 0.0, 0.0]
+        for a in self.nuclei:
+            dn[0] += a["Z"] * (a["i"] - self.N2) * self.hv
+            dn[1] += a["Z"] * (a["j"] - self.N2) * self.hv
+            dn[2] += a["Z"] * (a["k"] - self.N2) * self.hv
+        self.dipole = [dn[0] + float(sm[ne + 3]), dn[1] + float(sm[ne + 4]), dn[2] + float(sm[ne + 5])]
+        self.tStep += n
+
+    def compute_forces(self):
+        fd = np.zeros(3 * self.n, np.float32)
+        O().mf_force(self.pp, self.P[self.cur], fd)
+        nu = self.nuclei
+        for a in range(self.n):
+            f = [float(fd[3 * a]), float(fd[3 * a + 1]), float(fd[3 * a + 2])]
+            for b in range(self.n):
+                if b == a:
+                    continue
+                dx, dy, dz = ((nu[a][c] - nu[b][c]) * self.hv for c in "ijk")
+                r2 = dx * dx + dy * dy + dz * dz + self.h2v
+                inv_r3 = 1 / (r2 * math.sqrt(r2))
+                pref = nu[a]["Z"] * nu[b]["Z"] * inv_r3
+                f[0] += pref * dx
+                f[1] += pref * dy
+                f[2] += pref * dz
+            self.force[a] = f
+        return fd
+
+    def step_nuclei(self):
+        moved = False
+        for a, nu in enumerate(self.nuclei):
+            if nu["Z"] <= 0 or nu["fixed"]:
+                continue
+            v = self.vel[a]
+            for d in range(3):
+                v[d] = self.damp * (v[d] + self.dt_nuc * self.fscale * self.force[a][d] / self.mass[a])
+            di, dj, dk = (v[0] * self.dt_nuc) / self.hv, (v[1] * self.dt_nuc) / self.hv, (v[2] * self.dt_nuc) / self.hv
+            if abs(di) > 0.0001 or abs(dj) > 0.0001 or abs(dk) > 0.0001:
+                nu["i"] += di
+                nu["j"] += dj
+                nu["k"] += dk
+                moved = True
+        if moved:
+            self._write_atoms()
+            self.computeEKK()
+            O().mf_recompute_k(self.pp, self.K)
+        return moved
+
+    def extract(self):
+        out = np.zeros(3 * self.n * self.S * self.S, np.float32)
+        c = self.cur
+        O().mf_extract(self.pp, self.U[c], self.W[c], self.P[c], out)
+        return out
+
+    def fields(self, m):
+        c, S3 = self.cur, self.S3
+        return {"U": self.U[c][m * S3:(m + 1) * S3], "W": self.W[c][m * S3:(m + 1) * S3],
+                "P": self.P[c][m * S3:(m + 1) * S3]}

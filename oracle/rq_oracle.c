@@ -1340,3 +1340,539 @@ void orc_at_step(float* U, float* W, float* P, const float* K, const orc_shell* 
   }
   E4[0] = ET + EeK + Eee; E4[1] = ET; E4[2] = EeK; E4[3] = Eee;
 }
+
+/* ======================================================================
+ * mol_fast.js multi-field solver (mol_fast.js:1-1651), f32 WGSL semantics
+ *
+ * One U, W, P field per electron (one electron per nucleus), field m at offset m*S3.
+ * Every function follows the shader it names in the reference's operation order, with
+ * plain IEEE single operations (no contraction); the reductions repeat the shaders'
+ * workgroup trees exactly, so the f32 sums are the reference's bit for bit.
+ * ==================================================================== */
+
+#define MF_MAX 16
+typedef struct {
+  int32_t NN, S, N2, n, shell_mode, pad0;
+  float h, h2, inv_h, inv_h2, dt, half_d, h3, two_pi;
+  float R_out, field_x, alpha_tf, full_self;
+  float kc, kc_multi, beta, pad1;
+  float atoms[MF_MAX][4]; /* i, j, k, Z */
+  float rcs[MF_MAX][4];   /* rc, norm target, tilt_x, tilt_y */
+  float r_out[MF_MAX];
+  int32_t split_type[MF_MAX], split_idx[MF_MAX], split_fix[MF_MAX], split_group[MF_MAX];
+  float ax[MF_MAX][4];
+} orc_mf_params;
+
+/* pow and atan2: the f64 functions rounded once to f32 (WGSL leaves their accuracy to the
+ * implementation; the CUDA side does the same) */
+static inline float mf_pow(float x, float y) { return (float)pow((double)x, (double)y); }
+static inline float mf_atan2(float y, float x) { return (float)atan2((double)y, (double)x); }
+
+/* the smooth rc cusp t^2 (3 - 2t) on w (mol_fast.js:188-193, :255-260) */
+static inline float mf_cusp(float r, float rc, float h) {
+  const float edge = rc - 3.0f * h;
+  const float t = fminf(fmaxf((r - edge) / (rc - edge), 0.0f), 1.0f);
+  return t * t * (3.0f - 2.0f * t);
+}
+
+static inline float mf_dot3(const float* a, float x, float y, float z) { return a[0] * x + a[1] * y + a[2] * z; }
+
+/* the three-sector index around axis ax (mol_fast.js:206-216) */
+static inline uint32_t mf_third_sector(const float* ax, float x, float y, float z) {
+  const float dotA = mf_dot3(ax, x, y, z);
+  const float px = x - dotA * ax[0], py = y - dotA * ax[1], pz = z - dotA * ax[2];
+  float e1[3];
+  if (fabsf(ax[2]) < 0.9f) { e1[0] = ax[1]; e1[1] = -ax[0]; e1[2] = 0.0f; }
+  else { e1[0] = 0.0f; e1[1] = ax[2]; e1[2] = -ax[1]; }
+  const float L = sqrtf(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
+  e1[0] = e1[0] / L; e1[1] = e1[1] / L; e1[2] = e1[2] / L;
+  const float e2[3] = {ax[1] * e1[2] - ax[2] * e1[1], ax[2] * e1[0] - ax[0] * e1[2], ax[0] * e1[1] - ax[1] * e1[0]};
+  float theta = mf_atan2(mf_dot3(e2, px, py, pz), mf_dot3(e1, px, py, pz)) - 0.0f;
+  if (theta < -3.141592653589793f) theta = theta + 6.283185307179586f;
+  if (theta > 3.141592653589793f) theta = theta - 6.283185307179586f;
+  return ((uint32_t)floorf((theta + 3.141592653589793f) / 2.094395102393195f)) % 3u;
+}
+
+/* the angular split enforcement of SHELL_MODE (mol_fast.js:196-246); rel in grid cells */
+static inline int mf_in_sector(const orc_mf_params* p, int m, float x, float y, float z, float r_m) {
+  const int t = p->split_type[m];
+  const uint32_t sidx = (uint32_t)p->split_idx[m];
+  const float* ax = p->ax[m];
+  if (t == 2) {
+    const float d = mf_dot3(ax, x, y, z);
+    return sidx == 0 ? d < 0.0f : d >= 0.0f;
+  }
+  if (t == 3) return mf_third_sector(ax, x, y, z) == sidx;
+  if (t == 4) {
+    if (r_m > 1e-6f) {
+      const float ux = x / r_m, uy = y / r_m, uz = z / r_m;
+      uint32_t best = 0;
+      float bestD = 1.0f * ux + 1.0f * uy + 1.0f * uz;
+      const float d1 = 1.0f * ux + -1.0f * uy + -1.0f * uz;
+      if (d1 > bestD) { bestD = d1; best = 1; }
+      const float d2 = -1.0f * ux + 1.0f * uy + -1.0f * uz;
+      if (d2 > bestD) { bestD = d2; best = 2; }
+      const float d3 = -1.0f * ux + -1.0f * uy + 1.0f * uz;
+      if (d3 > bestD) { bestD = d3; best = 3; }
+      return best == sidx;
+    }
+    return 1;
+  }
+  if (t == 5) {
+    const float d = mf_dot3(ax, x, y, z);
+    if (sidx == 0) return d >= 0.0f;
+    if (d >= 0.0f) return 0;
+    return mf_third_sector(ax, x, y, z) == sidx - 1u;
+  }
+  return 1;
+}
+
+/* updateWGSL (mol_fast.js:134-351): front w, amplitude u and potential P of every electron,
+ * reading the old buffers (Ui, Wi, Pi) and writing the new ones at the interior cells. */
+void orc_mf_update(const orc_mf_params* p, const float* Ui, const float* Wi, const float* Pi, const float* K,
+                   float* Uo, float* Wo, float* Po) {
+  const int NN = p->NN, S = p->S, n = p->n;
+  const int64_t S2 = (int64_t)S * S, S3 = S2 * S;
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        const int64_t id = i * S2 + (int64_t)j * S + k;
+        for (int m = 0; m < n; ++m) {
+          const int64_t o = m * S3;
+          const float uc = Ui[o + id];
+          float umax = 0.0f;
+          for (int q = 0; q < n; ++q) {
+            if (q == m) continue;
+            const float un = Ui[q * S3 + id];
+            if (un > umax) umax = un;
+          }
+          const float cm = uc - umax;
+          const float wc = Wi[o + id];
+          const float wip = Wi[o + id + S2], wim = Wi[o + id - S2];
+          const float wjp = Wi[o + id + S], wjm = Wi[o + id - S];
+          const float wkp = Wi[o + id + 1], wkm = Wi[o + id - 1];
+          const float lw = (wip + wim + wjp + wjm + wkp + wkm - 6.0f * wc) * p->inv_h2;
+          const float gx = (wip - wim) * p->inv_h, gy = (wjp - wjm) * p->inv_h, gz = (wkp - wkm) * p->inv_h;
+          float nw = wc + 0.05f * p->dt * fabsf(cm) * lw + 1.0f * p->dt * cm * sqrtf(gx * gx + gy * gy + gz * gz);
+          nw = fminf(fmaxf(nw, 0.0f), 1.0f);
+          if (p->shell_mode) {
+            const float rc_m = p->rcs[m][0];
+            const float ro_m = p->r_out[m] * p->R_out;
+            const float dxm = (float)i - p->atoms[m][0], dym = (float)j - p->atoms[m][1], dzm = (float)k - p->atoms[m][2];
+            const float r_m = sqrtf(dxm * dxm + dym * dym + dzm * dzm) * p->h;
+            if (rc_m > 0.0f && r_m < rc_m) nw = fminf(nw, mf_cusp(r_m, rc_m, p->h));
+            if (ro_m > 0.0f && r_m > ro_m) nw = (r_m <= ro_m + p->h) ? nw : 0.0f;
+            if (p->split_type[m] != 0 && p->split_fix[m] == 1 && !mf_in_sector(p, m, dxm, dym, dzm, r_m)) nw = 0.0f;
+          } else {
+            for (int a = 0; a < n; ++a) {
+              const float dx = (float)i - p->atoms[a][0], dy = (float)j - p->atoms[a][1], dz = (float)k - p->atoms[a][2];
+              const float r = sqrtf(dx * dx + dy * dy + dz * dz) * p->h;
+              const float rc_a = p->rcs[a][0];
+              if (rc_a > 0.0f && r < rc_a) nw = fminf(nw, mf_cusp(r, rc_a, p->h));
+            }
+          }
+          Wo[o + id] = nw;
+          float Ptot = 0.0f, Pgrp = 0.0f;
+          for (int q = 0; q < n; ++q) {
+            const float Pn = Pi[q * S3 + id];
+            Ptot += Pn;
+            if (p->split_group[q] == p->split_group[m]) Pgrp += Pn;
+          }
+          const float selfN = p->rcs[m][1];
+          const float fm_multi = p->full_self > 0.5f ? 0.0f : 1.0f / selfN;
+          const float fm = selfN > 1.0f ? fm_multi : 1.0f;
+          const float Vother = 2.0f * (Ptot - fm * Pgrp);
+          const float rho_m = uc * uc;
+          const float V_TF = (selfN > 1.0f && p->alpha_tf > 0.0f) ? p->alpha_tf * mf_pow(fmaxf(rho_m, 1e-20f), 0.6666667f) : 0.0f;
+          const float tilt_y = p->rcs[m][3], tilt_x = p->rcs[m][2];
+          const float x_au = ((float)i - (float)p->N2) * p->h;
+          const float y_au = ((float)j - (float)p->N2) * p->h;
+          const float V_tilt = -tilt_x * x_au - tilt_y * y_au;
+          float rho_other = 0.0f;
+          for (int q = 0; q < n; ++q) {
+            if (q == m) continue;
+            const float un = Ui[q * S3 + id];
+            rho_other += un * un;
+          }
+          const float V_Pauli = p->beta * rho_other;
+          const float uip = Ui[o + id + S2], uim = Ui[o + id - S2];
+          const float ujp = Ui[o + id + S], ujm = Ui[o + id - S];
+          const float ukp = Ui[o + id + 1], ukm = Ui[o + id - 1];
+          const float k_mult = selfN > 1.0f ? p->kc_multi : 1.0f;
+          const float hd = p->half_d * k_mult;
+          Uo[o + id] = uc + hd * ((uip - uc) * (wip + nw) * 0.5f - (uc - uim) * (nw + wim) * 0.5f) +
+                       hd * ((ujp - uc) * (wjp + nw) * 0.5f - (uc - ujm) * (nw + wjm) * 0.5f) +
+                       hd * ((ukp - uc) * (wkp + nw) * 0.5f - (uc - ukm) * (nw + wkm) * 0.5f) +
+                       p->dt * (K[id] - Vother - V_TF - V_tilt - V_Pauli - p->field_x * x_au) * uc * wc;
+          const float Pc = Pi[o + id];
+          Po[o + id] = Pc +
+                       p->dt * (Pi[o + id + S2] + Pi[o + id - S2] + Pi[o + id + S] + Pi[o + id - S] + Pi[o + id + 1] +
+                                Pi[o + id - 1] - 6.0f * Pc) * p->inv_h2 +
+                       p->two_pi * p->dt * uc * uc;
+        }
+      }
+}
+
+/* reduceWGSL + finalizeWGSL (mol_fast.js:353-472): per-cell f32 terms, 128-cell workgroups over
+ * the interior in linear order, the shared-memory trees, and the single finalize workgroup.
+ * sums: n norms^2, T, V_eK, V_ee, dipole x, y, z. */
+void orc_mf_reduce(const orc_mf_params* p, const float* U, const float* W, const float* Pv, const float* K,
+                   float* sums) {
+  const int NN = p->NN, S = p->S, n = p->n, NR = n + 6;
+  const int64_t S2 = (int64_t)S * S, S3 = S2 * S;
+  const int64_t NM = NN - 1, tot = NM * NM * NM;
+  const int64_t nwg = (tot + 127) / 128;
+  float* part = (float*)calloc((size_t)(nwg * NR), sizeof(float));
+#pragma omp parallel for schedule(static)
+  for (int64_t wg = 0; wg < nwg; ++wg) {
+    float sn[128 * (MF_MAX + 6)];
+    for (int q = 0; q < 128 * NR; ++q) sn[q] = 0.0f;
+    for (int lid = 0; lid < 128; ++lid) {
+      const int64_t cell = wg * 128 + lid;
+      if (cell >= tot) continue;
+      const int k = (int)(cell % NM) + 1, j = (int)((cell / NM) % NM) + 1, i = (int)(cell / (NM * NM)) + 1;
+      const int64_t id = i * S2 + (int64_t)j * S + k;
+      float T = 0.0f, VeK = 0.0f, Vee = 0.0f, dx = 0.0f, dy = 0.0f, dz = 0.0f;
+      const float xc = ((float)i - (float)p->N2) * p->h;
+      const float yc = ((float)j - (float)p->N2) * p->h;
+      const float zc = ((float)k - (float)p->N2) * p->h;
+      float Ptot = 0.0f;
+      for (int q = 0; q < n; ++q) Ptot += Pv[q * S3 + id];
+      for (int m = 0; m < n; ++m) {
+        const int64_t o = m * S3;
+        const float v = U[o + id];
+        sn[lid * NR + m] = v * v * p->h3;
+        if (W[o + id] > 0.1f) {
+          const float a = U[o + id + S2] - v, b = U[o + id + S] - v, c = U[o + id + 1] - v;
+          const float kmt = p->rcs[m][1] > 1.0f ? p->kc_multi : 1.0f;
+          T += kmt * p->kc * (a * a + b * b + c * c) * p->h;
+        }
+        VeK -= K[id] * v * v * p->h3;
+        const float rho_cell = v * v * p->h3;
+        dx -= rho_cell * xc;
+        dy -= rho_cell * yc;
+        dz -= rho_cell * zc;
+        const float selfN = p->rcs[m][1];
+        const float fm = selfN > 1.0f ? 1.0f / selfN : 1.0f;
+        Vee += (Ptot - fm * Pv[o + id]) * v * v * p->h3;
+        if (selfN > 1.0f && p->alpha_tf > 0.0f) T += 0.6f * p->alpha_tf * mf_pow(fmaxf(v * v, 1e-20f), 1.6666667f) * p->h3;
+        const float tilt = p->rcs[m][3];
+        if (tilt != 0.0f) T += (-tilt) * yc * v * v * p->h3;
+      }
+      sn[lid * NR + n] = T;
+      sn[lid * NR + n + 1] = VeK;
+      sn[lid * NR + n + 2] = Vee;
+      sn[lid * NR + n + 3] = dx;
+      sn[lid * NR + n + 4] = dy;
+      sn[lid * NR + n + 5] = dz;
+    }
+    for (int s = 64; s > 0; s >>= 1)
+      for (int lid = 0; lid < s; ++lid)
+        for (int x = 0; x < NR; ++x) sn[lid * NR + x] += sn[(lid + s) * NR + x];
+    for (int x = 0; x < NR; ++x) part[wg * NR + x] = sn[x];
+  }
+  float* wgs = (float*)calloc((size_t)(128 * NR), sizeof(float));
+  for (int lid = 0; lid < 128; ++lid)
+    for (int64_t q = lid; q < nwg; q += 128)
+      for (int x = 0; x < NR; ++x) wgs[lid * NR + x] += part[q * NR + x];
+  for (int s = 64; s > 0; s >>= 1)
+    for (int lid = 0; lid < s; ++lid)
+      for (int x = 0; x < NR; ++x) wgs[lid * NR + x] += wgs[(lid + s) * NR + x];
+  for (int x = 0; x < NR; ++x) sums[x] = wgs[x];
+  free(wgs);
+  free(part);
+}
+
+/* normalizeWGSL (mol_fast.js:474-492) */
+void orc_mf_normalize(const orc_mf_params* p, float* U, const float* sums) {
+  const int NN = p->NN, S = p->S;
+  const int64_t S2 = (int64_t)S * S, S3 = S2 * S;
+  for (int m = 0; m < p->n; ++m) {
+    const float nrm = sums[m], tgt = p->rcs[m][1];
+    if (!(nrm > 0.0f && tgt > 0.0f)) continue;
+    const float sc = sqrtf(tgt / nrm);
+    for (int i = 1; i < NN; ++i)
+      for (int j = 1; j < NN; ++j)
+        for (int k = 1; k < NN; ++k) U[m * S3 + i * S2 + (int64_t)j * S + k] *= sc;
+  }
+}
+
+/* the per-electron V-cycle of doSteps (mol_fast.js:1262-1289) for electron m: rhoSource,
+ * residualPm, restrict, cleared coarse error, coarse_iters weighted-Jacobi sweeps (ping-pong,
+ * prolongation always reading buffer 0) and prolongCorrectPm (:645-785). */
+void orc_mf_vcycle(const orc_mf_params* p, const float* U, float* P, int m, int coarse_iters) {
+  const int NN = p->NN, S = p->S, NC = NN / 2, SC = NC + 1;
+  const int64_t S2 = (int64_t)S * S, S3 = S2 * S, SC2 = (int64_t)SC * SC, SC3 = SC2 * SC;
+  const float* Um = U + m * S3;
+  float* Pm = P + m * S3;
+  float* rho = (float*)malloc(sizeof(float) * S3);
+  float* res = (float*)calloc((size_t)S3, sizeof(float));
+  float* rhs = (float*)calloc((size_t)SC3, sizeof(float));
+  float* E0 = (float*)calloc((size_t)SC3, sizeof(float));
+  float* E1 = (float*)calloc((size_t)SC3, sizeof(float));
+  for (int64_t id = 0; id < S3; ++id) rho[id] = Um[id] * Um[id];
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        const int64_t id = i * S2 + (int64_t)j * S + k;
+        const float Pc = Pm[id];
+        const float lap = (Pm[id + S2] + Pm[id - S2] + Pm[id + S] + Pm[id - S] + Pm[id + 1] + Pm[id - 1] - 6.0f * Pc) * p->inv_h2;
+        res[id] = -p->two_pi * rho[id] - lap;
+      }
+#define MFF(a, b, c) res[(int64_t)(a) * S2 + (int64_t)(b) * S + (c)]
+  for (int I = 1; I < NC; ++I)
+    for (int J = 1; J < NC; ++J)
+      for (int L = 1; L < NC; ++L) {
+        const int fi = 2 * I, fj = 2 * J, fk = 2 * L;
+        float val = 8.0f * MFF(fi, fj, fk);
+        val += 4.0f * (MFF(fi + 1, fj, fk) + MFF(fi - 1, fj, fk) + MFF(fi, fj + 1, fk) + MFF(fi, fj - 1, fk) +
+                       MFF(fi, fj, fk + 1) + MFF(fi, fj, fk - 1));
+        val += 2.0f * (MFF(fi + 1, fj + 1, fk) + MFF(fi + 1, fj - 1, fk) + MFF(fi - 1, fj + 1, fk) + MFF(fi - 1, fj - 1, fk) +
+                       MFF(fi + 1, fj, fk + 1) + MFF(fi + 1, fj, fk - 1) + MFF(fi - 1, fj, fk + 1) + MFF(fi - 1, fj, fk - 1) +
+                       MFF(fi, fj + 1, fk + 1) + MFF(fi, fj + 1, fk - 1) + MFF(fi, fj - 1, fk + 1) + MFF(fi, fj - 1, fk - 1));
+        val += MFF(fi + 1, fj + 1, fk + 1) + MFF(fi + 1, fj + 1, fk - 1) + MFF(fi + 1, fj - 1, fk + 1) +
+               MFF(fi + 1, fj - 1, fk - 1) + MFF(fi - 1, fj + 1, fk + 1) + MFF(fi - 1, fj + 1, fk - 1) +
+               MFF(fi - 1, fj - 1, fk + 1) + MFF(fi - 1, fj - 1, fk - 1);
+        rhs[I * SC2 + (int64_t)J * SC + L] = val * 0.015625f;
+      }
+#undef MFF
+  const float hc2 = 4.0f * p->h2;
+  for (int cs = 0; cs < coarse_iters; ++cs) {
+    const float* Ein = (cs % 2) ? E1 : E0;
+    float* Eout = (cs % 2) ? E0 : E1;
+    for (int I = 1; I < NC; ++I)
+      for (int J = 1; J < NC; ++J)
+        for (int L = 1; L < NC; ++L) {
+          const int64_t c = I * SC2 + (int64_t)J * SC + L;
+          const float sum = Ein[c + SC2] + Ein[c - SC2] + Ein[c + SC] + Ein[c - SC] + Ein[c + 1] + Ein[c - 1];
+          Eout[c] = 0.3333f * Ein[c] + (sum + hc2 * rhs[c]) / 9.0f;
+        }
+  }
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        const int ci = i / 2, cj = j / 2, ck = k / 2;
+        const int ci1 = ci + (i & 1) < NC ? ci + (i & 1) : NC;
+        const int cj1 = cj + (j & 1) < NC ? cj + (j & 1) : NC;
+        const int ck1 = ck + (k & 1) < NC ? ck + (k & 1) : NC;
+        const float wi = (i & 1) ? 0.5f : 1.0f, wj = (j & 1) ? 0.5f : 1.0f, wk = (k & 1) ? 0.5f : 1.0f;
+        const float wi1 = 1.0f - wi, wj1 = 1.0f - wj, wk1 = 1.0f - wk;
+#define MFE(a, b, c) E0[(int64_t)(a) * SC2 + (int64_t)(b) * SC + (c)]
+        float corr = 0.0f;
+        corr += wi * wj * wk * MFE(ci, cj, ck);
+        corr += wi * wj * wk1 * MFE(ci, cj, ck1);
+        corr += wi * wj1 * wk * MFE(ci, cj1, ck);
+        corr += wi * wj1 * wk1 * MFE(ci, cj1, ck1);
+        corr += wi1 * wj * wk * MFE(ci1, cj, ck);
+        corr += wi1 * wj * wk1 * MFE(ci1, cj, ck1);
+        corr += wi1 * wj1 * wk * MFE(ci1, cj1, ck);
+        corr += wi1 * wj1 * wk1 * MFE(ci1, cj1, ck1);
+#undef MFE
+        Pm[i * S2 + (int64_t)j * S + k] += 0.5f * corr;
+      }
+  free(rho); free(res); free(rhs); free(E0); free(E1);
+}
+
+/* forceWGSL (mol_fast.js:500-563): 2 Z <grad sum_m P_m> over the ball of radius 4 cells */
+void orc_mf_force(const orc_mf_params* p, const float* P, float* F) {
+  const int S = p->S, n = p->n;
+  const int64_t S2 = (int64_t)S * S, S3 = S2 * S;
+  const float inv2h = 0.5f * p->inv_h;
+  for (int a = 0; a < n; ++a) {
+    const float Z = p->atoms[a][3];
+    if (Z <= 0.0f) { F[3 * a] = F[3 * a + 1] = F[3 * a + 2] = 0.0f; continue; }
+    const int ci = (int)p->atoms[a][0], cj = (int)p->atoms[a][1], ck = (int)p->atoms[a][2];
+    float sx = 0.0f, sy = 0.0f, sz = 0.0f, count = 0.0f;
+    for (int di = -4; di <= 4; ++di) {
+      const int ii = ci + di;
+      if (ii < 1 || ii >= S - 1) continue;
+      for (int dj = -4; dj <= 4; ++dj) {
+        const int jj = cj + dj;
+        if (jj < 1 || jj >= S - 1) continue;
+        for (int dk = -4; dk <= 4; ++dk) {
+          const int kk = ck + dk;
+          if (kk < 1 || kk >= S - 1) continue;
+          if ((float)(di * di + dj * dj + dk * dk) > 16.0f) continue;
+          float xp = 0, xm = 0, yp = 0, ym = 0, zp = 0, zm = 0;
+          for (int m = 0; m < n; ++m) {
+            const float* Pm = P + m * S3;
+            xp += Pm[(ii + 1) * S2 + (int64_t)jj * S + kk];
+            xm += Pm[(ii - 1) * S2 + (int64_t)jj * S + kk];
+            yp += Pm[ii * S2 + (int64_t)(jj + 1) * S + kk];
+            ym += Pm[ii * S2 + (int64_t)(jj - 1) * S + kk];
+            zp += Pm[ii * S2 + (int64_t)jj * S + kk + 1];
+            zm += Pm[ii * S2 + (int64_t)jj * S + kk - 1];
+          }
+          sx += (xp - xm) * inv2h;
+          sy += (yp - ym) * inv2h;
+          sz += (zp - zm) * inv2h;
+          count += 1.0f;
+        }
+      }
+    }
+    const float avg = count > 0.0f ? 1.0f / count : 0.0f;
+    F[3 * a] = 2.0f * Z * sx * avg;
+    F[3 * a + 1] = 2.0f * Z * sy * avg;
+    F[3 * a + 2] = 2.0f * Z * sz * avg;
+  }
+}
+
+/* recomputeK_WGSL (mol_fast.js:565-587) */
+void orc_mf_recompute_k(const orc_mf_params* p, float* K) {
+  const int S = p->S;
+  const int64_t S2 = (int64_t)S * S, S3 = S2 * S;
+#pragma omp parallel for schedule(static)
+  for (int64_t id = 0; id < S3; ++id) {
+    const int k = (int)(id % S), j = (int)((id / S) % S), i = (int)(id / S2);
+    float Kv = 0.0f;
+    for (int a = 0; a < p->n; ++a) {
+      const float Z = p->atoms[a][3];
+      if (Z <= 0.0f) continue;
+      const float di = ((float)i - p->atoms[a][0]) * p->h, dj = ((float)j - p->atoms[a][1]) * p->h,
+                  dk = ((float)k - p->atoms[a][2]) * p->h;
+      Kv += Z / sqrtf(di * di + dj * dj + dk * dk + 4.0f * p->h2);
+    }
+    K[id] = Kv;
+  }
+}
+
+/* extractWGSL (mol_fast.js:595-640) into out (3 n S^2 floats, zero-filled by the caller) */
+void orc_mf_extract(const orc_mf_params* p, const float* U, const float* W, const float* Pv, float* out) {
+  const int S = p->S, n = p->n, N2 = p->N2;
+  const int64_t S2 = (int64_t)S * S, S3 = S2 * S, SS = S;
+  for (int i = 0; i <= p->NN; ++i)
+    for (int j = 0; j <= p->NN; ++j)
+      for (int m = 0; m < n; ++m) {
+        const int64_t idx2 = m * S3 + i * S2 + (int64_t)j * S + N2;
+        out[m * SS * SS + i * SS + j] = W[idx2] > 0.1f ? U[idx2] : 0.0f;
+        if (j == 0) {
+          const int64_t line = i * S2 + (int64_t)N2 * S + N2, ml = m * S3 + line;
+          out[n * SS * SS + m * SS + i] = U[ml];
+          out[2 * n * SS * SS + m * SS + i] = W[ml];
+          float Ps = 0.0f;
+          for (int q = 0; q < n; ++q) Ps += Pv[q * S3 + line];
+          if (m == 0) out[n * SS * SS + n * SS + i] = 2.0f * Ps;
+          const float selfN = p->rcs[m][1];
+          float Vp = 0.0f;
+          if (selfN > 1.0f && p->alpha_tf > 0.0f) Vp = p->alpha_tf * mf_pow(fmaxf(U[ml] * U[ml], 1e-20f), 0.6666667f);
+          out[n * SS * SS + (n + 1 + m) * SS + i] = Vp;
+        }
+      }
+}
+
+/* inSplit (mol_fast.js:878-939), JS numbers (f64); the axis is the raw USER_NUCLEI one */
+static int mf_in_split_f64(double dx, double dy, double dz, double r, int split, int idx, const double* axr) {
+  if (split == 0 || split == 1 || r < 1e-6) return 1;
+  double L = sqrt(axr[0] * axr[0] + axr[1] * axr[1] + axr[2] * axr[2]);
+  if (L == 0) L = 1;
+  const double a0 = axr[0] / L, a1 = axr[1] / L, a2 = axr[2] / L;
+  const double PI = 3.141592653589793;
+  if (split == 2) {
+    const double d = dx * a0 + dy * a1 + dz * a2;
+    return idx == 0 ? d < 0 : d >= 0;
+  }
+  if (split == 3 || split == 5) {
+    const double d = dx * a0 + dy * a1 + dz * a2;
+    if (split == 5) {
+      if (idx == 0) return d >= 0;
+      if (d >= 0) return 0;
+    }
+    const double px = dx - d * a0, py = dy - d * a1, pz = dz - d * a2;
+    double e1x, e1y, e1z;
+    if (fabs(a2) < 0.9) { e1x = a1; e1y = -a0; e1z = 0; }
+    else { e1x = 0; e1y = a2; e1z = -a1; }
+    double e1L = sqrt(e1x * e1x + e1y * e1y + e1z * e1z);
+    if (e1L == 0) e1L = 1;
+    e1x /= e1L; e1y /= e1L; e1z /= e1L;
+    const double e2x = a1 * e1z - a2 * e1y, e2y = a2 * e1x - a0 * e1z, e2z = a0 * e1y - a1 * e1x;
+    const double pe1 = px * e1x + py * e1y + pz * e1z, pe2 = px * e2x + py * e2y + pz * e2z;
+    double theta = atan2(pe2, pe1) - 0;
+    if (theta < -PI) theta += 2 * PI;
+    if (theta > PI) theta -= 2 * PI;
+    const int sector = (int)fmod(floor((theta + PI) / (2 * PI / 3)), 3.0);
+    return split == 3 ? sector == idx : sector == idx - 1;
+  }
+  if (split == 4) {
+    static const double vs[4][3] = {{1, 1, 1}, {1, -1, -1}, {-1, 1, -1}, {-1, -1, 1}};
+    const double u0 = dx / r, u1 = dy / r, u2 = dz / r;
+    int best = 0;
+    double bestDot = -INFINITY;
+    for (int v = 0; v < 4; ++v) {
+      const double d = vs[v][0] * u0 + vs[v][1] * u1 + vs[v][2] * u2;
+      if (d > bestDot) { bestDot = d; best = v; }
+    }
+    return best == idx;
+  }
+  return 1;
+}
+
+/* uploadInitialData (mol_fast.js:941-1046) in JS numbers with f32 stores.  nuc: n records of 16
+ * doubles {i, j, k, Z, rc, r_out, hs, z_init, norm_target, split, split_idx, ax0, ax1, ax2, -, -}. */
+void orc_mf_init(int NN, double screen, int n, const double* nuc, float* K, float* U, float* W, float* P) {
+  const int S = NN + 1;
+  const int64_t S2 = (int64_t)S * S, S3 = S2 * S;
+  const double hv = screen / NN, h2v = hv * hv, h3v = hv * hv * hv, soft = 4 * h2v, R_init = 3.0;
+  const double midI0 = (nuc[0] + nuc[16 * (n - 1)]) / 2;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i <= NN; ++i)
+    for (int j = 0; j <= NN; ++j)
+      for (int k = 0; k <= NN; ++k) {
+        const int64_t id = i * S2 + (int64_t)j * S + k;
+        double Kacc = 0, rl[MF_MAX], ul[MF_MAX];
+        int bestM = -1;
+        double bestU = -1;
+        for (int a = 0; a < n; ++a) {
+          const double* c = nuc + 16 * a;
+          const double dx = (i - c[0]) * hv, dy = (j - c[1]) * hv, dz = (k - c[2]) * hv;
+          const double r_soft = sqrt(dx * dx + dy * dy + dz * dz + soft);
+          const double r = sqrt(dx * dx + dy * dy + dz * dz);
+          Kacc += c[3] / r_soft;
+          const double z = c[7];
+          const double uh = exp(-z * r);
+          rl[a] = r; ul[a] = uh;
+          const double tg = c[8] != 0 ? c[8] : 1;
+          const double uw = sqrt(tg * z * z * z) * uh;
+          const double roa = c[5];
+          const int okR = !(roa > 0 && r > roa + hv);
+          const double hs = c[6];
+          const int okHS = hs == 0 || ((hs > 0) == (i > midI0));
+          const int okS = mf_in_split_f64(dx, dy, dz, r, (int)c[9], (int)c[10], c + 11);
+          if (okR && okHS && okS && uw > bestU) { bestU = uw; bestM = a; }
+        }
+        K[id] = (float)Kacc;
+        for (int m = 0; m < n; ++m) {
+          const double rc = nuc[16 * m + 4];
+          double u = ul[m];
+          if (rc > 0 && rl[m] < rc) {
+            const double edge = rc - 3 * hv;
+            const double t = fmax(0, fmin(1, (rl[m] - edge) / (rc - edge)));
+            u *= t * t * (3 - 2 * t);
+          }
+          U[m * S3 + id] = (float)u;
+          W[m * S3 + id] = 0.0f;
+        }
+        if (bestM >= 0 && rl[bestM] < R_init) {
+          const double rc = nuc[16 * bestM + 4], ro = nuc[16 * bestM + 5];
+          double w = 1.0;
+          if (rc > 0 && rl[bestM] < rc) {
+            const double edge = rc - 3 * hv;
+            const double t = fmax(0, fmin(1, (rl[bestM] - edge) / (rc - edge)));
+            w = t * t * (3 - 2 * t);
+          }
+          if (ro > 0 && rl[bestM] > ro + hv) w = 0;
+          W[bestM * S3 + id] = (float)w;
+        }
+        for (int m = 0; m < n; ++m) P[m * S3 + id] = (float)(0.5 * nuc[16 * m + 3] / (rl[m] + h2v));
+      }
+  for (int m = 0; m < n; ++m) {
+    double nrm = 0;
+    for (int64_t id = 0; id < S3; ++id) nrm += (double)U[m * S3 + id] * (double)U[m * S3 + id];
+    nrm *= h3v;
+    const double tg = nuc[16 * m + 8];
+    if (nrm > 0 && tg > 0) {
+      const double sc = sqrt(tg / nrm);
+      for (int64_t id = 0; id < S3; ++id) U[m * S3 + id] = (float)(U[m * S3 + id] * sc);
+    }
+  }
+}

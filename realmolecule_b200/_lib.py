@@ -38,6 +38,21 @@ class Shell(C.Structure):
                 ("half_index", C.c_int32), ("outer_half", C.c_int32), ("fixed_w", C.c_int32)]
 
 
+class MfConfig(C.Structure):
+    _fields_ = [("NN", C.c_int32), ("shell_mode", C.c_int32), ("vcycle", C.c_int32), ("vcycle_interval", C.c_int32),
+                ("coarse_iters", C.c_int32), ("r_out_release_step", C.c_int32), ("full_self", C.c_int32),
+                ("reserved0", C.c_int32), ("screen", C.c_double), ("kinetic_coeff", C.c_double),
+                ("kc_multi", C.c_double), ("beta_pauli", C.c_double), ("field_x", C.c_double),
+                ("alpha_tf", C.c_double), ("line_j_offset", C.c_double), ("reserved", C.c_int32 * 8)]
+
+
+class MfNucleus(C.Structure):
+    _fields_ = [("i", C.c_double), ("j", C.c_double), ("k", C.c_double), ("Z", C.c_double), ("rc", C.c_double),
+                ("r_out", C.c_double), ("tilt_y", C.c_double), ("tilt_x", C.c_double), ("hs", C.c_double),
+                ("z_init", C.c_double), ("norm_target", C.c_double), ("split_axis", C.c_double * 3),
+                ("split", C.c_int32), ("split_idx", C.c_int32), ("split_fix", C.c_int32), ("reserved", C.c_int32)]
+
+
 class Config(C.Structure):
     _fields_ = [("NN", C.c_int32), ("flavor", C.c_int32), ("precision", C.c_int32), ("norm_interval", C.c_int32),
                 ("screen", C.c_double), ("dv", C.c_double), ("poisson_interval", C.c_int32),
@@ -116,6 +131,17 @@ SIGNATURES = {
     "rq_shells_download": (C.c_int, [_V, _I, _P, _P, _P]),
     "rq_shells_upload": (C.c_int, [_V, _I, _P, _P, _P]),
     "rq_shells_info": (C.c_int, [_V, _P]),
+    "rq_mf_create": (C.c_int, [_P, _P, _I, _P]),
+    "rq_mf_destroy": (None, [_V]),
+    "rq_mf_last_error": (C.c_char_p, [_V]),
+    "rq_mf_step": (C.c_int, [_V, _I, _P]),
+    "rq_mf_forces": (C.c_int, [_V, _P]),
+    "rq_mf_set_positions": (C.c_int, [_V, _P]),
+    "rq_mf_extract": (C.c_int, [_V, _P]),
+    "rq_mf_download": (C.c_int, [_V, _I, _P, _P, _P]),
+    "rq_mf_upload": (C.c_int, [_V, _I, _P, _P, _P]),
+    "rq_mf_download_K": (C.c_int, [_V, _P]),
+    "rq_mf_info": (C.c_int, [_V, _P, _P]),
     "rq_kernel_update_sp": (C.c_int, [_P, _P, _P, _P, _P, _I, _F, _F, _V]),
     "rq_kernel_jacobi_sp": (C.c_int, [_P, _P, _P, _I, _F, _F, _V]),
     "rq_kernel_labels_sp": (C.c_int, [_P, _P, _P, _I, _I, _F, _F, _V]),
