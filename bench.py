@@ -417,6 +417,43 @@ def caller_legs(a):
     out["atom_js_he"] = {"grid": "100^3", "shells": 2, "ms_per_step": gpu_ms,
                          "cpu_sequential_ms_per_step": cpu_ms, "cpu_cores": 1,
                          "cpu": "the oracle's sequential restatement of atom.js (2 steps)"}
+    out["mol_fast_ch4"] = mol_fast_leg(a)
+    return out
+
+
+def mol_fast_leg(a):
+    """mol_fast.js's CH4 page (NN = 200, 5 electrons, 500-step frames with forces and nuclear
+    moves) through the drop-in MolFast, against the oracle's restatement on the host cores."""
+    from realmolecule_b200 import configs
+    from realmolecule_b200.mol_fast import MolFast
+    cfg = configs.mol_fast_ch4_page()
+    mf = MolFast(**cfg)
+    mf.frame()
+    frames = 3
+    t0 = time.perf_counter()
+    for _ in range(frames):
+        mf.frame()
+    frame_ms = (time.perf_counter() - t0) / frames * 1e3
+    launches = mf.kernel_launches
+    mf.close()
+    n, vox = len(cfg["nuclei"]), (cfg["NN"] - 1) ** 3
+    upd_bytes = vox * (24 * n + 4)
+    out = {"grid": f"{cfg['NN']}^3", "electrons_fields": n, "steps_per_frame": 500, "frame_ms": frame_ms,
+           "ms_per_step": frame_ms / 500, "update_bytes_per_step": upd_bytes,
+           "update_GBps_if_all_time": upd_bytes / (frame_ms / 500 * 1e-3) / 1e9,
+           "timing": "host wall clock around frame() = doSteps(500) + computeForces + stepNuclei",
+           "librq_launches_total": launches}
+    if not a.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        ref = orc.MolFastDriver(cfg["nuclei"], NN=cfg["NN"], screen=cfg["screen"], norm_targets=cfg["norm_targets"])
+        ref.initialize()
+        steps = 10
+        t0 = time.perf_counter()
+        ref.do_steps(steps)
+        cpu_ms = (time.perf_counter() - t0) / steps * 1e3
+        out.update({"cpu_ms_per_step": cpu_ms, "cpu_cores": len(os.sched_getaffinity(0)),
+                    "cpu": f"the oracle's restatement of the shaders, OpenMP, {steps} steps (one reduction)"})
     return out
 
 

@@ -220,4 +220,38 @@ def reference_config(g: Geometry, **extra) -> dict:
     return cfg
 
 
+def _js_round(x: float) -> int:
+    """JavaScript's Math.round (halves round up)."""
+    return math.floor(x + 0.5)
+
+
+def mol_fast_h2_page(sep: float = 1.4) -> dict:
+    """The H2 page of mol_fast.js (mol_fast_h2.html:16-33): NN = 200, 10 bohr box, the two nuclei
+    sep apart on the i axis, dynamics on.  Keyword arguments of ``MolFast``."""
+    N, scr = 200, 10.0
+    h, N2 = scr / N, _js_round(N / 2)
+    di = _js_round(sep / h / 2)
+    return {"nuclei": [{"i": N2 - di, "j": N2, "k": N2, "Z": 1, "rc": 0.0, "z_init": 1.0},
+                       {"i": N2 + di, "j": N2, "k": N2, "Z": 1, "rc": 0.0, "z_init": 1.0}],
+            "NN": N, "screen": scr, "norm_targets": [1, 1], "max_steps": 50000, "dynamics": True}
+
+
+def mol_fast_ch4_page(bond: float = 2.054, scr: float = 12.0) -> dict:
+    """The CH4 page of mol_fast.js (mol_fast_ch4.html:18-54): NN = 200, a Z = 4 carbon pseudo-atom
+    (rc 0.5, one 4-electron orbital) at the centre and four tetrahedral H at `bond` bohr, grid-rounded;
+    dynamics on.  Keyword arguments of ``MolFast``."""
+    N = 200
+    h, N2 = scr / N, _js_round(N / 2)
+
+    def shift(dx, dy, dz):
+        return {"i": _js_round(N2 + dx * bond / h), "j": _js_round(N2 + dy * bond / h),
+                "k": _js_round(N2 + dz * bond / h)}
+
+    s2, s6 = math.sqrt(2), math.sqrt(6)
+    hs = [shift(1, 0, 0), shift(-1 / 3, 2 * s2 / 3, 0), shift(-1 / 3, -s2 / 3, s6 / 3), shift(-1 / 3, -s2 / 3, -s6 / 3)]
+    nuc = [{"i": N2, "j": N2, "k": N2, "Z": 4, "rc": 0.5}] + [dict(x, Z=1, rc=0.0) for x in hs]
+    return {"nuclei": nuc, "NN": N, "screen": scr, "norm_targets": [4, 1, 1, 1, 1], "max_steps": 100000,
+            "alpha_tf": 0.0, "dynamics": True}
+
+
 WORKLOADS = {"h2o64": h2o64, "glycine128": glycine128, "water100": water100, "water1000": water1000}

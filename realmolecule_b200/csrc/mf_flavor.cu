@@ -36,6 +36,11 @@ struct MfParams {  // writeParams (mol_fast.js:838-874) plus the constants templ
   float r_out[kMfMax];
   int split_type[kMfMax], split_idx[kMfMax], split_fix[kMfMax], split_group[kMfMax];
   float4 ax[kMfMax];
+  // per-electron constants of the shaders, formed on the host with the same f32 operations:
+  // upd = (fm, half_d * k_mult, 1 if the Thomas-Fermi term is on, tilt_x) of updateWGSL,
+  // red = (fm without USER_FULL_SELF, k_mult * KINETIC_COEFF, same flag, tilt_y) of reduceWGSL
+  float4 upd[kMfMax], red[kMfMax];
+  unsigned gmask[kMfMax];  // bit q set: electron q is in this electron's split group
 };
 
 constexpr int kMfNucLen = 16;  // doubles per nucleus record of the initialiser
@@ -111,12 +116,19 @@ __device__ bool mf_in_sector(const MfParams* __restrict__ p, int m, float x, flo
 
 constexpr int kMfTK = 32, kMfTJ = 8;
 
-// updateWGSL (mol_fast.js:134-351) for every electron of one interior cell
+
+// updateWGSL (mol_fast.js:134-351) for every electron of one interior cell.  One thread owns a
+// cell: the cross-electron terms (sum_q P_q, the competitor max) come from one read of each
+// electron's U and P at the cell.  The competitor max over the other electrons is the largest U
+// of the cell unless this electron holds it (then the second largest): both are exact
+// selections, equal to the shader's sequential scan.  The register cap (4 blocks of 256 per SM)
+// lets the per-electron stencil loads of enough warps overlap; the kernel is bound by the
+// instruction issue of the unfused f32 arithmetic, not by DRAM.
 template <int NMAX, bool SHELL>
-__global__ void __launch_bounds__(256) k_mf_update(const MfParams* __restrict__ p, const float* __restrict__ Ui,
-                                                   const float* __restrict__ Wi, const float* __restrict__ Pi,
-                                                   const float* __restrict__ K, float* __restrict__ Uo,
-                                                   float* __restrict__ Wo, float* __restrict__ Po) {
+__global__ void __launch_bounds__(256, 4) k_mf_update(const MfParams* __restrict__ p, const float* __restrict__ Ui,
+                                                      const float* __restrict__ Wi, const float* __restrict__ Pi,
+                                                      const float* __restrict__ K, float* __restrict__ Uo,
+                                                      float* __restrict__ Wo, float* __restrict__ Po) {
   const int NN = p->NN;
   const int k = blockIdx.x * kMfTK + threadIdx.x + 1;
   const int j = blockIdx.y * kMfTJ + threadIdx.y + 1;
@@ -125,17 +137,23 @@ __global__ void __launch_bounds__(256) k_mf_update(const MfParams* __restrict__ 
   const long long S = p->S, S2 = S * S, S3 = S2 * S;
   const long long id = (long long)i * S2 + (long long)j * S + k;
   const int n = p->n;
-  const float h = p->h, dt = p->dt, inv_h = p->inv_h, inv_h2 = p->inv_h2;
   float uq[NMAX], pq[NMAX];
 #pragma unroll
   for (int q = 0; q < NMAX; ++q) {
     uq[q] = q < n ? __ldg(Ui + q * S3 + id) : 0.0f;
     pq[q] = q < n ? __ldg(Pi + q * S3 + id) : 0.0f;
   }
-  float Ptot = 0.0f;
+  float Ptot = 0.0f, max1 = 0.0f, max2 = 0.0f;
+  int arg1 = -1;
 #pragma unroll
   for (int q = 0; q < NMAX; ++q)
-    if (q < n) Ptot = F_ADD(Ptot, pq[q]);
+    if (q < n) {
+      Ptot = F_ADD(Ptot, pq[q]);
+      const float u = uq[q];
+      if (u > max1) { max2 = max1; max1 = u; arg1 = q; }
+      else if (u > max2) max2 = u;
+    }
+  const float h = p->h, dt = p->dt, inv_h = p->inv_h, inv_h2 = p->inv_h2;
   // frozen-core mode: the rc cusps of all nuclei act on every electron's front; min is exact,
   // so the cap over the nuclei is taken once per cell (mol_fast.js:249-262)
   float cap = 2.0f;
@@ -151,34 +169,41 @@ __global__ void __launch_bounds__(256) k_mf_update(const MfParams* __restrict__ 
   const float Kc = __ldg(K + id);
   const float x_au = F_MUL(F_SUB((float)i, (float)p->N2), h);
   const float y_au = F_MUL(F_SUB((float)j, (float)p->N2), h);
-  const float beta = p->beta;
+  const float beta = p->beta, two_pi_dt = F_MUL(p->two_pi, dt), fxx = F_MUL(p->field_x, x_au);
+  const float dt005 = F_MUL(0.05f, dt), dt1 = F_MUL(1.0f, dt);
 #pragma unroll 1
   for (int m = 0; m < n; ++m) {
     const long long o = m * S3 + id;
-    float uc = 0.0f, umax = 0.0f, Pgrp = 0.0f, rho_other = 0.0f;
-    const int grp = p->split_group[m];
-#pragma unroll
-    for (int q = 0; q < NMAX; ++q) {
-      if (q >= n) break;
-      if (q == m) {
-        uc = uq[q];
-      } else {
-        if (uq[q] > umax) umax = uq[q];
-        rho_other = F_ADD(rho_other, F_MUL(uq[q], uq[q]));
-      }
-      if (p->split_group[q] == grp) Pgrp = F_ADD(Pgrp, pq[q]);
-    }
-    const float cm = F_SUB(uc, umax);
-    const float wc = __ldg(Wi + o);
+    const float uc = __ldg(Ui + o), wc = __ldg(Wi + o), Pc = __ldg(Pi + o);
     const float wip = __ldg(Wi + o + S2), wim = __ldg(Wi + o - S2);
     const float wjp = __ldg(Wi + o + S), wjm = __ldg(Wi + o - S);
     const float wkp = __ldg(Wi + o + 1), wkm = __ldg(Wi + o - 1);
+    const float uip = __ldg(Ui + o + S2), uim = __ldg(Ui + o - S2);
+    const float ujp = __ldg(Ui + o + S), ujm = __ldg(Ui + o - S);
+    const float ukp = __ldg(Ui + o + 1), ukm = __ldg(Ui + o - 1);
+    const float pip = __ldg(Pi + o + S2), pim = __ldg(Pi + o - S2);
+    const float pjp = __ldg(Pi + o + S), pjm = __ldg(Pi + o - S);
+    const float pkp = __ldg(Pi + o + 1), pkm = __ldg(Pi + o - 1);
+    const float4 cu = p->upd[m];
+    const float tilt_y = p->rcs[m].w;
+    const unsigned gm = p->gmask[m];
+    const float umax = m == arg1 ? max2 : max1;
+    float Pgrp = 0.0f, rho_other = 0.0f;
+#pragma unroll
+    for (int q = 0; q < NMAX; ++q)
+      if (q < n && ((gm >> q) & 1u)) Pgrp = F_ADD(Pgrp, pq[q]);
+    if (beta != 0.0f) {  // V_Pauli; with beta = 0 it is 0 * (a finite sum of squares) = 0
+#pragma unroll
+      for (int q = 0; q < NMAX; ++q)
+        if (q < n && q != m) rho_other = F_ADD(rho_other, F_MUL(uq[q], uq[q]));
+    }
+    const float cm = F_SUB(uc, umax);
     const float lw =
         F_MUL(F_SUB(F_ADD(F_ADD(F_ADD(F_ADD(F_ADD(wip, wim), wjp), wjm), wkp), wkm), F_MUL(6.0f, wc)), inv_h2);
     const float gx = F_MUL(F_SUB(wip, wim), inv_h), gy = F_MUL(F_SUB(wjp, wjm), inv_h),
                 gz = F_MUL(F_SUB(wkp, wkm), inv_h);
-    float nw = F_ADD(F_ADD(wc, F_MUL(F_MUL(F_MUL(0.05f, dt), fabsf(cm)), lw)),
-                     F_MUL(F_MUL(F_MUL(1.0f, dt), cm), F_SQRT(F_ADD(F_ADD(F_MUL(gx, gx), F_MUL(gy, gy)), F_MUL(gz, gz)))));
+    float nw = F_ADD(F_ADD(wc, F_MUL(F_MUL(dt005, fabsf(cm)), lw)),
+                     F_MUL(F_MUL(dt1, cm), F_SQRT(F_ADD(F_ADD(F_MUL(gx, gx), F_MUL(gy, gy)), F_MUL(gz, gz)))));
     nw = fminf(fmaxf(nw, 0.0f), 1.0f);
     if (SHELL) {
       const float4 at = p->atoms[m];
@@ -193,32 +218,19 @@ __global__ void __launch_bounds__(256) k_mf_update(const MfParams* __restrict__ 
       nw = fminf(nw, cap);
     }
     Wo[o] = nw;
-    const float4 rc4 = p->rcs[m];
-    const float selfN = rc4.y;
-    const float fm_multi = p->full_self > 0.5f ? 0.0f : F_DIV(1.0f, selfN);
-    const float fm = selfN > 1.0f ? fm_multi : 1.0f;
-    const float Vother = F_MUL(2.0f, F_SUB(Ptot, F_MUL(fm, Pgrp)));
-    float V_TF = 0.0f;
-    if (selfN > 1.0f && p->alpha_tf > 0.0f) V_TF = F_MUL(p->alpha_tf, mf_pow(fmaxf(F_MUL(uc, uc), 1e-20f), 0.6666667f));
-    const float V_tilt = F_SUB(F_MUL(-rc4.z, x_au), F_MUL(rc4.w, y_au));
+    const float Vother = F_MUL(2.0f, F_SUB(Ptot, F_MUL(cu.x, Pgrp)));
+    const float V_TF = cu.z != 0.0f ? F_MUL(p->alpha_tf, mf_pow(fmaxf(F_MUL(uc, uc), 1e-20f), 0.6666667f)) : 0.0f;
+    const float V_tilt = F_SUB(F_MUL(-cu.w, x_au), F_MUL(tilt_y, y_au));
     const float V_Pauli = F_MUL(beta, rho_other);
-    const float uip = __ldg(Ui + o + S2), uim = __ldg(Ui + o - S2);
-    const float ujp = __ldg(Ui + o + S), ujm = __ldg(Ui + o - S);
-    const float ukp = __ldg(Ui + o + 1), ukm = __ldg(Ui + o - 1);
-    const float hd = F_MUL(p->half_d, selfN > 1.0f ? p->kc_multi : 1.0f);
+    const float hd = cu.y;
     const float fx = F_SUB(F_MUL(F_MUL(F_SUB(uip, uc), F_ADD(wip, nw)), 0.5f), F_MUL(F_MUL(F_SUB(uc, uim), F_ADD(nw, wim)), 0.5f));
     const float fy = F_SUB(F_MUL(F_MUL(F_SUB(ujp, uc), F_ADD(wjp, nw)), 0.5f), F_MUL(F_MUL(F_SUB(uc, ujm), F_ADD(nw, wjm)), 0.5f));
     const float fz = F_SUB(F_MUL(F_MUL(F_SUB(ukp, uc), F_ADD(wkp, nw)), 0.5f), F_MUL(F_MUL(F_SUB(uc, ukm), F_ADD(nw, wkm)), 0.5f));
-    const float pot = F_SUB(F_SUB(F_SUB(F_SUB(F_SUB(Kc, Vother), V_TF), V_tilt), V_Pauli), F_MUL(p->field_x, x_au));
+    const float pot = F_SUB(F_SUB(F_SUB(F_SUB(F_SUB(Kc, Vother), V_TF), V_tilt), V_Pauli), fxx);
     Uo[o] = F_ADD(F_ADD(F_ADD(F_ADD(uc, F_MUL(hd, fx)), F_MUL(hd, fy)), F_MUL(hd, fz)),
                   F_MUL(F_MUL(F_MUL(dt, pot), uc), wc));
-    const float Pc = __ldg(Pi + o);
-    const float lap = F_SUB(F_ADD(F_ADD(F_ADD(F_ADD(F_ADD(__ldg(Pi + o + S2), __ldg(Pi + o - S2)), __ldg(Pi + o + S)),
-                                              __ldg(Pi + o - S)),
-                                        __ldg(Pi + o + 1)),
-                                  __ldg(Pi + o - 1)),
-                            F_MUL(6.0f, Pc));
-    Po[o] = F_ADD(F_ADD(Pc, F_MUL(F_MUL(dt, lap), inv_h2)), F_MUL(F_MUL(F_MUL(p->two_pi, dt), uc), uc));
+    const float lap = F_SUB(F_ADD(F_ADD(F_ADD(F_ADD(F_ADD(pip, pim), pjp), pjm), pkp), pkm), F_MUL(6.0f, Pc));
+    Po[o] = F_ADD(F_ADD(Pc, F_MUL(F_MUL(dt, lap), inv_h2)), F_MUL(F_MUL(two_pi_dt, uc), uc));
   }
 }
 
@@ -247,25 +259,22 @@ __global__ void __launch_bounds__(128) k_mf_reduce(const MfParams* __restrict__ 
     for (int m = 0; m < n; ++m) {
       const long long o = m * S3 + id;
       const float v = __ldg(U + o);
-      const float4 rc4 = p->rcs[m];
+      const float4 cr = p->red[m];
       const float vv = F_MUL(v, v);
       sn[lid * NR + m] = F_MUL(vv, h3);
       if (__ldg(W + o) > 0.1f) {
         const float a = F_SUB(__ldg(U + o + S2), v), b = F_SUB(__ldg(U + o + S), v), c = F_SUB(__ldg(U + o + 1), v);
-        const float kmt = rc4.y > 1.0f ? p->kc_multi : 1.0f;
-        T = F_ADD(T, F_MUL(F_MUL(F_MUL(kmt, p->kc), F_ADD(F_ADD(F_MUL(a, a), F_MUL(b, b)), F_MUL(c, c))), h));
+        T = F_ADD(T, F_MUL(F_MUL(cr.y, F_ADD(F_ADD(F_MUL(a, a), F_MUL(b, b)), F_MUL(c, c))), h));
       }
       VeK = F_SUB(VeK, F_MUL(F_MUL(F_MUL(Kc, v), v), h3));
       const float rho_cell = F_MUL(vv, h3);
       dx = F_SUB(dx, F_MUL(rho_cell, xc));
       dy = F_SUB(dy, F_MUL(rho_cell, yc));
       dz = F_SUB(dz, F_MUL(rho_cell, zc));
-      const float selfN = rc4.y;
-      const float fm = selfN > 1.0f ? F_DIV(1.0f, selfN) : 1.0f;
-      Vee = F_ADD(Vee, F_MUL(F_MUL(F_MUL(F_SUB(Ptot, F_MUL(fm, __ldg(Pv + o))), v), v), h3));
-      if (selfN > 1.0f && p->alpha_tf > 0.0f)
+      Vee = F_ADD(Vee, F_MUL(F_MUL(F_MUL(F_SUB(Ptot, F_MUL(cr.x, __ldg(Pv + o))), v), v), h3));
+      if (cr.z != 0.0f)
         T = F_ADD(T, F_MUL(F_MUL(F_MUL(0.6f, p->alpha_tf), mf_pow(fmaxf(vv, 1e-20f), 1.6666667f)), h3));
-      const float tilt = rc4.w;
+      const float tilt = cr.w;
       if (tilt != 0.0f) T = F_ADD(T, F_MUL(F_MUL(F_MUL(F_MUL(-tilt, yc), v), v), h3));
     }
     sn[lid * NR + n] = T;
@@ -722,6 +731,18 @@ void mf_fill_params(rq_mf* s) {
     p.split_group[a] = g;
   }
   if (s->n == kMfMax) p.rcs[kMfMax - 1].z = (float)c.line_j_offset;  // the reference's last rcs slot
+  for (int a = 0; a < s->n; ++a) {
+    const float selfN = p.rcs[a].y;
+    const float km = selfN > 1.0f ? p.kc_multi : 1.0f;
+    const float fm = selfN > 1.0f ? (p.full_self > 0.5f ? 0.0f : 1.0f / selfN) : 1.0f;
+    const float tf = (selfN > 1.0f && p.alpha_tf > 0.0f) ? 1.0f : 0.0f;
+    p.upd[a] = make_float4(fm, p.half_d * km, tf, p.rcs[a].z);
+    p.red[a] = make_float4(selfN > 1.0f ? 1.0f / selfN : 1.0f, km * p.kc, tf, p.rcs[a].w);
+    unsigned gmask = 0;
+    for (int b = 0; b < s->n; ++b)
+      if (p.split_group[b] == p.split_group[a]) gmask |= 1u << b;
+    p.gmask[a] = gmask;
+  }
 }
 
 int mf_upload_params(rq_mf* s) {
