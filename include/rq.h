@@ -330,6 +330,45 @@ RQ_API int rq_mf_upload(rq_mf* s, int32_t m, const float* U, const float* W, con
 RQ_API int rq_mf_download_K(rq_mf* s, float* K);
 RQ_API int rq_mf_info(const rq_mf* s, int64_t* kernel_launches, int64_t* steps_done);
 
+/* ---- realqm_rb.js red-black multi-field solver (realqm_rb.js:1-1222) -------------------------
+ * Replaces realqm_rb.js's GPU state, doSteps(), computeEnergy() and extractSlice(): one U, W, P
+ * field per electron (each nucleus carries `ne` electrons, 2..16 in all), updated in place by
+ * red-black colouring -- per step rho_total and each electron's competitor, then the red and
+ * the black passes (front and amplitude, then the potential) -- and normalised with the
+ * reference's f32 grid-stride reduction whenever the frame-local step index is a multiple of 5.
+ * The f32 arithmetic follows the shaders' operation order (no contraction). */
+typedef struct rq_rb rq_rb;
+typedef struct rq_rb_config {
+  int32_t NN;       /* USER_NN (100) */
+  int32_t reserved0;
+  double screen;    /* USER_SCREEN, box edge in bohr (8) */
+  int32_t reserved[8];
+} rq_rb_config;
+typedef struct rq_rb_nucleus {  /* one entry of USER_NUCLEI */
+  double i, j, k;               /* grid coordinates */
+  double Z, rc;                 /* rc > 0: the initial front is cut at rc bohr */
+  double rc_excl;               /* > 0: u and w held at 0 within rc_excl bohr of the nucleus */
+  int32_t ne;                   /* electrons of this nucleus (ne = 2: the left / right half split) */
+  int32_t reserved;
+} rq_rb_nucleus;
+/* norm_targets: one occupation per electron (USER_NORM_TARGETS) or NULL (the nucleus' ne).
+ * The initial state (runInitKernels and the r_c masks, :720-801, :519-544, :615-644) is built
+ * at creation. */
+RQ_API int rq_rb_create(const rq_rb_config* cfg, const rq_rb_nucleus* nuclei, int32_t n_nuclei,
+                        const double* norm_targets, rq_rb** out);
+RQ_API void rq_rb_destroy(rq_rb* s);
+RQ_API const char* rq_rb_last_error(const rq_rb* s);
+/* doSteps(n) (:891-965).  Synchronises. */
+RQ_API int rq_rb_step(rq_rb* s, int32_t n);
+/* computeEnergy (:982-1045) summed in FP64: out = {E_T, E_eK, E_ee} (without V_KK). */
+RQ_API int rq_rb_energy(rq_rb* s, double* out);
+/* extractSlice (:1047-1066) as a headless buffer of S*S*(3n+1) floats. */
+RQ_API int rq_rb_slice(rq_rb* s, float* out);
+RQ_API int rq_rb_download(rq_rb* s, int32_t m, float* U, float* W, float* P);
+RQ_API int rq_rb_upload(rq_rb* s, int32_t m, const float* U, const float* W, const float* P);
+RQ_API int rq_rb_download_K(rq_rb* s, float* K);
+RQ_API int rq_rb_info(const rq_rb* s, int64_t* kernel_launches, int64_t* steps_done);
+
 /* ---- single kernels on caller-owned device memory (zero-copy PyTorch interop) ---------------
  * Pointers are device pointers of S^3 elements; `stream` is a cudaStream_t or NULL.  These run
  * exactly the kernels rq_step uses and exist for kernel-level parity checks and custom drivers. */

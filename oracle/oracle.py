@@ -126,12 +126,20 @@ class _Oracle:
             "orc_mf_recompute_k": [C.c_void_p, _f32p],
             "orc_mf_extract": [C.c_void_p, _f32p, _f32p, _f32p, _f32p],
             "orc_mf_init": [_i, _d, _i, _f64p, _f32p, _f32p, _f32p, _f32p],
+            "orc_rb_rho_nearest": [C.c_void_p, _f32p, _f32p, _f32p],
+            "orc_rb_wu": [C.c_void_p, _i, _i, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p],
+            "orc_rb_p": [C.c_void_p, _i, _i, _f32p, _f32p, _f32p],
+            "orc_rb_normalize": [C.c_void_p, _i, _f32p],
+            "orc_rb_energy": [C.c_void_p, _f32p, _f32p, _f32p, _f32p, _d, _d, _f64p],
+            "orc_rb_init": [C.c_void_p, _i, _f32p, _i32p, _f32p, _f32p, _f32p, _f32p],
+            "orc_rb_slice": [C.c_void_p, _f32p, _f32p, _f32p, _f32p, _f32p],
         }
         for name, argt in sig.items():
             fn = getattr(L, name)
             fn.argtypes = argt
             fn.restype = None
             setattr(self, name[4:], fn)
+        L.orc_rb_normalize.restype = C.c_float
         self.lib = L
 
 
@@ -889,3 +897,97 @@ class MolFastDriver:
         c, S3 = self.cur, self.S3
         return {"U": self.U[c][m * S3:(m + 1) * S3], "W": self.W[c][m * S3:(m + 1) * S3],
                 "P": self.P[c][m * S3:(m + 1) * S3]}
+
+
+# ---- realqm_rb.js (realqm_rb.js:1-1222) ---------------------------------------------------------
+
+class RbParams(C.Structure):
+    _fields_ = [("NN", C.c_int32), ("S", C.c_int32), ("N2", C.c_int32), ("n", C.c_int32), ("h", C.c_float),
+                ("h2", C.c_float), ("inv_h", C.c_float), ("inv_h2", C.c_float), ("dt", C.c_float),
+                ("half_d", C.c_float), ("two_pi", C.c_float), ("h3", C.c_float), ("tgt", C.c_float * 16)]
+
+
+class RealqmRbDriver:
+    """realqm_rb.js restated on the CPU: the page constants (:8-35), electronNucleus (:73-82),
+    runInitKernels and the r_c masks (:720-801, :519-544, :615-644), doSteps (:891-965) with the
+    reference's sequential per-electron passes, computeEnergy (:982-1045), extractSlice."""
+
+    def __init__(self, nuclei, NN=100, screen=8.0, norm_targets=None):
+        self.nuclei = [dict(n, ne=1 if n.get("ne") is None else n["ne"], rc=n.get("rc") or 0) for n in nuclei]
+        self.enuc = [a for a, nu in enumerate(self.nuclei) for _ in range(int(nu["ne"]))]
+        self.n = len(self.enuc)
+        self.NN, self.S = NN, NN + 1
+        self.S3 = self.S ** 3
+        self.h = screen / NN
+        self.h2, self.h3 = self.h * self.h, self.h * self.h * self.h
+        p = self.p = RbParams()
+        f = lambda v: float(np.float32(v))
+        p.NN, p.S, p.N2, p.n = NN, self.S, NN // 2, self.n
+        p.h, p.h2, p.inv_h, p.inv_h2 = f(self.h), f(self.h2), f(1 / self.h), f(1 / self.h2)
+        p.dt, p.half_d, p.two_pi, p.h3 = f(0.1 * self.h2), f(0.5 * 0.1), f(2 * math.pi), f(self.h3)
+        for m in range(self.n):
+            p.tgt[m] = norm_targets[m] if norm_targets is not None else self.nuclei[self.enuc[m]]["ne"]
+        nS = self.n * self.S3
+        self.U, self.W, self.P = (np.zeros(nS, np.float32) for _ in range(3))
+        self.K = np.zeros(self.S3, np.float32)
+        self.mask = np.ones(nS, np.float32)
+        self.rho = np.zeros(self.S3, np.float32)
+        self.unear = np.zeros(nS, np.float32)
+        self.norms = np.zeros(self.n, np.float32)
+
+    @property
+    def pp(self):
+        return C.addressof(self.p)
+
+    def initialize(self):
+        nuc = np.zeros((len(self.nuclei), 8), np.float32)
+        for a, nu in enumerate(self.nuclei):
+            nuc[a, :6] = [nu["i"], nu["j"], nu["k"], nu["Z"], nu["rc"], nu["ne"]]
+        O().rb_init(self.pp, len(self.nuclei), np.ascontiguousarray(nuc.reshape(-1)),
+                    np.array(self.enuc, np.int32), self.K, self.U, self.W, self.P)
+        S, S2, h = self.S, self.S * self.S, self.h
+        for m in range(self.n):  # the r_c exclusion masks, in JS numbers
+            nu = self.nuclei[self.enuc[m]]
+            rc = nu.get("rc_excl") or 0
+            if not rc > 0 or any(float(nu[c]) != math.floor(nu[c]) for c in "ijk"):
+                continue
+            rcc = math.ceil(rc / h) + 1
+            for di in range(-rcc, rcc + 1):
+                for dj in range(-rcc, rcc + 1):
+                    for dk in range(-rcc, rcc + 1):
+                        gi, gj, gk = int(nu["i"]) + di, int(nu["j"]) + dj, int(nu["k"]) + dk
+                        if gi < 0 or gi >= S or gj < 0 or gj >= S or gk < 0 or gk >= S:
+                            continue
+                        r2 = (di * h) * (di * h) + (dj * h) * (dj * h) + (dk * h) * (dk * h)
+                        if r2 < rc * rc:
+                            idx = m * self.S3 + gi * S2 + gj * S + gk
+                            self.mask[idx] = 0.0
+                            self.U[idx] = 0.0
+                            self.W[idx] = 0.0
+
+    def do_steps(self, n):
+        o = O()
+        for s in range(n):
+            o.rb_rho_nearest(self.pp, self.U, self.rho, self.unear)
+            for color in (0, 1):
+                for m in range(self.n):
+                    o.rb_wu(self.pp, m, color, self.U, self.W, self.unear, self.K, self.P, self.mask)
+                for m in range(self.n):
+                    o.rb_p(self.pp, m, color, self.P, self.U, self.rho)
+            if s % 5 == 0:
+                for m in range(self.n):
+                    self.norms[m] = o.rb_normalize(self.pp, m, self.U)
+
+    def energy(self):
+        out = np.zeros(3)
+        O().rb_energy(self.pp, self.U, self.W, self.P, self.K, self.h, self.h3, out)
+        return out
+
+    def slice(self):
+        out = np.zeros(self.S * self.S * (3 * self.n + 1), np.float32)
+        O().rb_slice(self.pp, self.U, self.W, self.P, self.K, out)
+        return out
+
+    def fields(self, m):
+        S3 = self.S3
+        return {"U": self.U[m * S3:(m + 1) * S3], "W": self.W[m * S3:(m + 1) * S3], "P": self.P[m * S3:(m + 1) * S3]}

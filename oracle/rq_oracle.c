@@ -1876,3 +1876,239 @@ void orc_mf_init(int NN, double screen, int n, const double* nuc, float* K, floa
     }
   }
 }
+
+/* ======================================================================
+ * realqm_rb.js red-black multi-field solver (realqm_rb.js:1-1222), f32 WGSL semantics
+ *
+ * One U, W, P field per electron (field m at offset m*S3), updated IN PLACE by red-black
+ * colouring; exp is the f64 function rounded once to f32 (WGSL leaves its accuracy to the
+ * implementation; the CUDA side does the same).
+ * ==================================================================== */
+
+typedef struct {
+  int32_t NN, S, N2, n;   /* n electrons */
+  float h, h2, inv_h, inv_h2, dt, half_d, two_pi, h3;
+  float tgt[MF_MAX];      /* occupation (norm target) per electron */
+} orc_rb_params;
+
+/* rhoTotal (realqm_rb.js:190-215) and uNearest (:225-251): rho = u0^2 + u1^2 + ... and, per
+ * electron, the max of the other electrons' u in index order, at every interior cell */
+void orc_rb_rho_nearest(const orc_rb_params* p, const float* U, float* rho, float* unear) {
+  const int NN = p->NN, S = p->S, n = p->n;
+  const int64_t S2 = (int64_t)S * S, S3 = S2 * S;
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        const int64_t id = i * S2 + (int64_t)j * S + k;
+        float r = U[id] * U[id];
+        for (int m = 1; m < n; ++m) r = r + U[m * S3 + id] * U[m * S3 + id];
+        rho[id] = r;
+        for (int m = 0; m < n; ++m) {
+          int first = 1;
+          float v = 0.0f;
+          for (int q = 0; q < n; ++q) {
+            if (q == m) continue;
+            const float u = U[q * S3 + id];
+            if (first) { v = u; first = 0; }
+            else v = fmaxf(v, u);
+          }
+          unear[m * S3 + id] = v;
+        }
+      }
+}
+
+/* fusedWU_RB_WGSL (realqm_rb.js:256-311) for electron m on the cells of one colour, in place */
+void orc_rb_wu(const orc_rb_params* p, int m, int color, float* U, float* W, const float* unear, const float* K,
+               const float* P, const float* mask) {
+  const int NN = p->NN, S = p->S;
+  const int64_t S2 = (int64_t)S * S, S3 = S2 * S;
+  float* u = U + m * S3;
+  float* w = W + m * S3;
+  const float* un = unear + m * S3;
+  const float* Pm = P + m * S3;
+  const float* mk = mask + m * S3;
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        if ((i + j + k) % 2 != color) continue;
+        const int64_t id = i * S2 + (int64_t)j * S + k;
+        const float c = 0.1f * (u[id] - un[id]);
+        const float wc = w[id];
+        const float lap_w = w[id + S2] + w[id - S2] + w[id + S] + w[id - S] + w[id + 1] + w[id - 1] - 6.0f * wc;
+        const float gwx = (w[id + S2] - w[id - S2]) * p->inv_h;
+        const float gwy = (w[id + S] - w[id - S]) * p->inv_h;
+        const float gwz = (w[id + 1] - w[id - 1]) * p->inv_h;
+        const float grad_w = sqrtf(gwx * gwx + gwy * gwy + gwz * gwz);
+        w[id] = wc + 0.5f * p->dt * fabsf(c) * lap_w * p->inv_h2 + 10.0f * p->dt * c * grad_w;
+        const float wc2 = w[id];
+        const float uc = u[id];
+        const float fxp = (u[id + S2] - uc) * (w[id + S2] + wc2) * 0.5f;
+        const float fxm = (uc - u[id - S2]) * (wc2 + w[id - S2]) * 0.5f;
+        const float fyp = (u[id + S] - uc) * (w[id + S] + wc2) * 0.5f;
+        const float fym = (uc - u[id - S]) * (wc2 + w[id - S]) * 0.5f;
+        const float fzp = (u[id + 1] - uc) * (w[id + 1] + wc2) * 0.5f;
+        const float fzm = (uc - u[id - 1]) * (wc2 + w[id - 1]) * 0.5f;
+        const float wlap = (fxp - fxm) + (fyp - fym) + (fzp - fzm);
+        const float u_new = uc + p->half_d * wlap + p->dt * (K[id] - 2.0f * Pm[id]) * uc * wc2;
+        u[id] = u_new * mk[id];
+        w[id] = w[id] * mk[id];
+      }
+}
+
+/* updateP_RB_WGSL (realqm_rb.js:318-353) for electron m on the cells of one colour, in place */
+void orc_rb_p(const orc_rb_params* p, int m, int color, float* P, const float* U, const float* rho) {
+  const int NN = p->NN, S = p->S;
+  const int64_t S2 = (int64_t)S * S, S3 = S2 * S;
+  float* Pm = P + m * S3;
+  const float* u = U + m * S3;
+  const float selfN = p->tgt[m];
+  const float selfFrac = selfN > 1.0f ? 1.0f / selfN : 1.0f;
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        if ((i + j + k) % 2 != color) continue;
+        const int64_t id = i * S2 + (int64_t)j * S + k;
+        const float Pc = Pm[id];
+        const float lap = Pm[id + S2] + Pm[id - S2] + Pm[id + S] + Pm[id - S] + Pm[id + 1] + Pm[id - 1] - 6.0f * Pc;
+        const float us = u[id];
+        const float ro = fmaxf(rho[id] - selfFrac * us * us, 0.0f);
+        Pm[id] = Pc + p->dt * (lap * p->inv_h2 + p->two_pi * ro);
+      }
+}
+
+/* reduceNormWGSL + normalizeWGSL (realqm_rb.js:356-422) for electron m: nwg workgroups of 128
+ * threads, each thread a grid-stride f32 sum over the interior, the workgroup tree, then the
+ * sequential f32 sum of the partials and the scale sqrt(tgt / norm).  Returns the norm. */
+float orc_rb_normalize(const orc_rb_params* p, int m, float* U) {
+  const int NN = p->NN, S = p->S;
+  const int64_t S2 = (int64_t)S * S, S3 = S2 * S;
+  const int64_t NM = NN - 1, tot = NM * NM * NM;
+  int64_t nwg = (tot + 127) / 128;
+  if (nwg > 256) nwg = 256;
+  const int64_t stride = nwg * 128;
+  float* u = U + m * S3;
+  float part[256];
+  for (int64_t wg = 0; wg < nwg; ++wg) {
+    float sd[128];
+    for (int lid = 0; lid < 128; ++lid) {
+      float acc = 0.0f;
+      for (int64_t cell = wg * 128 + lid; cell < tot; cell += stride) {
+        const int k = (int)(cell % NM) + 1, j = (int)((cell / NM) % NM) + 1, i = (int)(cell / (NM * NM)) + 1;
+        const float v = u[i * S2 + (int64_t)j * S + k];
+        acc += v * v * p->h3;
+      }
+      sd[lid] = acc;
+    }
+    for (int s = 64; s > 0; s >>= 1)
+      for (int lid = 0; lid < s; ++lid) sd[lid] += sd[lid + s];
+    part[wg] = sd[0];
+  }
+  float norm = 0.0f;
+  for (int64_t q = 0; q < nwg; ++q) norm += part[q];
+  if (norm > 0.0f) {
+    const float sc = sqrtf(p->tgt[m] / norm);
+    for (int i = 1; i < NN; ++i)
+      for (int j = 1; j < NN; ++j)
+        for (int k = 1; k < NN; ++k) u[i * S2 + (int64_t)j * S + k] *= sc;
+  }
+  return norm;
+}
+
+/* computeEnergy (realqm_rb.js:982-1045) in JS numbers (h, h3 the page's f64 spacing):
+ * out = {E_T, E_eK, E_ee} */
+void orc_rb_energy(const orc_rb_params* p, const float* U, const float* W, const float* P, const float* K, double h,
+                   double h3, double* out) {
+  const int NN = p->NN, S = p->S, n = p->n;
+  const int64_t S2 = (int64_t)S * S, S3 = S2 * S;
+  double ET = 0, EK = 0, EE = 0;
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        const int64_t id = i * S2 + (int64_t)j * S + k;
+        for (int m = 0; m < n; ++m) {
+          const float* u = U + m * S3;
+          const float* w = W + m * S3;
+          const double v = u[id], rho = v * v;
+          if (w[id] > 0.1) {
+            double g2 = 0;
+            if (w[id + S2] > 0.1) { const double g = u[id + S2] - v; g2 += g * g; }
+            if (w[id + S] > 0.1) { const double g = u[id + S] - v; g2 += g * g; }
+            if (w[id + 1] > 0.1) { const double g = u[id + 1] - v; g2 += g * g; }
+            ET += 0.5 * g2 * h;
+          }
+          EK += -(double)K[id] * rho * h3;
+          EE += (double)P[m * S3 + id] * rho * h3;
+        }
+      }
+  out[0] = ET; out[1] = EK; out[2] = EE;
+}
+
+/* the init shader (realqm_rb.js:104-186) run as runInitKernels does (:720-801): K accumulated
+ * nucleus by nucleus (f32), then each electron's u, w, P on its Voronoi cell (at most 8 rivals),
+ * split half and 3 bohr sphere.  nuc: nn records of 8 floats {i, j, k, Z, rc, ne, -, -};
+ * enuc: the nucleus of each electron.  U, W, P, K are zero on entry. */
+void orc_rb_init(const orc_rb_params* p, int nn, const float* nuc, const int32_t* enuc, float* K, float* U, float* W,
+                 float* P) {
+  const int NN = p->NN, S = p->S, n = p->n, N2 = p->N2;
+  const int64_t S2 = (int64_t)S * S, S3 = S2 * S;
+  for (int a = 0; a < nn; ++a) {
+    const float* c = nuc + 8 * a;
+    for (int i = 1; i < NN; ++i)
+      for (int j = 1; j < NN; ++j)
+        for (int k = 1; k < NN; ++k) {
+          const float dx = ((float)i - c[0]) * p->h, dy = ((float)j - c[1]) * p->h, dz = ((float)k - c[2]) * p->h;
+          const float r2 = dx * dx + dy * dy + dz * dz;
+          K[i * S2 + (int64_t)j * S + k] += c[3] / sqrtf(r2 + 1.2f * p->h2);
+        }
+  }
+  for (int m = 0; m < n; ++m) {
+    const int a = enuc[m];
+    const float* c = nuc + 8 * a;
+    int sib = 0;
+    for (int q = 0; q < m; ++q) sib += enuc[q] == a;
+    const int splitDir = (int)c[5] == 1 ? 2 : (sib == 0 ? 0 : 1);
+    float riv[8][3];
+    int nriv = 0;
+    for (int b = 0; b < nn && nriv < 8; ++b)
+      if (b != a) { riv[nriv][0] = nuc[8 * b]; riv[nriv][1] = nuc[8 * b + 1]; riv[nriv][2] = nuc[8 * b + 2]; ++nriv; }
+    for (int i = 1; i < NN; ++i)
+      for (int j = 1; j < NN; ++j)
+        for (int k = 1; k < NN; ++k) {
+          const int64_t id = i * S2 + (int64_t)j * S + k;
+          const float dx = ((float)i - c[0]) * p->h, dy = ((float)j - c[1]) * p->h, dz = ((float)k - c[2]) * p->h;
+          const float r2 = dx * dx + dy * dy + dz * dz;
+          const float r_soft = sqrtf(r2 + 1.2f * p->h2);
+          const float r_au = sqrtf(r2);
+          int inV = 1;
+          for (int q = 0; q < nriv; ++q) {
+            const float ex = ((float)i - riv[q][0]) * p->h, ey = ((float)j - riv[q][1]) * p->h,
+                        ez = ((float)k - riv[q][2]) * p->h;
+            if (r2 > ex * ex + ey * ey + ez * ez) inV = 0;
+          }
+          const int inRc = c[4] <= 0.0f || r_au < c[4];
+          const int inSplit = splitDir == 2 ? 1 : (splitDir == 0 ? (unsigned)i < (unsigned)(N2 - 1) : (unsigned)i > (unsigned)(N2 + 1));
+          const int inSph = r_au < 3.0f;
+          if (inV && inSplit && inRc && inSph) W[m * S3 + id] = 1.0f;
+          if (inV && inSplit && inSph) U[m * S3 + id] = (float)exp((double)(-0.5f * c[3] * r_soft));
+          P[m * S3 + id] = 0.5f / r_soft;
+        }
+  }
+}
+
+/* extractSliceWGSL (realqm_rb.js:429-457): per pixel (i, j) of the k = N2 plane, u, w, P of every
+ * electron then K; out has S*S*(3n+1) floats */
+void orc_rb_slice(const orc_rb_params* p, const float* U, const float* W, const float* P, const float* K, float* out) {
+  const int S = p->S, n = p->n, N1 = S;
+  const int64_t S2 = (int64_t)S * S, S3 = S2 * S;
+  const int stride = 3 * n + 1;
+  for (int g = 0; g < N1 * N1; ++g) {
+    const int j = g / N1, i = g % N1;
+    const int64_t id = i * S2 + (int64_t)j * S + p->N2;
+    for (int m = 0; m < n; ++m) {
+      out[(int64_t)g * stride + 3 * m] = U[m * S3 + id];
+      out[(int64_t)g * stride + 3 * m + 1] = W[m * S3 + id];
+      out[(int64_t)g * stride + 3 * m + 2] = P[m * S3 + id];
+    }
+    out[(int64_t)g * stride + stride - 1] = K[id];
+  }
+}

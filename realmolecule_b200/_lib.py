@@ -53,6 +53,15 @@ class MfNucleus(C.Structure):
                 ("split", C.c_int32), ("split_idx", C.c_int32), ("split_fix", C.c_int32), ("reserved", C.c_int32)]
 
 
+class RbConfig(C.Structure):
+    _fields_ = [("NN", C.c_int32), ("reserved0", C.c_int32), ("screen", C.c_double), ("reserved", C.c_int32 * 8)]
+
+
+class RbNucleus(C.Structure):
+    _fields_ = [("i", C.c_double), ("j", C.c_double), ("k", C.c_double), ("Z", C.c_double), ("rc", C.c_double),
+                ("rc_excl", C.c_double), ("ne", C.c_int32), ("reserved", C.c_int32)]
+
+
 class Config(C.Structure):
     _fields_ = [("NN", C.c_int32), ("flavor", C.c_int32), ("precision", C.c_int32), ("norm_interval", C.c_int32),
                 ("screen", C.c_double), ("dv", C.c_double), ("poisson_interval", C.c_int32),
@@ -142,6 +151,16 @@ SIGNATURES = {
     "rq_mf_upload": (C.c_int, [_V, _I, _P, _P, _P]),
     "rq_mf_download_K": (C.c_int, [_V, _P]),
     "rq_mf_info": (C.c_int, [_V, _P, _P]),
+    "rq_rb_create": (C.c_int, [_P, _P, _I, _P, _P]),
+    "rq_rb_destroy": (None, [_V]),
+    "rq_rb_last_error": (C.c_char_p, [_V]),
+    "rq_rb_step": (C.c_int, [_V, _I]),
+    "rq_rb_energy": (C.c_int, [_V, _P]),
+    "rq_rb_slice": (C.c_int, [_V, _P]),
+    "rq_rb_download": (C.c_int, [_V, _I, _P, _P, _P]),
+    "rq_rb_upload": (C.c_int, [_V, _I, _P, _P, _P]),
+    "rq_rb_download_K": (C.c_int, [_V, _P]),
+    "rq_rb_info": (C.c_int, [_V, _P, _P]),
     "rq_kernel_update_sp": (C.c_int, [_P, _P, _P, _P, _P, _I, _F, _F, _V]),
     "rq_kernel_jacobi_sp": (C.c_int, [_P, _P, _P, _I, _F, _F, _V]),
     "rq_kernel_labels_sp": (C.c_int, [_P, _P, _P, _I, _I, _F, _F, _V]),
