@@ -418,6 +418,35 @@ def caller_legs(a):
                          "cpu_sequential_ms_per_step": cpu_ms, "cpu_cores": 1,
                          "cpu": "the oracle's sequential restatement of atom.js (2 steps)"}
     out["mol_fast_ch4"] = mol_fast_leg(a)
+    out["realqm_rb_h2"] = realqm_rb_leg(a)
+    return out
+
+
+def realqm_rb_leg(a):
+    """realqm_rb.js's direct H2 page (NN = 100, 2 electrons, 10-step frames) through the drop-in
+    RealqmRb, against the oracle's restatement (the reference's per-electron passes) on the host."""
+    from realmolecule_b200 import configs
+    from realmolecule_b200.realqm_rb import RealqmRb
+    cfg = configs.realqm_rb_h2_page()
+    g = RealqmRb(**cfg)
+    g.doSteps(100)
+    steps = 3000
+    t0 = time.perf_counter()
+    g.doSteps(steps)
+    ms = (time.perf_counter() - t0) / steps * 1e3
+    E = g.computeEnergy()["E_tot"]
+    g.close()
+    out = {"grid": f"{cfg['NN']}^3", "electrons_fields": 2, "ms_per_step": ms, "steps": steps, "E_tot": E,
+           "timing": "host wall clock around doSteps(3000) (one CUDA graph, synchronised)"}
+    if not a.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        ref = orc.RealqmRbDriver(cfg["nuclei"], NN=cfg["NN"], screen=cfg["screen"], norm_targets=cfg["norm_targets"])
+        ref.initialize()
+        t0 = time.perf_counter()
+        ref.do_steps(20)
+        out.update({"cpu_ms_per_step": (time.perf_counter() - t0) / 20 * 1e3, "cpu_cores": 1,
+                    "cpu": "the oracle's sequential restatement of the passes (20 steps)"})
     return out
 
 

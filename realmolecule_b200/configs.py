@@ -254,4 +254,15 @@ def mol_fast_ch4_page(bond: float = 2.054, scr: float = 12.0) -> dict:
             "alpha_tf": 0.0, "dynamics": True}
 
 
+def realqm_rb_h2_page(sep: float = 1.4) -> dict:
+    """The direct H2 page of realqm_rb.js (h2_rb_direct.html:12-31): NN = 100, 8 bohr box, the
+    nuclei sep apart on the i axis, one electron each.  Keyword arguments of ``RealqmRb``."""
+    N, scr = 100, 8.0
+    h, N2 = scr / N, _js_round(N / 2)
+    dI = _js_round(sep / h / 2)
+    return {"nuclei": [{"i": N2 - dI, "j": N2, "k": N2, "Z": 1, "rc": 0, "ne": 1},
+                       {"i": N2 + dI, "j": N2, "k": N2, "Z": 1, "rc": 0, "ne": 1}],
+            "NN": N, "screen": scr, "nelec": 2, "norm_targets": [1, 1], "max_steps": 30000}
+
+
 WORKLOADS = {"h2o64": h2o64, "glycine128": glycine128, "water100": water100, "water1000": water1000}
