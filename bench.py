@@ -349,6 +349,7 @@ def run_ours(a):
 # seconds to converge: mixed / batched against plain FP64 (new flavour)
 # ---------------------------------------------------------------------------------------
 TOL, CHECK, MAX_STEPS = 1e-6, 100, 40000
+TIGHT_STEPS = 12000  # untimed continuation of the glycine solves for the precision comparison
 
 
 def _timed(stream, fn):
@@ -487,7 +488,7 @@ def mol_fast_leg(a):
 
 
 def converge_leg(stream, dist, rank, world):
-    from realmolecule_b200 import Context, configs
+    from realmolecule_b200 import Context, configs, _lib as L
     from realmolecule_b200.batch import Batch
     from realmolecule_b200 import shard
     out = {"criterion": f"|dE| < {TOL:g} Ha between checks {CHECK} steps apart (labels frozen after step 1)",
@@ -501,13 +502,31 @@ def converge_leg(stream, dist, rank, world):
         c = Context(g.NN, g.screen, rows, flavor="new", precision=prec, label_until=1)
         c.set_stream(stream.cuda_stream)
         (steps, E), t = _timed(stream, lambda: (c.initialize(), c.solve(TOL, MAX_STEPS, CHECK))[1])
+        # untimed: the same solves carried on far past the criterion; the mixed one first in fp32
+        # (where it stalls), then promoted to FP64 in place
+        extra = {}
+        if prec == "mixed":
+            c.step(TIGHT_STEPS // 2)
+            extra["E_fp32_stalled"] = float(c.energy()[L.E_TOTAL])
+            c.promote()
+            c.step(TIGHT_STEPS // 2)
+        else:
+            c.step(TIGHT_STEPS)
+        extra["E"] = float(c.energy()[L.E_TOTAL])
+        gly[prec] = (_max_over_ranks(dist, t), int(steps), float(E), extra)
         c.close()
-        gly[prec] = (_max_over_ranks(dist, t), int(steps), float(E))
     out["glycine128"] = {"electrons": int(g.charges.sum()), "grid": f"{g.NN}^3 h={g.h}",
                          "mixed_s": gly["mixed"][0], "fp64_s": gly["fp64"][0],
                          "steps_mixed": gly["mixed"][1], "steps_fp64": gly["fp64"][1],
                          "E_mixed": gly["mixed"][2], "E_fp64": gly["fp64"][2],
-                         "abs_dE_Ha": abs(gly["mixed"][2] - gly["fp64"][2])}
+                         "abs_dE_Ha": abs(gly["mixed"][2] - gly["fp64"][2]),
+                         "tight": {"extra_steps": TIGHT_STEPS, "E_fp64": gly["fp64"][3]["E"],
+                                   "E_mixed_fp32_stalled": gly["mixed"][3]["E_fp32_stalled"],
+                                   "E_mixed_then_fp64": gly["mixed"][3]["E"],
+                                   "abs_dE_Ha_fp32_stalled": abs(gly["mixed"][3]["E_fp32_stalled"] - gly["fp64"][3]["E"]),
+                                   "abs_dE_Ha_mixed_then_fp64": abs(gly["mixed"][3]["E"] - gly["fp64"][3]["E"]),
+                                   "note": "untimed continuation past the criterion: the FP64 solve and the mixed "
+                                           "solve (fp32 for half, where it stalls, then promoted to FP64)"}}
 
     # 96 water clusters: this rank's cost share, mixed batch vs one FP64 context per instance
     geoms = configs.clusters96()

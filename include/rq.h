@@ -200,6 +200,11 @@ RQ_API int rq_forces(rq_ctx* ctx, int32_t method, double* F);
  * cloud/solver.py:462-474, :504-520 and molecule.js:3170-3185, :3218-3242). */
 RQ_API int rq_nuclear_terms(rq_ctx* ctx, double* E_KK, double* F /* n_atoms x 3 or NULL */);
 /* Step until |E_n - E_{n-1}| < tol_dE between checks every check_interval steps. */
+/* No counterpart in the reference.  New flavour, RQ_PREC_MIXED: continue in FP64 from the current
+ * state (psi and P widened, K recomputed in FP64); the context is RQ_PREC_FP64 afterwards.  fp32
+ * fields stop resolving the energy at a few 1e-8 |E|; a mixed solve followed by this and more
+ * steps reaches the FP64 fixed point.  No-op on an FP64 context; RQ_ENOTSUP for other flavours. */
+RQ_API int rq_promote(rq_ctx* ctx);
 RQ_API int rq_solve(rq_ctx* ctx, double tol_dE, int32_t max_steps, int32_t check_interval, int32_t* steps_taken,
              double* E_final);
 RQ_API int rq_synchronize(rq_ctx* ctx);

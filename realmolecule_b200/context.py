@@ -131,6 +131,11 @@ class Context:
         arr = None if v is None else np.ascontiguousarray(np.asarray(v, np.float64).reshape(-1))
         self._chk(self.lib.rq_set_external_potential(self.ctx, _ptr(arr)), "rq_set_external_potential")
 
+    def promote(self):
+        """New flavour: continue in FP64 from the current mixed-precision state (rq_promote)."""
+        self._chk(self.lib.rq_promote(self.ctx), "rq_promote")
+        self.fp64 = True
+
     def solve(self, tol_dE: float, max_steps: int, check_interval: int = 100):
         taken = C.c_int32()
         e = C.c_double()

@@ -763,6 +763,14 @@ extern "C" int rq_forces(rq_ctx* c, int32_t method, double* F) {
   return nm_forces(c, method, F);
 }
 
+extern "C" int rq_promote(rq_ctx* c) {
+  if (!c) return RQ_EINVAL;
+  if (c->cfg.flavor != RQ_FLAVOR_NEW) return rq_fail(c, RQ_ENOTSUP, "promotion to FP64 is for the new flavour");
+  const int rc = nm_promote(c);
+  if (rc == RQ_OK) c->cfg.precision = RQ_PREC_FP64;
+  return rc;
+}
+
 extern "C" int rq_solve(rq_ctx* c, double tol_dE, int32_t max_steps, int32_t check_interval, int32_t* steps_taken,
                         double* E_final) {
   if (!c || max_steps < 0 || check_interval <= 0) return RQ_EINVAL;

@@ -242,6 +242,62 @@ static int nm_init_t(rq_ctx* c) {
 
 int nm_initialize(rq_ctx* c) { return c->fp64 ? nm_init_t<double>(c) : nm_init_t<float>(c); }
 
+__global__ void __launch_bounds__(256) k_nm_widen(const float* __restrict__ a, double* __restrict__ d, long long n) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    d[q] = (double)a[q];
+}
+
+// Switch a mixed-precision context to FP64 in place, keeping the state it holds: psi (after its
+// pending normalisation) and P are widened, K is recomputed in FP64, the multigrid levels are
+// reallocated in FP64 and the captured schedule graphs are dropped.  fp32 fields stop resolving
+// the energy at a few 1e-8 |E| (updates below half an ulp round away); continuing in FP64 from
+// there reaches the FP64 fixed point.
+int nm_promote(rq_ctx* c) {
+  if (c->fp64) return RQ_OK;
+  int rc = nm_flush(c);
+  if (rc != RQ_OK) return rc;
+  const long long n = c->g.S3;
+  const size_t bytes = sizeof(double) * (size_t)n;
+  void* nb[6] = {};  // U0, U1, P0, P1, K, Kext
+  void* old[6] = {c->U[0], c->U[1], c->P[0], c->P[1], c->K, c->Kext};
+  for (int q = 0; q < 6; ++q) {
+    if (!old[q]) continue;
+    if (cudaMalloc(&nb[q], bytes) != cudaSuccess) {
+      for (void* p : nb)
+        if (p) cudaFree(p);
+      return rq_cuda(c, cudaErrorMemoryAllocation, "promotion to FP64");
+    }
+    if (q != 4) {  // K is recomputed below
+      k_nm_widen<<<148 * 4, 256, 0, c->st>>>((const float*)old[q], (double*)nb[q], n);
+      CK(cudaGetLastError());
+      c->launches++;
+    }
+  }
+  CK(cudaStreamSynchronize(c->st));
+  for (void* p : old)
+    if (p) cudaFree(p);
+  c->U[0] = nb[0]; c->U[1] = nb[1]; c->P[0] = nb[2]; c->P[1] = nb[3]; c->K = nb[4]; c->Kext = nb[5];
+  for (size_t l = 0; l < c->mg.size(); ++l) {
+    rq_mg_level& L = c->mg[l];
+    const size_t lb = sizeof(double) * (size_t)L.g.S3;
+    for (void** p : {&L.P, &L.f, &L.r}) {
+      if (!*p) continue;
+      cudaFree(*p);
+      *p = nullptr;
+      if (cudaMalloc(p, lb) != cudaSuccess) return rq_cuda(c, cudaErrorMemoryAllocation, "FP64 multigrid levels");
+      CK(cudaMemsetAsync(*p, 0, lb, c->st));
+    }
+  }
+  c->fp64 = true;
+  for (auto& gx : c->graph)
+    if (gx) {
+      cudaGraphExecDestroy(gx);
+      gx = nullptr;
+    }
+  if ((rc = nm_potential_t<double>(c)) != RQ_OK) return rc;
+  return cudaStreamSynchronize(c->st) == cudaSuccess ? RQ_OK : rq_cuda(c, cudaGetLastError(), "promotion to FP64");
+}
+
 void nm_nuclear_terms(rq_ctx* c, double* E, double* F) {
   // point-charge nuclear repulsion between entries with Z_nuc > 0 (bohr)
   double e = 0;

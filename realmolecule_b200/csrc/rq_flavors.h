@@ -21,6 +21,7 @@ void mj_nuclear_terms(rq_ctx* c, double* E, double* F);
 // new flavour (nm_flavor.cu)
 int nm_alloc_levels(rq_ctx* c);
 int nm_initialize(rq_ctx* c);
+int nm_promote(rq_ctx* c);  // mixed -> FP64 in place (psi, P widened; K recomputed)
 int nm_step_one(rq_ctx* c, int s);
 int nm_energy(rq_ctx* c, double* out, double* per_domain);
 int nm_forces(rq_ctx* c, int method, double* F);

@@ -260,3 +260,33 @@ class MolFast:
         n, t = C.c_int64(), C.c_int64()
         self._chk(self.lib.rq_mf_info(self.s, C.byref(n), C.byref(t)), "rq_mf_info")
         return n.value
+
+
+def _main(argv=None):
+    """Run a mol_fast.js page (realmolecule_b200.configs) on cuda:0.
+
+    python -m realmolecule_b200.mol_fast [--page ch4|h2] [--steps K] [--frames F]
+    Prints the energies after F frames of K steps (each followed by computeForces)."""
+    import argparse
+    import time
+
+    from . import configs
+    ap = argparse.ArgumentParser(description=_main.__doc__)
+    ap.add_argument("--page", default="ch4", choices=["ch4", "h2"])
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--frames", type=int, default=1)
+    a = ap.parse_args(argv)
+    cfg = configs.mol_fast_ch4_page() if a.page == "ch4" else configs.mol_fast_h2_page()
+    mf = MolFast(**cfg)
+    t0 = time.perf_counter()
+    for _ in range(a.frames):
+        mf.doSteps(a.steps)
+        mf.computeForces()
+    dt = time.perf_counter() - t0
+    print({**mf.energies(), "steps": a.steps * a.frames, "ms_per_step": dt / max(1, a.steps * a.frames) * 1e3},
+          flush=True)
+    mf.close()
+
+
+if __name__ == "__main__":
+    _main()

@@ -147,3 +147,27 @@ class RealqmRb:
         n, t = C.c_int64(), C.c_int64()
         self._chk(self.lib.rq_rb_info(self.s, C.byref(n), C.byref(t)), "rq_rb_info")
         return n.value
+
+
+def _main(argv=None):
+    """Run realqm_rb.js's direct H2 page (realmolecule_b200.configs.realqm_rb_h2_page) on cuda:0.
+
+    python -m realmolecule_b200.realqm_rb [--steps K]
+    Prints the energies after K steps."""
+    import argparse
+    import time
+
+    from . import configs
+    ap = argparse.ArgumentParser(description=_main.__doc__)
+    ap.add_argument("--steps", type=int, default=100)
+    a = ap.parse_args(argv)
+    g = RealqmRb(**configs.realqm_rb_h2_page())
+    t0 = time.perf_counter()
+    g.doSteps(a.steps)
+    dt = time.perf_counter() - t0
+    print({**g.computeEnergy(), "steps": a.steps, "ms_per_step": dt / max(1, a.steps) * 1e3}, flush=True)
+    g.close()
+
+
+if __name__ == "__main__":
+    _main()

@@ -104,6 +104,30 @@ def test_mixed_matches_fp64_converged_energy():
     assert abs(E["mixed"] - E["fp64"]) <= 1e-6 * abs(E["fp64"]), E
 
 
+def test_promoted_mixed_solve_reaches_the_fp64_fixed_point():
+    """fp32 fields stall a few 1e-8 |E| above the FP64 fixed point; continuing in FP64 from the
+    mixed state (rq_promote) reaches it."""
+    NN, scr, rows = water_rows()
+    ref = ctx_for(NN, scr, rows, precision="fp64", label_until=1)
+    ref.initialize()
+    ref.step(6000)
+    E64 = float(ref.energy()[0])
+    ref.close()
+    ctx = ctx_for(NN, scr, rows, precision="mixed", label_until=1)
+    ctx.initialize()
+    ctx.step(2000)
+    psi32 = ctx.download(psi=True)["psi"]
+    ctx.promote()
+    assert ctx.fp64
+    psi64 = ctx.download(psi=True)["psi"]
+    assert psi64.dtype == np.float64 and np.array_equal(psi64.astype(np.float32), psi32)
+    ctx.step(4000)
+    E = float(ctx.energy()[0])
+    ctx.promote()  # a no-op on an FP64 context
+    ctx.close()
+    assert abs(E - E64) <= 1e-9 * abs(E64), (E, E64)
+
+
 def test_adjoint_force_matches_finite_differences():
     from realmolecule_b200 import _lib as L
     NN, scr, rows = h2_rows()
