@@ -200,6 +200,10 @@ RQ_API int rq_forces(rq_ctx* ctx, int32_t method, double* F);
  * cloud/solver.py:462-474, :504-520 and molecule.js:3170-3185, :3218-3242). */
 RQ_API int rq_nuclear_terms(rq_ctx* ctx, double* E_KK, double* F /* n_atoms x 3 or NULL */);
 /* Step until |E_n - E_{n-1}| < tol_dE between checks every check_interval steps. */
+/* molecule.js flavour: extractWGSL (molecule.js:1108-1192, W_CUTOFF = 0) as a headless buffer of
+ * 3 S^2 + 2 S floats -- u^2 on the slice k = slice_k, label + 1000 Z of the label, boundary flags,
+ * then the K line and the w line along (i, slice_k, slice_k).  1 <= slice_k < NN. */
+RQ_API int rq_extract(rq_ctx* ctx, int32_t slice_k, float* out);
 /* No counterpart in the reference.  New flavour, RQ_PREC_MIXED: continue in FP64 from the current
  * state (psi and P widened, K recomputed in FP64); the context is RQ_PREC_FP64 afterwards.  fp32
  * fields stop resolving the energy at a few 1e-8 |E|; a mixed solve followed by this and more

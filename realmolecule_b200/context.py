@@ -131,6 +131,13 @@ class Context:
         arr = None if v is None else np.ascontiguousarray(np.asarray(v, np.float64).reshape(-1))
         self._chk(self.lib.rq_set_external_potential(self.ctx, _ptr(arr)), "rq_set_external_potential")
 
+    def extract(self, slice_k: int | None = None) -> np.ndarray:
+        """molecule.js flavour: the page's slice buffer (3 S^2 + 2 S floats) at k = slice_k (N2)."""
+        k = self.NN // 2 if slice_k is None else int(slice_k)
+        out = np.empty(3 * self.S * self.S + 2 * self.S, np.float32)
+        self._chk(self.lib.rq_extract(self.ctx, k, out.ctypes.data), "rq_extract")
+        return out
+
     def promote(self):
         """New flavour: continue in FP64 from the current mixed-precision state (rq_promote)."""
         self._chk(self.lib.rq_promote(self.ctx), "rq_promote")

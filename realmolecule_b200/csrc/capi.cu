@@ -763,6 +763,24 @@ extern "C" int rq_forces(rq_ctx* c, int32_t method, double* F) {
   return nm_forces(c, method, F);
 }
 
+extern "C" int rq_extract(rq_ctx* c, int32_t slice_k, float* out) {
+  if (!c || !out) return RQ_EINVAL;
+  if (c->cfg.flavor != RQ_FLAVOR_MOLECULE_JS) return rq_fail(c, RQ_ENOTSUP, "the slice buffer is molecule.js's");
+  if (slice_k < 1 || slice_k >= c->g.NN) return rq_fail(c, RQ_EINVAL, "slice_k outside the interior");
+  const size_t S = (size_t)c->g.S, n = 3 * S * S + 2 * S;
+  float* d = nullptr;
+  CK(cudaMallocAsync((void**)&d, n * sizeof(float), c->st));
+  cudaError_t e = launch_mj_extract((const float*)c->U[c->cu], c->lab[c->cl], (const float*)c->K,
+                                    (const MjAtom*)c->atoms_mj, c->n_atoms, c->g, slice_k, d, c->st);
+  if (e == cudaSuccess) {
+    c->launches++;
+    e = cudaMemcpyAsync(out, d, n * sizeof(float), cudaMemcpyDeviceToHost, c->st);
+  }
+  cudaFreeAsync(d, c->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+  return e == cudaSuccess ? RQ_OK : rq_cuda(c, e, "rq_extract");
+}
+
 extern "C" int rq_promote(rq_ctx* c) {
   if (!c) return RQ_EINVAL;
   if (c->cfg.flavor != RQ_FLAVOR_NEW) return rq_fail(c, RQ_ENOTSUP, "promotion to FP64 is for the new flavour");

@@ -735,3 +735,59 @@ cudaError_t launch_unpack_labels(const int* in, int* out, long long n, cudaStrea
   return cudaGetLastError();
 }
 }  // namespace rq
+
+namespace rq {
+
+// extractWGSL (molecule.js:1108-1192) with W_CUTOFF = 0 (:84): out = u^2 on the slice k = sk,
+// label + 1000 Z of the label, the boundary flags (1 a boundary with density on a side, 2 one
+// without), then the K line and the w line along (i, sk, sk)
+__global__ void __launch_bounds__(256) k_mj_extract(const float* __restrict__ U, const int* __restrict__ label,
+                                                    const float* __restrict__ K, const MjAtom* __restrict__ atoms,
+                                                    int nAt, Geo g, int sk, float* __restrict__ out) {
+  const int i = blockIdx.x * 16 + threadIdx.x, j = blockIdx.y * 16 + threadIdx.y;
+  const int NN = g.S - 1;
+  const long long SS = g.S, S2 = g.S2;
+  if (i > NN || j > NN) return;
+  if (j == 0) {
+    out[3 * SS * SS + i] = K[(long long)i * S2 + (long long)sk * SS + sk];
+    out[3 * SS * SS + SS + i] = 1.0f;
+  }
+  if (i < 1 || i >= NN || j < 1 || j >= NN) {
+    out[i * SS + j] = 0.0f;
+    out[SS * SS + i * SS + j] = 0.0f;
+    out[2 * SS * SS + i * SS + j] = 0.0f;
+    return;
+  }
+  const long long idx = (long long)i * S2 + (long long)j * SS + sk;
+  const float u = U[idx];
+  const int lbl = label[idx] & kMjMask;  // the stored label carries the exclusion bit
+  const float Zl = (lbl >= 0 && lbl < nAt) ? atoms[lbl].Z : 0.0f;
+  const float dens = __fmul_rn(u, u);
+  out[i * SS + j] = dens;
+  out[SS * SS + i * SS + j] = __fadd_rn((float)(unsigned)lbl, __fmul_rn(Zl, 1000.0f));
+  float bnd = 0.0f;
+  if (i > 1 && i < NN - 1) {
+    const long long nb = idx + S2;
+    if (lbl != (label[nb] & kMjMask)) {
+      const float nd = __fmul_rn(U[nb], U[nb]);
+      bnd = (dens > 1e-6f || nd > 1e-6f) ? 1.0f : 2.0f;
+    }
+  }
+  if (bnd < 1.5f && j > 1 && j < NN - 1) {
+    const long long nb = idx + SS;
+    if (lbl != (label[nb] & kMjMask)) {
+      const float nd = __fmul_rn(U[nb], U[nb]);
+      bnd = (dens > 1e-6f || nd > 1e-6f) ? fmaxf(bnd, 1.0f) : 2.0f;
+    }
+  }
+  out[2 * SS * SS + i * SS + j] = bnd;
+}
+
+cudaError_t launch_mj_extract(const float* U, const int* label, const float* K, const MjAtom* atoms, int nAt,
+                              const Geo& g, int sk, float* out, cudaStream_t st) {
+  const unsigned b = (unsigned)((g.S + 15) / 16);
+  k_mj_extract<<<dim3(b, b), dim3(16, 16), 0, st>>>(U, label, K, atoms, nAt, g, sk, out);
+  return cudaGetLastError();
+}
+
+}  // namespace rq

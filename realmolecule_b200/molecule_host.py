@@ -1,0 +1,361 @@
+"""The host side of a molecule.js page around the GPU step (molecule.js flavour of librq).
+
+molecule.js runs its frames on the GPU and everything else in the page's JavaScript: the frame
+loop and its convergence monitor (draw, molecule.js:4584-4671), the nuclear forces (the GPU's
+Hartree gradient plus the softened repulsion of the unique nuclei, :3205-3259), the nuclear
+integrator with its restraints and thermostats (moveNuclei, :3742-4583), the warm K rebuild
+after a move, and the restarts (restartWithPositions / activateAtoms, :2127-2195).
+``MoleculePage`` is that host over a ``Context(flavor="molecule.js")``; option names follow the
+page's ``window.USER_*`` globals.  Positions are grid coordinates (i, j, k).
+
+Kept from moveNuclei: user external forces, hinge atoms, bond-length and H-O-H angle
+restraints, coincident groups, rigid groups, frozen atoms, the shear body force, overdamped
+Brownian motion and the Andersen thermostat (a seeded generator stands in for Math.random).
+Not kept: the coarse-grained classical-MD backbone (USER_CLASSICAL_MD / USER_ELASTIC_BACKBONE)
+and the fold-force diagnostics, which only log.
+"""
+from __future__ import annotations
+
+import math
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import _lib as L
+from .context import Context
+
+_MASS = {1: 1, 2: 16, 3: 14, 4: 12}
+
+
+def nuc_mass(z: float) -> float:
+    """molecule.js:152 -- mass by valence charge (H, O, N, C pseudo-atoms) in electron masses."""
+    return _MASS.get(z, 1) * 1836
+
+
+class MoleculePage:
+    def __init__(self, atoms: Sequence[dict], NN: int = 100, screen: float = 10.0, steps_per_frame: Optional[int] = None,
+                 total_steps: int = 20000, n_move: int = 10, dynamics: bool = False, dt_nuc: Optional[float] = None,
+                 nuc_substeps: Optional[int] = None, damping: float = 0.98, force_scale: float = 1.0,
+                 langevin_kT: float = 0.0, langevin_gamma: float = 0.01, no_nuc_repulsion: bool = False,
+                 no_auto_dynamics: bool = False, convergence_threshold: Optional[float] = None,
+                 external_force=None, hinge_atoms=(), frozen_atoms=(), bond_constraints=(), water_triplets=(),
+                 hoh_eq: float = 104.5, bend_k: float = 1.5, coincident_groups=(), rigid_groups=None,
+                 shear_rate: float = 0.0, brownian: bool = False, brownian_gamma: float = 1.0,
+                 thermal_kick: Optional[float] = None, seed: int = 0, context=None, **ctx_opts):
+        self.rows = [dict(a) for a in atoms]
+        n = self.n = len(self.rows)
+        self.NN, self.screen = int(NN), float(screen)
+        self.h = self.screen / self.NN
+        self.Z_orig = [float(a.get("Z", 0.0)) for a in self.rows]
+        self.Z_nuc = [float(a["Z_nuc"]) if a.get("Z_nuc") is not None else float(a.get("Z", 0.0)) for a in self.rows]
+        self.Z = list(self.Z_orig)
+        self.mol_pos = [[float(a["i"]), float(a["j"]), float(a.get("k", self.NN // 2))] for a in self.rows]
+        self.pos = [list(p) for p in self.mol_pos]
+        # molecule.js:106, :116-121 -- defaults by the number of entries
+        self.spf = steps_per_frame or (50 if n <= 30 else 5 if n <= 100 else 2)
+        self.total_steps, self.n_move = int(total_steps), int(n_move)
+        self.dt_nuc = dt_nuc or (2.0 if n <= 5 else 0.2 if n > 200 else 0.8)
+        self.substeps = nuc_substeps or (2 if n <= 5 else 1)
+        self.damping, self.force_scale = float(damping), float(force_scale)
+        self.max_vel = 0.3 if n <= 5 else 0.03 if n > 200 else 0.1
+        self.langevin_kT, self.langevin_gamma = float(langevin_kT), float(langevin_gamma)
+        self.add_nuc_repulsion = not no_nuc_repulsion
+        self.no_auto_dynamics = bool(no_auto_dynamics)
+        self.convergence_threshold = convergence_threshold
+        self.dynamics = bool(dynamics)
+        self.external_force = external_force
+        self.hinge_atoms, self.frozen_atoms = list(hinge_atoms), set(frozen_atoms)
+        self.bond_constraints, self.water_triplets = list(bond_constraints), list(water_triplets)
+        self.hoh_eq, self.bend_k = float(hoh_eq), float(bend_k)
+        self.coincident_groups, self.rigid_groups = list(coincident_groups), rigid_groups
+        self.shear_rate, self.brownian, self.brownian_gamma = float(shear_rate), bool(brownian), float(brownian_gamma)
+        self.thermal_kick = thermal_kick
+        self.rng = np.random.default_rng(seed)
+        self._unique_nuclei()
+        # `context`: an object with the Context methods used here (tests drive the host logic with one)
+        self.ctx = context if context is not None else Context(self.NN, self.screen, self._ctx_rows(),
+                                                               flavor="molecule.js", steps_per_frame=self.spf,
+                                                               **ctx_opts)
+        self._reset_counters()
+        self.nuc_vel = [[0.0, 0.0, 0.0] for _ in range(n)]
+        self.nuc_force = [[0.0, 0.0, 0.0] for _ in range(n)]
+        self.nuc_force_total = [[0.0, 0.0, 0.0] for _ in range(n)]
+        self.nuc_steps = 0
+
+    # ---- set-up ---------------------------------------------------------------------------------
+    def _unique_nuclei(self):
+        """molecule.js:50-66 -- entries at one site share one nucleus of charge sum(Z_nuc || Z)."""
+        sites: Dict[tuple, dict] = {}
+        for e, a in enumerate(self.rows):
+            if self.Z_orig[e] == 0 and self.Z_nuc[e] == 0:
+                continue
+            key = (a["i"], a["j"], a.get("k", self.NN // 2))
+            q = self.Z_nuc[e] or self.Z_orig[e]
+            if key in sites:
+                sites[key]["Z_eff"] += q
+                sites[key]["elec"].append(e)
+            else:
+                sites[key] = {"Z_eff": q, "elec": [e]}
+        self.unique = list(sites.values())
+
+    def _ctx_rows(self):
+        rows = []
+        for e, a in enumerate(self.rows):
+            r = dict(a)
+            r["i"], r["j"], r["k"] = self.pos[e]
+            r["Z"], r["Z_nuc"] = self.Z[e], self.Z_nuc[e] if self.Z[e] or self.Z_nuc[e] else 0.0
+            rows.append(r)
+        return rows
+
+    def _reset_counters(self):
+        self.tStep = self.phase_steps = self.frame_count = 0
+        self.E_min = math.inf
+        self.phase = 0
+        self._prevE = None
+        self._conv_count = 0
+        self.converged_at = None
+
+    def initialize(self):
+        """uploadInitialData on the device."""
+        self.ctx.initialize()
+        self._reset_counters()
+
+    # ---- the frame loop -------------------------------------------------------------------------
+    def frame(self) -> Dict:
+        """One draw() tick (molecule.js:4612-4671): a frame of steps, the energies, the nuclear forces
+        when a force step fell in the frame (every N_MOVE steps, :2997-3004) and, with dynamics on,
+        moveNuclei; then the auto-dynamics, convergence and end-of-run checks."""
+        if self.phase != 0:
+            return self.energies()
+        t0 = self.tStep
+        self.ctx.step(self.spf)
+        self.tStep += self.spf
+        e = self.ctx.energy()
+        self.E, self.E_T, self.E_eK, self.E_ee, self.E_KK = (float(e[L.E_TOTAL]), float(e[L.E_T]), float(e[L.E_EK]),
+                                                             float(e[L.E_EE]), float(e[L.E_KK]))
+        # forces are read on the frame's final state: the reference's last force step of the frame is
+        # its final step whenever frames end on multiples of N_MOVE (every default frame length)
+        if any((t0 + s + 1) % self.n_move == 0 for s in range(self.spf)):
+            self._forces()
+            if self.dynamics:
+                self.move_nuclei()
+        self.phase_steps += self.spf
+        self.frame_count += 1
+        if math.isfinite(self.E) and self.E < self.E_min:
+            self.E_min = self.E
+        if (not self.dynamics and self.convergence_threshold is None and not self.no_auto_dynamics
+                and self.phase_steps >= 10000):
+            self.dynamics = True
+        if not self.dynamics and self.convergence_threshold is not None and self.phase_steps > 200:
+            if self._prevE is not None and abs(self.E - self._prevE) < self.convergence_threshold and math.isfinite(self.E):
+                self._conv_count += 1
+                if self._conv_count >= 3:  # 3 consecutive frames within the threshold
+                    self.phase = 1
+                    self._conv_count = 0
+                    self.converged_at = self.phase_steps
+            else:
+                self._conv_count = 0
+            self._prevE = self.E
+        if not self.dynamics and self.phase_steps >= self.total_steps:
+            self.phase = 1
+        return self.energies()
+
+    def energies(self) -> Dict:
+        return {k: getattr(self, k, None) for k in ("E", "E_T", "E_eK", "E_ee", "E_KK", "E_min", "phase_steps", "phase")}
+
+    def _forces(self):
+        """molecule.js:3205-3258: the GPU force per entry plus the softened repulsion of the unique
+        nuclei (applied to every entry of a site); hinge atoms show no force."""
+        F = self.ctx.forces(L.FORCE_GRADP)
+        n, h = self.n, self.h
+        self.nuc_force_elec = [[0.0] * 3 if (self.Z[a] == 0 and self.Z_nuc[a] == 0) else [float(v) for v in F[a]]
+                               for a in range(n)]
+        self.nuc_force_nuc = [[0.0, 0.0, 0.0] for _ in range(n)]
+        if self.add_nuc_repulsion:
+            for A in self.unique:
+                ea = A["elec"][0]
+                f = self._site_repulsion(A, ea)
+                for e in A["elec"]:
+                    self.nuc_force_nuc[e] = list(f)
+        for a in range(n):
+            if self.Z[a] == 0 and self.Z_nuc[a] == 0:
+                continue
+            self.nuc_force_total[a] = [self.nuc_force_elec[a][d] + self.nuc_force_nuc[a][d] for d in range(3)]
+        for a in self.hinge_atoms:
+            if a < n:
+                self.nuc_force_total[a] = [0.0, 0.0, 0.0]
+
+    def _site_repulsion(self, A, ea):
+        fx = fy = fz = 0.0
+        h = self.h
+        for B in self.unique:
+            if B is A:
+                continue
+            eb = B["elec"][0]
+            dx = (self.pos[ea][0] - self.pos[eb][0]) * h
+            dy = (self.pos[ea][1] - self.pos[eb][1]) * h
+            dz = (self.pos[ea][2] - self.pos[eb][2]) * h
+            r2 = dx * dx + dy * dy + dz * dz + h * h
+            r = math.sqrt(r2)
+            inv_r3 = 1.0 / (r * r2)
+            q = A["Z_eff"] * B["Z_eff"]
+            fx += q * dx * inv_r3
+            fy += q * dy * inv_r3
+            fz += q * dz * inv_r3
+        return fx, fy, fz
+
+    # ---- moveNuclei -------------------------------------------------------------------------------
+    def move_nuclei(self):
+        """moveNuclei (molecule.js:3742-4583) without the classical-MD backbone; then the warm K rebuild
+        (the converged psi, labels and P are kept)."""
+        n, h, NN = self.n, self.h, self.NN
+        F = [[0.0] * 3 if self.Z[a] == 0 else list(self.nuc_force_elec[a]) for a in range(n)]
+        if self.add_nuc_repulsion:
+            for A in self.unique:
+                f = self._site_repulsion(A, A["elec"][0])
+                for e in A["elec"]:
+                    F[e] = [F[e][0] + f[0], F[e][1] + f[1], F[e][2] + f[2]]
+        if self.external_force:
+            for a, f in enumerate(self.external_force[:n]):
+                if f:
+                    for d in range(3):
+                        F[a][d] += f[d] or 0
+                        self.nuc_force_total[a][d] += f[d] or 0
+        for a in self.hinge_atoms:
+            if a < n:
+                F[a] = [0.0, 0.0, 0.0]
+        pos = self.pos
+        for i1, i2, r0, kb in self.bond_constraints:  # :4331-4346
+            rx, ry, rz = ((pos[i1][d] - pos[i2][d]) * h for d in range(3))
+            r = math.sqrt(rx * rx + ry * ry + rz * rz)
+            if r < 1e-8:
+                continue
+            u = (rx / r, ry / r, rz / r)
+            f = -kb * (r - r0)
+            for d in range(3):
+                F[i1][d] += f * u[d]
+                F[i2][d] -= f * u[d]
+        th0 = self.hoh_eq * math.pi / 180
+        for o, h1, h2 in self.water_triplets:  # :4350-4385
+            r1 = [(pos[h1][d] - pos[o][d]) * h for d in range(3)]
+            r3 = [(pos[h2][d] - pos[o][d]) * h for d in range(3)]
+            d1, d3 = math.sqrt(sum(x * x for x in r1)), math.sqrt(sum(x * x for x in r3))
+            if d1 < 1e-6 or d3 < 1e-6:
+                continue
+            u1, u3 = [x / d1 for x in r1], [x / d3 for x in r3]
+            cos = min(0.9999, max(-0.9999, u1[0] * u3[0] + u1[1] * u3[1] + u1[2] * u3[2]))
+            th = math.acos(cos)
+            s = math.sin(th)
+            if s < 1e-6:
+                continue
+            c = self.bend_k * (th - th0) / s
+            f1 = [c * (u3[d] - cos * u1[d]) / d1 for d in range(3)]
+            f3 = [c * (u1[d] - cos * u3[d]) / d3 for d in range(3)]
+            for d in range(3):
+                F[h1][d] += f1[d]
+                F[h2][d] += f3[d]
+                F[o][d] -= f1[d] + f3[d]
+        for grp in self.coincident_groups:  # :4390-4403
+            g0 = grp[0]
+            for gm in grp[1:]:
+                for d in range(3):
+                    F[g0][d] += F[gm][d]
+                F[gm] = [0.0, 0.0, 0.0]
+        self.nuc_force = F
+        clamp = lambda x: max(5.0, min(NN - 5.0, x))
+        for _ in range(self.substeps):
+            if self.rigid_groups:
+                for grp in self.rigid_groups:
+                    g = [0.0, 0.0, 0.0]
+                    M = 0.0
+                    for a in grp:
+                        if a >= n or self.Z[a] == 0:
+                            continue
+                        for d in range(3):
+                            g[d] += F[a][d]
+                        M += nuc_mass(self.Z[a])
+                    if M == 0:
+                        continue
+                    v = self.nuc_vel[grp[0]]
+                    for d in range(3):
+                        v[d] += g[d] / M * self.dt_nuc * self.force_scale
+                        if self.langevin_kT <= 0:
+                            v[d] *= self.damping
+                        v[d] = max(-self.max_vel, min(self.max_vel, v[d]))
+                    for a in grp:
+                        if a >= n or self.Z[a] == 0:
+                            continue
+                        for d in range(3):
+                            pos[a][d] = clamp(pos[a][d] + v[d] * self.dt_nuc / h)
+                continue
+            movable = [a for a in range(n) if not (self.Z[a] == 0 and self.Z_nuc[a] == 0) and a not in self.frozen_atoms]
+            yc = (sum(pos[a][1] for a in movable) / len(movable)) if (self.shear_rate and movable) else 0.0
+            for a in movable:
+                m = nuc_mass(self.Z_nuc[a] or self.Z[a])
+                if self.shear_rate:
+                    fs = m * self.shear_rate * (pos[a][1] - yc) * h
+                    F[a][0] += fs
+                    self.nuc_force_total[a][0] += fs
+                if self.brownian:
+                    drift = self.dt_nuc * self.force_scale / self.brownian_gamma
+                    noise = math.sqrt(2 * max(self.langevin_kT, 0) * self.dt_nuc / self.brownian_gamma)
+                    for d in range(3):
+                        pos[a][d] = clamp(pos[a][d] + (F[a][d] * drift + noise * self.rng.standard_normal()) / h)
+                else:
+                    v = self.nuc_vel[a]
+                    for d in range(3):
+                        v[d] += F[a][d] / m * self.dt_nuc * self.force_scale
+                        if self.langevin_kT <= 0:
+                            v[d] *= self.damping
+                        v[d] = max(-self.max_vel, min(self.max_vel, v[d]))
+                        pos[a][d] = clamp(pos[a][d] + v[d] * self.dt_nuc / h)
+            if self.langevin_kT > 0 and not self.brownian:  # Andersen collisions (:4495-4524)
+                for a in movable:
+                    if self.rng.random() < self.langevin_gamma:
+                        m = nuc_mass(self.Z_nuc[a] or self.Z[a])
+                        sv = math.sqrt(self.langevin_kT / m)
+                        self.nuc_vel[a] = [sv * self.rng.standard_normal() for _ in range(3)]
+                        sx = self.thermal_kick or (sv * self.dt_nuc / h)
+                        for d in range(3):
+                            pos[a][d] = clamp(pos[a][d] + sx * self.rng.standard_normal())
+        for grp in self.coincident_groups:
+            for gm in grp[1:]:
+                pos[gm] = list(pos[grp[0]])
+        self.nuc_steps += 1
+        self.ctx.set_atoms(self._ctx_rows())
+
+    def temperature(self) -> float:
+        """The thermostat's kinetic temperature in K (molecule.js:4545-4556)."""
+        ke, na = 0.0, 0
+        for a in range(self.n):
+            if (self.Z[a] == 0 and self.Z_nuc[a] == 0) or a in self.frozen_atoms:
+                continue
+            ke += 0.5 * nuc_mass(self.Z_nuc[a] or self.Z[a]) * sum(v * v for v in self.nuc_vel[a])
+            na += 1
+        return 2 * ke / (3 * na) * 315775 if na and ke > 0 else 0.0
+
+    # ---- restarts ---------------------------------------------------------------------------------
+    def restartWithPositions(self, new_positions):  # noqa: N802 -- molecule.js:2127-2149
+        for e, p in enumerate(new_positions[:self.n]):
+            self.pos[e] = [float(x) for x in p]
+            self.mol_pos[e] = [float(x) for x in p]
+        self.ctx.set_atoms(self._ctx_rows())
+        self.initialize()
+
+    def activateAtoms(self, count: int):  # noqa: N802 -- molecule.js:2151-2195
+        count = max(1, min(int(count), self.n))
+        self.Z = [self.Z_orig[e] if e < count else 0.0 for e in range(self.n)]
+        self.nuc_vel = [[0.0, 0.0, 0.0] for _ in range(self.n)]
+        self.nuc_force = [[0.0, 0.0, 0.0] for _ in range(self.n)]
+        self.pos = [list(p) for p in self.mol_pos]
+        self.ctx.set_atoms(self._ctx_rows())
+        self.initialize()
+        self.nuc_steps = 0
+        self.active_count = count
+
+    def extract(self, slice_k: Optional[int] = None) -> np.ndarray:
+        """The page's slice buffer (extractWGSL, molecule.js:1108-1192)."""
+        return self.ctx.extract(slice_k)
+
+    def close(self):
+        self.ctx.close()

@@ -1,0 +1,142 @@
+"""CPU tests of the molecule.js page host (MoleculePage) with a stand-in context: the frame loop's
+force cadence and convergence monitor, the nuclear forces, restraints and integrator of
+moveNuclei, and the restarts.  The GPU side of the same host is in test_gpu_molecule_host.py."""
+import math
+
+import numpy as np
+import pytest
+
+from realmolecule_b200 import _lib as L
+from realmolecule_b200.molecule_host import MoleculePage, nuc_mass
+
+
+class FakeContext:
+    """Prescribed energies and electronic forces; records the calls the host makes."""
+
+    def __init__(self, n, E=(-1.0,), F=None):
+        self.n, self.E, self.k = n, list(E), 0
+        self.F = np.zeros((n, 3)) if F is None else np.asarray(F, float)
+        self.steps, self.atoms, self.inits = [], [], 0
+
+    def step(self, n):
+        self.steps.append(n)
+
+    def energy(self):
+        e = np.zeros(L.ENERGY_LEN)
+        e[L.E_TOTAL] = self.E[min(self.k, len(self.E) - 1)]
+        self.k += 1
+        return e
+
+    def forces(self, method):
+        assert method == L.FORCE_GRADP
+        return self.F.copy()
+
+    def set_atoms(self, rows):
+        self.atoms.append([(r["i"], r["j"], r["k"], r["Z"]) for r in rows])
+
+    def initialize(self):
+        self.inits += 1
+
+    def extract(self, k=None):
+        return np.zeros(1, np.float32)
+
+
+WATER = [{"i": 50, "j": 50, "k": 50, "Z": 2, "el": "O"}, {"i": 60, "j": 57, "k": 50, "Z": 1, "el": "H"},
+         {"i": 40, "j": 57, "k": 50, "Z": 1, "el": "H"}]
+
+
+def page(rows=WATER, F=None, E=(-1.0,), **kw):
+    ctx = FakeContext(len(rows), E=E, F=F)
+    return MoleculePage(rows, NN=100, screen=10.0, context=ctx, **kw), ctx
+
+
+def test_forces_every_n_move_steps_and_page_defaults():
+    p, ctx = page(steps_per_frame=5, dynamics=True)
+    assert p.dt_nuc == 2.0 and p.substeps == 2 and p.max_vel == 0.3
+    for _ in range(4):
+        p.frame()
+    assert ctx.steps == [5, 5, 5, 5]
+    assert len(ctx.atoms) == 2  # moves after frames 2 and 4 (steps 10 and 20)
+
+
+def test_site_repulsion_is_pairwise_and_shared_by_coincident_entries():
+    rows = WATER + [{"i": 50, "j": 50, "k": 50, "Z": 1, "Z_nuc": 0.5}]
+    p, _ = page(rows, dynamics=False)
+    assert len(p.unique) == 3 and p.unique[0]["Z_eff"] == 2.5
+    p.frame()
+    p.frame()
+    f = np.array(p.nuc_force_nuc)
+    assert np.allclose(f[0], f[3])
+    site_sum = f[0] + f[1] + f[2]
+    assert np.allclose(site_sum, 0.0, atol=1e-12)
+
+
+def test_frozen_hinge_clamp_damping_and_velocity_cap():
+    F = np.array([[0.0, 0.0, 0.0], [5e3, 0.0, 0.0], [1e-3, 0.0, 0.0]])
+    p, ctx = page(F=F, dynamics=True, frozen_atoms=[0], hinge_atoms=[2], no_nuc_repulsion=True, steps_per_frame=10)
+    p.frame()
+    assert p.pos[0] == [50.0, 50.0, 50.0]                       # frozen
+    assert p.pos[2] == [40.0, 57.0, 50.0]                       # hinge: no force, no velocity
+    assert p.nuc_vel[1][0] == pytest.approx(p.max_vel)          # capped
+    assert p.pos[1][0] <= p.NN - 5                              # clamped to the box
+    assert ctx.atoms[-1][1][0] == p.pos[1][0]                   # K rebuilt from the moved positions
+
+
+def test_bond_and_angle_restraints_are_internal_forces():
+    p, _ = page(dynamics=True, no_nuc_repulsion=True, bond_constraints=[[0, 1, 1.0, 2.0]],
+                water_triplets=[[0, 1, 2]], steps_per_frame=10)
+    p.frame()
+    F = np.array(p.nuc_force)
+    assert np.allclose(F.sum(axis=0), 0.0, atol=1e-12)
+    r01 = (np.array(WATER[1]["i"]) - WATER[0]["i"]) * p.h
+    assert F[1][0] < 0 < r01  # the stretched bond pulls H back towards O
+
+
+def test_coincident_groups_move_together_and_rigid_groups_share_a_displacement():
+    rows = WATER + [{"i": 60, "j": 57, "k": 50, "Z": 1}]
+    F = np.array([[0, 0, 0], [1e-2, 0, 0], [0, 0, 0], [0, 2e-2, 0]], float)
+    p, _ = page(rows, F=F, dynamics=True, no_nuc_repulsion=True, coincident_groups=[[1, 3]], steps_per_frame=10)
+    p.frame()
+    assert p.pos[3] == p.pos[1] and p.pos[1][1] > 57.0
+    q, _ = page(F=F[:3], dynamics=True, no_nuc_repulsion=True, rigid_groups=[[1, 2]], steps_per_frame=10)
+    q.frame()
+    d1 = np.subtract(q.pos[1], [60, 57, 50])
+    d2 = np.subtract(q.pos[2], [40, 57, 50])
+    assert np.allclose(d1, d2) and d1[0] > 0
+    assert q.nuc_vel[1][0] == pytest.approx((1e-2 / (2 * nuc_mass(1)) * q.dt_nuc) * q.damping
+                                            * (1 + q.damping) if q.substeps == 2 else 0, rel=1e-12)
+
+
+def test_thermostat_is_seeded_and_brownian_moves_without_velocity():
+    a, _ = page(dynamics=True, langevin_kT=1e-3, langevin_gamma=1.0, seed=7, steps_per_frame=10)
+    b, _ = page(dynamics=True, langevin_kT=1e-3, langevin_gamma=1.0, seed=7, steps_per_frame=10)
+    a.frame(); b.frame()
+    assert a.pos == b.pos and a.temperature() > 0
+    c, _ = page(dynamics=True, brownian=True, langevin_kT=0.0, steps_per_frame=10,
+                F=np.array([[0, 0, 0], [1e-2, 0, 0], [0, 0, 0]], float), no_nuc_repulsion=True)
+    c.frame()
+    assert c.pos[1][0] > 60 and c.nuc_vel[1] == [0.0, 0.0, 0.0]
+
+
+def test_convergence_after_three_quiet_frames_and_auto_dynamics():
+    E = [-1.0, -1.5] + [-1.6] * 20
+    p, _ = page(E=E, convergence_threshold=1e-6, steps_per_frame=50)
+    frames = 0
+    while p.phase == 0 and frames < 30:
+        p.frame()
+        frames += 1
+    assert p.converged_at is not None and p.converged_at > 200
+    q, _ = page(steps_per_frame=50)
+    for _ in range(200):
+        q.frame()
+    assert q.dynamics  # auto-enabled after 10000 steps
+
+
+def test_restart_and_activate():
+    p, ctx = page(dynamics=True, steps_per_frame=10)
+    p.frame()
+    p.restartWithPositions([[52, 50, 50], [62, 57, 50], [42, 57, 50]])
+    assert ctx.inits == 1 and p.tStep == 0 and p.mol_pos[0] == [52.0, 50.0, 50.0]
+    p.activateAtoms(2)
+    assert ctx.inits == 2 and ctx.atoms[-1][2][3] == 0.0 and p.Z[:2] == [2.0, 1.0]
+    assert p.pos[0] == [52.0, 50.0, 50.0]
