@@ -137,19 +137,13 @@ __global__ void __launch_bounds__(256, 4) k_mf_update(const MfParams* __restrict
   const long long S = p->S, S2 = S * S, S3 = S2 * S;
   const long long id = (long long)i * S2 + (long long)j * S + k;
   const int n = p->n;
-  float uq[NMAX], pq[NMAX];
-#pragma unroll
-  for (int q = 0; q < NMAX; ++q) {
-    uq[q] = q < n ? __ldg(Ui + q * S3 + id) : 0.0f;
-    pq[q] = q < n ? __ldg(Pi + q * S3 + id) : 0.0f;
-  }
   float Ptot = 0.0f, max1 = 0.0f, max2 = 0.0f;
   int arg1 = -1;
 #pragma unroll
   for (int q = 0; q < NMAX; ++q)
     if (q < n) {
-      Ptot = F_ADD(Ptot, pq[q]);
-      const float u = uq[q];
+      Ptot = F_ADD(Ptot, __ldg(Pi + q * S3 + id));
+      const float u = __ldg(Ui + q * S3 + id);
       if (u > max1) { max2 = max1; max1 = u; arg1 = q; }
       else if (u > max2) max2 = u;
     }
@@ -171,31 +165,38 @@ __global__ void __launch_bounds__(256, 4) k_mf_update(const MfParams* __restrict
   const float y_au = F_MUL(F_SUB((float)j, (float)p->N2), h);
   const float beta = p->beta, two_pi_dt = F_MUL(p->two_pi, dt), fxx = F_MUL(p->field_x, x_au);
   const float dt005 = F_MUL(0.05f, dt), dt1 = F_MUL(1.0f, dt);
+  const int s1 = (int)S, s2 = (int)S2;  // stencil offsets within one field (S^3 < 2^31)
 #pragma unroll 1
   for (int m = 0; m < n; ++m) {
     const long long o = m * S3 + id;
-    const float uc = __ldg(Ui + o), wc = __ldg(Wi + o), Pc = __ldg(Pi + o);
-    const float wip = __ldg(Wi + o + S2), wim = __ldg(Wi + o - S2);
-    const float wjp = __ldg(Wi + o + S), wjm = __ldg(Wi + o - S);
-    const float wkp = __ldg(Wi + o + 1), wkm = __ldg(Wi + o - 1);
-    const float uip = __ldg(Ui + o + S2), uim = __ldg(Ui + o - S2);
-    const float ujp = __ldg(Ui + o + S), ujm = __ldg(Ui + o - S);
-    const float ukp = __ldg(Ui + o + 1), ukm = __ldg(Ui + o - 1);
-    const float pip = __ldg(Pi + o + S2), pim = __ldg(Pi + o - S2);
-    const float pjp = __ldg(Pi + o + S), pjm = __ldg(Pi + o - S);
-    const float pkp = __ldg(Pi + o + 1), pkm = __ldg(Pi + o - 1);
+    const float* __restrict__ u = Ui + o;
+    const float* __restrict__ w = Wi + o;
+    const float* __restrict__ pp = Pi + o;
+    const float uc = __ldg(u), wc = __ldg(w), Pc = __ldg(pp);
+    const float wip = __ldg(w + s2), wim = __ldg(w - s2), wjp = __ldg(w + s1), wjm = __ldg(w - s1);
+    const float wkp = __ldg(w + 1), wkm = __ldg(w - 1);
+    const float uip = __ldg(u + s2), uim = __ldg(u - s2), ujp = __ldg(u + s1), ujm = __ldg(u - s1);
+    const float ukp = __ldg(u + 1), ukm = __ldg(u - 1);
+    const float pip = __ldg(pp + s2), pim = __ldg(pp - s2), pjp = __ldg(pp + s1), pjm = __ldg(pp - s1);
+    const float pkp = __ldg(pp + 1), pkm = __ldg(pp - 1);
     const float4 cu = p->upd[m];
     const float tilt_y = p->rcs[m].w;
     const unsigned gm = p->gmask[m];
     const float umax = m == arg1 ? max2 : max1;
-    float Pgrp = 0.0f, rho_other = 0.0f;
-#pragma unroll
-    for (int q = 0; q < NMAX; ++q)
-      if (q < n && ((gm >> q) & 1u)) Pgrp = F_ADD(Pgrp, pq[q]);
+    float Pgrp, rho_other = 0.0f;
+    if (gm == (1u << m)) {  // no split siblings: the group sum is this electron's own P
+      Pgrp = F_ADD(0.0f, Pc);
+    } else {
+      Pgrp = 0.0f;
+      for (int q = 0; q < n; ++q)
+        if ((gm >> q) & 1u) Pgrp = F_ADD(Pgrp, __ldg(Pi + q * S3 + id));
+    }
     if (beta != 0.0f) {  // V_Pauli; with beta = 0 it is 0 * (a finite sum of squares) = 0
-#pragma unroll
-      for (int q = 0; q < NMAX; ++q)
-        if (q < n && q != m) rho_other = F_ADD(rho_other, F_MUL(uq[q], uq[q]));
+      for (int q = 0; q < n; ++q)
+        if (q != m) {
+          const float un = __ldg(Ui + q * S3 + id);
+          rho_other = F_ADD(rho_other, F_MUL(un, un));
+        }
     }
     const float cm = F_SUB(uc, umax);
     const float lw =
