@@ -27,9 +27,13 @@ from .context import Context
 
 class EnergyModel:
     def __init__(self, NN: int, h: float, charges: Sequence[float], positions: np.ndarray,
-                 seeds: np.ndarray, precision: str = "fp64", tol: float = 1e-10, max_steps: int = 50000,
-                 check_interval: int = 100, warm_steps: int = 0, **opts):
+                 seeds: np.ndarray, precision: str = "fp64", tol: Optional[float] = 1e-10, max_steps: int = 50000,
+                 check_interval: int = 100, warm_steps: int = 0, want_rho: bool = True, **opts):
+        """tol None: each evaluation runs exactly ``warm_steps`` imaginary-time steps from the previous
+        state (the fixed warm-started iterations of the geometry workloads) instead of a solve.
+        want_rho False: evaluate returns None for h^3 rho (no density download)."""
         self.NN, self.h = int(NN), float(h)
+        self.want_rho = want_rho
         self.charges = np.asarray(charges, np.float64)
         self.n_nuc = len(self.charges)
         self.seeds = np.asarray(seeds, np.float64)
@@ -59,12 +63,17 @@ class EnergyModel:
             self._v = v
         if self.warm_steps:
             self.ctx.step(self.warm_steps)
-        steps, E = self.ctx.solve(self.tol, self.max_steps, self.check)
+        if self.tol is None:
+            steps, E = self.warm_steps, float(self.ctx.energy()[L.E_TOTAL])
+        else:
+            steps, E = self.ctx.solve(self.tol, self.max_steps, self.check)
         Fe = self.ctx.forces(L.FORCE_ADJOINT)[: self.n_nuc]
         _, Fn = self.ctx.nuclear_terms()
         F = Fe + Fn[: self.n_nuc]
-        psi = self.ctx.download(psi=True, label=False)["psi"].astype(np.float64)
-        rho_h3 = psi * psi * self.h ** 3
+        rho_h3 = None
+        if self.want_rho:
+            psi = self.ctx.download(psi=True, label=False)["psi"].astype(np.float64)
+            rho_h3 = psi * psi * self.h ** 3
         self.last = {"E": E, "F": F, "steps": steps}
         return E, F, rho_h3
 

@@ -64,8 +64,15 @@ __device__ __forceinline__ void nm_potential_body(T* __restrict__ K, const doubl
       const double Z = sa[m * 4 + 3];
       if (Z <= 0.0) continue;
       const double dx = x - sa[m * 4 + 0], dy = y - sa[m * 4 + 1], dz = z - sa[m * 4 + 2];
-      const double r = sqrt(dx * dx + dy * dy + dz * dz);
-      v += (r < 1e-12) ? Z * c0 : Z * erf(r * inv) / r;
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      // erf(r inv) is 1 to double precision from r inv = 6 on: there the term is Z / r, formed
+      // with the FP64 reciprocal square root (no divide)
+      if (r2 * inv * inv >= 36.0) {
+        v += Z * rsqrt(r2);
+      } else {
+        const double r = sqrt(r2);
+        v += (r < 1e-12) ? Z * c0 : Z * erf(r * inv) / r;
+      }
     }
   }
   if (inside) K[id] = interior ? (T)v : T(0);
@@ -467,9 +474,15 @@ __device__ __forceinline__ void nm_force_body(const T* __restrict__ U, const dou
         const double dx = (double)sx[q] - ax, dy = (double)sy[q] - ay, dz = (double)sz[q] - az;
         const double r2 = dx * dx + dy * dy + dz * dz;
         if (r2 < 1e-24) continue;
-        const double r = sqrt(r2);
-        const double dKdr = (r * inv < 6.0) ? Z * (gs * exp(-r2 * inv * inv) / r - erf(r * inv) / r2) : -Z / r2;
-        const double w = -h3 * rho * dKdr / r;
+        double w;
+        if (r2 * inv * inv >= 36.0) {  // Coulomb tail: -h3 rho dK/dr / r = h3 rho Z / r^3
+          const double ir = rsqrt(r2);
+          w = h3 * rho * Z * (ir * ir * ir);
+        } else {
+          const double r = sqrt(r2);
+          const double dKdr = Z * (gs * exp(-r2 * inv * inv) / r - erf(r * inv) / r2);
+          w = -h3 * rho * dKdr / r;
+        }
         lx += w * dx; ly += w * dy; lz += w * dz;
       }
       fx += lx; fy += ly; fz += lz;

@@ -85,3 +85,71 @@ def velocity_verlet(model, x0, v0, masses, dt: float, n_steps: int) -> Trajector
         E, F, _ = model.evaluate(x)
         v = v_half + 0.5 * dt * F / m
     return traj
+
+
+def geometry_model(g, precision: str = "mixed", iters: int = 200, label_until: int = 400):
+    """An EnergyModel for a configs.Geometry in the workloads' mode: each evaluation runs `iters`
+    warm-started imaginary-time steps (no solve to a tolerance, no density download)."""
+    from .autograd import EnergyModel
+    off = (g.NN // 2) * g.h  # geometries are centred on the centroid; the model uses the box frame
+    return EnergyModel(g.NN, g.h, g.charges, g.xyz + off, g.seeds + off, precision=precision, tol=None,
+                       warm_steps=iters, want_rho=False, label_until=label_until), g.charges, off
+
+
+def _main(argv=None):
+    """Run the geometry workloads of the benchmark configurations on cuda:0.
+
+    python -m realmolecule_b200.dynamics --workload water100 [--steps 100] [--iters 200]
+        FIRE relaxation of 100 waters (192^3), each step warm-started with `iters` iterations.
+    python -m realmolecule_b200.dynamics --workload water1000 [--steps 200] [--iters 50] [--dt-fs 0.5]
+        velocity Verlet of 1000 waters (320^3); prints the total-energy drift.
+    Prints one JSON line (per-step wall times, energies, fmax / drift)."""
+    import argparse
+    import json
+    import time
+
+    from . import _lib as L, configs
+    ap = argparse.ArgumentParser(description=_main.__doc__)
+    ap.add_argument("--workload", default="water100", choices=["water100", "water1000"])
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--iters", type=int, default=None)
+    ap.add_argument("--dt-fs", type=float, default=0.5)
+    ap.add_argument("--precision", default="mixed")
+    ap.add_argument("--preconverge", type=int, default=None,
+                    help="imaginary-time steps before the first geometry step (default 2000 / 3000)")
+    a = ap.parse_args(argv)
+    g = configs.water100() if a.workload == "water100" else configs.water1000()
+    iters = a.iters or (200 if a.workload == "water100" else 50)
+    t0 = time.perf_counter()
+    model, Z, off = geometry_model(g, a.precision, iters)
+    pre = a.preconverge if a.preconverge is not None else (2000 if a.workload == "water100" else 3000)
+    model.ctx.step(pre)  # converge the electrons at the start geometry
+    model.ctx.synchronize()
+    t_init = time.perf_counter() - t0
+    # one evaluation split into its parts (synchronised wall clock)
+    parts = {}
+    for name, fn in (("set_atoms_ms", lambda: model.ctx.set_atoms(model._rows(g.xyz + off))),
+                     ("iters_ms", lambda: model.ctx.step(iters)), ("energy_ms", lambda: model.ctx.energy()),
+                     ("forces_ms", lambda: model.ctx.forces(L.FORCE_ADJOINT))):
+        t1 = time.perf_counter(); fn(); model.ctx.synchronize(); parts[name] = (time.perf_counter() - t1) * 1e3
+    m = masses_for(Z)
+    t0 = time.perf_counter()
+    if a.workload == "water100":
+        tr = fire(model, g.xyz + off, max_steps=a.steps or 100, masses=m)
+        out = {"fmax_first": tr.fmax[0], "fmax_last": tr.fmax[-1], "E_first": tr.energies[0], "E_last": tr.energies[-1]}
+    else:
+        n = a.steps or 200
+        tr = velocity_verlet(model, g.xyz + off, np.zeros_like(g.xyz), m, a.dt_fs * FS, n)
+        Et = np.array(tr.energies) + np.array(tr.kinetic)
+        out = {"E_total_first": float(Et[0]), "E_total_last": float(Et[-1]),
+               "drift_Ha": float(Et[-1] - Et[0]), "max_excursion_Ha": float(np.abs(Et - Et[0]).max())}
+    dt = time.perf_counter() - t0
+    nstep = len(tr.energies)
+    print(json.dumps({"workload": a.workload, "grid": f"{g.NN}^3", "nuclei": len(Z), "domains": len(g.seeds),
+                      "iters_per_step": iters, "preconverge_steps": pre, "steps": nstep, "init_s": t_init, "s": dt,
+                      "evaluation_parts": parts,
+                      "ms_per_geometry_step": dt / max(1, nstep) * 1e3, **out}), flush=True)
+
+
+if __name__ == "__main__":
+    _main()
