@@ -82,7 +82,11 @@ typedef struct rq_config {
   double curv_reg;          /* molecule.js curvReg (0: 0.15 as :34; < 0: off) */
   double sigma;             /* new: Gaussian nucleus width in bohr (<=0: h) */
   int32_t label_until;      /* labels update only while steps_done < label_until (0: always) */
-  int32_t reserved[7];
+  int32_t chebyshev;        /* molecule.js flavour, 1: the Chebyshev semi-iterative update instead of plain
+                               ITP (molecule.js:345-421, :2915-2962), omega from the page's recurrence and the
+                               previous frame's energy; frames run eagerly; not with bare nuclei (Z = 0,
+                               Z_nuc > 0, rc > 0: RQ_ENOTSUP) */
+  int32_t reserved[6];
 } rq_config;
 
 /* One entry of the reference atom list: a nucleus and/or one electron domain. */

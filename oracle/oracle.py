@@ -97,6 +97,7 @@ class _Oracle:
             "orc_mj_copy_for_label": [_f32p, _f32p, _u32p, C.c_uint32, _i],
             "orc_mj_init_pdirect": [C.c_void_p, _i, C.c_uint32, _f32p, _f32p, _i, _f, _f],
             "orc_mj_sub_self": [_f32p, _f32p, _u32p, C.c_uint32, _f, _i],
+            "orc_mj_update_cheb": [_f32p, _f32p, _f32p, _u32p, _f32p, C.c_void_p, _i, _i, _f, _f, _f, _f],
             "orc_mj_residual": [_f32p, _f32p, _f32p, _i, _f, _f],
             "orc_mj_restrict": [_f32p, _f32p, _i, _i],
             "orc_mj_coarse_smooth": [_f32p, _f32p, _f32p, _i, _f],
@@ -365,7 +366,7 @@ class MoleculeJsDriver:
     """
 
     def __init__(self, NN, screen, atoms, dv=None, steps_per_frame=None, norm_interval=20, vcycle_interval=50,
-                 jacobi_per_step=2, boundary_speed=0.5, curv_reg=0.15, sic=False):
+                 jacobi_per_step=2, boundary_speed=0.5, curv_reg=0.15, sic=False, chebyshev=False):
         self.NN = NN
         self.S = NN + 1
         self.S3 = self.S ** 3
@@ -405,6 +406,8 @@ class MoleculeJsDriver:
         self.rho = np.zeros(S3, np.float32)
         self.steps_done = 0
         self.frame = 0  # molecule.js frameCount
+        self.chebyshev = bool(chebyshev)
+        self.cheb_state, self.cheb_E = 1.0, 0.0  # chebOmega (:1762) and the page's E (:1767)
         # SIC_INTERVAL (molecule.js:112); 0 = off
         nel = nelec or 3
         # sic=True takes the reference's own Pother path: the direct per-electron Poisson for
@@ -490,8 +493,12 @@ class MoleculeJsDriver:
                 self.P, self.P2 = self.P2, self.P
             if sf > 0 and sf % self.vcycle_interval == 0:
                 self.vcycle()
-        O().mj_update(self.U, self.Unext, self.K, self.label, self.Pother, C.addressof(self.atoms), self.nA,
-                      int(self.has_bare), self.S, self.h, self.half_d, self.dt)
+        if self.chebyshev:
+            O().mj_update_cheb(self.U, self.Unext, self.K, self.label, self.Pother, C.addressof(self.atoms), self.nA,
+                               self.S, self.h, self.half_d, self.dt, np.float32(self.cheb_omega_step()))
+        else:
+            O().mj_update(self.U, self.Unext, self.K, self.label, self.Pother, C.addressof(self.atoms), self.nA,
+                          int(self.has_bare), self.S, self.h, self.half_d, self.dt)
         self.U, self.Unext = self.Unext, self.U
         if (sf + 1) % self.norm_interval == 0 or sf == self.spf - 1:
             acc = np.zeros(self.nA, np.uint32)
@@ -509,6 +516,54 @@ class MoleculeJsDriver:
             for _ in range(max(1, self.spf)):
                 O().mj_evolve_boundary(self.label, self.label2, self.U, self.W, self.S, self.dt_w, self.curv)
                 self.label, self.label2 = self.label2, self.label
+            if self.chebyshev:
+                self.cheb_E = self.total_energy()
+
+    def cheb_omega_step(self):
+        """molecule.js:2924-2949 -- omega for the coming step from dv and the previous frame's E."""
+        dv, E = self.dv, self.cheb_E
+        dtv = dv * (self.hd * self.hd)
+        dtLmax = 6.0 * dv
+        dtLmin = dtv * (max(-100.0, E) if math.isfinite(E) else -10.0)
+        gMax, gMin = 1 - dtLmin, 1 - dtLmax
+        q = (gMax - gMin) / (gMax + gMin)
+        rhoSq = q * q
+        if self.cheb_state <= 1.0:
+            omega, self.cheb_state = 1.0, 1.001
+        elif self.cheb_state < 1.01:
+            omega = 1.0 / (1.0 - rhoSq / 2.0)
+            self.cheb_state = omega
+        else:
+            omega = 1.0 / (1.0 - rhoSq * self.cheb_state / 4.0)
+            self.cheb_state = omega
+        return min(1.95, max(1.0, omega))
+
+    def total_energy(self):
+        """E = E_T + E_eK + E_ee + E_KK as the page forms it (molecule.js:3124-3186): the per-H
+        exclusion correction (H_RAW, :3130-3139) and the unique nuclei's softened repulsion."""
+        T, EK, EE = self.energy()[:3]
+        nH = sum(1 for a in self.rows if a["Z"] == 1 and (a.get("rc") or 0) == 0)
+        raw = (0.5, -1.0) if self.NN in (100, 300) else (0.503, -1.028)
+        T += nH * (0.5 - raw[0])
+        EK += nH * (-1.0 - raw[1])
+        sites = {}
+        for e, a in enumerate(self.rows):
+            if a["Z"] == 0 and (a.get("Z_nuc") or 0) == 0:
+                continue
+            key = (a["i"], a["j"], a.get("k"))
+            q = (a.get("Z_nuc") or 0) or a["Z"]
+            if key in sites:
+                sites[key][1] += q
+            else:
+                sites[key] = [e, q]
+        G = list(sites.values())
+        ekk = 0.0
+        for x in range(len(G)):
+            for y in range(x + 1, len(G)):
+                A, B = self.rows[G[x][0]], self.rows[G[y][0]]
+                d2 = sum(((A[c] - B[c]) * self.hd) ** 2 for c in "ijk")
+                ekk += G[x][1] * G[y][1] / math.sqrt(d2 + 0.04 * self.hd * self.hd)
+        return T + EK + EE + ekk
 
     def energy(self):
         out = np.zeros(6)

@@ -425,6 +425,35 @@ void orc_mj_update(const float* U, float* Uo, const float* K, const uint32_t* la
 
 /* molecule.js:426-540 evolveBoundary without locked groups or shell splits
  * (both off unless a page sets them, :490-503): snapshot read labelIn, write labelOut and W. */
+/* chebyshevStepWGSL (molecule.js:345-421): the ITP step of orc_mj_update blended with psi_{n-1},
+ * which Uo holds on entry: Uo = omega * step + (1 - omega) * Uo; cells inside their own r_c are 0.
+ * (The shader tests only the own label's r_c sphere, as orc_mj_update does without bare nuclei.) */
+void orc_mj_update_cheb(const float* U, float* Uo, const float* K, const uint32_t* label, const float* Pother,
+                        const orc_mj_atom* atoms, int nElec, int S, float h, float half_d, float dt, float omega) {
+  const int NN = S - 1;
+  const int64_t S2 = (int64_t)S * S;
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        uint32_t L = label[id];
+        if (mj_inside_rc(i, j, k, L, atoms, nElec, 0, h)) { Uo[id] = 0.f; continue; }
+        float uc = U[id];
+        uint32_t lip = label[id + S2], lim = label[id - S2], ljp = label[id + S], ljm = label[id - S];
+        uint32_t lkp = label[id + 1], lkm = label[id - 1];
+        float uip = (lip == L && !mj_inside_rc(i + 1, j, k, lip, atoms, nElec, 0, h)) ? U[id + S2] : uc;
+        float uim = (lim == L && !mj_inside_rc(i - 1, j, k, lim, atoms, nElec, 0, h)) ? U[id - S2] : uc;
+        float ujp = (ljp == L && !mj_inside_rc(i, j + 1, k, ljp, atoms, nElec, 0, h)) ? U[id + S] : uc;
+        float ujm = (ljm == L && !mj_inside_rc(i, j - 1, k, ljm, atoms, nElec, 0, h)) ? U[id - S] : uc;
+        float ukp = (lkp == L && !mj_inside_rc(i, j, k + 1, lkp, atoms, nElec, 0, h)) ? U[id + 1] : uc;
+        float ukm = (lkm == L && !mj_inside_rc(i, j, k - 1, lkm, atoms, nElec, 0, h)) ? U[id - 1] : uc;
+        float lap = uip + uim + ujp + ujm + ukp + ukm - 6.0f * uc;
+        float step = uc + half_d * lap + dt * (K[id] - 2.0f * Pother[id]) * uc;
+        Uo[id] = omega * step + (1.0f - omega) * Uo[id];
+      }
+}
+
 void orc_mj_evolve_boundary(const uint32_t* labelIn, uint32_t* labelOut, const float* U, float* W, int S,
                             float dt_w, float curvReg) {
   const int NN = S - 1;

@@ -225,6 +225,11 @@ extern "C" int rq_create(const rq_config* cfg, const rq_atom* atoms, int32_t n_a
   if (cfg->flavor < 0 || cfg->flavor > 2 || cfg->precision < 0 || cfg->precision > 1) return RQ_EINVAL;
   if (cfg->precision == RQ_PREC_FP64 && cfg->flavor != RQ_FLAVOR_NEW) return RQ_ENOTSUP;
   if (cfg->sic != 0 && cfg->flavor != RQ_FLAVOR_MOLECULE_JS) return RQ_ENOTSUP;  // SIC is molecule.js's
+  if (cfg->chebyshev != 0) {  // molecule.js's Chebyshev update tests only the own r_c sphere (:368-372)
+    if (cfg->flavor != RQ_FLAVOR_MOLECULE_JS) return RQ_ENOTSUP;
+    for (int q = 0; q < n_atoms; ++q)
+      if (atoms[q].Z == 0 && atoms[q].Z_nuc > 0 && atoms[q].rc > 0) return RQ_ENOTSUP;
+  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return RQ_ENODEV;
   rq_ctx* c = new (std::nothrow) rq_ctx();
@@ -454,7 +459,7 @@ extern "C" int rq_step(rq_ctx* c, int32_t n) {
     // (a period boundary never leaves an early Jacobi sweep pending: the step before a Poisson step
     // is never the last of a period, as the period is a multiple of poisson_interval)
     // (with SIC, frame 0 never corrects: the first period runs eagerly, the later ones repeat)
-    const bool aligned = !c->prof && !straddle && period > 0 && c->steps_done % period == 0 && left >= period &&
+    const bool aligned = !c->prof && !c->cfg.chebyshev && !straddle && period > 0 && c->steps_done % period == 0 && left >= period &&
                          c->sp_jdone == 0 && !(mj_sic_interval(c) > 0 && c->frame == 0);
     if (!aligned) {
       // run eagerly up to the next period boundary (or all that is left)
@@ -511,6 +516,8 @@ extern "C" int rq_initialize(rq_ctx* c) {
   if (rc != RQ_OK) return rc;
   c->steps_done = 0;
   c->frame = 0;
+  c->cheb_omega = 1.0;
+  c->cheb_E = 0.0;
   CK(cudaStreamSynchronize(c->st));
   return RQ_OK;
 }

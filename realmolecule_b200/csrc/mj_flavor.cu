@@ -133,6 +133,28 @@ int mj_refresh_flags(rq_ctx* c) {
   return RQ_OK;
 }
 
+// The page's Chebyshev omega for the coming step (molecule.js:2924-2949): the spectral bounds of
+// the ITP iteration from dv and the previous frame's energy, the omega recurrence, the clamp.
+static float mj_cheb_omega(rq_ctx* c) {
+  const double dv = c->dv, dtv = dv * (c->h * c->h), E = c->cheb_E;
+  const double dtLmax = 6.0 * dv;
+  const double dtLmin = dtv * (std::isfinite(E) ? std::max(-100.0, E) : -10.0);
+  const double gMax = 1 - dtLmin, gMin = 1 - dtLmax;
+  const double q = (gMax - gMin) / (gMax + gMin), rhoSq = q * q;
+  double omega;
+  if (c->cheb_omega <= 1.0) {
+    omega = 1.0;
+    c->cheb_omega = 1.001;
+  } else if (c->cheb_omega < 1.01) {
+    omega = 1.0 / (1.0 - rhoSq / 2.0);
+    c->cheb_omega = omega;
+  } else {
+    omega = 1.0 / (1.0 - rhoSq * c->cheb_omega / 4.0);
+    c->cheb_omega = omega;
+  }
+  return (float)std::min(1.95, std::max(1.0, omega));
+}
+
 int mj_step_one(rq_ctx* c, int s) {
   const MjParams p = mj_params(c);
   const rq_config& f = c->cfg;
@@ -162,9 +184,16 @@ int mj_step_one(rq_ctx* c, int s) {
   }
   const bool norm = ((sf + 1) % f.norm_interval == 0) || sf == spf - 1;  // molecule.js:2972
   if (norm) CK(cudaMemsetAsync(c->unorm, 0, sizeof(unsigned) * c->n_atoms, c->st));
-  LAUNCH(RQ_KC_UPDATE, 20 * ip,
-         launch_mj_update((float*)c->U[c->cu], (float*)c->U[1 - c->cu], (float*)c->K, c->lab[c->cl], c->Pother, c->g,
-                          p.half_d, p.dt, p.h3, c->n_atoms, norm ? c->unorm : nullptr, c->st));
+  if (c->cfg.chebyshev) {
+    const float omega = mj_cheb_omega(c);
+    LAUNCH(RQ_KC_UPDATE, 24 * ip,
+           launch_mj_update_cheb((float*)c->U[c->cu], (float*)c->U[1 - c->cu], (float*)c->K, c->lab[c->cl], c->Pother,
+                                 c->g, p.half_d, p.dt, p.h3, c->n_atoms, norm ? c->unorm : nullptr, omega, c->st));
+  } else {
+    LAUNCH(RQ_KC_UPDATE, 20 * ip,
+           launch_mj_update((float*)c->U[c->cu], (float*)c->U[1 - c->cu], (float*)c->K, c->lab[c->cl], c->Pother, c->g,
+                            p.half_d, p.dt, p.h3, c->n_atoms, norm ? c->unorm : nullptr, c->st));
+  }
   c->cu ^= 1;
   if (norm) {
     LAUNCH(RQ_KC_NORMALIZE, 8.0 * c->n_atoms,
@@ -198,6 +227,13 @@ int mj_step_one(rq_ctx* c, int s) {
              launch_mj_evolve(c->lab[c->cl], c->lab[1 - c->cl], (float*)c->U[c->cu], c->W, atoms_dev(c), c->n_atoms,
                               c->g, p.dt_w, p.curvReg, p.h, p.hasBare, c->st));
       c->cl ^= 1;
+    }
+    if (c->cfg.chebyshev) {  // the page's E at the frame's end feeds the next frame's omega (:3186)
+      double e[RQ_ENERGY_LEN], ekk = 0;
+      int rc = mj_energy(c, e, nullptr);
+      if (rc != RQ_OK) return rc;
+      mj_nuclear_terms(c, &ekk, nullptr);
+      c->cheb_E = e[RQ_E_T] + e[RQ_E_EK] + e[RQ_E_EE] + ekk;
     }
   }
   return RQ_OK;
@@ -248,9 +284,10 @@ void mj_nuclear_terms(rq_ctx* c, double* E, double* F) {
       fy += zeff[a] * zeff[b] * dy * inv_r3;
       fz += zeff[a] * zeff[b] * dz * inv_r3;
     }
-    for (int q : groups[a]) {
-      F[q * 3] = fx; F[q * 3 + 1] = fy; F[q * 3 + 2] = fz;
-    }
+    if (F)
+      for (int q : groups[a]) {
+        F[q * 3] = fx; F[q * 3 + 1] = fy; F[q * 3 + 2] = fz;
+      }
   }
   *E = e;
 }

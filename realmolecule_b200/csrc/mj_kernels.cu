@@ -120,11 +120,15 @@ __global__ void __launch_bounds__(256) k_mj_flags(int* __restrict__ label, const
 // updateU (molecule.js:263-343, W_CUTOFF = 0): 20 B per interior point.  With ACC the new
 // psi's u32 fixed-point norm per label (molecule.js:912-933) is accumulated as well.
 // ---------------------------------------------------------------------------------------
-template <bool ACC>
+// With CHEB the Chebyshev step (molecule.js:345-421): out = omega * (the ITP step) + (1 - omega) *
+// psi_{n-1}, where psi_{n-1} is what Uo holds (the input of the previous step), read at the cell
+// before it is overwritten.
+template <bool ACC, bool CHEB = false>
 __global__ void __launch_bounds__(256) k_mj_update(const float* __restrict__ U, float* __restrict__ Uo,
                                                    const float* __restrict__ K, const int* __restrict__ label,
                                                    const float* __restrict__ Pother, Geo g, float half_d, float dt,
-                                                   float h3, int nDom, unsigned* __restrict__ unorm) {
+                                                   float h3, int nDom, unsigned* __restrict__ unorm,
+                                                   float omega = 1.0f) {
   constexpr int NSLOT = 128;
   __shared__ int keys[NSLOT];
   __shared__ unsigned vals[NSLOT];
@@ -174,6 +178,7 @@ __global__ void __launch_bounds__(256) k_mj_update(const float* __restrict__ U, 
         const float lap = F_SUB(F_ADD(F_ADD(F_ADD(F_ADD(F_ADD(a, b), c), d), e), f), F_MUL(6.0f, u_c));
         out = F_ADD(F_ADD(u_c, F_MUL(half_d, lap)),
                     F_MUL(F_MUL(dt, F_SUB(__ldg(K + id), F_MUL(2.0f, __ldg(Pother + id)))), u_c));
+        if (CHEB) out = F_ADD(F_MUL(omega, out), F_MUL(F_SUB(1.0f, omega), Uo[id]));
       }
       Uo[id] = out;
       if (ACC) {
@@ -618,6 +623,18 @@ cudaError_t launch_mj_update(const float* U, float* Uo, const float* K, const in
   else
     k_mj_update<false><<<march_grid(g), march_block(), 0, st>>>(U, Uo, K, label, Pother, g, half_d, dt, h3, nDom,
                                                                  nullptr);
+  return cudaGetLastError();
+}
+cudaError_t launch_mj_update_cheb(const float* U, float* Uo, const float* K, const int* label, const float* Pother,
+                                  const Geo& g, float half_d, float dt, float h3, int nDom, unsigned* unorm,
+                                  float omega, cudaStream_t st) {
+  if (g.NN < 2) return cudaSuccess;
+  if (unorm)
+    k_mj_update<true, true><<<march_grid(g), march_block(), 0, st>>>(U, Uo, K, label, Pother, g, half_d, dt, h3, nDom,
+                                                                      unorm, omega);
+  else
+    k_mj_update<false, true><<<march_grid(g), march_block(), 0, st>>>(U, Uo, K, label, Pother, g, half_d, dt, h3, nDom,
+                                                                       nullptr, omega);
   return cudaGetLastError();
 }
 cudaError_t launch_mj_norm_scale(const unsigned* unorm, const MjAtom* atoms, int nDom, float* scale, cudaStream_t st) {

@@ -81,6 +81,8 @@ struct rq_ctx {
 
   int steps_done = 0;
   int frame = 0;
+  double cheb_omega = 1.0;  // molecule.js Chebyshev recurrence state (chebOmega, :1762)
+  double cheb_E = 0.0;      // the page's E of the last frame (0 before the first, :1767)
   std::string last_error;
 
   // CUDA graphs of one schedule period, keyed by buffer parity (cu, cp, cl) and whether the

@@ -63,6 +63,9 @@ cudaError_t launch_mj_flags(int* label, const MjAtom* atoms, int nAt, const Geo&
 cudaError_t launch_mj_update(const float* U, float* Uo, const float* K, const int* label, const float* Pother,
                              const Geo& g, float half_d, float dt, float h3, int nDom, unsigned* unorm, cudaStream_t st);
 cudaError_t launch_mj_norm_scale(const unsigned* unorm, const MjAtom* atoms, int nDom, float* scale, cudaStream_t st);
+cudaError_t launch_mj_update_cheb(const float* U, float* Uo, const float* K, const int* label, const float* Pother,
+                                  const Geo& g, float half_d, float dt, float h3, int nDom, unsigned* unorm,
+                                  float omega, cudaStream_t st);
 cudaError_t launch_mj_extract(const float* U, const int* label, const float* K, const MjAtom* atoms, int nAt,
                               const Geo& g, int sk, float* out, cudaStream_t st);
 cudaError_t launch_mj_apply_scale(float* U, const int* label, const float* scale, const Geo& g, cudaStream_t st);

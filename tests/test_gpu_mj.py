@@ -195,3 +195,32 @@ def test_direct_per_electron_poisson_bit_exact(kind):
     Fo = np.zeros(ref.nA * 3)
     orc.O().mj_force_gradP(ref.Pother, orc.C.addressof(ref.atoms), ref.nA, ref.S, np.float32(1 / ref.hd), R, Fo)
     np.testing.assert_allclose(ctx.forces(L.FORCE_GRADP).reshape(-1), Fo, rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.parametrize("kind", ["water", "ten"])
+def test_frames_with_chebyshev_bit_exact(kind):
+    """The Chebyshev update (molecule.js:345-421) with the page's omega recurrence fed by each
+    frame's energy (both sides form E from FP64 sums; omega is rounded to f32 before use)."""
+    from realmolecule_b200 import Context
+    NN, screen, rows = atoms_case(kind)
+    ref = orc.MoleculeJsDriver(NN, screen, rows, steps_per_frame=10, chebyshev=True)
+    ref.initialize()
+    ctx = Context(NN, screen, rows, flavor="molecule.js", steps_per_frame=10, chebyshev=1)
+    ctx.initialize()
+    ctx.upload(psi=ref.U, label=ref.label.astype(np.int32))
+    for _ in range(30):  # three frames: omega 1, then the recurrence with E of frames 1 and 2
+        ref.step()
+    ctx.step(30)
+    st = ctx.download(psi=True, label=True, W=True, P=True)
+    assert np.array_equal(st["psi"].view(np.uint32), ref.U.view(np.uint32))
+    assert np.array_equal(st["label"], ref.label.astype(np.int32))
+    assert np.array_equal(st["W"].view(np.uint32), ref.W.view(np.uint32))
+    assert ref.cheb_state > 1.01
+
+
+def test_chebyshev_is_refused_with_bare_nuclei():
+    from realmolecule_b200 import Context, _lib as L
+    NN, screen, rows = atoms_case("bare")
+    with pytest.raises(L.RqError) as e:
+        Context(NN, screen, rows, flavor="molecule.js", chebyshev=1)
+    assert e.value.status == L.RQ_ENOTSUP
