@@ -86,7 +86,12 @@ typedef struct rq_config {
                                ITP (molecule.js:345-421, :2915-2962), omega from the page's recurrence and the
                                previous frame's energy; frames run eagerly; not with bare nuclei (Z = 0,
                                Z_nuc > 0, rc > 0: RQ_ENOTSUP) */
-  int32_t reserved[6];
+  int32_t lobpcg;           /* molecule.js flavour, 1: every step is one LOBPCG frame (doLOBPCGStep,
+                               molecule.js:3323-3740; the page's useLOBPCG, :1751): the Poisson solve and
+                               Pother, 10 LOBPCG iterations per domain (Ritz problems solved on the device
+                               in FP64), normalisation, one ITP update, the level-set passes; not with
+                               chebyshev (RQ_EINVAL) */
+  int32_t reserved[5];
 } rq_config;
 
 /* One entry of the reference atom list: a nucleus and/or one electron domain. */

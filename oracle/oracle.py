@@ -134,6 +134,12 @@ class _Oracle:
             "orc_rb_energy": [C.c_void_p, _f32p, _f32p, _f32p, _f32p, _d, _d, _f64p],
             "orc_rb_init": [C.c_void_p, _i, _f32p, _i32p, _f32p, _f32p, _f32p, _f32p],
             "orc_rb_slice": [C.c_void_p, _f32p, _f32p, _f32p, _f32p, _f32p],
+            "orc_lob_apply_h": [_f32p, _f32p, _f32p, _u32p, _f32p, C.c_void_p, _i, _f, _f],
+            "orc_lob_inner": [_f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _u32p, C.c_uint32, _i, _f, _f32p],
+            "orc_lob_residual": [_f32p, _f32p, _f32p, _u32p, _f32p, _f32p, _f, C.c_uint32, _i, _f],
+            "orc_lob_update": [_f32p, _f32p, _f32p, _u32p, _f, _f, _f, C.c_uint32, _i],
+            "orc_lob_ritz2": [_f64p, _f64p],
+            "orc_lob_ritz3": [_f64p, _f64p],
         }
         for name, argt in sig.items():
             fn = getattr(L, name)
@@ -366,7 +372,7 @@ class MoleculeJsDriver:
     """
 
     def __init__(self, NN, screen, atoms, dv=None, steps_per_frame=None, norm_interval=20, vcycle_interval=50,
-                 jacobi_per_step=2, boundary_speed=0.5, curv_reg=0.15, sic=False, chebyshev=False):
+                 jacobi_per_step=2, boundary_speed=0.5, curv_reg=0.15, sic=False, chebyshev=False, lobpcg=False):
         self.NN = NN
         self.S = NN + 1
         self.S3 = self.S ** 3
@@ -408,6 +414,11 @@ class MoleculeJsDriver:
         self.frame = 0  # molecule.js frameCount
         self.chebyshev = bool(chebyshev)
         self.cheb_state, self.cheb_E = 1.0, 0.0  # chebOmega (:1762) and the page's E (:1767)
+        # useLOBPCG (molecule.js:1751): one step() is one doLOBPCGStep frame
+        self.lobpcg = bool(lobpcg)
+        self.sic = bool(sic)
+        if self.lobpcg:
+            self.HX, self.LW, self.HW, self.LP, self.HP = (np.zeros(S3, np.float32) for _ in range(5))
         # SIC_INTERVAL (molecule.js:112); 0 = off
         nel = nelec or 3
         # sic=True takes the reference's own Pother path: the direct per-electron Poisson for
@@ -474,7 +485,81 @@ class MoleculeJsDriver:
                 O().mj_jacobi(*((a, b) if js % 2 == 0 else (b, a)), self.rho, self.S, self.h2, two_pi)
             O().mj_sub_self(a, self.Pother, self.label, m, Zm, self.S)
 
+    def lobpcg_inner(self, m):
+        out = np.zeros(12, np.float32)
+        O().lob_inner(self.U, self.HX, self.LW, self.HW, self.LP, self.HP, self.label, m, self.S, self.h3, out)
+        return out
+
+    def lobpcg_frame(self):
+        """doLOBPCGStep (molecule.js:3323-3740).  Phase 1: the Poisson solve on the current psi (the
+        direct per-electron path, or 4 Jacobi sweeps and the V-cycle) and Pother (P, minus every
+        domain's own potential with the self-interaction correction).  Phase 2: per domain, 10
+        LOBPCG iterations (H applied to X, the Rayleigh quotient, the preconditioned residual W,
+        H applied to W and P, the Ritz problem over span{X, W[, P]}, X and P updated on the
+        domain).  Phase 3: normalisation, one ITP update, the level-set passes."""
+        two_pi = np.float32(2 * np.pi)
+        S = self.S
+        poisson = self.n_electrons > 1
+        if poisson and self.direct:
+            for m, Pm in self.Pdirect.items():
+                O().mj_rho_other(self.U, self.label, m, self.rho, S)
+                scratch = np.zeros(self.S3, np.float32)
+                for js in range(10):
+                    O().mj_jacobi(*((Pm, scratch) if js % 2 == 0 else (scratch, Pm)), self.rho, S, self.h2, two_pi)
+                O().mj_copy_for_label(Pm, self.Pother, self.label, m, S)
+        elif poisson:
+            O().mj_rho(self.U, self.rho, S)
+            for _ in range(4):
+                O().mj_jacobi(self.P, self.P2, self.rho, S, self.h2, two_pi)
+                self.P, self.P2 = self.P2, self.P
+            self.vcycle()
+        if not poisson:
+            self.Pother[:] = 0
+        elif not self.direct:
+            self.Pother[:] = self.P
+            if self.sic:
+                self.sic_pass()
+        if self.frame == 0:
+            self.LP[:] = 0
+            self.HP[:] = 0
+        at = C.addressof(self.atoms)
+        for m, r in enumerate(self.rows):
+            if np.float32(r["Z"]) == 0:
+                continue
+            for it in range(10):
+                hasP = self.frame > 0 or it > 0
+                O().lob_apply_h(self.U, self.HX, self.K, self.label, self.Pother, at, S, self.h, self.inv_h2)
+                if it == 0 and not hasP:
+                    self.LW[:] = 0
+                    self.HW[:] = 0
+                ip = self.lobpcg_inner(m).astype(np.float64)
+                lam = np.float32(ip[1] / ip[0]) if ip[0] > 0 else np.float32(0)
+                O().lob_residual(self.U, self.HX, self.LW, self.label, self.K, self.Pother, lam, m, S, self.inv_h2)
+                O().lob_apply_h(self.LW, self.HW, self.K, self.label, self.Pother, at, S, self.h, self.inv_h2)
+                if hasP:
+                    O().lob_apply_h(self.LP, self.HP, self.K, self.label, self.Pother, at, S, self.h, self.inv_h2)
+                ip2 = self.lobpcg_inner(m).astype(np.float64)
+                res = np.zeros(4)
+                (O().lob_ritz3 if hasP and ip2[6] > 1e-20 else O().lob_ritz2)(ip2, res)
+                c = res[1:].astype(np.float32)
+                O().lob_update(self.U, self.LW, self.LP, self.label, c[0], c[1], c[2], m, S)
+        acc = np.zeros(self.nA, np.uint32)
+        nf = np.zeros(self.nA, np.float32)
+        O().mj_norms_fixed(self.U, self.label, S, self.h3, self.nA, acc, nf)
+        O().mj_normalize(self.U, nf, self.label, at, S)
+        O().mj_update(self.U, self.Unext, self.K, self.label, self.Pother, at, self.nA, int(self.has_bare), S, self.h,
+                      self.half_d, self.dt)
+        self.U, self.Unext = self.Unext, self.U
+        self.frame += 1
+        for _ in range(max(1, self.spf)):
+            O().mj_evolve_boundary(self.label, self.label2, self.U, self.W, S, self.dt_w, self.curv)
+            self.label, self.label2 = self.label2, self.label
+
     def step(self):
+        if self.lobpcg:
+            self.steps_done += 1
+            self.lobpcg_frame()
+            return
         self.steps_done += 1
         sf = (self.steps_done - 1) % self.spf
         poisson = self.n_electrons > 1

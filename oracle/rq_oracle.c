@@ -2141,3 +2141,256 @@ void orc_rb_slice(const orc_rb_params* p, const float* U, const float* W, const 
     out[(int64_t)g * stride + stride - 1] = K[id];
   }
 }
+
+/* ======================================================================
+ * molecule.js LOBPCG frame (shaders molecule.js:1455-1724, host :3265-3740; the page's
+ * useLOBPCG switch, off by default, :1751).  f32 shaders restated with the same operation
+ * order; the Ritz solves are the page's double-precision JavaScript.
+ * ==================================================================== */
+
+/* applyH's own isInsideRc (molecule.js:1473-1477): only the label's own r_c sphere. */
+static inline int lob_inside_rc(int ci, int cj, int ck, uint32_t lbl, const orc_mj_atom* atoms, float h) {
+  const float rc = atoms[lbl].rc;
+  if (rc <= 0.f) return 0;
+  return mj_dist(ci, cj, ck, &atoms[lbl], h) < rc;
+}
+
+/* applyH (molecule.js:1483-1525): HU = -0.5*lap/h^2 + (-K + 2*Pother)*u on interior cells, 0 inside
+ * the own r_c sphere; a neighbour of another label or inside its label's sphere counts as the
+ * centre value (Neumann). */
+void orc_lob_apply_h(const float* U, float* HU, const float* K, const uint32_t* label, const float* Pother,
+                     const orc_mj_atom* atoms, int S, float h, float inv_h2) {
+  const int NN = S - 1;
+  const int64_t S2 = (int64_t)S * S;
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        const int64_t id = IDX(i, j, k, S);
+        const uint32_t L = label[id];
+        if (lob_inside_rc(i, j, k, L, atoms, h)) { HU[id] = 0.f; continue; }
+        const float uc = U[id];
+        const uint32_t lip = label[id + S2], lim = label[id - S2], ljp = label[id + S], ljm = label[id - S];
+        const uint32_t lkp = label[id + 1], lkm = label[id - 1];
+        const float uip = (lip == L && !lob_inside_rc(i + 1, j, k, lip, atoms, h)) ? U[id + S2] : uc;
+        const float uim = (lim == L && !lob_inside_rc(i - 1, j, k, lim, atoms, h)) ? U[id - S2] : uc;
+        const float ujp = (ljp == L && !lob_inside_rc(i, j + 1, k, ljp, atoms, h)) ? U[id + S] : uc;
+        const float ujm = (ljm == L && !lob_inside_rc(i, j - 1, k, ljm, atoms, h)) ? U[id - S] : uc;
+        const float ukp = (lkp == L && !lob_inside_rc(i, j, k + 1, lkp, atoms, h)) ? U[id + 1] : uc;
+        const float ukm = (lkm == L && !lob_inside_rc(i, j, k - 1, lkm, atoms, h)) ? U[id - 1] : uc;
+        const float lap = uip + uim + ujp + ujm + ukp + ukm - 6.0f * uc;
+        HU[id] = -0.5f * lap * inv_h2 + (-K[id] + 2.0f * Pother[id]) * uc;
+      }
+}
+
+/* lobpcgInner + lobpcgFinalize (molecule.js:1535-1648): the 12 f32 inner products over the
+ * cells of domain m -- <X|X> <X|HX> <W|W> <W|HW> <X|W> <X|HW> <P|P> <P|HP> <X|P> <X|HP> <W|P>
+ * <W|HP>, each term a*b*h^3 -- summed in the shaders' order.  Interior cells are numbered with k
+ * fastest; workgroup w (of nwg = min(256, ceil(cells/128))) thread l takes cells w*128+l, then
+ * every nwg*128-th; the 128 per-thread sums of a workgroup fold pairwise (l += l+s for s = 64 ..
+ * 1); the one finalize workgroup's thread l adds workgroup results l, l+128, .. in order and
+ * folds the same way. */
+#define LOB_NR 12
+#define LOB_WG 128
+void orc_lob_inner(const float* X, const float* HX, const float* W, const float* HW, const float* Pv,
+                   const float* HP, const uint32_t* label, uint32_t m, int S, float h3, float* sums) {
+  const int NM = S - 2;
+  const int64_t tot = (int64_t)NM * NM * NM;
+  const int nwg = (int)((tot + LOB_WG - 1) / LOB_WG) < 256 ? (int)((tot + LOB_WG - 1) / LOB_WG) : 256;
+  const int64_t stride = (int64_t)nwg * LOB_WG;
+  float* part = (float*)calloc((size_t)nwg * LOB_NR, sizeof(float));
+#pragma omp parallel for schedule(static)
+  for (int w = 0; w < nwg; ++w) {
+    float sn[LOB_WG][LOB_NR];
+    for (int l = 0; l < LOB_WG; ++l) {
+      for (int q = 0; q < LOB_NR; ++q) sn[l][q] = 0.f;
+      for (int64_t cell = (int64_t)w * LOB_WG + l; cell < tot; cell += stride) {
+        const int k = (int)(cell % NM) + 1, j = (int)((cell / NM) % NM) + 1, i = (int)(cell / ((int64_t)NM * NM)) + 1;
+        const int64_t id = IDX(i, j, k, S);
+        if (label[id] != m) continue;
+        const float x = X[id], hx = HX[id], wv = W[id], hw = HW[id], pv = Pv[id], hp = HP[id];
+        sn[l][0] += x * x * h3;
+        sn[l][1] += x * hx * h3;
+        sn[l][2] += wv * wv * h3;
+        sn[l][3] += wv * hw * h3;
+        sn[l][4] += x * wv * h3;
+        sn[l][5] += x * hw * h3;
+        sn[l][6] += pv * pv * h3;
+        sn[l][7] += pv * hp * h3;
+        sn[l][8] += x * pv * h3;
+        sn[l][9] += x * hp * h3;
+        sn[l][10] += wv * pv * h3;
+        sn[l][11] += wv * hp * h3;
+      }
+    }
+    for (int s = LOB_WG / 2; s > 0; s >>= 1)
+      for (int l = 0; l < s; ++l)
+        for (int q = 0; q < LOB_NR; ++q) sn[l][q] += sn[l + s][q];
+    for (int q = 0; q < LOB_NR; ++q) part[(size_t)w * LOB_NR + q] = sn[0][q];
+  }
+  float wg[LOB_WG][LOB_NR];
+  for (int l = 0; l < LOB_WG; ++l) {
+    for (int q = 0; q < LOB_NR; ++q) wg[l][q] = 0.f;
+    for (int w = l; w < nwg; w += LOB_WG)
+      for (int q = 0; q < LOB_NR; ++q) wg[l][q] += part[(size_t)w * LOB_NR + q];
+  }
+  for (int s = LOB_WG / 2; s > 0; s >>= 1)
+    for (int l = 0; l < s; ++l)
+      for (int q = 0; q < LOB_NR; ++q) wg[l][q] += wg[l + s][q];
+  for (int q = 0; q < LOB_NR; ++q) sums[q] = wg[0][q];
+  free(part);
+}
+
+/* lobpcgResidual (molecule.js:1652-1689): W = (HX - lambda*X) / (3/h^2 + |-K + 2*Pother| + 0.1) on
+ * domain m, 0 on every other interior cell. */
+void orc_lob_residual(const float* X, const float* HX, float* W, const uint32_t* label, const float* K,
+                      const float* Pot, float lam, uint32_t m, int S, float inv_h2) {
+  const int NN = S - 1;
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        const int64_t id = IDX(i, j, k, S);
+        if (label[id] != m) { W[id] = 0.f; continue; }
+        const float r = HX[id] - lam * X[id];
+        const float vEff = fabsf(-K[id] + 2.0f * Pot[id]);
+        const float diagH = 3.0f * inv_h2 + vEff + 0.1f;
+        W[id] = r / diagH;
+      }
+}
+
+/* lobpcgUpdate (molecule.js:1693-1724): on domain m, X = c0*X + c1*W + c2*P and P = c1*W + c2*P. */
+void orc_lob_update(float* X, const float* W, float* Pv, const uint32_t* label, float c0, float c1, float c2,
+                    uint32_t m, int S) {
+  const int NN = S - 1;
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        const int64_t id = IDX(i, j, k, S);
+        if (label[id] != m) continue;
+        const float x = X[id], w = W[id], pv = Pv[id];
+        X[id] = c0 * x + c1 * w + c2 * pv;
+        Pv[id] = c1 * w + c2 * pv;
+      }
+}
+
+/* Math.min / Math.max of JavaScript: NaN if either argument is NaN, -0 below +0. */
+static double js_min(double a, double b) {
+  if (a != a || b != b) return NAN;
+  if (a < b) return a;
+  if (b < a) return b;
+  return signbit(a) ? a : b;
+}
+static double js_max(double a, double b) {
+  if (a != a || b != b) return NAN;
+  if (a > b) return a;
+  if (b > a) return b;
+  return signbit(a) ? b : a;
+}
+
+/* solveRitz2x2 (molecule.js:3265-3295): the smaller root of det(H - lambda S) = 0 over span{X, W},
+ * its vector scaled to c'Sc = 1.  ip = the 12 sums; out = {lambda, c0, c1, c2}. */
+void orc_lob_ritz2(const double* ip, double* out) {
+  const double a11 = ip[1], a12 = ip[5], a22 = ip[3];
+  const double s11 = ip[0], s12 = ip[4], s22 = ip[2];
+  const double A = s11 * s22 - s12 * s12;
+  const double B = -(a11 * s22 + a22 * s11 - 2 * a12 * s12);
+  const double Cq = a11 * a22 - a12 * a12;
+  const double disc = B * B - 4 * A * Cq;
+  const double sq = sqrt(js_max(0, disc));
+  const double lam1 = (-B - sq) / (2 * A), lam2 = (-B + sq) / (2 * A);
+  const double lam = js_min(lam1, lam2);
+  const double r1 = a11 - lam * s11, r2 = a12 - lam * s12;
+  double c0, c1;
+  if (fabs(r1) > fabs(r2)) {
+    c1 = 1;
+    c0 = -r2 / r1;
+  } else if (fabs(r2) > 1e-15) {
+    c0 = 1;
+    c1 = -r1 / r2;
+  } else {
+    c0 = 1;
+    c1 = 0;
+  }
+  const double norm2 = c0 * c0 * s11 + 2 * c0 * c1 * s12 + c1 * c1 * s22;
+  const double inv = 1 / sqrt(js_max(1e-30, norm2));
+  out[0] = lam;
+  out[1] = c0 * inv;
+  out[2] = c1 * inv;
+  out[3] = 0;
+}
+
+/* solveRitz3x3 (molecule.js:3297-3388) over span{X, W, P}: Cholesky S = L L', the standard problem
+ * L^-1 H L^-T by 20 sweeps of cyclic Jacobi rotations, the smallest diagonal entry, c = L^-T y;
+ * the 2x2 solve when the Cholesky factor is not finite or has a diagonal below 1e-15. */
+void orc_lob_ritz3(const double* ip, double* out) {
+  const double S[3][3] = {{ip[0], ip[4], ip[8]}, {ip[4], ip[2], ip[10]}, {ip[8], ip[10], ip[6]}};
+  const double H[3][3] = {{ip[1], ip[5], ip[9]}, {ip[5], ip[3], ip[11]}, {ip[9], ip[11], ip[7]}};
+  double L[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  L[0][0] = sqrt(js_max(1e-30, S[0][0]));
+  L[1][0] = S[1][0] / L[0][0];
+  L[2][0] = S[2][0] / L[0][0];
+  L[1][1] = sqrt(js_max(1e-30, S[1][1] - L[1][0] * L[1][0]));
+  L[2][1] = (S[2][1] - L[2][0] * L[1][0]) / L[1][1];
+  L[2][2] = sqrt(js_max(1e-30, S[2][2] - L[2][0] * L[2][0] - L[2][1] * L[2][1]));
+  if (!isfinite(L[2][2]) || L[0][0] < 1e-15 || L[1][1] < 1e-15 || L[2][2] < 1e-15) {
+    orc_lob_ritz2(ip, out);
+    return;
+  }
+  double Li[3][3] = {{1 / L[0][0], 0, 0}, {0, 1 / L[1][1], 0}, {0, 0, 1 / L[2][2]}};
+  Li[1][0] = -L[1][0] * Li[0][0] * Li[1][1];
+  Li[2][0] = -(L[2][0] * Li[0][0] + L[2][1] * Li[1][0]) * Li[2][2];
+  Li[2][1] = -L[2][1] * Li[1][1] * Li[2][2];
+  double Bm[3][3], A[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += H[i][k] * Li[j][k];
+      Bm[i][j] = s;
+    }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += Li[i][k] * Bm[k][j];
+      A[i][j] = s;
+    }
+  double V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  static const int PQ[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+  for (int sweep = 0; sweep < 20; ++sweep)
+    for (int e = 0; e < 3; ++e) {
+      const int p = PQ[e][0], q = PQ[e][1];
+      const double apq = A[p][q];
+      if (fabs(apq) < 1e-15) continue;
+      const double tau = (A[q][q] - A[p][p]) / (2 * apq);
+      const double t = (tau >= 0 ? 1 : -1) / (fabs(tau) + sqrt(1 + tau * tau));
+      const double c = 1 / sqrt(1 + t * t);
+      const double s = t * c;
+      const double app = A[p][p], aqq = A[q][q];
+      A[p][p] = c * c * app - 2 * s * c * apq + s * s * aqq;
+      A[q][q] = s * s * app + 2 * s * c * apq + c * c * aqq;
+      A[p][q] = 0;
+      A[q][p] = 0;
+      for (int r = 0; r < 3; ++r) {
+        if (r == p || r == q) continue;
+        const double arp = A[r][p], arq = A[r][q];
+        A[r][p] = c * arp - s * arq;
+        A[p][r] = A[r][p];
+        A[r][q] = s * arp + c * arq;
+        A[q][r] = A[r][q];
+      }
+      for (int r = 0; r < 3; ++r) {
+        const double vrp = V[r][p], vrq = V[r][q];
+        V[r][p] = c * vrp - s * vrq;
+        V[r][q] = s * vrp + c * vrq;
+      }
+    }
+  int mi = 0;
+  if (A[1][1] < A[mi][mi]) mi = 1;
+  if (A[2][2] < A[mi][mi]) mi = 2;
+  const double y0 = V[0][mi], y1 = V[1][mi], y2 = V[2][mi];
+  out[0] = A[mi][mi];
+  out[1] = Li[0][0] * y0 + Li[1][0] * y1 + Li[2][0] * y2;
+  out[2] = Li[1][1] * y1 + Li[2][1] * y2;
+  out[3] = Li[2][2] * y2;
+}

@@ -69,7 +69,8 @@ class Config(C.Structure):
                 ("vcycle_interval", C.c_int32), ("mg_levels", C.c_int32), ("mg_pre", C.c_int32),
                 ("mg_post", C.c_int32), ("mg_coarse_sweeps", C.c_int32), ("sic", C.c_int32),
                 ("boundary_speed", C.c_double), ("curv_reg", C.c_double), ("sigma", C.c_double),
-                ("label_until", C.c_int32), ("chebyshev", C.c_int32), ("reserved", C.c_int32 * 6)]
+                ("label_until", C.c_int32), ("chebyshev", C.c_int32), ("lobpcg", C.c_int32),
+                ("reserved", C.c_int32 * 5)]
 
 
 class Atom(C.Structure):

@@ -135,7 +135,7 @@ static void free_ctx(rq_ctx* c) {
   for (auto& gx : c->graph)
     if (gx) cudaGraphExecDestroy(gx);
   void* ptrs[] = {c->U[0], c->U[1], c->P[0], c->P[1], c->K, c->W, c->bestU, c->rho, c->Pother, c->resid, c->lab[0], c->lab[1],
-                  c->Ec[0], c->Ec[1], c->fc, c->atoms5, c->scratch_atoms5, c->sic, c->sic2, c->pdirect, c->bin_start, c->bin_idx, c->bin_far, c->bin_zmax, c->atoms_mj, c->atoms_nm, c->Zdom, c->Zdom64, c->dnorm,
+                  c->Ec[0], c->Ec[1], c->fc, c->atoms5, c->scratch_atoms5, c->sic, c->sic2, c->pdirect, c->lob, c->lob_part, c->lob_scal, c->bin_start, c->bin_idx, c->bin_far, c->bin_zmax, c->atoms_mj, c->atoms_nm, c->Zdom, c->Zdom64, c->dnorm,
                   c->dpd, c->dF, c->dsum, c->unorm, c->scale, c->err, c->seeds, c->scale64, c->Kext};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -179,6 +179,11 @@ static int alloc_all(rq_ctx* c) {
       DALLOC(c->sic, S3 * sizeof(float));
       DALLOC(c->sic2, S3 * sizeof(float));
       if (mj_direct(c)) DALLOC(c->pdirect, S3 * sizeof(float) * n);
+    }
+    if (c->cfg.lobpcg) {
+      DALLOC(c->lob, S3 * sizeof(float) * 5);
+      DALLOC(c->lob_part, sizeof(float) * kLobMaxWG * kLobNR);
+      DALLOC(c->lob_scal, sizeof(float) * kLobScal);
     }
     const int SC = c->g.NN / 2 + 1;
     c->gc = make_geo(SC);
@@ -225,6 +230,8 @@ extern "C" int rq_create(const rq_config* cfg, const rq_atom* atoms, int32_t n_a
   if (cfg->flavor < 0 || cfg->flavor > 2 || cfg->precision < 0 || cfg->precision > 1) return RQ_EINVAL;
   if (cfg->precision == RQ_PREC_FP64 && cfg->flavor != RQ_FLAVOR_NEW) return RQ_ENOTSUP;
   if (cfg->sic != 0 && cfg->flavor != RQ_FLAVOR_MOLECULE_JS) return RQ_ENOTSUP;  // SIC is molecule.js's
+  if (cfg->lobpcg != 0 && cfg->flavor != RQ_FLAVOR_MOLECULE_JS) return RQ_ENOTSUP;
+  if (cfg->lobpcg != 0 && cfg->chebyshev != 0) return RQ_EINVAL;  // the page switches one off (:5472-5478)
   if (cfg->chebyshev != 0) {  // molecule.js's Chebyshev update tests only the own r_c sphere (:368-372)
     if (cfg->flavor != RQ_FLAVOR_MOLECULE_JS) return RQ_ENOTSUP;
     for (int q = 0; q < n_atoms; ++q)
@@ -433,7 +440,9 @@ static int schedule_period(const rq_ctx* c) {
   long p = 1;
   switch (f.flavor) {
     case RQ_FLAVOR_SOLVER_PY: p = lcm(lcm(f.poisson_interval, f.norm_interval), f.label_interval); break;
-    case RQ_FLAVOR_MOLECULE_JS: p = (long)f.steps_per_frame * std::max(1, mj_sic_interval(c)); break;
+    case RQ_FLAVOR_MOLECULE_JS:
+      p = f.lobpcg ? 1 : (long)f.steps_per_frame * std::max(1, mj_sic_interval(c));
+      break;
     default: p = lcm(lcm(f.poisson_interval, f.norm_interval), f.label_interval); break;
   }
   return p > 4096 ? 0 : (int)p;
@@ -458,9 +467,11 @@ extern "C" int rq_step(rq_ctx* c, int32_t n) {
     const bool straddle = lu > 0 && c->steps_done < lu && c->steps_done + period > lu;
     // (a period boundary never leaves an early Jacobi sweep pending: the step before a Poisson step
     // is never the last of a period, as the period is a multiple of poisson_interval)
-    // (with SIC, frame 0 never corrects: the first period runs eagerly, the later ones repeat)
+    // (with SIC, frame 0 never corrects: the first period runs eagerly, the later ones repeat;
+    // likewise a first LOBPCG frame, which starts without a search direction)
     const bool aligned = !c->prof && !c->cfg.chebyshev && !straddle && period > 0 && c->steps_done % period == 0 && left >= period &&
-                         c->sp_jdone == 0 && !(mj_sic_interval(c) > 0 && c->frame == 0);
+                         c->sp_jdone == 0 && !(mj_sic_interval(c) > 0 && c->frame == 0) &&
+                         !(c->cfg.lobpcg && c->frame == 0);
     if (!aligned) {
       // run eagerly up to the next period boundary (or all that is left)
       int todo = left;
@@ -497,7 +508,7 @@ extern "C" int rq_step(rq_ctx* c, int32_t n) {
       c->nm_pending = (post >> 4) & 1;
       c->nm_age = post >> 5;
       c->steps_done += period;
-      if (c->cfg.flavor == RQ_FLAVOR_MOLECULE_JS) c->frame += period / c->cfg.steps_per_frame;
+      if (c->cfg.flavor == RQ_FLAVOR_MOLECULE_JS) c->frame += c->cfg.lobpcg ? period : period / c->cfg.steps_per_frame;
       c->launches += c->graph_launches[key];
     }
     left -= period;

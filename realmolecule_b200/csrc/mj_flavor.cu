@@ -155,7 +155,108 @@ static float mj_cheb_omega(rq_ctx* c) {
   return (float)std::min(1.95, std::max(1.0, omega));
 }
 
+// One LOBPCG frame (doLOBPCGStep, molecule.js:3323-3740).  Phase 1: the Poisson solve on the current
+// psi -- the direct per-electron path, or 4 Jacobi sweeps and the V-cycle (vcycleEnabled, :1815) --
+// and Pother: P, minus every domain's own potential when the correction is on (:3405-3451; no
+// SIC_INTERVAL here).  Phase 2: per domain 10 iterations (:3460-3588) of H applied to X, the
+// Rayleigh quotient, the preconditioned residual W, H applied to W and P, the Ritz problem over
+// span{X, W[, P]} and the update of X and P on the domain; the page reads the sums back and solves
+// the small problem on the host, here one device thread does it (k_lob_finalize), so no step waits
+// for the host.  Phase 3 (:3591-3660): the fixed-point normalisation, one ITP update, the level-set
+// passes.  The search direction P persists across frames; frame 0 starts without one.
+static int mj_lobpcg_frame(rq_ctx* c) {
+  const MjParams p = mj_params(c);
+  const rq_config& f = c->cfg;
+  const bool poisson = p.n_electrons > 1.0;
+  const double ip = interior(c->g);
+  const bool direct = mj_direct(c);
+  const size_t S3 = (size_t)c->g.S3;
+  if (poisson && direct) {
+    for (int m = 0; m < c->n_atoms; ++m) {
+      if ((float)c->atoms[m].Z == 0.f) continue;
+      LAUNCH(RQ_KC_POISSON, 128 * ip,
+             launch_mj_direct_domain((float*)c->U[c->cu], c->lab[c->cl], c->Pother, m, c->pdirect + (size_t)m * S3,
+                                     c->sic, c->rho, c->g, p.h2, p.two_pi, c->st));
+    }
+  } else if (poisson) {
+    for (int js = 0; js < 4; ++js) {
+      LAUNCH(RQ_KC_POISSON, 12 * ip,
+             launch_mj_jacobi((float*)c->P[c->cp], (float*)c->P[1 - c->cp], (float*)c->U[c->cu], c->g, p.h2, p.two_pi,
+                              c->st));
+      c->cp ^= 1;
+    }
+    LAUNCH(RQ_KC_MG, 40 * ip,
+           launch_mj_vcycle((float*)c->P[c->cp], (float*)c->U[c->cu], c->rho, c->resid, c->Ec[0], c->Ec[1], c->fc, c->g,
+                            c->gc, p.h2, p.inv_h2, p.two_pi, c->st));
+  }
+  if (!poisson) {
+    CK(cudaMemsetAsync(c->Pother, 0, S3 * sizeof(float), c->st));
+  } else if (!direct) {
+    CK(cudaMemcpyAsync(c->Pother, c->P[c->cp], S3 * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
+    if (f.sic)
+      for (int m = 0; m < c->n_atoms; ++m) {
+        const float Zm = (float)c->atoms[m].Z;
+        if (Zm == 0.f) continue;
+        const float frac = Zm > 1.f ? 1.0f / Zm : 1.0f;
+        LAUNCH(RQ_KC_MG, 120 * ip,
+               launch_mj_sic_domain((float*)c->U[c->cu], c->lab[c->cl], c->Pother, m, frac, c->rho, c->sic, c->sic2,
+                                    c->resid, c->Ec[0], c->Ec[1], c->fc, c->g, c->gc, p.h2, p.inv_h2, p.two_pi,
+                                    c->st));
+      }
+  }
+  float *HX = c->lob, *LW = HX + S3, *HW = LW + S3, *LP = HW + S3, *HP = LP + S3;
+  if (c->frame == 0) CK(cudaMemsetAsync(LP, 0, 2 * S3 * sizeof(float), c->st));  // P and HP
+  const int nwg = lob_workgroups(c->g);
+  float* X = (float*)c->U[c->cu];
+  const MjAtom* at = atoms_dev(c);
+  for (int m = 0; m < c->n_atoms; ++m) {
+    if ((float)c->atoms[m].Z == 0.f) continue;
+    for (int it = 0; it < 10; ++it) {
+      const bool hasP = c->frame > 0 || it > 0;
+      LAUNCH(RQ_KC_UPDATE, 20 * ip,
+             launch_lob_apply_h(X, HX, (float*)c->K, c->lab[c->cl], c->Pother, at, c->g, p.h, p.inv_h2, p.hasBare,
+                                c->st));
+      if (it == 0 && !hasP) CK(cudaMemsetAsync(LW, 0, 2 * S3 * sizeof(float), c->st));  // W and HW
+      LAUNCH(RQ_KC_NORMALIZE, 28 * ip,
+             launch_lob_inner(X, HX, LW, HW, LP, HP, c->lab[c->cl], m, c->g, p.h3, c->lob_part, c->st));
+      LAUNCH(RQ_KC_NORMALIZE, 48.0 * nwg, launch_lob_finalize(c->lob_part, nwg, true, hasP, c->lob_scal, c->st));
+      LAUNCH(RQ_KC_UPDATE, 24 * ip,
+             launch_lob_residual(X, HX, LW, c->lab[c->cl], (float*)c->K, c->Pother, c->lob_scal, m, c->g, p.inv_h2,
+                                 c->st));
+      LAUNCH(RQ_KC_UPDATE, 20 * ip,
+             launch_lob_apply_h(LW, HW, (float*)c->K, c->lab[c->cl], c->Pother, at, c->g, p.h, p.inv_h2, p.hasBare,
+                                c->st));
+      if (hasP)
+        LAUNCH(RQ_KC_UPDATE, 20 * ip,
+               launch_lob_apply_h(LP, HP, (float*)c->K, c->lab[c->cl], c->Pother, at, c->g, p.h, p.inv_h2, p.hasBare,
+                                  c->st));
+      LAUNCH(RQ_KC_NORMALIZE, 28 * ip,
+             launch_lob_inner(X, HX, LW, HW, LP, HP, c->lab[c->cl], m, c->g, p.h3, c->lob_part, c->st));
+      LAUNCH(RQ_KC_NORMALIZE, 48.0 * nwg, launch_lob_finalize(c->lob_part, nwg, false, hasP, c->lob_scal, c->st));
+      LAUNCH(RQ_KC_UPDATE, 24 * ip, launch_lob_update(X, LW, LP, c->lab[c->cl], c->lob_scal + 1, m, c->g, c->st));
+    }
+  }
+  CK(cudaMemsetAsync(c->unorm, 0, sizeof(unsigned) * c->n_atoms, c->st));
+  LAUNCH(RQ_KC_NORMALIZE, 8 * ip, launch_mj_accum_norms(X, c->lab[c->cl], c->g, p.h3, c->unorm, c->st));
+  LAUNCH(RQ_KC_NORMALIZE, 8.0 * c->n_atoms, launch_mj_norm_scale(c->unorm, at, c->n_atoms, c->scale, c->st));
+  LAUNCH(RQ_KC_NORMALIZE, 12 * ip, launch_mj_apply_scale(X, c->lab[c->cl], c->scale, c->g, c->st));
+  LAUNCH(RQ_KC_UPDATE, 20 * ip,
+         launch_mj_update(X, (float*)c->U[1 - c->cu], (float*)c->K, c->lab[c->cl], c->Pother, c->g, p.half_d, p.dt,
+                          p.h3, c->n_atoms, nullptr, c->st));
+  c->cu ^= 1;
+  c->frame++;
+  const int wsteps = f.steps_per_frame > 1 ? f.steps_per_frame : 1;  // W_STEPS_PER_FRAME (:107)
+  for (int q = 0; q < wsteps; ++q) {
+    LAUNCH(RQ_KC_LABELS, 20 * ip,
+           launch_mj_evolve(c->lab[c->cl], c->lab[1 - c->cl], (float*)c->U[c->cu], c->W, at, c->n_atoms, c->g, p.dt_w,
+                            p.curvReg, p.h, p.hasBare, c->st));
+    c->cl ^= 1;
+  }
+  return RQ_OK;
+}
+
 int mj_step_one(rq_ctx* c, int s) {
+  if (c->cfg.lobpcg) return mj_lobpcg_frame(c);
   const MjParams p = mj_params(c);
   const rq_config& f = c->cfg;
   const int spf = f.steps_per_frame;

@@ -9,6 +9,8 @@
 //  * rhoTotal = psi^2 is computed inside the Jacobi sweep (no separate pass);
 //  * the u32 fixed-point norms (molecule.js:912-946) are aggregated per block in shared memory
 //    before the global atomics -- integer adds, so the result is bit-exact in any order.
+#include <algorithm>
+
 #include "rq_flavors.h"
 #include "rq_kernels.h"
 
@@ -804,6 +806,398 @@ cudaError_t launch_mj_extract(const float* U, const int* label, const float* K, 
                               const Geo& g, int sk, float* out, cudaStream_t st) {
   const unsigned b = (unsigned)((g.S + 15) / 16);
   k_mj_extract<<<dim3(b, b), dim3(16, 16), 0, st>>>(U, label, K, atoms, nAt, g, sk, out);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------
+// LOBPCG frames (molecule.js:1455-1724 shaders, :3265-3740 host).  f32 shaders restated with
+// the same operations in the same order; the inner products keep the shaders' workgroup trees;
+// the Ritz problems -- double-precision JavaScript in the page, solved on the host between
+// dispatches -- run in one device thread with explicitly rounded FP64 operations in the page's
+// order, so the whole frame stays on the GPU (no read-back per iteration) and its results are
+// those of the page's arithmetic.
+// ---------------------------------------------------------------------------------------
+#define D_ADD(a, b) __dadd_rn((a), (b))
+#define D_SUB(a, b) __dsub_rn((a), (b))
+#define D_MUL(a, b) __dmul_rn((a), (b))
+#define D_DIV(a, b) __ddiv_rn((a), (b))
+#define D_SQRT(a) __dsqrt_rn((a))
+
+// applyH's own isInsideRc (molecule.js:1473-1477): only the label's own r_c sphere.
+__device__ __forceinline__ bool lob_inside_rc(int ci, int cj, int ck, int lbl, const MjAtom* __restrict__ atoms,
+                                              float h) {
+  const MjAtom a = atoms[lbl];
+  return a.rc > 0.f && mj_dist(ci, cj, ck, a, h) < a.rc;
+}
+
+// applyH (molecule.js:1483-1525): HU = -0.5*lap/h^2 + (-K + 2*Pother)*u, 0 inside the own r_c
+// sphere, a neighbour of another label or inside its label's sphere replaced by the centre.
+// Without bare nuclei the stored exclusion bit is exactly this test (packed words compare equal
+// iff same label and the neighbour is not excluded); with them (BARE) the bit also marks the
+// bare nuclei's spheres, which this shader ignores, so the spheres are tested directly.
+template <bool BARE>
+__global__ void __launch_bounds__(256) k_lob_apply_h(const float* __restrict__ U, float* __restrict__ HU,
+                                                     const float* __restrict__ K, const int* __restrict__ label,
+                                                     const float* __restrict__ Pother, const MjAtom* __restrict__ atoms,
+                                                     Geo g, float h, float inv_h2) {
+  const int k = 1 + blockIdx.x * kThreadsK + threadIdx.x;
+  const int j = 1 + blockIdx.y * kThreadsJ + threadIdx.y;
+  const int i0 = 1 + blockIdx.z * kMarch;
+  if (k >= g.NN || j >= g.NN || i0 >= g.NN) return;
+  const int iend = min(i0 + kMarch, g.NN);
+  const long long S = g.S, S2 = g.S2;
+  long long id = (long long)i0 * S2 + j * S + k;
+  float u_m = __ldg(U + id - S2), u_c = __ldg(U + id);
+  int l_m = __ldg(label + id - S2), l_c = __ldg(label + id);
+  for (int i = i0; i < iend; ++i, id += S2) {
+    const float u_p = __ldg(U + id + S2);
+    const int l_p = __ldg(label + id + S2);
+    const int ljp = __ldg(label + id + S), ljm = __ldg(label + id - S), lkp = __ldg(label + id + 1),
+              lkm = __ldg(label + id - 1);
+    bool excl, up, um, ujp, ujm, ukp, ukm;  // excl: centre excluded; uX: neighbour X is used
+    if (BARE) {
+      const int L = l_c & kMjMask;
+      excl = lob_inside_rc(i, j, k, L, atoms, h);
+      up = (l_p & kMjMask) == L && !lob_inside_rc(i + 1, j, k, l_p & kMjMask, atoms, h);
+      um = (l_m & kMjMask) == L && !lob_inside_rc(i - 1, j, k, l_m & kMjMask, atoms, h);
+      ujp = (ljp & kMjMask) == L && !lob_inside_rc(i, j + 1, k, ljp & kMjMask, atoms, h);
+      ujm = (ljm & kMjMask) == L && !lob_inside_rc(i, j - 1, k, ljm & kMjMask, atoms, h);
+      ukp = (lkp & kMjMask) == L && !lob_inside_rc(i, j, k + 1, lkp & kMjMask, atoms, h);
+      ukm = (lkm & kMjMask) == L && !lob_inside_rc(i, j, k - 1, lkm & kMjMask, atoms, h);
+    } else {
+      excl = (l_c & kMjExcl) != 0;
+      up = l_p == l_c; um = l_m == l_c; ujp = ljp == l_c; ujm = ljm == l_c; ukp = lkp == l_c; ukm = lkm == l_c;
+    }
+    float out = 0.0f;
+    if (!excl) {
+      const float a = up ? u_p : u_c;
+      const float b = um ? u_m : u_c;
+      const float c = ujp ? __ldg(U + id + S) : u_c;
+      const float d = ujm ? __ldg(U + id - S) : u_c;
+      const float e = ukp ? __ldg(U + id + 1) : u_c;
+      const float f = ukm ? __ldg(U + id - 1) : u_c;
+      const float lap = F_SUB(F_ADD(F_ADD(F_ADD(F_ADD(F_ADD(a, b), c), d), e), f), F_MUL(6.0f, u_c));
+      out = F_ADD(F_MUL(F_MUL(-0.5f, lap), inv_h2), F_MUL(F_ADD(-__ldg(K + id), F_MUL(2.0f, __ldg(Pother + id))), u_c));
+    }
+    HU[id] = out;
+    u_m = u_c; u_c = u_p; l_m = l_c; l_c = l_p;
+  }
+}
+
+// lobpcgInner (molecule.js:1535-1610): interior cells numbered with k fastest; block w thread l
+// takes cells w*128+l, then every gridDim*128-th, summing a*b*h^3 for the 12 products over the
+// cells of domain m; the block's 128 sums fold pairwise (l += l+s, s = 64 .. 1).
+__global__ void __launch_bounds__(kLobWG) k_lob_inner(const float* __restrict__ X, const float* __restrict__ HX,
+                                                      const float* __restrict__ W, const float* __restrict__ HW,
+                                                      const float* __restrict__ Pv, const float* __restrict__ HP,
+                                                      const int* __restrict__ label, int m, Geo g, float h3,
+                                                      float* __restrict__ partials) {
+  __shared__ float sn[kLobWG][kLobNR + 1];
+  const int l = threadIdx.x;
+  float acc[kLobNR];
+#pragma unroll
+  for (int q = 0; q < kLobNR; ++q) acc[q] = 0.0f;
+  const unsigned NM = (unsigned)(g.NN - 1), tot = NM * NM * NM, stride = gridDim.x * kLobWG;
+  for (unsigned cell = blockIdx.x * kLobWG + l; cell < tot; cell += stride) {
+    const unsigned k = cell % NM + 1, j = (cell / NM) % NM + 1, i = cell / (NM * NM) + 1;
+    const long long id = (long long)i * g.S2 + (long long)j * g.S + k;
+    if ((__ldg(label + id) & kMjMask) != m) continue;
+    const float x = __ldg(X + id), hx = __ldg(HX + id), w = __ldg(W + id), hw = __ldg(HW + id), pv = __ldg(Pv + id),
+                hp = __ldg(HP + id);
+    acc[0] = F_ADD(acc[0], F_MUL(F_MUL(x, x), h3));
+    acc[1] = F_ADD(acc[1], F_MUL(F_MUL(x, hx), h3));
+    acc[2] = F_ADD(acc[2], F_MUL(F_MUL(w, w), h3));
+    acc[3] = F_ADD(acc[3], F_MUL(F_MUL(w, hw), h3));
+    acc[4] = F_ADD(acc[4], F_MUL(F_MUL(x, w), h3));
+    acc[5] = F_ADD(acc[5], F_MUL(F_MUL(x, hw), h3));
+    acc[6] = F_ADD(acc[6], F_MUL(F_MUL(pv, pv), h3));
+    acc[7] = F_ADD(acc[7], F_MUL(F_MUL(pv, hp), h3));
+    acc[8] = F_ADD(acc[8], F_MUL(F_MUL(x, pv), h3));
+    acc[9] = F_ADD(acc[9], F_MUL(F_MUL(x, hp), h3));
+    acc[10] = F_ADD(acc[10], F_MUL(F_MUL(w, pv), h3));
+    acc[11] = F_ADD(acc[11], F_MUL(F_MUL(w, hp), h3));
+  }
+#pragma unroll
+  for (int q = 0; q < kLobNR; ++q) sn[l][q] = acc[q];
+  __syncthreads();
+  for (int s = kLobWG / 2; s > 0; s >>= 1) {
+    if (l < s)
+#pragma unroll
+      for (int q = 0; q < kLobNR; ++q) sn[l][q] = F_ADD(sn[l][q], sn[l + s][q]);
+    __syncthreads();
+  }
+  if (l == 0)
+#pragma unroll
+    for (int q = 0; q < kLobNR; ++q) partials[blockIdx.x * kLobNR + q] = sn[0][q];
+}
+
+// JavaScript Math.min / Math.max: NaN if either argument is NaN, -0 below +0.
+__device__ __forceinline__ double js_min(double a, double b) {
+  if (isnan(a) || isnan(b)) return __longlong_as_double(0x7ff8000000000000LL);
+  if (a < b) return a;
+  if (b < a) return b;
+  return signbit(a) ? a : b;
+}
+__device__ __forceinline__ double js_max(double a, double b) {
+  if (isnan(a) || isnan(b)) return __longlong_as_double(0x7ff8000000000000LL);
+  if (a > b) return a;
+  if (b > a) return b;
+  return signbit(a) ? b : a;
+}
+
+// solveRitz2x2 (molecule.js:3265-3295) on ip = the 12 sums: the smaller root lambda of
+// det(H - lambda S) = 0 over span{X, W} and its vector scaled to c'Sc = 1.  out = {lambda, c0..c2}.
+__device__ void lob_ritz2(const double* ip, double* out) {
+  const double a11 = ip[1], a12 = ip[5], a22 = ip[3], s11 = ip[0], s12 = ip[4], s22 = ip[2];
+  const double A = D_SUB(D_MUL(s11, s22), D_MUL(s12, s12));
+  const double B = -D_SUB(D_ADD(D_MUL(a11, s22), D_MUL(a22, s11)), D_MUL(D_MUL(2.0, a12), s12));
+  const double Cq = D_SUB(D_MUL(a11, a22), D_MUL(a12, a12));
+  const double disc = D_SUB(D_MUL(B, B), D_MUL(D_MUL(4.0, A), Cq));
+  const double sq = D_SQRT(js_max(0.0, disc));
+  const double lam1 = D_DIV(D_SUB(-B, sq), D_MUL(2.0, A));
+  const double lam2 = D_DIV(D_ADD(-B, sq), D_MUL(2.0, A));
+  const double lam = js_min(lam1, lam2);
+  const double r1 = D_SUB(a11, D_MUL(lam, s11)), r2 = D_SUB(a12, D_MUL(lam, s12));
+  double c0, c1;
+  if (fabs(r1) > fabs(r2)) {
+    c1 = 1.0;
+    c0 = D_DIV(-r2, r1);
+  } else if (fabs(r2) > 1e-15) {
+    c0 = 1.0;
+    c1 = D_DIV(-r1, r2);
+  } else {
+    c0 = 1.0;
+    c1 = 0.0;
+  }
+  const double norm2 =
+      D_ADD(D_ADD(D_MUL(D_MUL(c0, c0), s11), D_MUL(D_MUL(D_MUL(2.0, c0), c1), s12)), D_MUL(D_MUL(c1, c1), s22));
+  const double inv = D_DIV(1.0, D_SQRT(js_max(1e-30, norm2)));
+  out[0] = lam;
+  out[1] = D_MUL(c0, inv);
+  out[2] = D_MUL(c1, inv);
+  out[3] = 0.0;
+}
+
+// solveRitz3x3 (molecule.js:3297-3388) over span{X, W, P}: Cholesky S = L L', the standard
+// problem L^-1 H L^-T by 20 sweeps of cyclic Jacobi rotations, the smallest diagonal entry,
+// c = L^-T y; the 2x2 problem when the factor is not finite or a diagonal is below 1e-15.
+__device__ void lob_ritz3(const double* ip, double* out) {
+  const double S[3][3] = {{ip[0], ip[4], ip[8]}, {ip[4], ip[2], ip[10]}, {ip[8], ip[10], ip[6]}};
+  const double H[3][3] = {{ip[1], ip[5], ip[9]}, {ip[5], ip[3], ip[11]}, {ip[9], ip[11], ip[7]}};
+  double L00 = D_SQRT(js_max(1e-30, S[0][0]));
+  double L10 = D_DIV(S[1][0], L00), L20 = D_DIV(S[2][0], L00);
+  double L11 = D_SQRT(js_max(1e-30, D_SUB(S[1][1], D_MUL(L10, L10))));
+  double L21 = D_DIV(D_SUB(S[2][1], D_MUL(L20, L10)), L11);
+  double L22 = D_SQRT(js_max(1e-30, D_SUB(D_SUB(S[2][2], D_MUL(L20, L20)), D_MUL(L21, L21))));
+  if (!isfinite(L22) || L00 < 1e-15 || L11 < 1e-15 || L22 < 1e-15) {
+    lob_ritz2(ip, out);
+    return;
+  }
+  double Li[3][3] = {{D_DIV(1.0, L00), 0.0, 0.0}, {0.0, D_DIV(1.0, L11), 0.0}, {0.0, 0.0, D_DIV(1.0, L22)}};
+  Li[1][0] = D_MUL(D_MUL(-L10, Li[0][0]), Li[1][1]);
+  Li[2][0] = D_MUL(-D_ADD(D_MUL(L20, Li[0][0]), D_MUL(L21, Li[1][0])), Li[2][2]);
+  Li[2][1] = D_MUL(D_MUL(-L21, Li[1][1]), Li[2][2]);
+  double Bm[3][3], A[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) s = D_ADD(s, D_MUL(H[i][k], Li[j][k]));
+      Bm[i][j] = s;
+    }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) s = D_ADD(s, D_MUL(Li[i][k], Bm[k][j]));
+      A[i][j] = s;
+    }
+  double V[3][3] = {{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {0.0, 0.0, 1.0}};
+  for (int sweep = 0; sweep < 20; ++sweep)
+    for (int e = 0; e < 3; ++e) {
+      const int p = e == 2 ? 1 : 0, q = e == 0 ? 1 : 2;  // (0,1), (0,2), (1,2)
+      const double apq = A[p][q];
+      if (fabs(apq) < 1e-15) continue;
+      const double tau = D_DIV(D_SUB(A[q][q], A[p][p]), D_MUL(2.0, apq));
+      const double t = D_DIV(tau >= 0 ? 1.0 : -1.0, D_ADD(fabs(tau), D_SQRT(D_ADD(1.0, D_MUL(tau, tau)))));
+      const double c = D_DIV(1.0, D_SQRT(D_ADD(1.0, D_MUL(t, t))));
+      const double s = D_MUL(t, c);
+      const double app = A[p][p], aqq = A[q][q];
+      A[p][p] = D_ADD(D_SUB(D_MUL(D_MUL(c, c), app), D_MUL(D_MUL(D_MUL(2.0, s), c), apq)), D_MUL(D_MUL(s, s), aqq));
+      A[q][q] = D_ADD(D_ADD(D_MUL(D_MUL(s, s), app), D_MUL(D_MUL(D_MUL(2.0, s), c), apq)), D_MUL(D_MUL(c, c), aqq));
+      A[p][q] = 0.0;
+      A[q][p] = 0.0;
+      for (int r = 0; r < 3; ++r) {
+        if (r == p || r == q) continue;
+        const double arp = A[r][p], arq = A[r][q];
+        A[r][p] = D_SUB(D_MUL(c, arp), D_MUL(s, arq));
+        A[p][r] = A[r][p];
+        A[r][q] = D_ADD(D_MUL(s, arp), D_MUL(c, arq));
+        A[q][r] = A[r][q];
+      }
+      for (int r = 0; r < 3; ++r) {
+        const double vrp = V[r][p], vrq = V[r][q];
+        V[r][p] = D_SUB(D_MUL(c, vrp), D_MUL(s, vrq));
+        V[r][q] = D_ADD(D_MUL(s, vrp), D_MUL(c, vrq));
+      }
+    }
+  int mi = 0;
+  if (A[1][1] < A[mi][mi]) mi = 1;
+  if (A[2][2] < A[mi][mi]) mi = 2;
+  const double y0 = V[0][mi], y1 = V[1][mi], y2 = V[2][mi];
+  out[0] = A[mi][mi];
+  out[1] = D_ADD(D_ADD(D_MUL(Li[0][0], y0), D_MUL(Li[1][0], y1)), D_MUL(Li[2][0], y2));
+  out[2] = D_ADD(D_MUL(Li[1][1], y1), D_MUL(Li[2][1], y2));
+  out[3] = D_MUL(Li[2][2], y2);
+}
+
+// lobpcgFinalize (molecule.js:1612-1648) -- thread l adds block results l, l+128, .. in order, the
+// same pairwise fold -- and then, in thread 0, the page's host step on the 12 sums:
+//   FIRST pass: lambda = <X|HX> / <X|X> in double, stored as f32 (0 when <X|X> <= 0, :3486);
+//   second pass: the Ritz problem (3x3 when hasP and <P|P> > 1e-20, else 2x2, :3570-3576), its
+//   coefficients stored as f32 (:3581).
+// scal: [0] lambda, [1..3] coefficients, [4..15] second-pass sums, [16..27] first-pass sums,
+// [28] the Ritz value (f32).
+template <bool FIRST>
+__global__ void __launch_bounds__(kLobWG) k_lob_finalize(const float* __restrict__ partials, int nwg, int hasP,
+                                                         float* __restrict__ scal) {
+  __shared__ float wg[kLobWG][kLobNR + 1];
+  const int l = threadIdx.x;
+  float acc[kLobNR];
+#pragma unroll
+  for (int q = 0; q < kLobNR; ++q) acc[q] = 0.0f;
+  for (int w = l; w < nwg; w += kLobWG)
+#pragma unroll
+    for (int q = 0; q < kLobNR; ++q) acc[q] = F_ADD(acc[q], partials[w * kLobNR + q]);
+#pragma unroll
+  for (int q = 0; q < kLobNR; ++q) wg[l][q] = acc[q];
+  __syncthreads();
+  for (int s = kLobWG / 2; s > 0; s >>= 1) {
+    if (l < s)
+#pragma unroll
+      for (int q = 0; q < kLobNR; ++q) wg[l][q] = F_ADD(wg[l][q], wg[l + s][q]);
+    __syncthreads();
+  }
+  if (l != 0) return;
+  double ip[kLobNR];
+  for (int q = 0; q < kLobNR; ++q) {
+    ip[q] = (double)wg[0][q];
+    scal[(FIRST ? 16 : 4) + q] = wg[0][q];
+  }
+  if (FIRST) {
+    scal[0] = ip[0] > 0.0 ? __double2float_rn(D_DIV(ip[1], ip[0])) : 0.0f;
+  } else {
+    double r[4];
+    if (hasP && ip[6] > 1e-20)
+      lob_ritz3(ip, r);
+    else
+      lob_ritz2(ip, r);
+    scal[1] = __double2float_rn(r[1]);
+    scal[2] = __double2float_rn(r[2]);
+    scal[3] = __double2float_rn(r[3]);
+    scal[28] = __double2float_rn(r[0]);
+  }
+}
+
+// lobpcgResidual (molecule.js:1652-1689): on domain m W = (HX - lambda*X) / (3/h^2 + |-K + 2*Pother|
+// + 0.1), 0 on every other interior cell; lambda read from the device.
+__global__ void __launch_bounds__(256) k_lob_residual(const float* __restrict__ X, const float* __restrict__ HX,
+                                                      float* __restrict__ W, const int* __restrict__ label,
+                                                      const float* __restrict__ K, const float* __restrict__ Pot,
+                                                      const float* __restrict__ lam, int m, Geo g, float inv_h2) {
+  const int k = 1 + blockIdx.x * 32 + threadIdx.x, j = 1 + blockIdx.y * 8 + threadIdx.y, i = 1 + blockIdx.z;
+  if (k >= g.NN || j >= g.NN) return;
+  const long long id = (long long)i * g.S2 + (long long)j * g.S + k;
+  if ((__ldg(label + id) & kMjMask) != m) {
+    W[id] = 0.0f;
+    return;
+  }
+  const float r = F_SUB(__ldg(HX + id), F_MUL(*lam, __ldg(X + id)));
+  const float vEff = fabsf(F_ADD(-__ldg(K + id), F_MUL(2.0f, __ldg(Pot + id))));
+  const float diagH = F_ADD(F_ADD(F_MUL(3.0f, inv_h2), vEff), 0.1f);
+  W[id] = F_DIV(r, diagH);
+}
+
+// lobpcgUpdate (molecule.js:1693-1724): on domain m X = c0*X + c1*W + c2*P, P = c1*W + c2*P.
+__global__ void __launch_bounds__(256) k_lob_update(float* __restrict__ X, const float* __restrict__ W,
+                                                    float* __restrict__ Pv, const int* __restrict__ label,
+                                                    const float* __restrict__ coef, int m, Geo g) {
+  const int k = 1 + blockIdx.x * 32 + threadIdx.x, j = 1 + blockIdx.y * 8 + threadIdx.y, i = 1 + blockIdx.z;
+  if (k >= g.NN || j >= g.NN) return;
+  const long long id = (long long)i * g.S2 + (long long)j * g.S + k;
+  if ((__ldg(label + id) & kMjMask) != m) return;
+  const float c0 = coef[0], c1 = coef[1], c2 = coef[2];
+  const float x = X[id], w = __ldg(W + id), pv = Pv[id];
+  X[id] = F_ADD(F_ADD(F_MUL(c0, x), F_MUL(c1, w)), F_MUL(c2, pv));
+  Pv[id] = F_ADD(F_MUL(c1, w), F_MUL(c2, pv));
+}
+
+// accumNorms (molecule.js:911-930) as its own pass: norm[label] += u32(u*u*h3*2^24) over the
+// interior; a warp's lanes with equal labels add their integers first (exact, modulo 2^32 like
+// the shader's atomics), one atomic per label and warp.
+__global__ void __launch_bounds__(256) k_mj_accum_norms(const float* __restrict__ U, const int* __restrict__ label,
+                                                        Geo g, float h3, unsigned* __restrict__ unorm) {
+  const int k = 1 + blockIdx.x * 32 + threadIdx.x, j = 1 + blockIdx.y * 8 + threadIdx.y, i = 1 + blockIdx.z;
+  int L = -1;
+  unsigned v = 0u;
+  if (k < g.NN && j < g.NN) {
+    const long long id = (long long)i * g.S2 + (long long)j * g.S + k;
+    const float u = __ldg(U + id);
+    v = __float2uint_rz(F_MUL(F_MUL(F_MUL(u, u), h3), 16777216.0f));
+    L = __ldg(label + id) & kMjMask;
+  }
+  const unsigned peers = __match_any_sync(0xffffffffu, L);
+  const unsigned sum = __reduce_add_sync(peers, v);
+  if (L >= 0 && (int)threadIdx.x == __ffs(peers) - 1) atomicAdd(&unorm[L], sum);
+}
+
+static dim3 lob_cells_grid(const Geo& g) {
+  const unsigned n = (unsigned)(g.NN - 1);
+  return dim3((n + 31) / 32, (n + 7) / 8, n);
+}
+
+int lob_workgroups(const Geo& g) {
+  const long long n = g.NN - 1, tot = n * n * n;
+  return (int)std::min<long long>(kLobMaxWG, (tot + kLobWG - 1) / kLobWG);
+}
+
+cudaError_t launch_lob_apply_h(const float* U, float* HU, const float* K, const int* label, const float* Pother,
+                               const MjAtom* atoms, const Geo& g, float h, float inv_h2, bool bare, cudaStream_t st) {
+  if (bare)
+    k_lob_apply_h<true><<<march_grid(g), march_block(), 0, st>>>(U, HU, K, label, Pother, atoms, g, h, inv_h2);
+  else
+    k_lob_apply_h<false><<<march_grid(g), march_block(), 0, st>>>(U, HU, K, label, Pother, atoms, g, h, inv_h2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lob_inner(const float* X, const float* HX, const float* W, const float* HW, const float* Pv,
+                             const float* HP, const int* label, int m, const Geo& g, float h3, float* partials,
+                             cudaStream_t st) {
+  k_lob_inner<<<lob_workgroups(g), kLobWG, 0, st>>>(X, HX, W, HW, Pv, HP, label, m, g, h3, partials);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lob_finalize(const float* partials, int nwg, bool first, bool hasP, float* scal, cudaStream_t st) {
+  if (first)
+    k_lob_finalize<true><<<1, kLobWG, 0, st>>>(partials, nwg, hasP ? 1 : 0, scal);
+  else
+    k_lob_finalize<false><<<1, kLobWG, 0, st>>>(partials, nwg, hasP ? 1 : 0, scal);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lob_residual(const float* X, const float* HX, float* W, const int* label, const float* K,
+                                const float* Pot, const float* lam, int m, const Geo& g, float inv_h2, cudaStream_t st) {
+  k_lob_residual<<<lob_cells_grid(g), dim3(32, 8), 0, st>>>(X, HX, W, label, K, Pot, lam, m, g, inv_h2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lob_update(float* X, const float* W, float* Pv, const int* label, const float* coef, int m,
+                              const Geo& g, cudaStream_t st) {
+  k_lob_update<<<lob_cells_grid(g), dim3(32, 8), 0, st>>>(X, W, Pv, label, coef, m, g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mj_accum_norms(const float* U, const int* label, const Geo& g, float h3, unsigned* unorm,
+                                  cudaStream_t st) {
+  k_mj_accum_norms<<<lob_cells_grid(g), dim3(32, 8), 0, st>>>(U, label, g, h3, unorm);
   return cudaGetLastError();
 }
 

@@ -55,6 +55,11 @@ struct rq_ctx {
   float* scratch_atoms5 = nullptr;  // per-call atom table for force variants
   float *sic = nullptr, *sic2 = nullptr;  // molecule.js flavour with SIC: self-potential ping-pong
   float* pdirect = nullptr;   // molecule.js direct path: persistent P_m of every domain (n_atoms x S^3)
+  // molecule.js LOBPCG frames: HX, W, HW, P, HP (5 x S^3), the inner-product partial sums of
+  // each workgroup (256 x 12) and the scalars (lambda, Ritz coefficients, the 12 sums of each pass)
+  float* lob = nullptr;
+  float* lob_part = nullptr;
+  float* lob_scal = nullptr;
   // solver.py flavour: atom bins of the label step's argmax (rebuilt whenever atoms change)
   int bins_nb = 0, bins_bin = 0;
   int *bin_start = nullptr, *bin_idx = nullptr, *bin_far = nullptr;

@@ -92,6 +92,22 @@ cudaError_t launch_mj_energy(const float* U, const float* Pv, const float* K, co
 cudaError_t launch_mj_gradp(const float* P, const MjAtom* atoms, int nAt, const Geo& g, float inv_h, int R, double* F,
                             cudaStream_t st);
 cudaError_t launch_fill(float* f, float v, long long n, cudaStream_t st);
+// LOBPCG frames (molecule.js:1455-1724): inner products in workgroups of kLobWG threads, at most
+// kLobMaxWG of them (molecule.js:1533-1534); kLobScal floats of per-iteration scalars
+constexpr int kLobNR = 12, kLobWG = 128, kLobMaxWG = 256, kLobScal = 32;
+int lob_workgroups(const Geo& g);
+cudaError_t launch_lob_apply_h(const float* U, float* HU, const float* K, const int* label, const float* Pother,
+                               const MjAtom* atoms, const Geo& g, float h, float inv_h2, bool bare, cudaStream_t st);
+cudaError_t launch_lob_inner(const float* X, const float* HX, const float* W, const float* HW, const float* Pv,
+                             const float* HP, const int* label, int m, const Geo& g, float h3, float* partials,
+                             cudaStream_t st);
+cudaError_t launch_lob_finalize(const float* partials, int nwg, bool first, bool hasP, float* scal, cudaStream_t st);
+cudaError_t launch_lob_residual(const float* X, const float* HX, float* W, const int* label, const float* K,
+                                const float* Pot, const float* lam, int m, const Geo& g, float inv_h2, cudaStream_t st);
+cudaError_t launch_lob_update(float* X, const float* W, float* Pv, const int* label, const float* coef, int m,
+                              const Geo& g, cudaStream_t st);
+cudaError_t launch_mj_accum_norms(const float* U, const int* label, const Geo& g, float h3, unsigned* unorm,
+                                  cudaStream_t st);
 
 // ---- new flavour (nm_kernels.cu), T = float (mixed) or double (FP64) --------------------
 template <typename T>

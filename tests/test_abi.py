@@ -58,6 +58,13 @@ def test_create_rejects_bad_config_without_touching_a_device():
     cfg.flavor = 1
     assert lib.rq_create(ctypes.byref(cfg), atoms, 1, ctypes.byref(h)) == _lib.RQ_ENOTSUP
     assert lib.rq_create(ctypes.byref(cfg), atoms, 0, ctypes.byref(h)) == _lib.RQ_EINVAL
+    cfg.precision = 0
+    cfg.flavor = 1  # solver.py
+    cfg.lobpcg = 1  # LOBPCG frames are molecule.js's
+    assert lib.rq_create(ctypes.byref(cfg), atoms, 1, ctypes.byref(h)) == _lib.RQ_ENOTSUP
+    cfg.flavor = 0  # molecule.js
+    cfg.chebyshev = 1  # the page runs one of the two alternatives at a time
+    assert lib.rq_create(ctypes.byref(cfg), atoms, 1, ctypes.byref(h)) == _lib.RQ_EINVAL
 
 
 def test_kernel_entry_points_validate_arguments():

@@ -224,3 +224,30 @@ def test_chebyshev_is_refused_with_bare_nuclei():
     with pytest.raises(L.RqError) as e:
         Context(NN, screen, rows, flavor="molecule.js", chebyshev=1)
     assert e.value.status == L.RQ_ENOTSUP
+
+
+@pytest.mark.parametrize("kind,sic", [("water", False), ("bare", False), ("water", True), ("ten", True),
+                                      ("many", False)],
+                         ids=["water", "bare_nuclei", "water_direct_poisson", "ten_sic", "many"])
+def test_lobpcg_frames_bit_exact(kind, sic):
+    """LOBPCG frames (doLOBPCGStep, molecule.js:3323-3740): the Poisson solve and Pother, 10
+    iterations per domain with the inner products in the shaders' workgroup trees and the Ritz
+    problems in the page's FP64 arithmetic (one device thread here), normalisation, one ITP
+    update, the level-set passes.  Three frames: the first without a search direction (eager),
+    the second captured into a CUDA graph, the third replayed from it."""
+    from realmolecule_b200 import Context
+    NN, screen, rows = atoms_case(kind)
+    ref = orc.MoleculeJsDriver(NN, screen, rows, steps_per_frame=5, sic=sic, lobpcg=True)
+    ref.initialize()
+    ctx = Context(NN, screen, rows, flavor="molecule.js", steps_per_frame=5, sic=int(sic), lobpcg=1)
+    ctx.initialize()
+    ctx.upload(psi=ref.U, label=ref.label.astype(np.int32))
+    for _ in range(3):
+        ref.step()
+    ctx.step(3)
+    st = ctx.download(psi=True, label=True, W=True, P=True)
+    assert np.array_equal(st["psi"].view(np.uint32), ref.U.view(np.uint32))
+    assert np.array_equal(st["label"] & 0x3FFFFFFF, ref.label.astype(np.int32))
+    assert np.array_equal(st["W"].view(np.uint32), ref.W.view(np.uint32))
+    assert np.array_equal(st["P"].view(np.uint32), ref.P.view(np.uint32))
+    assert ref.frame == 3
