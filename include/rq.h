@@ -181,6 +181,12 @@ RQ_API const char* rq_status_string(int status);
 RQ_API int rq_initialize(rq_ctx* ctx);
 /* Move nuclei and rebuild K (cloud/solver.py:538-548, molecule.js:4563-4582 without relabel). */
 RQ_API int rq_set_atoms(rq_ctx* ctx, const rq_atom* atoms, int32_t n_atoms);
+/* molecule.js locked groups (window.USER_LOCKED_GROUPS, molecule.js:490-503, compiled into the
+ * page's evolveBoundary shader): group g holds the labels members[offsets[g] .. offsets[g+1]-1]; a
+ * boundary cell whose label and best neighbouring label are in one group keeps its label and its
+ * level-set value becomes max(W, 0.5).  n_groups = 0 removes the groups.  At most 64 groups
+ * (RQ_ENOTSUP above), members in [0, n_atoms) (RQ_EINVAL); molecule.js flavour only. */
+RQ_API int rq_set_locked_groups(rq_ctx* ctx, int32_t n_groups, const int32_t* offsets, const int32_t* members);
 /* External potential v (host array of S^3 doubles, Ha) added to the nuclear potential K of the
  * new flavour: the update uses K + v and E_eK = -h^3 sum (K + v) rho.  NULL removes it.  No
  * reference counterpart: the handle through which dE/dv = -h^3 rho is exposed to autograd. */

@@ -89,7 +89,7 @@ class _Oracle:
             "orc_sp_energy_f64": [_f32p, _f32p, _f32p, _i32p, _i, _d, _d, _f64p, _i, C.c_void_p],
             "orc_sp_forces": [_f32p, _f32p, _i, _i, _f, _f, _f, _f64p],
             "orc_mj_update": [_f32p, _f32p, _f32p, _u32p, _f32p, C.c_void_p, _i, _i, _i, _f, _f, _f],
-            "orc_mj_evolve_boundary": [_u32p, _u32p, _f32p, _f32p, _i, _f, _f],
+            "orc_mj_evolve_boundary": [_u32p, _u32p, _f32p, _f32p, _i, _f, _f, C.c_void_p],
             "orc_mj_jacobi": [_f32p, _f32p, _f32p, _i, _f, _f],
             "orc_mj_rho": [_f32p, _f32p, _i],
             "orc_mj_rho_self": [_f32p, _u32p, C.c_uint32, _f32p, _i],
@@ -372,7 +372,8 @@ class MoleculeJsDriver:
     """
 
     def __init__(self, NN, screen, atoms, dv=None, steps_per_frame=None, norm_interval=20, vcycle_interval=50,
-                 jacobi_per_step=2, boundary_speed=0.5, curv_reg=0.15, sic=False, chebyshev=False, lobpcg=False):
+                 jacobi_per_step=2, boundary_speed=0.5, curv_reg=0.15, sic=False, chebyshev=False, lobpcg=False,
+                 locked_groups=None):
         self.NN = NN
         self.S = NN + 1
         self.S3 = self.S ** 3
@@ -414,6 +415,11 @@ class MoleculeJsDriver:
         self.frame = 0  # molecule.js frameCount
         self.chebyshev = bool(chebyshev)
         self.cheb_state, self.cheb_E = 1.0, 0.0  # chebOmega (:1762) and the page's E (:1767)
+        # USER_LOCKED_GROUPS (molecule.js:490-503) as the bit set of each label's groups
+        self.lock = np.zeros(self.nA, np.uint64)
+        for g, members in enumerate(locked_groups or []):
+            for mbr in members:
+                self.lock[int(mbr)] |= np.uint64(1) << np.uint64(g)
         # useLOBPCG (molecule.js:1751): one step() is one doLOBPCGStep frame
         self.lobpcg = bool(lobpcg)
         self.sic = bool(sic)
@@ -552,7 +558,8 @@ class MoleculeJsDriver:
         self.U, self.Unext = self.Unext, self.U
         self.frame += 1
         for _ in range(max(1, self.spf)):
-            O().mj_evolve_boundary(self.label, self.label2, self.U, self.W, S, self.dt_w, self.curv)
+            O().mj_evolve_boundary(self.label, self.label2, self.U, self.W, S, self.dt_w, self.curv,
+                                   self.lock.ctypes.data)
             self.label, self.label2 = self.label2, self.label
 
     def step(self):
@@ -599,7 +606,8 @@ class MoleculeJsDriver:
                 self.sic_pass()
             self.frame += 1
             for _ in range(max(1, self.spf)):
-                O().mj_evolve_boundary(self.label, self.label2, self.U, self.W, self.S, self.dt_w, self.curv)
+                O().mj_evolve_boundary(self.label, self.label2, self.U, self.W, self.S, self.dt_w, self.curv,
+                                      self.lock.ctypes.data)
                 self.label, self.label2 = self.label2, self.label
             if self.chebyshev:
                 self.cheb_E = self.total_energy()

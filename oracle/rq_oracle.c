@@ -454,8 +454,11 @@ void orc_mj_update_cheb(const float* U, float* Uo, const float* K, const uint32_
       }
 }
 
+/* evolveBoundary (molecule.js:426-540) without shell splits.  Locked groups (:490-503): lock[l]
+ * has bit g set when label l is in group g (lock may be NULL); a boundary cell whose label and
+ * best other label share a group keeps its label with W = max(W, 0.5). */
 void orc_mj_evolve_boundary(const uint32_t* labelIn, uint32_t* labelOut, const float* U, float* W, int S,
-                            float dt_w, float curvReg) {
+                            float dt_w, float curvReg, const uint64_t* lock) {
   const int NN = S - 1;
   const int64_t S2 = (int64_t)S * S;
 #pragma omp parallel for schedule(static)
@@ -478,6 +481,7 @@ void orc_mj_evolve_boundary(const uint32_t* labelIn, uint32_t* labelOut, const f
         }
         float w = W[id];
         if (myCnt >= 6.0f) { w = fmaxf(w, 1.0f); W[id] = w; labelOut[id] = myL; continue; }
+        if (lock && (lock[myL] & lock[bestL])) { W[id] = fmaxf(w, 0.5f); labelOut[id] = myL; continue; }
         float denom = myRho + bestRho;
         float vel = (denom < 1e-20f) ? 0.0f : (myRho - bestRho) / denom;
         w += dt_w * vel;

@@ -126,6 +126,16 @@ class Context:
         self._chk(self.lib.rq_set_atoms(self.ctx, arr, len(arr)), "rq_set_atoms")
         self._atoms = arr
 
+    def set_locked_groups(self, groups):
+        """molecule.js flavour: window.USER_LOCKED_GROUPS (molecule.js:490-503), a list of label
+        lists; a boundary between two labels of one group does not move.  [] removes them."""
+        groups = [list(map(int, g)) for g in (groups or [])]
+        offsets = np.zeros(len(groups) + 1, np.int32)
+        offsets[1:] = np.cumsum([len(g) for g in groups], dtype=np.int64)
+        members = np.asarray([m for g in groups for m in g] or [0], np.int32)
+        self._chk(self.lib.rq_set_locked_groups(self.ctx, len(groups), _ptr(offsets), _ptr(members)),
+                  "rq_set_locked_groups")
+
     def set_external_potential(self, v):
         """Add an external potential v (S^3 values, Ha) to K (new flavour); None removes it."""
         arr = None if v is None else np.ascontiguousarray(np.asarray(v, np.float64).reshape(-1))

@@ -135,7 +135,7 @@ static void free_ctx(rq_ctx* c) {
   for (auto& gx : c->graph)
     if (gx) cudaGraphExecDestroy(gx);
   void* ptrs[] = {c->U[0], c->U[1], c->P[0], c->P[1], c->K, c->W, c->bestU, c->rho, c->Pother, c->resid, c->lab[0], c->lab[1],
-                  c->Ec[0], c->Ec[1], c->fc, c->atoms5, c->scratch_atoms5, c->sic, c->sic2, c->pdirect, c->lob, c->lob_part, c->lob_scal, c->bin_start, c->bin_idx, c->bin_far, c->bin_zmax, c->atoms_mj, c->atoms_nm, c->Zdom, c->Zdom64, c->dnorm,
+                  c->Ec[0], c->Ec[1], c->fc, c->atoms5, c->scratch_atoms5, c->sic, c->sic2, c->pdirect, c->lob, c->lob_part, c->lob_scal, c->lock, c->bin_start, c->bin_idx, c->bin_far, c->bin_zmax, c->atoms_mj, c->atoms_nm, c->Zdom, c->Zdom64, c->dnorm,
                   c->dpd, c->dF, c->dsum, c->unorm, c->scale, c->err, c->seeds, c->scale64, c->Kext};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -180,6 +180,7 @@ static int alloc_all(rq_ctx* c) {
       DALLOC(c->sic2, S3 * sizeof(float));
       if (mj_direct(c)) DALLOC(c->pdirect, S3 * sizeof(float) * n);
     }
+    DALLOC(c->lock, sizeof(unsigned long long) * n);
     if (c->cfg.lobpcg) {
       DALLOC(c->lob, S3 * sizeof(float) * 5);
       DALLOC(c->lob_part, sizeof(float) * kLobMaxWG * kLobNR);
@@ -513,6 +514,24 @@ extern "C" int rq_step(rq_ctx* c, int32_t n) {
     }
     left -= period;
   }
+  return RQ_OK;
+}
+
+extern "C" int rq_set_locked_groups(rq_ctx* c, int32_t n_groups, const int32_t* offsets, const int32_t* members) {
+  if (!c || n_groups < 0 || (n_groups > 0 && (!offsets || !members))) return RQ_EINVAL;
+  if (c->cfg.flavor != RQ_FLAVOR_MOLECULE_JS) return rq_fail(c, RQ_ENOTSUP, "locked groups are molecule.js's");
+  if (n_groups > 64) return rq_fail(c, RQ_ENOTSUP, "at most 64 locked groups");
+  std::vector<unsigned long long> mask((size_t)c->n_atoms, 0ull);
+  for (int g = 0; g < n_groups; ++g) {
+    if (offsets[g] < 0 || offsets[g + 1] < offsets[g]) return rq_fail(c, RQ_EINVAL, "locked group offsets");
+    for (int q = offsets[g]; q < offsets[g + 1]; ++q) {
+      if (members[q] < 0 || members[q] >= c->n_atoms)
+        return rq_fail(c, RQ_EINVAL, "locked group member " + std::to_string(members[q]) + " outside [0, n_atoms)");
+      mask[members[q]] |= 1ull << g;
+    }
+  }
+  CK(cudaMemcpyAsync(c->lock, mask.data(), mask.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
   return RQ_OK;
 }
 

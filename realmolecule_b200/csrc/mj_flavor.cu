@@ -249,7 +249,7 @@ static int mj_lobpcg_frame(rq_ctx* c) {
   for (int q = 0; q < wsteps; ++q) {
     LAUNCH(RQ_KC_LABELS, 20 * ip,
            launch_mj_evolve(c->lab[c->cl], c->lab[1 - c->cl], (float*)c->U[c->cu], c->W, at, c->n_atoms, c->g, p.dt_w,
-                            p.curvReg, p.h, p.hasBare, c->st));
+                            p.curvReg, p.h, p.hasBare, c->lock, c->st));
     c->cl ^= 1;
   }
   return RQ_OK;
@@ -326,7 +326,7 @@ int mj_step_one(rq_ctx* c, int s) {
     for (int q = 0; q < wsteps; ++q) {
       LAUNCH(RQ_KC_LABELS, 20 * ip,
              launch_mj_evolve(c->lab[c->cl], c->lab[1 - c->cl], (float*)c->U[c->cu], c->W, atoms_dev(c), c->n_atoms,
-                              c->g, p.dt_w, p.curvReg, p.h, p.hasBare, c->st));
+                              c->g, p.dt_w, p.curvReg, p.h, p.hasBare, c->lock, c->st));
       c->cl ^= 1;
     }
     if (c->cfg.chebyshev) {  // the page's E at the frame's end feeds the next frame's omega (:3186)

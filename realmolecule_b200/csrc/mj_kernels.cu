@@ -429,13 +429,16 @@ __global__ void k_mj_prolong(const float* __restrict__ Ec, float* __restrict__ P
 }
 
 // ---------------------------------------------------------------------------------------
-// evolveBoundary (molecule.js:426-540 without locked groups / shell splits): snapshot
-// labels in, labels + W out; the new label word carries its recomputed exclusion bit.
+// evolveBoundary (molecule.js:426-540 without shell splits): snapshot labels in, labels + W
+// out; the new label word carries its recomputed exclusion bit.  Locked groups (USER_LOCKED_GROUPS,
+// :490-503, compiled into the page's shader): lock[l] has bit g set when label l is in group g; a
+// boundary cell whose label and best other label share a group keeps its label, W = max(W, 0.5).
 // ---------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_mj_evolve(const int* __restrict__ labIn, int* __restrict__ labOut,
                                                    const float* __restrict__ U, float* __restrict__ W,
                                                    const MjAtom* __restrict__ atoms, int nAt, Geo g, float dt_w,
-                                                   float curvReg, float h, bool hasBare) {
+                                                   float curvReg, float h, bool hasBare,
+                                                   const unsigned long long* __restrict__ lock) {
   const int k = 1 + blockIdx.x * kThreadsK + threadIdx.x;
   const int j = 1 + blockIdx.y * kThreadsJ + threadIdx.y;
   const int i0 = 1 + blockIdx.z * kMarch;
@@ -465,6 +468,11 @@ __global__ void __launch_bounds__(256) k_mj_evolve(const int* __restrict__ labIn
     float w = W[id];
     if (myCnt >= 6.0f) {
       W[id] = fmaxf(w, 1.0f);
+      labOut[id] = stored;
+      continue;
+    }
+    if ((__ldg(lock + myL) & __ldg(lock + bestL)) != 0ull) {
+      W[id] = fmaxf(w, 0.5f);
       labOut[id] = stored;
       continue;
     }
@@ -716,9 +724,11 @@ cudaError_t launch_mj_sic_domain(const float* U, const int* label, float* Pother
   return cudaGetLastError();
 }
 cudaError_t launch_mj_evolve(const int* labIn, int* labOut, const float* U, float* W, const MjAtom* atoms, int nAt,
-                             const Geo& g, float dt_w, float curvReg, float h, bool hasBare, cudaStream_t st) {
+                             const Geo& g, float dt_w, float curvReg, float h, bool hasBare,
+                             const unsigned long long* lock, cudaStream_t st) {
   if (g.NN < 2) return cudaSuccess;
-  k_mj_evolve<<<march_grid(g), march_block(), 0, st>>>(labIn, labOut, U, W, atoms, nAt, g, dt_w, curvReg, h, hasBare);
+  k_mj_evolve<<<march_grid(g), march_block(), 0, st>>>(labIn, labOut, U, W, atoms, nAt, g, dt_w, curvReg, h, hasBare,
+                                                       lock);
   return cudaGetLastError();
 }
 cudaError_t launch_mj_energy(const float* U, const float* Pv, const float* K, const int* label, const MjAtom* atoms,

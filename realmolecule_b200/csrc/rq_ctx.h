@@ -58,6 +58,8 @@ struct rq_ctx {
   // molecule.js LOBPCG frames: HX, W, HW, P, HP (5 x S^3), the inner-product partial sums of
   // each workgroup (256 x 12) and the scalars (lambda, Ritz coefficients, the 12 sums of each pass)
   float* lob = nullptr;
+  // molecule.js locked groups: per label the bit set of its groups (n_atoms, zero = none)
+  unsigned long long* lock = nullptr;
   float* lob_part = nullptr;
   float* lob_scal = nullptr;
   // solver.py flavour: atom bins of the label step's argmax (rebuilt whenever atoms change)

@@ -84,8 +84,10 @@ cudaError_t launch_mj_direct_domain(const float* U, const int* label, float* Pot
 cudaError_t launch_mj_sic_domain(const float* U, const int* label, float* Pother, int m, float frac, float* rho,
                                  float* sic, float* sic2, float* resid, float* Ec0, float* Ec1, float* fc, const Geo& g,
                                  const Geo& gc, float h2, float inv_h2, float two_pi, cudaStream_t st);
+// lock: per label the bit set of its locked groups (all 0 without groups)
 cudaError_t launch_mj_evolve(const int* labIn, int* labOut, const float* U, float* W, const MjAtom* atoms, int nAt,
-                             const Geo& g, float dt_w, float curvReg, float h, bool hasBare, cudaStream_t st);
+                             const Geo& g, float dt_w, float curvReg, float h, bool hasBare,
+                             const unsigned long long* lock, cudaStream_t st);
 cudaError_t launch_mj_energy(const float* U, const float* Pv, const float* K, const int* label, const MjAtom* atoms,
                              const Geo& g, float h, float h3, float Rsing, int nDom, double* pd, double* dip,
                              cudaStream_t st);

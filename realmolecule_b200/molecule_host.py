@@ -32,6 +32,9 @@ def nuc_mass(z: float) -> float:
     return _MASS.get(z, 1) * 1836
 
 
+LOBPCG_ITERS = 10  # molecule.js:1752, iterations per domain in one LOBPCG frame
+
+
 class MoleculePage:
     def __init__(self, atoms: Sequence[dict], NN: int = 100, screen: float = 10.0, steps_per_frame: Optional[int] = None,
                  total_steps: int = 20000, n_move: int = 10, dynamics: bool = False, dt_nuc: Optional[float] = None,
@@ -41,7 +44,7 @@ class MoleculePage:
                  external_force=None, hinge_atoms=(), frozen_atoms=(), bond_constraints=(), water_triplets=(),
                  hoh_eq: float = 104.5, bend_k: float = 1.5, coincident_groups=(), rigid_groups=None,
                  shear_rate: float = 0.0, brownian: bool = False, brownian_gamma: float = 1.0,
-                 thermal_kick: Optional[float] = None, seed: int = 0, context=None, **ctx_opts):
+                 thermal_kick: Optional[float] = None, seed: int = 0, locked_groups=(), context=None, **ctx_opts):
         self.rows = [dict(a) for a in atoms]
         n = self.n = len(self.rows)
         self.NN, self.screen = int(NN), float(screen)
@@ -76,6 +79,12 @@ class MoleculePage:
         self.ctx = context if context is not None else Context(self.NN, self.screen, self._ctx_rows(),
                                                                flavor="molecule.js", steps_per_frame=self.spf,
                                                                **ctx_opts)
+        # useLOBPCG (molecule.js:1751): a frame is one doLOBPCGStep, counted as LOBPCG_ITERS steps
+        self.lobpcg = bool(ctx_opts.get("lobpcg"))
+        # USER_LOCKED_GROUPS (molecule.js:490-503)
+        self.locked_groups = [list(g) for g in locked_groups]
+        if self.locked_groups:
+            self.ctx.set_locked_groups(self.locked_groups)
         self._reset_counters()
         self.nuc_vel = [[0.0, 0.0, 0.0] for _ in range(n)]
         self.nuc_force = [[0.0, 0.0, 0.0] for _ in range(n)]
@@ -128,18 +137,20 @@ class MoleculePage:
         if self.phase != 0:
             return self.energies()
         t0 = self.tStep
-        self.ctx.step(self.spf)
-        self.tStep += self.spf
+        # doLOBPCGStep computes no forces and moves no nuclei (molecule.js:3323-3740, :4614-4616)
+        nsteps = LOBPCG_ITERS if self.lobpcg else self.spf
+        self.ctx.step(1 if self.lobpcg else self.spf)
+        self.tStep += nsteps
         e = self.ctx.energy()
         self.E, self.E_T, self.E_eK, self.E_ee, self.E_KK = (float(e[L.E_TOTAL]), float(e[L.E_T]), float(e[L.E_EK]),
                                                              float(e[L.E_EE]), float(e[L.E_KK]))
         # forces are read on the frame's final state: the reference's last force step of the frame is
         # its final step whenever frames end on multiples of N_MOVE (every default frame length)
-        if any((t0 + s + 1) % self.n_move == 0 for s in range(self.spf)):
+        if not self.lobpcg and any((t0 + s + 1) % self.n_move == 0 for s in range(self.spf)):
             self._forces()
             if self.dynamics:
                 self.move_nuclei()
-        self.phase_steps += self.spf
+        self.phase_steps += nsteps
         self.frame_count += 1
         if math.isfinite(self.E) and self.E < self.E_min:
             self.E_min = self.E

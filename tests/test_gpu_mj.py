@@ -251,3 +251,37 @@ def test_lobpcg_frames_bit_exact(kind, sic):
     assert np.array_equal(st["W"].view(np.uint32), ref.W.view(np.uint32))
     assert np.array_equal(st["P"].view(np.uint32), ref.P.view(np.uint32))
     assert ref.frame == 3
+
+
+@pytest.mark.parametrize("kind,groups", [("water", [[0, 1]]), ("many", [[0, 3, 5], [1, 2], [7, 9, 11, 13]])],
+                         ids=["water", "many"])
+def test_locked_groups_frames_bit_exact(kind, groups):
+    """USER_LOCKED_GROUPS (molecule.js:490-503): boundaries between labels of one group stay put
+    (W = max(W, 0.5)); frames bit-exact against the restatement, and different from the frames
+    without the groups."""
+    from realmolecule_b200 import Context, _lib as L
+    opts = dict(steps_per_frame=7, norm_interval=5, vcycle_interval=3)
+    NN, screen, rows = atoms_case(kind)
+    ref = orc.MoleculeJsDriver(NN, screen, rows, locked_groups=groups, **opts)
+    ref.initialize()
+    free = orc.MoleculeJsDriver(NN, screen, rows, **opts)
+    free.initialize()
+    ctx = Context(NN, screen, rows, flavor="molecule.js", **opts)
+    ctx.initialize()
+    ctx.set_locked_groups(groups)
+    ctx.upload(psi=ref.U, label=ref.label.astype(np.int32))
+    for _ in range(3 * 7 + 2):
+        ref.step()
+        free.step()
+    ctx.step(3 * 7 + 2)
+    st = ctx.download(psi=True, label=True, W=True)
+    assert np.array_equal(st["label"], ref.label.astype(np.int32))
+    assert np.array_equal(st["W"].view(np.uint32), ref.W.view(np.uint32))
+    assert np.array_equal(st["psi"].view(np.uint32), ref.U.view(np.uint32))
+    assert not np.array_equal(ref.W, free.W)
+    with pytest.raises(L.RqError):
+        ctx.set_locked_groups([[0, len(rows)]])
+    with pytest.raises(L.RqError) as e:
+        ctx.set_locked_groups([[0]] * 65)
+    assert e.value.status == L.RQ_ENOTSUP
+    ctx.set_locked_groups([])

@@ -40,6 +40,9 @@ class FakeContext:
     def extract(self, k=None):
         return np.zeros(1, np.float32)
 
+    def set_locked_groups(self, groups):
+        self.locked = groups
+
 
 WATER = [{"i": 50, "j": 50, "k": 50, "Z": 2, "el": "O"}, {"i": 60, "j": 57, "k": 50, "Z": 1, "el": "H"},
          {"i": 40, "j": 57, "k": 50, "Z": 1, "el": "H"}]
@@ -140,3 +143,19 @@ def test_restart_and_activate():
     p.activateAtoms(2)
     assert ctx.inits == 2 and ctx.atoms[-1][2][3] == 0.0 and p.Z[:2] == [2.0, 1.0]
     assert p.pos[0] == [52.0, 50.0, 50.0]
+
+
+def test_lobpcg_frames_count_ten_steps_and_skip_forces():
+    """In LOBPCG mode a frame is one doLOBPCGStep (one rq_step) counted as LOBPCG_ITERS = 10 steps;
+    the page computes no forces and moves no nuclei in it (molecule.js:3323-3740, :4614-4616)."""
+    p, ctx = page(dynamics=True, n_move=10, lobpcg=1)
+    for _ in range(3):
+        p.frame()
+    assert ctx.steps == [1, 1, 1]
+    assert p.tStep == 30 and p.phase_steps == 30
+    assert ctx.atoms == []  # no moveNuclei
+
+
+def test_locked_groups_reach_the_context():
+    p, ctx = page(locked_groups=[[0, 1], [2]])
+    assert ctx.locked == [[0, 1], [2]]
