@@ -187,6 +187,19 @@ RQ_API int rq_set_atoms(rq_ctx* ctx, const rq_atom* atoms, int32_t n_atoms);
  * level-set value becomes max(W, 0.5).  n_groups = 0 removes the groups.  At most 64 groups
  * (RQ_ENOTSUP above), members in [0, n_atoms) (RQ_EINVAL); molecule.js flavour only. */
 RQ_API int rq_set_locked_groups(rq_ctx* ctx, int32_t n_groups, const int32_t* offsets, const int32_t* members);
+/* molecule.js shell splits (window.USER_SPLIT_TYPE / _IDX / _AXIS / _ROT, molecule.js:27-32, the atom
+ * record's split fields :183-191, inSplitAtom :197-226), one record per atom entry: the entry owns
+ * only the cells of its angular sector around its nucleus -- type 2 a half space (idx 0: d.axis < 0,
+ * else >= 0), type 3 one of three 120-degree sectors about the axis (sector idx, offset rot in
+ * radians); 0, 1 (and 4, which the page leaves unrestricted) the whole sphere.  Used by the trial
+ * labelling of rq_initialize and rq_set_atoms (gpuInitAccum, :1377-1426) and by the level-set step
+ * (:514-533), so set them before rq_initialize.  NULL removes them.  molecule.js flavour only. */
+typedef struct rq_split {
+  int32_t type, idx;
+  double axis[3];
+  double rot;
+} rq_split;
+RQ_API int rq_set_splits(rq_ctx* ctx, const rq_split* splits);
 /* External potential v (host array of S^3 doubles, Ha) added to the nuclear potential K of the
  * new flavour: the update uses K + v and E_eK = -h^3 sum (K + v) rho.  NULL removes it.  No
  * reference counterpart: the handle through which dE/dv = -h^3 rho is exposed to autograd. */

@@ -55,6 +55,15 @@ class MjAtom(C.Structure):
                 ("rc", C.c_float), ("Z_nuc", C.c_float), ("initZeff", C.c_float), ("initRcut", C.c_float)]
 
 
+class MjSplit(C.Structure):
+    """Shell split of one entry (molecule.js:183-191 split fields) as the oracle takes it."""
+    _fields_ = [("type", C.c_uint32), ("idx", C.c_uint32), ("ax", C.c_float), ("ay", C.c_float), ("az", C.c_float),
+                ("rot", C.c_float)]
+
+
+SPLIT_CODES = {"sphere": 0, "hemi": 2, "third": 3, "tetra": 4}  # fillAtomBuf's stCode (molecule.js:1894)
+
+
 def mj_atoms(rows):
     """rows: iterable of dicts with i,j,k,Z[,rc,Z_nuc,initZeff,initRcut] -> ctypes array.
 
@@ -89,7 +98,8 @@ class _Oracle:
             "orc_sp_energy_f64": [_f32p, _f32p, _f32p, _i32p, _i, _d, _d, _f64p, _i, C.c_void_p],
             "orc_sp_forces": [_f32p, _f32p, _i, _i, _f, _f, _f, _f64p],
             "orc_mj_update": [_f32p, _f32p, _f32p, _u32p, _f32p, C.c_void_p, _i, _i, _i, _f, _f, _f],
-            "orc_mj_evolve_boundary": [_u32p, _u32p, _f32p, _f32p, _i, _f, _f, C.c_void_p],
+            "orc_mj_evolve_boundary": [_u32p, _u32p, _f32p, _f32p, _i, _f, _f, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       _f],
             "orc_mj_jacobi": [_f32p, _f32p, _f32p, _i, _f, _f],
             "orc_mj_rho": [_f32p, _f32p, _i],
             "orc_mj_rho_self": [_f32p, _u32p, C.c_uint32, _f32p, _i],
@@ -107,8 +117,8 @@ class _Oracle:
             "orc_mj_energy": [_f32p, _f32p, _f32p, _u32p, C.c_void_p, _i, _f, _f, _f, _f64p],
             "orc_mj_force_gradP": [_f32p, C.c_void_p, _i, _i, _f, _i, _f64p],
             "orc_mj_force_hf": [_f32p, C.c_void_p, _i, _i, _f, _f, _f64p],
-            "orc_mj_init": [_f32p, _f32p, _u32p, C.c_void_p, _i, _i, _f, _f, _f],
-            "orc_mj_init_persist": [_f32p, _f32p, _u32p, C.c_void_p, _i, _i, _f, _f, _f],
+            "orc_mj_init": [_f32p, _f32p, _u32p, C.c_void_p, _i, _i, _f, _f, _f, C.c_void_p],
+            "orc_mj_init_persist": [_f32p, _f32p, _u32p, C.c_void_p, _i, _i, _f, _f, _f, C.c_void_p],
             "orc_nm_potential": [_f64p, _f64p, _f64p, _i, _i, _d, _d],
             "orc_nm_update": [_f64p, _f64p, _f64p, _f64p, _i32p, _i, _d, _d],
             "orc_nm_vcycle": [_f64p, _f64p, _i, _d, _i, _i, _i, _i],
@@ -373,7 +383,7 @@ class MoleculeJsDriver:
 
     def __init__(self, NN, screen, atoms, dv=None, steps_per_frame=None, norm_interval=20, vcycle_interval=50,
                  jacobi_per_step=2, boundary_speed=0.5, curv_reg=0.15, sic=False, chebyshev=False, lobpcg=False,
-                 locked_groups=None):
+                 locked_groups=None, splits=None):
         self.NN = NN
         self.S = NN + 1
         self.S3 = self.S ** 3
@@ -420,6 +430,8 @@ class MoleculeJsDriver:
         for g, members in enumerate(locked_groups or []):
             for mbr in members:
                 self.lock[int(mbr)] |= np.uint64(1) << np.uint64(g)
+        # shell splits per entry (USER_SPLIT_*, molecule.js:27-32): dicts of type, idx, axis, rot
+        self.set_splits(splits)
         # useLOBPCG (molecule.js:1751): one step() is one doLOBPCGStep frame
         self.lobpcg = bool(lobpcg)
         self.sic = bool(sic)
@@ -436,7 +448,8 @@ class MoleculeJsDriver:
         self.SC = SC
 
     def initialize(self):
-        O().mj_init(self.K, self.U, self.label, C.addressof(self.atoms), self.nA, self.S, self.h, self.h2, self.Rsing)
+        O().mj_init(self.K, self.U, self.label, C.addressof(self.atoms), self.nA, self.S, self.h, self.h2, self.Rsing,
+                    self._splits_ptr())
         self.bestU[:] = self.U
         self.Unext[:] = self.U
         self.label2[:] = self.label
@@ -449,13 +462,30 @@ class MoleculeJsDriver:
                 O().mj_init_pdirect(C.addressof(self.atoms), self.nA, m, self.Pdirect[m], self.Pother, self.S, self.h,
                                     self.h2)
 
+    def set_splits(self, splits):
+        self.splits = None
+        if splits:
+            self.splits = (MjSplit * self.nA)()
+            for n, sp in enumerate(splits):
+                if not sp:
+                    continue
+                t = sp.get("type", 0)  # fillAtomBuf: a name through stCode, else the number (:1894-1896)
+                self.splits[n].type = SPLIT_CODES.get(t, 0) if isinstance(t, str) else int(t or 0)
+                self.splits[n].idx = int(sp.get("idx", 0))
+                ax = sp.get("axis") or (0.0, 0.0, 1.0)
+                self.splits[n].ax, self.splits[n].ay, self.splits[n].az = (float(v) for v in ax)
+                self.splits[n].rot = float(sp.get("rot", 0.0))
+
+    def _splits_ptr(self):
+        return C.addressof(self.splits) if self.splits is not None else None
+
     def set_positions(self, rows):
         self.rows = [dict(a) for a in rows]
         for r in self.rows:
             r.setdefault("Z_nuc", r["Z"])
         self.atoms = mj_atoms(self.rows)
         O().mj_init_persist(self.K, self.bestU, self.label, C.addressof(self.atoms), self.nA, self.S, self.h, self.h2,
-                            self.Rsing)
+                            self.Rsing, self._splits_ptr())
         self.label2[:] = self.label
 
     def vcycle(self):
@@ -559,7 +589,7 @@ class MoleculeJsDriver:
         self.frame += 1
         for _ in range(max(1, self.spf)):
             O().mj_evolve_boundary(self.label, self.label2, self.U, self.W, S, self.dt_w, self.curv,
-                                   self.lock.ctypes.data)
+                                   self.lock.ctypes.data, C.addressof(self.atoms), self._splits_ptr(), self.h)
             self.label, self.label2 = self.label2, self.label
 
     def step(self):
@@ -607,7 +637,7 @@ class MoleculeJsDriver:
             self.frame += 1
             for _ in range(max(1, self.spf)):
                 O().mj_evolve_boundary(self.label, self.label2, self.U, self.W, self.S, self.dt_w, self.curv,
-                                      self.lock.ctypes.data)
+                                      self.lock.ctypes.data, C.addressof(self.atoms), self._splits_ptr(), self.h)
                 self.label, self.label2 = self.label2, self.label
             if self.chebyshev:
                 self.cheb_E = self.total_energy()

@@ -377,6 +377,47 @@ static inline float mj_dist(int ci, int cj, int ck, const orc_mj_atom* a, float 
   return sqrtf(dx * dx + dy * dy + dz * dz);
 }
 
+/* Shell split of an entry (window.USER_SPLIT_TYPE/_IDX/_AXIS/_ROT, molecule.js:27-32, the atom
+ * record's split fields :183-191): type 0/1 = whole sphere, 2 = half space, 3 = 120-degree sector. */
+typedef struct {
+  uint32_t type, idx;
+  float ax, ay, az, rot;
+} orc_mj_split;
+
+/* inSplitAtom (molecule.js:197-226); d = cell - nucleus in bohr, r = |d|.  atan2 is the f64
+ * function rounded once to f32 (WGSL leaves its accuracy to the implementation). */
+static int mj_in_split(float dx, float dy, float dz, float r, const orc_mj_split* s) {
+  if (s->type <= 1u || r < 1e-6f) return 1;
+  const float axL = fmaxf(sqrtf(s->ax * s->ax + s->ay * s->ay + s->az * s->az), 1e-12f);
+  const float a0 = s->ax / axL, a1 = s->ay / axL, a2 = s->az / axL;
+  const float dotp = dx * a0 + dy * a1 + dz * a2;
+  if (s->type == 2u) return s->idx == 0u ? dotp < 0.f : dotp >= 0.f;
+  if (s->type == 3u) {
+    const float px = dx - dotp * a0, py = dy - dotp * a1, pz = dz - dotp * a2;
+    float e1x, e1y, e1z;
+    if (fabsf(a2) < 0.9f) { e1x = a1; e1y = -a0; e1z = 0.f; } else { e1x = 0.f; e1y = a2; e1z = -a1; }
+    const float e1L = fmaxf(sqrtf(e1x * e1x + e1y * e1y + e1z * e1z), 1e-12f);
+    e1x = e1x / e1L; e1y = e1y / e1L; e1z = e1z / e1L;
+    const float e2x = a1 * e1z - a2 * e1y, e2y = a2 * e1x - a0 * e1z, e2z = a0 * e1y - a1 * e1x;
+    const float pe1 = px * e1x + py * e1y + pz * e1z, pe2 = px * e2x + py * e2y + pz * e2z;
+    float th = (float)atan2((double)pe2, (double)pe1) - s->rot;
+    if (th < -3.14159265f) th = th + 6.28318530f;
+    if (th > 3.14159265f) th = th - 6.28318530f;
+    const uint32_t sector = ((uint32_t)floorf((th + 3.14159265f) / 2.09439510f)) % 3u;
+    return sector == s->idx;
+  }
+  return 1;
+}
+
+/* evolveBoundary's cellSectorOK (molecule.js:437-442): d = (cell - nucleus) * h. */
+static int mj_sector_ok(int i, int j, int k, uint32_t n, const orc_mj_atom* atoms, const orc_mj_split* splits, float h) {
+  if (!splits || splits[n].type <= 1u) return 1;
+  const float dx = ((float)i - (float)atoms[n].posI) * h;
+  const float dy = ((float)j - (float)atoms[n].posJ) * h;
+  const float dz = ((float)k - (float)atoms[n].posK) * h;
+  return mj_in_split(dx, dy, dz, sqrtf(dx * dx + dy * dy + dz * dz), &splits[n]);
+}
+
 /* molecule.js:246-259 isInsideRc (own r_c sphere; bare nuclei when present). */
 static inline int mj_inside_rc(int ci, int cj, int ck, uint32_t lbl, const orc_mj_atom* atoms, int nElec,
                                int hasBare, float h) {
@@ -454,11 +495,14 @@ void orc_mj_update_cheb(const float* U, float* Uo, const float* K, const uint32_
       }
 }
 
-/* evolveBoundary (molecule.js:426-540) without shell splits.  Locked groups (:490-503): lock[l]
- * has bit g set when label l is in group g (lock may be NULL); a boundary cell whose label and
- * best other label share a group keeps its label with W = max(W, 0.5). */
+/* evolveBoundary (molecule.js:426-540).  Locked groups (:490-503): lock[l] has bit g set when
+ * label l is in group g (lock may be NULL); a boundary cell whose label and best other label share
+ * a group keeps its label with W = max(W, 0.5).  Shell splits (:514-533, splits may be NULL): a
+ * flip into a domain whose sector excludes the cell is cancelled, and a cell outside its own
+ * domain's sector goes to the best neighbour whose sector holds it. */
 void orc_mj_evolve_boundary(const uint32_t* labelIn, uint32_t* labelOut, const float* U, float* W, int S,
-                            float dt_w, float curvReg, const uint64_t* lock) {
+                            float dt_w, float curvReg, const uint64_t* lock, const orc_mj_atom* atoms,
+                            const orc_mj_split* splits, float h) {
   const int NN = S - 1;
   const int64_t S2 = (int64_t)S * S;
 #pragma omp parallel for schedule(static)
@@ -489,6 +533,14 @@ void orc_mj_evolve_boundary(const uint32_t* labelIn, uint32_t* labelOut, const f
         w += curvReg * curv;
         uint32_t newL = myL;
         if (w < 0.0f) { newL = bestL; w = 0.1f; }
+        const int myOK = mj_sector_ok(i, j, k, myL, atoms, splits, h);
+        if (!mj_sector_ok(i, j, k, newL, atoms, splits, h)) {
+          newL = myL;
+          w = fmaxf(w, 0.1f);
+          if (!myOK && bestL != myL && mj_sector_ok(i, j, k, bestL, atoms, splits, h)) { newL = bestL; w = 0.1f; }
+        } else if (!myOK && newL == myL) {
+          if (bestL != myL && mj_sector_ok(i, j, k, bestL, atoms, splits, h)) { newL = bestL; w = 0.1f; }
+        }
         W[id] = w;
         labelOut[id] = newL;
       }
@@ -814,7 +866,7 @@ void orc_mj_force_hf(const float* U, const orc_mj_atom* atoms, int nElec, int S,
  * K = sum Zn/r_eff, trial u = Ze^2/sqrt(pi) e^{-Ze r} (0 beyond initRcut or for bare nuclei),
  * label = argmax (strict >, first wins).  K/bestU/label start from 0/0/0 over ALL S^3 points. */
 void orc_mj_init(float* K, float* U, uint32_t* label, const orc_mj_atom* atoms, int nElec, int S, float h,
-                 float h2, float Rsing) {
+                 float h2, float Rsing, const orc_mj_split* splits) {
 #pragma omp parallel for schedule(static)
   for (int i = 0; i < S; ++i)
     for (int j = 0; j < S; ++j)
@@ -835,7 +887,9 @@ void orc_mj_init(float* K, float* U, uint32_t* label, const orc_mj_atom* atoms, 
           Kval += Zn / r;
           float Ze = atoms[n].initZeff;
           float rReal = sqrtf(r2);
-          float uT = (rReal > atoms[n].initRcut || Za <= 0.f) ? 0.f : Ze * Ze * 0.5641895835f * expf(-Ze * r);
+          const int okSplit = !splits || mj_in_split(dx, dy, dz, rReal, &splits[n]);
+          float uT = (rReal > atoms[n].initRcut || Za <= 0.f || !okSplit) ? 0.f
+                                                                            : Ze * Ze * 0.5641895835f * expf(-Ze * r);
           if (uT > bU) { bU = uT; bestN = (uint32_t)n; }
         }
         K[id] = Kval; U[id] = bU; label[id] = bestN;
@@ -846,7 +900,7 @@ void orc_mj_init(float* K, float* U, uint32_t* label, const orc_mj_atom* atoms, 
  * formula, the running maximum bestU and the current labels persist (an atom may take cells
  * over); psi is not touched. */
 void orc_mj_init_persist(float* K, float* bestU, uint32_t* label, const orc_mj_atom* atoms, int nElec, int S, float h,
-                         float h2, float Rsing) {
+                         float h2, float Rsing, const orc_mj_split* splits) {
 #pragma omp parallel for schedule(static)
   for (int i = 0; i < S; ++i)
     for (int j = 0; j < S; ++j)
@@ -867,7 +921,9 @@ void orc_mj_init_persist(float* K, float* bestU, uint32_t* label, const orc_mj_a
           Kval += Zn / r;
           float Ze = atoms[n].initZeff;
           float rReal = sqrtf(r2);
-          float uT = (rReal > atoms[n].initRcut || Za <= 0.f) ? 0.f : Ze * Ze * 0.5641895835f * expf(-Ze * r);
+          const int okSplit = !splits || mj_in_split(dx, dy, dz, rReal, &splits[n]);
+          float uT = (rReal > atoms[n].initRcut || Za <= 0.f || !okSplit) ? 0.f
+                                                                            : Ze * Ze * 0.5641895835f * expf(-Ze * r);
           if (uT > bU) { bU = uT; bestN = (uint32_t)n; }
         }
         K[id] = Kval; bestU[id] = bU; label[id] = bestN;

@@ -73,6 +73,10 @@ class Config(C.Structure):
                 ("reserved", C.c_int32 * 5)]
 
 
+class Split(C.Structure):
+    _fields_ = [("type", C.c_int32), ("idx", C.c_int32), ("axis", C.c_double * 3), ("rot", C.c_double)]
+
+
 class Atom(C.Structure):
     _fields_ = [("i", C.c_double), ("j", C.c_double), ("k", C.c_double), ("Z", C.c_double), ("Z_nuc", C.c_double),
                 ("rc", C.c_double), ("init_zeff", C.c_double), ("init_rcut", C.c_double)]
@@ -165,6 +169,7 @@ SIGNATURES = {
     "rq_rb_download_K": (C.c_int, [_V, _P]),
     "rq_rb_info": (C.c_int, [_V, _P, _P]),
     "rq_set_locked_groups": (C.c_int, [_V, _I, _P, _P]),
+    "rq_set_splits": (C.c_int, [_V, _P]),
     "rq_kernel_update_sp": (C.c_int, [_P, _P, _P, _P, _P, _I, _F, _F, _V]),
     "rq_kernel_jacobi_sp": (C.c_int, [_P, _P, _P, _I, _F, _F, _V]),
     "rq_kernel_labels_sp": (C.c_int, [_P, _P, _P, _I, _I, _F, _F, _V]),

@@ -136,6 +136,25 @@ class Context:
         self._chk(self.lib.rq_set_locked_groups(self.ctx, len(groups), _ptr(offsets), _ptr(members)),
                   "rq_set_locked_groups")
 
+    def set_splits(self, splits):
+        """molecule.js flavour: the shell split of every entry (USER_SPLIT_TYPE / _IDX / _AXIS / _ROT,
+        molecule.js:27-32) as dicts {type: 'hemi'|'third'|2|3, idx, axis, rot} (None or {} = whole
+        sphere); set before initialize().  None removes them."""
+        if not splits:
+            self._chk(self.lib.rq_set_splits(self.ctx, None), "rq_set_splits")
+            return
+        arr = (L.Split * len(self._atoms))()
+        codes = {"sphere": 0, "hemi": 2, "third": 3, "tetra": 4}
+        for n, sp in enumerate(splits):
+            if not sp:
+                continue
+            t = sp.get("type", 0)
+            arr[n].type = codes.get(t, 0) if isinstance(t, str) else int(t or 0)
+            arr[n].idx = int(sp.get("idx", 0))
+            arr[n].axis[:] = [float(v) for v in (sp.get("axis") or (0.0, 0.0, 1.0))]
+            arr[n].rot = float(sp.get("rot", 0.0))
+        self._chk(self.lib.rq_set_splits(self.ctx, arr), "rq_set_splits")
+
     def set_external_potential(self, v):
         """Add an external potential v (S^3 values, Ha) to K (new flavour); None removes it."""
         arr = None if v is None else np.ascontiguousarray(np.asarray(v, np.float64).reshape(-1))

@@ -135,7 +135,7 @@ static void free_ctx(rq_ctx* c) {
   for (auto& gx : c->graph)
     if (gx) cudaGraphExecDestroy(gx);
   void* ptrs[] = {c->U[0], c->U[1], c->P[0], c->P[1], c->K, c->W, c->bestU, c->rho, c->Pother, c->resid, c->lab[0], c->lab[1],
-                  c->Ec[0], c->Ec[1], c->fc, c->atoms5, c->scratch_atoms5, c->sic, c->sic2, c->pdirect, c->lob, c->lob_part, c->lob_scal, c->lock, c->bin_start, c->bin_idx, c->bin_far, c->bin_zmax, c->atoms_mj, c->atoms_nm, c->Zdom, c->Zdom64, c->dnorm,
+                  c->Ec[0], c->Ec[1], c->fc, c->atoms5, c->scratch_atoms5, c->sic, c->sic2, c->pdirect, c->lob, c->lob_part, c->lob_scal, c->lock, c->splits, c->bin_start, c->bin_idx, c->bin_far, c->bin_zmax, c->atoms_mj, c->atoms_nm, c->Zdom, c->Zdom64, c->dnorm,
                   c->dpd, c->dF, c->dsum, c->unorm, c->scale, c->err, c->seeds, c->scale64, c->Kext};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -181,6 +181,7 @@ static int alloc_all(rq_ctx* c) {
       if (mj_direct(c)) DALLOC(c->pdirect, S3 * sizeof(float) * n);
     }
     DALLOC(c->lock, sizeof(unsigned long long) * n);
+    DALLOC(c->splits, sizeof(MjSplit) * n);
     if (c->cfg.lobpcg) {
       DALLOC(c->lob, S3 * sizeof(float) * 5);
       DALLOC(c->lob_part, sizeof(float) * kLobMaxWG * kLobNR);
@@ -531,6 +532,22 @@ extern "C" int rq_set_locked_groups(rq_ctx* c, int32_t n_groups, const int32_t* 
     }
   }
   CK(cudaMemcpyAsync(c->lock, mask.data(), mask.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return RQ_OK;
+}
+
+extern "C" int rq_set_splits(rq_ctx* c, const rq_split* splits) {
+  if (!c) return RQ_EINVAL;
+  if (c->cfg.flavor != RQ_FLAVOR_MOLECULE_JS) return rq_fail(c, RQ_ENOTSUP, "shell splits are molecule.js's");
+  std::vector<MjSplit> d((size_t)c->n_atoms, MjSplit{0u, 0u, 0.f, 0.f, 1.f, 0.f});
+  if (splits)
+    for (int n = 0; n < c->n_atoms; ++n) {
+      const rq_split& s = splits[n];
+      if (s.type < 0 || s.idx < 0) return rq_fail(c, RQ_EINVAL, "negative split type or index");
+      d[n] = MjSplit{(uint32_t)s.type, (uint32_t)s.idx, (float)s.axis[0], (float)s.axis[1], (float)s.axis[2],
+                     (float)s.rot};
+    }
+  CK(cudaMemcpyAsync(c->splits, d.data(), d.size() * sizeof(MjSplit), cudaMemcpyHostToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
   return RQ_OK;
 }

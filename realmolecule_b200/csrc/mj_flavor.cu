@@ -97,7 +97,7 @@ int mj_initialize(rq_ctx* c) {
   // points; both psi buffers, both label buffers, P = Pother = 0, W = 1
   LAUNCH(RQ_KC_OTHER, 12.0 * c->g.S3,
          launch_mj_init((float*)c->K, (float*)c->U[0], c->bestU, c->lab[0], atoms_dev(c), c->n_atoms, c->g, p.h, p.h2,
-                        p.Rsing, p.hasBare, false, c->st));
+                        p.Rsing, p.hasBare, false, c->splits, c->st));
   CK(cudaMemcpyAsync(c->U[1], c->U[0], n * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
   CK(cudaMemcpyAsync(c->lab[1], c->lab[0], n * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
   for (int b = 0; b < 2; ++b) CK(cudaMemsetAsync(c->P[b], 0, n * sizeof(float), c->st));
@@ -119,7 +119,7 @@ int mj_set_atoms(rq_ctx* c) {
   const MjParams p = mj_params(c);
   LAUNCH(RQ_KC_OTHER, 16.0 * c->g.S3,
          launch_mj_init((float*)c->K, nullptr, c->bestU, c->lab[c->cl], atoms_dev(c), c->n_atoms, c->g, p.h, p.h2,
-                        p.Rsing, p.hasBare, true, c->st));
+                        p.Rsing, p.hasBare, true, c->splits, c->st));
   CK(cudaMemcpyAsync(c->lab[1 - c->cl], c->lab[c->cl], (size_t)c->g.S3 * sizeof(int), cudaMemcpyDeviceToDevice,
                      c->st));
   return RQ_OK;
@@ -249,7 +249,7 @@ static int mj_lobpcg_frame(rq_ctx* c) {
   for (int q = 0; q < wsteps; ++q) {
     LAUNCH(RQ_KC_LABELS, 20 * ip,
            launch_mj_evolve(c->lab[c->cl], c->lab[1 - c->cl], (float*)c->U[c->cu], c->W, at, c->n_atoms, c->g, p.dt_w,
-                            p.curvReg, p.h, p.hasBare, c->lock, c->st));
+                            p.curvReg, p.h, p.hasBare, c->lock, c->splits, c->st));
     c->cl ^= 1;
   }
   return RQ_OK;
@@ -326,7 +326,7 @@ int mj_step_one(rq_ctx* c, int s) {
     for (int q = 0; q < wsteps; ++q) {
       LAUNCH(RQ_KC_LABELS, 20 * ip,
              launch_mj_evolve(c->lab[c->cl], c->lab[1 - c->cl], (float*)c->U[c->cu], c->W, atoms_dev(c), c->n_atoms,
-                              c->g, p.dt_w, p.curvReg, p.h, p.hasBare, c->lock, c->st));
+                              c->g, p.dt_w, p.curvReg, p.h, p.hasBare, c->lock, c->splits, c->st));
       c->cl ^= 1;
     }
     if (c->cfg.chebyshev) {  // the page's E at the frame's end feeds the next frame's omega (:3186)

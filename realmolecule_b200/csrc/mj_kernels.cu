@@ -39,6 +39,46 @@ __device__ __forceinline__ bool mj_inside_rc(int ci, int cj, int ck, int lbl, co
   return false;
 }
 
+// inSplitAtom (molecule.js:197-226), d = cell - nucleus in bohr, r = |d|: the entry owns the
+// cell iff it lies in its sector.  atan2 is the f64 function rounded once to f32 (WGSL leaves its
+// accuracy to the implementation; the oracle does the same).
+__device__ bool mj_in_split(float dx, float dy, float dz, float r, const MjSplit& s) {
+  if (s.type <= 1u || r < 1e-6f) return true;
+  const float axL = fmaxf(F_SQRT(F_ADD(F_ADD(F_MUL(s.ax, s.ax), F_MUL(s.ay, s.ay)), F_MUL(s.az, s.az))), 1e-12f);
+  const float a0 = F_DIV(s.ax, axL), a1 = F_DIV(s.ay, axL), a2 = F_DIV(s.az, axL);
+  const float dotp = F_ADD(F_ADD(F_MUL(dx, a0), F_MUL(dy, a1)), F_MUL(dz, a2));
+  if (s.type == 2u) return s.idx == 0u ? dotp < 0.f : dotp >= 0.f;
+  if (s.type == 3u) {
+    const float px = F_SUB(dx, F_MUL(dotp, a0)), py = F_SUB(dy, F_MUL(dotp, a1)), pz = F_SUB(dz, F_MUL(dotp, a2));
+    float e1x, e1y, e1z;
+    if (fabsf(a2) < 0.9f) { e1x = a1; e1y = -a0; e1z = 0.f; } else { e1x = 0.f; e1y = a2; e1z = -a1; }
+    const float e1L = fmaxf(F_SQRT(F_ADD(F_ADD(F_MUL(e1x, e1x), F_MUL(e1y, e1y)), F_MUL(e1z, e1z))), 1e-12f);
+    e1x = F_DIV(e1x, e1L); e1y = F_DIV(e1y, e1L); e1z = F_DIV(e1z, e1L);
+    const float e2x = F_SUB(F_MUL(a1, e1z), F_MUL(a2, e1y)), e2y = F_SUB(F_MUL(a2, e1x), F_MUL(a0, e1z)),
+                e2z = F_SUB(F_MUL(a0, e1y), F_MUL(a1, e1x));
+    const float pe1 = F_ADD(F_ADD(F_MUL(px, e1x), F_MUL(py, e1y)), F_MUL(pz, e1z));
+    const float pe2 = F_ADD(F_ADD(F_MUL(px, e2x), F_MUL(py, e2y)), F_MUL(pz, e2z));
+    float th = F_SUB((float)atan2((double)pe2, (double)pe1), s.rot);
+    if (th < -3.14159265f) th = F_ADD(th, 6.28318530f);
+    if (th > 3.14159265f) th = F_SUB(th, 6.28318530f);
+    const unsigned sector = __float2uint_rz(floorf(F_DIV(F_ADD(th, 3.14159265f), 2.09439510f))) % 3u;
+    return sector == s.idx;
+  }
+  return true;
+}
+
+// evolveBoundary's cellSectorOK (molecule.js:437-442): d = (cell - nucleus) * h.
+__device__ __forceinline__ bool mj_sector_ok(int i, int j, int k, int n, const MjAtom* __restrict__ atoms,
+                                             const MjSplit* __restrict__ splits, float h) {
+  const MjSplit s = splits[n];
+  if (s.type <= 1u) return true;
+  const MjAtom a = atoms[n];
+  const float dx = F_MUL(F_SUB((float)i, (float)a.posI), h);
+  const float dy = F_MUL(F_SUB((float)j, (float)a.posJ), h);
+  const float dz = F_MUL(F_SUB((float)k, (float)a.posK), h);
+  return mj_in_split(dx, dy, dz, F_SQRT(F_ADD(F_ADD(F_MUL(dx, dx), F_MUL(dy, dy)), F_MUL(dz, dz))), s);
+}
+
 __device__ __forceinline__ int mj_pack(int ci, int cj, int ck, int lbl, const MjAtom* atoms, int nAt, bool hasBare,
                                        float h) {
   return lbl | (mj_inside_rc(ci, cj, ck, lbl, atoms, nAt, hasBare, h) ? kMjExcl : 0);
@@ -54,7 +94,8 @@ __device__ __forceinline__ int mj_pack(int ci, int cj, int ck, int lbl, const Mj
 template <bool PERSIST>
 __global__ void __launch_bounds__(256) k_mj_init(float* __restrict__ K, float* __restrict__ U, float* __restrict__ bestU,
                                                  int* __restrict__ label, const MjAtom* __restrict__ atoms, int nAt,
-                                                 Geo g, float h, float h2, float Rsing, bool hasBare) {
+                                                 Geo g, float h, float h2, float Rsing, bool hasBare,
+                                                 const MjSplit* __restrict__ splits) {
   const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= g.S3) return;
   const int S = g.S;
@@ -75,7 +116,8 @@ __global__ void __launch_bounds__(256) k_mj_init(float* __restrict__ K, float* _
     Kval = F_ADD(Kval, F_DIV(Zn, r));
     const float rReal = F_SQRT(r2);
     const float Ze = a.initZeff;
-    const float uT = (rReal > a.initRcut || Za <= 0.f) ? 0.f
+    const bool okSplit = mj_in_split(dx, dy, dz, rReal, splits[n]);  // the entry's sector (:1413)
+    const float uT = (rReal > a.initRcut || Za <= 0.f || !okSplit) ? 0.f
                                                        : F_MUL(F_MUL(F_MUL(Ze, Ze), 0.5641895835f), expf(F_MUL(-Ze, r)));
     if (uT > bU) { bU = uT; bestN = n; }
   }
@@ -438,7 +480,8 @@ __global__ void __launch_bounds__(256) k_mj_evolve(const int* __restrict__ labIn
                                                    const float* __restrict__ U, float* __restrict__ W,
                                                    const MjAtom* __restrict__ atoms, int nAt, Geo g, float dt_w,
                                                    float curvReg, float h, bool hasBare,
-                                                   const unsigned long long* __restrict__ lock) {
+                                                   const unsigned long long* __restrict__ lock,
+                                                   const MjSplit* __restrict__ splits) {
   const int k = 1 + blockIdx.x * kThreadsK + threadIdx.x;
   const int j = 1 + blockIdx.y * kThreadsJ + threadIdx.y;
   const int i0 = 1 + blockIdx.z * kMarch;
@@ -483,6 +526,16 @@ __global__ void __launch_bounds__(256) k_mj_evolve(const int* __restrict__ labIn
     w = F_ADD(w, F_MUL(curvReg, curv));
     int newL = myL;
     if (w < 0.0f) { newL = bestL; w = 0.1f; }
+    // shell splits (:514-533): a flip into a domain whose sector excludes the cell is cancelled; a
+    // cell outside its own domain's sector goes to the best neighbour whose sector holds it
+    const bool myOK = mj_sector_ok(i, j, k, myL, atoms, splits, h);
+    if (!mj_sector_ok(i, j, k, newL, atoms, splits, h)) {
+      newL = myL;
+      w = fmaxf(w, 0.1f);
+      if (!myOK && bestL != myL && mj_sector_ok(i, j, k, bestL, atoms, splits, h)) { newL = bestL; w = 0.1f; }
+    } else if (!myOK && newL == myL) {
+      if (bestL != myL && mj_sector_ok(i, j, k, bestL, atoms, splits, h)) { newL = bestL; w = 0.1f; }
+    }
     W[id] = w;
     labOut[id] = (newL == myL) ? stored : mj_pack(i, j, k, newL, atoms, nAt, hasBare, h);
   }
@@ -607,11 +660,13 @@ __global__ void __launch_bounds__(256) k_mj_gradp(const float* __restrict__ Pt, 
 static unsigned flat_blocks(long long n) { return (unsigned)((n + 255) / 256); }
 
 cudaError_t launch_mj_init(float* K, float* U, float* bestU, int* label, const MjAtom* atoms, int nAt, const Geo& g,
-                           float h, float h2, float Rsing, bool hasBare, bool persist, cudaStream_t st) {
+                           float h, float h2, float Rsing, bool hasBare, bool persist, const MjSplit* splits,
+                           cudaStream_t st) {
   if (persist)
-    k_mj_init<true><<<flat_blocks(g.S3), 256, 0, st>>>(K, U, bestU, label, atoms, nAt, g, h, h2, Rsing, hasBare);
+    k_mj_init<true><<<flat_blocks(g.S3), 256, 0, st>>>(K, U, bestU, label, atoms, nAt, g, h, h2, Rsing, hasBare, splits);
   else
-    k_mj_init<false><<<flat_blocks(g.S3), 256, 0, st>>>(K, U, bestU, label, atoms, nAt, g, h, h2, Rsing, hasBare);
+    k_mj_init<false><<<flat_blocks(g.S3), 256, 0, st>>>(K, U, bestU, label, atoms, nAt, g, h, h2, Rsing, hasBare,
+                                                         splits);
   return cudaGetLastError();
 }
 cudaError_t launch_mj_recompute_k(float* K, const MjAtom* atoms, int nAt, const Geo& g, float h, float Rsing,
@@ -725,10 +780,10 @@ cudaError_t launch_mj_sic_domain(const float* U, const int* label, float* Pother
 }
 cudaError_t launch_mj_evolve(const int* labIn, int* labOut, const float* U, float* W, const MjAtom* atoms, int nAt,
                              const Geo& g, float dt_w, float curvReg, float h, bool hasBare,
-                             const unsigned long long* lock, cudaStream_t st) {
+                             const unsigned long long* lock, const MjSplit* splits, cudaStream_t st) {
   if (g.NN < 2) return cudaSuccess;
   k_mj_evolve<<<march_grid(g), march_block(), 0, st>>>(labIn, labOut, U, W, atoms, nAt, g, dt_w, curvReg, h, hasBare,
-                                                       lock);
+                                                       lock, splits);
   return cudaGetLastError();
 }
 cudaError_t launch_mj_energy(const float* U, const float* Pv, const float* K, const int* label, const MjAtom* atoms,

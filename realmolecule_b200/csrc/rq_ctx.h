@@ -60,6 +60,8 @@ struct rq_ctx {
   float* lob = nullptr;
   // molecule.js locked groups: per label the bit set of its groups (n_atoms, zero = none)
   unsigned long long* lock = nullptr;
+  // molecule.js shell splits per entry (n_atoms, zero = none)
+  MjSplit* splits = nullptr;
   float* lob_part = nullptr;
   float* lob_scal = nullptr;
   // solver.py flavour: atom bins of the label step's argmax (rebuilt whenever atoms change)

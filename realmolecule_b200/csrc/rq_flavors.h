@@ -8,6 +8,12 @@ struct MjAtom {
   uint32_t posI, posJ, posK;
   float Z, rc, Z_nuc, initZeff, initRcut;
 };
+// An entry's shell split (the atom record's split fields, molecule.js:183-191): type 0/1 whole
+// sphere, 2 half space, 3 one of three 120-degree sectors; idx, axis, angular offset rot.
+struct MjSplit {
+  uint32_t type, idx;
+  float ax, ay, az, rot;
+};
 
 // molecule.js flavour (mj_flavor.cu)
 int mj_initialize(rq_ctx* c);

@@ -51,11 +51,13 @@ cudaError_t launch_zero_faces(T* f, const Geo& g, cudaStream_t st);
 // ---- molecule.js flavour (mj_kernels.cu); labels carry the r_c-exclusion flag in bit 30 ---
 }  // namespace rq
 struct MjAtom;
+struct MjSplit;
 namespace rq {
 constexpr int kMjExclBit = 0x40000000;
 constexpr int kMjLabelMask = 0x3FFFFFFF;
 cudaError_t launch_mj_init(float* K, float* U, float* bestU, int* label, const MjAtom* atoms, int nAt, const Geo& g,
-                           float h, float h2, float Rsing, bool hasBare, bool persist, cudaStream_t st);
+                           float h, float h2, float Rsing, bool hasBare, bool persist,
+                           const MjSplit* splits, cudaStream_t st);
 cudaError_t launch_mj_recompute_k(float* K, const MjAtom* atoms, int nAt, const Geo& g, float h, float Rsing,
                                   cudaStream_t st);
 cudaError_t launch_mj_flags(int* label, const MjAtom* atoms, int nAt, const Geo& g, float h, bool hasBare,
@@ -87,7 +89,7 @@ cudaError_t launch_mj_sic_domain(const float* U, const int* label, float* Pother
 // lock: per label the bit set of its locked groups (all 0 without groups)
 cudaError_t launch_mj_evolve(const int* labIn, int* labOut, const float* U, float* W, const MjAtom* atoms, int nAt,
                              const Geo& g, float dt_w, float curvReg, float h, bool hasBare,
-                             const unsigned long long* lock, cudaStream_t st);
+                             const unsigned long long* lock, const MjSplit* splits, cudaStream_t st);
 cudaError_t launch_mj_energy(const float* U, const float* Pv, const float* K, const int* label, const MjAtom* atoms,
                              const Geo& g, float h, float h3, float Rsing, int nDom, double* pd, double* dip,
                              cudaStream_t st);

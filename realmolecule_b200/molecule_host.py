@@ -44,7 +44,8 @@ class MoleculePage:
                  external_force=None, hinge_atoms=(), frozen_atoms=(), bond_constraints=(), water_triplets=(),
                  hoh_eq: float = 104.5, bend_k: float = 1.5, coincident_groups=(), rigid_groups=None,
                  shear_rate: float = 0.0, brownian: bool = False, brownian_gamma: float = 1.0,
-                 thermal_kick: Optional[float] = None, seed: int = 0, locked_groups=(), context=None, **ctx_opts):
+                 thermal_kick: Optional[float] = None, seed: int = 0, locked_groups=(), splits=(), split_groups=(),
+                 context=None, **ctx_opts):
         self.rows = [dict(a) for a in atoms]
         n = self.n = len(self.rows)
         self.NN, self.screen = int(NN), float(screen)
@@ -85,6 +86,15 @@ class MoleculePage:
         self.locked_groups = [list(g) for g in locked_groups]
         if self.locked_groups:
             self.ctx.set_locked_groups(self.locked_groups)
+        # USER_SPLIT_TYPE / _IDX / _AXIS / _ROT per entry (molecule.js:27-32) and USER_SPLIT_GROUPS,
+        # whose sector frames follow the water molecules (updateSplitFrames, :1840-1878)
+        sp = list(splits) + [None] * (n - len(splits))
+        self.split_type = [(s or {}).get("type", 0) for s in sp]
+        self.split_idx = [int((s or {}).get("idx", 0)) for s in sp]
+        self.split_axis = [list((s or {}).get("axis") or (0.0, 0.0, 1.0)) for s in sp]
+        self.split_rot = [float((s or {}).get("rot", 0.0)) for s in sp]
+        self.split_groups = [dict(g) for g in split_groups]
+        self._push_splits()
         self._reset_counters()
         self.nuc_vel = [[0.0, 0.0, 0.0] for _ in range(n)]
         self.nuc_force = [[0.0, 0.0, 0.0] for _ in range(n)]
@@ -115,6 +125,51 @@ class MoleculePage:
             r["Z"], r["Z_nuc"] = self.Z[e], self.Z_nuc[e] if self.Z[e] or self.Z_nuc[e] else 0.0
             rows.append(r)
         return rows
+
+    def _update_split_frames(self):
+        """updateSplitFrames (molecule.js:1840-1878): for each water of USER_SPLIT_GROUPS ({o: the O-site
+        entries, h: the two H entries, type}), the sector axis is the molecular-plane normal and the
+        offset puts the two O-H bonds in sectors 0 and 1 and the lone pair in sector 2; a 'hemi'
+        group splits along the H-H bisector instead."""
+        for g in self.split_groups:
+            o, h1, h2 = self.pos[g["o"][0]], self.pos[g["h"][0]], self.pos[g["h"][1]]
+            u1 = [h1[c] - o[c] for c in range(3)]
+            u2 = [h2[c] - o[c] for c in range(3)]
+            n1, n2 = math.hypot(*u1) or 1.0, math.hypot(*u2) or 1.0
+            u1 = [x / n1 for x in u1]
+            u2 = [x / n2 for x in u2]
+            a = [u1[1] * u2[2] - u1[2] * u2[1], u1[2] * u2[0] - u1[0] * u2[2], u1[0] * u2[1] - u1[1] * u2[0]]
+            na = math.hypot(*a)
+            if na < 1e-4:  # collinear: any normal
+                a, na = [0.0, 0.0, 1.0], 1.0
+            a = [x / na for x in a]
+            b = [u1[c] + u2[c] for c in range(3)]
+            nb = math.hypot(*b) or 1.0
+            b = [x / nb for x in b]
+            if g.get("type") == "hemi":
+                for e in g["o"]:
+                    self.split_axis[e], self.split_rot[e] = list(b), 0.0
+                continue
+            e1 = [a[1], -a[0], 0.0] if abs(a[2]) < 0.9 else [0.0, a[2], -a[1]]
+            ne1 = math.hypot(*e1) or 1.0
+            e1 = [x / ne1 for x in e1]
+            e2 = [a[1] * e1[2] - a[2] * e1[1], a[2] * e1[0] - a[0] * e1[2], a[0] * e1[1] - a[1] * e1[0]]
+            rot = math.atan2(sum(b[c] * e2[c] for c in range(3)), sum(b[c] * e1[c] for c in range(3))) + math.pi / 3
+            for e in g["o"]:
+                self.split_axis[e], self.split_rot[e] = list(a), rot
+
+    def _push_splits(self):
+        if not self.split_groups and not any(t not in (0, 1, "sphere", None) for t in self.split_type):
+            return
+        self._update_split_frames()
+        self.ctx.set_splits([{"type": t, "idx": i, "axis": ax, "rot": r}
+                             for t, i, ax, r in zip(self.split_type, self.split_idx, self.split_axis, self.split_rot)])
+
+    def _upload_atoms(self):
+        """fillAtomBuf + the device rebuild (molecule.js:1879-1903, :4563-4582): the split frames are
+        recomputed from the new positions before the rebuild labels cells with them."""
+        self._push_splits()
+        self.ctx.set_atoms(self._ctx_rows())
 
     def _reset_counters(self):
         self.tStep = self.phase_steps = self.frame_count = 0
@@ -333,7 +388,7 @@ class MoleculePage:
             for gm in grp[1:]:
                 pos[gm] = list(pos[grp[0]])
         self.nuc_steps += 1
-        self.ctx.set_atoms(self._ctx_rows())
+        self._upload_atoms()
 
     def temperature(self) -> float:
         """The thermostat's kinetic temperature in K (molecule.js:4545-4556)."""
@@ -350,7 +405,7 @@ class MoleculePage:
         for e, p in enumerate(new_positions[:self.n]):
             self.pos[e] = [float(x) for x in p]
             self.mol_pos[e] = [float(x) for x in p]
-        self.ctx.set_atoms(self._ctx_rows())
+        self._upload_atoms()
         self.initialize()
 
     def activateAtoms(self, count: int):  # noqa: N802 -- molecule.js:2151-2195
@@ -359,7 +414,7 @@ class MoleculePage:
         self.nuc_vel = [[0.0, 0.0, 0.0] for _ in range(self.n)]
         self.nuc_force = [[0.0, 0.0, 0.0] for _ in range(self.n)]
         self.pos = [list(p) for p in self.mol_pos]
-        self.ctx.set_atoms(self._ctx_rows())
+        self._upload_atoms()
         self.initialize()
         self.nuc_steps = 0
         self.active_count = count

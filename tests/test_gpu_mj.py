@@ -285,3 +285,46 @@ def test_locked_groups_frames_bit_exact(kind, groups):
         ctx.set_locked_groups([[0]] * 65)
     assert e.value.status == L.RQ_ENOTSUP
     ctx.set_locked_groups([])
+
+
+
+SPLIT_CASES = {
+    # three O-site domains in 120-degree sectors about the molecular-plane normal, two H domains
+    "third": ([{"i": 20, "j": 20, "k": 20, "Z": 1, "Z_nuc": 2}, {"i": 20, "j": 20, "k": 20, "Z": 1, "Z_nuc": 2},
+               {"i": 20, "j": 20, "k": 20, "Z": 1, "Z_nuc": 2}, {"i": 23, "j": 17, "k": 20, "Z": 1, "Z_nuc": 1},
+               {"i": 17, "j": 17, "k": 20, "Z": 1, "Z_nuc": 1}],
+              [{"type": "third", "idx": q, "axis": (0.0, 0.1, 1.0), "rot": 0.35} for q in range(3)] + [None, None]),
+    # a two-electron site split into half spaces along a tilted axis, next to a whole-sphere H
+    "hemi": ([{"i": 19, "j": 20, "k": 20, "Z": 1, "Z_nuc": 1}, {"i": 19, "j": 20, "k": 20, "Z": 1, "Z_nuc": 1},
+              {"i": 23, "j": 21, "k": 20, "Z": 1, "Z_nuc": 1}],
+             [{"type": "hemi", "idx": 0, "axis": (1.0, 1.0, 0.2)}, {"type": 2, "idx": 1, "axis": (1.0, 1.0, 0.2)},
+              None]),
+}
+
+
+@pytest.mark.parametrize("case", sorted(SPLIT_CASES))
+def test_shell_split_frames_bit_exact(case):
+    """Shell splits (USER_SPLIT_*, molecule.js:27-32; inSplitAtom :197-226): the trial labelling
+    keeps each split entry to its sector, and the level-set step cancels flips into foreign sectors
+    and hands cells that left their sector to a neighbour whose sector holds them (:514-533)."""
+    from realmolecule_b200 import Context
+    rows, splits = SPLIT_CASES[case]
+    opts = dict(steps_per_frame=7, norm_interval=5, vcycle_interval=3)
+    ref = orc.MoleculeJsDriver(40, 10.0, rows, splits=splits, **opts)
+    ref.initialize()
+    whole = orc.MoleculeJsDriver(40, 10.0, rows, **opts)
+    whole.initialize()
+    assert (ref.label != whole.label).sum() > 1000  # the sectors decide the initial labelling
+    ctx = Context(40, 10.0, rows, flavor="molecule.js", **opts)
+    ctx.set_splits(splits)
+    ctx.initialize()
+    lab0 = ctx.download(psi=False, label=True)["label"]
+    assert (lab0 != ref.label.astype(np.int32)).sum() <= 3  # init psi goes through expf: near-ties only
+    ctx.upload(psi=ref.U, label=ref.label.astype(np.int32))
+    for _ in range(3 * 7 + 2):
+        ref.step()
+    ctx.step(3 * 7 + 2)
+    st = ctx.download(psi=True, label=True, W=True)
+    assert np.array_equal(st["label"], ref.label.astype(np.int32))
+    assert np.array_equal(st["W"].view(np.uint32), ref.W.view(np.uint32))
+    assert np.array_equal(st["psi"].view(np.uint32), ref.U.view(np.uint32))

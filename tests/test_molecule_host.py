@@ -16,7 +16,7 @@ class FakeContext:
     def __init__(self, n, E=(-1.0,), F=None):
         self.n, self.E, self.k = n, list(E), 0
         self.F = np.zeros((n, 3)) if F is None else np.asarray(F, float)
-        self.steps, self.atoms, self.inits = [], [], 0
+        self.steps, self.atoms, self.inits, self.splits = [], [], 0, []
 
     def step(self, n):
         self.steps.append(n)
@@ -42,6 +42,9 @@ class FakeContext:
 
     def set_locked_groups(self, groups):
         self.locked = groups
+
+    def set_splits(self, splits):
+        self.splits.append([dict(x) for x in splits])
 
 
 WATER = [{"i": 50, "j": 50, "k": 50, "Z": 2, "el": "O"}, {"i": 60, "j": 57, "k": 50, "Z": 1, "el": "H"},
@@ -159,3 +162,48 @@ def test_lobpcg_frames_count_ten_steps_and_skip_forces():
 def test_locked_groups_reach_the_context():
     p, ctx = page(locked_groups=[[0, 1], [2]])
     assert ctx.locked == [[0, 1], [2]]
+
+
+def _sector(d, sp):
+    """inSplitAtom's sector index (molecule.js:209-224) in double precision."""
+    L = math.hypot(*sp["axis"])
+    a = [x / L for x in sp["axis"]]
+    dp = sum(d[c] * a[c] for c in range(3))
+    p = [d[c] - dp * a[c] for c in range(3)]
+    e1 = [a[1], -a[0], 0.0] if abs(a[2]) < 0.9 else [0.0, a[2], -a[1]]
+    n = math.hypot(*e1)
+    e1 = [x / n for x in e1]
+    e2 = [a[1] * e1[2] - a[2] * e1[1], a[2] * e1[0] - a[0] * e1[2], a[0] * e1[1] - a[1] * e1[0]]
+    th = math.atan2(sum(p[c] * e2[c] for c in range(3)), sum(p[c] * e1[c] for c in range(3))) - sp["rot"]
+    th += 2 * math.pi if th < -math.pi else -2 * math.pi if th > math.pi else 0.0
+    return int(math.floor((th + math.pi) / (2 * math.pi / 3))) % 3
+
+
+def test_split_frames_follow_the_water_and_precede_each_rebuild():
+    """updateSplitFrames (molecule.js:1840-1878): the O-site entries' sector frame puts the two O-H
+    bonds in sectors 0 and 1 and the lone pair in sector 2, is pushed before the context is
+    initialised and again before every rebuild after the nuclei move."""
+    rows = [{"i": 50, "j": 50, "k": 50, "Z": 1}] * 3 + [{"i": 57, "j": 55, "k": 52, "Z": 1},
+                                                         {"i": 43, "j": 56, "k": 49, "Z": 1}]
+    p, ctx = page(rows=rows, splits=[{"type": "third", "idx": q} for q in range(3)],
+                  split_groups=[{"o": [0, 1, 2], "h": [3, 4]}])
+    assert len(ctx.splits) == 1 and ctx.atoms == []
+    for move in range(2):
+        sp = ctx.splits[-1]
+        o = p.pos[0]
+        d1, d2 = ([p.pos[e][c] - o[c] for c in range(3)] for e in (3, 4))
+        lone = [-(d1[c] / math.hypot(*d1) + d2[c] / math.hypot(*d2)) for c in range(3)]
+        assert [_sector(d, sp[0]) for d in (d1, d2, lone)] == [0, 1, 2]
+        assert sp[0]["axis"] == sp[1]["axis"] == sp[2]["axis"] and sp[3]["type"] == 0
+        p.pos[3] = [p.pos[3][0] + 1.5, p.pos[3][1] - 2.0, p.pos[3][2] + 0.7]  # the molecule turns
+        p.restartWithPositions(p.pos)
+        assert len(ctx.splits) == move + 2 and len(ctx.atoms) == move + 1
+
+
+def test_hemi_split_group_uses_the_bisector():
+    rows = [{"i": 50, "j": 50, "k": 50, "Z": 1}] * 2 + [{"i": 57, "j": 55, "k": 50, "Z": 1},
+                                                         {"i": 43, "j": 55, "k": 50, "Z": 1}]
+    p, ctx = page(rows=rows, splits=[{"type": "hemi", "idx": 0}, {"type": "hemi", "idx": 1}],
+                  split_groups=[{"o": [0, 1], "h": [2, 3], "type": "hemi"}])
+    ax = ctx.splits[-1][0]["axis"]
+    assert abs(ax[0]) < 1e-12 and abs(ax[1] - 1.0) < 1e-12 and abs(ax[2]) < 1e-12
