@@ -179,6 +179,11 @@ RQ_API const char* rq_status_string(int status);
  * 100 Poisson bootstrap steps; molecule.js uploadInitialData (:1905-2101) for that flavour;
  * new flavour: nearest-seed labels, psi ~ exp(-|x-seed|) normalised per domain, one MG solve. */
 RQ_API int rq_initialize(rq_ctx* ctx);
+/* The molecule.js classical-MD backbone's full restart (USER_CLASSICAL_MD, molecule.js:4236-4286),
+ * after rq_set_atoms with the moved positions: K, the trial psi and the labels rebuilt from scratch,
+ * P cleared; unlike rq_initialize the level-set W and Pother (the stale potential the next frame's
+ * updates read) are kept.  molecule.js flavour only. */
+RQ_API int rq_restart(rq_ctx* ctx);
 /* Move nuclei and rebuild K (cloud/solver.py:538-548, molecule.js:4563-4582 without relabel). */
 RQ_API int rq_set_atoms(rq_ctx* ctx, const rq_atom* atoms, int32_t n_atoms);
 /* molecule.js locked groups (window.USER_LOCKED_GROUPS, molecule.js:490-503, compiled into the

@@ -462,6 +462,16 @@ class MoleculeJsDriver:
                 O().mj_init_pdirect(C.addressof(self.atoms), self.nA, m, self.Pdirect[m], self.Pother, self.S, self.h,
                                     self.h2)
 
+    def restart(self):
+        """The classical-MD backbone's full restart (molecule.js:4236-4286): K, labels and the trial
+        psi from scratch at the current positions, P cleared, W and Pother kept."""
+        O().mj_init(self.K, self.U, self.label, C.addressof(self.atoms), self.nA, self.S, self.h, self.h2, self.Rsing,
+                    self._splits_ptr())
+        self.bestU[:] = self.U
+        self.Unext[:] = self.U
+        self.P[:] = 0
+        self.P2[:] = 0
+
     def set_splits(self, splits):
         self.splits = None
         if splits:
@@ -485,8 +495,7 @@ class MoleculeJsDriver:
             r.setdefault("Z_nuc", r["Z"])
         self.atoms = mj_atoms(self.rows)
         O().mj_init_persist(self.K, self.bestU, self.label, C.addressof(self.atoms), self.nA, self.S, self.h, self.h2,
-                            self.Rsing, self._splits_ptr())
-        self.label2[:] = self.label
+                            self.Rsing, self._splits_ptr())  # labelBuf only; label2Buf keeps its faces
 
     def vcycle(self):
         O().mj_rho(self.U, self.rho, self.S)
@@ -590,7 +599,7 @@ class MoleculeJsDriver:
         for _ in range(max(1, self.spf)):
             O().mj_evolve_boundary(self.label, self.label2, self.U, self.W, S, self.dt_w, self.curv,
                                    self.lock.ctypes.data, C.addressof(self.atoms), self._splits_ptr(), self.h)
-            self.label, self.label2 = self.label2, self.label
+            self.label[:] = self.label2  # label2Buf -> labelBuf, all S^3 cells (molecule.js:3650)
 
     def step(self):
         if self.lobpcg:
@@ -638,7 +647,7 @@ class MoleculeJsDriver:
             for _ in range(max(1, self.spf)):
                 O().mj_evolve_boundary(self.label, self.label2, self.U, self.W, self.S, self.dt_w, self.curv,
                                       self.lock.ctypes.data, C.addressof(self.atoms), self._splits_ptr(), self.h)
-                self.label, self.label2 = self.label2, self.label
+                self.label[:] = self.label2  # label2Buf -> labelBuf, all S^3 cells (molecule.js:3103)
             if self.chebyshev:
                 self.cheb_E = self.total_energy()
 

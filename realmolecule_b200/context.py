@@ -126,6 +126,11 @@ class Context:
         self._chk(self.lib.rq_set_atoms(self.ctx, arr, len(arr)), "rq_set_atoms")
         self._atoms = arr
 
+    def restart(self):
+        """molecule.js flavour: the classical-MD backbone's full restart at the current positions
+        (K, trial psi, labels from scratch, P cleared; W and Pother kept)."""
+        self._chk(self.lib.rq_restart(self.ctx), "rq_restart")
+
     def set_locked_groups(self, groups):
         """molecule.js flavour: window.USER_LOCKED_GROUPS (molecule.js:490-503), a list of label
         lists; a boundary between two labels of one group does not move.  [] removes them."""

@@ -552,6 +552,16 @@ extern "C" int rq_set_splits(rq_ctx* c, const rq_split* splits) {
   return RQ_OK;
 }
 
+extern "C" int rq_restart(rq_ctx* c) {
+  if (!c) return RQ_EINVAL;
+  if (c->cfg.flavor != RQ_FLAVOR_MOLECULE_JS) return rq_fail(c, RQ_ENOTSUP, "the restart is molecule.js's");
+  c->sp_jdone = 0;
+  int rc = mj_restart(c);
+  if (rc != RQ_OK) return rc;
+  CK(cudaStreamSynchronize(c->st));
+  return RQ_OK;
+}
+
 extern "C" int rq_initialize(rq_ctx* c) {
   if (!c) return RQ_EINVAL;
   int rc;

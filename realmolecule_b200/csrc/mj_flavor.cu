@@ -113,15 +113,35 @@ int mj_initialize(rq_ctx* c) {
   return RQ_OK;
 }
 
+// The classical-MD backbone's full restart (molecule.js:4236-4286): K, the trial psi and the labels
+// rebuilt from scratch at the current positions (all S^3 cells of the current label buffer), P
+// cleared; unlike uploadInitialData the level-set W, Pother, the direct path's P_m and the spare
+// label buffer (the page's label2Buf, whose faces the next level-set pass hands back) are kept.
+int mj_restart(rq_ctx* c) {
+  const MjParams p = mj_params(c);
+  const size_t n = (size_t)c->g.S3;
+  LAUNCH(RQ_KC_OTHER, 12.0 * c->g.S3,
+         launch_mj_init((float*)c->K, (float*)c->U[c->cu], c->bestU, c->lab[c->cl], atoms_dev(c), c->n_atoms, c->g, p.h,
+                        p.h2, p.Rsing, p.hasBare, false, c->splits, c->st));
+  CK(cudaMemcpyAsync(c->U[1 - c->cu], c->U[c->cu], n * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
+  LAUNCH(RQ_KC_OTHER, 8.0 * c->g.S3,
+         launch_mj_flags(c->lab[1 - c->cl], atoms_dev(c), c->n_atoms, c->g, p.h, p.hasBare, c->st));
+  for (int b = 0; b < 2; ++b) CK(cudaMemsetAsync(c->P[b], 0, n * sizeof(float), c->st));
+  return RQ_OK;
+}
+
 int mj_set_atoms(rq_ctx* c) {
   // moveNuclei's rebuild (molecule.js:4563-4582): K from 0 with the init formula, persistent
-  // bestU / labels (a moved atom may take cells over); then the exclusion bits of every label
+  // bestU / labels (a moved atom may take cells over) in the current label buffer, all S^3 cells.
+  // The spare buffer stands for the page's label2Buf, which the rebuild does not touch: it keeps
+  // its face labels (the next level-set pass hands them back), with exclusion bits for the new
+  // positions.
   const MjParams p = mj_params(c);
   LAUNCH(RQ_KC_OTHER, 16.0 * c->g.S3,
          launch_mj_init((float*)c->K, nullptr, c->bestU, c->lab[c->cl], atoms_dev(c), c->n_atoms, c->g, p.h, p.h2,
                         p.Rsing, p.hasBare, true, c->splits, c->st));
-  CK(cudaMemcpyAsync(c->lab[1 - c->cl], c->lab[c->cl], (size_t)c->g.S3 * sizeof(int), cudaMemcpyDeviceToDevice,
-                     c->st));
+  LAUNCH(RQ_KC_OTHER, 8.0 * c->g.S3,
+         launch_mj_flags(c->lab[1 - c->cl], atoms_dev(c), c->n_atoms, c->g, p.h, p.hasBare, c->st));
   return RQ_OK;
 }
 
@@ -251,6 +271,8 @@ static int mj_lobpcg_frame(rq_ctx* c) {
            launch_mj_evolve(c->lab[c->cl], c->lab[1 - c->cl], (float*)c->U[c->cu], c->W, at, c->n_atoms, c->g, p.dt_w,
                             p.curvReg, p.h, p.hasBare, c->lock, c->splits, c->st));
     c->cl ^= 1;
+    // the spare buffer takes the new labels' faces: those of the page's label2Buf
+    LAUNCH(RQ_KC_LABELS, 8.0 * 6 * c->g.S2, launch_copy_faces(c->lab[c->cl], c->lab[1 - c->cl], c->g, c->st));
   }
   return RQ_OK;
 }
@@ -328,6 +350,7 @@ int mj_step_one(rq_ctx* c, int s) {
              launch_mj_evolve(c->lab[c->cl], c->lab[1 - c->cl], (float*)c->U[c->cu], c->W, atoms_dev(c), c->n_atoms,
                               c->g, p.dt_w, p.curvReg, p.h, p.hasBare, c->lock, c->splits, c->st));
       c->cl ^= 1;
+      LAUNCH(RQ_KC_LABELS, 8.0 * 6 * c->g.S2, launch_copy_faces(c->lab[c->cl], c->lab[1 - c->cl], c->g, c->st));
     }
     if (c->cfg.chebyshev) {  // the page's E at the frame's end feeds the next frame's omega (:3186)
       double e[RQ_ENERGY_LEN], ekk = 0;

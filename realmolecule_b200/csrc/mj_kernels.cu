@@ -1214,6 +1214,35 @@ __global__ void __launch_bounds__(256) k_mj_accum_norms(const float* __restrict_
   if (L >= 0 && (int)threadIdx.x == __ffs(peers) - 1) atomicAdd(&unorm[L], sum);
 }
 
+// Copy the six faces (any index 0 or NN) of one label buffer into another: the level-set pass
+// writes interior cells only, and in the page its output buffer (label2Buf, molecule.js:3103)
+// keeps the face labels of the last full copy (uploadInitialData, :2090).
+__global__ void k_copy_faces(const int* __restrict__ src, int* __restrict__ dst, Geo g) {
+  const long long n = g.S2;
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= 6 * n) return;
+  const int face = (int)(q / n);
+  const long long r = q % n;
+  const int a = (int)(r / g.S), b = (int)(r % g.S);
+  int i, j, k;
+  switch (face) {
+    case 0: i = 0; j = a; k = b; break;
+    case 1: i = g.NN; j = a; k = b; break;
+    case 2: i = a; j = 0; k = b; break;
+    case 3: i = a; j = g.NN; k = b; break;
+    case 4: i = a; j = b; k = 0; break;
+    default: i = a; j = b; k = g.NN; break;
+  }
+  const long long id = (long long)i * g.S2 + (long long)j * g.S + k;
+  dst[id] = src[id];
+}
+
+cudaError_t launch_copy_faces(const int* src, int* dst, const Geo& g, cudaStream_t st) {
+  const long long n = 6 * g.S2;
+  k_copy_faces<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(src, dst, g);
+  return cudaGetLastError();
+}
+
 static dim3 lob_cells_grid(const Geo& g) {
   const unsigned n = (unsigned)(g.NN - 1);
   return dim3((n + 31) / 32, (n + 7) / 8, n);

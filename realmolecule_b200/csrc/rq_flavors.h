@@ -17,6 +17,7 @@ struct MjSplit {
 
 // molecule.js flavour (mj_flavor.cu)
 int mj_initialize(rq_ctx* c);
+int mj_restart(rq_ctx* c);
 int mj_step_one(rq_ctx* c, int s);
 int mj_energy(rq_ctx* c, double* out, double* per_domain);
 int mj_forces(rq_ctx* c, int method, double* F);

@@ -96,6 +96,8 @@ cudaError_t launch_mj_energy(const float* U, const float* Pv, const float* K, co
 cudaError_t launch_mj_gradp(const float* P, const MjAtom* atoms, int nAt, const Geo& g, float inv_h, int R, double* F,
                             cudaStream_t st);
 cudaError_t launch_fill(float* f, float v, long long n, cudaStream_t st);
+// the six faces of label buffer src copied into dst
+cudaError_t launch_copy_faces(const int* src, int* dst, const Geo& g, cudaStream_t st);
 // LOBPCG frames (molecule.js:1455-1724): inner products in workgroups of kLobWG threads, at most
 // kLobMaxWG of them (molecule.js:1533-1534); kLobScal floats of per-iteration scalars
 constexpr int kLobNR = 12, kLobWG = 128, kLobMaxWG = 256, kLobScal = 32;

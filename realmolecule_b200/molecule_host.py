@@ -45,7 +45,7 @@ class MoleculePage:
                  hoh_eq: float = 104.5, bend_k: float = 1.5, coincident_groups=(), rigid_groups=None,
                  shear_rate: float = 0.0, brownian: bool = False, brownian_gamma: float = 1.0,
                  thermal_kick: Optional[float] = None, seed: int = 0, locked_groups=(), splits=(), split_groups=(),
-                 context=None, **ctx_opts):
+                 classical_md=None, sasa=None, context=None, **ctx_opts):
         self.rows = [dict(a) for a in atoms]
         n = self.n = len(self.rows)
         self.NN, self.screen = int(NN), float(screen)
@@ -74,6 +74,9 @@ class MoleculePage:
         self.coincident_groups, self.rigid_groups = list(coincident_groups), rigid_groups
         self.shear_rate, self.brownian, self.brownian_gamma = float(shear_rate), bool(brownian), float(brownian_gamma)
         self.thermal_kick = thermal_kick
+        # USER_CLASSICAL_MD / USER_SASA (molecule.js:3856-4291): the coarse-grained backbone mode
+        self.classical_md, self.sasa = classical_md, sasa
+        self.compact_rg = None
         self.rng = np.random.default_rng(seed)
         self._unique_nuclei()
         # `context`: an object with the Context methods used here (tests drive the host logic with one)
@@ -125,6 +128,179 @@ class MoleculePage:
             r["Z"], r["Z_nuc"] = self.Z[e], self.Z_nuc[e] if self.Z[e] or self.Z_nuc[e] else 0.0
             rows.append(r)
         return rows
+
+    # ---- the coarse-grained classical-MD backbone (molecule.js:3856-4291) -------------------------
+    def _moves(self, a) -> bool:
+        return a < self.n and self.Z[a] != 0
+
+    def _shift(self, group, d, sign=1.0):
+        for a in group:
+            if self._moves(a):
+                for c in range(3):
+                    self.pos[a][c] += sign * d[c]
+
+    def _classical_md(self, F):
+        """USER_CLASSICAL_MD: residues (groups, Ca atoms caIndices) move as rigid bodies under their
+        summed nuclear forces -- plus the SASA pressure toward the Ca centroid (USER_SASA) -- either
+        by per-residue translation ('translate': end damping, contact-driven damping of the quantum
+        forces, a helical radial bias, SHAKE on Ca-Ca distances, Ca-Ca steric repulsion, H-bond and
+        contact biases) or as two rigid strands turning about the hinge (default); positions are
+        clamped to [5, NN-5], and the electrons restart from scratch (rq_restart, :4236-4286) with
+        the step counters reset."""
+        cmd, pos, h, NN = self.classical_md, self.pos, self.h, self.NN
+        ca, groups = list(cmd["caIndices"]), [list(g) for g in cmd["groups"]]
+        nres, md_dt, fscale = len(ca), float(cmd["mdDt"]), self.force_scale
+        res = [[0.0, 0.0, 0.0] for _ in range(nres)]
+        for g in range(nres):  # 1. summed quantum forces per residue
+            for a in groups[g]:
+                if self._moves(a):
+                    for c in range(3):
+                        res[g][c] += F[a][c]
+        if self.sasa:  # SASA: exposed residues pushed toward the Ca centroid (:3885-3927)
+            probe = self.sasa.get("probeRadius") or 15.0
+            gamma = self.sasa.get("gamma") or 0.5
+            max_nb = self.sasa.get("maxNeighbors") or 6
+            cen = [sum(pos[ca[g]][c] for g in range(nres)) / nres for c in range(3)]
+            for g in range(nres):
+                p = pos[ca[g]]
+                nb = sum(1 for q in range(nres) if q != g and
+                         sum((pos[ca[q]][c] - p[c]) ** 2 for c in range(3)) < probe * probe)
+                exposure = max(0.0, 1 - nb / max_nb)
+                if exposure > 0:
+                    d = [cen[c] - p[c] for c in range(3)]
+                    dist = math.sqrt(sum(x * x for x in d)) + 0.01
+                    for c in range(3):
+                        res[g][c] += gamma * exposure * d[c] / dist
+        if cmd.get("mode") == "translate":
+            self._md_translate(cmd, ca, groups, res, md_dt, fscale)
+        else:
+            self._md_rigid_strands(cmd, ca, groups, res, md_dt, fscale)
+        for a in range(self.n):  # boundary clamp (:4224-4230)
+            if self.Z[a] != 0:
+                pos[a] = [max(5.0, min(NN - 5.0, x)) for x in pos[a]]
+        self.nuc_steps += 1
+        self._push_splits()  # fillAtomBuf (:4237)
+        self.ctx.set_atoms(self._ctx_rows())
+        self.ctx.restart()
+        self.tStep = 0
+        self.phase_steps = 0
+
+    def _md_translate(self, cmd, ca, groups, res, md_dt, fscale):
+        pos, h, nres = self.pos, self.h, len(ca)
+        max_disp = 1.0
+        pin_n = 0 if cmd.get("pinEnds") is False else 2
+        cb = cmd.get("contactBias")
+        q_damp = 1.0
+        if cb:  # quantum forces damped while a contact is far from its target (:3937-3955)
+            excess_max = 0.0
+            for pr in list(cb.get("hbonds") or []) + list(cb.get("contacts") or []):
+                d = math.sqrt(sum((pos[pr["b"]][c] - pos[pr["a"]][c]) ** 2 for c in range(3))) * h
+                excess_max = max(excess_max, (d - pr["target"]) / pr["target"])
+            q_damp = 0.0 if excess_max > 1.0 else 0.1 if excess_max > 0.5 else 0.5 if excess_max > 0.2 else 1.0
+
+        def capped(f, damp):
+            d = [f[c] * fscale * md_dt * 0.01 * damp for c in range(3)]
+            mag = math.sqrt(sum(x * x for x in d))
+            return [x * max_disp / mag for x in d] if mag > max_disp else d
+
+        for g in range(nres):
+            end_damp = 1.0
+            if pin_n > 0:
+                dfe = min(g, nres - 1 - g)
+                if dfe < pin_n:
+                    end_damp = (dfe + 1) / (pin_n + 1)
+            self._shift(groups[g], capped(res[g], end_damp * q_damp))
+        if len(groups) > nres:  # the C-terminal group follows the last residue
+            self._shift(groups[nres], capped(res[nres - 1], 1.0))
+        hb = cmd.get("helicalBias")
+        if hb:  # radial nudge toward the ideal helix radius (:3988-4034)
+            c0, cl = pos[ca[0]], pos[ca[nres - 1]]
+            ax = [cl[c] - c0[c] for c in range(3)]
+            al = math.sqrt(sum(x * x for x in ax)) + 1e-10
+            ax = [x / al for x in ax]
+            cen = [sum(pos[ca[g]][c] for g in range(nres)) / nres for c in range(3)]
+            r_ideal = (hb.get("idealRadius") or 4.35) / h
+            strength = hb.get("strength") or 0.02
+            for g in range(1, nres):
+                r = [pos[ca[g]][c] - cen[c] for c in range(3)]
+                axial = sum(r[c] * ax[c] for c in range(3))
+                p = [r[c] - axial * ax[c] for c in range(3)]
+                pl = math.sqrt(sum(x * x for x in p)) + 1e-10
+                radial = (r_ideal - pl) * strength
+                self._shift(groups[g], [p[c] / pl * radial for c in range(3)])
+        target = (cmd.get("targetCaCa") or 7.18) / h  # SHAKE on Ca-Ca distances (:4037-4064)
+        tol = cmd.get("shakeTolerance") or 0.15
+        lo, hi = target * (1 - tol), target * (1 + tol)
+        for _ in range(5):
+            for g in range(nres - 1):
+                a1, a2 = ca[g], ca[g + 1]
+                d = [pos[a2][c] - pos[a1][c] for c in range(3)]
+                dist = math.sqrt(sum(x * x for x in d))
+                if dist < lo or dist > hi:
+                    corr = ((lo if dist < lo else hi) - dist) / (2 * dist + 1e-10)
+                    cv = [x * corr for x in d]
+                    self._shift(groups[g], cv, -1.0)
+                    self._shift(groups[g + 1], cv)
+        min_nb = 3.0 * 1.8897 / h  # Ca-Ca steric repulsion beyond bonded neighbours (:4066-4094)
+        for g1 in range(nres):
+            for g2 in range(g1 + 2, nres):
+                d = [pos[ca[g2]][c] - pos[ca[g1]][c] for c in range(3)]
+                dist = math.sqrt(sum(x * x for x in d)) + 1e-10
+                if dist < min_nb:
+                    push = 0.5 * (min_nb - dist) / dist
+                    pv = [x * push * 0.5 for x in d]
+                    self._shift(groups[g1], pv, -1.0)
+                    self._shift(groups[g2], pv)
+        if cb:  # H-bond and contact biases (:4096-4161)
+            owner = {}
+            for g, grp in enumerate(groups):
+                for a in grp:
+                    owner[a] = g  # the last group holding an atom, as the page's search keeps
+
+            def pair_bias(a, b, target_au, strength):
+                d = [pos[b][c] - pos[a][c] for c in range(3)]
+                dg = math.sqrt(sum(x * x for x in d)) + 1e-10
+                if dg * h <= target_au:
+                    return
+                nudge = strength * (dg * h - target_au) / (dg * h)
+                nv = [x / dg * nudge * 0.5 for x in d]
+                if a in owner:
+                    self._shift(groups[owner[a]], nv)
+                if b in owner:
+                    self._shift(groups[owner[b]], nv, -1.0)
+
+            for pr in cb.get("hbonds") or []:
+                pair_bias(pr["a"], pr["b"], pr["target"], cb.get("hbondStrength") or 0.5)
+            for pr in cb.get("contacts") or []:
+                pair_bias(pr["a"], pr["b"], pr["target"], cb.get("contactStrength") or 1.0)
+            cm = [sum(pos[ca[g]][c] for g in range(nres)) / nres for c in range(3)]
+            rg2 = sum(sum((pos[ca[g]][c] - cm[c]) ** 2 for c in range(3)) for g in range(nres))
+            self.compact_rg = math.sqrt(rg2 / nres) * h
+
+    def _md_rigid_strands(self, cmd, ca, groups, res, md_dt, fscale):
+        pos, nres = self.pos, len(ca)
+        hinge = cmd.get("hingeRes") or nres // 2
+        hx = (pos[ca[hinge - 1]][0] + pos[ca[hinge]][0]) / 2
+        hy = (pos[ca[hinge - 1]][1] + pos[ca[hinge]][1]) / 2
+        t1 = sum((pos[ca[g]][0] - hx) * res[g][1] - (pos[ca[g]][1] - hy) * res[g][0] for g in range(hinge))
+        t2 = sum((pos[ca[g]][0] - hx) * res[g][1] - (pos[ca[g]][1] - hy) * res[g][0] for g in range(hinge, nres))
+        max_angle = 0.02
+        th1 = max(-max_angle, min(max_angle, t1 * fscale * md_dt * 0.0001))
+        th2 = max(-max_angle, min(max_angle, t2 * fscale * md_dt * 0.0001))
+
+        def turn(group, th):
+            cs, sn = math.cos(th), math.sin(th)
+            for a in group:
+                if self._moves(a):
+                    rx, ry = pos[a][0] - hx, pos[a][1] - hy
+                    pos[a][0], pos[a][1] = hx + rx * cs - ry * sn, hy + rx * sn + ry * cs
+
+        for g in range(hinge):
+            turn(groups[g], th1)
+        for g in range(hinge, nres):
+            turn(groups[g], th2)
+        if len(groups) > nres:
+            turn(groups[nres], th2)
 
     def _update_split_frames(self):
         """updateSplitFrames (molecule.js:1840-1878): for each water of USER_SPLIT_GROUPS ({o: the O-site
@@ -290,6 +466,10 @@ class MoleculePage:
         for a in self.hinge_atoms:
             if a < n:
                 F[a] = [0.0, 0.0, 0.0]
+        if self.classical_md and self.classical_md.get("caIndices"):
+            self.nuc_force = F
+            self._classical_md(F)
+            return
         pos = self.pos
         for i1, i2, r0, kb in self.bond_constraints:  # :4331-4346
             rx, ry, rz = ((pos[i1][d] - pos[i2][d]) * h for d in range(3))

@@ -46,6 +46,9 @@ class FakeContext:
     def set_splits(self, splits):
         self.splits.append([dict(x) for x in splits])
 
+    def restart(self):
+        self.restarts = getattr(self, "restarts", 0) + 1
+
 
 WATER = [{"i": 50, "j": 50, "k": 50, "Z": 2, "el": "O"}, {"i": 60, "j": 57, "k": 50, "Z": 1, "el": "H"},
          {"i": 40, "j": 57, "k": 50, "Z": 1, "el": "H"}]
@@ -207,3 +210,61 @@ def test_hemi_split_group_uses_the_bisector():
                   split_groups=[{"o": [0, 1], "h": [2, 3], "type": "hemi"}])
     ax = ctx.splits[-1][0]["axis"]
     assert abs(ax[0]) < 1e-12 and abs(ax[1] - 1.0) < 1e-12 and abs(ax[2]) < 1e-12
+
+
+# three residues of two atoms each, Ca atoms 0, 2, 4 thirty cells (3 bohr) apart on the 0.1-bohr grid
+# of page(): beyond the 3-angstrom steric minimum (56.7 cells) for the non-bonded pair 0-4
+CHAIN = [{"i": 12 + 30 * r + d, "j": 50, "k": 50, "Z": 1} for r in range(3) for d in (0, 1)]
+CMD = {"caIndices": [0, 2, 4], "groups": [[0, 1], [2, 3], [4, 5]], "mdDt": 10.0, "targetCaCa": 3.0}
+
+
+def test_classical_md_translate_moves_residues_then_restarts():
+    """USER_CLASSICAL_MD 'translate' (molecule.js:3929-4166): each residue moves by its summed force
+    x forceScale x mdDt x 0.01, damped toward the pinned ends by (d+1)/3 at distance d < 2 from an
+    end, capped at one cell; the electrons restart from scratch and the step counters reset."""
+    F = np.zeros((6, 3))
+    F[2:4, 1] = 0.2  # the middle residue is pulled along +j
+    F[0:2, 2] = 0.1  # the first residue along +k
+    p, ctx = page(rows=CHAIN, F=F, dynamics=True, n_move=5, steps_per_frame=5, no_nuc_repulsion=True,
+                  classical_md=dict(CMD, mode="translate"))
+    pos0 = [list(x) for x in p.pos]
+    p.frame()
+    assert getattr(ctx, "restarts", 0) == 1 and len(ctx.atoms) == 1
+    assert p.tStep == 0 and p.phase_steps == 5
+    dj = p.pos[2][1] - pos0[2][1]
+    assert abs(dj - 0.4 * 10.0 * 0.01 * 2 / 3) < 1e-12  # middle residue: distance 1 from the ends
+    assert abs((p.pos[0][2] - pos0[0][2]) - 0.2 * 10.0 * 0.01 / 3) < 1e-12  # first residue: damping 1/3
+    assert p.pos[4] == pos0[4] and p.pos[5] == pos0[5]
+
+
+def test_classical_md_shake_restores_the_ca_spacing():
+    F = np.zeros((6, 3))
+    F[4:6, 0] = 100.0  # the last residue pulled away: capped at one cell, then SHAKE pulls back
+    p, ctx = page(rows=CHAIN, F=F, dynamics=True, n_move=5, steps_per_frame=5, no_nuc_repulsion=True,
+                  classical_md=dict(CMD, mode="translate", shakeTolerance=0.01))
+    p.frame()
+    d = math.dist(p.pos[2], p.pos[4])
+    assert 30.0 < d <= 30.0 * 1.01 + 1e-9  # stretched, and back within the tolerance
+
+
+def test_classical_md_rigid_strands_turn_about_the_hinge():
+    """The default mode (molecule.js:4167-4222): two strands turn about the hinge between residues
+    hingeRes-1 and hingeRes by their torques, each angle capped at 0.02 rad."""
+    rows = [{"i": 10 + 6 * r, "j": 20, "k": 20, "Z": 1} for r in range(4)]
+    F = np.zeros((4, 3))
+    F[0, 1] = 50.0   # strand 1 (residues 0, 1) pushed to +j: turns by the cap
+    F[3, 1] = 1e-3   # strand 2: a small torque
+    cmd = {"caIndices": [0, 1, 2, 3], "groups": [[0], [1], [2], [3]], "mdDt": 1.0}
+    p, ctx = page(rows=rows, F=F, dynamics=True, n_move=5, steps_per_frame=5, no_nuc_repulsion=True,
+                  classical_md=cmd)
+    hinge = (19.0, 20.0)
+    pos0 = [list(x) for x in p.pos]
+    p.frame()
+    for a in range(4):  # rotations keep the distance to the hinge
+        r0 = math.hypot(pos0[a][0] - hinge[0], pos0[a][1] - hinge[1])
+        assert abs(math.hypot(p.pos[a][0] - hinge[0], p.pos[a][1] - hinge[1]) - r0) < 1e-9
+    th1 = math.atan2(p.pos[0][1] - hinge[1], p.pos[0][0] - hinge[0]) - math.pi
+    assert abs(abs(th1) - 0.02) < 1e-12
+    th2 = math.atan2(p.pos[3][1] - hinge[1], p.pos[3][0] - hinge[0])
+    assert 0 < th2 < 0.02
+    assert getattr(ctx, "restarts", 0) == 1
