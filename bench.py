@@ -420,6 +420,46 @@ def caller_legs(a):
                          "cpu": "the oracle's sequential restatement of atom.js (2 steps)"}
     out["mol_fast_ch4"] = mol_fast_leg(a)
     out["realqm_rb_h2"] = realqm_rb_leg(a)
+    out["molecule_js_lobpcg"] = lobpcg_leg(a)
+    return out
+
+
+def lobpcg_leg(a):
+    """molecule.js's LOBPCG frames (doLOBPCGStep, the page's 'L' solver) on the water molecule of the
+    C1 geometry (O with a 0.4-bohr core at the centre, H at (+-1.4305, 1.1078, 0) bohr; 64^3,
+    h = 0.25 bohr): frames from the third on replay one CUDA graph each; the oracle's restatement
+    of the same frames on the host cores beside them."""
+    import torch
+    from realmolecule_b200 import Context
+    rows = [{"i": 32, "j": 32, "k": 32, "Z": 6, "Z_nuc": 6, "rc": 0.4},
+            {"i": 37, "j": 36, "k": 32, "Z": 1, "Z_nuc": 1, "rc": 0.0},
+            {"i": 26, "j": 36, "k": 32, "Z": 1, "Z_nuc": 1, "rc": 0.0}]
+    ctx = Context(64, 16.0, rows, flavor="molecule.js", steps_per_frame=10, lobpcg=1)
+    ctx.initialize()
+    ctx.step(2)  # frame 0 (no search direction yet) eagerly, frame 1 captured
+    torch.cuda.synchronize()
+    frames, l0 = 50, ctx.kernel_launches
+    t0 = time.perf_counter()
+    ctx.step(frames)
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) / frames * 1e3
+    launches = (ctx.kernel_launches - l0) / frames
+    ctx.close()
+    out = {"grid": "64^3", "domains": 3, "iterations_per_domain": 10, "ms_per_frame": ms,
+           "launches_per_frame": launches,
+           "timing": "host wall clock around 50 frames (one CUDA-graph replay each, synchronised)"}
+    if not a.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        ref = orc.MoleculeJsDriver(64, 16.0, rows, steps_per_frame=10, lobpcg=True)
+        ref.initialize()
+        ref.step()
+        t0 = time.perf_counter()
+        ref.step()
+        ref.step()
+        out.update({"cpu_ms_per_frame": (time.perf_counter() - t0) / 2 * 1e3,
+                    "cpu_cores": len(os.sched_getaffinity(0)),
+                    "cpu": "the oracle's restatement of the frame, OpenMP, 2 frames"})
     return out
 
 
