@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--workload", default="glycine128")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-converge", action="store_true")
+    ap.add_argument("--leg", default=None, choices=["molecule_js_lobpcg", "mol_fast_ch4", "realqm_rb_h2"],
+                    help="run only this caller leg on one GPU and print its JSON (for profiling)")
     return ap.parse_args()
 
 
@@ -607,6 +609,12 @@ def converge_leg(stream, dist, rank, world):
 
 def main():
     a = parse()
+    if a.leg:
+        import torch
+        torch.cuda.set_device(0)
+        leg = {"molecule_js_lobpcg": lobpcg_leg, "mol_fast_ch4": mol_fast_leg, "realqm_rb_h2": realqm_rb_leg}[a.leg]
+        print(json.dumps({a.leg: leg(a)}), flush=True)
+        return
     if a.impl == "reference":
         run_reference_arm(a)
         return
