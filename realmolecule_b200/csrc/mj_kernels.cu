@@ -905,48 +905,42 @@ __global__ void __launch_bounds__(256) k_lob_apply_h(const float* __restrict__ U
                                                      const float* __restrict__ K, const int* __restrict__ label,
                                                      const float* __restrict__ Pother, const MjAtom* __restrict__ atoms,
                                                      Geo g, float h, float inv_h2) {
-  const int k = 1 + blockIdx.x * kThreadsK + threadIdx.x;
-  const int j = 1 + blockIdx.y * kThreadsJ + threadIdx.y;
-  const int i0 = 1 + blockIdx.z * kMarch;
-  if (k >= g.NN || j >= g.NN || i0 >= g.NN) return;
-  const int iend = min(i0 + kMarch, g.NN);
+  // one interior cell per thread: the LOBPCG grids are small, and a march along i would leave
+  // most SMs idle (64 blocks at 64^3)
+  const int k = 1 + blockIdx.x * 32 + threadIdx.x, j = 1 + blockIdx.y * 8 + threadIdx.y, i = 1 + blockIdx.z;
+  if (k >= g.NN || j >= g.NN) return;
   const long long S = g.S, S2 = g.S2;
-  long long id = (long long)i0 * S2 + j * S + k;
-  float u_m = __ldg(U + id - S2), u_c = __ldg(U + id);
-  int l_m = __ldg(label + id - S2), l_c = __ldg(label + id);
-  for (int i = i0; i < iend; ++i, id += S2) {
-    const float u_p = __ldg(U + id + S2);
-    const int l_p = __ldg(label + id + S2);
-    const int ljp = __ldg(label + id + S), ljm = __ldg(label + id - S), lkp = __ldg(label + id + 1),
-              lkm = __ldg(label + id - 1);
-    bool excl, up, um, ujp, ujm, ukp, ukm;  // excl: centre excluded; uX: neighbour X is used
-    if (BARE) {
-      const int L = l_c & kMjMask;
-      excl = lob_inside_rc(i, j, k, L, atoms, h);
-      up = (l_p & kMjMask) == L && !lob_inside_rc(i + 1, j, k, l_p & kMjMask, atoms, h);
-      um = (l_m & kMjMask) == L && !lob_inside_rc(i - 1, j, k, l_m & kMjMask, atoms, h);
-      ujp = (ljp & kMjMask) == L && !lob_inside_rc(i, j + 1, k, ljp & kMjMask, atoms, h);
-      ujm = (ljm & kMjMask) == L && !lob_inside_rc(i, j - 1, k, ljm & kMjMask, atoms, h);
-      ukp = (lkp & kMjMask) == L && !lob_inside_rc(i, j, k + 1, lkp & kMjMask, atoms, h);
-      ukm = (lkm & kMjMask) == L && !lob_inside_rc(i, j, k - 1, lkm & kMjMask, atoms, h);
-    } else {
-      excl = (l_c & kMjExcl) != 0;
-      up = l_p == l_c; um = l_m == l_c; ujp = ljp == l_c; ujm = ljm == l_c; ukp = lkp == l_c; ukm = lkm == l_c;
-    }
-    float out = 0.0f;
-    if (!excl) {
-      const float a = up ? u_p : u_c;
-      const float b = um ? u_m : u_c;
-      const float c = ujp ? __ldg(U + id + S) : u_c;
-      const float d = ujm ? __ldg(U + id - S) : u_c;
-      const float e = ukp ? __ldg(U + id + 1) : u_c;
-      const float f = ukm ? __ldg(U + id - 1) : u_c;
-      const float lap = F_SUB(F_ADD(F_ADD(F_ADD(F_ADD(F_ADD(a, b), c), d), e), f), F_MUL(6.0f, u_c));
-      out = F_ADD(F_MUL(F_MUL(-0.5f, lap), inv_h2), F_MUL(F_ADD(-__ldg(K + id), F_MUL(2.0f, __ldg(Pother + id))), u_c));
-    }
-    HU[id] = out;
-    u_m = u_c; u_c = u_p; l_m = l_c; l_c = l_p;
+  const long long id = (long long)i * S2 + j * S + k;
+  const int l_c = __ldg(label + id), l_p = __ldg(label + id + S2), l_m = __ldg(label + id - S2);
+  const int ljp = __ldg(label + id + S), ljm = __ldg(label + id - S), lkp = __ldg(label + id + 1),
+            lkm = __ldg(label + id - 1);
+  bool excl, up, um, ujp, ujm, ukp, ukm;  // excl: centre excluded; uX: neighbour X is used
+  if (BARE) {
+    const int L = l_c & kMjMask;
+    excl = lob_inside_rc(i, j, k, L, atoms, h);
+    up = (l_p & kMjMask) == L && !lob_inside_rc(i + 1, j, k, l_p & kMjMask, atoms, h);
+    um = (l_m & kMjMask) == L && !lob_inside_rc(i - 1, j, k, l_m & kMjMask, atoms, h);
+    ujp = (ljp & kMjMask) == L && !lob_inside_rc(i, j + 1, k, ljp & kMjMask, atoms, h);
+    ujm = (ljm & kMjMask) == L && !lob_inside_rc(i, j - 1, k, ljm & kMjMask, atoms, h);
+    ukp = (lkp & kMjMask) == L && !lob_inside_rc(i, j, k + 1, lkp & kMjMask, atoms, h);
+    ukm = (lkm & kMjMask) == L && !lob_inside_rc(i, j, k - 1, lkm & kMjMask, atoms, h);
+  } else {
+    excl = (l_c & kMjExcl) != 0;
+    up = l_p == l_c; um = l_m == l_c; ujp = ljp == l_c; ujm = ljm == l_c; ukp = lkp == l_c; ukm = lkm == l_c;
   }
+  float out = 0.0f;
+  if (!excl) {
+    const float u_c = __ldg(U + id);
+    const float a = up ? __ldg(U + id + S2) : u_c;
+    const float b = um ? __ldg(U + id - S2) : u_c;
+    const float c = ujp ? __ldg(U + id + S) : u_c;
+    const float d = ujm ? __ldg(U + id - S) : u_c;
+    const float e = ukp ? __ldg(U + id + 1) : u_c;
+    const float f = ukm ? __ldg(U + id - 1) : u_c;
+    const float lap = F_SUB(F_ADD(F_ADD(F_ADD(F_ADD(F_ADD(a, b), c), d), e), f), F_MUL(6.0f, u_c));
+    out = F_ADD(F_MUL(F_MUL(-0.5f, lap), inv_h2), F_MUL(F_ADD(-__ldg(K + id), F_MUL(2.0f, __ldg(Pother + id))), u_c));
+  }
+  HU[id] = out;
 }
 
 // lobpcgInner (molecule.js:1535-1610): interior cells numbered with k fastest; block w thread l
@@ -1256,9 +1250,9 @@ int lob_workgroups(const Geo& g) {
 cudaError_t launch_lob_apply_h(const float* U, float* HU, const float* K, const int* label, const float* Pother,
                                const MjAtom* atoms, const Geo& g, float h, float inv_h2, bool bare, cudaStream_t st) {
   if (bare)
-    k_lob_apply_h<true><<<march_grid(g), march_block(), 0, st>>>(U, HU, K, label, Pother, atoms, g, h, inv_h2);
+    k_lob_apply_h<true><<<lob_cells_grid(g), dim3(32, 8), 0, st>>>(U, HU, K, label, Pother, atoms, g, h, inv_h2);
   else
-    k_lob_apply_h<false><<<march_grid(g), march_block(), 0, st>>>(U, HU, K, label, Pother, atoms, g, h, inv_h2);
+    k_lob_apply_h<false><<<lob_cells_grid(g), dim3(32, 8), 0, st>>>(U, HU, K, label, Pother, atoms, g, h, inv_h2);
   return cudaGetLastError();
 }
 
