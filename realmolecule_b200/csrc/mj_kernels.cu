@@ -476,6 +476,11 @@ __global__ void k_mj_prolong(const float* __restrict__ Ec, float* __restrict__ P
 // :490-503, compiled into the page's shader): lock[l] has bit g set when label l is in group g; a
 // boundary cell whose label and best other label share a group keeps its label, W = max(W, 0.5).
 // ---------------------------------------------------------------------------------------
+// One plane per block: a cell's pass reuses nothing from the plane before it, and the page runs
+// the pass W_STEPS_PER_FRAME times a frame on grids from 32^3 up, where a 16-plane march leaves
+// most SMs idle.
+constexpr int kEvolveMarch = 1;
+
 __global__ void __launch_bounds__(256) k_mj_evolve(const int* __restrict__ labIn, int* __restrict__ labOut,
                                                    const float* __restrict__ U, float* __restrict__ W,
                                                    const MjAtom* __restrict__ atoms, int nAt, Geo g, float dt_w,
@@ -484,9 +489,9 @@ __global__ void __launch_bounds__(256) k_mj_evolve(const int* __restrict__ labIn
                                                    const MjSplit* __restrict__ splits) {
   const int k = 1 + blockIdx.x * kThreadsK + threadIdx.x;
   const int j = 1 + blockIdx.y * kThreadsJ + threadIdx.y;
-  const int i0 = 1 + blockIdx.z * kMarch;
+  const int i0 = 1 + blockIdx.z * kEvolveMarch;
   if (k >= g.NN || j >= g.NN || i0 >= g.NN) return;
-  const int iend = min(i0 + kMarch, g.NN);
+  const int iend = min(i0 + kEvolveMarch, g.NN);
   const long long S = g.S, S2 = g.S2;
   for (int i = i0; i < iend; ++i) {
     const long long id = (long long)i * S2 + j * S + k;
@@ -782,7 +787,8 @@ cudaError_t launch_mj_evolve(const int* labIn, int* labOut, const float* U, floa
                              const Geo& g, float dt_w, float curvReg, float h, bool hasBare,
                              const unsigned long long* lock, const MjSplit* splits, cudaStream_t st) {
   if (g.NN < 2) return cudaSuccess;
-  k_mj_evolve<<<march_grid(g), march_block(), 0, st>>>(labIn, labOut, U, W, atoms, nAt, g, dt_w, curvReg, h, hasBare,
+  k_mj_evolve<<<march_grid(g, kEvolveMarch), march_block(), 0, st>>>(labIn, labOut, U, W, atoms, nAt, g, dt_w, curvReg,
+                                                                     h, hasBare,
                                                        lock, splits);
   return cudaGetLastError();
 }
