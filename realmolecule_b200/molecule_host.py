@@ -45,7 +45,8 @@ class MoleculePage:
                  hoh_eq: float = 104.5, bend_k: float = 1.5, coincident_groups=(), rigid_groups=None,
                  shear_rate: float = 0.0, brownian: bool = False, brownian_gamma: float = 1.0,
                  thermal_kick: Optional[float] = None, seed: int = 0, locked_groups=(), splits=(), split_groups=(),
-                 classical_md=None, sasa=None, context=None, **ctx_opts):
+                 classical_md=None, sasa=None, init_zeff=None, init_rcut=None, user_init_zeff=None,
+                 user_init_rcut=None, context=None, **ctx_opts):
         self.rows = [dict(a) for a in atoms]
         n = self.n = len(self.rows)
         self.NN, self.screen = int(NN), float(screen)
@@ -53,6 +54,10 @@ class MoleculePage:
         self.Z_orig = [float(a.get("Z", 0.0)) for a in self.rows]
         self.Z_nuc = [float(a["Z_nuc"]) if a.get("Z_nuc") is not None else float(a.get("Z", 0.0)) for a in self.rows]
         self.Z = list(self.Z_orig)
+        # the trial psi's exponent and cut-off radius (fillAtomBuf, molecule.js:1886-1891): per atom
+        # USER_INIT_ZEFF / USER_INIT_RCUT, else the page-wide INIT_ZEFF / INIT_RCUT, else Z / 1e6
+        self.init_zeff, self.init_rcut = init_zeff, init_rcut
+        self.user_init_zeff, self.user_init_rcut = user_init_zeff, user_init_rcut
         self.mol_pos = [[float(a["i"]), float(a["j"]), float(a.get("k", self.NN // 2))] for a in self.rows]
         self.pos = [list(p) for p in self.mol_pos]
         # molecule.js:106, :116-121 -- defaults by the number of entries
@@ -120,12 +125,21 @@ class MoleculePage:
                 sites[key] = {"Z_eff": q, "elec": [e]}
         self.unique = list(sites.values())
 
+    def _init_params(self, e):
+        """fillAtomBuf's initZeff / initRcut of entry e (molecule.js:1886-1891)."""
+        zl, rl = self.user_init_zeff, self.user_init_rcut
+        zeff = ((zl[e] if e < len(zl) else 0) or self.Z[e]) if zl else (self.init_zeff or self.Z[e])
+        rcut = ((rl[e] if e < len(rl) else 0) or 1e6) if rl else (self.init_rcut or 1e6)
+        return float(zeff), float(rcut)
+
     def _ctx_rows(self):
         rows = []
         for e, a in enumerate(self.rows):
             r = dict(a)
             r["i"], r["j"], r["k"] = self.pos[e]
             r["Z"], r["Z_nuc"] = self.Z[e], self.Z_nuc[e] if self.Z[e] or self.Z_nuc[e] else 0.0
+            if self.init_zeff or self.init_rcut or self.user_init_zeff or self.user_init_rcut:
+                r["initZeff"], r["initRcut"] = self._init_params(e)
             rows.append(r)
         return rows
 

@@ -268,3 +268,18 @@ def test_classical_md_rigid_strands_turn_about_the_hinge():
     th2 = math.atan2(p.pos[3][1] - hinge[1], p.pos[3][0] - hinge[0])
     assert 0 < th2 < 0.02
     assert getattr(ctx, "restarts", 0) == 1
+
+
+def test_init_zeff_and_rcut_follow_fill_atom_buf():
+    """fillAtomBuf (molecule.js:1886-1891): the per-atom lists win, a 0 entry falls back to Z (and
+    1e6 for the radius); without a list the page-wide INIT_ZEFF / INIT_RCUT, else Z / 1e6."""
+    p, ctx = page(init_zeff=1.7, init_rcut=3.0)
+    p.restartWithPositions(p.pos)
+    assert [(r[3]) for r in ctx.atoms[-1]] == [2, 1, 1]
+    assert [p._init_params(e) for e in range(3)] == [(1.7, 3.0)] * 3
+    p, ctx = page(init_zeff=1.7, user_init_zeff=[3.1, 0, 0.9], user_init_rcut=[0, 2.5])
+    assert [p._init_params(e) for e in range(3)] == [(3.1, 1e6), (1.0, 2.5), (0.9, 1e6)]
+    rows = p._ctx_rows()
+    assert rows[0]["initZeff"] == 3.1 and rows[1]["initRcut"] == 2.5
+    p, ctx = page()
+    assert "initZeff" not in p._ctx_rows()[0]  # nothing set: the rows carry no override
