@@ -179,6 +179,10 @@ RQ_API const char* rq_status_string(int status);
  * 100 Poisson bootstrap steps; molecule.js uploadInitialData (:1905-2101) for that flavour;
  * new flavour: nearest-seed labels, psi ~ exp(-|x-seed|) normalised per domain, one MG solve. */
 RQ_API int rq_initialize(rq_ctx* ctx);
+/* molecule.js window.FREEZE_BOUNDARY (molecule.js:3095, :3643): with on != 0 the frames skip the
+ * level-set passes (labels and W stay as they are; the frame counter still advances); 0 lets the
+ * boundaries move again (the page's UNLOCK_AT_STEP, :4621-4624).  molecule.js flavour only. */
+RQ_API int rq_set_freeze_boundary(rq_ctx* ctx, int32_t on);
 /* The molecule.js classical-MD backbone's full restart (USER_CLASSICAL_MD, molecule.js:4236-4286),
  * after rq_set_atoms with the moved positions: K, the trial psi and the labels rebuilt from scratch,
  * P cleared; unlike rq_initialize the level-set W and Pother (the stale potential the next frame's

@@ -435,6 +435,7 @@ class MoleculeJsDriver:
         # useLOBPCG (molecule.js:1751): one step() is one doLOBPCGStep frame
         self.lobpcg = bool(lobpcg)
         self.sic = bool(sic)
+        self.freeze = False  # window.FREEZE_BOUNDARY (molecule.js:3095, :3643)
         if self.lobpcg:
             self.HX, self.LW, self.HW, self.LP, self.HP = (np.zeros(S3, np.float32) for _ in range(5))
         # SIC_INTERVAL (molecule.js:112); 0 = off
@@ -596,7 +597,7 @@ class MoleculeJsDriver:
                       self.half_d, self.dt)
         self.U, self.Unext = self.Unext, self.U
         self.frame += 1
-        for _ in range(max(1, self.spf)):
+        for _ in range(0 if self.freeze else max(1, self.spf)):
             O().mj_evolve_boundary(self.label, self.label2, self.U, self.W, S, self.dt_w, self.curv,
                                    self.lock.ctypes.data, C.addressof(self.atoms), self._splits_ptr(), self.h)
             self.label[:] = self.label2  # label2Buf -> labelBuf, all S^3 cells (molecule.js:3650)
@@ -644,7 +645,7 @@ class MoleculeJsDriver:
             if poisson and self.sic_interval and self.frame > 0 and self.frame % self.sic_interval == 0:
                 self.sic_pass()
             self.frame += 1
-            for _ in range(max(1, self.spf)):
+            for _ in range(0 if self.freeze else max(1, self.spf)):
                 O().mj_evolve_boundary(self.label, self.label2, self.U, self.W, self.S, self.dt_w, self.curv,
                                       self.lock.ctypes.data, C.addressof(self.atoms), self._splits_ptr(), self.h)
                 self.label[:] = self.label2  # label2Buf -> labelBuf, all S^3 cells (molecule.js:3103)

@@ -126,6 +126,10 @@ class Context:
         self._chk(self.lib.rq_set_atoms(self.ctx, arr, len(arr)), "rq_set_atoms")
         self._atoms = arr
 
+    def set_freeze_boundary(self, on: bool):
+        """molecule.js flavour: window.FREEZE_BOUNDARY -- frames skip the level-set passes while on."""
+        self._chk(self.lib.rq_set_freeze_boundary(self.ctx, 1 if on else 0), "rq_set_freeze_boundary")
+
     def restart(self):
         """molecule.js flavour: the classical-MD backbone's full restart at the current positions
         (K, trial psi, labels from scratch, P cleared; W and Pother kept)."""

@@ -552,6 +552,20 @@ extern "C" int rq_set_splits(rq_ctx* c, const rq_split* splits) {
   return RQ_OK;
 }
 
+extern "C" int rq_set_freeze_boundary(rq_ctx* c, int32_t on) {
+  if (!c) return RQ_EINVAL;
+  if (c->cfg.flavor != RQ_FLAVOR_MOLECULE_JS) return rq_fail(c, RQ_ENOTSUP, "FREEZE_BOUNDARY is molecule.js's");
+  if ((on != 0) != c->freeze) {
+    c->freeze = on != 0;
+    for (auto& gx : c->graph)  // captured periods hold the old choice
+      if (gx) {
+        cudaGraphExecDestroy(gx);
+        gx = nullptr;
+      }
+  }
+  return RQ_OK;
+}
+
 extern "C" int rq_restart(rq_ctx* c) {
   if (!c) return RQ_EINVAL;
   if (c->cfg.flavor != RQ_FLAVOR_MOLECULE_JS) return rq_fail(c, RQ_ENOTSUP, "the restart is molecule.js's");

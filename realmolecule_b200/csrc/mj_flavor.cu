@@ -265,7 +265,7 @@ static int mj_lobpcg_frame(rq_ctx* c) {
                           p.h3, c->n_atoms, nullptr, c->st));
   c->cu ^= 1;
   c->frame++;
-  const int wsteps = f.steps_per_frame > 1 ? f.steps_per_frame : 1;  // W_STEPS_PER_FRAME (:107)
+  const int wsteps = c->freeze ? 0 : f.steps_per_frame > 1 ? f.steps_per_frame : 1;  // :107; FREEZE_BOUNDARY :3643
   for (int q = 0; q < wsteps; ++q) {
     LAUNCH(RQ_KC_LABELS, 20 * ip,
            launch_mj_evolve(c->lab[c->cl], c->lab[1 - c->cl], (float*)c->U[c->cu], c->W, at, c->n_atoms, c->g, p.dt_w,
@@ -344,7 +344,7 @@ int mj_step_one(rq_ctx* c, int s) {
       }
     }
     c->frame++;
-    const int wsteps = spf > 1 ? spf : 1;  // W_STEPS_PER_FRAME (:107)
+    const int wsteps = c->freeze ? 0 : spf > 1 ? spf : 1;  // W_STEPS_PER_FRAME (:107); FREEZE_BOUNDARY (:3095)
     for (int q = 0; q < wsteps; ++q) {
       LAUNCH(RQ_KC_LABELS, 20 * ip,
              launch_mj_evolve(c->lab[c->cl], c->lab[1 - c->cl], (float*)c->U[c->cu], c->W, atoms_dev(c), c->n_atoms,

@@ -60,6 +60,8 @@ struct rq_ctx {
   float* lob = nullptr;
   // molecule.js locked groups: per label the bit set of its groups (n_atoms, zero = none)
   unsigned long long* lock = nullptr;
+  // molecule.js window.FREEZE_BOUNDARY: frames skip the level-set passes
+  bool freeze = false;
   // molecule.js shell splits per entry (n_atoms, zero = none)
   MjSplit* splits = nullptr;
   float* lob_part = nullptr;

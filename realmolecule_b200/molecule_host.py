@@ -46,7 +46,7 @@ class MoleculePage:
                  shear_rate: float = 0.0, brownian: bool = False, brownian_gamma: float = 1.0,
                  thermal_kick: Optional[float] = None, seed: int = 0, locked_groups=(), splits=(), split_groups=(),
                  classical_md=None, sasa=None, init_zeff=None, init_rcut=None, user_init_zeff=None,
-                 user_init_rcut=None, context=None, **ctx_opts):
+                 user_init_rcut=None, freeze_boundary=False, unlock_at_step=None, context=None, **ctx_opts):
         self.rows = [dict(a) for a in atoms]
         n = self.n = len(self.rows)
         self.NN, self.screen = int(NN), float(screen)
@@ -103,6 +103,10 @@ class MoleculePage:
         self.split_rot = [float((s or {}).get("rot", 0.0)) for s in sp]
         self.split_groups = [dict(g) for g in split_groups]
         self._push_splits()
+        # window.FREEZE_BOUNDARY / UNLOCK_AT_STEP (molecule.js:3095, :3643, :4621-4624)
+        self.freeze_boundary, self.unlock_at_step = bool(freeze_boundary), unlock_at_step
+        if self.freeze_boundary:
+            self.ctx.set_freeze_boundary(True)
         self._reset_counters()
         self.nuc_vel = [[0.0, 0.0, 0.0] for _ in range(n)]
         self.nuc_force = [[0.0, 0.0, 0.0] for _ in range(n)]
@@ -396,6 +400,9 @@ class MoleculePage:
             if self.dynamics:
                 self.move_nuclei()
         self.phase_steps += nsteps
+        if self.freeze_boundary and self.unlock_at_step and self.phase_steps >= self.unlock_at_step:
+            self.freeze_boundary = False  # the boundaries move from the next frame on (:4621-4624)
+            self.ctx.set_freeze_boundary(False)
         self.frame_count += 1
         if math.isfinite(self.E) and self.E < self.E_min:
             self.E_min = self.E

@@ -376,3 +376,38 @@ def test_restart_rebuilds_from_scratch_and_keeps_W_and_the_spare_faces():
     lab = ctx.download(psi=False, label=True)["label"]
     assert np.array_equal(ref.label[faces].astype(np.int32), faces0)
     assert np.array_equal(lab[faces], faces0)
+
+
+
+def test_freeze_boundary_then_release_bit_exact():
+    """FREEZE_BOUNDARY (molecule.js:3095): frozen frames keep labels and W; after the release the
+    level set moves again.  Frozen and released periods both run from CUDA graphs."""
+    from realmolecule_b200 import Context
+    opts = dict(steps_per_frame=7, norm_interval=5, vcycle_interval=3)
+    NN, screen, rows = atoms_case("many")
+    ref = orc.MoleculeJsDriver(NN, screen, rows, **opts)
+    ref.initialize()
+    ref.freeze = True
+    ctx = Context(NN, screen, rows, flavor="molecule.js", **opts)
+    ctx.initialize()
+    ctx.set_freeze_boundary(True)
+    ctx.upload(psi=ref.U, label=ref.label.astype(np.int32))
+    lab0, W0 = ref.label.copy(), ref.W.copy()
+    for _ in range(21):
+        ref.step()
+    ctx.step(21)
+    st = ctx.download(psi=True, label=True, W=True)
+    assert np.array_equal(ref.label, lab0) and np.array_equal(ref.W, W0)
+    assert np.array_equal(st["label"], lab0.astype(np.int32))
+    assert np.array_equal(st["W"].view(np.uint32), W0.view(np.uint32))
+    assert np.array_equal(st["psi"].view(np.uint32), ref.U.view(np.uint32))
+    ref.freeze = False
+    ctx.set_freeze_boundary(False)
+    for _ in range(21):
+        ref.step()
+    ctx.step(21)
+    st = ctx.download(psi=True, label=True, W=True)
+    assert not np.array_equal(ref.label, lab0)
+    assert np.array_equal(st["label"], ref.label.astype(np.int32))
+    assert np.array_equal(st["W"].view(np.uint32), ref.W.view(np.uint32))
+    assert np.array_equal(st["psi"].view(np.uint32), ref.U.view(np.uint32))

@@ -49,6 +49,9 @@ class FakeContext:
     def restart(self):
         self.restarts = getattr(self, "restarts", 0) + 1
 
+    def set_freeze_boundary(self, on):
+        self.freeze = getattr(self, "freeze", []) + [bool(on)]
+
 
 WATER = [{"i": 50, "j": 50, "k": 50, "Z": 2, "el": "O"}, {"i": 60, "j": 57, "k": 50, "Z": 1, "el": "H"},
          {"i": 40, "j": 57, "k": 50, "Z": 1, "el": "H"}]
@@ -283,3 +286,17 @@ def test_init_zeff_and_rcut_follow_fill_atom_buf():
     assert rows[0]["initZeff"] == 3.1 and rows[1]["initRcut"] == 2.5
     p, ctx = page()
     assert "initZeff" not in p._ctx_rows()[0]  # nothing set: the rows carry no override
+
+
+def test_freeze_boundary_until_the_unlock_step():
+    """FREEZE_BOUNDARY with UNLOCK_AT_STEP (molecule.js:4621-4624): frozen from the start, released
+    once phaseSteps reaches the unlock step."""
+    p, ctx = page(steps_per_frame=5, freeze_boundary=True, unlock_at_step=12)
+    assert ctx.freeze == [True]
+    p.frame()
+    p.frame()
+    assert ctx.freeze == [True] and p.freeze_boundary
+    p.frame()  # phase_steps 15 >= 12
+    assert ctx.freeze == [True, False] and not p.freeze_boundary
+    p.frame()
+    assert ctx.freeze == [True, False]
