@@ -1,0 +1,110 @@
+"""Second, pure-Python restatements of molecule.js's per-step shaders, written from the WGSL text
+independently of oracle/rq_oracle.c: updateU with the r_c exclusion and a bare nucleus
+(molecule.js:228-343, W_CUTOFF = 0 so mix(uc, u_raw, 1) = u_raw), the weighted Jacobi sweep with its
+literal 0.3333 (:723-749), the fixed-point norms and their decoding (:911-946) and normalize
+(:1077-1105).  Each is compared bit for bit with the C restatement on a small random grid (CPU);
+the GPU kernels are compared with the C restatement in test_gpu_mj.py."""
+import numpy as np
+
+import oracle as orc
+
+f32 = np.float32
+S = 9
+ROWS = [{"i": 3, "j": 4, "k": 4, "Z": 2.0, "Z_nuc": 2.0, "rc": 0.5},
+        {"i": 6, "j": 4, "k": 5, "Z": 1.0, "Z_nuc": 1.0, "rc": 0.0},
+        {"i": 4, "j": 6, "k": 3, "Z": 0.0, "Z_nuc": 1.0, "rc": 0.35}]  # a bare nucleus
+H = f32(0.4)
+
+
+def state(seed):
+    rng = np.random.default_rng(seed)
+    n = S ** 3
+    return (rng.random(n).astype(np.float32), rng.integers(0, 2, n).astype(np.uint32),
+            np.abs(rng.normal(size=n)).astype(np.float32), rng.normal(size=n).astype(np.float32) * f32(0.3))
+
+
+def dist(c, a):
+    d = [f32(f32(f32(x) - f32(a[q])) * H) for q, x in zip("ijk", c)]
+    return f32(np.sqrt(f32(f32(f32(d[0] * d[0]) + f32(d[1] * d[1])) + f32(d[2] * d[2]))))
+
+
+def inside_rc(c, lbl, has_bare):
+    """updateU's isInsideRc (molecule.js:246-259), the bare-nuclei loop compiled in when present."""
+    a = ROWS[lbl]
+    if a["rc"] > 0 and dist(c, a) < f32(a["rc"]):
+        return True
+    if has_bare:
+        for b in ROWS:
+            if b["Z"] <= 0 and b["Z_nuc"] > 0 and b["rc"] > 0 and dist(c, b) < f32(b["rc"]):
+                return True
+    return False
+
+
+def interior():
+    for i in range(1, S - 1):
+        for j in range(1, S - 1):
+            for k in range(1, S - 1):
+                yield i, j, k, (i * S + j) * S + k
+
+
+def test_update_matches_a_python_restatement():
+    U, label, K, Pother = state(1)
+    half_d, dt = f32(0.06), f32(0.12 * 0.16)
+    got = np.zeros_like(U)
+    atoms = orc.mj_atoms(ROWS)
+    orc.O().mj_update(U, got, K, label, Pother, orc.C.addressof(atoms), len(ROWS), 1, S, H, half_d, dt)
+    steps = {(1, 0, 0): S * S, (-1, 0, 0): -S * S, (0, 1, 0): S, (0, -1, 0): -S, (0, 0, 1): 1, (0, 0, -1): -1}
+    excluded = 0
+    for i, j, k, idx in interior():
+        my = int(label[idx])
+        if inside_rc((i, j, k), my, True):
+            want = f32(0)
+            excluded += 1
+        else:
+            uc = U[idx]
+            acc = None
+            for (di, dj, dk), off in steps.items():
+                ln = int(label[idx + off])
+                v = U[idx + off] if ln == my and not inside_rc((i + di, j + dj, k + dk), ln, True) else uc
+                acc = v if acc is None else f32(acc + v)
+            lap = f32(acc - f32(f32(6) * uc))
+            want = f32(f32(uc + f32(half_d * lap)) + f32(f32(dt * f32(K[idx] - f32(f32(2) * Pother[idx]))) * uc))
+        assert got[idx].view(np.uint32) == want.view(np.uint32), (i, j, k)
+    assert excluded > 0
+
+
+def test_weighted_jacobi_matches_a_python_restatement():
+    U, _, _, P = state(2)
+    rho = np.zeros_like(U)
+    orc.O().mj_rho(U, rho, S)
+    got = np.zeros_like(P)
+    h2, two_pi = f32(0.16), f32(2 * np.pi)
+    orc.O().mj_jacobi(P, got, rho, S, h2, two_pi)
+    for i, j, k, idx in interior():
+        s = P[idx + S * S]
+        for off in (-S * S, S, -S, 1, -1):
+            s = f32(s + P[idx + off])
+        rhs = f32(f32(h2 * two_pi) * f32(U[idx] * U[idx]))
+        want = f32(f32(f32(0.3333) * P[idx]) + f32(f32(s + rhs) / f32(9)))
+        assert got[idx].view(np.uint32) == want.view(np.uint32), (i, j, k)
+
+
+def test_fixed_point_norms_and_normalize_match_a_python_restatement():
+    U, label, _, _ = state(3)
+    h3 = f32(0.064)
+    acc = np.zeros(len(ROWS), np.uint32)
+    nf = np.zeros(len(ROWS), np.float32)
+    orc.O().mj_norms_fixed(U, label, S, h3, len(ROWS), acc, nf)
+    want = [0, 0, 0]
+    for *_, idx in interior():
+        want[int(label[idx])] = (want[int(label[idx])] + int(f32(f32(f32(U[idx] * U[idx]) * h3) * f32(16777216)))) % 2 ** 32
+    assert list(acc) == want
+    dec = [f32(f32(a) * f32(1 / 16777216)) for a in want]
+    assert np.array_equal(nf.view(np.uint32), np.array(dec, np.float32).view(np.uint32))
+    V = U.copy()
+    orc.O().mj_normalize(V, nf, label, orc.C.addressof(orc.mj_atoms(ROWS)), S)
+    for *_, idx in interior():
+        l = int(label[idx])
+        n, Z = dec[l], f32(ROWS[l]["Z"])
+        w = f32(U[idx] * f32(np.sqrt(f32(Z / n)))) if (n > 0 and Z > 0) else U[idx]
+        assert V[idx].view(np.uint32) == w.view(np.uint32)
