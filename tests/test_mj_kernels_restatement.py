@@ -108,3 +108,78 @@ def test_fixed_point_norms_and_normalize_match_a_python_restatement():
         n, Z = dec[l], f32(ROWS[l]["Z"])
         w = f32(U[idx] * f32(np.sqrt(f32(Z / n)))) if (n > 0 and Z > 0) else U[idx]
         assert V[idx].view(np.uint32) == w.view(np.uint32)
+
+
+def test_two_level_correction_matches_a_python_restatement():
+    """The V-cycle pieces (molecule.js:772-909): residual r = -2 pi rho - lap P, the 27-point
+    full-weighting restriction (weights 8/4/2/1, times 1/64), the coarse weighted Jacobi with
+    h_c^2 = 4 h^2 and 0.3333, and the trilinear prolongation added at half weight."""
+    rng = np.random.default_rng(5)
+    NN = S - 1
+    NC, SC = NN // 2, NN // 2 + 1
+    P = rng.normal(size=S ** 3).astype(np.float32)
+    rho = rng.random(S ** 3).astype(np.float32)
+    inv_h2, h2, two_pi = f32(1 / 0.16), f32(0.16), f32(2 * np.pi)
+    R = np.zeros_like(P)
+    orc.O().mj_residual(P, R, rho, S, inv_h2, two_pi)
+    for i, j, k, idx in interior():
+        s = P[idx + S * S]
+        for off in (-S * S, S, -S, 1, -1):
+            s = f32(s + P[idx + off])
+        lap = f32(f32(s - f32(f32(6) * P[idx])) * inv_h2)
+        want = f32(f32(-two_pi * rho[idx]) - lap)
+        assert R[idx].view(np.uint32) == want.view(np.uint32)
+    fc = np.zeros(SC ** 3, np.float32)
+    orc.O().mj_restrict(R, fc, S, SC)
+    F3 = R.reshape(S, S, S)
+    faces = [(1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)]
+    edges = [(1, 1, 0), (1, -1, 0), (-1, 1, 0), (-1, -1, 0), (1, 0, 1), (1, 0, -1), (-1, 0, 1), (-1, 0, -1),
+             (0, 1, 1), (0, 1, -1), (0, -1, 1), (0, -1, -1)]
+    corners = [(1, 1, 1), (1, 1, -1), (1, -1, 1), (1, -1, -1), (-1, 1, 1), (-1, 1, -1), (-1, -1, 1), (-1, -1, -1)]
+
+    def ssum(fi, fj, fk, offs):
+        acc = None
+        for a, b, c in offs:
+            v = F3[fi + a, fj + b, fk + c]
+            acc = v if acc is None else f32(acc + v)
+        return acc
+
+    want_c = np.zeros_like(fc)
+    for I in range(1, NC):
+        for J in range(1, NC):
+            for K2 in range(1, NC):
+                fi, fj, fk = 2 * I, 2 * J, 2 * K2
+                val = f32(f32(8) * F3[fi, fj, fk])
+                val = f32(val + f32(f32(4) * ssum(fi, fj, fk, faces)))
+                val = f32(val + f32(f32(2) * ssum(fi, fj, fk, edges)))
+                val = f32(val + ssum(fi, fj, fk, corners))
+                want_c[(I * SC + J) * SC + K2] = f32(val * f32(0.015625))
+    assert np.array_equal(fc.view(np.uint32), want_c.view(np.uint32))
+    E0 = rng.normal(size=SC ** 3).astype(np.float32)
+    E1 = np.zeros_like(E0)
+    orc.O().mj_coarse_smooth(E0, E1, fc, SC, h2)
+    for I in range(1, NC):
+        for J in range(1, NC):
+            for K2 in range(1, NC):
+                c = (I * SC + J) * SC + K2
+                s = E0[c + SC * SC]
+                for off in (-SC * SC, SC, -SC, 1, -1):
+                    s = f32(s + E0[c + off])
+                want = f32(f32(f32(0.3333) * E0[c]) + f32(f32(s + f32(f32(f32(4) * h2) * fc[c])) / f32(9)))
+                assert E1[c].view(np.uint32) == want.view(np.uint32)
+    Pf = P.copy()
+    orc.O().mj_prolong(E1, Pf, S, SC)
+    for i, j, k, idx in interior():
+        ci, cj, ck = i // 2, j // 2, k // 2
+        c1 = [min(x // 2 + (x & 1), NC) for x in (i, j, k)]
+        w = [f32(0.5) if (x & 1) else f32(1) for x in (i, j, k)]
+        w1 = [f32(f32(1) - x) for x in w]
+        corr = f32(0)
+        for a in (0, 1):
+            for b in (0, 1):
+                for c in (0, 1):
+                    wa, wb, wc = (w[0] if a == 0 else w1[0]), (w[1] if b == 0 else w1[1]), (w[2] if c == 0 else w1[2])
+                    ii, jj, kk = (ci if a == 0 else c1[0]), (cj if b == 0 else c1[1]), (ck if c == 0 else c1[2])
+                    corr = f32(corr + f32(f32(f32(wa * wb) * wc) * E1[(ii * SC + jj) * SC + kk]))
+        want = f32(P[idx] + f32(f32(0.5) * corr))
+        assert Pf[idx].view(np.uint32) == want.view(np.uint32), (i, j, k)
