@@ -183,3 +183,41 @@ def test_two_level_correction_matches_a_python_restatement():
                     corr = f32(corr + f32(f32(f32(wa * wb) * wc) * E1[(ii * SC + jj) * SC + kk]))
         want = f32(P[idx] + f32(f32(0.5) * corr))
         assert Pf[idx].view(np.uint32) == want.view(np.uint32), (i, j, k)
+
+
+def test_self_interaction_and_direct_path_helpers_match_a_python_restatement():
+    """computeRhoSelf / computeRhoOther (molecule.js:572-619), initPdirect (:621-662),
+    copyPotherForLabel (:665-692) and subtractPself (:694-720, fraction 1/Z for Z > 1)."""
+    U, label, _, Pother = state(4)
+    label = (label + (np.arange(S ** 3) % 3 == 0)).astype(np.uint32)  # labels 0, 1, 2
+    m = 1
+    rs, ro = np.full_like(U, 7.0), np.full_like(U, 7.0)
+    orc.O().mj_rho_self(U, label, m, rs, S)
+    orc.O().mj_rho_other(U, label, m, ro, S)
+    Pm = np.random.default_rng(6).normal(size=S ** 3).astype(np.float32)
+    cp, sub = Pother.copy(), Pother.copy()
+    orc.O().mj_copy_for_label(Pm, cp, label, m, S)
+    Z = f32(2.0)
+    orc.O().mj_sub_self(Pm, sub, label, m, Z, S)
+    atoms = orc.mj_atoms(ROWS)
+    pd, po = np.zeros_like(U), Pother.copy()
+    orc.O().mj_init_pdirect(orc.C.addressof(atoms), len(ROWS), 0, pd, po, S, H, f32(H * H))
+    h2 = f32(H * H)
+    for i, j, k, idx in interior():
+        u2 = f32(U[idx] * U[idx])
+        own = int(label[idx]) == m
+        assert rs[idx].view(np.uint32) == (u2 if own else f32(0)).view(np.uint32)
+        assert ro[idx].view(np.uint32) == (f32(0) if own else u2).view(np.uint32)
+        assert cp[idx].view(np.uint32) == (Pm[idx] if own else Pother[idx]).view(np.uint32)
+        want = f32(Pother[idx] - f32(Pm[idx] * f32(f32(1) / Z))) if own else Pother[idx]
+        assert sub[idx].view(np.uint32) == want.view(np.uint32)
+        xi, yj, zk = (f32(f32(c) * H) for c in (i, j, k))
+        val = f32(0)
+        for q, a in enumerate(ROWS):
+            if f32(a["Z"]) <= 0 or q == 0:
+                continue
+            dx, dy, dz = (f32(x - f32(f32(a[c]) * H)) for x, c in zip((xi, yj, zk), "ijk"))
+            r = f32(np.sqrt(f32(f32(f32(f32(dx * dx) + f32(dy * dy)) + f32(dz * dz)) + h2)))
+            val = f32(val + f32(f32(0.5) / r))
+        assert pd[idx].view(np.uint32) == val.view(np.uint32)
+        assert po[idx].view(np.uint32) == f32(Pother[idx] + val).view(np.uint32)
