@@ -194,3 +194,81 @@ def test_shell_mode_update_matches_a_python_restatement():
     Uo, Wo, Po = compare(d, 9)
     S3 = d.p.S ** 3
     assert (Wo[2 * S3:3 * S3] == 0).sum() > (Wo[5 * S3:] == 0).sum()  # sectors and r_out zero w cells
+
+
+def test_reduction_trees_match_a_python_restatement():
+    """reduceWGSL + finalizeWGSL (mol_fast.js:353-472): per cell the n norms and T (kinetic where
+    w > 0.1, Thomas-Fermi, tilt), V_eK, V_ee (P_tot - f_m P_m) and the dipole; each 128-cell
+    workgroup folds pairwise, one workgroup adds the partials in strides of 128 and folds again."""
+    nuc = [{"i": 4, "j": 5, "k": 5, "Z": 3, "rc": 0.6, "z_init": 2.5, "tilt_y": 0.01},
+           {"i": 7, "j": 5.5, "k": 6, "Z": 1, "tilt_x": -0.02},
+           {"i": 3.25, "j": 6, "k": 5, "Z": 0, "z_init": 1.2}]
+    d = orc.MolFastDriver(nuc, NN=12, screen=4.8, norm_targets=[2, 1, 1], kc_multi=1.5, alpha_tf=0.2)
+    p = d.p
+    n, S, NN = p.n, p.S, p.NN
+    S2, S3 = S * S, S ** 3
+    rng = np.random.default_rng(12)
+    U = rng.random(n * S3).astype(np.float32)
+    W = rng.random(n * S3).astype(np.float32)
+    P = (rng.random(n * S3) * 0.5).astype(np.float32)
+    K = (rng.random(S3) * 3).astype(np.float32)
+    got = np.zeros(n + 6, np.float32)
+    orc.O().mf_reduce(orc.C.addressof(p), U, W, P, K, got)
+    h, h3, n2 = f32(p.h), f32(p.h3), f32(p.N2)
+    kc, kcm, alpha = f32(p.kc), f32(p.kc_multi), f32(p.alpha_tf)
+    rcs = [[f32(v) for v in p.rcs[a]] for a in range(n)]
+    NR, NM = n + 6, NN - 1
+    tot = NM ** 3
+    nwg = -(-tot // 128)
+    parts = []
+    for w in range(nwg):
+        sn = [[f32(0)] * NR for _ in range(128)]
+        for lid in range(128):
+            cell = w * 128 + lid
+            if cell >= tot:
+                continue
+            k, j, i = cell % NM + 1, (cell // NM) % NM + 1, cell // (NM * NM) + 1
+            idx = (i * S + j) * S + k
+            T = VeK = Vee = dx = dy = dz = f32(0)
+            xc, yc, zc = (f32(f32(f32(c) - n2) * h) for c in (i, j, k))
+            ptot = f32(0)
+            for q in range(n):
+                ptot = f32(ptot + P[q * S3 + idx])
+            for m in range(n):
+                o = m * S3
+                v = U[o + idx]
+                sn[lid][m] = f32(f32(v * v) * h3)
+                self_n = rcs[m][1]
+                if W[o + idx] > f32(0.1):
+                    a_, b_, c_ = (f32(U[o + idx + s] - v) for s in (S2, S, 1))
+                    km = kcm if self_n > 1 else f32(1)
+                    T = f32(T + f32(f32(f32(km * kc) * f32(f32(f32(a_ * a_) + f32(b_ * b_)) + f32(c_ * c_))) * h))
+                VeK = f32(VeK - f32(f32(f32(K[idx] * v) * v) * h3))
+                rho_cell = f32(f32(v * v) * h3)
+                dx, dy, dz = f32(dx - f32(rho_cell * xc)), f32(dy - f32(rho_cell * yc)), f32(dz - f32(rho_cell * zc))
+                fm = f32(f32(1) / self_n) if self_n > 1 else f32(1)
+                Vee = f32(Vee + f32(f32(f32(f32(ptot - f32(fm * P[o + idx])) * v) * v) * h3))
+                if self_n > 1 and alpha > 0:
+                    rho_m = f32(v * v)
+                    pw = f32(math.pow(float(max(rho_m, f32(1e-20))), float(f32(1.6666667))))
+                    T = f32(T + f32(f32(f32(f32(0.6) * alpha) * pw) * h3))
+                tilt = rcs[m][3]
+                if tilt != 0:
+                    T = f32(T + f32(f32(f32(f32(f32(-tilt) * yc) * v) * v) * h3))
+            sn[lid][n:] = [T, VeK, Vee, dx, dy, dz]
+        s = 64
+        while s > 0:
+            for lid in range(s):
+                sn[lid] = [f32(x + y) for x, y in zip(sn[lid], sn[lid + s])]
+            s //= 2
+        parts.append(sn[0])
+    wg = [[f32(0)] * NR for _ in range(128)]
+    for lid in range(128):
+        for w in range(lid, nwg, 128):
+            wg[lid] = [f32(x + y) for x, y in zip(wg[lid], parts[w])]
+    s = 64
+    while s > 0:
+        for lid in range(s):
+            wg[lid] = [f32(x + y) for x, y in zip(wg[lid], wg[lid + s])]
+        s //= 2
+    assert np.array_equal(np.array(wg[0], np.float32).view(np.uint32), got.view(np.uint32))
