@@ -98,3 +98,51 @@ def test_poisson_pass(color, tgt):
         others = max(f32(rho[idx] - f32(f32(sf * us[idx]) * us[idx])), f32(0))
         Pm[idx] = f32(Pm[idx] + f32(dt * f32(f32(lap * inv_h2) + f32(two_pi * others))))
     assert np.array_equal(P1[m * S3:(m + 1) * S3].view(np.uint32), Pm.view(np.uint32))
+
+
+def test_norm_reduction_and_normalize():
+    """reduceNormWGSL + normalizeWGSL (realqm_rb.js:356-427): N_REDUCE_WG = min(256, ceil(cells/128))
+    workgroups of 128 threads, each thread striding over the interior cells, the pairwise fold, then
+    every normalize thread adds the partials in order and scales u by sqrt(tgt / norm)."""
+    rng = np.random.default_rng(31)
+    S3 = S ** 3
+    U = rng.random(2 * S3).astype(np.float32)
+    p = params([1.0, 2.0])
+    m = 1
+    U1 = U.copy()
+    got = orc.O().rb_normalize(orc.C.addressof(p), m, U1)
+    h3 = f32(p.h3)
+    NM = NN - 1
+    tot = NM ** 3
+    nwg = min(256, -(-tot // 128))
+    u = U[m * S3:(m + 1) * S3]
+    parts = []
+    for w in range(nwg):
+        sd = []
+        for lid in range(128):
+            acc = f32(0)
+            cell = w * 128 + lid
+            while cell < tot:
+                k, j, i = cell % NM + 1, (cell // NM) % NM + 1, cell // (NM * NM) + 1
+                v = u[(i * S + j) * S + k]
+                acc = f32(acc + f32(f32(v * v) * h3))
+                cell += nwg * 128
+            sd.append(acc)
+        s = 64
+        while s > 0:
+            for lid in range(s):
+                sd[lid] = f32(sd[lid] + sd[lid + s])
+            s //= 2
+        parts.append(sd[0])
+    norm = f32(0)
+    for x in parts:
+        norm = f32(norm + x)
+    assert np.float32(got).view(np.uint32) == norm.view(np.uint32)
+    sc = f32(np.sqrt(f32(f32(2.0) / norm)))
+    want = u.copy()
+    for i in range(1, NN):
+        for j in range(1, NN):
+            for k in range(1, NN):
+                idx = (i * S + j) * S + k
+                want[idx] = f32(u[idx] * sc)
+    assert np.array_equal(U1[m * S3:(m + 1) * S3].view(np.uint32), want.view(np.uint32))
