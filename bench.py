@@ -1,6 +1,7 @@
 """Benchmark of the RealQM solver step on B200 (one JSON line on rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload glycine128]
+                    [--leg molecule_js_lobpcg|mol_fast_ch4|realqm_rb_h2]
 
 Metric: grid-point updates per second (Gpt-updates/s): one update = one imaginary-time
 update of psi at one interior voxel; one solver step updates (NN-1)^3 voxels.
@@ -28,6 +29,11 @@ period with the flush before EVERY solver step (every kernel reads HBM cold).
            mixed precision and in FP64, and the 96 water clusters (1-12 waters, 48^3-128^3) as one
            mixed-precision batch against the plain FP64 path (one FP64 context per instance, one
            after another).  Times are CUDA events around initialise + solve on the solver stream.
+
+``callers`` the other reference callers of the step through their drop-ins, each beside its CPU
+           restatement: the recorded hairpin job (RealQMSolver), atom.js's He page, mol_fast.js's
+           CH4 page, realqm_rb.js's H2 page and molecule.js's LOBPCG frames (water, 64^3).
+           ``--leg NAME`` runs one of mol_fast_ch4, realqm_rb_h2 or molecule_js_lobpcg alone.
 
 ``--impl reference`` times that reference CPU implementation alone (the reference has no
 GPU path that can run here: its kernels need CuPy, which is not installed).
