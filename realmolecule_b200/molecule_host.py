@@ -10,9 +10,11 @@ page's ``window.USER_*`` globals.  Positions are grid coordinates (i, j, k).
 
 Kept from moveNuclei: user external forces, hinge atoms, bond-length and H-O-H angle
 restraints, coincident groups, rigid groups, frozen atoms, the shear body force, overdamped
-Brownian motion and the Andersen thermostat (a seeded generator stands in for Math.random).
-Not kept: the coarse-grained classical-MD backbone (USER_CLASSICAL_MD / USER_ELASTIC_BACKBONE)
-and the fold-force diagnostics, which only log.
+Brownian motion, the Andersen thermostat (a seeded generator stands in for Math.random) and the
+coarse-grained classical-MD backbone with its SASA pressure and full restart (USER_CLASSICAL_MD,
+USER_SASA).  Page options of the GPU frame: locked groups, shell splits and their water frames,
+FREEZE_BOUNDARY / UNLOCK_AT_STEP, INIT_ZEFF / INIT_RCUT, and the LOBPCG solver (lobpcg=1).
+Not kept: the fold-force diagnostics (USER_FOLD_ATOMS), which only log.
 """
 from __future__ import annotations
 
