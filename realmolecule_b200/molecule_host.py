@@ -115,6 +115,68 @@ class MoleculePage:
         self.nuc_force_total = [[0.0, 0.0, 0.0] for _ in range(n)]
         self.nuc_steps = 0
 
+    @classmethod
+    def from_page(cls, g: Dict, context=None) -> "MoleculePage":
+        """Build from a dict of a molecule.js page's window globals (molecule.js:4-152 and the
+        options read later): USER_ATOMS (i, j and optionally k, else round(NN/2)) with USER_Z,
+        USER_Z_NUC and USER_RC per entry -- the first NELEC entries, those with Z > 0 or Z_nuc > 0
+        counted as the page counts them -- and every page option MoleculePage keeps.  Options the
+        page reads with `||` take their defaults when falsy; USER_BEND_K and USER_CURV_REG keep an
+        explicit 0 (a curvature term of 0 is off)."""
+        def js(key):  # `window.KEY || default`: falsy means unset
+            v = g.get(key)
+            return v if v else None
+
+        NN = js("USER_NN") or 200
+        z = list(js("USER_Z") or [2, 3, 1, 0, 0])
+        zn = list(js("USER_Z_NUC") or z)
+        rc = list(js("USER_RC") or [])
+        atoms = list(js("USER_ATOMS") or [{"i": 80, "j": 120}, {"i": 100, "j": 77}, {"i": 120, "j": 120},
+                                           {"i": 100, "j": 100}, {"i": 100, "j": 100}])
+        at = lambda a, n, d=0.0: a[n] if n < len(a) and a[n] else d  # noqa: E731
+        nelec = sum(1 for n in range(len(atoms)) if at(z, n) > 0 or at(zn, n) > 0) or 3
+        rows = []
+        for n in range(nelec):
+            a = atoms[n] if n < len(atoms) else {"i": round(NN / 2), "j": round(NN / 2)}
+            rows.append({"i": a["i"], "j": a["j"], "k": a.get("k", round(NN / 2)), "Z": at(z, n),
+                         "Z_nuc": zn[n] if n < len(zn) else at(z, n), "rc": at(rc, n), "el": a.get("el", "")})
+        kw = {"NN": NN, "screen": js("USER_SCREEN") or 10.0}
+        for key, name in (("USER_STEPS_PER_FRAME", "steps_per_frame"), ("USER_STEPS", "total_steps"),
+                          ("USER_N_MOVE", "n_move"), ("USER_DYNAMICS", "dynamics"), ("USER_DT_NUC", "dt_nuc"),
+                          ("USER_NUC_SUBSTEPS", "nuc_substeps"), ("USER_DAMPING", "damping"),
+                          ("USER_FORCE_SCALE", "force_scale"), ("USER_LANGEVIN_GAMMA", "langevin_gamma"),
+                          ("NO_NUC_REPULSION", "no_nuc_repulsion"), ("NO_AUTO_DYNAMICS", "no_auto_dynamics"),
+                          ("CONVERGENCE_THRESHOLD", "convergence_threshold"),
+                          ("USER_EXTERNAL_FORCE", "external_force"), ("USER_HINGE_ATOMS", "hinge_atoms"),
+                          ("USER_FROZEN_ATOMS", "frozen_atoms"), ("USER_BOND_CONSTRAINTS", "bond_constraints"),
+                          ("USER_WATER_TRIPLETS", "water_triplets"), ("USER_HOH_EQ", "hoh_eq"),
+                          ("USER_COINCIDENT_GROUPS", "coincident_groups"), ("USER_RIGID_GROUPS", "rigid_groups"),
+                          ("USER_SHEAR_RATE", "shear_rate"), ("USER_BROWNIAN", "brownian"),
+                          ("USER_BROWNIAN_GAMMA", "brownian_gamma"), ("USER_THERMAL_KICK", "thermal_kick"),
+                          ("USER_LOCKED_GROUPS", "locked_groups"), ("USER_SPLIT_GROUPS", "split_groups"),
+                          ("USER_CLASSICAL_MD", "classical_md"), ("USER_SASA", "sasa"), ("INIT_ZEFF", "init_zeff"),
+                          ("INIT_RCUT", "init_rcut"), ("USER_INIT_ZEFF", "user_init_zeff"),
+                          ("USER_INIT_RCUT", "user_init_rcut"), ("FREEZE_BOUNDARY", "freeze_boundary"),
+                          ("UNLOCK_AT_STEP", "unlock_at_step"),
+                          # context options of the GPU frame
+                          ("USER_DV", "dv"), ("USER_JACOBI_PER_STEP", "jacobi_per_step"),
+                          ("USER_POISSON_INTERVAL", "vcycle_interval")):
+            if js(key) is not None:
+                kw[name] = js(key)
+        if js("USER_TEMPERATURE_K"):  # kT = T / 315775 Ha (molecule.js:123-128)
+            kw["langevin_kT"] = g["USER_TEMPERATURE_K"] / 315775.0
+        if g.get("USER_BEND_K") is not None:
+            kw["bend_k"] = g["USER_BEND_K"]
+        if g.get("USER_CURV_REG") is not None:  # 0 switches the curvature term off
+            kw["curv_reg"] = g["USER_CURV_REG"] if g["USER_CURV_REG"] else -1.0
+        st = list(g.get("USER_SPLIT_TYPE") or [])
+        if st:
+            si, sa, sr = (list(g.get(k) or []) for k in ("USER_SPLIT_IDX", "USER_SPLIT_AXIS", "USER_SPLIT_ROT"))
+            kw["splits"] = [{"type": at(st, n, 0), "idx": at(si, n, 0), "axis": at(sa, n, [0, 0, 1]),
+                             "rot": at(sr, n, 0.0)} for n in range(nelec)]
+        kw["sic"] = 1  # the page's own Pother path (direct Poisson for <= 5 domains, else the correction)
+        return cls(rows, context=context, **kw)
+
     # ---- set-up ---------------------------------------------------------------------------------
     def _unique_nuclei(self):
         """molecule.js:50-66 -- entries at one site share one nucleus of charge sum(Z_nuc || Z)."""

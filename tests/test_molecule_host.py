@@ -300,3 +300,24 @@ def test_freeze_boundary_until_the_unlock_step():
     assert ctx.freeze == [True, False] and not p.freeze_boundary
     p.frame()
     assert ctx.freeze == [True, False]
+
+
+def test_from_page_reads_the_page_globals():
+    """from_page builds rows and options from a page's window globals as molecule.js reads them
+    (molecule.js:4-152): k defaults to round(NN/2), only the first NELEC entries count, `||` options
+    take their defaults when falsy, temperatures become kT = T / 315775."""
+    g = {"USER_NN": 120, "USER_SCREEN": 12.0,
+         "USER_ATOMS": [{"i": 60, "j": 60, "el": "O"}, {"i": 66, "j": 64, "k": 58, "el": "H"},
+                        {"i": 54, "j": 64, "el": "H"}, {"i": 10, "j": 10, "el": ""}],
+         "USER_Z": [6, 1, 1, 0], "USER_RC": [0.4, 0, 0, 0], "USER_DT_NUC": 0, "USER_TEMPERATURE_K": 300,
+         "USER_LOCKED_GROUPS": [[0, 1]], "USER_CURV_REG": 0, "USER_DV": 0.1, "FREEZE_BOUNDARY": True,
+         "UNLOCK_AT_STEP": 500, "INIT_ZEFF": 1.7}
+    ctx = FakeContext(3)
+    p = MoleculePage.from_page(g, context=ctx)
+    assert p.n == 3 and p.NN == 120 and p.screen == 12.0
+    assert [r["k"] for r in p.rows] == [60, 58, 60] and [r["Z"] for r in p.rows] == [6, 1, 1]
+    assert p.rows[0]["rc"] == 0.4 and p.rows[1]["Z_nuc"] == 1
+    assert abs(p.langevin_kT - 300 / 315775.0) < 1e-15
+    assert p.dt_nuc == 2.0  # USER_DT_NUC = 0 falls back to the default for <= 5 entries
+    assert ctx.locked == [[0, 1]] and ctx.freeze == [True] and p.unlock_at_step == 500
+    assert p._init_params(0) == (1.7, 1e6)
