@@ -90,6 +90,14 @@ def interior(NN):
     return (NN - 1) ** 3
 
 
+def bench_config(desc, world):
+    """The workload description both arms print (identical, so the two lines compare)."""
+    return {"workload": desc,
+            "step": f"one schedule period = {PERIOD} solver steps (GPU arm: one CUDA-graph replay)",
+            "l2": "GPU arm: flushed (256 MB write) before every timed period; flush not timed",
+            "parallelism": f"replicas x{world}"}
+
+
 # ---------------------------------------------------------------------------------------
 # reference CPU implementation (oracle/_ref: the reference's kernel text compiled for the host)
 # ---------------------------------------------------------------------------------------
@@ -118,7 +126,7 @@ def run_reference_arm(a):
     line = {"metric": METRIC, "value": rate, "unit": "Gpt/s", "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": dt / a.steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": desc, "step": f"one schedule period = {per} solver steps"},
+            "config": bench_config(desc, a.gpus),
             "cpu_baseline": {"value": rate, "unit": "Gpt/s", "cores": threads, "kind": "reference",
                              "sample": f"{per * a.steps} solver steps after {per * a.warmup} warm-up"},
             "e2e": {"value": rate, "unit": "Gpt/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -326,10 +334,7 @@ def run_ours(a):
             "metric": METRIC, "value": value, "unit": "Gpt/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": desc,
-                       "step": f"one schedule period = {PERIOD} solver steps (one CUDA-graph replay)",
-                       "l2": "flushed (256 MB write) before every timed period; flush not timed",
-                       "parallelism": f"replicas x{world}"},
+            "config": bench_config(desc, world),
             "value_l2_flushed_every_solver_step": value_cold,
             "e2e": {"value": e2e, "unit": "Gpt/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -433,7 +433,9 @@ RQ_API int rq_kernel_init_sp(float* U, int32_t* label, float* K, float* bestU, c
 RQ_API int rq_kernel_recompute_k_sp(float* K, const float* atoms5, int32_t n_atoms, int32_t S, float h, float h2,
                              void* stream);
 /* FP64 per-label sums of psi^2*h3 (label clipped to [0,n) like cloud/solver.py:427), then
- * normalizeU (:210-225) with scale sqrt(Z/n).  norms_out (n doubles, device) may be NULL. */
+ * normalizeU (:210-225) with scale sqrt(Z/n).  norms_out (n doubles, device) may be NULL.
+ * Synchronises the stream; RQ_ENONFINITE when a domain's norm is NaN/Inf as an f32 (that
+ * domain is left unscaled). */
 RQ_API int rq_kernel_normalize_sp(float* U, const int32_t* label, const float* Zeff, int32_t n_atoms, int32_t S, float h3,
                            double* norms_out, void* stream);
 /* No counterpart in the reference.  The same normalisation as rq_kernel_normalize_sp, for
@@ -444,8 +446,11 @@ RQ_API int rq_kernel_normalize_sp(float* U, const int32_t* label, const float* Z
  * Limit: n_atoms <= RQ_NOALLOC_MAX_DOMAINS, otherwise RQ_EINVAL and nothing runs.
  * The array is shared by every call on a device and keeps the last call's contents (each call
  * clears what it sums into first); calls that overlap on the GPU race on it, so order them on
- * one stream.  The first call on each device looks up the array's device address; make it
- * before starting any stream capture on that device.  The per-domain sums are not returned. */
+ * one stream.  The first call in each CUDA context looks up the array's device address (cached
+ * per context: a context created again after cudaDeviceReset, or a non-primary context the
+ * caller made current, gets its own look-up); make it before starting any stream capture in
+ * that context.  The per-domain sums are not returned.  Like rq_kernel_normalize_sp it
+ * synchronises the stream and returns RQ_ENONFINITE for a NaN/Inf domain norm. */
 #define RQ_NOALLOC_MAX_DOMAINS 16384
 RQ_API int rq_kernel_normalize_sp_noalloc(float* U, const int32_t* label, const float* Zeff, int32_t n_atoms, int32_t S,
                                           float h3, void* stream);

@@ -14,7 +14,10 @@ compiled; the oracle restates that one (oracle/rq_oracle.c).
 The built .so travels with the repository snapshot to machines without the
 reference tree; nothing here runs there.
 
-Usage:  python oracle/ref_build.py [--reference /root/reference] [--force]
+Usage:  python oracle/ref_build.py [--reference DIR] [--force]
+
+The reference tree is DIR, else the environment variable REALQM_REFERENCE_DIR, else
+/root/reference (where the build container mounts it).
 """
 from __future__ import annotations
 
@@ -27,7 +30,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_ref")
 LIB = os.path.join(OUT_DIR, "libsolverpy_ref.so")
-DEFAULT_REFERENCE = "/root/reference"
+DEFAULT_REFERENCE = os.environ.get("REALQM_REFERENCE_DIR", "/root/reference")
 
 _KERNEL_RE = re.compile(r"cp\.RawKernel\(r'''(.*?)''',\s*'(\w+)'\)", re.S)
 _SIG_RE = re.compile(r"void\s+(\w+)\s*\(([^)]*)\)", re.S)

@@ -55,7 +55,8 @@ class EnergyModel:
         return rows
 
     def evaluate(self, positions: np.ndarray, v: Optional[np.ndarray] = None):
-        """Converged energy, total forces on the nuclei (n_nuc x 3) and h^3 rho for positions R."""
+        """Converged energy, total forces on the nuclei (n_nuc x 3) and h^3 rho for positions R
+        (h^3 rho is None when the model was built with want_rho=False and no v is given)."""
         positions = np.asarray(positions, np.float64).reshape(self.n_nuc, 3)
         self.ctx.set_atoms(self._rows(positions))
         if v is not None or self._v is not None:
@@ -71,7 +72,7 @@ class EnergyModel:
         _, Fn = self.ctx.nuclear_terms()
         F = Fe + Fn[: self.n_nuc]
         rho_h3 = None
-        if self.want_rho:
+        if self.want_rho or v is not None:  # dE/dv = -h^3 rho needs the density whenever v is given
             psi = self.ctx.download(psi=True, label=False)["psi"].astype(np.float64)
             rho_h3 = psi * psi * self.h ** 3
         self.last = {"E": E, "F": F, "steps": steps}

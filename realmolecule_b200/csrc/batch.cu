@@ -843,8 +843,16 @@ extern "C" int rq_batch_energy(rq_batch* b, double* out) {
     return RQ_OK;
   }));
   std::vector<double> pd((size_t)4 * b->D);
+  int bad_norm = 0;
   BCK(cudaMemcpyAsync(pd.data(), b->dpd, sizeof(double) * pd.size(), cudaMemcpyDeviceToHost, b->st));
+  BCK(cudaMemcpyAsync(&bad_norm, b->err, sizeof(int), cudaMemcpyDeviceToHost, b->st));
   BCK(cudaStreamSynchronize(b->st));
+  if (bad_norm) {  // a normalisation met a NaN/Inf domain norm and left that domain unscaled
+    BCK(cudaMemsetAsync(b->err, 0, sizeof(int), b->st));
+    BCK(cudaStreamSynchronize(b->st));
+    b->last_error = "non-finite domain norm in a normalisation";
+    return RQ_ENONFINITE;
+  }
   for (int q = 0; q < b->n; ++q) {
     const BInst& I = b->hin[q];
     double* o = out + (size_t)q * RQ_ENERGY_LEN;

@@ -820,6 +820,16 @@ extern "C" int rq_energy(rq_ctx* c, double* out, double* per_domain) {
   rq_nuclear_terms(c, &ekk, nullptr);
   out[RQ_E_KK] = ekk;
   out[RQ_E_TOTAL] = out[RQ_E_T] + out[RQ_E_EK] + out[RQ_E_EE] + out[RQ_E_KK];
+  // a normalisation since the last readout met a NaN/Inf domain norm (the kernel left that
+  // domain unscaled and set the word): report it once, then clear the word
+  int bad_norm = 0;
+  CK(cudaMemcpyAsync(&bad_norm, c->err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (bad_norm) {
+    CK(cudaMemsetAsync(c->err, 0, sizeof(int), c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return rq_fail(c, RQ_ENONFINITE, "non-finite domain norm in a normalisation");
+  }
   for (int q = 0; q < RQ_ENERGY_LEN; ++q)
     if (!std::isfinite(out[q])) return rq_fail(c, RQ_ENONFINITE, "non-finite energy component");
   return RQ_OK;
@@ -948,22 +958,34 @@ extern "C" int rq_kernel_normalize_sp(float* U, const int32_t* label, const floa
   if (!U || !label || !Zeff || n_atoms < 1 || S < 3) return RQ_EINVAL;
   Geo g = make_geo(S);
   cudaStream_t st = (cudaStream_t)stream;
+  // scratch for the per-domain sums when the caller passes none, the scale table and the error
+  // word; released on every exit, also when a step below fails
+  struct Scratch {
+    cudaStream_t st;
+    void* p[3] = {nullptr, nullptr, nullptr};
+    ~Scratch() {
+      for (void* q : p)
+        if (q) cudaFreeAsync(q, st);
+    }
+  } tmp{st};
   double* norms = norms_out;
-  float* scale = nullptr;
-  int* err = nullptr;
-  // scratch for the per-domain sums when the caller passes none, the scale table and the error word
-  if (!norms) KCHK(cudaMallocAsync((void**)&norms, sizeof(double) * n_atoms, st));
-  KCHK(cudaMallocAsync((void**)&scale, sizeof(float) * n_atoms, st));
-  KCHK(cudaMallocAsync((void**)&err, sizeof(int), st));
+  if (!norms) {
+    KCHK(cudaMallocAsync(&tmp.p[0], sizeof(double) * n_atoms, st));
+    norms = (double*)tmp.p[0];
+  }
+  KCHK(cudaMallocAsync(&tmp.p[1], sizeof(float) * n_atoms, st));
+  KCHK(cudaMallocAsync(&tmp.p[2], sizeof(int), st));
+  float* scale = (float*)tmp.p[1];
+  int* err = (int*)tmp.p[2];
   KCHK(cudaMemsetAsync(norms, 0, sizeof(double) * n_atoms, st));
   KCHK(cudaMemsetAsync(err, 0, sizeof(int), st));
   KCHK(launch_norms_flat(U, label, g, (double)h3, n_atoms, norms, st));
   KCHK(launch_norm_scale_sp(norms, Zeff, n_atoms, scale, err, st));
   KCHK(launch_apply_scale_sp(U, label, scale, g, n_atoms, st));
-  if (!norms_out) KCHK(cudaFreeAsync(norms, st));
-  KCHK(cudaFreeAsync(scale, st));
-  KCHK(cudaFreeAsync(err, st));
-  return RQ_OK;
+  int err_host = 0;
+  KCHK(cudaMemcpyAsync(&err_host, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  KCHK(cudaStreamSynchronize(st));
+  return err_host ? RQ_ENONFINITE : RQ_OK;
 }
 
 extern "C" int rq_kernel_energy_sp(const float* U, const float* K, const float* P, const int32_t* label,

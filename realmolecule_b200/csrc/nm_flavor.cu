@@ -258,36 +258,64 @@ int nm_promote(rq_ctx* c) {
   if (rc != RQ_OK) return rc;
   const long long n = c->g.S3;
   const size_t bytes = sizeof(double) * (size_t)n;
+  // Every FP64 buffer (fields and multigrid levels) is allocated before anything is freed or
+  // swapped: if one allocation fails the context is left exactly as it was (fp32, its captured
+  // graphs still valid).
   void* nb[6] = {};  // U0, U1, P0, P1, K, Kext
   void* old[6] = {c->U[0], c->U[1], c->P[0], c->P[1], c->K, c->Kext};
-  for (int q = 0; q < 6; ++q) {
-    if (!old[q]) continue;
-    if (cudaMalloc(&nb[q], bytes) != cudaSuccess) {
-      for (void* p : nb)
-        if (p) cudaFree(p);
+  std::vector<void*> lv;  // new multigrid buffers, in the order of the (L.P, L.f, L.r) walk below
+  auto undo = [&]() {
+    for (void* p : nb)
+      if (p) cudaFree(p);
+    for (void* p : lv)
+      if (p) cudaFree(p);
+  };
+  for (int q = 0; q < 6; ++q)
+    if (old[q] && cudaMalloc(&nb[q], bytes) != cudaSuccess) {
+      undo();
       return rq_cuda(c, cudaErrorMemoryAllocation, "promotion to FP64");
     }
-    if (q != 4) {  // K is recomputed below
+  for (const rq_mg_level& L : c->mg)
+    for (void* p : {L.P, L.f, L.r}) {
+      if (!p) continue;
+      void* q = nullptr;
+      if (cudaMalloc(&q, sizeof(double) * (size_t)L.g.S3) != cudaSuccess) {
+        undo();
+        return rq_cuda(c, cudaErrorMemoryAllocation, "FP64 multigrid levels");
+      }
+      lv.push_back(q);
+    }
+  for (int q = 0; q < 6; ++q)
+    if (old[q] && q != 4) {  // K is recomputed below
       k_nm_widen<<<148 * 4, 256, 0, c->st>>>((const float*)old[q], (double*)nb[q], n);
-      CK(cudaGetLastError());
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) {
+        cudaStreamSynchronize(c->st);
+        undo();
+        return rq_cuda(c, e, "promotion to FP64");
+      }
       c->launches++;
     }
+  size_t li = 0;
+  for (const rq_mg_level& L : c->mg)
+    for (void* p : {L.P, L.f, L.r})
+      if (p) cudaMemsetAsync(lv[li++], 0, sizeof(double) * (size_t)L.g.S3, c->st);
+  if (cudaStreamSynchronize(c->st) != cudaSuccess) {
+    const cudaError_t e = cudaGetLastError();
+    undo();
+    return rq_cuda(c, e, "promotion to FP64");
   }
-  CK(cudaStreamSynchronize(c->st));
+  // commit: free the fp32 buffers and swap in the FP64 ones
   for (void* p : old)
     if (p) cudaFree(p);
   c->U[0] = nb[0]; c->U[1] = nb[1]; c->P[0] = nb[2]; c->P[1] = nb[3]; c->K = nb[4]; c->Kext = nb[5];
-  for (size_t l = 0; l < c->mg.size(); ++l) {
-    rq_mg_level& L = c->mg[l];
-    const size_t lb = sizeof(double) * (size_t)L.g.S3;
-    for (void** p : {&L.P, &L.f, &L.r}) {
-      if (!*p) continue;
-      cudaFree(*p);
-      *p = nullptr;
-      if (cudaMalloc(p, lb) != cudaSuccess) return rq_cuda(c, cudaErrorMemoryAllocation, "FP64 multigrid levels");
-      CK(cudaMemsetAsync(*p, 0, lb, c->st));
-    }
-  }
+  li = 0;
+  for (rq_mg_level& L : c->mg)
+    for (void** p : {&L.P, &L.f, &L.r})
+      if (*p) {
+        cudaFree(*p);
+        *p = lv[li++];
+      }
   c->fp64 = true;
   for (auto& gx : c->graph)
     if (gx) {

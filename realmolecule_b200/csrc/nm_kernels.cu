@@ -36,14 +36,19 @@ __global__ void __launch_bounds__(256) k_nm_update(const T* U, T* Unew, const T*
   }
 }
 
-// scale[l] = sqrt(Zdom_l / n_l) (FP64) for every domain of the (concatenated) arrays
+// scale[l] = sqrt(Zdom_l / n_l) (FP64) for every domain of the (concatenated) arrays; a norm
+// that is NaN or Inf sets bit 0 of *err and leaves its domain unscaled
 template <typename T>
 __global__ void k_nm_norm_scale(const double* __restrict__ norms, const double* __restrict__ Zdom, int nDom,
                                 double* __restrict__ scale, int* __restrict__ err) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= nDom) return;
   const double n = norms[l];
-  if (!isfinite(n)) atomicOr(err, 1);
+  if (!isfinite(n)) {
+    atomicOr(err, 1);
+    scale[l] = 1.0;
+    return;
+  }
   scale[l] = (Zdom[l] > 0.0 && n > 1e-300) ? sqrt(Zdom[l] / n) : 1.0;
 }
 

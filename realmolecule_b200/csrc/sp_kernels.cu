@@ -400,13 +400,19 @@ __global__ void __launch_bounds__(256) k_norms_flat(const float* __restrict__ U,
 }
 
 // scale[l] = sqrt(Z_l / n_l) when Z_l > 0 and n_l > 1e-20 (f32 like the reference), else 1.
+// A norm that is not finite as an f32 (NaN or Inf in the FP64 sum, or a finite sum above
+// FLT_MAX) sets bit 0 of *err and leaves the domain unscaled: sqrt(z / inf) would zero it.
 __global__ void k_norm_scale_sp(const double* __restrict__ norms, const float* __restrict__ Zeff, int nDom,
                                 float* __restrict__ scale, int* __restrict__ err) {
   int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= nDom) return;
   const float z = Zeff[l];
   const float n = (float)norms[l];
-  if (!isfinite(norms[l])) atomicOr(err, 1);
+  if (!isfinite(n)) {
+    atomicOr(err, 1);
+    scale[l] = 1.0f;
+    return;
+  }
   scale[l] = (z > 0.f && n > 1e-20f) ? F_SQRT(F_DIV(z, n)) : 1.0f;
 }
 

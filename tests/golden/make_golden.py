@@ -1,8 +1,9 @@
 """Generate the golden fixtures under tests/golden/ from the reference itself.
 
-Run in a container that has the reference tree (default /root/reference):
+Run in a container that has the reference tree (--reference, else REALQM_REFERENCE_DIR, else
+/root/reference):
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py [--reference DIR]
 
 What it records (all small, committed):
 
@@ -154,7 +155,7 @@ def hairpin_fixtures(reference, cfg_path, gold_path):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("REALQM_REFERENCE_DIR", "/root/reference"))
     a = ap.parse_args()
     kernels_fixture(os.path.join(HERE, "solverpy_kernels_nn16.npz"))
     run_fixture(a.reference, os.path.join(HERE, "solverpy_run_h2o_nn32.json"))
