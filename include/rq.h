@@ -158,7 +158,9 @@ typedef struct rq_profile {
 /* Force methods for rq_forces. */
 #define RQ_FORCE_HF 0      /* Hellmann-Feynman integral: cloud/solver.py:282-315, molecule.js:1271-1330 */
 #define RQ_FORCE_GRADP 1   /* molecule.js gradPtotal (:1200-1269) */
-#define RQ_FORCE_ADJOINT 2 /* dE/dR of the converged energy (labels frozen); new flavour: Gaussian nuclei */
+#define RQ_FORCE_ADJOINT 2 /* new flavour: -dE/dR of the energy readout, by the reverse sweep through the steps
+                              recorded since the last reset (rq_set_adjoint_window); without a window the
+                              Hellmann-Feynman gather, exact at a converged state.  Other flavours: as HF */
 
 /* ---- lifecycle ---------------------------------------------------------------------- */
 /* Replaces RealQMSolver.__init__ (cloud/solver.py:321-400) and molecule.js initGPU buffer
@@ -248,6 +250,24 @@ RQ_API int rq_extract(rq_ctx* ctx, int32_t slice_k, float* out);
 RQ_API int rq_promote(rq_ctx* ctx);
 RQ_API int rq_solve(rq_ctx* ctx, double tol_dE, int32_t max_steps, int32_t check_interval, int32_t* steps_taken,
              double* E_final);
+/* Exact gradients of the new flavour's energy readout (no single reference call site: the reference
+ * forces are the Hellmann-Feynman integral cloud/solver.py:282-315 / molecule.js:1271-1330 and the
+ * Hartree-gradient ball molecule.js:1200-1269, exact only at convergence).
+ * rq_set_adjoint_window(ctx, K): from now on every rq_step records the state each step starts
+ * from, keeping the last K steps (K x S^3 psi, K / poisson_interval + 2 x S^3 P and K x n_atoms
+ * scales of device memory; 0 switches recording off).  Recorded steps run eagerly (no CUDA-graph
+ * replay).  The window forgets its steps whenever the state or the geometry changes
+ * (rq_initialize, rq_set_atoms, rq_set_external_potential, uploads, rq_promote): the state at that
+ * moment is the fixed starting point of the gradient.
+ * rq_adjoint(ctx, F, dE_dv): reverse sweep from the current readout back through the recorded steps
+ * (update, per-domain normalisation and multigrid V-cycle transposed, labels held fixed), giving
+ * F = -dE/dR of every entry (n_atoms x 3, electronic part, NULL to skip) and dE/dv for an external
+ * potential (S^3 doubles, NULL to skip).  The gradient is exact for the energy reached from the
+ * window's starting state when every step since it fits in the window; with more steps the sweep
+ * stops at the oldest kept step.  RQ_ENOTSUP if a label pass ran inside the window (set
+ * label_until).  Synchronises. */
+RQ_API int rq_set_adjoint_window(rq_ctx* ctx, int32_t steps);
+RQ_API int rq_adjoint(rq_ctx* ctx, double* F, double* dE_dv);
 RQ_API int rq_synchronize(rq_ctx* ctx);
 /* Per-kernel timing (the reference only times whole frames, molecule.js:2823, :3168,
  * and whole runs, cloud/solver.py:559-597): between begin and end every launch of the context

@@ -127,6 +127,7 @@ class _Oracle:
             "orc_nm_force": [_f64p, _f64p, _f64p, _i, _i, _d, _d, _f64p],
             "orc_nm_init": [_f64p, _i32p, _f32p, _i32p, _i, _i, _f],
             "orc_nm_evolve": [_i32p, _i32p, _f64p, _f32p, _i, _d, _d],
+            "orc_nm_evolve_f32": [_i32p, _i32p, _f32p, _f32p, _i, _f, _f],
             "orc_at_init": [_f32p, _f32p, _f32p, _f32p, C.c_void_p, _i, _i, _d, _d],
             "orc_at_step": [_f32p, _f32p, _f32p, _f32p, C.c_void_p, _i, _i, _d, _d, _i, _f64p, _f64p],
             "orc_mf_update": [C.c_void_p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p],

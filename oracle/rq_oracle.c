@@ -1212,6 +1212,48 @@ void orc_nm_evolve(const int32_t* labelIn, int32_t* labelOut, const double* U, f
       }
 }
 
+/* The same level-set rule on fp32 psi with every operation in f32 (the mixed-precision path's
+ * label pass): products, sums and the quotient each rounded to single precision, in the order of
+ * orc_nm_evolve.  dt_w and curvReg are the f32 values of the parameters. */
+void orc_nm_evolve_f32(const int32_t* labelIn, int32_t* labelOut, const float* U, float* W, int S, float dt_w,
+                       float curvReg) {
+  const int NN = S - 1;
+  const int64_t S2 = (int64_t)S * S;
+  memcpy(labelOut, labelIn, sizeof(int32_t) * (size_t)S2 * S);
+#pragma omp parallel for schedule(static)
+  for (int i = 1; i < NN; ++i)
+    for (int j = 1; j < NN; ++j)
+      for (int k = 1; k < NN; ++k) {
+        int64_t id = IDX(i, j, k, S);
+        int32_t myL = labelIn[id];
+        float uc = U[id];
+        float myRho = uc * uc;
+        const int64_t nb[6] = {id + S2, id - S2, id + S, id - S, id + 1, id - 1};
+        int32_t bestL = myL;
+        float bestRho = 0.0f, myCnt = 0.0f;
+        for (int q = 0; q < 6; ++q) {
+          int32_t l = labelIn[nb[q]];
+          if (l == myL) myCnt = myCnt + 1.0f;
+          else {
+            float un = U[nb[q]];
+            float r = un * un;
+            if (r > bestRho) { bestRho = r; bestL = l; }
+          }
+        }
+        float w = W[id];
+        if (myCnt >= 6.0f) { W[id] = w > 1.0f ? w : 1.0f; labelOut[id] = myL; continue; }
+        float denom = myRho + bestRho;
+        float vel = (denom < 1e-20f) ? 0.0f : (myRho - bestRho) / denom;
+        w = w + dt_w * vel;
+        float curv = (myCnt - 3.0f) / 3.0f;
+        w = w + curvReg * curv;
+        int32_t newL = myL;
+        if (w < 0.0f) { newL = bestL; w = 0.1f; }
+        W[id] = w;
+        labelOut[id] = newL;
+      }
+}
+
 /* ====================================================================
  * atom.js flavour: per-shell fields U[m], W[m], P[m] (atom.js:1-346).  JS numbers are f64 and
  * every Float32Array store rounds to f32; loops run in the reference's lexicographic in-place

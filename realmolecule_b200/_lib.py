@@ -122,6 +122,8 @@ SIGNATURES = {
     "rq_forces": (C.c_int, [_V, _I, _P]),
     "rq_nuclear_terms": (C.c_int, [_V, _DP, _P]),
     "rq_promote": (C.c_int, [_V]),
+    "rq_set_adjoint_window": (C.c_int, [_V, _I]),
+    "rq_adjoint": (C.c_int, [_V, _P, _P]),
     "rq_extract": (C.c_int, [_V, _I, _P]),
     "rq_solve": (C.c_int, [_V, _D, _I, _I, C.POINTER(C.c_int32), _DP]),
     "rq_synchronize": (C.c_int, [_V]),

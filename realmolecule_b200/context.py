@@ -181,6 +181,20 @@ class Context:
         self._chk(self.lib.rq_promote(self.ctx), "rq_promote")
         self.fp64 = True
 
+    def set_adjoint_window(self, steps: int):
+        """New flavour: record the state of every following step, keeping the last `steps`, so that
+        ``adjoint`` can run the reverse sweep through them (rq_set_adjoint_window; 0 = off)."""
+        self._chk(self.lib.rq_set_adjoint_window(self.ctx, int(steps)), "rq_set_adjoint_window")
+
+    def adjoint(self, forces: bool = True, potential: bool = False):
+        """Exact gradient of the energy readout through the recorded steps (rq_adjoint): returns
+        (F, dE_dv) -- F = -dE/dR per entry (n_atoms x 3, electronic part) and dE/dv on the grid
+        (S^3 doubles) -- each None unless asked for."""
+        F = np.zeros((self.n_atoms, 3), np.float64) if forces else None
+        g = np.zeros(self.S3, np.float64) if potential else None
+        self._chk(self.lib.rq_adjoint(self.ctx, _ptr(F), _ptr(g)), "rq_adjoint")
+        return F, g
+
     def solve(self, tol_dE: float, max_steps: int, check_interval: int = 100):
         taken = C.c_int32()
         e = C.c_double()

@@ -131,6 +131,7 @@ static int upload_atoms(rq_ctx* c) {
 }
 
 static void free_ctx(rq_ctx* c) {
+  nm_adj_free(c);
   for (auto e : c->evpool) cudaEventDestroy(e);
   for (auto& gx : c->graph)
     if (gx) cudaGraphExecDestroy(gx);
@@ -471,7 +472,9 @@ extern "C" int rq_step(rq_ctx* c, int32_t n) {
     // is never the last of a period, as the period is a multiple of poisson_interval)
     // (with SIC, frame 0 never corrects: the first period runs eagerly, the later ones repeat;
     // likewise a first LOBPCG frame, which starts without a search direction)
-    const bool aligned = !c->prof && !c->cfg.chebyshev && !straddle && period > 0 && c->steps_done % period == 0 && left >= period &&
+    // (steps recorded for the adjoint run eagerly: each copies its starting state into the window)
+    const bool aligned = !c->prof && !c->cfg.chebyshev && c->adj.cap == 0 && !straddle && period > 0 &&
+                         c->steps_done % period == 0 && left >= period &&
                          c->sp_jdone == 0 && !(mj_sic_interval(c) > 0 && c->frame == 0) &&
                          !(c->cfg.lobpcg && c->frame == 0);
     if (!aligned) {
@@ -639,6 +642,7 @@ extern "C" int rq_upload_state(rq_ctx* c, const float* psi, const int32_t* label
     if (mj && (rc = mj_refresh_flags(c)) != RQ_OK) return rc;  // r_c-exclusion bits of the new labels
   }
   if (psi || P) c->sp_jdone = 0;  // an early Jacobi sweep used the old psi and P: redo it
+  if (psi || P || label) nm_adj_reset(c);  // the recorded steps led to another state
   if (psi) {
     c->nm_pending = false;
     c->nm_age = 0;
@@ -680,6 +684,7 @@ extern "C" int rq_upload_state_f64(rq_ctx* c, const double* psi, const double* P
   if (!c) return RQ_EINVAL;
   if (!c->fp64) return rq_fail(c, RQ_EINVAL, "mixed-precision context: use rq_upload_state");
   const size_t n = (size_t)c->g.S3;
+  if (psi || P) nm_adj_reset(c);
   if (psi) {
     c->nm_pending = false;
     c->nm_age = 0;
@@ -875,6 +880,20 @@ extern "C" int rq_promote(rq_ctx* c) {
   const int rc = nm_promote(c);
   if (rc == RQ_OK) c->cfg.precision = RQ_PREC_FP64;
   return rc;
+}
+
+extern "C" int rq_set_adjoint_window(rq_ctx* c, int32_t steps) {
+  if (!c) return RQ_EINVAL;
+  if (c->cfg.flavor != RQ_FLAVOR_NEW) return rq_fail(c, RQ_ENOTSUP, "the adjoint is the new flavour's");
+  if (steps < 0) return rq_fail(c, RQ_EINVAL, "negative adjoint window");
+  CK(cudaStreamSynchronize(c->st));
+  return nm_adj_set_window(c, steps);
+}
+
+extern "C" int rq_adjoint(rq_ctx* c, double* F, double* dE_dv) {
+  if (!c) return RQ_EINVAL;
+  if (c->cfg.flavor != RQ_FLAVOR_NEW) return rq_fail(c, RQ_ENOTSUP, "the adjoint is the new flavour's");
+  return nm_adjoint(c, F, dE_dv);
 }
 
 extern "C" int rq_solve(rq_ctx* c, double tol_dE, int32_t max_steps, int32_t check_interval, int32_t* steps_taken,

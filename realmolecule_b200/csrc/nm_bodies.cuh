@@ -438,11 +438,15 @@ __device__ __forceinline__ void nm_evolve_body(const int* __restrict__ labIn, in
 }
 
 // Gaussian-nucleus force: tiles t = t0, t0+stride, ... of interior points staged in smem (in
-// the field type), thread = nucleus a of chunk `chunk`; F_a = -h^3 sum rho dK/dr (x-R)/r.
+// the field type), thread = nucleus a of chunk `chunk`.  With gw == nullptr the Hellmann-Feynman
+// gather F_a = -h^3 sum rho dK/dr (x-R)/r; with a weight field gw = dE/dK (one value per grid
+// point) the gradient gather F_a = -dE/dR_a = sum gw dK_a/dr (x-R)/r, of which the first is the
+// case gw = -h^3 rho.
 template <typename T>
 __device__ __forceinline__ void nm_force_body(const T* __restrict__ U, const double* __restrict__ at, int nAt,
                                               const Geo& g, double h, double sigma, double* __restrict__ F,
-                                              long long t0, long long tstride, int chunk, T* sx, T* sy, T* sz, T* sr) {
+                                              long long t0, long long tstride, int chunk, T* sx, T* sy, T* sz, T* sr,
+                                              const double* __restrict__ gw = nullptr) {
   const int a = chunk * blockDim.x + threadIdx.x;
   const bool valid = a < nAt && at[a * 4 + 3] > 0.0;
   const double Z = valid ? at[a * 4 + 3] : 0.0;
@@ -456,32 +460,38 @@ __device__ __forceinline__ void nm_force_body(const T* __restrict__ U, const dou
     __syncthreads();
     for (int q = threadIdx.x; q < kNmForceTile; q += blockDim.x) {
       const long long v = t * kNmForceTile + q;
-      T rho = T(0), x = T(0), y = T(0), z = T(0);
+      T wt = T(0), x = T(0), y = T(0), z = T(0);
       if (v < nInt) {
         const int i = 1 + (int)(v / (n1 * n1)), j = 1 + (int)((v / n1) % n1), k = 1 + (int)(v % n1);
-        const double u = (double)U[(long long)i * g.S2 + (long long)j * g.S + k];
-        rho = (T)(u * u);
+        const long long id = (long long)i * g.S2 + (long long)j * g.S + k;
+        if (gw) {
+          wt = (T)gw[id];
+        } else {
+          const double u = (double)U[id];
+          wt = (T)(u * u);
+        }
         x = (T)(i * h); y = (T)(j * h); z = (T)(k * h);
       }
-      sx[q] = x; sy[q] = y; sz[q] = z; sr[q] = rho;
+      sx[q] = x; sy[q] = y; sz[q] = z; sr[q] = wt;
     }
     __syncthreads();
     if (valid) {
+      const double wscale = gw ? 1.0 : -h3;  // HF: the staged value is rho, its weight -h^3 rho
       double lx = 0, ly = 0, lz = 0;
       for (int q = 0; q < kNmForceTile; ++q) {
-        const double rho = sr[q];
-        if (rho == 0.0) continue;
+        const double s = sr[q];
+        if (s == 0.0) continue;
         const double dx = (double)sx[q] - ax, dy = (double)sy[q] - ay, dz = (double)sz[q] - az;
         const double r2 = dx * dx + dy * dy + dz * dz;
         if (r2 < 1e-24) continue;
         double w;
-        if (r2 * inv * inv >= 36.0) {  // Coulomb tail: -h3 rho dK/dr / r = h3 rho Z / r^3
+        if (r2 * inv * inv >= 36.0) {  // Coulomb tail: dK/dr / r = -Z / r^3
           const double ir = rsqrt(r2);
-          w = h3 * rho * Z * (ir * ir * ir);
+          w = -wscale * s * Z * (ir * ir * ir);
         } else {
           const double r = sqrt(r2);
           const double dKdr = Z * (gs * exp(-r2 * inv * inv) / r - erf(r * inv) / r2);
-          w = -h3 * rho * dKdr / r;
+          w = wscale * s * dKdr / r;
         }
         lx += w * dx; ly += w * dy; lz += w * dz;
       }

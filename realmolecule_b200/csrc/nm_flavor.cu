@@ -156,6 +156,7 @@ static int nm_step_t(rq_ctx* c, int s) {
   // and always after the update that precedes a V-cycle or ends with a label pass.
   const bool label_step = s % f.label_interval == 0 && (f.label_until <= 0 || s <= f.label_until);
   const bool norm = (s + 1) % f.norm_interval == 0 || (s + 1) % f.poisson_interval == 0 || label_step;
+  if (c->adj.cap > 0 && (rc = nm_adj_record_step(c, s % f.poisson_interval == 0, norm)) != RQ_OK) return rc;
   if (norm) CK(cudaMemsetAsync(c->dnorm, 0, sizeof(double) * c->n_atoms, c->st));
   LAUNCH(RQ_KC_UPDATE, (4.0 * sizeof(T) + 4.0) * interior(c->g),
          nm_update<T>((const T*)c->U[c->cu], (T*)c->U[1 - c->cu], (const T*)c->K, (const T*)c->P[c->cp], c->lab[c->cl],
@@ -167,6 +168,7 @@ static int nm_step_t(rq_ctx* c, int s) {
     LAUNCH(RQ_KC_NORMALIZE, 12.0 * c->n_atoms,
            nm_norm_scale<T>(c->dnorm, c->Zdom64, c->n_atoms, (double*)c->scale64, c->err, c->st));
     c->nm_pending = true;
+    if (c->adj.cap > 0 && (rc = nm_adj_record_scale(c)) != RQ_OK) return rc;
   }
   c->nm_age = norm ? 0 : c->nm_age + 1;
   if (label_step) {
@@ -175,6 +177,7 @@ static int nm_step_t(rq_ctx* c, int s) {
            nm_evolve<T>(c->lab[c->cl], c->lab[1 - c->cl], (const T*)c->U[c->cu], c->W, c->g, f.boundary_speed, f.curv_reg,
                         c->st));
     c->cl ^= 1;
+    if (c->adj.cap > 0) nm_adj_record_label(c);
   }
   return RQ_OK;
 }
@@ -208,7 +211,10 @@ int nm_set_external(rq_ctx* c, const double* v) {
   return nm_set_atoms(c);  // K = K_nuclei (+ v)
 }
 
-int nm_set_atoms(rq_ctx* c) { return c->fp64 ? nm_potential_t<double>(c) : nm_potential_t<float>(c); }
+int nm_set_atoms(rq_ctx* c) {
+  nm_adj_reset(c);  // the recorded steps ran with the old K
+  return c->fp64 ? nm_potential_t<double>(c) : nm_potential_t<float>(c);
+}
 
 template <typename T>
 static int nm_init_t(rq_ctx* c) {
@@ -240,7 +246,10 @@ static int nm_init_t(rq_ctx* c) {
   return RQ_OK;
 }
 
-int nm_initialize(rq_ctx* c) { return c->fp64 ? nm_init_t<double>(c) : nm_init_t<float>(c); }
+int nm_initialize(rq_ctx* c) {
+  nm_adj_reset(c);
+  return c->fp64 ? nm_init_t<double>(c) : nm_init_t<float>(c);
+}
 
 __global__ void __launch_bounds__(256) k_nm_widen(const float* __restrict__ a, double* __restrict__ d, long long n) {
   for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
@@ -323,6 +332,7 @@ int nm_promote(rq_ctx* c) {
       gx = nullptr;
     }
   if ((rc = nm_potential_t<double>(c)) != RQ_OK) return rc;
+  if (c->adj.cap > 0 && (rc = nm_adj_set_window(c, c->adj.cap)) != RQ_OK) return rc;  // FP64 window buffers
   return cudaStreamSynchronize(c->st) == cudaSuccess ? RQ_OK : rq_cuda(c, cudaGetLastError(), "promotion to FP64");
 }
 
@@ -383,6 +393,8 @@ int nm_energy(rq_ctx* c, double* out, double* per_domain) {
 
 int nm_forces(rq_ctx* c, int method, double* F) {
   if (method != RQ_FORCE_HF && method != RQ_FORCE_ADJOINT) return RQ_ENOTSUP;
+  // the adjoint through the recorded window; with no window it is the Hellmann-Feynman gather
+  if (method == RQ_FORCE_ADJOINT && c->adj.cap > 0) return nm_adjoint(c, F, nullptr);
   const int n = c->n_atoms;
   int frc = nm_ready(c);
   if (frc != RQ_OK) return frc;

@@ -113,9 +113,9 @@ __global__ void __launch_bounds__(256) k_nm_evolve(const int* labIn, int* labOut
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_nm_force(const T* U, const double* at, int nAt, Geo g, double h, double sigma,
-                                                  double* F) {
+                                                  double* F, const double* gw) {
   __shared__ T sx[kNmForceTile], sy[kNmForceTile], sz[kNmForceTile], sr[kNmForceTile];
-  nm_force_body<T>(U, at, nAt, g, h, sigma, F, blockIdx.x, gridDim.x, blockIdx.y, sx, sy, sz, sr);
+  nm_force_body<T>(U, at, nAt, g, h, sigma, F, blockIdx.x, gridDim.x, blockIdx.y, sx, sy, sz, sr, gw);
 }
 
 template <typename T>
@@ -232,7 +232,7 @@ cudaError_t nm_evolve(const int* labIn, int* labOut, const T* U, float* W, const
 }
 template <typename T>
 cudaError_t nm_force(const T* U, const double* at, int nAt, const Geo& g, double h, double sigma, double* F,
-                     cudaStream_t st) {
+                     cudaStream_t st, const double* gw) {
   if (g.NN < 2 || nAt <= 0) return cudaSuccess;
   const long long n1 = g.NN - 1, nInt = n1 * n1 * n1;
   const long long ntiles = (nInt + kNmForceTile - 1) / kNmForceTile;
@@ -240,7 +240,7 @@ cudaError_t nm_force(const T* U, const double* at, int nAt, const Geo& g, double
   long long bx = 148 * 8 / chunks;
   if (bx < 1) bx = 1;
   if (bx > ntiles) bx = ntiles;
-  k_nm_force<T><<<dim3((unsigned)bx, (unsigned)chunks), 256, 0, st>>>(U, at, nAt, g, h, sigma, F);
+  k_nm_force<T><<<dim3((unsigned)bx, (unsigned)chunks), 256, 0, st>>>(U, at, nAt, g, h, sigma, F, gw);
   return cudaGetLastError();
 }
 template <typename T>
@@ -268,7 +268,8 @@ cudaError_t nm_add(T* K, const T* v, long long n, cudaStream_t st) {
   template cudaError_t nm_energy<T>(const T*, const T*, const T*, const int*, const Geo&, double, int, double*,     \
                                     cudaStream_t);                                                                   \
   template cudaError_t nm_evolve<T>(const int*, int*, const T*, float*, const Geo&, double, double, cudaStream_t);  \
-  template cudaError_t nm_force<T>(const T*, const double*, int, const Geo&, double, double, double*, cudaStream_t);
+  template cudaError_t nm_force<T>(const T*, const double*, int, const Geo&, double, double, double*, cudaStream_t,  \
+                                   const double*);
 RQ_NM_INSTANTIATE(float)
 RQ_NM_INSTANTIATE(double)
 

@@ -18,8 +18,36 @@ struct rq_mg_level {  // one level of the new flavour's multigrid hierarchy
   void* r = nullptr;  // residual (T)
 };
 
+// Recording window of the new flavour's adjoint: the state each recorded step started from, so
+// the reverse sweep can run back through the last `cap` steps (nm_adjoint.cu).
+struct rq_adj {
+  int cap = 0;                   // window length in steps (0: recording off)
+  int np = 0;                    // P snapshot slots
+  void* psi = nullptr;           // cap x S^3 (T): normalised psi each recorded step started from
+  void* psum = nullptr;          // np x S^3 (T): P in effect (after each V-cycle; at the window start)
+  double* scales = nullptr;      // cap x n_atoms: the per-domain scale of each normalising step
+  struct Rec {
+    int psi_slot, p_slot;
+    bool vcycle, norm, label;    // V-cycle before the update, normalisation after it, label pass after it
+  };
+  std::vector<Rec> rec;          // recorded steps, oldest first (at most cap)
+  long long next_psi = 0;        // ring positions
+  int next_p = 0, cur_p = -1;
+  // reverse-sweep buffers (allocated with the window)
+  void* lam[2] = {nullptr, nullptr};  // adjoint of psi (T, S^3)
+  void* muP[2] = {nullptr, nullptr};  // adjoint of the fine P (T, S^3; ping-pong through smoothing)
+  void* muf = nullptr;                // adjoint of the fine right-hand side (T, S^3)
+  double* gK = nullptr;               // dE/dK accumulated (S^3 doubles); dE/dv for the external potential
+  struct Level { void* mu[2] = {nullptr, nullptr}; void* muf = nullptr; void* mur = nullptr; };
+  std::vector<Level> lv;              // per multigrid level (level 0: only mur is used)
+  double* dots = nullptr;             // per-domain <psi, lambda>
+  double* coef = nullptr;             // per-domain (scale, beta) of a transposed normalisation
+  double* wq = nullptr;               // per-domain (Z/N, Q/N) of the energy readout
+};
+
 struct rq_ctx {
   rq_config cfg{};
+  rq_adj adj;
   rq::Geo g{};
   double h = 0, h2 = 0, h3 = 0, dv = 0, dt = 0, half_dv = 0, sigma = 0;
   int n_atoms = 0;

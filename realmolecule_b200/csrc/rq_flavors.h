@@ -38,4 +38,12 @@ bool mj_direct(const rq_ctx* c);      // molecule.js flavour on the direct per-e
 int mj_sic_interval(const rq_ctx* c);  // frames between SIC passes of the molecule.js flavour (0: off)
 int nm_flush(rq_ctx* c);  // materialise a pending per-domain normalisation of psi
 int nm_ready(rq_ctx* c);  // nm_flush, or normalise now when updates ran since the last normalisation
+// adjoint of the new flavour (nm_adjoint.cu)
+int nm_adj_set_window(rq_ctx* c, int steps);  // allocate / free the recording window (0: off)
+void nm_adj_reset(rq_ctx* c);                 // forget the recorded steps (state or geometry changed)
+int nm_adj_record_step(rq_ctx* c, bool vcycle, bool norm);  // before the update of a step
+int nm_adj_record_scale(rq_ctx* c);           // after the normalisation scale of that step
+void nm_adj_record_label(rq_ctx* c);          // a label pass followed the step
+int nm_adjoint(rq_ctx* c, double* F, double* dEdv);
+void nm_adj_free(rq_ctx* c);
 void nm_nuclear_terms(rq_ctx* c, double* E, double* F);

@@ -150,9 +150,10 @@ cudaError_t nm_evolve(const int* labIn, int* labOut, const T* U, float* W, const
                       cudaStream_t st);
 template <typename T>
 cudaError_t nm_add(T* K, const T* v, long long n, cudaStream_t st);
+// HF gather (gw null) or the gradient gather with the weight field gw = dE/dK (S^3 doubles)
 template <typename T>
 cudaError_t nm_force(const T* U, const double* at, int nAt, const Geo& g, double h, double sigma, double* F,
-                     cudaStream_t st);
+                     cudaStream_t st, const double* gw = nullptr);
 cudaError_t launch_unpack_labels(const int* in, int* out, long long n, cudaStream_t st);
 
 }  // namespace rq
