@@ -500,8 +500,7 @@ int adjoint_t(rq_ctx* c, double* F, double* dEdv) {
     if (r.label)
       return rq_fail(c, RQ_ENOTSUP,
                      "a label pass ran inside the recorded window: the adjoint holds the labels fixed (set label_until)");
-  const bool renorm = c->nm_age > 0;  // the readout normalises the state once more
-  int rc = nm_ready(c);
+  int rc = nm_ready(c);  // a normalisation it performs is recorded as the last step's
   if (rc != RQ_OK) return rc;
   const T* psi = (const T*)c->U[c->cu];
   const T* K = (const T*)c->K;
@@ -526,7 +525,6 @@ int adjoint_t(rq_ctx* c, double* F, double* dEdv) {
          (k_adj_seed<T><<<nblk(ni), 256, 0, c->st>>>(psi, K, (const T*)c->P[c->cp], lab, g, c->h, n, A.wq, lam[li],
                                                      muP[mi], A.gK),
           cudaGetLastError()));
-  if (renorm && !A.rec.empty() && (rc = adj_norm<T>(c, psi, lam[li], (const double*)c->scale64)) != RQ_OK) return rc;
   for (int r = (int)A.rec.size() - 1; r >= 0; --r) {
     const rq_adj::Rec& R = A.rec[r];
     const T* psi_prev = slot<T>(A.psi, R.psi_slot, S3);

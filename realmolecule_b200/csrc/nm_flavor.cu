@@ -135,8 +135,14 @@ int nm_flush(rq_ctx* c) { return c->fp64 ? nm_flush_t<double>(c) : nm_flush_t<fl
 template <typename T>
 static int nm_ready_t(rq_ctx* c) {
   if (c->nm_age == 0) return nm_flush_t<T>(c);
-  const int rc = nm_normalize_t<T>(c, true);
+  int rc = nm_normalize_t<T>(c, true);
   c->nm_age = 0;
+  // a readout that normalises changes the state the energy is read from: while steps are
+  // recorded it becomes the normalisation of the last recorded step, for the reverse sweep
+  if (rc == RQ_OK && c->adj.cap > 0 && !c->adj.rec.empty() && !c->adj.rec.back().norm) {
+    c->adj.rec.back().norm = true;
+    rc = nm_adj_record_scale(c);
+  }
   return rc;
 }
 
