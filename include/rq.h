@@ -211,9 +211,10 @@ typedef struct rq_split {
   double rot;
 } rq_split;
 RQ_API int rq_set_splits(rq_ctx* ctx, const rq_split* splits);
-/* External potential v (host array of S^3 doubles, Ha) added to the nuclear potential K of the
- * new flavour: the update uses K + v and E_eK = -h^3 sum (K + v) rho.  NULL removes it.  No
- * reference counterpart: the handle through which dE/dv = -h^3 rho is exposed to autograd. */
+/* External potential v (S^3 doubles, Ha, in host memory or in this GPU's device memory) added to
+ * the nuclear potential K of the new flavour: the update uses K + v and E_eK = -h^3 sum (K + v) rho.
+ * NULL removes it.  No reference counterpart: the handle through which dE/dv (rq_adjoint) is
+ * exposed to autograd. */
 RQ_API int rq_set_external_potential(rq_ctx* ctx, const double* v);
 /* Copy a full state in / out (host arrays of S^3 elements; any pointer may be NULL to skip).
  * Labels must lie in [0, n_atoms).  Replaces window.restartWithPositions re-uploads
@@ -261,8 +262,8 @@ RQ_API int rq_solve(rq_ctx* ctx, double tol_dE, int32_t max_steps, int32_t check
  * moment is the fixed starting point of the gradient.
  * rq_adjoint(ctx, F, dE_dv): reverse sweep from the current readout back through the recorded steps
  * (update, per-domain normalisation and multigrid V-cycle transposed, labels held fixed), giving
- * F = -dE/dR of every entry (n_atoms x 3, electronic part, NULL to skip) and dE/dv for an external
- * potential (S^3 doubles, NULL to skip).  The gradient is exact for the energy reached from the
+ * F = -dE/dR of every entry (n_atoms x 3 in host memory, electronic part, NULL to skip) and dE/dv
+ * for an external potential (S^3 doubles in host or device memory, NULL to skip).  The gradient is exact for the energy reached from the
  * window's starting state when every step since it fits in the window; with more steps the sweep
  * stops at the oldest kept step.  RQ_ENOTSUP if a label pass ran inside the window (set
  * label_until).  Synchronises. */

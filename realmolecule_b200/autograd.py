@@ -1,18 +1,22 @@
-"""Differentiable converged energy of the new flavour, for PyTorch.
+"""Differentiable energy of the new flavour, for PyTorch.
 
 ``EnergyModel`` owns one new-flavour context (Gaussian nuclei, multigrid Hartree, FP64 domain
-sums) and evaluates the converged energy E(R, v) for nuclear positions R (bohr, box frame:
-x = i*h) and an optional external potential v on the grid.  ``RealQMEnergy`` wraps it as a
-``torch.autograd.Function``:
+sums) and evaluates the energy E(R, v) for nuclear positions R (bohr, box frame: x = i*h) and an
+optional external potential v on the grid.  Every evaluation warm-starts from the previous
+state (labels frozen after the first ``label_until`` steps) and either
 
-* dE/dR  = -(F_electronic + F_nuclear), with F_electronic the gradient kernel of librq
-  (``rq_forces(RQ_FORCE_ADJOINT)``).  At a converged state with the domain labels held fixed the
-  electronic energy is stationary in psi under the per-domain norm constraints, so the adjoint
-  of the psi equations vanishes and this is the exact derivative of the discrete energy
-  (checked against central finite differences in the tests);
-* dE/dv  = -h^3 rho  (v enters as K + v, E_eK = -h^3 sum (K + v) rho).
+* solves to a tolerance (``tol`` given): E is the converged energy; or
+* runs exactly ``warm_steps`` imaginary-time steps (``tol=None``, the geometry workloads): E is
+  the energy those steps reach.
 
-Every evaluation warm-starts from the previous state: labels are frozen after the first solve.
+Its gradients come from librq's adjoint (``rq_adjoint``): the steps of each evaluation are
+recorded (``rq_set_adjoint_window``) and a reverse sweep through them -- the update, the
+per-domain normalisation and the multigrid V-cycle transposed -- gives the exact dE/dR and
+dE/dv of the energy actually reached, converged or not.  For a solve to a tolerance the
+recorded window is empty and the gradient is the Hellmann-Feynman one, exact at convergence.
+
+``RealQMEnergy`` wraps an EnergyModel as a ``torch.autograd.Function``.  An external potential
+given as a float64 CUDA tensor is read on the device and its gradient written on the device.
 """
 from __future__ import annotations
 
@@ -28,12 +32,13 @@ from .context import Context
 class EnergyModel:
     def __init__(self, NN: int, h: float, charges: Sequence[float], positions: np.ndarray,
                  seeds: np.ndarray, precision: str = "fp64", tol: Optional[float] = 1e-10, max_steps: int = 50000,
-                 check_interval: int = 100, warm_steps: int = 0, want_rho: bool = True, **opts):
+                 check_interval: int = 100, warm_steps: int = 0, adjoint: bool = True, **opts):
         """tol None: each evaluation runs exactly ``warm_steps`` imaginary-time steps from the previous
-        state (the fixed warm-started iterations of the geometry workloads) instead of a solve.
-        want_rho False: evaluate returns None for h^3 rho (no density download)."""
+        state (the fixed warm-started iterations of the geometry workloads) instead of a solve, and
+        those steps are recorded for the adjoint.  adjoint False: no recording; the gradient is the
+        Hellmann-Feynman one (exact only at convergence), for comparison."""
         self.NN, self.h = int(NN), float(h)
-        self.want_rho = want_rho
+        self.S3 = (self.NN + 1) ** 3
         self.charges = np.asarray(charges, np.float64)
         self.n_nuc = len(self.charges)
         self.seeds = np.asarray(seeds, np.float64)
@@ -44,7 +49,9 @@ class EnergyModel:
         self.ctx = Context(self.NN, self.NN * self.h, rows, flavor="new", precision=precision, **opts)
         self.ctx.initialize()
         self.ctx.step(opts["label_until"])  # let the level set settle, then labels stay fixed
-        self._v = None
+        if adjoint and tol is None and warm_steps > 0:
+            self.ctx.set_adjoint_window(warm_steps)
+        self._has_v = False
         self.last = None
 
     def _rows(self, pos: np.ndarray):
@@ -54,41 +61,40 @@ class EnergyModel:
                  for s in self.seeds]
         return rows
 
-    def evaluate(self, positions: np.ndarray, v: Optional[np.ndarray] = None):
-        """Converged energy, total forces on the nuclei (n_nuc x 3) and h^3 rho for positions R
-        (h^3 rho is None when the model was built with want_rho=False and no v is given)."""
+    def evaluate(self, positions: np.ndarray, v=None, dE_dv=None):
+        """Energy and total forces on the nuclei (n_nuc x 3) for positions R and external potential v
+        (S^3 values: numpy array or float64 torch tensor, None for none).  With dE_dv (True, or a
+        float64 tensor of S^3 values to fill) also returns dE/dv, else None."""
         positions = np.asarray(positions, np.float64).reshape(self.n_nuc, 3)
         self.ctx.set_atoms(self._rows(positions))
-        if v is not None or self._v is not None:
+        if v is not None or self._has_v:
             self.ctx.set_external_potential(v)
-            self._v = v
-        if self.warm_steps:
-            self.ctx.step(self.warm_steps)
+            self._has_v = v is not None
         if self.tol is None:
+            self.ctx.step(self.warm_steps)
             steps, E = self.warm_steps, float(self.ctx.energy()[L.E_TOTAL])
         else:
             steps, E = self.ctx.solve(self.tol, self.max_steps, self.check)
-        Fe = self.ctx.forces(L.FORCE_ADJOINT)[: self.n_nuc]
+        Fe, g = self.ctx.adjoint(forces=True, potential=dE_dv if dE_dv is not None else False)
         _, Fn = self.ctx.nuclear_terms()
-        F = Fe + Fn[: self.n_nuc]
-        rho_h3 = None
-        if self.want_rho or v is not None:  # dE/dv = -h^3 rho needs the density whenever v is given
-            psi = self.ctx.download(psi=True, label=False)["psi"].astype(np.float64)
-            rho_h3 = psi * psi * self.h ** 3
+        F = Fe[: self.n_nuc] + Fn[: self.n_nuc]
         self.last = {"E": E, "F": F, "steps": steps}
-        return E, F, rho_h3
+        return E, F, g
 
 
 class RealQMEnergy(torch.autograd.Function):
     """E = RealQMEnergy.apply(positions, v_ext, model): positions (n_nuc, 3) float64 bohr,
-    v_ext (S^3,) float64 or an empty tensor for none."""
+    v_ext (S^3,) float64 (host or CUDA) or an empty tensor for none."""
 
     @staticmethod
     def forward(ctx, positions, v_ext, model: EnergyModel):
-        v = v_ext.detach().cpu().numpy() if v_ext.numel() else None
-        E, F, rho_h3 = model.evaluate(positions.detach().cpu().numpy(), v)
-        ctx.save_for_backward(torch.from_numpy(-F).to(positions.device),
-                              torch.from_numpy(-rho_h3).to(v_ext.device) if v_ext.numel() else v_ext.new_zeros(0))
+        has_v = v_ext.numel() > 0
+        v = v_ext.detach().contiguous() if has_v else None
+        dv = torch.empty(model.S3, dtype=torch.float64, device=v_ext.device) if has_v else None
+        if has_v and v.is_cuda:
+            torch.cuda.synchronize(v.device)  # librq reads v on its own stream
+        E, F, _ = model.evaluate(positions.detach().cpu().numpy(), v, dE_dv=dv)
+        ctx.save_for_backward(torch.from_numpy(-F).to(positions.device), dv if has_v else v_ext.new_zeros(0))
         return torch.tensor(E, dtype=torch.float64, device=positions.device)
 
     @staticmethod

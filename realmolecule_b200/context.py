@@ -165,7 +165,12 @@ class Context:
         self._chk(self.lib.rq_set_splits(self.ctx, arr), "rq_set_splits")
 
     def set_external_potential(self, v):
-        """Add an external potential v (S^3 values, Ha) to K (new flavour); None removes it."""
+        """Add an external potential v (S^3 values, Ha) to K (new flavour); None removes it.  A
+        contiguous float64 torch tensor on this GPU is read in place (no host round trip)."""
+        if v is not None and hasattr(v, "data_ptr"):
+            assert v.dtype.itemsize == 8 and v.is_contiguous() and v.numel() == self.S3
+            self._chk(self.lib.rq_set_external_potential(self.ctx, v.data_ptr()), "rq_set_external_potential")
+            return
         arr = None if v is None else np.ascontiguousarray(np.asarray(v, np.float64).reshape(-1))
         self._chk(self.lib.rq_set_external_potential(self.ctx, _ptr(arr)), "rq_set_external_potential")
 
@@ -186,13 +191,19 @@ class Context:
         ``adjoint`` can run the reverse sweep through them (rq_set_adjoint_window; 0 = off)."""
         self._chk(self.lib.rq_set_adjoint_window(self.ctx, int(steps)), "rq_set_adjoint_window")
 
-    def adjoint(self, forces: bool = True, potential: bool = False):
+    def adjoint(self, forces: bool = True, potential=False):
         """Exact gradient of the energy readout through the recorded steps (rq_adjoint): returns
         (F, dE_dv) -- F = -dE/dR per entry (n_atoms x 3, electronic part) and dE/dv on the grid
-        (S^3 doubles) -- each None unless asked for."""
+        (S^3 doubles) -- each None unless asked for.  `potential` may be a contiguous float64 torch
+        tensor of S^3 values (on this GPU or the host), which is filled in place and returned."""
         F = np.zeros((self.n_atoms, 3), np.float64) if forces else None
-        g = np.zeros(self.S3, np.float64) if potential else None
-        self._chk(self.lib.rq_adjoint(self.ctx, _ptr(F), _ptr(g)), "rq_adjoint")
+        if hasattr(potential, "data_ptr"):
+            assert potential.dtype.itemsize == 8 and potential.is_contiguous() and potential.numel() == self.S3
+            g, gp = potential, potential.data_ptr()
+        else:
+            g = np.zeros(self.S3, np.float64) if potential else None
+            gp = _ptr(g)
+        self._chk(self.lib.rq_adjoint(self.ctx, _ptr(F), gp), "rq_adjoint")
         return F, g
 
     def solve(self, tol_dE: float, max_steps: int, check_interval: int = 100):

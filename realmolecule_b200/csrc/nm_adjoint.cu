@@ -550,7 +550,7 @@ int adjoint_t(rq_ctx* c, double* F, double* dEdv) {
     LAUNCH(RQ_KC_FORCES, 8.0 * ni, nm_force<T>(psi, c->atoms_nm, n, g, c->h, c->sigma, c->dF, c->st, A.gK));
     CK(cudaMemcpyAsync(F, c->dF, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->st));
   }
-  if (dEdv) CK(cudaMemcpyAsync(dEdv, A.gK, sizeof(double) * S3, cudaMemcpyDeviceToHost, c->st));
+  if (dEdv) CK(cudaMemcpyAsync(dEdv, A.gK, sizeof(double) * S3, cudaMemcpyDefault, c->st));  // host or device
   CK(cudaStreamSynchronize(c->st));
   return RQ_OK;
 }
@@ -559,8 +559,9 @@ int adjoint_t(rq_ctx* c, double* F, double* dEdv) {
 
 int nm_adjoint(rq_ctx* c, double* F, double* dEdv) {
   if (c->adj.cap > 0) return c->fp64 ? adjoint_t<double>(c, F, dEdv) : adjoint_t<float>(c, F, dEdv);
-  // no recording window: the gradient of the readout alone (the Hellmann-Feynman terms), with the
-  // reverse-sweep buffers held only for this call
+  // no recording window: the gradient of the readout alone (the Hellmann-Feynman terms); the
+  // forces alone are the HF gather, dE/dv needs the reverse-sweep buffers for this call
+  if (!dEdv) return F ? nm_forces(c, RQ_FORCE_HF, F) : RQ_OK;
   int rc = nm_adj_set_window(c, 1);
   if (rc == RQ_OK) rc = c->fp64 ? adjoint_t<double>(c, F, dEdv) : adjoint_t<float>(c, F, dEdv);
   nm_adj_free(c);

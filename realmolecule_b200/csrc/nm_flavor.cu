@@ -198,6 +198,13 @@ static int nm_potential_t(rq_ctx* c) {
   return RQ_OK;
 }
 
+__global__ void __launch_bounds__(256) k_nm_narrow(const double* __restrict__ d, float* __restrict__ a, long long n) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    a[q] = (float)d[q];
+}
+
+// v: S^3 doubles in host memory or in device memory of this GPU (a device pointer stays on the
+// device: no round trip through the host)
 int nm_set_external(rq_ctx* c, const double* v) {
   const size_t n = (size_t)c->g.S3;
   if (!v) {
@@ -205,8 +212,16 @@ int nm_set_external(rq_ctx* c, const double* v) {
   } else {
     if (!c->Kext && cudaMalloc(&c->Kext, n * esize(c)) != cudaSuccess)
       return rq_cuda(c, cudaErrorMemoryAllocation, "external potential");
+    cudaPointerAttributes pa{};
+    const bool on_device = cudaPointerGetAttributes(&pa, v) == cudaSuccess &&
+                           (pa.type == cudaMemoryTypeDevice || pa.type == cudaMemoryTypeManaged);
+    cudaGetLastError();  // a plain host pointer may leave an error behind on older drivers
     if (c->fp64) {
-      CK(cudaMemcpyAsync(c->Kext, v, n * sizeof(double), cudaMemcpyHostToDevice, c->st));
+      CK(cudaMemcpyAsync(c->Kext, v, n * sizeof(double), cudaMemcpyDefault, c->st));
+    } else if (on_device) {
+      k_nm_narrow<<<148 * 8, 256, 0, c->st>>>(v, (float*)c->Kext, (long long)n);
+      CK(cudaGetLastError());
+      c->launches++;
     } else {
       std::vector<float> f(n);
       for (size_t q = 0; q < n; ++q) f[q] = (float)v[q];

@@ -87,13 +87,15 @@ def velocity_verlet(model, x0, v0, masses, dt: float, n_steps: int) -> Trajector
     return traj
 
 
-def geometry_model(g, precision: str = "mixed", iters: int = 200, label_until: int = 400):
+def geometry_model(g, precision: str = "mixed", iters: int = 200, label_until: int = 400, adjoint: bool = True):
     """An EnergyModel for a configs.Geometry in the workloads' mode: each evaluation runs `iters`
-    warm-started imaginary-time steps (no solve to a tolerance, no density download)."""
+    warm-started imaginary-time steps (no solve to a tolerance) and its forces are the exact
+    gradient of the energy those steps reach (the adjoint through them; adjoint False: the
+    Hellmann-Feynman force of the state reached)."""
     from .autograd import EnergyModel
     off = (g.NN // 2) * g.h  # geometries are centred on the centroid; the model uses the box frame
     return EnergyModel(g.NN, g.h, g.charges, g.xyz + off, g.seeds + off, precision=precision, tol=None,
-                       warm_steps=iters, want_rho=False, label_until=label_until), g.charges, off
+                       warm_steps=iters, label_until=label_until, adjoint=adjoint), g.charges, off
 
 
 def _main(argv=None):
@@ -115,13 +117,15 @@ def _main(argv=None):
     ap.add_argument("--iters", type=int, default=None)
     ap.add_argument("--dt-fs", type=float, default=0.5)
     ap.add_argument("--precision", default="mixed")
+    ap.add_argument("--forces", default="adjoint", choices=["adjoint", "hf"],
+                    help="adjoint: exact gradient of the energy reached; hf: Hellmann-Feynman of the state")
     ap.add_argument("--preconverge", type=int, default=None,
                     help="imaginary-time steps before the first geometry step (default 2000 / 3000)")
     a = ap.parse_args(argv)
     g = configs.water100() if a.workload == "water100" else configs.water1000()
     iters = a.iters or (200 if a.workload == "water100" else 50)
     t0 = time.perf_counter()
-    model, Z, off = geometry_model(g, a.precision, iters)
+    model, Z, off = geometry_model(g, a.precision, iters, adjoint=a.forces == "adjoint")
     pre = a.preconverge if a.preconverge is not None else (2000 if a.workload == "water100" else 3000)
     model.ctx.step(pre)  # converge the electrons at the start geometry
     model.ctx.synchronize()
@@ -145,7 +149,8 @@ def _main(argv=None):
                "drift_Ha": float(Et[-1] - Et[0]), "max_excursion_Ha": float(np.abs(Et - Et[0]).max())}
     dt = time.perf_counter() - t0
     nstep = len(tr.energies)
-    print(json.dumps({"workload": a.workload, "grid": f"{g.NN}^3", "nuclei": len(Z), "domains": len(g.seeds),
+    print(json.dumps({"workload": a.workload, "forces": a.forces, "grid": f"{g.NN}^3", "nuclei": len(Z),
+                      "domains": len(g.seeds),
                       "iters_per_step": iters, "preconverge_steps": pre, "steps": nstep, "init_s": t_init, "s": dt,
                       "evaluation_parts": parts,
                       "ms_per_geometry_step": dt / max(1, nstep) * 1e3, **out}), flush=True)

@@ -8,21 +8,25 @@ from realmolecule_b200.dynamics import fire, velocity_verlet
 
 
 class Harmonic:
-    """E = sum_a k/2 |x_a - c_a|^2 + sum_x v(x) w(x): forces -k (x - c); dE/dv = w."""
+    """E = sum_a k/2 |x_a - c_a|^2 + sum_x v(x) w(x): forces -k (x - c); dE/dv = w.  The same
+    interface as autograd.EnergyModel: evaluate(x, v, dE_dv) fills a given dE_dv tensor."""
 
     def __init__(self, centres, k=0.3, w=None):
         self.c = np.asarray(centres, float)
         self.k = k
         self.w = w
+        self.S3 = len(w) if w is not None else 0
         self.calls = 0
 
-    def evaluate(self, x, v=None):
+    def evaluate(self, x, v=None, dE_dv=None):
         self.calls += 1
         x = np.asarray(x, float).reshape(self.c.shape)
         E = 0.5 * self.k * np.sum((x - self.c) ** 2)
         if v is not None:
-            E += float(np.dot(v, self.w))
-        return E, -self.k * (x - self.c), -self.w if self.w is not None else np.zeros(1)
+            E += float(np.dot(np.asarray(v.cpu() if hasattr(v, "cpu") else v), self.w))
+        if dE_dv is not None:
+            dE_dv.copy_(torch.from_numpy(self.w))
+        return E, -self.k * (x - self.c), dE_dv
 
 
 def test_autograd_function_routes_gradients():
