@@ -24,11 +24,16 @@ period with the flush before EVERY solver step (every kernel reads HBM cold).
 ``cpu_baseline`` the reference's own cloud/solver.py kernels compiled for the host
            (oracle/_ref, OpenMP over all host cores) on a bounded sample of the same workload.
 
-``converge`` the second half of the metric, seconds to converge (|dE| < 1e-6 Ha between checks
-           100 steps apart) with the new flavour: glycine (40 electrons, 128^3) as one context in
-           mixed precision and in FP64, and the 96 water clusters (1-12 waters, 48^3-128^3) as one
-           mixed-precision batch against the plain FP64 path (one FP64 context per instance, one
-           after another).  Times are CUDA events around initialise + solve on the solver stream.
+``converge`` the second half of the metric, seconds to converge with the new flavour: glycine
+           (40 electrons, 128^3) as one context in mixed precision and in FP64, and the 96 water
+           clusters (1-12 waters, 64^3-128^3) as one mixed-precision batch against the plain FP64 path
+           (one FP64 context per instance, one after another).  Converged: |dE| < 1e-9 Ha on 3
+           consecutive checks 100 steps apart, which keeps every solve within 1e-6 Ha of its fixed
+           point; mixed solves finish in FP64 in place.  ``max_abs_dE_Ha`` compares the mixed and
+           FP64 answers; ``forces`` the mixed and FP64 forces.  Times are CUDA events around
+           initialise + solve on the solver stream.
+``batch_step`` the C3 batch step alone (all 96 clusters active, mixed precision): Gpt/s, launches
+           per step and the composite HBM roofline of its kernels.
 
 ``callers`` the other reference callers of the step through their drop-ins, each beside its CPU
            restatement: the recorded hairpin job (RealQMSolver), atom.js's He page, mol_fast.js's
@@ -312,15 +317,17 @@ def run_ours(a):
 
     ctx.close()
     conv = None if a.no_converge else converge_leg(stream, dist, rank, world)
+    batch = None if a.no_converge or rank != 0 else batch_leg(stream, measured_peak()[0])
     callers = None if a.no_converge or rank != 0 else caller_legs(a)
 
     if rank == 0:
         peak, peak_kind = measured_peak()
         up = prof.get("update", {"ms": 0, "bytes": 0, "launches": 1})
-        upd_ms = up["ms"] / max(1, up["launches"])
         upd_bytes = up["bytes"] / max(1, up["launches"])
+        upd_ms = amortised_update_ms(prof, ms / a.steps)
         achieved = upd_bytes / (upd_ms * 1e-3) / 1e9 if upd_ms > 0 else None
         period_bytes = sum(v["bytes"] for v in prof.values())
+        hbm = hbm_leg(stream, peak)
         cpu = None
         if world == 1 and not a.no_cpu_baseline:
             try:
@@ -341,6 +348,11 @@ def run_ours(a):
                          "frac": achieved / peak if achieved else None, "traffic": ncu_traffic(a.workload),
                          "kernel": "k_step_sp (ITP update fused with a Jacobi sweep)", "bytes_per_launch": upd_bytes,
                          "peak_kind": peak_kind,
+                         "duration": "in-graph: (timed period - the eager event time of every other kernel class) "
+                                     "/ update launches, so launches x duration <= ms_per_step",
+                         "us_per_launch_in_graph": upd_ms * 1e3,
+                         "us_per_launch_eager_events": up["ms"] / max(1, up["launches"]) * 1e3,
+                         "hbm_bound_320": hbm,
                          # every kernel of the period: its algorithmic bytes over the timed period time
                          "composite": {"achieved": period_bytes / (ms / a.steps * 1e-3) / 1e9,
                                        "frac": period_bytes / (ms / a.steps * 1e-3) / 1e9 / peak,
@@ -349,6 +361,7 @@ def run_ours(a):
                         for k, v in prof.items()},
             "cpu_baseline": cpu,
             "converge": conv,
+            "batch_step": batch,
             "callers": callers,
             "clocks": clk.summary(),
             "gpu_launches": launches,
@@ -358,11 +371,113 @@ def run_ours(a):
         dist.destroy_process_group()
 
 
+def amortised_update_ms(prof, period_ms):
+    """Duration of one update launch inside the replayed period: the period's time less the eager
+    CUDA-event time of every other kernel class, over the update launches of the period."""
+    up = prof.get("update")
+    if not up or not up["launches"]:
+        return 0.0
+    other = sum(v["ms"] for k, v in prof.items() if k != "update")
+    return max(period_ms - other, 1e-6) / up["launches"]
+
+
+def hbm_leg(stream, peak):
+    """The same solver.py step on a 320^3 grid (the 1000-water geometry, 3000 atoms, all-electron
+    idiom): 33 M points per field, every pass streams HBM (the 128^3 fields fit the 126 MB L2)."""
+    import torch
+    from realmolecule_b200 import Context, configs
+    g = configs.water1000()
+    cfg = configs.reference_config(g)
+    ctx = Context(g.NN, cfg["screen"], cfg["atoms"], flavor="solver.py")
+    ctx.set_stream(stream.cuda_stream)
+    ctx.initialize()
+    for _ in range(2):
+        ctx.step(PERIOD)
+    periods = 5
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    ctx.step(PERIOD * periods)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    period_ms = e0.elapsed_time(e1) / periods
+    ctx.profile_begin()
+    ctx.step(PERIOD)
+    prof = ctx.profile_end()
+    ctx.close()
+    up = prof["update"]
+    b = up["bytes"] / up["launches"]
+    t = amortised_update_ms(prof, period_ms)
+    return {"workload": f"water1000 geometry, {len(cfg['atoms'])} atoms, {g.NN}^3 at h={g.h} (solver.py schedule)",
+            "value_gpts": interior(g.NN) * PERIOD / (period_ms * 1e-3) / 1e9, "ms_per_period": period_ms,
+            "achieved": b / (t * 1e-3) / 1e9, "frac": b / (t * 1e-3) / 1e9 / peak, "us_per_launch_in_graph": t * 1e3,
+            "bytes_per_launch": b}
+
+
+def nm_step_bytes(NN, es=4, pi=4, pre=1, post=1):
+    """Algorithmic bytes per new-flavour step on one grid (the byte counts of nm_flavor.cu's launches):
+    the update every step (psi, K, P, label read; psi written); every pi steps the materialised
+    normalisation (psi, label read; psi written) and one V(pre, post) cycle (each red-black colour
+    2.5 field values per point, the residual 3, full weighting and the coarse zeroing, the
+    prolongation 2 fine + 1 coarse, the coarsest level 2 values per point)."""
+    levels, nn = [NN], NN
+    while nn % 2 == 0 and nn // 2 >= 6:
+        nn //= 2
+        levels.append(nn)
+    n_in = [(x - 1) ** 3 for x in levels]
+    s3 = [(x + 1) ** 3 for x in levels]
+    v = 0.0
+    for l in range(len(levels) - 1):
+        v += (pre + post) * 2 * 2.5 * es * n_in[l] + 3 * es * n_in[l] + es * (n_in[l] + n_in[l + 1])
+        v += es * s3[l + 1] + es * (2 * n_in[l] + n_in[l + 1])
+    v += 2 * es * s3[-1]
+    return (4 * es + 4) * n_in[0] + ((2 * es + 4) * s3[0] + v) / pi
+
+
+def batch_leg(stream, peak):
+    """The C3 batch step on its own: all 96 clusters active in one mixed-precision batch (one launch
+    per kernel over the (instance, tile) work lists, a period per CUDA-graph replay), timed with CUDA
+    events over 400 steps; composite roofline = the algorithmic bytes of every kernel of the step
+    (nm_step_bytes) over the step time."""
+    import torch
+    from realmolecule_b200 import configs
+    from realmolecule_b200.batch import Batch
+    geoms = configs.clusters96()
+    inst = [{"NN": x.NN, "screen": x.screen, "atoms": configs.to_domain_atoms(x)} for x in geoms]
+    b = Batch(inst, precision="mixed", label_until=LABEL_UNTIL)
+    b.set_stream(stream.cuda_stream)
+    b.initialize()
+    b.step(LABEL_UNTIL + 200)
+    n = 400
+    l0 = b.info()["kernel_launches"]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    b.step(n)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / n
+    info = b.info()
+    b.close()
+    byts = sum(nm_step_bytes(x.NN) for x in geoms)
+    return {"instances": len(geoms), "interior_points": info["interior_points"], "ms_per_step": ms,
+            "value_gpts": info["interior_points"] / (ms * 1e-3) / 1e9,
+            "launches_per_step": (info["kernel_launches"] - l0) / n,
+            "roofline": {"bound": "hbm", "bytes_per_step": byts, "achieved": byts / (ms * 1e-3) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": byts / (ms * 1e-3) / 1e9 / peak,
+                         "kernels": "update + normalisation + V(1,1) multigrid, composite"}}
+
+
 # ---------------------------------------------------------------------------------------
 # seconds to converge: mixed / batched against plain FP64 (new flavour)
 # ---------------------------------------------------------------------------------------
-TOL, CHECK, MAX_STEPS = 1e-6, 100, 40000
-TIGHT_STEPS = 12000  # untimed continuation of the glycine solves for the precision comparison
+# Convergence: |dE| < TOL on CHECKS consecutive checks CHECK steps apart (molecule.js counts 3 frames
+# within CONVERGENCE_THRESHOLD, :4645-4659).  On these workloads |dE| < 1e-6 between checks stops up to
+# 3e-4 Ha short of the fixed point: the ITP energy has plateaus (an electron crossing its domain to a
+# lower well) that a loose threshold takes for convergence; 1e-9 on 3 checks stays within 1e-6 Ha.
+TOL, CHECK, CHECKS, MAX_STEPS = 1e-9, 100, 3, 60000
+LABEL_UNTIL = 1    # the level set moves the labels for the first LABEL_UNTIL steps, then they are frozen
+ADJ_STEPS = 48     # warm-started steps of the adjoint comparison
 
 
 def _timed(stream, fn):
@@ -540,63 +655,84 @@ def mol_fast_leg(a):
     return out
 
 
+def _glycine_forces(g, rows, c64, stream):
+    """Mixed-vs-FP64 force errors on glycine: (1) the Hellmann-Feynman force of the fp32 fields at the
+    point where they stop resolving the energy, against the converged FP64 force; (2) the adjoint
+    through ADJ_STEPS warm-started steps from the converged FP64 state, fp32 fields against FP64."""
+    from realmolecule_b200 import Context, _lib as L
+    n_nuc = len(g.elements)
+    F64 = c64.forces(L.FORCE_HF)[:n_nuc]
+    c32 = Context(g.NN, g.screen, rows, flavor="new", precision="mixed", label_until=LABEL_UNTIL)
+    c32.set_stream(stream.cuda_stream)
+    c32.initialize()
+    E32 = float(c32.energy()[L.E_TOTAL])
+    c32.solve(3e-9 * abs(E32), MAX_STEPS, CHECK)  # the fp32 stall point (no promotion at this tolerance)
+    assert not c32.fp64
+    F32 = c32.forces(L.FORCE_HF)[:n_nuc]
+    # the adjoint from one state, in the same schedule phase on both contexts
+    st = c64.download(psi=True, label=True, P=True)
+    adj = {}
+    for name, c in (("fp64", c64), ("mixed", c32)):
+        c.step((4 - c.info().steps_done % 4) % 4)
+        c.set_adjoint_window(ADJ_STEPS)
+        c.upload(psi=st["psi"], label=st["label"], P=st["P"])
+        c.set_atoms(rows)
+        c.step(ADJ_STEPS)
+        adj[name] = c.adjoint()[0][:n_nuc]
+    c32.close()
+    return {"hf_fp32_stall_vs_fp64_converged_max_abs": float(np.abs(F32 - F64).max()),
+            "adjoint_fp32_vs_fp64_max_abs": float(np.abs(adj["mixed"] - adj["fp64"]).max()),
+            "max_abs_force": float(np.abs(F64).max()), "unit": "Ha/bohr", "adjoint_steps": ADJ_STEPS}
+
+
 def converge_leg(stream, dist, rank, world):
     from realmolecule_b200 import Context, configs, _lib as L
     from realmolecule_b200.batch import Batch
     from realmolecule_b200 import shard
-    out = {"criterion": f"|dE| < {TOL:g} Ha between checks {CHECK} steps apart (labels frozen after step 1)",
+    out = {"criterion": f"|dE| < {TOL:g} Ha on {CHECKS} consecutive checks {CHECK} steps apart; mixed solves "
+                        "converge in fp32 to max(tol, 3e-9 |E|), then continue in FP64 in place",
+           "labels": f"level set for the first {LABEL_UNTIL} steps, then frozen",
            "timing": "CUDA events around initialise + solve on the solver stream (allocation excluded)"}
 
     # glycine 128^3, one context per precision (every rank solves it; rank 0 reports)
     g = configs.glycine128()
     rows = configs.to_domain_atoms(g)
-    gly = {}
+    gly, keep = {}, None
     for prec in ("mixed", "fp64"):
-        c = Context(g.NN, g.screen, rows, flavor="new", precision=prec, label_until=1)
+        c = Context(g.NN, g.screen, rows, flavor="new", precision=prec, label_until=LABEL_UNTIL,
+                    converge_checks=CHECKS)
         c.set_stream(stream.cuda_stream)
         (steps, E), t = _timed(stream, lambda: (c.initialize(), c.solve(TOL, MAX_STEPS, CHECK))[1])
-        # untimed: the same solves carried on far past the criterion; the mixed one first in fp32
-        # (where it stalls), then promoted to FP64 in place
-        extra = {}
-        if prec == "mixed":
-            c.step(TIGHT_STEPS // 2)
-            extra["E_fp32_stalled"] = float(c.energy()[L.E_TOTAL])
-            c.promote()
-            c.step(TIGHT_STEPS // 2)
+        gly[prec] = (_max_over_ranks(dist, t), int(steps), float(E), bool(c.fp64))
+        if prec == "fp64":
+            keep = c
         else:
-            c.step(TIGHT_STEPS)
-        extra["E"] = float(c.energy()[L.E_TOTAL])
-        gly[prec] = (_max_over_ranks(dist, t), int(steps), float(E), extra)
-        c.close()
+            c.close()
+    forces = _glycine_forces(g, rows, keep, stream)
+    keep.close()
     out["glycine128"] = {"electrons": int(g.charges.sum()), "grid": f"{g.NN}^3 h={g.h}",
                          "mixed_s": gly["mixed"][0], "fp64_s": gly["fp64"][0],
+                         "speedup_vs_fp64": gly["fp64"][0] / gly["mixed"][0],
                          "steps_mixed": gly["mixed"][1], "steps_fp64": gly["fp64"][1],
+                         "mixed_promoted_to_fp64": gly["mixed"][3],
                          "E_mixed": gly["mixed"][2], "E_fp64": gly["fp64"][2],
-                         "abs_dE_Ha": abs(gly["mixed"][2] - gly["fp64"][2]),
-                         "tight": {"extra_steps": TIGHT_STEPS, "E_fp64": gly["fp64"][3]["E"],
-                                   "E_mixed_fp32_stalled": gly["mixed"][3]["E_fp32_stalled"],
-                                   "E_mixed_then_fp64": gly["mixed"][3]["E"],
-                                   "abs_dE_Ha_fp32_stalled": abs(gly["mixed"][3]["E_fp32_stalled"] - gly["fp64"][3]["E"]),
-                                   "abs_dE_Ha_mixed_then_fp64": abs(gly["mixed"][3]["E"] - gly["fp64"][3]["E"]),
-                                   "note": "untimed continuation past the criterion: the FP64 solve and the mixed "
-                                           "solve (fp32 for half, where it stalls, then promoted to FP64)"}}
+                         "abs_dE_Ha": abs(gly["mixed"][2] - gly["fp64"][2]), "forces": forces}
 
     # 96 water clusters: this rank's cost share, mixed batch vs one FP64 context per instance
     geoms = configs.clusters96()
     inst = [{"NN": x.NN, "screen": x.screen, "atoms": configs.to_domain_atoms(x)} for x in geoms]
     share = [inst[q] for q in shard.my_share(inst, rank, world)]
-    b = Batch(share, precision="mixed", label_until=1)
+    b = Batch(share, precision="mixed", label_until=LABEL_UNTIL, converge_checks=CHECKS)
     b.set_stream(stream.cuda_stream)
     (cb, Eb), tb = _timed(stream, lambda: (b.initialize(), b.solve(TOL, MAX_STEPS, CHECK))[1])
-    if len(share) and (cb <= 0).any():
-        raise RuntimeError(f"mixed batch: {(cb <= 0).sum()} instances did not converge in {MAX_STEPS} steps")
     pts = b.info()["interior_points"]
     b.close()
 
     def plain():
         E, steps = [], []
         for it in share:
-            c = Context(it["NN"], it["screen"], it["atoms"], flavor="new", precision="fp64", label_until=1)
+            c = Context(it["NN"], it["screen"], it["atoms"], flavor="new", precision="fp64",
+                        label_until=LABEL_UNTIL, converge_checks=CHECKS)
             c.set_stream(stream.cuda_stream)
             c.initialize()
             n, e = c.solve(TOL, MAX_STEPS, CHECK)
@@ -612,6 +748,8 @@ def converge_leg(stream, dist, rank, world):
                          "mixed_batched_s": tb, "fp64_plain_s": tp,
                          "solves_per_s_mixed_batched": len(inst) / tb, "solves_per_s_fp64_plain": len(inst) / tp,
                          "speedup_vs_fp64_plain": tp / tb, "max_abs_dE_Ha": dE,
+                         "unconverged_rank0": {"mixed_batched": int((cb < 0).sum()) if len(share) else 0,
+                                               "fp64_plain": int((sp >= MAX_STEPS).sum()) if len(share) else 0},
                          "steps_rank0": {"mixed_batched_max": int(cb.max()) if len(share) else 0,
                                          "fp64_plain_max": int(sp.max()) if len(share) else 0,
                                          "fp64_plain_sum": int(sp.sum()) if len(share) else 0}}

@@ -211,6 +211,7 @@ class Context:
         e = C.c_double()
         self._chk(self.lib.rq_solve(self.ctx, float(tol_dE), int(max_steps), int(check_interval), C.byref(taken),
                                     C.byref(e)), "rq_solve")
+        self.fp64 = self.info().precision == L.PREC_FP64  # a mixed new-flavour solve may have promoted
         return taken.value, e.value
 
     def profile_begin(self):

@@ -220,7 +220,6 @@ namespace {
 // one as they reach the fp32 resolution of their energy; each kernel of a step is then one
 // launch per non-empty set.
 constexpr int kF32 = 0, kF64 = 1;
-constexpr double kMixedFloor = 3e-9;  // relative |dE| between checks that fp32 fields resolve
 }  // namespace
 
 // Work items of one instance for every list; built once at creation, concatenated by build_plans.
@@ -972,7 +971,8 @@ extern "C" int rq_batch_solve(rq_batch* b, double tol_dE, int32_t max_steps, int
     prev[q] = e[(size_t)q * RQ_ENERGY_LEN];
     tol[q] = b->f64[q] ? tol_dE : std::max(tol_dE, kMixedFloor * std::fabs(prev[q]));
   }
-  std::vector<int> conv(b->n, -1);
+  std::vector<int> conv(b->n, -1), run(b->n, 0);
+  const int need = b->cfg.converge_checks > 0 ? b->cfg.converge_checks : 1;
   int taken = 0, left = b->n;
   while (taken < max_steps && left > 0) {
     const int n = std::min(check_interval, max_steps - taken);
@@ -984,12 +984,17 @@ extern "C" int rq_batch_solve(rq_batch* b, double tol_dE, int32_t max_steps, int
       if (!b->active[q]) continue;
       const double E = e[(size_t)q * RQ_ENERGY_LEN], d = std::fabs(E - prev[q]);
       prev[q] = E;
-      if (d >= tol[q]) continue;
-      changed = true;
-      if (!b->f64[q] && tol[q] > tol_dE) {
+      if (d >= tol[q]) {
+        run[q] = 0;
+        continue;
+      }
+      if (!b->f64[q] && tol[q] > tol_dE) {  // fp32 has stalled: refine in FP64 from here
+        changed = true;
         BRC(b_promote(b, q));
         tol[q] = tol_dE;
-      } else {
+        run[q] = 0;
+      } else if (++run[q] >= need) {
+        changed = true;
         conv[q] = taken;
         b->active[q] = 0;
         left--;

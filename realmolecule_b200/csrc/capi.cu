@@ -903,7 +903,12 @@ extern "C" int rq_solve(rq_ctx* c, double tol_dE, int32_t max_steps, int32_t che
   int rc = rq_energy(c, e, nullptr);
   if (rc != RQ_OK) return rc;
   double prev = e[RQ_E_TOTAL];
-  int taken = 0;
+  const int need = c->cfg.converge_checks > 0 ? c->cfg.converge_checks : 1;
+  // a mixed-precision new-flavour context first converges as far as its fp32 fields resolve, then
+  // continues in FP64 from there (the same staging as rq_batch_solve)
+  bool staged = c->cfg.flavor == RQ_FLAVOR_NEW && !c->fp64;
+  double tol = staged ? std::max(tol_dE, kMixedFloor * std::fabs(prev)) : tol_dE;
+  int taken = 0, run = 0;
   while (taken < max_steps) {
     const int n = std::min(check_interval, max_steps - taken);
     if ((rc = rq_step(c, n)) != RQ_OK) return rc;
@@ -911,7 +916,18 @@ extern "C" int rq_solve(rq_ctx* c, double tol_dE, int32_t max_steps, int32_t che
     if ((rc = rq_energy(c, e, nullptr)) != RQ_OK) return rc;
     const double d = std::fabs(e[RQ_E_TOTAL] - prev);
     prev = e[RQ_E_TOTAL];
-    if (d < tol_dE) break;
+    if (d >= tol) {
+      run = 0;
+      continue;
+    }
+    if (staged && tol > tol_dE) {  // fp32 has stalled: refine in FP64 from here
+      if ((rc = rq_promote(c)) != RQ_OK) return rc;
+      staged = false;
+      tol = tol_dE;
+      run = 0;
+      continue;
+    }
+    if (++run >= need) break;
   }
   if (steps_taken) *steps_taken = taken;
   if (E_final) *E_final = prev;

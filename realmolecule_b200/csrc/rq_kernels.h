@@ -116,6 +116,9 @@ cudaError_t launch_mj_accum_norms(const float* U, const int* label, const Geo& g
                                   cudaStream_t st);
 
 // ---- new flavour (nm_kernels.cu), T = float (mixed) or double (FP64) --------------------
+// |dE| between checks, relative to |E|, below which fp32 fields stop resolving the energy: a
+// mixed-precision solve that needs less is promoted to FP64 there
+constexpr double kMixedFloor = 3e-9;
 template <typename T>
 cudaError_t nm_potential(T* K, const double* at, int nAt, const Geo& g, double h, double sigma, cudaStream_t st);
 template <typename T>
