@@ -54,8 +54,10 @@ struct BItem {
 template <typename T, bool ACC>
 __global__ void __launch_bounds__(256) kb_update(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cu,
                                                  int cp, int cl, T half_dv, T dt, double* __restrict__ norms,
-                                                 const double* __restrict__ scale) {
+                                                 const double* __restrict__ scale, const unsigned* __restrict__ seed,
+                                                 unsigned* __restrict__ seed_next) {
   __shared__ DomTable<1, 128> tab;
+  if (seed && blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) *seed_next = *seed + 1u;
   const BItem it = items[blockIdx.x];
   const BInst& I = ins[it.inst];
   double* nrm = norms ? norms + I.dom0 : nullptr;
@@ -65,7 +67,8 @@ __global__ void __launch_bounds__(256) kb_update(const BInst* __restrict__ ins, 
   }
   const Geo g = I.g;
   nm_update_body<T, ACC>((const T*)I.U[cu], (T*)I.U[1 - cu], (const T*)I.K, (const T*)I.P[cp], I.lab[cl], g, half_dv,
-                         dt, I.h * I.h * I.h, I.nDom, nrm, tab, it.bx, it.by, it.bz, scale ? scale + I.dom0 : nullptr);
+                         dt, I.h * I.h * I.h, I.nDom, nrm, tab, it.bx, it.by, it.bz, scale ? scale + I.dom0 : nullptr,
+                         seed);
   if (ACC) {
     __syncthreads();
     dom_table_flush(tab, nrm);
@@ -241,6 +244,7 @@ struct rq_batch {
   int D = 0, A = 0;               // total domains / entries
   double *dnorm = nullptr, *dpd = nullptr, *dF = nullptr, *Zdom = nullptr, *at_all = nullptr, *scale = nullptr;
   int* err = nullptr;
+  unsigned* rseed = nullptr;      // the step seed of the fp32 set's unbiased rounding (2 words by parity)
   float4* seeds_all = nullptr;
   int maxlev = 0;
   // work lists, one set per precision
@@ -407,6 +411,7 @@ static int build(rq_batch* b) {
   BALLOC(b->at_all, sizeof(double) * 4 * b->A);
   BALLOC(b->seeds_all, sizeof(float4) * b->A);
   BALLOC(b->err, sizeof(int) * 4);
+  BALLOC(b->rseed, sizeof(unsigned) * 2);
   std::vector<double> zd(b->D), at(4 * (size_t)b->A);
   std::vector<float4> seeds;
   seeds.reserve(b->A);
@@ -582,12 +587,14 @@ static int b_step(rq_batch* b, int s) {
     using T = decltype(tag);
     const rq_batch::Plan& m = b->pl[p].march[0];
     if (!m.n) return RQ_OK;
+    const unsigned* sd = p == kF32 ? b->rseed + b->cu : nullptr;
+    unsigned* sn = p == kF32 ? b->rseed + (1 - b->cu) : nullptr;
     if (norm)
       kb_update<T, true><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cp, b->cl, (T)hd, (T)dt, b->dnorm,
-                                                             sc);
+                                                             sc, sd, sn);
     else
       kb_update<T, false><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cp, b->cl, (T)hd, (T)dt, nullptr,
-                                                              sc);
+                                                              sc, sd, sn);
     BL("update");
     return RQ_OK;
   }));

@@ -108,19 +108,45 @@ __device__ __forceinline__ void nm_init_body(T* __restrict__ U, int* __restrict_
   U[id] = interior ? (T)exp(-sqrt((double)best)) : T(0);
 }
 
+// Unbiased rounding of the fp32 update.  With round-to-nearest, a change of psi smaller than half
+// an ulp is lost at every step and the fp32 iteration stops short of the fixed point.  Instead the
+// new value is formed exactly in FP64 and rounded down or up with probability proportional to the
+// distance to each neighbour, so its expected value is exact.  The uniform variate is a
+// counter-based hash of (grid point, step seed) -- the SplitMix64 finaliser (Steele, Lea and Flood,
+// OOPSLA 2014) -- so a run is reproducible.
+__device__ __forceinline__ unsigned sr_uniform24(unsigned long long id, unsigned seed) {
+  unsigned long long x = id * 0x9E3779B97F4A7C15ull + (unsigned long long)seed * 0xD1B54A32D192ED03ull;
+  x ^= x >> 30;
+  x *= 0xBF58476D1CE4E5B9ull;
+  x ^= x >> 27;
+  x *= 0x94D049BB133111EBull;
+  x ^= x >> 31;
+  return (unsigned)(x >> 40);  // 24 bits
+}
+__device__ __forceinline__ float sr_round(double v, unsigned u24) {
+  const float a = __double2float_rz(v);  // the neighbour toward zero
+  const double rem = v - (double)a;      // same sign as v, |rem| < the ulp of a
+  if (rem == 0.0) return a;
+  const float b = nextafterf(a, v > 0.0 ? 3.0e38f : -3.0e38f);  // the neighbour away from zero
+  const double frac = rem / ((double)b - (double)a);             // in (0, 1)
+  return (double)u24 * 5.9604644775390625e-08 < frac ? b : a;   // u24 / 2^24
+}
+
 // ITP update (same-label Neumann Laplacian) on the march tile (bx, by, bz); with ACC the FP64
 // norm of the new psi per label goes through the block table (caller inits and flushes it).
 // With a non-null `scale` the stored psi is one normalisation behind.  The update is linear in
 // psi and reads only neighbours of the centre's label (a neighbour of another label is replaced
 // by the centre value), so the pending per-domain scale multiplies the result once: psi' =
 // scale[label] * update(psi), formed in FP64 and rounded once -- normalise-then-update up to
-// rounding, without a separate pass over psi.
+// rounding, without a separate pass over psi.  With a non-null `seed` (fp32 fields) the stored
+// value is rounded without bias (sr_round) from its exact FP64 form.
 template <typename T, bool ACC>
 __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __restrict__ Unew, const T* __restrict__ K,
                                                const T* __restrict__ P, const int* __restrict__ label, const Geo& g,
                                                T half_dv, T dt, double h3, int nDom, double* __restrict__ norms,
                                                DomTable<1, 128>& tab, int bx, int by, int bz,
-                                               const double* __restrict__ scale = nullptr) {
+                                               const double* __restrict__ scale = nullptr,
+                                               const unsigned* __restrict__ seed = nullptr) {
   using A = Ar<T>;
   RunSum<1> rs;
   rs.reset();
@@ -131,6 +157,7 @@ __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __res
     const int iend = min(i0 + kMarch, g.NN);
     const long long S = g.S, S2 = g.S2;
     long long id = (long long)i0 * S2 + j * S + k;
+    const unsigned sd = seed ? __ldg(seed) : 0u;
     T u_m = __ldg(U + id - S2), u_c = __ldg(U + id);
     int l_m = __ldg(label + id - S2), l_c = __ldg(label + id);
     for (int i = i0; i < iend; ++i, id += S2) {
@@ -147,8 +174,16 @@ __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __res
       const T e = (lkp == l_c) ? ukp : u_c;
       const T f = (lkm == l_c) ? ukm : u_c;
       const T lap = A::sub(A::add(A::add(A::add(A::add(A::add(a, b), c), d), e), f), A::mul(T(6), u_c));
-      T out = A::add(A::add(u_c, A::mul(half_dv, lap)), A::mul(A::mul(dt, A::sub(kv, A::mul(T(2), pv))), u_c));
-      if (scale) out = (T)((double)out * __ldg(scale + min(max(l_c, 0), nDom - 1)));
+      T out;
+      if (sizeof(T) == sizeof(float) && seed) {
+        // the same f32 terms, summed exactly in FP64, scaled, then one unbiased rounding
+        double v = ((double)u_c + (double)A::mul(half_dv, lap)) + (double)A::mul(A::mul(dt, A::sub(kv, A::mul(T(2), pv))), u_c);
+        if (scale) v *= __ldg(scale + min(max(l_c, 0), nDom - 1));
+        out = (T)sr_round(v, sr_uniform24((unsigned long long)id, sd));
+      } else {
+        out = A::add(A::add(u_c, A::mul(half_dv, lap)), A::mul(A::mul(dt, A::sub(kv, A::mul(T(2), pv))), u_c));
+        if (scale) out = (T)((double)out * __ldg(scale + min(max(l_c, 0), nDom - 1)));
+      }
       Unew[id] = out;
       if (ACC) {
         const double r = (double)out * (double)out * h3;

@@ -66,8 +66,10 @@ int nm_alloc_levels(rq_ctx* c) {
     nn /= 2;
   }
   if (cudaMalloc(&c->seeds, sizeof(float4) * c->n_atoms) != cudaSuccess ||
-      cudaMalloc(&c->scale64, sizeof(double) * c->n_atoms) != cudaSuccess)
+      cudaMalloc(&c->scale64, sizeof(double) * c->n_atoms) != cudaSuccess ||
+      cudaMalloc((void**)&c->rseed, sizeof(unsigned) * 2) != cudaSuccess)
     return rq_cuda(c, cudaErrorMemoryAllocation, "seed table");
+  cudaMemsetAsync(c->rseed, 0, sizeof(unsigned) * 2, c->st);
   return RQ_OK;
 }
 
@@ -167,7 +169,8 @@ static int nm_step_t(rq_ctx* c, int s) {
   LAUNCH(RQ_KC_UPDATE, (4.0 * sizeof(T) + 4.0) * interior(c->g),
          nm_update<T>((const T*)c->U[c->cu], (T*)c->U[1 - c->cu], (const T*)c->K, (const T*)c->P[c->cp], c->lab[c->cl],
                       c->g, (T)c->half_dv, (T)c->dt, c->h3, c->n_atoms, norm ? c->dnorm : nullptr, c->st,
-                      c->nm_pending ? (const double*)c->scale64 : nullptr));
+                      c->nm_pending ? (const double*)c->scale64 : nullptr, c->fp64 ? nullptr : c->rseed + c->cu,
+                      c->fp64 ? nullptr : c->rseed + (1 - c->cu)));
   c->cu ^= 1;
   c->nm_pending = false;  // the update consumed the pending scale
   if (norm) {  // the scale of this step is applied by the next update (or a flush)

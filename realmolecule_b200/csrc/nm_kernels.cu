@@ -20,16 +20,22 @@ __global__ void __launch_bounds__(256) k_nm_init(T* U, int* label, const float4*
   nm_init_body<T>(U, label, seeds, nSeed, g, h, blockIdx.x, ss);
 }
 
+// seed[0]: the step seed of the unbiased fp32 rounding (null: round to nearest); the next step's
+// seed, seed[0] + 1, goes to seed_next (read and written in different words, so every block reads
+// the same value)
 template <typename T, bool ACC>
 __global__ void __launch_bounds__(256) k_nm_update(const T* U, T* Unew, const T* K, const T* P, const int* label, Geo g,
-                                                   T half_dv, T dt, double h3, int nDom, double* norms, const double* scale) {
+                                                   T half_dv, T dt, double h3, int nDom, double* norms, const double* scale,
+                                                   const unsigned* seed, unsigned* seed_next) {
   __shared__ DomTable<1, 128> tab;
+  if (seed && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && threadIdx.y == 0)
+    *seed_next = *seed + 1u;
   if (ACC) {
     dom_table_init(tab);
     __syncthreads();
   }
   nm_update_body<T, ACC>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, norms, tab, blockIdx.x, blockIdx.y,
-                         blockIdx.z, scale);
+                         blockIdx.z, scale, seed);
   if (ACC) {
     __syncthreads();
     dom_table_flush(tab, norms);
@@ -141,14 +147,15 @@ cudaError_t nm_init(T* U, int* label, const float4* seeds, int nSeed, const Geo&
 }
 template <typename T>
 cudaError_t nm_update(const T* U, T* Unew, const T* K, const T* P, const int* label, const Geo& g, T half_dv, T dt,
-                      double h3, int nDom, double* norms, cudaStream_t st, const double* scale) {
+                      double h3, int nDom, double* norms, cudaStream_t st, const double* scale, const unsigned* seed,
+                      unsigned* seed_next) {
   if (g.NN < 2) return cudaSuccess;
   if (norms)
     k_nm_update<T, true><<<nm_march_grid(g), nm_march_block(), 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, norms,
-                                                                   scale);
+                                                                   scale, seed, seed_next);
   else
     k_nm_update<T, false><<<nm_march_grid(g), nm_march_block(), 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom,
-                                                                    nullptr, scale);
+                                                                    nullptr, scale, seed, seed_next);
   return cudaGetLastError();
 }
 template <typename T>
@@ -254,7 +261,7 @@ cudaError_t nm_add(T* K, const T* v, long long n, cudaStream_t st) {
   template cudaError_t nm_potential<T>(T*, const double*, int, const Geo&, double, double, cudaStream_t);           \
   template cudaError_t nm_init<T>(T*, int*, const float4*, int, const Geo&, float, cudaStream_t);                   \
   template cudaError_t nm_update<T>(const T*, T*, const T*, const T*, const int*, const Geo&, T, T, double, int,     \
-                                    double*, cudaStream_t, const double*);                                           \
+                                    double*, cudaStream_t, const double*, const unsigned*, unsigned*);               \
   template cudaError_t nm_apply<T>(T*, const int*, const double*, int, const Geo&, cudaStream_t);                   \
   template cudaError_t nm_normalize<T>(T*, const int*, const double*, const double*, int, double*, int*, const Geo&, \
                                        cudaStream_t);                                                                \

@@ -102,6 +102,7 @@ struct rq_ctx {
   double* atoms_nm = nullptr; // new flavour: x,y,z (bohr), Z_nuc per atom
   void* seeds = nullptr;      // new flavour: float4 (x, y, z, entry) per domain seed
   void* scale64 = nullptr;    // new flavour: per-domain scale (FP64 for both precisions)
+  unsigned* rseed = nullptr;  // new flavour, fp32 fields: the step seed of the unbiased rounding (2 words by parity)
   void* Kext = nullptr;       // new flavour: external potential added to K (T), or null
   bool nm_pending = false;    // new flavour: psi awaits scale64 (applied by the next update or a flush)
   int sp_jdone = 0;           // solver.py flavour: the next Poisson step's first sweep is done (in P[1-cp])

@@ -125,7 +125,8 @@ template <typename T>
 cudaError_t nm_init(T* U, int* label, const float4* seeds, int nSeed, const Geo& g, float h, cudaStream_t st);
 template <typename T>
 cudaError_t nm_update(const T* U, T* Unew, const T* K, const T* P, const int* label, const Geo& g, T half_dv, T dt,
-                      double h3, int nDom, double* norms, cudaStream_t st, const double* scale = nullptr);
+                      double h3, int nDom, double* norms, cudaStream_t st, const double* scale = nullptr,
+                      const unsigned* seed = nullptr, unsigned* seed_next = nullptr);
 template <typename T>
 cudaError_t nm_apply(T* U, const int* label, const double* scale, int nDom, const Geo& g, cudaStream_t st);
 template <typename T>
