@@ -243,9 +243,9 @@ RQ_API int rq_forces(rq_ctx* ctx, int32_t method, double* F);
  * cloud/solver.py:462-474, :504-520 and molecule.js:3170-3185, :3218-3242). */
 RQ_API int rq_nuclear_terms(rq_ctx* ctx, double* E_KK, double* F /* n_atoms x 3 or NULL */);
 /* Step until |E_n - E_{n-1}| < tol_dE on converge_checks consecutive checks every check_interval
- * steps.  New flavour, RQ_PREC_MIXED: fp32 fields resolve the energy only to ~3e-9 |E| between
- * checks, so a context first converges to max(tol_dE, 3e-9 |E|); if that is looser than tol_dE it is
- * promoted to FP64 in place (rq_promote) and continues to tol_dE, as rq_batch_solve does. */
+ * steps.  New flavour, RQ_PREC_MIXED: a context first converges to max(tol_dE, 1e-12 |E|), the change
+ * between checks its fp32 fields resolve; if that is looser than tol_dE it is promoted to FP64 in
+ * place (rq_promote) and continues to tol_dE, as rq_batch_solve does. */
 /* molecule.js flavour: extractWGSL (molecule.js:1108-1192, W_CUTOFF = 0) as a headless buffer of
  * 3 S^2 + 2 S floats -- u^2 on the slice k = slice_k, label + 1000 Z of the label, boundary flags,
  * then the K line and the w line along (i, slice_k, slice_k).  1 <= slice_k < NN. */

@@ -9,7 +9,8 @@ The forward step (oracle.NewMethodDriver.step) is, on the normalised state,
     [V-cycle]    P <- M P + B f,  f = 2 pi psi^2        (every poisson_interval steps)
     update       psi~ = psi + half_dv L psi + dt (K - 2P) psi     (L: same-label Laplacian)
     [normalise]  psi = c psi~,  c_d = sqrt(Z_d / (h^3 sum_d psi~^2))
-and the readout is E = sum_d (Z_d / N_d)(T_d + V_eK,d + V_ee,d).  The reverse sweep applies the
+and the readout is E = sum_d (Z_d / N_d)(T_d + V_eK,d + 2 h^3 sum_d P rho) - (h^3 / 2 pi) sum P A P
+(the P-stationary Hartree form, A = -lap_h).  The reverse sweep applies the
 transposes newest step first: normalise^T lam <- c (lam - (h^3/Z) psi <psi, lam>_d); update^T
 lam <- A lam with dE/dK += dt psi lam and dE/dP += -2 dt psi lam; V-cycle^T by transposing every
 red-black colour, the residual, full weighting (its transpose is the prolongation / 8), the
@@ -168,14 +169,16 @@ def gradient(drv, n_steps):
     _, pd = drv.domain_sums()
     N = pd[:, 0]
     w = np.where((Z > 0) & (N > 0), Z / np.where(N > 0, N, 1.0), 1.0)
-    qn = np.where(N > 0, pd[:, 1:].sum(1) / np.where(N > 0, N, 1.0), 0.0)
+    Q = pd[:, 1] + pd[:, 2] + 2.0 * pd[:, 3]  # the readout's per-domain part, w Q (NewMethodDriver.energy)
+    qn = np.where(N > 0, Q / np.where(N > 0, N, 1.0), 0.0)
     Lc = np.clip(L, 0, n - 1)
     lam = np.zeros(shp)
     muP = np.zeros(shp)
     gK = np.zeros(shp)
     wl, ql, u = _in(w[Lc]), _in(qn[Lc]), _in(psi)
-    _in(lam)[...] = wl * (-h * _same_label_lap(psi, L) + 2.0 * h3 * u * (_in(P) - _in(K) - ql))
-    _in(muP)[...] = wl * h3 * u * u
+    AP = (6.0 * _in(P) - sum(_nb(P, d) for d in _SH)) / (h * h)
+    _in(lam)[...] = wl * (-h * _same_label_lap(psi, L) + 2.0 * h3 * u * (2.0 * _in(P) - _in(K) - ql))
+    _in(muP)[...] = 2.0 * wl * h3 * u * u - h3 / math.pi * AP
     _in(gK)[...] = -wl * h3 * u * u
     if c_final is not None and recs:
         lam = _adj_norm(psi, lam, c_final, L, Z, h3)

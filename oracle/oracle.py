@@ -773,10 +773,11 @@ class NewMethodDriver:
             self.vcycle()
 
     def domain_sums(self):
+        """(sums, per domain (norm, T, V_eK, h^3 sum P rho, h^3 sum P A P)) of the current state."""
         out = np.zeros(3)
-        pd = np.zeros(self.n * 4)
+        pd = np.zeros(self.n * 5)
         O().nm_energy(self.U, self.K, self.P, self.label, self.S, self.h, out, self.n, pd)
-        return out, pd.reshape(self.n, 4)
+        return out, pd.reshape(self.n, 5)
 
     def normalize(self):
         _, pd = self.domain_sums()
@@ -815,9 +816,11 @@ class NewMethodDriver:
     def energy(self):
         self.ready()
         out, pd = self.domain_sums()
-        # partials of the exactly normalised domains (each is linear in its density for this P)
+        # kinetic and nuclear partials of the exactly normalised domains (linear in each domain's
+        # density); the P-stationary Hartree energy 2 sum_d w_d h^3 sum P rho - (h^3/2pi) sum P A P
         w = np.where((self.Zdom > 0) & (pd[:, 0] > 0), self.Zdom / np.where(pd[:, 0] > 0, pd[:, 0], 1.0), 1.0)
-        out = np.array([(w * pd[:, 1]).sum(), (w * pd[:, 2]).sum(), (w * pd[:, 3]).sum()])
+        out = np.array([(w * pd[:, 1]).sum(), (w * pd[:, 2]).sum(),
+                        2.0 * (w * pd[:, 3]).sum() - pd[:, 4].sum() / (2.0 * math.pi)])
         xyz, Z = self.nuclei()
         xyz = xyz.reshape(-1, 3)
         ekk = 0.0

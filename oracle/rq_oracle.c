@@ -1077,13 +1077,15 @@ void orc_nm_vcycle(double* P, const double* U, int S, double h, int levels, int 
   free(f);
 }
 
-/* Per-label FP64 norm / T / V_eK / V_ee (same terms as orc_sp_energy_f64) for FP64 fields. */
+/* Per-label FP64 sums of the new flavour's readout, 5 per domain: norm, T, V_eK, h^3 sum P rho and
+ * h^3 sum P (A P) with A = -lap_h (Dirichlet faces; attributed to the point's label).  out[0..2]: the
+ * sums of T, V_eK and h^3 sum P rho over the domains. */
 void orc_nm_energy(const double* U, const double* K, const double* P, const int32_t* label, int S, double h,
                    double* out, int nDom, double* per_domain) {
   const int NN = S - 1;
   const int64_t S2 = (int64_t)S * S;
   const double h3 = h * h * h;
-  double* pd = (double*)calloc((size_t)S * nDom * 4, sizeof(double));
+  double* pd = (double*)calloc((size_t)S * nDom * 5, sizeof(double));
 #pragma omp parallel for schedule(static)
   for (int i = 1; i < NN; ++i)
     for (int j = 1; j < NN; ++j)
@@ -1101,15 +1103,16 @@ void orc_nm_energy(const double* U, const double* K, const double* P, const int3
         if (i == 1 && label[id - S2] == L) t += u * u;
         if (j == 1 && label[id - S] == L) t += u * u;
         if (k == 1 && label[id - 1] == L) t += u * u;
-        double* q = pd + ((size_t)i * nDom + L) * 4;
+        double* q = pd + ((size_t)i * nDom + L) * 5;
+        double ap = (6.0 * P[id] - (P[id + S2] + P[id - S2] + P[id + S] + P[id - S] + P[id + 1] + P[id - 1])) / (h * h);
         q[0] += rho * h3; q[1] += 0.5 * t * h; q[2] += -K[id] * rho * h3;
-        q[3] += P[id] * rho * h3;
+        q[3] += P[id] * rho * h3; q[4] += P[id] * ap * h3;
       }
-  memset(per_domain, 0, sizeof(double) * nDom * 4);
+  memset(per_domain, 0, sizeof(double) * nDom * 5);
   for (int i = 0; i < S; ++i)
-    for (int q = 0; q < nDom * 4; ++q) per_domain[q] += pd[(size_t)i * nDom * 4 + q];
+    for (int q = 0; q < nDom * 5; ++q) per_domain[q] += pd[(size_t)i * nDom * 5 + q];
   out[0] = out[1] = out[2] = 0;
-  for (int d = 0; d < nDom; ++d) { out[0] += per_domain[4 * d + 1]; out[1] += per_domain[4 * d + 2]; out[2] += per_domain[4 * d + 3]; }
+  for (int d = 0; d < nDom; ++d) { out[0] += per_domain[5 * d + 1]; out[1] += per_domain[5 * d + 2]; out[2] += per_domain[5 * d + 3]; }
   free(pd);
 }
 

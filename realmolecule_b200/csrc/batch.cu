@@ -162,16 +162,16 @@ __global__ void __launch_bounds__(1024) kb_coarsest(const BInst* __restrict__ in
 template <typename T>
 __global__ void __launch_bounds__(256) kb_energy(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cu,
                                                  int cp, int cl, double* __restrict__ pd) {
-  __shared__ DomTable<4, 128> tab;
+  __shared__ DomTable<kNmPD, 128> tab;
   const BItem it = items[blockIdx.x];
   const BInst& I = ins[it.inst];
   dom_table_init(tab);
   __syncthreads();
   const Geo g = I.g;
-  nm_energy_body<T>((const T*)I.U[cu], (const T*)I.K, (const T*)I.P[cp], I.lab[cl], g, I.h, I.nDom, pd + 4 * I.dom0, tab,
-                    it.bx, it.by, it.bz);
+  nm_energy_body<T>((const T*)I.U[cu], (const T*)I.K, (const T*)I.P[cp], I.lab[cl], g, I.h, I.nDom,
+                    pd + kNmPD * I.dom0, tab, it.bx, it.by, it.bz);
   __syncthreads();
-  dom_table_flush(tab, pd + 4 * I.dom0);
+  dom_table_flush(tab, pd + kNmPD * I.dom0);
 }
 
 template <typename T>
@@ -404,7 +404,7 @@ static int build(rq_batch* b) {
   }
   // batch-wide per-domain arrays and atom tables
   BALLOC(b->dnorm, sizeof(double) * b->D);
-  BALLOC(b->dpd, sizeof(double) * 4 * b->D);
+  BALLOC(b->dpd, sizeof(double) * kNmPD * b->D);
   BALLOC(b->Zdom, sizeof(double) * b->D);
   BALLOC(b->scale, sizeof(double) * b->D);
   BALLOC(b->dF, sizeof(double) * 3 * b->A);
@@ -839,7 +839,7 @@ extern "C" int rq_batch_energy(rq_batch* b, double* out) {
     return RQ_OK;
   }
   BRC(b_ready(b));
-  BCK(cudaMemsetAsync(b->dpd, 0, sizeof(double) * 4 * b->D, b->st));
+  BCK(cudaMemsetAsync(b->dpd, 0, sizeof(double) * kNmPD * b->D, b->st));
   BRC(each_set([&](auto tag, int p) -> int {
     using T = decltype(tag);
     const rq_batch::Plan& m = b->pl[p].march[0];
@@ -848,7 +848,7 @@ extern "C" int rq_batch_energy(rq_batch* b, double* out) {
     BL("energy");
     return RQ_OK;
   }));
-  std::vector<double> pd((size_t)4 * b->D);
+  std::vector<double> pd((size_t)kNmPD * b->D);
   int bad_norm = 0;
   BCK(cudaMemcpyAsync(pd.data(), b->dpd, sizeof(double) * pd.size(), cudaMemcpyDeviceToHost, b->st));
   BCK(cudaMemcpyAsync(&bad_norm, b->err, sizeof(int), cudaMemcpyDeviceToHost, b->st));
@@ -867,13 +867,16 @@ extern "C" int rq_batch_energy(rq_batch* b, double* out) {
       continue;
     }
     std::memset(o, 0, sizeof(double) * RQ_ENERGY_LEN);
+    double pap = 0;
     for (int d = 0; d < I.nDom; ++d) {  // partials of the exactly normalised domains
-      const double* x = &pd[4 * ((size_t)I.dom0 + d)];
+      const double* x = &pd[kNmPD * ((size_t)I.dom0 + d)];
       const double w = domain_norm_weight(b->atoms[q][d].Z, x[0]);
       o[RQ_E_T] += w * x[1];
       o[RQ_E_EK] += w * x[2];
-      o[RQ_E_EE] += w * x[3];
+      o[RQ_E_EE] += 2.0 * w * x[3];
+      pap += x[4];
     }
+    o[RQ_E_EE] -= pap / (2.0 * M_PI);  // the P-stationary Hartree energy (nm_energy_readout)
     double ekk = 0;  // point-charge nuclear repulsion (bohr)
     const auto& at = b->atoms[q];
     for (size_t x = 0; x < at.size(); ++x)

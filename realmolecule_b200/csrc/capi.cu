@@ -213,7 +213,7 @@ static int alloc_all(rq_ctx* c) {
   DALLOC(c->Zdom, sizeof(float) * n);
   DALLOC(c->Zdom64, sizeof(double) * n);
   DALLOC(c->dnorm, sizeof(double) * n);
-  DALLOC(c->dpd, sizeof(double) * 4 * n);
+  DALLOC(c->dpd, sizeof(double) * 5 * n);  // 4 sums per domain (solver.py), 5 (new flavour)
   DALLOC(c->dF, sizeof(double) * 3 * n);
   DALLOC(c->dsum, sizeof(double) * 8);
   DALLOC(c->unorm, sizeof(unsigned) * n);

@@ -62,9 +62,10 @@ __device__ __forceinline__ long long n_interior(const Geo& g) {
   return n * n * n;
 }
 
-// dE/dpsi, dE/dP and dE/dK of the readout at psi.  wq: per domain (Z/N, Q/N) with Q = T + V_eK
-// + V_ee and N = h^3 sum psi^2 of the domain.  T = h/2 sum over same-label edges (psi_a - psi_b)^2
-// (edges to a Dirichlet face included), so dT/dpsi = -h L psi with the update's Laplacian.
+// dE/dpsi, dE/dP and dE/dK of the readout at psi (nm_energy: E = sum_d w_d Q_d - (h^3 / 2 pi) <P, A P>,
+// Q_d = T_d + V_eK,d + 2 h^3 sum_d P rho, w_d = Z_d / N_d).  wq: per domain (w, Q/N).  T = h/2 sum
+// over same-label edges (psi_a - psi_b)^2 (edges to a Dirichlet face included), so dT/dpsi = -h L psi
+// with the update's Laplacian; dE/dP = 2 w h^3 rho - (h^3 / pi) A P.
 template <typename T>
 __global__ void __launch_bounds__(256) k_adj_seed(const T* __restrict__ U, const T* __restrict__ K,
                                                   const T* __restrict__ P, const int* __restrict__ label, Geo g,
@@ -88,8 +89,11 @@ __global__ void __launch_bounds__(256) k_adj_seed(const T* __restrict__ U, const
   for (int t = 0; t < 6; ++t)
     if (label[nb[t]] == L) lap += (double)U[nb[t]] - u;
   const double w = wq[2 * L], qn = wq[2 * L + 1];
-  lam[id] = (T)(w * (-h * lap + 2.0 * h3 * u * ((double)P[id] - (double)K[id] - qn)));
-  muP[id] = (T)(w * h3 * u * u);
+  const double pc = (double)P[id];
+  const double ap = (6.0 * pc - ((double)P[id + S2] + (double)P[id - S2] + (double)P[id + S] + (double)P[id - S] +
+                                 (double)P[id + 1] + (double)P[id - 1])) / (h * h);
+  lam[id] = (T)(w * (-h * lap + 2.0 * h3 * u * (2.0 * pc - (double)K[id] - qn)));
+  muP[id] = (T)(2.0 * w * h3 * u * u - h3 / M_PI * ap);
   gK[id] = -w * h3 * u * u;
 }
 
@@ -506,16 +510,16 @@ int adjoint_t(rq_ctx* c, double* F, double* dEdv) {
   const T* K = (const T*)c->K;
   const int* lab = c->lab[c->cl];
   // the readout's per-domain partials -> (Z/N, Q/N)
-  CK(cudaMemsetAsync(c->dpd, 0, sizeof(double) * 4 * n, c->st));
+  CK(cudaMemsetAsync(c->dpd, 0, sizeof(double) * kNmPD * n, c->st));
   LAUNCH(RQ_KC_ENERGY, (4.0 * sizeof(T) + 4.0) * ni,
          nm_energy<T>(psi, K, (const T*)c->P[c->cp], lab, g, c->h, n, c->dpd, c->st));
-  std::vector<double> pd((size_t)4 * n), wq((size_t)2 * n);
+  std::vector<double> pd((size_t)kNmPD * n), wq((size_t)2 * n);
   CK(cudaMemcpyAsync(pd.data(), c->dpd, sizeof(double) * pd.size(), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   for (int d = 0; d < n; ++d) {
-    const double N = pd[4 * d];
-    wq[2 * d] = domain_norm_weight(c->atoms[d].Z, N);
-    wq[2 * d + 1] = N > 0.0 ? (pd[4 * d + 1] + pd[4 * d + 2] + pd[4 * d + 3]) / N : 0.0;
+    const double* x = &pd[(size_t)kNmPD * d];
+    wq[2 * d] = domain_norm_weight(c->atoms[d].Z, x[0]);
+    wq[2 * d + 1] = x[0] > 0.0 ? (x[1] + x[2] + 2.0 * x[3]) / x[0] : 0.0;
   }
   CK(cudaMemcpyAsync(A.wq, wq.data(), sizeof(double) * wq.size(), cudaMemcpyHostToDevice, c->st));
   int li = 0, mi = 0;

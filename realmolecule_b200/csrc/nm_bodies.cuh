@@ -389,13 +389,18 @@ __device__ __forceinline__ void nm_coarsest_body(T* __restrict__ P, const T* __r
   for (long long q = threadIdx.x; q < g.S3; q += blockDim.x) P[q] = (T)sP[q];
 }
 
-// per-domain (norm, T, V_eK, V_ee) on the march tile; T counts every same-label edge with an
-// interior end point once (forward edges + the edge to the Dirichlet face on the first layer)
+// Per-domain readout sums, kNmPD per domain: (norm, T, V_eK, h^3 sum P rho, h^3 sum P (A P)) on the
+// march tile, A = -lap_h with Dirichlet faces (the multigrid's operator).  T counts every
+// same-label edge with an interior end point once (forward edges + the edge to the Dirichlet face
+// on the first layer).  The last sum is attributed to the point's domain only for bookkeeping: the
+// readout uses its total in the P-stationary Hartree energy 2 h^3 sum P rho - (h^3 / 2 pi) sum P A P
+// (kNmPD, rq_internal.cuh).
 template <typename T>
 __device__ __forceinline__ void nm_energy_body(const T* __restrict__ U, const T* __restrict__ K, const T* __restrict__ P,
                                                const int* __restrict__ label, const Geo& g, double h, int nDom,
-                                               double* __restrict__ pd, DomTable<4, 128>& tab, int bx, int by, int bz) {
-  RunSum<4> rs;
+                                               double* __restrict__ pd, DomTable<kNmPD, 128>& tab, int bx, int by,
+                                               int bz) {
+  RunSum<kNmPD> rs;
   rs.reset();
   const double h3 = h * h * h;
   const int k = 1 + bx * kNmTK + threadIdx.x;
@@ -416,7 +421,10 @@ __device__ __forceinline__ void nm_energy_body(const T* __restrict__ U, const T*
       if (i == 1 && label[id - S2] == L) t += u * u;
       if (j == 1 && label[id - S] == L) t += u * u;
       if (k == 1 && label[id - 1] == L) t += u * u;
-      double v[4] = {rho * h3, 0.5 * t * h, -(double)K[id] * rho * h3, (double)P[id] * rho * h3};
+      const double pc = (double)P[id];
+      const double ap = (6.0 * pc - ((double)P[id + S2] + (double)P[id - S2] + (double)P[id + S] + (double)P[id - S] +
+                                     (double)P[id + 1] + (double)P[id - 1])) / (h * h);
+      double v[kNmPD] = {rho * h3, 0.5 * t * h, -(double)K[id] * rho * h3, pc * rho * h3, pc * ap * h3};
       rs.add(L, v, tab, pd);
     }
   }

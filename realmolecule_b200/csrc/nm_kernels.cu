@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(1024) k_nm_coarsest(T* P, const T* f, Geo g, d
 template <typename T>
 __global__ void __launch_bounds__(256) k_nm_energy(const T* U, const T* K, const T* P, const int* label, Geo g, double h,
                                                    int nDom, double* pd) {
-  __shared__ DomTable<4, 128> tab;
+  __shared__ DomTable<kNmPD, 128> tab;
   dom_table_init(tab);
   __syncthreads();
   nm_energy_body<T>(U, K, P, label, g, h, nDom, pd, tab, blockIdx.x, blockIdx.y, blockIdx.z);

@@ -23,6 +23,7 @@ namespace rq {
 constexpr int kThreadsK = 32;  // threads along k (contiguous) per block
 constexpr int kThreadsJ = 8;   // threads along j per block
 constexpr int kMarch = 16;     // planes along i marched by one thread
+constexpr int kNmPD = 5;       // new flavour: readout sums per domain (norm, T, V_eK, P rho, P A P)
 
 struct Geo {
   int S;      // points per axis

@@ -117,8 +117,10 @@ cudaError_t launch_mj_accum_norms(const float* U, const int* label, const Geo& g
 
 // ---- new flavour (nm_kernels.cu), T = float (mixed) or double (FP64) --------------------
 // |dE| between checks, relative to |E|, below which fp32 fields stop resolving the energy: a
-// mixed-precision solve that needs less is promoted to FP64 there
-constexpr double kMixedFloor = 3e-9;
+// mixed-precision solve that needs less is promoted to FP64 there.  With the P-stationary readout
+// (nm_energy) the fp32 readout changes smoothly between checks down to ~1e-13 |E| (glycine, 128^3);
+// read as h^3 sum P rho it jittered at ~1e-9 |E|, which needed promotion at 3e-9 |E|.
+constexpr double kMixedFloor = 1e-12;
 template <typename T>
 cudaError_t nm_potential(T* K, const double* at, int nAt, const Geo& g, double h, double sigma, cudaStream_t st);
 template <typename T>
