@@ -94,7 +94,11 @@ typedef struct rq_config {
   int32_t converge_checks;  /* rq_solve / rq_batch_solve: converged after this many consecutive checks with
                                |dE| < tol (molecule.js counts 3 frames within CONVERGENCE_THRESHOLD,
                                :4645-4659); <= 0: 1 */
-  int32_t reserved[4];
+  int32_t fp32_rounding;    /* new flavour, RQ_PREC_MIXED: 0 = the psi update rounds to nearest; 1 = it rounds
+                               without bias (exact FP64 value, rounded down or up with the probability of
+                               its position between the two f32 neighbours; a counter-based hash per point
+                               and step, so runs repeat) */
+  int32_t reserved[3];
 } rq_config;
 
 /* One entry of the reference atom list: a nucleus and/or one electron domain. */

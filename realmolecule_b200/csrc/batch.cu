@@ -40,6 +40,7 @@ struct BInst {
   int nAt, at0;      // entries and their offset in the batch-wide force array
   const float4* seeds;
   int nSeed;
+  const double* K64;  // fp32 instances of a mixed batch: the FP64 K of its promotion set, read by the readout
 };
 
 struct BItem {
@@ -169,7 +170,7 @@ __global__ void __launch_bounds__(256) kb_energy(const BInst* __restrict__ ins, 
   __syncthreads();
   const Geo g = I.g;
   nm_energy_body<T>((const T*)I.U[cu], (const T*)I.K, (const T*)I.P[cp], I.lab[cl], g, I.h, I.nDom,
-                    pd + kNmPD * I.dom0, tab, it.bx, it.by, it.bz);
+                    pd + kNmPD * I.dom0, tab, it.bx, it.by, it.bz, sizeof(T) == sizeof(float) ? I.K64 : nullptr);
   __syncthreads();
   dom_table_flush(tab, pd + kNmPD * I.dom0);
 }
@@ -449,6 +450,11 @@ static int build(rq_batch* b) {
     for (int q = 0; q < n; ++q) BRC(alloc_fields(b, b->hin64[q], sizeof(double)));
     BALLOC(b->din64, sizeof(BInst) * n);
     BCK(cudaMemcpyAsync(b->din64, b->hin64.data(), sizeof(BInst) * n, cudaMemcpyHostToDevice, b->st));
+    // the fp32 instances read their energy with the FP64 K of their promotion set (computed by
+    // initialisation): the f32 rounding of K then enters the readout at second order only
+    for (int q = 0; q < n; ++q)
+      if (!b->f64[q]) b->hin[q].K64 = (const double*)b->hin64[q].K;
+    BCK(cudaMemcpyAsync(b->din, b->hin.data(), sizeof(BInst) * n, cudaMemcpyHostToDevice, b->st));
   }
   b->items.resize(n);
   for (int q = 0; q < n; ++q) make_items(b->hin[q], q, b->items[q]);
@@ -587,8 +593,9 @@ static int b_step(rq_batch* b, int s) {
     using T = decltype(tag);
     const rq_batch::Plan& m = b->pl[p].march[0];
     if (!m.n) return RQ_OK;
-    const unsigned* sd = p == kF32 ? b->rseed + b->cu : nullptr;
-    unsigned* sn = p == kF32 ? b->rseed + (1 - b->cu) : nullptr;
+    const bool sr = p == kF32 && b->cfg.fp32_rounding == 1;
+    const unsigned* sd = sr ? b->rseed + b->cu : nullptr;
+    unsigned* sn = sr ? b->rseed + (1 - b->cu) : nullptr;
     if (norm)
       kb_update<T, true><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cp, b->cl, (T)hd, (T)dt, b->dnorm,
                                                              sc, sd, sn);

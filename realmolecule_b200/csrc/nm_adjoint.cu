@@ -70,7 +70,8 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_adj_seed(const T* __restrict__ U, const T* __restrict__ K,
                                                   const T* __restrict__ P, const int* __restrict__ label, Geo g,
                                                   double h, int nDom, const double* __restrict__ wq,
-                                                  T* __restrict__ lam, T* __restrict__ muP, double* __restrict__ gK) {
+                                                  T* __restrict__ lam, T* __restrict__ muP, double* __restrict__ gK,
+                                                  const double* __restrict__ K64) {
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n_interior(g)) return;
   const Pt p = interior_pt(g, q);
@@ -92,7 +93,8 @@ __global__ void __launch_bounds__(256) k_adj_seed(const T* __restrict__ U, const
   const double pc = (double)P[id];
   const double ap = (6.0 * pc - ((double)P[id + S2] + (double)P[id - S2] + (double)P[id + S] + (double)P[id - S] +
                                  (double)P[id + 1] + (double)P[id - 1])) / (h * h);
-  lam[id] = (T)(w * (-h * lap + 2.0 * h3 * u * (2.0 * pc - (double)K[id] - qn)));
+  const double kv = K64 ? K64[id] : (double)K[id];  // the readout's K (nm_energy_body)
+  lam[id] = (T)(w * (-h * lap + 2.0 * h3 * u * (2.0 * pc - kv - qn)));
   muP[id] = (T)(2.0 * w * h3 * u * u - h3 / M_PI * ap);
   gK[id] = -w * h3 * u * u;
 }
@@ -512,7 +514,7 @@ int adjoint_t(rq_ctx* c, double* F, double* dEdv) {
   // the readout's per-domain partials -> (Z/N, Q/N)
   CK(cudaMemsetAsync(c->dpd, 0, sizeof(double) * kNmPD * n, c->st));
   LAUNCH(RQ_KC_ENERGY, (4.0 * sizeof(T) + 4.0) * ni,
-         nm_energy<T>(psi, K, (const T*)c->P[c->cp], lab, g, c->h, n, c->dpd, c->st));
+         nm_energy<T>(psi, K, (const T*)c->P[c->cp], lab, g, c->h, n, c->dpd, c->st, c->K64));
   std::vector<double> pd((size_t)kNmPD * n), wq((size_t)2 * n);
   CK(cudaMemcpyAsync(pd.data(), c->dpd, sizeof(double) * pd.size(), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
@@ -527,7 +529,7 @@ int adjoint_t(rq_ctx* c, double* F, double* dEdv) {
   T* muP[2] = {(T*)A.muP[0], (T*)A.muP[1]};
   LAUNCH(RQ_KC_FORCES, (4.0 * sizeof(T) + 4.0 + 2.0 * sizeof(T) + 8.0) * ni,
          (k_adj_seed<T><<<nblk(ni), 256, 0, c->st>>>(psi, K, (const T*)c->P[c->cp], lab, g, c->h, n, A.wq, lam[li],
-                                                     muP[mi], A.gK),
+                                                     muP[mi], A.gK, c->K64),
           cudaGetLastError()));
   for (int r = (int)A.rec.size() - 1; r >= 0; --r) {
     const rq_adj::Rec& R = A.rec[r];

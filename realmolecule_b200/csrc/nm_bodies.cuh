@@ -395,11 +395,14 @@ __device__ __forceinline__ void nm_coarsest_body(T* __restrict__ P, const T* __r
 // on the first layer).  The last sum is attributed to the point's domain only for bookkeeping: the
 // readout uses its total in the P-stationary Hartree energy 2 h^3 sum P rho - (h^3 / 2 pi) sum P A P
 // (kNmPD, rq_internal.cuh).
+// With K64 (fp32 fields) the nuclear term reads the FP64 potential: the fields evolve with the f32
+// rounding of K, and reading the energy with the unrounded K removes that rounding from it at first
+// order (the state is stationary, so what is left is second order).
 template <typename T>
 __device__ __forceinline__ void nm_energy_body(const T* __restrict__ U, const T* __restrict__ K, const T* __restrict__ P,
                                                const int* __restrict__ label, const Geo& g, double h, int nDom,
                                                double* __restrict__ pd, DomTable<kNmPD, 128>& tab, int bx, int by,
-                                               int bz) {
+                                               int bz, const double* __restrict__ K64 = nullptr) {
   RunSum<kNmPD> rs;
   rs.reset();
   const double h3 = h * h * h;
@@ -424,7 +427,8 @@ __device__ __forceinline__ void nm_energy_body(const T* __restrict__ U, const T*
       const double pc = (double)P[id];
       const double ap = (6.0 * pc - ((double)P[id + S2] + (double)P[id - S2] + (double)P[id + S] + (double)P[id - S] +
                                      (double)P[id + 1] + (double)P[id - 1])) / (h * h);
-      double v[kNmPD] = {rho * h3, 0.5 * t * h, -(double)K[id] * rho * h3, pc * rho * h3, pc * ap * h3};
+      const double kv = K64 ? K64[id] : (double)K[id];
+      double v[kNmPD] = {rho * h3, 0.5 * t * h, -kv * rho * h3, pc * rho * h3, pc * ap * h3};
       rs.add(L, v, tab, pd);
     }
   }

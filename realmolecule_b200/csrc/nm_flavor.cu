@@ -70,6 +70,8 @@ int nm_alloc_levels(rq_ctx* c) {
       cudaMalloc((void**)&c->rseed, sizeof(unsigned) * 2) != cudaSuccess)
     return rq_cuda(c, cudaErrorMemoryAllocation, "seed table");
   cudaMemsetAsync(c->rseed, 0, sizeof(unsigned) * 2, c->st);
+  if (!c->fp64 && cudaMalloc((void**)&c->K64, sizeof(double) * (size_t)c->g.S3) != cudaSuccess)
+    return rq_cuda(c, cudaErrorMemoryAllocation, "FP64 potential of the readout");
   return RQ_OK;
 }
 
@@ -166,11 +168,12 @@ static int nm_step_t(rq_ctx* c, int s) {
   const bool norm = (s + 1) % f.norm_interval == 0 || (s + 1) % f.poisson_interval == 0 || label_step;
   if (c->adj.cap > 0 && (rc = nm_adj_record_step(c, s % f.poisson_interval == 0, norm)) != RQ_OK) return rc;
   if (norm) CK(cudaMemsetAsync(c->dnorm, 0, sizeof(double) * c->n_atoms, c->st));
+  const bool sr = !c->fp64 && f.fp32_rounding == 1;
   LAUNCH(RQ_KC_UPDATE, (4.0 * sizeof(T) + 4.0) * interior(c->g),
          nm_update<T>((const T*)c->U[c->cu], (T*)c->U[1 - c->cu], (const T*)c->K, (const T*)c->P[c->cp], c->lab[c->cl],
                       c->g, (T)c->half_dv, (T)c->dt, c->h3, c->n_atoms, norm ? c->dnorm : nullptr, c->st,
-                      c->nm_pending ? (const double*)c->scale64 : nullptr, c->fp64 ? nullptr : c->rseed + c->cu,
-                      c->fp64 ? nullptr : c->rseed + (1 - c->cu)));
+                      c->nm_pending ? (const double*)c->scale64 : nullptr, sr ? c->rseed + c->cu : nullptr,
+                      sr ? c->rseed + (1 - c->cu) : nullptr));
   c->cu ^= 1;
   c->nm_pending = false;  // the update consumed the pending scale
   if (norm) {  // the scale of this step is applied by the next update (or a flush)
@@ -193,11 +196,22 @@ static int nm_step_t(rq_ctx* c, int s) {
 
 int nm_step_one(rq_ctx* c, int s) { return c->fp64 ? nm_step_t<double>(c, s) : nm_step_t<float>(c, s); }
 
+__global__ void __launch_bounds__(256) k_nm_add_f2d(double* __restrict__ K, const float* __restrict__ v, long long n) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    K[q] += (double)v[q];
+}
+
 template <typename T>
 static int nm_potential_t(rq_ctx* c) {
   LAUNCH(RQ_KC_OTHER, sizeof(T) * c->g.S3,
          nm_potential<T>((T*)c->K, c->atoms_nm, c->n_atoms, c->g, c->h, c->sigma, c->st));
   if (c->Kext) LAUNCH(RQ_KC_OTHER, 3.0 * sizeof(T) * c->g.S3, nm_add<T>((T*)c->K, (const T*)c->Kext, c->g.S3, c->st));
+  if (!c->fp64 && c->K64) {  // the readout's FP64 copy
+    LAUNCH(RQ_KC_OTHER, 8.0 * c->g.S3, nm_potential<double>(c->K64, c->atoms_nm, c->n_atoms, c->g, c->h, c->sigma, c->st));
+    if (c->Kext)
+      LAUNCH(RQ_KC_OTHER, 20.0 * c->g.S3,
+             (k_nm_add_f2d<<<148 * 8, 256, 0, c->st>>>(c->K64, (const float*)c->Kext, c->g.S3), cudaGetLastError()));
+  }
   return RQ_OK;
 }
 
@@ -356,6 +370,10 @@ int nm_promote(rq_ctx* c) {
       gx = nullptr;
     }
   if ((rc = nm_potential_t<double>(c)) != RQ_OK) return rc;
+  if (c->K64) {  // the fields are FP64 now: K itself is the readout's potential
+    cudaFree(c->K64);
+    c->K64 = nullptr;
+  }
   if (c->adj.cap > 0 && (rc = nm_adj_set_window(c, c->adj.cap)) != RQ_OK) return rc;  // FP64 window buffers
   return cudaStreamSynchronize(c->st) == cudaSuccess ? RQ_OK : rq_cuda(c, cudaGetLastError(), "promotion to FP64");
 }
@@ -401,7 +419,7 @@ int nm_energy(rq_ctx* c, double* out, double* per_domain) {
   else
     LAUNCH(RQ_KC_ENERGY, 16 * interior(c->g),
            nm_energy<float>((const float*)c->U[c->cu], (const float*)c->K, (const float*)c->P[c->cp], c->lab[c->cl],
-                            c->g, c->h, n, c->dpd, c->st));
+                            c->g, c->h, n, c->dpd, c->st, c->K64));
   std::vector<double> pd((size_t)kNmPD * n);
   CK(cudaMemcpyAsync(pd.data(), c->dpd, sizeof(double) * kNmPD * n, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));

@@ -102,11 +102,11 @@ __global__ void __launch_bounds__(1024) k_nm_coarsest(T* P, const T* f, Geo g, d
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_nm_energy(const T* U, const T* K, const T* P, const int* label, Geo g, double h,
-                                                   int nDom, double* pd) {
+                                                   int nDom, double* pd, const double* K64) {
   __shared__ DomTable<kNmPD, 128> tab;
   dom_table_init(tab);
   __syncthreads();
-  nm_energy_body<T>(U, K, P, label, g, h, nDom, pd, tab, blockIdx.x, blockIdx.y, blockIdx.z);
+  nm_energy_body<T>(U, K, P, label, g, h, nDom, pd, tab, blockIdx.x, blockIdx.y, blockIdx.z, K64);
   __syncthreads();
   dom_table_flush(tab, pd);
 }
@@ -225,9 +225,9 @@ cudaError_t nm_coarsest(T* P, const T* f, const Geo& g, double h2, int sweeps, c
 }
 template <typename T>
 cudaError_t nm_energy(const T* U, const T* K, const T* P, const int* label, const Geo& g, double h, int nDom, double* pd,
-                      cudaStream_t st) {
+                      cudaStream_t st, const double* K64) {
   if (g.NN < 2) return cudaSuccess;
-  k_nm_energy<T><<<nm_march_grid(g), nm_march_block(), 0, st>>>(U, K, P, label, g, h, nDom, pd);
+  k_nm_energy<T><<<nm_march_grid(g), nm_march_block(), 0, st>>>(U, K, P, label, g, h, nDom, pd, K64);
   return cudaGetLastError();
 }
 template <typename T>
@@ -273,7 +273,7 @@ cudaError_t nm_add(T* K, const T* v, long long n, cudaStream_t st) {
   template cudaError_t nm_prolong<T>(const T*, T*, const Geo&, const Geo&, cudaStream_t);                           \
   template cudaError_t nm_coarsest<T>(T*, const T*, const Geo&, double, int, cudaStream_t);                         \
   template cudaError_t nm_energy<T>(const T*, const T*, const T*, const int*, const Geo&, double, int, double*,     \
-                                    cudaStream_t);                                                                   \
+                                    cudaStream_t, const double*);                                                    \
   template cudaError_t nm_evolve<T>(const int*, int*, const T*, float*, const Geo&, double, double, cudaStream_t);  \
   template cudaError_t nm_force<T>(const T*, const double*, int, const Geo&, double, double, double*, cudaStream_t,  \
                                    const double*);

@@ -150,7 +150,7 @@ template <typename T>
 cudaError_t nm_coarsest(T* P, const T* f, const Geo& g, double h2, int sweeps, cudaStream_t st);
 template <typename T>
 cudaError_t nm_energy(const T* U, const T* K, const T* P, const int* label, const Geo& g, double h, int nDom, double* pd,
-                      cudaStream_t st);
+                      cudaStream_t st, const double* K64 = nullptr);
 template <typename T>
 cudaError_t nm_evolve(const int* labIn, int* labOut, const T* U, float* W, const Geo& g, double dt_w, double curvReg,
                       cudaStream_t st);

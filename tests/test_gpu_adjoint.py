@@ -153,10 +153,9 @@ def test_empty_window_is_the_hellmann_feynman_gather():
 
 
 def test_adjoint_reaches_hellmann_feynman_at_convergence():
-    """From a converged state, the energy after N more steps tends to the converged energy of the
-    new geometry as N grows, and its gradient to the Hellmann-Feynman force (the form of the
-    reference's force routine).  For a short window they differ: the readout's P and psi respond
-    to a move only over many steps.  Bar: 1e-4 Ha/bohr after 2000 recorded steps."""
+    """From a converged state the gradient of the energy after N more steps is the Hellmann-Feynman
+    force (the form of the reference's force routine): the readout is stationary in psi and, in its
+    P-stationary Hartree form, in P.  Bar: 1e-6 Ha/bohr for windows of 48 and 2000 steps."""
     from realmolecule_b200 import _lib as L
     NN, screen, rows = _water_pair_rows(NN=32, h=0.35)
     ctx, _ = _prepared(NN, screen, rows, settle=200, extra=100)
@@ -169,7 +168,7 @@ def test_adjoint_reaches_hellmann_feynman_at_convergence():
         ctx.step(n)
         Fa, _ = ctx.adjoint()
         gaps.append(np.max(np.abs(Fa - Fh)))
-    assert gaps[1] < 1e-4 and gaps[1] < gaps[0], gaps
+    assert max(gaps) < 1e-6, gaps
     ctx.close()
 
 
