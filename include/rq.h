@@ -98,7 +98,14 @@ typedef struct rq_config {
                                without bias (exact FP64 value, rounded down or up with the probability of
                                its position between the two f32 neighbours; a counter-based hash per point
                                and step, so runs repeat) */
-  int32_t reserved[3];
+  int32_t nuclear_sum;      /* new flavour: how K and the force gathers sum over nuclei.  0 (auto): tiled when
+                               the interior has >= 64 points per axis and there are >= 64 nuclei, else direct;
+                               1: direct (every nucleus at every voxel); 2: tiled whenever the interior has
+                               >= 32 points per axis.  Tiled: per 32^3 tile, nuclei within 3 tile half-widths
+                               direct, the rest through a 16^3-node Chebyshev interpolant of their Coulomb
+                               field (K within 1e-12 relative of the direct sum; the force gather is its exact
+                               transpose) */
+  int32_t reserved[2];
 } rq_config;
 
 /* One entry of the reference atom list: a nucleus and/or one electron domain. */

@@ -70,7 +70,8 @@ class Config(C.Structure):
                 ("mg_post", C.c_int32), ("mg_coarse_sweeps", C.c_int32), ("sic", C.c_int32),
                 ("boundary_speed", C.c_double), ("curv_reg", C.c_double), ("sigma", C.c_double),
                 ("label_until", C.c_int32), ("chebyshev", C.c_int32), ("lobpcg", C.c_int32),
-                ("converge_checks", C.c_int32), ("fp32_rounding", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("converge_checks", C.c_int32), ("fp32_rounding", C.c_int32), ("nuclear_sum", C.c_int32),
+                ("reserved", C.c_int32 * 2)]
 
 
 class Split(C.Structure):

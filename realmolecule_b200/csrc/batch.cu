@@ -190,7 +190,10 @@ __global__ void __launch_bounds__(256) kb_potential(const BInst* __restrict__ in
   __shared__ double sa[128 * 4];
   const BItem it = items[blockIdx.x];
   const BInst& I = ins[it.inst];
-  nm_potential_body<T>((T*)I.K, I.at, I.nAt, I.g, I.h, sigma_scale > 0 ? sigma_scale : I.h, it.bx, sa);
+  // fp32 instances of a mixed batch also write the FP64 K of their promotion set (read by the
+  // readout, used after a promotion)
+  nm_potential_body<T>((T*)I.K, I.at, I.nAt, I.g, I.h, sigma_scale > 0 ? sigma_scale : I.h, it.bx, sa,
+                       sizeof(T) == sizeof(float) ? const_cast<double*>(I.K64) : nullptr);
 }
 
 template <typename T>
@@ -204,7 +207,7 @@ __global__ void __launch_bounds__(256) kb_init(const BInst* __restrict__ ins, co
 template <typename T>
 __global__ void __launch_bounds__(256) kb_force(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cu,
                                                 double sigma_scale, double* __restrict__ F) {
-  __shared__ T sx[kNmForceTile], sy[kNmForceTile], sz[kNmForceTile], sr[kNmForceTile];
+  __shared__ double sx[kNmForceTile], sy[kNmForceTile], sz[kNmForceTile], sr[kNmForceTile];
   const BItem it = items[blockIdx.x];
   const BInst& I = ins[it.inst];
   nm_force_body<T>((const T*)I.U[cu], I.at, I.nAt, I.g, I.h, sigma_scale > 0 ? sigma_scale : I.h, F + 3 * I.at0, it.bx,
@@ -238,7 +241,6 @@ struct rq_batch {
   double dv = 0.2;
   std::vector<BInst> hin;         // host copy of the instance table
   std::vector<BInst> hin64;       // mixed batches: each instance's FP64 field set, taken over on promotion
-  BInst* din64 = nullptr;         // device copy of hin64 (to compute the FP64 K at initialisation)
   BInst* din = nullptr;           // device copy
   std::vector<std::vector<rq_atom>> atoms;
   std::vector<void*> allocs;
@@ -255,7 +257,6 @@ struct rq_batch {
     Plan flat16, flat1, force;
   };
   Plans pl[2];
-  Plan one;                       // scratch list: one instance's flat items
   size_t coarse_smem[kMaxLev] = {};
   cudaStream_t st = nullptr, own = nullptr;
   int cu = 0, cp = 0, cl = 0, steps_done = 0;
@@ -448,10 +449,9 @@ static int build(rq_batch* b) {
   if (mixed) {  // allocated up front, so a promotion during a solve allocates and synchronises nothing
     b->hin64 = b->hin;
     for (int q = 0; q < n; ++q) BRC(alloc_fields(b, b->hin64[q], sizeof(double)));
-    BALLOC(b->din64, sizeof(BInst) * n);
-    BCK(cudaMemcpyAsync(b->din64, b->hin64.data(), sizeof(BInst) * n, cudaMemcpyHostToDevice, b->st));
-    // the fp32 instances read their energy with the FP64 K of their promotion set (computed by
-    // initialisation): the f32 rounding of K then enters the readout at second order only
+    // the fp32 instances read their energy with the FP64 K of their promotion set (written by the
+    // potential pass of initialisation): the f32 rounding of K then enters the readout at second
+    // order only
     for (int q = 0; q < n; ++q)
       if (!b->f64[q]) b->hin[q].K64 = (const double*)b->hin64[q].K;
     BCK(cudaMemcpyAsync(b->din, b->hin.data(), sizeof(BInst) * n, cudaMemcpyHostToDevice, b->st));
@@ -648,14 +648,6 @@ static int b_initialize(rq_batch* b) {
     BCK(cudaMemsetAsync(I.U[1], 0, es * I.g.S3, b->st));
     for (int k = 0; k < 2; ++k) BCK(cudaMemsetAsync(I.P[k], 0, es * I.g.S3, b->st));
     BCK(launch_fill(I.W, 1.0f, I.g.S3, b->st));
-  }
-  if (b->din64) {  // the FP64 K that promoted instances use
-    std::vector<BItem> f1;
-    for (int q = 0; q < b->n; ++q) f1.insert(f1.end(), b->items[q].flat1.begin(), b->items[q].flat1.end());
-    BRC(upload_plan(b, b->one, f1));
-    kb_potential<double><<<b->one.n, 256, 0, b->st>>>(b->din64, b->one.d, b->cfg.sigma);
-    BL("potential");
-    BCK(cudaStreamSynchronize(b->st));  // f1 is the source of an asynchronous copy
   }
   BRC(b_normalize(b));
   for (int v = 0; v < 10; ++v) BRC(each_set([&](auto tag, int p) { return b_vcycle<decltype(tag)>(b, p); }));

@@ -132,6 +132,7 @@ static int upload_atoms(rq_ctx* c) {
 
 static void free_ctx(rq_ctx* c) {
   nm_adj_free(c);
+  nm_ff_free(c);
   for (auto e : c->evpool) cudaEventDestroy(e);
   for (auto& gx : c->graph)
     if (gx) cudaGraphExecDestroy(gx);
@@ -795,7 +796,8 @@ extern "C" int rq_nuclear_terms(rq_ctx* c, double* E_KK, double* F) {
   } else if (c->cfg.flavor == RQ_FLAVOR_MOLECULE_JS) {
     mj_nuclear_terms(c, &e, f.data());
   } else {
-    nm_nuclear_terms(c, &e, f.data());
+    const int rc = nm_nuclear_terms(c, &e, f.data());
+    if (rc != RQ_OK) return rc;
   }
   if (E_KK) *E_KK = e;
   if (F) std::memcpy(F, f.data(), sizeof(double) * f.size());
@@ -822,7 +824,7 @@ extern "C" int rq_energy(rq_ctx* c, double* out, double* per_domain) {
   }
   if (rc != RQ_OK) return rc;
   double ekk = 0;
-  rq_nuclear_terms(c, &ekk, nullptr);
+  if ((rc = rq_nuclear_terms(c, &ekk, nullptr)) != RQ_OK) return rc;
   out[RQ_E_KK] = ekk;
   out[RQ_E_TOTAL] = out[RQ_E_T] + out[RQ_E_EK] + out[RQ_E_EE] + out[RQ_E_KK];
   // a normalisation since the last readout met a NaN/Inf domain norm (the kernel left that

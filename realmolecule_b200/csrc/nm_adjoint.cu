@@ -5,7 +5,8 @@
 //   [V-cycle]    P <- M P + B f,  f = 2 pi psi^2                 (every poisson_interval steps)
 //   update       psi~ = A psi,  A = I + half_dv L + dt diag(K - 2P)   (L: same-label Laplacian)
 //   [normalise]  psi = c psi~,  c_d = sqrt(Z_d / (h^3 sum_d psi~^2))
-// and the readout is E = sum_d (Z_d / N_d)(T_d + V_eK,d + V_ee,d) with K = K_nuclei(R) + v.
+// and the readout is E = sum_d w_d (T_d + V_eK,d + 2 h^3 sum_d P rho) - (h^3 / 2 pi) sum P (A_h P),
+// w_d = Z_d / N_d, A_h = -lap_h (the P-stationary Hartree form), with K = K_nuclei(R) + v.
 // The reverse sweep starts from dE/dpsi, dE/dP and dE/dK of the readout and applies the
 // transposes step by step, newest first:
 //   normalise^T  lam <- c (lam - (h^3 / Z) psi <psi, lam>_d)
@@ -553,7 +554,7 @@ int adjoint_t(rq_ctx* c, double* F, double* dEdv) {
   }
   if (F) {
     CK(cudaMemsetAsync(c->dF, 0, sizeof(double) * 3 * n, c->st));
-    LAUNCH(RQ_KC_FORCES, 8.0 * ni, nm_force<T>(psi, c->atoms_nm, n, g, c->h, c->sigma, c->dF, c->st, A.gK));
+    if ((rc = nm_gather(c, psi, A.gK)) != RQ_OK) return rc;
     CK(cudaMemcpyAsync(F, c->dF, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->st));
   }
   if (dEdv) CK(cudaMemcpyAsync(dEdv, A.gK, sizeof(double) * S3, cudaMemcpyDefault, c->st));  // host or device

@@ -39,13 +39,31 @@ inline dim3 nm_march_grid(const Geo& g) {
 inline dim3 nm_march_block() { return dim3(kNmTK, kNmTJ, 1); }
 constexpr int kCoarsestThreads = 256; // one block solves the coarsest level (<= 29^3 points)
 
+// FP64 1/sqrt(x) for x in the normal FP32 range: the FP32 hardware estimate y0 (relative error
+// e0 below 2^-21) refined by the binomial series (1 - e)^(-1/2) = 1 + e/2 + 3e^2/8 + O(e^3),
+// e = 1 - x y0^2 (Householder's third-order step for the reciprocal square root).  The truncation
+// is 5e^3/16 < 1e-18 relative, below FP64 rounding; the FP64 work is five FMA-pipe operations
+// where the FP64 reciprocal square root costs a slow-pipe estimate and Newton steps.
+__device__ __forceinline__ double rsqrt_refined(double x) {
+  const double y0 = (double)rsqrtf((float)x);
+  const double e = fma(-x * y0, y0, 1.0);
+  return fma(y0 * e, fma(0.375, e, 0.5), y0);
+}
+
+// Squared distance from which erf(r / (sqrt2 sigma)) is 1 to double precision (r / (sqrt2
+// sigma) >= 6: erfc(6) = 2e-17): beyond it a Gaussian nucleus is a point charge.
+__device__ __forceinline__ double nm_point_r2(double sigma) { return 72.0 * sigma * sigma; }
+
 // ---------------------------------------------------------------------------------------
 // K = sum Z erf(r/(sqrt2 sigma))/r in FP64 (K(0) = Z sqrt(2/pi)/sigma); boundary planes 0.
 // One block of 256 threads covers points [blk*256, blk*256+256); sa: 512 doubles of smem.
+// K64 (optional): the same sums kept in FP64 (the fp32 fields' readout copy), from the same
+// pass.
 // ---------------------------------------------------------------------------------------
 template <typename T>
 __device__ __forceinline__ void nm_potential_body(T* __restrict__ K, const double* __restrict__ at, int nAt,
-                                                  const Geo& g, double h, double sigma, long long blk, double* sa) {
+                                                  const Geo& g, double h, double sigma, long long blk, double* sa,
+                                                  double* __restrict__ K64 = nullptr) {
   const long long id = blk * blockDim.x + threadIdx.x;
   const bool inside = id < g.S3;
   int i = 0, j = 0, k = 0;
@@ -53,6 +71,7 @@ __device__ __forceinline__ void nm_potential_body(T* __restrict__ K, const doubl
   const bool interior = inside && i >= 1 && i < g.NN && j >= 1 && j < g.NN && k >= 1 && k < g.NN;
   const double x = i * h, y = j * h, z = k * h;
   const double inv = 1.0 / (1.4142135623730951 * sigma), c0 = 0.7978845608028654 / sigma;  // sqrt(2/pi)
+  const double rp2 = nm_point_r2(sigma);
   double v = 0.0;
   for (int base = 0; base < nAt; base += 128) {
     const int cnt = min(128, nAt - base);
@@ -64,18 +83,19 @@ __device__ __forceinline__ void nm_potential_body(T* __restrict__ K, const doubl
       const double Z = sa[m * 4 + 3];
       if (Z <= 0.0) continue;
       const double dx = x - sa[m * 4 + 0], dy = y - sa[m * 4 + 1], dz = z - sa[m * 4 + 2];
-      const double r2 = dx * dx + dy * dy + dz * dz;
-      // erf(r inv) is 1 to double precision from r inv = 6 on: there the term is Z / r, formed
-      // with the FP64 reciprocal square root (no divide)
-      if (r2 * inv * inv >= 36.0) {
-        v += Z * rsqrt(r2);
+      const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+      if (r2 >= rp2) {  // point charge: Z / r
+        v = fma(Z, rsqrt_refined(r2), v);
       } else {
         const double r = sqrt(r2);
         v += (r < 1e-12) ? Z * c0 : Z * erf(r * inv) / r;
       }
     }
   }
-  if (inside) K[id] = interior ? (T)v : T(0);
+  if (inside) {
+    K[id] = interior ? (T)v : T(0);
+    if (K64) K64[id] = interior ? v : 0.0;
+  }
 }
 
 // initial state: nearest domain seed (f32 squared distances, first wins ties), psi = exp(-d)
@@ -484,21 +504,23 @@ __device__ __forceinline__ void nm_evolve_body(const int* __restrict__ labIn, in
   }
 }
 
-// Gaussian-nucleus force: tiles t = t0, t0+stride, ... of interior points staged in smem (in
-// the field type), thread = nucleus a of chunk `chunk`.  With gw == nullptr the Hellmann-Feynman
-// gather F_a = -h^3 sum rho dK/dr (x-R)/r; with a weight field gw = dE/dK (one value per grid
-// point) the gradient gather F_a = -dE/dR_a = sum gw dK_a/dr (x-R)/r, of which the first is the
-// case gw = -h^3 rho.
+// Gaussian-nucleus force: tiles t = t0, t0+stride, ... of interior points staged in smem as FP64
+// (x, y, z, weight) whatever the field type, thread = nucleus a of chunk `chunk`.  With gw ==
+// nullptr the Hellmann-Feynman gather F_a = -h^3 sum rho dK/dr (x-R)/r; with a weight field gw =
+// dE/dK (one value per grid point) the gradient gather F_a = -dE/dR_a = sum gw dK_a/dr (x-R)/r,
+// of which the first is the case gw = -h^3 rho.  The per-nucleus factor (weight scale x Z) is
+// applied once, after the sums.
 template <typename T>
 __device__ __forceinline__ void nm_force_body(const T* __restrict__ U, const double* __restrict__ at, int nAt,
                                               const Geo& g, double h, double sigma, double* __restrict__ F,
-                                              long long t0, long long tstride, int chunk, T* sx, T* sy, T* sz, T* sr,
-                                              const double* __restrict__ gw = nullptr) {
+                                              long long t0, long long tstride, int chunk, double* sx, double* sy,
+                                              double* sz, double* sr, const double* __restrict__ gw = nullptr) {
   const int a = chunk * blockDim.x + threadIdx.x;
   const bool valid = a < nAt && at[a * 4 + 3] > 0.0;
   const double Z = valid ? at[a * 4 + 3] : 0.0;
   const double ax = valid ? at[a * 4 + 0] : 0.0, ay = valid ? at[a * 4 + 1] : 0.0, az = valid ? at[a * 4 + 2] : 0.0;
   const double inv = 1.0 / (1.4142135623730951 * sigma), gs = 0.7978845608028654 / sigma;
+  const double inv2 = inv * inv, rp2 = nm_point_r2(sigma);
   const double h3 = h * h * h;
   const long long n1 = g.NN - 1, nInt = n1 * n1 * n1;
   const long long ntiles = (nInt + kNmForceTile - 1) / kNmForceTile;
@@ -507,48 +529,47 @@ __device__ __forceinline__ void nm_force_body(const T* __restrict__ U, const dou
     __syncthreads();
     for (int q = threadIdx.x; q < kNmForceTile; q += blockDim.x) {
       const long long v = t * kNmForceTile + q;
-      T wt = T(0), x = T(0), y = T(0), z = T(0);
+      double wt = 0.0, x = 0.0, y = 0.0, z = 0.0;
       if (v < nInt) {
         const int i = 1 + (int)(v / (n1 * n1)), j = 1 + (int)((v / n1) % n1), k = 1 + (int)(v % n1);
         const long long id = (long long)i * g.S2 + (long long)j * g.S + k;
         if (gw) {
-          wt = (T)gw[id];
+          wt = gw[id];
         } else {
           const double u = (double)U[id];
-          wt = (T)(u * u);
+          wt = u * u;
         }
-        x = (T)(i * h); y = (T)(j * h); z = (T)(k * h);
+        x = i * h; y = j * h; z = k * h;
       }
       sx[q] = x; sy[q] = y; sz[q] = z; sr[q] = wt;
     }
     __syncthreads();
     if (valid) {
-      const double wscale = gw ? 1.0 : -h3;  // HF: the staged value is rho, its weight -h^3 rho
-      double lx = 0, ly = 0, lz = 0;
+      double lx = 0, ly = 0, lz = 0;  // sum weight x (dK/dr / Z) (x - R) / r
       for (int q = 0; q < kNmForceTile; ++q) {
         const double s = sr[q];
-        if (s == 0.0) continue;
-        const double dx = (double)sx[q] - ax, dy = (double)sy[q] - ay, dz = (double)sz[q] - az;
-        const double r2 = dx * dx + dy * dy + dz * dz;
-        if (r2 < 1e-24) continue;
+        const double dx = sx[q] - ax, dy = sy[q] - ay, dz = sz[q] - az;
+        const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
         double w;
-        if (r2 * inv * inv >= 36.0) {  // Coulomb tail: dK/dr / r = -Z / r^3
-          const double ir = rsqrt(r2);
-          w = -wscale * s * Z * (ir * ir * ir);
+        if (r2 >= rp2) {  // point charge: dK/dr / r = -Z / r^3
+          const double ir = rsqrt_refined(r2);
+          w = -s * (ir * ir * ir);
+        } else if (r2 < 1e-24) {
+          w = 0.0;
         } else {
           const double r = sqrt(r2);
-          const double dKdr = Z * (gs * exp(-r2 * inv * inv) / r - erf(r * inv) / r2);
-          w = wscale * s * dKdr / r;
+          w = s * (gs * exp(-r2 * inv2) / r - erf(r * inv) / r2) / r;
         }
-        lx += w * dx; ly += w * dy; lz += w * dz;
+        lx = fma(w, dx, lx); ly = fma(w, dy, ly); lz = fma(w, dz, lz);
       }
       fx += lx; fy += ly; fz += lz;
     }
   }
   if (valid) {
-    atomicAdd(&F[a * 3 + 0], fx);
-    atomicAdd(&F[a * 3 + 1], fy);
-    atomicAdd(&F[a * 3 + 2], fz);
+    const double f = (gw ? 1.0 : -h3) * Z;  // HF: the staged value is rho, its weight -h^3 rho
+    atomicAdd(&F[a * 3 + 0], f * fx);
+    atomicAdd(&F[a * 3 + 1], f * fy);
+    atomicAdd(&F[a * 3 + 2], f * fz);
   }
 }
 

@@ -203,11 +203,12 @@ __global__ void __launch_bounds__(256) k_nm_add_f2d(double* __restrict__ K, cons
 
 template <typename T>
 static int nm_potential_t(rq_ctx* c) {
-  LAUNCH(RQ_KC_OTHER, sizeof(T) * c->g.S3,
-         nm_potential<T>((T*)c->K, c->atoms_nm, c->n_atoms, c->g, c->h, c->sigma, c->st));
+  // fp32 fields: the readout's FP64 copy comes from the same pass
+  double* K64 = (!c->fp64 && c->K64) ? c->K64 : nullptr;
+  int rc = nm_nuclear_potential(c, c->K, K64);
+  if (rc != RQ_OK) return rc;
   if (c->Kext) LAUNCH(RQ_KC_OTHER, 3.0 * sizeof(T) * c->g.S3, nm_add<T>((T*)c->K, (const T*)c->Kext, c->g.S3, c->st));
-  if (!c->fp64 && c->K64) {  // the readout's FP64 copy
-    LAUNCH(RQ_KC_OTHER, 8.0 * c->g.S3, nm_potential<double>(c->K64, c->atoms_nm, c->n_atoms, c->g, c->h, c->sigma, c->st));
+  if (K64) {
     if (c->Kext)
       LAUNCH(RQ_KC_OTHER, 20.0 * c->g.S3,
              (k_nm_add_f2d<<<148 * 8, 256, 0, c->st>>>(c->K64, (const float*)c->Kext, c->g.S3), cudaGetLastError()));
@@ -378,24 +379,50 @@ int nm_promote(rq_ctx* c) {
   return cudaStreamSynchronize(c->st) == cudaSuccess ? RQ_OK : rq_cuda(c, cudaGetLastError(), "promotion to FP64");
 }
 
-void nm_nuclear_terms(rq_ctx* c, double* E, double* F) {
-  // point-charge nuclear repulsion between entries with Z_nuc > 0 (bohr)
-  double e = 0;
-  const double h = c->h;
-  for (int a = 0; a < c->n_atoms; ++a) {
-    const rq_atom& A = c->atoms[a];
-    if (A.Z_nuc <= 0) continue;
-    for (int b = 0; b < c->n_atoms; ++b) {
-      const rq_atom& B = c->atoms[b];
-      if (b == a || B.Z_nuc <= 0) continue;
-      const double dx = (A.i - B.i) * h, dy = (A.j - B.j) * h, dz = (A.k - B.k) * h;
-      const double r2 = dx * dx + dy * dy + dz * dz, r = std::sqrt(r2);
-      if (b > a) e += A.Z_nuc * B.Z_nuc / r;
-      const double w = A.Z_nuc * B.Z_nuc / (r2 * r);
-      F[a * 3] += w * dx; F[a * 3 + 1] += w * dy; F[a * 3 + 2] += w * dz;
+// Point-charge nuclear repulsion between entries with Z_nuc > 0 (bohr): thread a sums over all b
+// != a (each pair enters twice; the energy is half the per-entry sums, added in entry order).
+__global__ void __launch_bounds__(256) k_nm_nuclear(const double* __restrict__ at, int n, double* __restrict__ out) {
+  __shared__ double sa[256 * 4];
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = a < n && at[a * 4 + 3] > 0.0;
+  const double X = valid ? at[a * 4] : 0.0, Y = valid ? at[a * 4 + 1] : 0.0, Z = valid ? at[a * 4 + 2] : 0.0;
+  const double Za = valid ? at[a * 4 + 3] : 0.0;
+  double e = 0, fx = 0, fy = 0, fz = 0;
+  for (int base = 0; base < n; base += 256) {
+    const int cnt = min(256, n - base);
+    __syncthreads();
+    for (int q = threadIdx.x; q < cnt * 4; q += blockDim.x) sa[q] = at[base * 4 + q];
+    __syncthreads();
+    if (!valid) continue;
+    for (int m = 0; m < cnt; ++m) {
+      const double Zb = sa[m * 4 + 3];
+      if (Zb <= 0.0 || base + m == a) continue;
+      const double dx = X - sa[m * 4], dy = Y - sa[m * 4 + 1], dz = Z - sa[m * 4 + 2];
+      const double r2 = dx * dx + dy * dy + dz * dz, r = sqrt(r2), zz = Za * Zb;
+      e += zz / r;
+      const double w = zz / (r2 * r);
+      fx += w * dx; fy += w * dy; fz += w * dz;
     }
   }
-  *E = e;
+  if (a < n) { out[a * 4] = e; out[a * 4 + 1] = fx; out[a * 4 + 2] = fy; out[a * 4 + 3] = fz; }
+}
+
+int nm_nuclear_terms(rq_ctx* c, double* E, double* F) {
+  const int n = c->n_atoms;
+  *E = 0;
+  if (n <= 0) return RQ_OK;
+  LAUNCH(RQ_KC_FORCES, 32.0 * n, (k_nm_nuclear<<<(n + 255) / 256, 256, 0, c->st>>>(c->atoms_nm, n, c->dpd),
+                                  cudaGetLastError()));
+  std::vector<double> o((size_t)4 * n);
+  CK(cudaMemcpyAsync(o.data(), c->dpd, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  double e = 0;
+  for (int a = 0; a < n; ++a) {
+    e += o[a * 4];
+    F[a * 3] += o[a * 4 + 1]; F[a * 3 + 1] += o[a * 4 + 2]; F[a * 3 + 2] += o[a * 4 + 3];
+  }
+  *E = 0.5 * e;
+  return RQ_OK;
 }
 
 // The readout.  Per domain d with norm N_d and charge Z_d the state is read as if exactly
@@ -448,12 +475,7 @@ int nm_forces(rq_ctx* c, int method, double* F) {
   int frc = nm_ready(c);
   if (frc != RQ_OK) return frc;
   CK(cudaMemsetAsync(c->dF, 0, sizeof(double) * 3 * n, c->st));
-  if (c->fp64)
-    LAUNCH(RQ_KC_FORCES, 8 * interior(c->g),
-           nm_force<double>((const double*)c->U[c->cu], c->atoms_nm, n, c->g, c->h, c->sigma, c->dF, c->st));
-  else
-    LAUNCH(RQ_KC_FORCES, 4 * interior(c->g),
-           nm_force<float>((const float*)c->U[c->cu], c->atoms_nm, n, c->g, c->h, c->sigma, c->dF, c->st));
+  if ((frc = nm_gather(c, c->U[c->cu], nullptr)) != RQ_OK) return frc;
   CK(cudaMemcpyAsync(F, c->dF, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   return RQ_OK;

@@ -9,9 +9,10 @@
 namespace rq {
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_nm_potential(T* K, const double* at, int nAt, Geo g, double h, double sigma) {
+__global__ void __launch_bounds__(256) k_nm_potential(T* K, const double* at, int nAt, Geo g, double h, double sigma,
+                                                      double* K64) {
   __shared__ double sa[128 * 4];
-  nm_potential_body<T>(K, at, nAt, g, h, sigma, blockIdx.x, sa);
+  nm_potential_body<T>(K, at, nAt, g, h, sigma, blockIdx.x, sa, K64);
 }
 
 template <typename T>
@@ -120,7 +121,7 @@ __global__ void __launch_bounds__(256) k_nm_evolve(const int* labIn, int* labOut
 template <typename T>
 __global__ void __launch_bounds__(256) k_nm_force(const T* U, const double* at, int nAt, Geo g, double h, double sigma,
                                                   double* F, const double* gw) {
-  __shared__ T sx[kNmForceTile], sy[kNmForceTile], sz[kNmForceTile], sr[kNmForceTile];
+  __shared__ double sx[kNmForceTile], sy[kNmForceTile], sz[kNmForceTile], sr[kNmForceTile];
   nm_force_body<T>(U, at, nAt, g, h, sigma, F, blockIdx.x, gridDim.x, blockIdx.y, sx, sy, sz, sr, gw);
 }
 
@@ -136,8 +137,9 @@ __global__ void k_nm_add(T* __restrict__ K, const T* __restrict__ v, long long n
 static unsigned nblk(long long n, long long b = 256) { return (unsigned)((n + b - 1) / b); }
 
 template <typename T>
-cudaError_t nm_potential(T* K, const double* at, int nAt, const Geo& g, double h, double sigma, cudaStream_t st) {
-  k_nm_potential<T><<<nblk(g.S3), 256, 0, st>>>(K, at, nAt, g, h, sigma);
+cudaError_t nm_potential(T* K, const double* at, int nAt, const Geo& g, double h, double sigma, cudaStream_t st,
+                         double* K64) {
+  k_nm_potential<T><<<nblk(g.S3), 256, 0, st>>>(K, at, nAt, g, h, sigma, K64);
   return cudaGetLastError();
 }
 template <typename T>
@@ -258,7 +260,7 @@ cudaError_t nm_add(T* K, const T* v, long long n, cudaStream_t st) {
 
 #define RQ_NM_INSTANTIATE(T)                                                                                          \
   template cudaError_t nm_add<T>(T*, const T*, long long, cudaStream_t);                                           \
-  template cudaError_t nm_potential<T>(T*, const double*, int, const Geo&, double, double, cudaStream_t);           \
+  template cudaError_t nm_potential<T>(T*, const double*, int, const Geo&, double, double, cudaStream_t, double*);  \
   template cudaError_t nm_init<T>(T*, int*, const float4*, int, const Geo&, float, cudaStream_t);                   \
   template cudaError_t nm_update<T>(const T*, T*, const T*, const T*, const int*, const Geo&, T, T, double, int,     \
                                     double*, cudaStream_t, const double*, const unsigned*, unsigned*);               \

@@ -45,9 +45,25 @@ struct rq_adj {
   double* wq = nullptr;               // per-domain (Z/N, Q/N) of the energy readout
 };
 
+// Tiled nuclear sums of the new flavour (nm_farfield.cu): tiles of <= 32^3 interior points,
+// per tile the list of near nuclei and 16^3 Chebyshev node values / weights.
+struct rq_ff {
+  bool active = false;          // K and the gathers use the tiles for the current nuclei
+  int nt = 0, base = 0, rem = 0, nTiles = 0;
+  int nNuc = 0, capNuc = 0, capTiles = 0;
+  double* nuc = nullptr;        // nNuc x (x, y, z, Z) bohr: the entries with Z_nuc > 0
+  int* entry = nullptr;         // nNuc: their entry indices
+  int* near_idx = nullptr;      // nTiles x nNuc: per tile the near nuclei, in order
+  int* near_cnt = nullptr;      // nTiles
+  double* nodes = nullptr;      // nTiles x 16^3: far-field node values (K) or node weights (gathers)
+  double* tabs = nullptr;       // Chebyshev nodes and the Lagrange tables of every tile size
+  double* Fraw = nullptr;       // nNuc x 3: the gathers' raw sums
+};
+
 struct rq_ctx {
   rq_config cfg{};
   rq_adj adj;
+  rq_ff ff;
   rq::Geo g{};
   double h = 0, h2 = 0, h3 = 0, dv = 0, dt = 0, half_dv = 0, sigma = 0;
   int n_atoms = 0;

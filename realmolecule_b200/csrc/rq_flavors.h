@@ -46,4 +46,10 @@ int nm_adj_record_scale(rq_ctx* c);           // after the normalisation scale o
 void nm_adj_record_label(rq_ctx* c);          // a label pass followed the step
 int nm_adjoint(rq_ctx* c, double* F, double* dEdv);
 void nm_adj_free(rq_ctx* c);
-void nm_nuclear_terms(rq_ctx* c, double* E, double* F);
+int nm_nuclear_terms(rq_ctx* c, double* E, double* F);
+// nuclear sums (nm_farfield.cu): K (field type, and K64 when given) for the current nuclei, tiled
+// or direct by cfg.nuclear_sum; a force gather over psi (weight rho) or over gw = dE/dK, added
+// into c->dF; the tiles' buffers
+int nm_nuclear_potential(rq_ctx* c, void* K, double* K64);
+int nm_gather(rq_ctx* c, const void* U, const double* gw);
+void nm_ff_free(rq_ctx* c);

@@ -122,7 +122,9 @@ cudaError_t launch_mj_accum_norms(const float* U, const int* label, const Geo& g
 // read as h^3 sum P rho it jittered at ~1e-9 |E|, which needed promotion at 3e-9 |E|.
 constexpr double kMixedFloor = 1e-12;
 template <typename T>
-cudaError_t nm_potential(T* K, const double* at, int nAt, const Geo& g, double h, double sigma, cudaStream_t st);
+// K64 (optional): FP64 copy of the same sums, from the same pass
+cudaError_t nm_potential(T* K, const double* at, int nAt, const Geo& g, double h, double sigma, cudaStream_t st,
+                         double* K64 = nullptr);
 template <typename T>
 cudaError_t nm_init(T* U, int* label, const float4* seeds, int nSeed, const Geo& g, float h, cudaStream_t st);
 template <typename T>

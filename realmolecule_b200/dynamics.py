@@ -130,12 +130,14 @@ def _main(argv=None):
     model.ctx.step(pre)  # converge the electrons at the start geometry
     model.ctx.synchronize()
     t_init = time.perf_counter() - t0
-    # one evaluation split into its parts (synchronised wall clock)
-    parts = {}
+    # one evaluation split into its parts (synchronised wall clock; per kernel class, CUDA events)
+    parts, kernels = {}, {}
     for name, fn in (("set_atoms_ms", lambda: model.ctx.set_atoms(model._rows(g.xyz + off))),
                      ("iters_ms", lambda: model.ctx.step(iters)), ("energy_ms", lambda: model.ctx.energy()),
                      ("forces_ms", lambda: model.ctx.forces(L.FORCE_ADJOINT))):
+        model.ctx.profile_begin()
         t1 = time.perf_counter(); fn(); model.ctx.synchronize(); parts[name] = (time.perf_counter() - t1) * 1e3
+        kernels[name] = {k: round(v["ms"], 3) for k, v in model.ctx.profile_end().items()}
     m = masses_for(Z)
     t0 = time.perf_counter()
     if a.workload == "water100":
@@ -152,7 +154,7 @@ def _main(argv=None):
     print(json.dumps({"workload": a.workload, "forces": a.forces, "grid": f"{g.NN}^3", "nuclei": len(Z),
                       "domains": len(g.seeds),
                       "iters_per_step": iters, "preconverge_steps": pre, "steps": nstep, "init_s": t_init, "s": dt,
-                      "evaluation_parts": parts,
+                      "evaluation_parts": parts, "evaluation_kernel_ms": kernels,
                       "ms_per_geometry_step": dt / max(1, nstep) * 1e3, **out}), flush=True)
 
 
