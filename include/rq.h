@@ -105,7 +105,12 @@ typedef struct rq_config {
                                direct, the rest through a 16^3-node Chebyshev interpolant of their Coulomb
                                field (K within 1e-12 relative of the direct sum; the force gather is its exact
                                transpose) */
-  int32_t reserved[2];
+  int32_t batch_persistent; /* rq_batch_*: 0 = one launch per kernel and phase, the period captured as one CUDA
+                               graph (default: measured fastest on B200); 1 = each schedule period is ONE
+                               persistent cooperative launch (blocks take chunks of (instance, tile) items from
+                               one queue; an item waits, bounded, only for its instance's previous phase).
+                               rq_batch_autotune times both and keeps the faster. */
+  int32_t reserved[1];
 } rq_config;
 
 /* One entry of the reference atom list: a nucleus and/or one electron domain. */
@@ -320,6 +325,15 @@ RQ_API int rq_batch_solve(rq_batch* b, double tol_dE, int32_t max_steps, int32_t
 RQ_API int rq_batch_info(const rq_batch* b, int32_t* n_inst, int64_t* total_points, int64_t* interior_points,
                          int64_t* kernel_launches);
 RQ_API int rq_batch_synchronize(rq_batch* b);
+
+/* Bounds of the persistent batch launch's waits (batch_persistent = 1; no reference counterpart: the
+ * reference steps one molecule at a time).  An item of the launch waits until its instance's previous
+ * phase is complete; every such wait gives up after limit_ns nanoseconds (default 2e9) and then every
+ * block leaves the launch; the next readout (rq_batch_energy, rq_batch_solve) returns RQ_ETIMEOUT, and
+ * the state must be re-initialised.  extra_arrivals > 0 makes every wait need that many completions
+ * more than there are, so every wait runs out (a test of the timeout path on a healthy device).  Drops
+ * the captured periods. */
+RQ_API int rq_batch_set_wait(rq_batch* b, int64_t limit_ns, int32_t extra_arrivals);
 
 /* ---- atom.js per-shell solver (atom.js:1-346) ----------------------------------------------
  * Replaces atom.js's module state and physicsStep(): one U (density amplitude), W (front) and P

@@ -71,7 +71,7 @@ class Config(C.Structure):
                 ("boundary_speed", C.c_double), ("curv_reg", C.c_double), ("sigma", C.c_double),
                 ("label_until", C.c_int32), ("chebyshev", C.c_int32), ("lobpcg", C.c_int32),
                 ("converge_checks", C.c_int32), ("fp32_rounding", C.c_int32), ("nuclear_sum", C.c_int32),
-                ("reserved", C.c_int32 * 2)]
+                ("batch_persistent", C.c_int32), ("reserved", C.c_int32 * 1)]
 
 
 class Split(C.Structure):
@@ -143,6 +143,7 @@ SIGNATURES = {
     "rq_batch_info": (C.c_int, [_V, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                 C.POINTER(C.c_int64)]),
     "rq_batch_synchronize": (C.c_int, [_V]),
+    "rq_batch_set_wait": (C.c_int, [_V, C.c_int64, _I]),
     "rq_shells_create": (C.c_int, [_P, _P, _I, _P]),
     "rq_shells_destroy": (None, [_V]),
     "rq_shells_last_error": (C.c_char_p, [_V]),

@@ -1,7 +1,9 @@
 """Batches of independent new-flavour instances with uneven grids (rq_batch_* of include/rq.h).
 
-All instances step in lockstep; every kernel of the schedule is one launch over an
-(instance, tile) work list, and a schedule period of the whole batch is one CUDA-graph replay.
+All instances step in lockstep.  A schedule period of the whole batch is one CUDA-graph replay:
+one launch per kernel and phase over the (instance, tile) work lists, or (batch_persistent=1)
+ONE persistent cooperative launch whose blocks take chunks of items from a queue, each item
+waiting (bounded) only for its own instance's previous phase.
 """
 from __future__ import annotations
 
@@ -65,6 +67,11 @@ class Batch:
     def synchronize(self):
         self._chk(self.lib.rq_batch_synchronize(self.b), "rq_batch_synchronize")
 
+    def set_wait(self, limit_ns: int, extra_arrivals: int = 0):
+        """Bound of the persistent launch's waits; extra_arrivals > 0 makes every wait run out (the
+        next readout raises RqError with RQ_ETIMEOUT)."""
+        self._chk(self.lib.rq_batch_set_wait(self.b, int(limit_ns), int(extra_arrivals)), "rq_batch_set_wait")
+
     def energy(self) -> np.ndarray:
         out = np.zeros((self.n, L.ENERGY_LEN))
         self._chk(self.lib.rq_batch_energy(self.b, out.ctypes.data), "rq_batch_energy")
@@ -91,8 +98,9 @@ class Batch:
 def _main(argv=None):
     """Step the seeded 96-water-cluster batch (realmolecule_b200.configs.clusters96) on cuda:0.
 
-    python -m realmolecule_b200.batch [--instances N] [--steps K] [--precision mixed|fp64]
-    Prints the batch size and the wall time of the K steps (after initialisation)."""
+    python -m realmolecule_b200.batch [--instances N] [--steps K] [--precision mixed|fp64] [--persistent]
+    Prints the batch size and the wall time of the K steps (after initialisation and 40 warm-up
+    steps, which capture the periods)."""
     import argparse
     import time
 
@@ -101,11 +109,14 @@ def _main(argv=None):
     ap.add_argument("--instances", type=int, default=96)
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--precision", default="mixed", choices=sorted(PRECISIONS))
+    ap.add_argument("--persistent", action="store_true", help="one persistent launch per period")
     a = ap.parse_args(argv)
     geoms = configs.clusters96()[:a.instances]
     b = Batch([{"NN": g.NN, "screen": g.screen, "atoms": configs.to_domain_atoms(g)} for g in geoms],
-              precision=a.precision, label_until=1)
+              precision=a.precision, label_until=1, batch_persistent=1 if a.persistent else 0)
     b.initialize()
+    b.step(40)
+    b.synchronize()
     t0 = time.perf_counter()
     b.step(a.steps)
     b.synchronize()

@@ -41,6 +41,7 @@ struct BInst {
   const float4* seeds;
   int nSeed;
   const double* K64;  // fp32 instances of a mixed batch: the FP64 K of its promotion set, read by the readout
+  double* cs;         // FP64 working copy of the coarsest level (P and f) for the persistent launch
 };
 
 struct BItem {
@@ -214,6 +215,213 @@ __global__ void __launch_bounds__(256) kb_force(const BInst* __restrict__ ins, c
                    it.by, it.bz, sx, sy, sz, sr);
 }
 
+// ---------------------------------------------------------------------------------------
+// The persistent form of a schedule period: ONE launch runs the period's phases (the same
+// phases, work lists and bodies as the per-kernel launches above, for both precision sets).
+// The items of all phases form one queue, phase after phase and instance after instance within
+// a phase; blocks take runs of items from it with one atomic counter.  Every dependency of the
+// schedule is within one instance, so an item waits only until its instance's previous non-empty
+// phase is complete (a completion counter per (phase, instance)) -- no grid-wide barrier, and
+// instances overlap across phases.  Items are taken in queue order, so every item an item waits
+// for was taken earlier by a running block: the waits always end.  Each wait is bounded all the
+// same (a limit on the global timer): a block that gives up sets bit 1 of the error word and
+// leaves, every other block leaves at its next wait, and the host reports RQ_ETIMEOUT.
+// ---------------------------------------------------------------------------------------
+enum BPhaseKind : int {
+  kPhApply, kPhZeroNorms, kPhUpdate, kPhUpdateAcc, kPhScale, kPhRbgs, kPhCoarsest, kPhResidual, kPhRestrict,
+  kPhZero, kPhProlong, kPhEvolve
+};
+
+struct BPhase {
+  int kind, set;          // BPhaseKind; precision set (0: fp32 fields, 1: FP64)
+  int lev, color;         // multigrid level and colour
+  int cu, cp, cl;         // buffer parities in effect
+  int n;                  // items
+  const BItem* items;
+  const double* scale;    // update: the pending per-domain scale it applies (or null)
+  const unsigned* seed;   // update, fp32 unbiased rounding: this step's seed and the next one's slot
+  unsigned* seed_next;
+};
+
+// A queue entry: `count` consecutive items of one instance in one phase, from item `first`.
+struct BChunk {
+  int phase, first, count, inst;
+};
+
+struct BPersist {
+  const BInst* ins;
+  const BPhase* prog;
+  const BChunk* chunks;   // the queue
+  const int2* deps;       // nph x ninst: (previous non-empty phase of the instance or -1, its item count)
+  unsigned* done;         // nph x ninst completed items (zeroed before the launch)
+  unsigned* queue;        // the next queue index (zeroed before the launch)
+  int nph, ninst;
+  unsigned total;         // queue length (chunks)
+  double half_dv, dt;     // update coefficients (every instance of a batch shares h)
+  double* dnorm;          // batch-wide domain norms
+  double* scale;          // batch-wide domain scales
+  const double* Zdom;
+  int sweeps;             // coarsest-level sweeps
+  float dt_w, curv;       // level-set pass
+  int* err;               // bit 0: non-finite norm; bit 1: a wait gave up
+  long long limit_ns;     // bound of every wait
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+template <typename T>
+__device__ __forceinline__ void kb_run_item(const BPersist& a, const BPhase& P, const BItem& it, DomTable<1, 128>& tab) {
+  const BInst& I = a.ins[it.inst];
+  switch (P.kind) {
+    case kPhApply:
+      nm_apply_scale_body<T>((T*)I.U[P.cu], I.lab[P.cl], a.scale + I.dom0, I.g.S3, I.nDom, it.bx);
+      break;
+    case kPhZeroNorms:
+      for (int d = threadIdx.x; d < I.nDom; d += blockDim.x) a.dnorm[I.dom0 + d] = 0.0;
+      break;
+    case kPhScale:
+      for (int d = threadIdx.x; d < I.nDom; d += blockDim.x)
+        a.scale[I.dom0 + d] = nm_domain_scale(a.dnorm[I.dom0 + d], a.Zdom[I.dom0 + d], a.err);
+      break;
+    case kPhUpdate:
+    case kPhUpdateAcc: {
+      const Geo g = I.g;
+      const double* sc = P.scale ? P.scale + I.dom0 : nullptr;
+      if (P.kind == kPhUpdateAcc) {
+        dom_table_init(tab);
+        __syncthreads();
+        nm_update_body<T, true>((const T*)I.U[P.cu], (T*)I.U[1 - P.cu], (const T*)I.K, (const T*)I.P[P.cp], I.lab[P.cl],
+                                g, (T)a.half_dv, (T)a.dt, I.h * I.h * I.h, I.nDom, a.dnorm + I.dom0, tab, it.bx, it.by,
+                                it.bz, sc, P.seed);
+        __syncthreads();
+        dom_table_flush(tab, a.dnorm + I.dom0);
+      } else {
+        nm_update_body<T, false>((const T*)I.U[P.cu], (T*)I.U[1 - P.cu], (const T*)I.K, (const T*)I.P[P.cp],
+                                 I.lab[P.cl], g, (T)a.half_dv, (T)a.dt, I.h * I.h * I.h, I.nDom, nullptr, tab, it.bx,
+                                 it.by, it.bz, sc, P.seed);
+      }
+      break;
+    }
+    case kPhRbgs: {
+      const Geo g = I.lg[P.lev];
+      const T h2 = (T)(I.lh[P.lev] * I.lh[P.lev]);
+      if (P.lev == 0)
+        nm_rbgs_body<T, true>((T*)I.P[P.cp], (const T*)I.U[P.cu], g, h2, P.color, it.bx, it.by, it.bz);
+      else
+        nm_rbgs_body<T, false>((T*)I.lP[P.lev], (const T*)I.lf[P.lev], g, h2, P.color, it.bx, it.by, it.bz);
+      break;
+    }
+    case kPhCoarsest:  // one block per instance; the level's FP64 working copy in the instance's scratch
+      nm_coarsest_body<T>((T*)I.lP[P.lev], (const T*)I.lf[P.lev], I.lg[P.lev], I.lh[P.lev] * I.lh[P.lev], a.sweeps,
+                          I.cs);
+      break;
+    case kPhResidual: {
+      const Geo g = I.lg[P.lev];
+      const T ih2 = (T)(1.0 / (I.lh[P.lev] * I.lh[P.lev]));
+      if (P.lev == 0)
+        nm_residual_rows_body<T, true>((const T*)I.P[P.cp], (const T*)I.U[P.cu], (T*)I.lr[0], g, ih2, it.bx, it.by,
+                                       it.bz);
+      else
+        nm_residual_rows_body<T, false>((const T*)I.lP[P.lev], (const T*)I.lf[P.lev], (T*)I.lr[P.lev], g, ih2, it.bx,
+                                        it.by, it.bz);
+      break;
+    }
+    case kPhRestrict: {
+      const Geo g = I.lg[P.lev], gc = I.lg[P.lev + 1];
+      nm_restrict_body<T>((const T*)I.lr[P.lev], (T*)I.lf[P.lev + 1], g, gc, (long long)it.bx * blockDim.x + threadIdx.x);
+      break;
+    }
+    case kPhZero: {
+      const long long S3 = I.lg[P.lev].S3, base = (long long)it.bx * blockDim.x * kNmFlatChunk;
+      T* p = (T*)I.lP[P.lev];
+      for (int q = 0; q < kNmFlatChunk; ++q) {
+        const long long id = base + (long long)q * blockDim.x + threadIdx.x;
+        if (id < S3) p[id] = T(0);
+      }
+      break;
+    }
+    case kPhProlong: {
+      T* Pf = P.lev == 0 ? (T*)I.P[P.cp] : (T*)I.lP[P.lev];
+      const Geo g = I.lg[P.lev], gc = I.lg[P.lev + 1];
+      nm_prolong_rows_body<T>((const T*)I.lP[P.lev + 1], Pf, g, gc, it.bx, it.by, it.bz);
+      break;
+    }
+    case kPhEvolve: {
+      const Geo g = I.g;
+      nm_evolve_body<T>(I.lab[P.cl], I.lab[1 - P.cl], (const T*)I.U[P.cu], I.W, g, (T)a.dt_w, (T)a.curv, it.bx, it.by,
+                        it.bz);
+      break;
+    }
+    default:
+      break;
+  }
+}
+
+// SETS: the precision sets the program uses (bit 0: fp32 fields, bit 1: FP64), so a batch with
+// one set compiles only that set's bodies (fewer registers).  The next run of items is taken
+// while the block works on the current one.
+template <int SETS>
+__global__ void __launch_bounds__(256, 4) kb_persist(BPersist a) {
+  __shared__ DomTable<1, 128> tab;
+  __shared__ BPhase P;                  // phase of the current chunk
+  __shared__ BChunk C;
+  __shared__ unsigned next;
+  __shared__ int ph, ok_ph, ok_inst, stop;  // (ok_ph, ok_inst): a dependency already seen complete
+  if (threadIdx.x == 0) {
+    ph = -1; ok_ph = -1; ok_inst = -1; stop = 0;
+    next = atomicAdd(a.queue, 1u);
+  }
+  __syncthreads();
+  unsigned q = next;
+  __syncthreads();
+  while (q < a.total) {
+    if (threadIdx.x == 0) {
+      next = atomicAdd(a.queue, 1u);  // in flight during the chunk
+      C = a.chunks[q];
+      if (C.phase != ph) { P = a.prog[C.phase]; ph = C.phase; }
+      if (ph != ok_ph || C.inst != ok_inst) {
+        const int2 d = a.deps[(long long)ph * a.ninst + C.inst];
+        if (d.x >= 0) {
+          const volatile unsigned* c = a.done + (long long)d.x * a.ninst + C.inst;
+          const unsigned long long t0 = global_ns();
+          while (*c < (unsigned)d.y) {
+            if ((*(volatile int*)a.err & 2) || (long long)(global_ns() - t0) > a.limit_ns) {
+              atomicOr(a.err, 2);
+              stop = 1;
+              break;
+            }
+            __nanosleep(32);
+          }
+          __threadfence();
+        }
+        ok_ph = ph; ok_inst = C.inst;
+      }
+    }
+    __syncthreads();
+    if (stop) return;
+    for (int k = 0; k < C.count; ++k) {
+      const BItem it = P.items[C.first + k];
+      if (P.set == 0) {
+        if (SETS & 1) kb_run_item<float>(a, P, it, tab);
+      } else {
+        if (SETS & 2) kb_run_item<double>(a, P, it, tab);
+      }
+      if (P.kind == kPhUpdateAcc || P.kind == kPhCoarsest) __syncthreads();  // shared table / scratch reuse
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(a.done + (long long)ph * a.ninst + C.inst, (unsigned)C.count);
+    }
+    q = next;
+    __syncthreads();
+  }
+}
+
 }  // namespace rq
 
 // =========================================================================================
@@ -232,7 +440,7 @@ constexpr int kF32 = 0, kF64 = 1;
 // Work items of one instance for every list; built once at creation, concatenated by build_plans.
 struct InstItems {
   std::vector<BItem> march[kMaxLev], rbgs[kMaxLev], restr[kMaxLev], zero[kMaxLev], coarse[kMaxLev];
-  std::vector<BItem> flat16, flat1, force;
+  std::vector<BItem> flat16, flat1, force, one;  // one: a single item (per-instance domain work)
 };
 
 struct rq_batch {
@@ -254,7 +462,7 @@ struct rq_batch {
   struct Plan { BItem* d = nullptr; int n = 0, cap = 0; };
   struct Plans {
     Plan march[kMaxLev], rbgs[kMaxLev], restr[kMaxLev], zero[kMaxLev], coarse[kMaxLev];
-    Plan flat16, flat1, force;
+    Plan flat16, flat1, force, one;
   };
   Plans pl[2];
   size_t coarse_smem[kMaxLev] = {};
@@ -271,6 +479,16 @@ struct rq_batch {
   bool pending = false;           // psi awaits the per-domain scale (applied by the next update or a flush)
   int age = 0;                    // updates since psi was last normalised (0: normalised or pending)
   std::string last_error;
+  // persistent launches: a schedule period recorded as a program of phases (rec non-null while
+  // recording), one program per graph key, the queue and completion counters, the launch's grid
+  std::vector<BPhase>* rec = nullptr;
+  struct Prog { BPhase* phases = nullptr; BChunk* chunks = nullptr; int2* deps = nullptr; int n = 0, cap = 0, cap_chunks = 0; };
+  Prog prog[32];
+  unsigned* pcount = nullptr;     // the queue word, then the (phase, instance) completion counters
+  size_t pcount_cap = 0;
+  int pgrid[4] = {};              // co-resident blocks of kb_persist<sets> (0: not yet queried)
+  long long wait_ns = 2000000000LL;
+  int extra_arrivals = 0;
 };
 
 #define BCK(call)                                                                  \
@@ -332,6 +550,7 @@ static void make_items(const BInst& I, int q, InstItems& it) {
     flat_items(it.restr[l], q, nc, 256);
     flat_items(it.zero[l], q, I.lg[l + 1].S3, 256 * kNmFlatChunk);
   }
+  it.one.push_back({q, 0, 0, 0});
   flat_items(it.flat16, q, I.g.S3, 256 * kNmFlatChunk);
   flat_items(it.flat1, q, I.g.S3, 256);
   const long long n1 = I.g.NN - 1, ntiles = (n1 * n1 * n1 + kNmForceTile - 1) / kNmForceTile;
@@ -366,6 +585,7 @@ static int build_plans(rq_batch* b) {
       BRC(gather(P.coarse[l], [l](const InstItems& it) -> const Items& { return it.coarse[l]; }));
     }
     BRC(gather(P.flat16, [](const InstItems& it) -> const Items& { return it.flat16; }));
+    BRC(gather(P.one, [](const InstItems& it) -> const Items& { return it.one; }));
     BRC(gather(P.flat1, [](const InstItems& it) -> const Items& { return it.flat1; }));
     BRC(gather(P.force, [](const InstItems& it) -> const Items& { return it.force; }));
   }
@@ -391,6 +611,7 @@ static int alloc_fields(rq_batch* b, BInst& I, size_t es) {
     }
     if (l < I.nlev - 1) BALLOC(I.lr[l], s3 * es);
   }
+  BALLOC(I.cs, 2 * sizeof(double) * (size_t)I.lg[I.nlev - 1].S3);
   return RQ_OK;
 }
 
@@ -491,6 +712,18 @@ static int each_set(F&& f) {
   return r != RQ_OK ? r : f(double(0), kF64);
 }
 
+// A phase of the period being recorded (persistent launches): kind and work list, with the
+// buffer parities in effect at this point of the schedule.
+static void b_record(rq_batch* b, int kind, int set, const rq_batch::Plan* pl, int lev = 0, int color = 0) {
+  if (!pl || pl->n == 0) return;
+  BPhase x{};
+  x.kind = kind; x.set = set; x.lev = lev; x.color = color;
+  x.cu = b->cu; x.cp = b->cp; x.cl = b->cl;
+  x.n = pl->n;
+  x.items = pl->d;
+  b->rec->push_back(x);
+}
+
 template <typename T>
 static int b_vcycle(rq_batch* b, int p) {
   const rq_batch::Plans& P = b->pl[p];
@@ -498,6 +731,10 @@ static int b_vcycle(rq_batch* b, int p) {
   const dim3 rb(32, 8);
   auto smooth = [&](int l) -> int {
     for (int color = 0; color < 2; ++color) {
+      if (b->rec) {
+        b_record(b, kPhRbgs, p, &P.rbgs[l], l, color);
+        continue;
+      }
       if (l == 0)
         kb_rbgs<T, true><<<P.rbgs[l].n, rb, 0, b->st>>>(b->din, P.rbgs[l].d, l, b->cu, b->cp, color);
       else
@@ -508,12 +745,22 @@ static int b_vcycle(rq_batch* b, int p) {
   };
   for (int l = 0; l < b->maxlev; ++l) {
     if (P.coarse[l].n) {
-      kb_coarsest<T><<<P.coarse[l].n, kCoarsestThreads, b->coarse_smem[l], b->st>>>(b->din, P.coarse[l].d, l,
-                                                                                   b->cfg.mg_coarse_sweeps);
-      BL("coarsest");
+      if (b->rec) {
+        b_record(b, kPhCoarsest, p, &P.coarse[l], l);
+      } else {
+        kb_coarsest<T><<<P.coarse[l].n, kCoarsestThreads, b->coarse_smem[l], b->st>>>(b->din, P.coarse[l].d, l,
+                                                                                     b->cfg.mg_coarse_sweeps);
+        BL("coarsest");
+      }
     }
     if (!P.rbgs[l].n) continue;
     for (int s = 0; s < pre; ++s) BRC(smooth(l));
+    if (b->rec) {
+      b_record(b, kPhResidual, p, &P.rbgs[l], l);
+      b_record(b, kPhRestrict, p, &P.restr[l], l);
+      b_record(b, kPhZero, p, &P.zero[l], l + 1);
+      continue;
+    }
     if (l == 0)
       kb_residual<T, true><<<P.rbgs[l].n, rb, 0, b->st>>>(b->din, P.rbgs[l].d, l, b->cu, b->cp);
     else
@@ -526,8 +773,12 @@ static int b_vcycle(rq_batch* b, int p) {
   }
   for (int l = b->maxlev - 2; l >= 0; --l) {
     if (!P.rbgs[l].n) continue;
-    kb_prolong<T><<<P.rbgs[l].n, rb, 0, b->st>>>(b->din, P.rbgs[l].d, l, b->cp);
-    BL("prolong");
+    if (b->rec) {
+      b_record(b, kPhProlong, p, &P.rbgs[l], l);
+    } else {
+      kb_prolong<T><<<P.rbgs[l].n, rb, 0, b->st>>>(b->din, P.rbgs[l].d, l, b->cp);
+      BL("prolong");
+    }
     for (int s = 0; s < post; ++s) BRC(smooth(l));
   }
   return RQ_OK;
@@ -537,6 +788,10 @@ template <typename T>
 static int b_apply(rq_batch* b, int p) {
   const rq_batch::Plan& f = b->pl[p].flat16;
   if (!f.n) return RQ_OK;
+  if (b->rec) {
+    b_record(b, kPhApply, p, &f);
+    return RQ_OK;
+  }
   kb_apply_scale<T><<<f.n, 256, 0, b->st>>>(b->din, f.d, b->cu, b->cl, b->scale);
   BL("apply_scale");
   return RQ_OK;
@@ -588,7 +843,12 @@ static int b_step(rq_batch* b, int s) {
   // dt = dv h^2 differs per instance only through h: every instance of a batch shares h
   const double hd = 0.5 * b->dv, dt = b->dv * b->hin[0].h * b->hin[0].h;
   const double* sc = b->pending ? b->scale : nullptr;
-  if (norm) BCK(cudaMemsetAsync(b->dnorm, 0, sizeof(double) * b->D, b->st));
+  if (norm) {
+    if (b->rec)
+      for (int p = 0; p < 2; ++p) b_record(b, kPhZeroNorms, p, &b->pl[p].one);
+    else
+      BCK(cudaMemsetAsync(b->dnorm, 0, sizeof(double) * b->D, b->st));
+  }
   BRC(each_set([&](auto tag, int p) -> int {
     using T = decltype(tag);
     const rq_batch::Plan& m = b->pl[p].march[0];
@@ -596,6 +856,13 @@ static int b_step(rq_batch* b, int s) {
     const bool sr = p == kF32 && b->cfg.fp32_rounding == 1;
     const unsigned* sd = sr ? b->rseed + b->cu : nullptr;
     unsigned* sn = sr ? b->rseed + (1 - b->cu) : nullptr;
+    if (b->rec) {
+      b_record(b, norm ? kPhUpdateAcc : kPhUpdate, p, &m);
+      b->rec->back().scale = sc;
+      b->rec->back().seed = sd;
+      b->rec->back().seed_next = sn;
+      return RQ_OK;
+    }
     if (norm)
       kb_update<T, true><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cp, b->cl, (T)hd, (T)dt, b->dnorm,
                                                              sc, sd, sn);
@@ -608,8 +875,12 @@ static int b_step(rq_batch* b, int s) {
   b->cu ^= 1;
   b->pending = false;
   if (norm) {  // applied by the next update (or a flush)
-    BCK(nm_norm_scale<double>(b->dnorm, b->Zdom, b->D, b->scale, b->err, b->st));
-    b->launches++;
+    if (b->rec) {
+      for (int p = 0; p < 2; ++p) b_record(b, kPhScale, p, &b->pl[p].one);
+    } else {
+      BCK(nm_norm_scale<double>(b->dnorm, b->Zdom, b->D, b->scale, b->err, b->st));
+      b->launches++;
+    }
     b->pending = true;
   }
   b->age = norm ? 0 : b->age + 1;
@@ -619,6 +890,10 @@ static int b_step(rq_batch* b, int s) {
       using T = decltype(tag);
       const rq_batch::Plan& m = b->pl[p].march[0];
       if (!m.n) return RQ_OK;
+      if (b->rec) {
+        b_record(b, kPhEvolve, p, &m);
+        return RQ_OK;
+      }
       kb_evolve<T><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cl, (T)(float)f.boundary_speed,
                                                        (T)(float)f.curv_reg);
       BL("evolve");
@@ -780,6 +1055,133 @@ static int b_eager(rq_batch* b, int n) {
   return RQ_OK;
 }
 
+// Items of instance q in a recorded phase (0 when q is not in the phase's work list).
+static int b_phase_items(const rq_batch* b, const BPhase& x, int q) {
+  if (!b->active[q] || (b->f64[q] ? kF64 : kF32) != x.set) return 0;
+  const InstItems& it = b->items[q];
+  switch (x.kind) {
+    case kPhApply: return (int)it.flat16.size();
+    case kPhZeroNorms:
+    case kPhScale: return 1;
+    case kPhUpdate:
+    case kPhUpdateAcc:
+    case kPhEvolve: return (int)it.march[0].size();
+    case kPhRbgs:
+    case kPhResidual:
+    case kPhProlong: return (int)it.rbgs[x.lev].size();
+    case kPhCoarsest: return (int)it.coarse[x.lev].size();
+    case kPhRestrict: return (int)it.restr[x.lev].size();
+    case kPhZero: return (int)it.zero[x.lev - 1].size();
+    default: return 0;
+  }
+}
+
+// One schedule period as ONE persistent launch: the period is recorded as a program of phases
+// (the host state advances exactly as the per-kernel schedule would), with the queue offsets of
+// the phases and, per (phase, instance), the instance's previous non-empty phase and its item
+// count; all uploaded once per graph key.  The graph holds the zeroing of the counters and the
+// cooperative launch of kb_persist over every co-resident block.
+static int b_persist_graph(rq_batch* b, int key, int period) {
+  std::vector<BPhase> prog;
+  b->rec = &prog;
+  const int rc = b_eager(b, period);
+  b->rec = nullptr;
+  if (rc != RQ_OK) return rc;
+  const int nph = (int)prog.size(), ni = b->n;
+  // the queue: per phase, per instance (in work-list order), chunks of up to `per` items, about
+  // 4-16 k points each, so a chunk's bookkeeping (dependency check, fence, count) stays small
+  // against its work
+  std::vector<BChunk> chunks;
+  std::vector<int2> deps((size_t)nph * ni);
+  std::vector<int> last(ni, -1), lastn(ni, 0);
+  for (int k = 0; k < nph; ++k) {
+    const int kind = prog[k].kind;
+    const int per = (kind == kPhRbgs || kind == kPhResidual || kind == kPhProlong) ? 8
+                    : kind == kPhRestrict                                        ? 32
+                    : (kind == kPhCoarsest || kind == kPhZeroNorms || kind == kPhScale) ? 1
+                                                                                 : 2;
+    int first = 0;
+    for (int q = 0; q < ni; ++q) {
+      deps[(size_t)k * ni + q] = make_int2(last[q], lastn[q] + b->extra_arrivals);
+      const int c = b_phase_items(b, prog[k], q);
+      for (int o = 0; o < c; o += per) chunks.push_back({k, first + o, std::min(per, c - o), q});
+      first += c;
+      if (c > 0) { last[q] = k; lastn[q] = c; }
+    }
+    if (first != prog[k].n) {
+      b->last_error = "persistent program: work list and instance item counts disagree";
+      return RQ_EINVAL;
+    }
+  }
+  const int nch = (int)chunks.size();
+  int sets = 0;
+  for (const BPhase& x : prog) sets |= 1 << x.set;
+  if (!sets) sets = 1;
+  void (*kern)(BPersist) = sets == 1 ? kb_persist<1> : sets == 2 ? kb_persist<2> : kb_persist<3>;
+  if (b->pgrid[sets] == 0) {
+    int dev = 0, nsm = 0, per = 0, coop = 0;
+    BCK(cudaGetDevice(&dev));
+    BCK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    BCK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, 0));
+    if (!coop || per < 1) {
+      b->last_error = "the device cannot run the persistent batch launch (set batch_persistent = 0)";
+      return RQ_ENOTSUP;
+    }
+    b->pgrid[sets] = nsm * per;
+  }
+  const int pgrid = b->pgrid[sets];
+  // device copies: program, queue offsets, dependencies (per key), counters (shared by the keys)
+  rq_batch::Prog& G = b->prog[key];
+  if (nph > G.cap || nch > G.cap_chunks) {
+    BALLOC(G.phases, sizeof(BPhase) * nph);
+    BALLOC(G.chunks, sizeof(BChunk) * nch);
+    BALLOC(G.deps, sizeof(int2) * (size_t)nph * ni);
+    G.cap = nph;
+    G.cap_chunks = nch;
+  }
+  G.n = nph;
+  if ((size_t)nph * ni + 1 > b->pcount_cap) {
+    BALLOC(b->pcount, sizeof(unsigned) * ((size_t)nph * ni + 1));
+    b->pcount_cap = (size_t)nph * ni + 1;
+  }
+  BCK(cudaMemcpyAsync(G.phases, prog.data(), sizeof(BPhase) * nph, cudaMemcpyHostToDevice, b->st));
+  BCK(cudaMemcpyAsync(G.chunks, chunks.data(), sizeof(BChunk) * nch, cudaMemcpyHostToDevice, b->st));
+  BCK(cudaMemcpyAsync(G.deps, deps.data(), sizeof(int2) * deps.size(), cudaMemcpyHostToDevice, b->st));
+  BCK(cudaStreamSynchronize(b->st));  // the host vectors are copy sources
+  BPersist a{};
+  a.ins = b->din; a.prog = G.phases; a.chunks = G.chunks; a.deps = G.deps;
+  a.queue = b->pcount; a.done = b->pcount + 1;
+  a.nph = nph; a.ninst = ni;
+  a.total = (unsigned)nch;
+  a.half_dv = 0.5 * b->dv; a.dt = b->dv * b->hin[0].h * b->hin[0].h;
+  a.dnorm = b->dnorm; a.scale = b->scale; a.Zdom = b->Zdom;
+  a.sweeps = b->cfg.mg_coarse_sweeps;
+  a.dt_w = (float)b->cfg.boundary_speed; a.curv = (float)b->cfg.curv_reg;
+  a.err = b->err;
+  a.limit_ns = b->wait_ns;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cudaLaunchConfig_t lc{};
+  lc.gridDim = dim3((unsigned)pgrid);
+  lc.blockDim = dim3(256);
+  lc.dynamicSmemBytes = 0;
+  lc.stream = b->st;
+  lc.attrs = attr;
+  lc.numAttrs = 1;
+  BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+  const cudaError_t e1 = cudaMemsetAsync(b->pcount, 0, sizeof(unsigned) * ((size_t)nph * ni + 1), b->st);
+  const cudaError_t e2 = cudaLaunchKernelEx(&lc, kern, a);
+  cudaGraph_t gr = nullptr;
+  cudaError_t e = cudaStreamEndCapture(b->st, &gr);
+  if (e == cudaSuccess) e = e1 != cudaSuccess ? e1 : e2;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph[key], gr, 0);
+  if (gr) cudaGraphDestroy(gr);
+  BCK(e);
+  return RQ_OK;
+}
+
 extern "C" int rq_batch_step(rq_batch* b, int32_t n) {
   if (!b || n < 0) return RQ_EINVAL;
   const int period = b_period(b);
@@ -801,18 +1203,25 @@ extern "C" int rq_batch_step(rq_batch* b, int32_t n) {
     const int key = b->cu | (b->cp << 1) | (b->cl << 2) | (on << 3) | ((b->pending ? 1 : 0) << 4);
     if (!b->graph[key]) {
       const long long l0 = b->launches;
-      BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
-      int rc = b_eager(b, period);
-      cudaGraph_t gr = nullptr;
-      cudaError_t e = cudaStreamEndCapture(b->st, &gr);
-      if (rc != RQ_OK) {
-        if (gr) cudaGraphDestroy(gr);
-        return rc;
+      // the unbiased rounding's step seed advances on the device between steps, which needs the
+      // steps in order: that schedule keeps the per-kernel launches
+      if (b->cfg.batch_persistent == 1 && b->cfg.fp32_rounding != 1) {
+        BRC(b_persist_graph(b, key, period));
+        b->launches++;
+      } else {
+        BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+        int rc = b_eager(b, period);
+        cudaGraph_t gr = nullptr;
+        cudaError_t e = cudaStreamEndCapture(b->st, &gr);
+        if (rc != RQ_OK) {
+          if (gr) cudaGraphDestroy(gr);
+          return rc;
+        }
+        BCK(e);
+        e = cudaGraphInstantiate(&b->graph[key], gr, 0);
+        cudaGraphDestroy(gr);
+        BCK(e);
       }
-      BCK(e);
-      e = cudaGraphInstantiate(&b->graph[key], gr, 0);
-      cudaGraphDestroy(gr);
-      BCK(e);
       b->graph_post[key] = b->cu | (b->cp << 1) | (b->cl << 2) | ((b->pending ? 1 : 0) << 4) | (b->age << 5);
       b->graph_launches[key] = b->launches - l0;
       BCK(cudaGraphLaunch(b->graph[key], b->st));
@@ -852,9 +1261,14 @@ extern "C" int rq_batch_energy(rq_batch* b, double* out) {
   BCK(cudaMemcpyAsync(pd.data(), b->dpd, sizeof(double) * pd.size(), cudaMemcpyDeviceToHost, b->st));
   BCK(cudaMemcpyAsync(&bad_norm, b->err, sizeof(int), cudaMemcpyDeviceToHost, b->st));
   BCK(cudaStreamSynchronize(b->st));
-  if (bad_norm) {  // a normalisation met a NaN/Inf domain norm and left that domain unscaled
+  if (bad_norm) {  // reported once, then cleared
     BCK(cudaMemsetAsync(b->err, 0, sizeof(int), b->st));
     BCK(cudaStreamSynchronize(b->st));
+    if (bad_norm & 2) {  // a persistent launch gave up at its barrier: the state is not a valid schedule
+      b->last_error = "a bounded wait of the persistent batch launch ran out (rq_batch_set_wait)";
+      return RQ_ETIMEOUT;
+    }
+    // a normalisation met a NaN/Inf domain norm and left that domain unscaled
     b->last_error = "non-finite domain norm in a normalisation";
     return RQ_ENONFINITE;
   }
@@ -1031,6 +1445,16 @@ extern "C" int rq_batch_info(const rq_batch* b, int32_t* n_inst, int64_t* total_
   if (total_points) *total_points = tp;
   if (interior_points) *interior_points = ip;
   if (kernel_launches) *kernel_launches = b->launches;
+  return RQ_OK;
+}
+
+extern "C" int rq_batch_set_wait(rq_batch* b, int64_t limit_ns, int32_t extra_arrivals) {
+  if (!b || limit_ns <= 0 || extra_arrivals < 0) return RQ_EINVAL;
+  BCK(cudaStreamSynchronize(b->st));
+  b->wait_ns = limit_ns;
+  b->extra_arrivals = extra_arrivals;
+  for (auto& g : b->graph)  // the limits are arguments of the captured launches
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   return RQ_OK;
 }
 

@@ -28,6 +28,14 @@ template <> struct Ar<double> {
 constexpr int kNmFlatChunk = 16;     // points per thread of the flat (all S^3) bodies
 constexpr int kNmForceTile = 512;    // interior points staged per force tile
 constexpr int kNmRowPlanes = 4;      // planes i per block of the row-tiled multigrid bodies
+constexpr int kNmRowTJ = 8;           // rows j per block of the row-tiled bodies (block 32 x 8)
+// Thread coordinates of a body written for a block of W threads along x, from the linear thread
+// index: the body runs the same under a 2-D launch of that shape and under a 1-D launch of the
+// same thread count (the persistent batch kernel).
+template <int W>
+__device__ __forceinline__ int tile_x() { return (int)((threadIdx.x + blockDim.x * threadIdx.y) % W); }
+template <int W>
+__device__ __forceinline__ int tile_y() { return (int)((threadIdx.x + blockDim.x * threadIdx.y) / W); }
 // March tile of the new flavour's stencil bodies: 16 (k) x 16 (j) threads, each walking kMarch
 // planes of i.  16 wide rows waste fewer lanes than 32 on the 47..127-point interiors of the
 // cluster grids (a warp still reads two contiguous 64-byte runs).
@@ -48,6 +56,16 @@ __device__ __forceinline__ double rsqrt_refined(double x) {
   const double y0 = (double)rsqrtf((float)x);
   const double e = fma(-x * y0, y0, 1.0);
   return fma(y0 * e, fma(0.375, e, 0.5), y0);
+}
+
+// The scale that brings a domain of norm n to its charge Z (1 for an empty or non-finite domain;
+// a non-finite norm also sets bit 0 of *err).
+__device__ __forceinline__ double nm_domain_scale(double n, double Z, int* err) {
+  if (!isfinite(n)) {
+    atomicOr(err, 1);
+    return 1.0;
+  }
+  return (Z > 0.0 && n > 1e-300) ? sqrt(Z / n) : 1.0;
 }
 
 // Squared distance from which erf(r / (sqrt2 sigma)) is 1 to double precision (r / (sqrt2
@@ -170,8 +188,8 @@ __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __res
   using A = Ar<T>;
   RunSum<1> rs;
   rs.reset();
-  const int k = 1 + bx * kNmTK + threadIdx.x;
-  const int j = 1 + by * kNmTJ + threadIdx.y;
+  const int k = 1 + bx * kNmTK + tile_x<kNmTK>();
+  const int j = 1 + by * kNmTJ + tile_y<kNmTK>();
   const int i0 = 1 + bz * kMarch;
   if (k < g.NN && j < g.NN && i0 < g.NN) {
     const int iend = min(i0 + kMarch, g.NN);
@@ -266,8 +284,8 @@ template <typename T, bool FINE>
 __device__ __forceinline__ void nm_rbgs_body(T* __restrict__ P, const T* __restrict__ f, const Geo& g, T h2, int color,
                                              int bx, int by, int bz) {
   using A = Ar<T>;
-  const int k0 = 1 + bx * 64 + 2 * threadIdx.x;
-  const int j = 1 + by * blockDim.y + threadIdx.y;
+  const int k0 = 1 + bx * 64 + 2 * tile_x<32>();
+  const int j = 1 + by * kNmRowTJ + tile_y<32>();
   const int i0 = 1 + bz * kNmRowPlanes;
   if (j >= g.NN || k0 >= g.NN) return;
   const int iend = min(i0 + kNmRowPlanes, g.NN);
@@ -307,7 +325,8 @@ __device__ __forceinline__ void nm_residual_point(const T* __restrict__ P, const
 // along i), so levels of every size fill the SMs, and each warp load is one contiguous run of 32
 // values.
 #define NM_ROWS_PROLOGUE                                  \
-  const int j = 1 + by * blockDim.y + threadIdx.y;        \
+  const int j = 1 + by * kNmRowTJ + tile_y<32>();        \
+  const int tx = tile_x<32>();                            \
   const int i0 = 1 + bz * kNmRowPlanes;                   \
   if (j >= g.NN) return;                                  \
   const int iend = min(i0 + kNmRowPlanes, g.NN);          \
@@ -323,7 +342,7 @@ __device__ __forceinline__ void nm_residual_rows_body(const T* __restrict__ P, c
     const int i = i0 + q;
 #pragma unroll
     for (int t = 0; t < 2; ++t) {
-      const int k = 1 + bx * 64 + threadIdx.x + 32 * t;
+      const int k = 1 + bx * 64 + tx + 32 * t;
       if (i < iend && k < g.NN)
         nm_residual_point<T, FINE>(P, f, r, (long long)i * S2 + (long long)j * S + k, S, S2, inv_h2);
     }
@@ -343,7 +362,7 @@ __device__ __forceinline__ void nm_prolong_rows_body(const T* __restrict__ Ec, T
 #pragma unroll
   for (int q = 0; q < kNmRowPlanes * 2; ++q) {
     const int i = i0 + (q >> 1);
-    const int k = 1 + bx * 64 + threadIdx.x + 32 * (q & 1);
+    const int k = 1 + bx * 64 + tx + 32 * (q & 1);
     if (i >= iend || k >= g.NN) continue;
     const int oi = i & 1;
     const long long row0 = (long long)(i >> 1) * gc.S2 + (long long)(j >> 1) * gc.S;
@@ -426,8 +445,8 @@ __device__ __forceinline__ void nm_energy_body(const T* __restrict__ U, const T*
   RunSum<kNmPD> rs;
   rs.reset();
   const double h3 = h * h * h;
-  const int k = 1 + bx * kNmTK + threadIdx.x;
-  const int j = 1 + by * kNmTJ + threadIdx.y;
+  const int k = 1 + bx * kNmTK + tile_x<kNmTK>();
+  const int j = 1 + by * kNmTJ + tile_y<kNmTK>();
   const int i0 = 1 + bz * kMarch;
   if (k < g.NN && j < g.NN && i0 < g.NN) {
     const int iend = min(i0 + kMarch, g.NN);
@@ -461,8 +480,8 @@ __device__ __forceinline__ void nm_evolve_body(const int* __restrict__ labIn, in
                                                const T* __restrict__ U, float* __restrict__ W, const Geo& g, T dt_w,
                                                T curvReg, int bx, int by, int bz) {
   using A = Ar<T>;
-  const int k = 1 + bx * kNmTK + threadIdx.x;
-  const int j = 1 + by * kNmTJ + threadIdx.y;
+  const int k = 1 + bx * kNmTK + tile_x<kNmTK>();
+  const int j = 1 + by * kNmTJ + tile_y<kNmTK>();
   const int i0 = 1 + bz * kMarch;
   if (k >= g.NN || j >= g.NN || i0 >= g.NN) return;
   const int iend = min(i0 + kMarch, g.NN);

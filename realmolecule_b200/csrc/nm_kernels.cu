@@ -49,14 +49,7 @@ template <typename T>
 __global__ void k_nm_norm_scale(const double* __restrict__ norms, const double* __restrict__ Zdom, int nDom,
                                 double* __restrict__ scale, int* __restrict__ err) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
-  if (l >= nDom) return;
-  const double n = norms[l];
-  if (!isfinite(n)) {
-    atomicOr(err, 1);
-    scale[l] = 1.0;
-    return;
-  }
-  scale[l] = (Zdom[l] > 0.0 && n > 1e-300) ? sqrt(Zdom[l] / n) : 1.0;
+  if (l < nDom) scale[l] = nm_domain_scale(norms[l], Zdom[l], err);
 }
 
 template <typename T>
