@@ -436,10 +436,11 @@ def nm_step_bytes(NN, es=4, pi=4, pre=1, post=1):
 
 
 def batch_leg(stream, peak):
-    """The C3 batch step on its own: all 96 clusters active in one mixed-precision batch (one launch
-    per kernel over the (instance, tile) work lists, a period per CUDA-graph replay), timed with CUDA
-    events over 400 steps; composite roofline = the algorithmic bytes of every kernel of the step
-    (nm_step_bytes) over the step time."""
+    """The C3 batch step on its own: all 96 clusters active in one mixed-precision batch (a period
+    per CUDA-graph replay), timed with CUDA events over 200 steps with the default configuration,
+    then autotuned (march tile x launch form, smoother sweeps) and timed over 400 steps; composite
+    roofline = the algorithmic bytes of every kernel of the step (nm_step_bytes, at the tuned
+    sweeps) over the step time."""
     import torch
     from realmolecule_b200 import configs
     from realmolecule_b200.batch import Batch
@@ -449,19 +450,29 @@ def batch_leg(stream, peak):
     b.set_stream(stream.cuda_stream)
     b.initialize()
     b.step(LABEL_UNTIL + 200)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed_steps(n):
+        torch.cuda.synchronize()
+        e0.record(stream)
+        b.step(n)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+    ms_default = timed_steps(200)
+    tune = b.autotune()  # march tile x launch form, then smoother sweeps (their steps are steps of the run)
+    b.step(200)          # capture the tuned periods
     n = 400
     l0 = b.info()["kernel_launches"]
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    b.step(n)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / n
+    ms = timed_steps(n)
     info = b.info()
     b.close()
-    byts = sum(nm_step_bytes(x.NN) for x in geoms)
+    cfg = tune["config"]
+    byts = sum(nm_step_bytes(x.NN, pre=cfg.get("mg_pre", 1), post=cfg.get("mg_post", 1)) for x in geoms)
+    byts_default = sum(nm_step_bytes(x.NN) for x in geoms)
     return {"instances": len(geoms), "interior_points": info["interior_points"], "ms_per_step": ms,
+            "ms_per_step_default_config": ms_default,
+            "frac_default_config": byts_default / (ms_default * 1e-3) / 1e9 / peak, "autotune": tune,
             "value_gpts": info["interior_points"] / (ms * 1e-3) / 1e9,
             "launches_per_step": (info["kernel_launches"] - l0) / n,
             "roofline": {"bound": "hbm", "bytes_per_step": byts, "achieved": byts / (ms * 1e-3) / 1e9, "peak": peak,
@@ -716,6 +727,10 @@ def converge_leg(stream, dist, rank, world):
     share = [inst[q] for q in shard.my_share(inst, rank, world)]
     b = Batch(share, precision="mixed", label_until=LABEL_UNTIL, converge_checks=CHECKS)
     b.set_stream(stream.cuda_stream)
+    tune, t_tune = None, 0.0
+    if share:  # tuned once for this batch before the timed solve (a deployment keeps the choice)
+        b.initialize()
+        tune, t_tune = _timed(stream, b.autotune)
     (cb, Eb), tb = _timed(stream, lambda: (b.initialize(), b.solve(TOL, MAX_STEPS, CHECK))[1])
     pts = b.info()["interior_points"]
     b.close()
@@ -738,6 +753,7 @@ def converge_leg(stream, dist, rank, world):
     out["clusters96"] = {"instances": len(inst), "ranks": world, "scaling": "strong",
                          "interior_points_rank0": pts,
                          "mixed_batched_s": tb, "fp64_plain_s": tp,
+                         "autotune_rank0": {"s": t_tune, "config": tune["config"] if tune else None},
                          "solves_per_s_mixed_batched": len(inst) / tb, "solves_per_s_fp64_plain": len(inst) / tp,
                          "speedup_vs_fp64_plain": tp / tb, "max_abs_dE_Ha": dE,
                          "unconverged_rank0": {"mixed_batched": int((cb < 0).sum()) if len(share) else 0,

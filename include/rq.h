@@ -110,7 +110,9 @@ typedef struct rq_config {
                                persistent cooperative launch (blocks take chunks of (instance, tile) items from
                                one queue; an item waits, bounded, only for its instance's previous phase).
                                rq_batch_autotune times both and keeps the faster. */
-  int32_t reserved[1];
+  int32_t batch_tile;       /* rq_batch_*: march tile of the update, readout and level-set work lists, as
+                               log2(points along k) | (planes per thread << 8), 256 threads per tile; 0 = 16 x 16
+                               x 16 (4 | 16 << 8).  rq_batch_autotune picks it. */
 } rq_config;
 
 /* One entry of the reference atom list: a nucleus and/or one electron domain. */
@@ -334,6 +336,29 @@ RQ_API int rq_batch_synchronize(rq_batch* b);
  * more than there are, so every wait runs out (a test of the timeout path on a healthy device).  Drops
  * the captured periods. */
 RQ_API int rq_batch_set_wait(rq_batch* b, int64_t limit_ns, int32_t extra_arrivals);
+
+/* The batch's own autotuner (no reference counterpart).  Needs an initialised batch; its timing runs
+ * are steps of the solve (the state moves on as under rq_batch_step) and leave the multigrid
+ * correction P as it was.
+ *   1. March tile x launch form: each candidate (tiles 16 x 16 and 32 x 8 points with 8, 16 or 32
+ *      planes per thread; per-kernel graph or persistent launch) runs one schedule period to capture
+ *      it and one timed by CUDA events; the fastest per step is kept.
+ *   2. Smoother sweeps (mg_pre, mg_post, mg_coarse_sweeps): from P = 0 each candidate runs 3 V-cycles
+ *      on the batch's current psi; the one with the largest -ln(rho) per ms (rho: fine-grid residual
+ *      reduction per cycle) is kept.
+ * The kept values go into the batch's configuration (batch_tile, batch_persistent, mg_*), and the
+ * report lists every candidate. */
+typedef struct rq_tune_report {
+  int32_t n_tile;                  /* tile x launch candidates timed */
+  int32_t tile[12], persistent[12];
+  double ms_per_step[12];
+  int32_t n_smooth;                /* smoother candidates */
+  int32_t pre[8], post[8], coarse_sweeps[8];
+  double rho[8], ms_per_cycle[8];
+  int32_t best_tile, best_smooth;  /* indices of the kept candidates */
+  int32_t reserved[6];
+} rq_tune_report;
+RQ_API int rq_batch_autotune(rq_batch* b, rq_tune_report* out);
 
 /* ---- atom.js per-shell solver (atom.js:1-346) ----------------------------------------------
  * Replaces atom.js's module state and physicsStep(): one U (density amplitude), W (front) and P

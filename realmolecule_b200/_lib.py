@@ -71,7 +71,15 @@ class Config(C.Structure):
                 ("boundary_speed", C.c_double), ("curv_reg", C.c_double), ("sigma", C.c_double),
                 ("label_until", C.c_int32), ("chebyshev", C.c_int32), ("lobpcg", C.c_int32),
                 ("converge_checks", C.c_int32), ("fp32_rounding", C.c_int32), ("nuclear_sum", C.c_int32),
-                ("batch_persistent", C.c_int32), ("reserved", C.c_int32 * 1)]
+                ("batch_persistent", C.c_int32), ("batch_tile", C.c_int32)]
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("n_tile", C.c_int32), ("tile", C.c_int32 * 12), ("persistent", C.c_int32 * 12),
+                ("ms_per_step", C.c_double * 12), ("n_smooth", C.c_int32), ("pre", C.c_int32 * 8),
+                ("post", C.c_int32 * 8), ("coarse_sweeps", C.c_int32 * 8), ("rho", C.c_double * 8),
+                ("ms_per_cycle", C.c_double * 8), ("best_tile", C.c_int32), ("best_smooth", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
 
 
 class Split(C.Structure):
@@ -144,6 +152,7 @@ SIGNATURES = {
                                 C.POINTER(C.c_int64)]),
     "rq_batch_synchronize": (C.c_int, [_V]),
     "rq_batch_set_wait": (C.c_int, [_V, C.c_int64, _I]),
+    "rq_batch_autotune": (C.c_int, [_V, _P]),
     "rq_shells_create": (C.c_int, [_P, _P, _I, _P]),
     "rq_shells_destroy": (None, [_V]),
     "rq_shells_last_error": (C.c_char_p, [_V]),

@@ -67,6 +67,26 @@ class Batch:
     def synchronize(self):
         self._chk(self.lib.rq_batch_synchronize(self.b), "rq_batch_synchronize")
 
+    def autotune(self) -> dict:
+        """rq_batch_autotune: pick the march tile and launch form (timed per step) and the smoother
+        sweeps (V-cycle convergence per ms); the choice stays in the batch.  Returns the choice and
+        every candidate's measurement."""
+        r = L.TuneReport()
+        self._chk(self.lib.rq_batch_autotune(self.b, C.byref(r)), "rq_batch_autotune")
+        tiles = [{"tile": f"{1 << (r.tile[i] & 0xff)}x{256 >> (r.tile[i] & 0xff)}x{r.tile[i] >> 8}",
+                  "batch_tile": r.tile[i], "persistent": r.persistent[i], "ms_per_step": r.ms_per_step[i]}
+                 for i in range(r.n_tile)]
+        smooth = [{"mg_pre": r.pre[i], "mg_post": r.post[i], "mg_coarse_sweeps": r.coarse_sweeps[i], "rho": r.rho[i],
+                   "ms_per_cycle": r.ms_per_cycle[i]} for i in range(r.n_smooth)]
+        best = {}
+        if r.n_tile:
+            t = tiles[r.best_tile]
+            best.update(batch_tile=t["batch_tile"], batch_persistent=t["persistent"])
+        if r.n_smooth:
+            m = smooth[r.best_smooth]
+            best.update(mg_pre=m["mg_pre"], mg_post=m["mg_post"], mg_coarse_sweeps=m["mg_coarse_sweeps"])
+        return {"config": best, "tiles": tiles, "smoothers": smooth}
+
     def set_wait(self, limit_ns: int, extra_arrivals: int = 0):
         """Bound of the persistent launch's waits; extra_arrivals > 0 makes every wait run out (the
         next readout raises RqError with RQ_ETIMEOUT)."""

@@ -57,7 +57,7 @@ template <typename T, bool ACC>
 __global__ void __launch_bounds__(256) kb_update(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cu,
                                                  int cp, int cl, T half_dv, T dt, double* __restrict__ norms,
                                                  const double* __restrict__ scale, const unsigned* __restrict__ seed,
-                                                 unsigned* __restrict__ seed_next) {
+                                                 unsigned* __restrict__ seed_next, NmTile tile) {
   __shared__ DomTable<1, 128> tab;
   if (seed && blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) *seed_next = *seed + 1u;
   const BItem it = items[blockIdx.x];
@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(256) kb_update(const BInst* __restrict__ ins, 
   const Geo g = I.g;
   nm_update_body<T, ACC>((const T*)I.U[cu], (T*)I.U[1 - cu], (const T*)I.K, (const T*)I.P[cp], I.lab[cl], g, half_dv,
                          dt, I.h * I.h * I.h, I.nDom, nrm, tab, it.bx, it.by, it.bz, scale ? scale + I.dom0 : nullptr,
-                         seed);
+                         seed, tile);
   if (ACC) {
     __syncthreads();
     dom_table_flush(tab, nrm);
@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(1024) kb_coarsest(const BInst* __restrict__ in
 
 template <typename T>
 __global__ void __launch_bounds__(256) kb_energy(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cu,
-                                                 int cp, int cl, double* __restrict__ pd) {
+                                                 int cp, int cl, double* __restrict__ pd, NmTile tile) {
   __shared__ DomTable<kNmPD, 128> tab;
   const BItem it = items[blockIdx.x];
   const BInst& I = ins[it.inst];
@@ -171,18 +171,18 @@ __global__ void __launch_bounds__(256) kb_energy(const BInst* __restrict__ ins, 
   __syncthreads();
   const Geo g = I.g;
   nm_energy_body<T>((const T*)I.U[cu], (const T*)I.K, (const T*)I.P[cp], I.lab[cl], g, I.h, I.nDom,
-                    pd + kNmPD * I.dom0, tab, it.bx, it.by, it.bz, sizeof(T) == sizeof(float) ? I.K64 : nullptr);
+                    pd + kNmPD * I.dom0, tab, it.bx, it.by, it.bz, sizeof(T) == sizeof(float) ? I.K64 : nullptr, tile);
   __syncthreads();
   dom_table_flush(tab, pd + kNmPD * I.dom0);
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256) kb_evolve(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cu,
-                                                 int cl, T dt_w, T curv) {
+                                                 int cl, T dt_w, T curv, NmTile tile) {
   const BItem it = items[blockIdx.x];
   const BInst& I = ins[it.inst];
   const Geo g = I.g;
-  nm_evolve_body<T>(I.lab[cl], I.lab[1 - cl], (const T*)I.U[cu], I.W, g, dt_w, curv, it.bx, it.by, it.bz);
+  nm_evolve_body<T>(I.lab[cl], I.lab[1 - cl], (const T*)I.U[cu], I.W, g, dt_w, curv, it.bx, it.by, it.bz, tile);
 }
 
 template <typename T>
@@ -213,6 +213,46 @@ __global__ void __launch_bounds__(256) kb_force(const BInst* __restrict__ ins, c
   const BInst& I = ins[it.inst];
   nm_force_body<T>((const T*)I.U[cu], I.at, I.nAt, I.g, I.h, sigma_scale > 0 ? sigma_scale : I.h, F + 3 * I.at0, it.bx,
                    it.by, it.bz, sx, sy, sz, sr);
+}
+
+// Sum over the fine interior of the squared residual 2 pi psi^2 - A P (FP64), added into *out:
+// the autotuner's multigrid convergence measure.  Row tiling of kb_residual.
+template <typename T>
+__global__ void __launch_bounds__(256) kb_resnorm(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cu,
+                                                  int cp, double* __restrict__ out) {
+  __shared__ double part[8];
+  const BItem it = items[blockIdx.x];
+  const BInst& I = ins[it.inst];
+  const Geo g = I.g;
+  const T* P = (const T*)I.P[cp];
+  const T* U = (const T*)I.U[cu];
+  const double ih2 = 1.0 / (I.h * I.h);
+  const int j = 1 + it.by * kNmRowTJ + tile_y<32>(), tx = tile_x<32>(), i0 = 1 + it.bz * kNmRowPlanes;
+  double acc = 0.0;
+  if (j < g.NN) {
+    const int iend = min(i0 + kNmRowPlanes, g.NN);
+    const long long S = g.S, S2 = g.S2;
+    for (int i = i0; i < iend; ++i)
+      for (int t = 0; t < 2; ++t) {
+        const int k = 1 + it.bx * 64 + tx + 32 * t;
+        if (k >= g.NN) continue;
+        const long long id = (long long)i * S2 + (long long)j * S + k;
+        const double sd = (double)P[id + S2] + (double)P[id - S2] + (double)P[id + S] + (double)P[id - S] +
+                          (double)P[id + 1] + (double)P[id - 1];
+        const double u = (double)U[id];
+        const double r = 6.283185307179586 * u * u + (sd - 6.0 * (double)P[id]) * ih2;
+        acc += r * r;
+      }
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  const int lin = (int)(threadIdx.x + blockDim.x * threadIdx.y);
+  if ((lin & 31) == 0) part[lin >> 5] = acc;
+  __syncthreads();
+  if (lin == 0) {
+    double sum = 0.0;
+    for (int w = 0; w < 8; ++w) sum += part[w];
+    atomicAdd(out, sum);
+  }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -265,6 +305,7 @@ struct BPersist {
   float dt_w, curv;       // level-set pass
   int* err;               // bit 0: non-finite norm; bit 1: a wait gave up
   long long limit_ns;     // bound of every wait
+  NmTile tile;            // march tile of the update and level-set items
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -296,13 +337,13 @@ __device__ __forceinline__ void kb_run_item(const BPersist& a, const BPhase& P, 
         __syncthreads();
         nm_update_body<T, true>((const T*)I.U[P.cu], (T*)I.U[1 - P.cu], (const T*)I.K, (const T*)I.P[P.cp], I.lab[P.cl],
                                 g, (T)a.half_dv, (T)a.dt, I.h * I.h * I.h, I.nDom, a.dnorm + I.dom0, tab, it.bx, it.by,
-                                it.bz, sc, P.seed);
+                                it.bz, sc, P.seed, a.tile);
         __syncthreads();
         dom_table_flush(tab, a.dnorm + I.dom0);
       } else {
         nm_update_body<T, false>((const T*)I.U[P.cu], (T*)I.U[1 - P.cu], (const T*)I.K, (const T*)I.P[P.cp],
                                  I.lab[P.cl], g, (T)a.half_dv, (T)a.dt, I.h * I.h * I.h, I.nDom, nullptr, tab, it.bx,
-                                 it.by, it.bz, sc, P.seed);
+                                 it.by, it.bz, sc, P.seed, a.tile);
       }
       break;
     }
@@ -353,7 +394,7 @@ __device__ __forceinline__ void kb_run_item(const BPersist& a, const BPhase& P, 
     case kPhEvolve: {
       const Geo g = I.g;
       nm_evolve_body<T>(I.lab[P.cl], I.lab[1 - P.cl], (const T*)I.U[P.cu], I.W, g, (T)a.dt_w, (T)a.curv, it.bx, it.by,
-                        it.bz);
+                        it.bz, a.tile);
       break;
     }
     default:
@@ -489,6 +530,8 @@ struct rq_batch {
   int pgrid[4] = {};              // co-resident blocks of kb_persist<sets> (0: not yet queried)
   long long wait_ns = 2000000000LL;
   int extra_arrivals = 0;
+  NmTile tile = kNmTile;          // march tile of the update, readout and level-set work lists
+  double* dtune = nullptr;        // the autotuner's residual sum
 };
 
 #define BCK(call)                                                                  \
@@ -524,8 +567,8 @@ static int upload_plan(rq_batch* b, rq_batch::Plan& p, const std::vector<BItem>&
   return RQ_OK;
 }
 
-static void march_items(std::vector<BItem>& v, int inst, const Geo& g) {
-  const dim3 gr = nm_march_grid(g);
+static void march_items(std::vector<BItem>& v, int inst, const Geo& g, NmTile tile) {
+  const dim3 gr = nm_march_grid(g, tile);
   for (unsigned z = 0; z < gr.z; ++z)
     for (unsigned y = 0; y < gr.y; ++y)
       for (unsigned x = 0; x < gr.x; ++x) v.push_back({inst, (int)x, (int)y, (int)z});
@@ -535,9 +578,10 @@ static void flat_items(std::vector<BItem>& v, int inst, long long npts, long lon
   for (long long x = 0; x < (npts + per_block - 1) / per_block; ++x) v.push_back({inst, (int)x, 0, 0});
 }
 
-static void make_items(const BInst& I, int q, InstItems& it) {
+static void make_items(const BInst& I, int q, InstItems& it, NmTile tile) {
+  it = InstItems{};
   for (int l = 0; l < I.nlev; ++l) {
-    march_items(it.march[l], q, I.lg[l]);
+    march_items(it.march[l], q, I.lg[l], tile);
     if (l == I.nlev - 1) {
       it.coarse[l].push_back({q, 0, 0, 0});
       continue;
@@ -678,7 +722,7 @@ static int build(rq_batch* b) {
     BCK(cudaMemcpyAsync(b->din, b->hin.data(), sizeof(BInst) * n, cudaMemcpyHostToDevice, b->st));
   }
   b->items.resize(n);
-  for (int q = 0; q < n; ++q) make_items(b->hin[q], q, b->items[q]);
+  for (int q = 0; q < n; ++q) make_items(b->hin[q], q, b->items[q], b->tile);
   BRC(build_plans(b));
   size_t smax = 0;
   for (int l = 0; l < b->maxlev; ++l) smax = std::max(smax, b->coarse_smem[l]);
@@ -865,10 +909,10 @@ static int b_step(rq_batch* b, int s) {
     }
     if (norm)
       kb_update<T, true><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cp, b->cl, (T)hd, (T)dt, b->dnorm,
-                                                             sc, sd, sn);
+                                                             sc, sd, sn, b->tile);
     else
       kb_update<T, false><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cp, b->cl, (T)hd, (T)dt, nullptr,
-                                                              sc, sd, sn);
+                                                              sc, sd, sn, b->tile);
     BL("update");
     return RQ_OK;
   }));
@@ -895,7 +939,7 @@ static int b_step(rq_batch* b, int s) {
         return RQ_OK;
       }
       kb_evolve<T><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cl, (T)(float)f.boundary_speed,
-                                                       (T)(float)f.curv_reg);
+                                                       (T)(float)f.curv_reg, b->tile);
       BL("evolve");
       return RQ_OK;
     }));
@@ -963,6 +1007,12 @@ extern "C" int rq_batch_create(const rq_config* cfgs, const rq_atom* atoms, cons
   if (f.boundary_speed <= 0) f.boundary_speed = 0.5;
   if (f.curv_reg == 0) f.curv_reg = 0.15;
   if (f.curv_reg < 0) f.curv_reg = 0;
+  if (f.batch_tile == 0) f.batch_tile = kNmTile.lgk | (kNmTile.march << 8);
+  b->tile = NmTile{f.batch_tile & 0xff, f.batch_tile >> 8};
+  if (b->tile.lgk < 3 || b->tile.lgk > 6 || b->tile.march < 1 || b->tile.march > 64) {
+    delete b;
+    return RQ_EINVAL;  // 8..64 points along k, 1..64 planes per thread
+  }
   b->dv = f.dv > 0 ? f.dv : 0.2;
   if (cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking) != cudaSuccess) {
     delete b;
@@ -1082,6 +1132,24 @@ static int b_phase_items(const rq_batch* b, const BPhase& x, int q) {
 // count; all uploaded once per graph key.  The graph holds the zeroing of the counters and the
 // cooperative launch of kb_persist over every co-resident block.
 static int b_persist_graph(rq_batch* b, int key, int period) {
+  // the kernel for the sets in use, and whether the device runs it (checked before recording,
+  // which advances the host state)
+  int sets = (b->pl[kF32].march[0].n ? 1 : 0) | (b->pl[kF64].march[0].n ? 2 : 0);
+  if (!sets) sets = 1;
+  void (*kern)(BPersist) = sets == 1 ? kb_persist<1> : sets == 2 ? kb_persist<2> : kb_persist<3>;
+  if (b->pgrid[sets] == 0) {
+    int dev = 0, nsm = 0, per = 0, coop = 0;
+    BCK(cudaGetDevice(&dev));
+    BCK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    BCK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, 0));
+    if (!coop || per < 1) {
+      b->last_error = "the device cannot run the persistent batch launch (set batch_persistent = 0)";
+      return RQ_ENOTSUP;
+    }
+    b->pgrid[sets] = nsm * per;
+  }
+  const int pgrid = b->pgrid[sets];
   std::vector<BPhase> prog;
   b->rec = &prog;
   const int rc = b_eager(b, period);
@@ -1114,23 +1182,6 @@ static int b_persist_graph(rq_batch* b, int key, int period) {
     }
   }
   const int nch = (int)chunks.size();
-  int sets = 0;
-  for (const BPhase& x : prog) sets |= 1 << x.set;
-  if (!sets) sets = 1;
-  void (*kern)(BPersist) = sets == 1 ? kb_persist<1> : sets == 2 ? kb_persist<2> : kb_persist<3>;
-  if (b->pgrid[sets] == 0) {
-    int dev = 0, nsm = 0, per = 0, coop = 0;
-    BCK(cudaGetDevice(&dev));
-    BCK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    BCK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
-    BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, 256, 0));
-    if (!coop || per < 1) {
-      b->last_error = "the device cannot run the persistent batch launch (set batch_persistent = 0)";
-      return RQ_ENOTSUP;
-    }
-    b->pgrid[sets] = nsm * per;
-  }
-  const int pgrid = b->pgrid[sets];
   // device copies: program, queue offsets, dependencies (per key), counters (shared by the keys)
   rq_batch::Prog& G = b->prog[key];
   if (nph > G.cap || nch > G.cap_chunks) {
@@ -1160,6 +1211,7 @@ static int b_persist_graph(rq_batch* b, int key, int period) {
   a.dt_w = (float)b->cfg.boundary_speed; a.curv = (float)b->cfg.curv_reg;
   a.err = b->err;
   a.limit_ns = b->wait_ns;
+  a.tile = b->tile;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
   attr[0].val.cooperative = 1;
@@ -1252,7 +1304,7 @@ extern "C" int rq_batch_energy(rq_batch* b, double* out) {
     using T = decltype(tag);
     const rq_batch::Plan& m = b->pl[p].march[0];
     if (!m.n) return RQ_OK;
-    kb_energy<T><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cp, b->cl, b->dpd);
+    kb_energy<T><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cp, b->cl, b->dpd, b->tile);
     BL("energy");
     return RQ_OK;
   }));
@@ -1456,6 +1508,148 @@ extern "C" int rq_batch_set_wait(rq_batch* b, int64_t limit_ns, int32_t extra_ar
   for (auto& g : b->graph)  // the limits are arguments of the captured launches
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   return RQ_OK;
+}
+
+static void b_drop_graphs(rq_batch* b) {
+  for (auto& g : b->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+// the work lists for another march tile (the per-instance items, then the plans)
+static int b_retile(rq_batch* b, NmTile t) {
+  b->tile = t;
+  b->cfg.batch_tile = t.lgk | (t.march << 8);
+  for (int q = 0; q < b->n; ++q) make_items(b->hin[q], q, b->items[q], t);
+  return build_plans(b);
+}
+
+// sum of the squared fine-grid residual over the active instances
+static int b_resnorm(rq_batch* b, double* dsum, double& out) {
+  BCK(cudaMemsetAsync(dsum, 0, sizeof(double), b->st));
+  BRC(each_set([&](auto tag, int p) -> int {
+    using T = decltype(tag);
+    const rq_batch::Plan& r = b->pl[p].rbgs[0];
+    if (!r.n) return RQ_OK;
+    kb_resnorm<T><<<r.n, dim3(32, 8), 0, b->st>>>(b->din, r.d, b->cu, b->cp, dsum);
+    BL("resnorm");
+    return RQ_OK;
+  }));
+  BCK(cudaMemcpyAsync(&out, dsum, sizeof(double), cudaMemcpyDeviceToHost, b->st));
+  BCK(cudaStreamSynchronize(b->st));
+  return RQ_OK;
+}
+
+extern "C" int rq_batch_autotune(rq_batch* b, rq_tune_report* out) {
+  if (!b || !out) return RQ_EINVAL;
+  std::memset(out, 0, sizeof(*out));
+  if (!any_active(b)) return RQ_OK;
+  const int period = b_period(b);
+  BRC(b_ready(b));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  BCK(cudaEventCreate(&e0));
+  BCK(cudaEventCreate(&e1));
+  auto cleanup = [&]() { cudaEventDestroy(e0); cudaEventDestroy(e1); };
+  int rc = RQ_OK;
+  // 1. march tile x launch form, timed per step over one captured period
+  const NmTile keep = b->tile;
+  const int keep_persistent = b->cfg.batch_persistent;
+  double best = 1e300;
+  int nt = 0;
+  for (int lgk : {4, 5})
+    for (int march : {8, 16, 32})
+      for (int pers : {0, 1}) {
+        if (pers && b->cfg.fp32_rounding == 1) continue;  // that schedule keeps the per-kernel launches
+        if ((rc = b_retile(b, NmTile{lgk, march})) != RQ_OK) break;
+        b->cfg.batch_persistent = pers;
+        b_drop_graphs(b);
+        if (b->steps_done % period) rc = rq_batch_step(b, period - b->steps_done % period);
+        if (rc == RQ_OK) rc = rq_batch_step(b, period);  // captures the period
+        if (pers && rc == RQ_ENOTSUP) {  // no cooperative launch here: per-kernel graphs only
+          rc = RQ_OK;
+          continue;
+        }
+        if (rc == RQ_OK && cudaEventRecord(e0, b->st) != cudaSuccess) rc = RQ_ECUDA;
+        if (rc == RQ_OK) rc = rq_batch_step(b, period);
+        if (rc == RQ_OK && cudaEventRecord(e1, b->st) != cudaSuccess) rc = RQ_ECUDA;
+        float ms = 0.f;
+        if (rc == RQ_OK && (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+          rc = RQ_ECUDA;
+        if (rc != RQ_OK) break;
+        out->tile[nt] = lgk | (march << 8);
+        out->persistent[nt] = pers;
+        out->ms_per_step[nt] = ms / period;
+        if (out->ms_per_step[nt] < best) { best = out->ms_per_step[nt]; out->best_tile = nt; }
+        ++nt;
+      }
+  out->n_tile = nt;
+  if (rc == RQ_OK && nt > 0) {
+    const int t = out->tile[out->best_tile];
+    rc = b_retile(b, NmTile{t & 0xff, t >> 8});
+    b->cfg.batch_persistent = out->persistent[out->best_tile];
+    b_drop_graphs(b);
+  } else {
+    b_retile(b, keep);
+    b->cfg.batch_persistent = keep_persistent;
+  }
+  // 2. smoother sweeps: 3 V-cycles from P = 0 on the current psi, P restored after each
+  if (rc == RQ_OK && !b->dtune) rc = balloc(b, (void**)&b->dtune, sizeof(double));
+  if (rc == RQ_OK) rc = b_flush(b);
+  const int cand[7][3] = {{1, 1, 16}, {2, 1, 16}, {1, 2, 16}, {2, 2, 16}, {1, 1, 8}, {1, 1, 32}, {2, 2, 32}};
+  const rq_config keepc = b->cfg;
+  double best_eff = -1.0;
+  int ns = 0;
+  for (int c = 0; c < 7 && rc == RQ_OK; ++c) {
+    b->cfg.mg_pre = cand[c][0];
+    b->cfg.mg_post = cand[c][1];
+    b->cfg.mg_coarse_sweeps = cand[c][2];
+    for (int q = 0; q < b->n && rc == RQ_OK; ++q) {
+      if (!b->active[q]) continue;
+      const BInst& I = b->hin[q];
+      const size_t bytes = (b->f64[q] ? sizeof(double) : sizeof(float)) * (size_t)I.g.S3;
+      if (cudaMemcpyAsync(I.P[1 - b->cp], I.P[b->cp], bytes, cudaMemcpyDeviceToDevice, b->st) != cudaSuccess ||
+          cudaMemsetAsync(I.P[b->cp], 0, bytes, b->st) != cudaSuccess)
+        rc = RQ_ECUDA;
+    }
+    double r0 = 0, r3 = 0;
+    if (rc == RQ_OK) rc = b_resnorm(b, b->dtune, r0);
+    if (rc == RQ_OK && cudaEventRecord(e0, b->st) != cudaSuccess) rc = RQ_ECUDA;
+    for (int v = 0; v < 3 && rc == RQ_OK; ++v)
+      rc = each_set([&](auto tag, int p) { return b_vcycle<decltype(tag)>(b, p); });
+    if (rc == RQ_OK && cudaEventRecord(e1, b->st) != cudaSuccess) rc = RQ_ECUDA;
+    if (rc == RQ_OK) rc = b_resnorm(b, b->dtune, r3);
+    float ms = 0.f;
+    if (rc == RQ_OK && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) rc = RQ_ECUDA;
+    for (int q = 0; q < b->n && rc == RQ_OK; ++q) {
+      if (!b->active[q]) continue;
+      const BInst& I = b->hin[q];
+      const size_t bytes = (b->f64[q] ? sizeof(double) : sizeof(float)) * (size_t)I.g.S3;
+      if (cudaMemcpyAsync(I.P[b->cp], I.P[1 - b->cp], bytes, cudaMemcpyDeviceToDevice, b->st) != cudaSuccess) rc = RQ_ECUDA;
+    }
+    if (rc != RQ_OK) break;
+    const double rho = r0 > 0 ? std::pow(std::sqrt(r3 / r0), 1.0 / 3.0) : 1.0;
+    out->pre[ns] = cand[c][0];
+    out->post[ns] = cand[c][1];
+    out->coarse_sweeps[ns] = cand[c][2];
+    out->rho[ns] = rho;
+    out->ms_per_cycle[ns] = ms / 3.0;
+    const double eff = (rho > 0 && rho < 1) ? -std::log(rho) / (ms / 3.0) : 0.0;
+    if (eff > best_eff) { best_eff = eff; out->best_smooth = ns; }
+    ++ns;
+  }
+  out->n_smooth = ns;
+  if (rc == RQ_OK && ns > 0) {
+    b->cfg.mg_pre = out->pre[out->best_smooth];
+    b->cfg.mg_post = out->post[out->best_smooth];
+    b->cfg.mg_coarse_sweeps = out->coarse_sweeps[out->best_smooth];
+  } else {
+    b->cfg.mg_pre = keepc.mg_pre;
+    b->cfg.mg_post = keepc.mg_post;
+    b->cfg.mg_coarse_sweeps = keepc.mg_coarse_sweeps;
+  }
+  b_drop_graphs(b);  // the periods change with the sweeps
+  if (rc == RQ_OK && cudaStreamSynchronize(b->st) != cudaSuccess) rc = RQ_ECUDA;
+  cleanup();
+  return rc;
 }
 
 extern "C" int rq_batch_synchronize(rq_batch* b) {

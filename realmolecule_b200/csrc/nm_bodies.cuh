@@ -36,15 +36,27 @@ template <int W>
 __device__ __forceinline__ int tile_x() { return (int)((threadIdx.x + blockDim.x * threadIdx.y) % W); }
 template <int W>
 __device__ __forceinline__ int tile_y() { return (int)((threadIdx.x + blockDim.x * threadIdx.y) / W); }
-// March tile of the new flavour's stencil bodies: 16 (k) x 16 (j) threads, each walking kMarch
-// planes of i.  16 wide rows waste fewer lanes than 32 on the 47..127-point interiors of the
-// cluster grids (a warp still reads two contiguous 64-byte runs).
+// March tile of the new flavour's stencil bodies (update, readout, level set): 2^lgk points along
+// k x 256 / 2^lgk rows j per block of 256 threads, each thread walking `march` planes of i.  The
+// single-grid kernels use kNmTile (16 x 16 x 16: 16 wide rows waste fewer lanes than 32 on the
+// 47..127-point interiors of the cluster grids); a batch uses the tile its autotuner picked.
+struct NmTile {
+  int lgk, march;
+};
 constexpr int kNmTK = 16, kNmTJ = 16;
-inline dim3 nm_march_grid(const Geo& g) {
-  const int n = g.NN - 1;
-  return dim3((n + kNmTK - 1) / kNmTK, (n + kNmTJ - 1) / kNmTJ, (n + kMarch - 1) / kMarch);
+constexpr NmTile kNmTile{4, kMarch};
+inline dim3 nm_march_grid(const Geo& g, NmTile t = kNmTile) {
+  const int n = g.NN - 1, tk = 1 << t.lgk, tj = 256 >> t.lgk;
+  return dim3((n + tk - 1) / tk, (n + tj - 1) / tj, (n + t.march - 1) / t.march);
 }
 inline dim3 nm_march_block() { return dim3(kNmTK, kNmTJ, 1); }
+// a thread's column (k, j) and first plane i0 in march tile (bx, by, bz)
+__device__ __forceinline__ void nm_tile_origin(const NmTile& t, int bx, int by, int bz, int& k, int& j, int& i0) {
+  const int lin = (int)(threadIdx.x + blockDim.x * threadIdx.y);
+  k = 1 + (bx << t.lgk) + (lin & ((1 << t.lgk) - 1));
+  j = 1 + by * (256 >> t.lgk) + (lin >> t.lgk);
+  i0 = 1 + bz * t.march;
+}
 constexpr int kCoarsestThreads = 256; // one block solves the coarsest level (<= 29^3 points)
 
 // FP64 1/sqrt(x) for x in the normal FP32 range: the FP32 hardware estimate y0 (relative error
@@ -184,15 +196,15 @@ __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __res
                                                T half_dv, T dt, double h3, int nDom, double* __restrict__ norms,
                                                DomTable<1, 128>& tab, int bx, int by, int bz,
                                                const double* __restrict__ scale = nullptr,
-                                               const unsigned* __restrict__ seed = nullptr) {
+                                               const unsigned* __restrict__ seed = nullptr,
+                                               const NmTile t = kNmTile) {
   using A = Ar<T>;
   RunSum<1> rs;
   rs.reset();
-  const int k = 1 + bx * kNmTK + tile_x<kNmTK>();
-  const int j = 1 + by * kNmTJ + tile_y<kNmTK>();
-  const int i0 = 1 + bz * kMarch;
+  int k, j, i0;
+  nm_tile_origin(t, bx, by, bz, k, j, i0);
   if (k < g.NN && j < g.NN && i0 < g.NN) {
-    const int iend = min(i0 + kMarch, g.NN);
+    const int iend = min(i0 + t.march, g.NN);
     const long long S = g.S, S2 = g.S2;
     long long id = (long long)i0 * S2 + j * S + k;
     const unsigned sd = seed ? __ldg(seed) : 0u;
@@ -441,15 +453,15 @@ template <typename T>
 __device__ __forceinline__ void nm_energy_body(const T* __restrict__ U, const T* __restrict__ K, const T* __restrict__ P,
                                                const int* __restrict__ label, const Geo& g, double h, int nDom,
                                                double* __restrict__ pd, DomTable<kNmPD, 128>& tab, int bx, int by,
-                                               int bz, const double* __restrict__ K64 = nullptr) {
+                                               int bz, const double* __restrict__ K64 = nullptr,
+                                               const NmTile t = kNmTile) {
   RunSum<kNmPD> rs;
   rs.reset();
   const double h3 = h * h * h;
-  const int k = 1 + bx * kNmTK + tile_x<kNmTK>();
-  const int j = 1 + by * kNmTJ + tile_y<kNmTK>();
-  const int i0 = 1 + bz * kMarch;
+  int k, j, i0;
+  nm_tile_origin(t, bx, by, bz, k, j, i0);
   if (k < g.NN && j < g.NN && i0 < g.NN) {
-    const int iend = min(i0 + kMarch, g.NN);
+    const int iend = min(i0 + t.march, g.NN);
     const long long S = g.S, S2 = g.S2;
     for (int i = i0; i < iend; ++i) {
       const long long id = (long long)i * S2 + j * S + k;
@@ -478,13 +490,12 @@ __device__ __forceinline__ void nm_energy_body(const T* __restrict__ U, const T*
 template <typename T>
 __device__ __forceinline__ void nm_evolve_body(const int* __restrict__ labIn, int* __restrict__ labOut,
                                                const T* __restrict__ U, float* __restrict__ W, const Geo& g, T dt_w,
-                                               T curvReg, int bx, int by, int bz) {
+                                               T curvReg, int bx, int by, int bz, const NmTile t = kNmTile) {
   using A = Ar<T>;
-  const int k = 1 + bx * kNmTK + tile_x<kNmTK>();
-  const int j = 1 + by * kNmTJ + tile_y<kNmTK>();
-  const int i0 = 1 + bz * kMarch;
+  int k, j, i0;
+  nm_tile_origin(t, bx, by, bz, k, j, i0);
   if (k >= g.NN || j >= g.NN || i0 >= g.NN) return;
-  const int iend = min(i0 + kMarch, g.NN);
+  const int iend = min(i0 + t.march, g.NN);
   const long long S = g.S, S2 = g.S2;
   for (int i = i0; i < iend; ++i) {
     const long long id = (long long)i * S2 + j * S + k;
