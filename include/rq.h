@@ -206,6 +206,11 @@ RQ_API int rq_initialize(rq_ctx* ctx);
  * level-set passes (labels and W stay as they are; the frame counter still advances); 0 lets the
  * boundaries move again (the page's UNLOCK_AT_STEP, :4621-4624).  molecule.js flavour only. */
 RQ_API int rq_set_freeze_boundary(rq_ctx* ctx, int32_t on);
+/* molecule.js window.USER_INIT_POS (molecule.js:1905-1981): for the next rq_initialize, the trial psi
+ * and the initial labels are built with entry q moved to (pos[2q], pos[2q+1]) in grid units where
+ * has[q] != 0 (k unchanged); K is then rebuilt from 0 at the true positions with the page's recomputeK
+ * (:1337-1370).  n = 0 clears.  molecule.js flavour only. */
+RQ_API int rq_set_init_positions(rq_ctx* ctx, const double* pos, const int32_t* has, int32_t n);
 /* The molecule.js classical-MD backbone's full restart (USER_CLASSICAL_MD, molecule.js:4236-4286),
  * after rq_set_atoms with the moved positions: K, the trial psi and the labels rebuilt from scratch,
  * P cleared; unlike rq_initialize the level-set W and Pother (the stale potential the next frame's

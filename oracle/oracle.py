@@ -119,6 +119,7 @@ class _Oracle:
             "orc_mj_force_hf": [_f32p, C.c_void_p, _i, _i, _f, _f, _f64p],
             "orc_mj_init": [_f32p, _f32p, _u32p, C.c_void_p, _i, _i, _f, _f, _f, C.c_void_p],
             "orc_mj_init_persist": [_f32p, _f32p, _u32p, C.c_void_p, _i, _i, _f, _f, _f, C.c_void_p],
+            "orc_mj_recompute_k": [_f32p, C.c_void_p, _i, _i, _f, _f],
             "orc_nm_potential": [_f64p, _f64p, _f64p, _i, _i, _d, _d],
             "orc_nm_update": [_f64p, _f64p, _f64p, _f64p, _i32p, _i, _d, _d],
             "orc_nm_vcycle": [_f64p, _f64p, _i, _d, _i, _i, _i, _i],
@@ -449,9 +450,21 @@ class MoleculeJsDriver:
         SC = NN // 2 + 1
         self.SC = SC
 
-    def initialize(self):
-        O().mj_init(self.K, self.U, self.label, C.addressof(self.atoms), self.nA, self.S, self.h, self.h2, self.Rsing,
+    def initialize(self, init_pos=None):
+        """uploadInitialData (molecule.js:1905-2101).  init_pos: window.USER_INIT_POS, per entry an
+        (i, j) or None -- the trial psi and labels are built with those entries moved there (k kept,
+        :1909-1921), then K is rebuilt from 0 by recomputeK at the true positions (:1959-1981)."""
+        moved = self.atoms
+        if init_pos:
+            rows = [dict(r) for r in self.rows]
+            for n, p in enumerate(init_pos):
+                if p is not None and n < len(rows):
+                    rows[n]["i"], rows[n]["j"] = p[0], p[1]
+            moved = mj_atoms(rows)
+        O().mj_init(self.K, self.U, self.label, C.addressof(moved), self.nA, self.S, self.h, self.h2, self.Rsing,
                     self._splits_ptr())
+        if init_pos:
+            O().mj_recompute_k(self.K, C.addressof(self.atoms), self.nA, self.S, self.h, self.Rsing)
         self.bestU[:] = self.U
         self.Unext[:] = self.U
         self.label2[:] = self.label

@@ -896,6 +896,31 @@ void orc_mj_init(float* K, float* U, uint32_t* label, const orc_mj_atom* atoms, 
       }
 }
 
+/* molecule.js:1337-1370 recomputeK_WGSL: K from 0 over all S^3 points from the atoms' stored (u32)
+ * positions, distances ((f32)i - (f32)posI) * h, r_eff = max(r, rc) for pseudopotential atoms and
+ * max(r, R_SING) for bare Coulomb ones.  uploadInitialData runs it after a USER_INIT_POS
+ * initialisation, at the restored nucleus positions (:1959-1981). */
+void orc_mj_recompute_k(float* K, const orc_mj_atom* atoms, int nElec, int S, float h, float Rsing) {
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < S; ++i)
+    for (int j = 0; j < S; ++j)
+      for (int kk = 0; kk < S; ++kk) {
+        float Kval = 0.f;
+        for (int n = 0; n < nElec; ++n) {
+          float Za = atoms[n].Z;
+          float Zn = (atoms[n].Z_nuc > 0.f) ? atoms[n].Z_nuc : Za;
+          if (Za <= 0.f && Zn <= 0.f) continue;
+          float di = ((float)i - (float)atoms[n].posI) * h;
+          float dj = ((float)j - (float)atoms[n].posJ) * h;
+          float dk = ((float)kk - (float)atoms[n].posK) * h;
+          float r = sqrtf(di * di + dj * dj + dk * dk);
+          float reff = (atoms[n].rc > 0.f) ? fmaxf(r, atoms[n].rc) : fmaxf(r, Rsing);
+          Kval += Zn / reff;
+        }
+        K[IDX(i, j, kk, S)] = Kval;
+      }
+}
+
 /* molecule.js:4563-4582 + :1377-1426: moveNuclei's K rebuild -- K from 0 with the init
  * formula, the running maximum bestU and the current labels persist (an atom may take cells
  * over); psi is not touched. */

@@ -185,6 +185,7 @@ SIGNATURES = {
     "rq_set_splits": (C.c_int, [_V, _P]),
     "rq_restart": (C.c_int, [_V]),
     "rq_set_freeze_boundary": (C.c_int, [_V, _I]),
+    "rq_set_init_positions": (C.c_int, [_V, _P, _P, _I]),
     "rq_kernel_update_sp": (C.c_int, [_P, _P, _P, _P, _P, _I, _F, _F, _V]),
     "rq_kernel_jacobi_sp": (C.c_int, [_P, _P, _P, _I, _F, _F, _V]),
     "rq_kernel_labels_sp": (C.c_int, [_P, _P, _P, _I, _I, _F, _F, _V]),

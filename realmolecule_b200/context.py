@@ -126,6 +126,18 @@ class Context:
         self._chk(self.lib.rq_set_atoms(self.ctx, arr, len(arr)), "rq_set_atoms")
         self._atoms = arr
 
+    def set_init_positions(self, init_pos):
+        """molecule.js window.USER_INIT_POS: per entry an (i, j) grid position for the next
+        initialisation's trial psi and labels, or None (the entry's own position); K is rebuilt at
+        the true positions.  An empty list clears."""
+        n = len(init_pos)
+        pos = np.zeros(2 * n, np.float64)
+        has = np.zeros(n, np.int32)
+        for q, p in enumerate(init_pos):
+            if p is not None:
+                pos[2 * q], pos[2 * q + 1], has[q] = float(p[0]), float(p[1]), 1
+        self._chk(self.lib.rq_set_init_positions(self.ctx, _ptr(pos), _ptr(has), n), "rq_set_init_positions")
+
     def set_freeze_boundary(self, on: bool):
         """molecule.js flavour: window.FREEZE_BOUNDARY -- frames skip the level-set passes while on."""
         self._chk(self.lib.rq_set_freeze_boundary(self.ctx, 1 if on else 0), "rq_set_freeze_boundary")

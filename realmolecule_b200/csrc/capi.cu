@@ -105,12 +105,7 @@ static int upload_atoms(rq_ctx* c) {
     a5[q * 5 + 0] = (float)a.i; a5[q * 5 + 1] = (float)a.j; a5[q * 5 + 2] = (float)a.k;
     a5[q * 5 + 3] = (float)a.Z; a5[q * 5 + 4] = (float)a.rc;
     zd[q] = (float)a.Z; zd64[q] = a.Z;
-    // molecule.js:1882-1884 stores positions in a Uint32Array: truncation toward zero
-    mj[q].posI = (uint32_t)(a.i < 0 ? 0 : a.i); mj[q].posJ = (uint32_t)(a.j < 0 ? 0 : a.j);
-    mj[q].posK = (uint32_t)(a.k < 0 ? 0 : a.k);
-    mj[q].Z = (float)a.Z; mj[q].rc = (float)a.rc; mj[q].Z_nuc = (float)a.Z_nuc;
-    mj[q].initZeff = (float)(a.init_zeff > 0 ? a.init_zeff : a.Z);
-    mj[q].initRcut = (float)(a.init_rcut > 0 ? a.init_rcut : 1e6);
+    mj[q] = mj_record(a);
     nm[q * 4 + 0] = a.i * c->h; nm[q * 4 + 1] = a.j * c->h; nm[q * 4 + 2] = a.k * c->h; nm[q * 4 + 3] = a.Z_nuc;
   }
   CK(cudaMemcpyAsync(c->atoms5, a5.data(), sizeof(float) * a5.size(), cudaMemcpyHostToDevice, c->st));
@@ -553,6 +548,14 @@ extern "C" int rq_set_splits(rq_ctx* c, const rq_split* splits) {
     }
   CK(cudaMemcpyAsync(c->splits, d.data(), d.size() * sizeof(MjSplit), cudaMemcpyHostToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
+  return RQ_OK;
+}
+
+extern "C" int rq_set_init_positions(rq_ctx* c, const double* pos, const int32_t* has, int32_t n) {
+  if (!c || n < 0 || (n > 0 && (!pos || !has))) return RQ_EINVAL;
+  if (c->cfg.flavor != RQ_FLAVOR_MOLECULE_JS) return rq_fail(c, RQ_ENOTSUP, "USER_INIT_POS is molecule.js's");
+  c->init_pos.assign(pos, pos + 2 * (size_t)n);
+  c->init_has.assign(has, has + n);
   return RQ_OK;
 }
 

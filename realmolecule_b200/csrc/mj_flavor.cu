@@ -94,10 +94,33 @@ int mj_initialize(rq_ctx* c) {
   const size_t n = (size_t)c->g.S3;
   c->cu = c->cp = c->cl = 0;
   // molecule.js uploadInitialData (:1905-2101): K, trial psi and argmax labels over all S^3
-  // points; both psi buffers, both label buffers, P = Pother = 0, W = 1
+  // points; both psi buffers, both label buffers, P = Pother = 0, W = 1.  With USER_INIT_POS
+  // (:1909-1921) the trial psi and the labels come from the atoms moved to their init positions
+  // (i, j; k kept), then the true records go back and K is rebuilt from 0 by recomputeK
+  // (:1959-1981), and the labels' exclusion bits are recomputed for the true positions.
+  bool moved = false;
+  std::vector<MjAtom> tab((size_t)c->n_atoms);
+  for (int q = 0; q < c->n_atoms; ++q) {
+    rq_atom a = c->atoms[q];
+    if (q < (int)c->init_has.size() && c->init_has[q]) {
+      a.i = c->init_pos[2 * q];
+      a.j = c->init_pos[2 * q + 1];
+      moved = true;
+    }
+    tab[q] = mj_record(a);
+  }
+  if (moved) CK(cudaMemcpyAsync(c->atoms_mj, tab.data(), sizeof(MjAtom) * tab.size(), cudaMemcpyHostToDevice, c->st));
   LAUNCH(RQ_KC_OTHER, 12.0 * c->g.S3,
          launch_mj_init((float*)c->K, (float*)c->U[0], c->bestU, c->lab[0], atoms_dev(c), c->n_atoms, c->g, p.h, p.h2,
                         p.Rsing, p.hasBare, false, c->splits, c->st));
+  if (moved) {
+    for (int q = 0; q < c->n_atoms; ++q) tab[q] = mj_record(c->atoms[q]);
+    CK(cudaMemcpyAsync(c->atoms_mj, tab.data(), sizeof(MjAtom) * tab.size(), cudaMemcpyHostToDevice, c->st));
+    LAUNCH(RQ_KC_OTHER, 4.0 * c->g.S3,
+           launch_mj_recompute_k((float*)c->K, atoms_dev(c), c->n_atoms, c->g, p.h, p.Rsing, c->st));
+    LAUNCH(RQ_KC_OTHER, 8.0 * c->g.S3, launch_mj_flags(c->lab[0], atoms_dev(c), c->n_atoms, c->g, p.h, p.hasBare, c->st));
+    CK(cudaStreamSynchronize(c->st));  // the table is a copy source
+  }
   CK(cudaMemcpyAsync(c->U[1], c->U[0], n * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
   CK(cudaMemcpyAsync(c->lab[1], c->lab[0], n * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
   for (int b = 0; b < 2; ++b) CK(cudaMemsetAsync(c->P[b], 0, n * sizeof(float), c->st));

@@ -106,6 +106,9 @@ struct rq_ctx {
   unsigned long long* lock = nullptr;
   // molecule.js window.FREEZE_BOUNDARY: frames skip the level-set passes
   bool freeze = false;
+  // molecule.js window.USER_INIT_POS: (i, j) per entry where init_has is set (the next initialisation)
+  std::vector<double> init_pos;
+  std::vector<int> init_has;
   // molecule.js shell splits per entry (n_atoms, zero = none)
   MjSplit* splits = nullptr;
   float* lob_part = nullptr;

@@ -8,6 +8,20 @@ struct MjAtom {
   uint32_t posI, posJ, posK;
   float Z, rc, Z_nuc, initZeff, initRcut;
 };
+// The record of one entry: molecule.js:1882-1884 stores positions in a Uint32Array (truncation
+// toward zero), the rest as f32; initZeff defaults to Z, initRcut to 1e6.
+inline MjAtom mj_record(const rq_atom& a) {
+  MjAtom m;
+  m.posI = (uint32_t)(a.i < 0 ? 0 : a.i);
+  m.posJ = (uint32_t)(a.j < 0 ? 0 : a.j);
+  m.posK = (uint32_t)(a.k < 0 ? 0 : a.k);
+  m.Z = (float)a.Z;
+  m.rc = (float)a.rc;
+  m.Z_nuc = (float)a.Z_nuc;
+  m.initZeff = (float)(a.init_zeff > 0 ? a.init_zeff : a.Z);
+  m.initRcut = (float)(a.init_rcut > 0 ? a.init_rcut : 1e6);
+  return m;
+}
 // An entry's shell split (the atom record's split fields, molecule.js:183-191): type 0/1 whole
 // sphere, 2 half space, 3 one of three 120-degree sectors; idx, axis, angular offset rot.
 struct MjSplit {

@@ -48,9 +48,12 @@ class MoleculePage:
                  shear_rate: float = 0.0, brownian: bool = False, brownian_gamma: float = 1.0,
                  thermal_kick: Optional[float] = None, seed: int = 0, locked_groups=(), splits=(), split_groups=(),
                  classical_md=None, sasa=None, init_zeff=None, init_rcut=None, user_init_zeff=None,
-                 user_init_rcut=None, freeze_boundary=False, unlock_at_step=None, context=None, **ctx_opts):
+                 user_init_rcut=None, freeze_boundary=False, unlock_at_step=None, init_pos=None, context=None,
+                 **ctx_opts):
         self.rows = [dict(a) for a in atoms]
         n = self.n = len(self.rows)
+        # USER_INIT_POS (molecule.js:1909-1921): per entry (i, j) of its trial psi, or None
+        self.init_pos = [None if p is None else (float(p[0]), float(p[1])) for p in (init_pos or [])]
         self.NN, self.screen = int(NN), float(screen)
         self.h = self.screen / self.NN
         self.Z_orig = [float(a.get("Z", 0.0)) for a in self.rows]
@@ -155,7 +158,7 @@ class MoleculePage:
                           ("USER_BROWNIAN_GAMMA", "brownian_gamma"), ("USER_THERMAL_KICK", "thermal_kick"),
                           ("USER_LOCKED_GROUPS", "locked_groups"), ("USER_SPLIT_GROUPS", "split_groups"),
                           ("USER_CLASSICAL_MD", "classical_md"), ("USER_SASA", "sasa"), ("INIT_ZEFF", "init_zeff"),
-                          ("INIT_RCUT", "init_rcut"), ("USER_INIT_ZEFF", "user_init_zeff"),
+                          ("INIT_RCUT", "init_rcut"), ("USER_INIT_ZEFF", "user_init_zeff"), ("USER_INIT_POS", "init_pos"),
                           ("USER_INIT_RCUT", "user_init_rcut"), ("FREEZE_BOUNDARY", "freeze_boundary"),
                           ("UNLOCK_AT_STEP", "unlock_at_step"),
                           # context options of the GPU frame
@@ -438,7 +441,9 @@ class MoleculePage:
         self.converged_at = None
 
     def initialize(self):
-        """uploadInitialData on the device."""
+        """uploadInitialData on the device (with USER_INIT_POS, molecule.js:1905-1981, when given)."""
+        if self.init_pos:
+            self.ctx.set_init_positions(self.init_pos)
         self.ctx.initialize()
         self._reset_counters()
 

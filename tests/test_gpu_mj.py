@@ -411,3 +411,33 @@ def test_freeze_boundary_then_release_bit_exact():
     assert np.array_equal(st["label"], ref.label.astype(np.int32))
     assert np.array_equal(st["W"].view(np.uint32), ref.W.view(np.uint32))
     assert np.array_equal(st["psi"].view(np.uint32), ref.U.view(np.uint32))
+
+
+@pytest.mark.parametrize("kind", ["water", "bare"])
+def test_init_positions(kind):
+    """window.USER_INIT_POS (molecule.js:1905-1981): trial psi and labels from the atoms moved to
+    their init positions (k kept), K rebuilt by recomputeK at the true positions -- K bit-exact,
+    psi within 2 ulp, labels up to near-ties; then frames from the uploaded state bit-exact."""
+    from realmolecule_b200 import Context
+    NN, screen, rows = atoms_case(kind)
+    init = [(r["i"] + 2, r["j"] - 1) if q % 2 == 0 else None for q, r in enumerate(rows)]
+    opts = dict(steps_per_frame=7, norm_interval=5, vcycle_interval=3)
+    ref = orc.MoleculeJsDriver(NN, screen, rows, **opts)
+    ref.initialize(init_pos=init)
+    plain = orc.MoleculeJsDriver(NN, screen, rows, **opts)
+    plain.initialize()
+    assert (ref.label != plain.label).sum() > 100  # the moved trial psi changes the labels
+    ctx = Context(NN, screen, rows, flavor="molecule.js", **opts)
+    ctx.set_init_positions(init)
+    ctx.initialize()
+    assert np.array_equal(ctx.download_K().view(np.uint32), ref.K.view(np.uint32))
+    st = ctx.download(psi=True, label=True)
+    np.testing.assert_allclose(st["psi"], ref.U, rtol=3e-7, atol=0)
+    assert np.flatnonzero(st["label"] != ref.label.astype(np.int32)).size <= 3
+    ctx.upload(psi=ref.U, label=ref.label.astype(np.int32))
+    for _ in range(14):
+        ref.step()
+    ctx.step(14)
+    st = ctx.download(psi=True, label=True)
+    assert np.array_equal(st["psi"].view(np.uint32), ref.U.view(np.uint32))
+    assert np.array_equal(st["label"], ref.label.astype(np.int32))
