@@ -349,8 +349,9 @@ RQ_API int rq_batch_set_wait(rq_batch* b, int64_t limit_ns, int32_t extra_arriva
  *      planes per thread; per-kernel graph or persistent launch) runs one schedule period to capture
  *      it and one timed by CUDA events; the fastest per step is kept.
  *   2. Smoother sweeps (mg_pre, mg_post, mg_coarse_sweeps): from P = 0 each candidate runs 3 V-cycles
- *      on the batch's current psi; the one with the largest -ln(rho) per ms (rho: fine-grid residual
- *      reduction per cycle) is kept.
+ *      on the batch's current psi (rho: fine-grid residual reduction per cycle); the cheapest cycle
+ *      whose rho is within 5 % of V(1,1)'s is kept (a warm-started cycle every poisson_interval steps
+ *      at V(1,1)'s rate already keeps P on the ITP state).
  * The kept values go into the batch's configuration (batch_tile, batch_persistent, mg_*), and the
  * report lists every candidate. */
 typedef struct rq_tune_report {

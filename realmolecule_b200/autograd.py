@@ -32,11 +32,14 @@ from .context import Context
 class EnergyModel:
     def __init__(self, NN: int, h: float, charges: Sequence[float], positions: np.ndarray,
                  seeds: np.ndarray, precision: str = "fp64", tol: Optional[float] = 1e-10, max_steps: int = 50000,
-                 check_interval: int = 100, warm_steps: int = 0, adjoint: bool = True, **opts):
+                 check_interval: int = 100, warm_steps: int = 0, adjoint: bool = True, cold: bool = False,
+                 **opts):
         """tol None: each evaluation runs exactly ``warm_steps`` imaginary-time steps from the previous
         state (the fixed warm-started iterations of the geometry workloads) instead of a solve, and
         those steps are recorded for the adjoint.  adjoint False: no recording; the gradient is the
-        Hellmann-Feynman one (exact only at convergence), for comparison."""
+        Hellmann-Feynman one (exact only at convergence), for comparison.  cold True (with tol None):
+        every evaluation starts from the initial state (nearest-seed labels, held fixed), so E is a
+        function of the positions alone -- E_N(R) -- and the adjoint force is its exact gradient."""
         self.NN, self.h = int(NN), float(h)
         self.S3 = (self.NN + 1) ** 3
         self.charges = np.asarray(charges, np.float64)
@@ -45,10 +48,12 @@ class EnergyModel:
         self.tol, self.max_steps, self.check = tol, max_steps, check_interval
         self.warm_steps = warm_steps
         rows = self._rows(np.asarray(positions, np.float64))
-        opts.setdefault("label_until", 400)
+        self.cold = bool(cold) and tol is None
+        opts.setdefault("label_until", 1 if self.cold else 400)
         self.ctx = Context(self.NN, self.NN * self.h, rows, flavor="new", precision=precision, **opts)
         self.ctx.initialize()
-        self.ctx.step(opts["label_until"])  # let the level set settle, then labels stay fixed
+        if not self.cold:
+            self.ctx.step(opts["label_until"])  # let the level set settle, then labels stay fixed
         if adjoint and tol is None and warm_steps > 0:
             self.ctx.set_adjoint_window(warm_steps)
         self._has_v = False
@@ -71,6 +76,8 @@ class EnergyModel:
             self.ctx.set_external_potential(v)
             self._has_v = v is not None
         if self.tol is None:
+            if self.cold:
+                self.ctx.initialize()  # the state every evaluation starts from (independent of R)
             self.ctx.step(self.warm_steps)
             steps, E = self.warm_steps, float(self.ctx.energy()[L.E_TOTAL])
         else:

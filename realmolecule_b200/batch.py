@@ -69,8 +69,8 @@ class Batch:
 
     def autotune(self) -> dict:
         """rq_batch_autotune: pick the march tile and launch form (timed per step) and the smoother
-        sweeps (V-cycle convergence per ms); the choice stays in the batch.  Returns the choice and
-        every candidate's measurement."""
+        sweeps (the cheapest V-cycle converging within 5 % of V(1,1)'s rate); the choice stays in
+        the batch.  Returns the choice and every candidate's measurement."""
         r = L.TuneReport()
         self._chk(self.lib.rq_batch_autotune(self.b, C.byref(r)), "rq_batch_autotune")
         tiles = [{"tile": f"{1 << (r.tile[i] & 0xff)}x{256 >> (r.tile[i] & 0xff)}x{r.tile[i] >> 8}",

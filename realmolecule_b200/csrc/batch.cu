@@ -1596,7 +1596,7 @@ extern "C" int rq_batch_autotune(rq_batch* b, rq_tune_report* out) {
   if (rc == RQ_OK) rc = b_flush(b);
   const int cand[7][3] = {{1, 1, 16}, {2, 1, 16}, {1, 2, 16}, {2, 2, 16}, {1, 1, 8}, {1, 1, 32}, {2, 2, 32}};
   const rq_config keepc = b->cfg;
-  double best_eff = -1.0;
+  double best_eff = -1.0;  // the kept candidate's ms per cycle
   int ns = 0;
   for (int c = 0; c < 7 && rc == RQ_OK; ++c) {
     b->cfg.mg_pre = cand[c][0];
@@ -1632,11 +1632,18 @@ extern "C" int rq_batch_autotune(rq_batch* b, rq_tune_report* out) {
     out->coarse_sweeps[ns] = cand[c][2];
     out->rho[ns] = rho;
     out->ms_per_cycle[ns] = ms / 3.0;
-    const double eff = (rho > 0 && rho < 1) ? -std::log(rho) / (ms / 3.0) : 0.0;
-    if (eff > best_eff) { best_eff = eff; out->best_smooth = ns; }
     ++ns;
   }
   out->n_smooth = ns;
+  // The cheapest cycle that reduces the residual at least as well as V(1,1) with 16 coarsest sweeps
+  // (candidate 0, to 5 %): one warm-started cycle every poisson_interval steps already keeps P on
+  // the ITP state at that rate (mixed and FP64 solves take the same steps), so more smoothing only
+  // costs time.
+  for (int c = 0; c < ns; ++c)
+    if (out->rho[c] <= 1.05 * out->rho[0] && (best_eff < 0 || out->ms_per_cycle[c] < best_eff)) {
+      best_eff = out->ms_per_cycle[c];
+      out->best_smooth = c;
+    }
   if (rc == RQ_OK && ns > 0) {
     b->cfg.mg_pre = out->pre[out->best_smooth];
     b->cfg.mg_post = out->post[out->best_smooth];
