@@ -34,7 +34,10 @@ period with the flush before EVERY solver step (every kernel reads HBM cold).
            ``max_abs_dE_Ha`` compares the mixed and FP64 answers; ``forces`` the mixed and FP64
            forces.  Times are CUDA events around initialise + solve on the solver stream.
 ``batch_step`` the C3 batch step alone (all 96 clusters active, mixed precision): Gpt/s, launches
-           per step and the composite HBM roofline of its kernels.
+           per step and the composite HBM roofline of its kernels, before and after the autotuner.
+``geometry`` the C4 / C5 geometry workloads for a few geometry steps each (100 waters, 192^3, FIRE,
+           200 iterations per step; 1000 waters, 320^3, velocity Verlet, 50 iterations per step;
+           mixed precision, adjoint forces): wall time per geometry step and its parts.
 
 ``callers`` the other reference callers of the step through their drop-ins, each beside its CPU
            restatement: the recorded hairpin job (RealQMSolver), atom.js's He page, mol_fast.js's
@@ -320,6 +323,7 @@ def run_ours(a):
     conv = None if a.no_converge else converge_leg(stream, dist, rank, world)
     batch = None if a.no_converge or rank != 0 else batch_leg(stream, measured_peak()[0])
     callers = None if a.no_converge or rank != 0 else caller_legs(a)
+    geometry = None if a.no_converge or rank != 0 else geometry_leg()
 
     if rank == 0:
         peak, peak_kind = measured_peak()
@@ -364,6 +368,7 @@ def run_ours(a):
             "converge": conv,
             "batch_step": batch,
             "callers": callers,
+            "geometry": geometry,
             "clocks": clk.summary(),
             "gpu_launches": launches,
         }
@@ -510,6 +515,41 @@ def _max_over_ranks(dist, x):
     t = torch.tensor([x], device="cuda", dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def geometry_leg():
+    """C4 and C5 for a few geometry steps each, through dynamics.geometry_model (each evaluation:
+    the warm-started iterations recorded for the adjoint, the energy, the adjoint forces and the
+    nuclear terms).  Synchronised wall clock per geometry step; per-class CUDA-event kernel times of
+    one evaluation's parts."""
+    import time
+    from realmolecule_b200 import configs, dynamics, _lib as L
+    out = {}
+    for name, g, iters, pre, n in (("water100_fire", configs.water100(), 200, 2000, 4),
+                                    ("water1000_verlet", configs.water1000(), 50, 3000, 3)):
+        model, Z, off = dynamics.geometry_model(g, "mixed", iters, adjoint=True)
+        model.ctx.step(pre)
+        model.ctx.synchronize()
+        parts = {}
+        for part, fn in (("K", lambda: model.ctx.set_atoms(model._rows(g.xyz + off))),
+                         ("iterations", lambda: model.ctx.step(iters)), ("energy", lambda: model.ctx.energy()),
+                         ("adjoint_forces", lambda: model.ctx.forces(L.FORCE_ADJOINT))):
+            model.ctx.profile_begin()
+            fn()
+            model.ctx.synchronize()
+            parts[part] = round(sum(v["ms"] for v in model.ctx.profile_end().values()), 3)
+        x0, m = g.xyz + off, dynamics.masses_for(Z)
+        t0 = time.perf_counter()
+        if name.endswith("fire"):
+            tr = dynamics.fire(model, x0, max_steps=n, masses=m)
+        else:
+            tr = dynamics.velocity_verlet(model, x0, np.zeros_like(x0), m, 0.5 * dynamics.FS, n)
+        dt = time.perf_counter() - t0
+        out[name] = {"grid": f"{g.NN}^3", "nuclei": len(Z), "domains": len(g.seeds), "iterations_per_step": iters,
+                     "geometry_steps": len(tr.energies), "ms_per_geometry_step": dt / len(tr.energies) * 1e3,
+                     "kernel_ms_of_one_evaluation": parts, "E_first": tr.energies[0], "E_last": tr.energies[-1]}
+        model.ctx.close()
+    return out
 
 
 def caller_legs(a):
@@ -713,13 +753,35 @@ def converge_leg(stream, dist, rank, world):
     forces = _glycine_forces(g, rows, keep["mixed"], keep["fp64"])
     for c in keep.values():
         c.close()
+    n_int = (g.NN - 1) ** 3
     out["glycine128"] = {"electrons": int(g.charges.sum()), "grid": f"{g.NN}^3 h={g.h}",
                          "mixed_s": gly["mixed"][0], "fp64_s": gly["fp64"][0],
+                         "gpts_mixed": gly["mixed"][1] * n_int / gly["mixed"][0] / 1e9,
+                         "gpts_fp64": gly["fp64"][1] * n_int / gly["fp64"][0] / 1e9,
                          "speedup_vs_fp64": gly["fp64"][0] / gly["mixed"][0],
                          "steps_mixed": gly["mixed"][1], "steps_fp64": gly["fp64"][1],
                          "mixed_promoted_to_fp64": gly["mixed"][3],
                          "E_mixed": gly["mixed"][2], "E_fp64": gly["fp64"][2],
                          "abs_dE_Ha": abs(gly["mixed"][2] - gly["fp64"][2]), "forces": forces}
+
+    # water 64^3 (the H2O configuration in the new flavour), one context per precision
+    w = configs.h2o64()
+    rows_w = configs.to_domain_atoms(w)
+    wat = {}
+    for prec in ("fp64", "mixed"):
+        c = Context(w.NN, w.screen, rows_w, flavor="new", precision=prec, label_until=LABEL_UNTIL,
+                    converge_checks=CHECKS)
+        c.set_stream(stream.cuda_stream)
+        (steps, E), t = _timed(stream, lambda: (c.initialize(), c.solve(TOL, MAX_STEPS, CHECK))[1])
+        wat[prec] = (_max_over_ranks(dist, t), int(steps), float(E))
+        c.close()
+    n_w = (w.NN - 1) ** 3
+    out["water64"] = {"electrons": int(w.charges.sum()), "grid": f"{w.NN}^3 h={w.h}",
+                      "fp64_s": wat["fp64"][0], "mixed_s": wat["mixed"][0],
+                      "steps_fp64": wat["fp64"][1], "steps_mixed": wat["mixed"][1],
+                      "gpts_fp64": wat["fp64"][1] * n_w / wat["fp64"][0] / 1e9,
+                      "gpts_mixed": wat["mixed"][1] * n_w / wat["mixed"][0] / 1e9,
+                      "E_fp64": wat["fp64"][2], "abs_dE_Ha": abs(wat["fp64"][2] - wat["mixed"][2])}
 
     # 96 water clusters: this rank's cost share, mixed batch vs one FP64 context per instance
     geoms = configs.clusters96()
