@@ -42,6 +42,7 @@ struct BInst {
   int nSeed;
   const double* K64;  // fp32 instances of a mixed batch: the FP64 K of its promotion set, read by the readout
   double* cs;         // FP64 working copy of the coarsest level (P and f) for the persistent launch
+  unsigned char* nbm; // same-label neighbour mask of the current labels (rebuilt after every label change)
 };
 
 struct BItem {
@@ -53,13 +54,13 @@ struct BItem {
 // registers first: through a reference into the instance table the compiler would re-read it
 // after every store, as it cannot prove the field pointers do not alias the table.
 // ---------------------------------------------------------------------------------------
-template <typename T, bool ACC>
+template <typename T, bool ACC, bool SR>
 __global__ void __launch_bounds__(256) kb_update(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cu,
                                                  int cp, int cl, T half_dv, T dt, double* __restrict__ norms,
                                                  const double* __restrict__ scale, const unsigned* __restrict__ seed,
                                                  unsigned* __restrict__ seed_next, NmTile tile) {
   __shared__ DomTable<1, 128> tab;
-  if (seed && blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) *seed_next = *seed + 1u;
+  if (SR && blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) *seed_next = *seed + 1u;
   const BItem it = items[blockIdx.x];
   const BInst& I = ins[it.inst];
   double* nrm = norms ? norms + I.dom0 : nullptr;
@@ -68,9 +69,9 @@ __global__ void __launch_bounds__(256) kb_update(const BInst* __restrict__ ins, 
     __syncthreads();
   }
   const Geo g = I.g;
-  nm_update_body<T, ACC>((const T*)I.U[cu], (T*)I.U[1 - cu], (const T*)I.K, (const T*)I.P[cp], I.lab[cl], g, half_dv,
-                         dt, I.h * I.h * I.h, I.nDom, nrm, tab, it.bx, it.by, it.bz, scale ? scale + I.dom0 : nullptr,
-                         seed, tile);
+  nm_update_body<T, ACC, true, SR>((const T*)I.U[cu], (T*)I.U[1 - cu], (const T*)I.K, (const T*)I.P[cp], I.lab[cl], g,
+                               half_dv, dt, I.h * I.h * I.h, I.nDom, nrm, tab, it.bx, it.by, it.bz,
+                               scale ? scale + I.dom0 : nullptr, seed, tile, I.nbm);
   if (ACC) {
     __syncthreads();
     dom_table_flush(tab, nrm);
@@ -185,6 +186,13 @@ __global__ void __launch_bounds__(256) kb_evolve(const BInst* __restrict__ ins, 
   nm_evolve_body<T>(I.lab[cl], I.lab[1 - cl], (const T*)I.U[cu], I.W, g, dt_w, curv, it.bx, it.by, it.bz, tile);
 }
 
+// the same-label neighbour mask of the current labels (flat16 items)
+__global__ void __launch_bounds__(256) kb_mask(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cl) {
+  const BItem it = items[blockIdx.x];
+  const BInst& I = ins[it.inst];
+  nm_mask_body(I.lab[cl], I.nbm, I.g, it.bx);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) kb_potential(const BInst* __restrict__ ins, const BItem* __restrict__ items,
                                                     double sigma_scale) {
@@ -269,7 +277,7 @@ __global__ void __launch_bounds__(256) kb_resnorm(const BInst* __restrict__ ins,
 // ---------------------------------------------------------------------------------------
 enum BPhaseKind : int {
   kPhApply, kPhZeroNorms, kPhUpdate, kPhUpdateAcc, kPhScale, kPhRbgs, kPhCoarsest, kPhResidual, kPhRestrict,
-  kPhZero, kPhProlong, kPhEvolve
+  kPhZero, kPhProlong, kPhEvolve, kPhMask
 };
 
 struct BPhase {
@@ -335,15 +343,15 @@ __device__ __forceinline__ void kb_run_item(const BPersist& a, const BPhase& P, 
       if (P.kind == kPhUpdateAcc) {
         dom_table_init(tab);
         __syncthreads();
-        nm_update_body<T, true>((const T*)I.U[P.cu], (T*)I.U[1 - P.cu], (const T*)I.K, (const T*)I.P[P.cp], I.lab[P.cl],
-                                g, (T)a.half_dv, (T)a.dt, I.h * I.h * I.h, I.nDom, a.dnorm + I.dom0, tab, it.bx, it.by,
-                                it.bz, sc, P.seed, a.tile);
+        nm_update_body<T, true, true>((const T*)I.U[P.cu], (T*)I.U[1 - P.cu], (const T*)I.K, (const T*)I.P[P.cp],
+                                      I.lab[P.cl], g, (T)a.half_dv, (T)a.dt, I.h * I.h * I.h, I.nDom, a.dnorm + I.dom0,
+                                      tab, it.bx, it.by, it.bz, sc, P.seed, a.tile, I.nbm);
         __syncthreads();
         dom_table_flush(tab, a.dnorm + I.dom0);
       } else {
-        nm_update_body<T, false>((const T*)I.U[P.cu], (T*)I.U[1 - P.cu], (const T*)I.K, (const T*)I.P[P.cp],
-                                 I.lab[P.cl], g, (T)a.half_dv, (T)a.dt, I.h * I.h * I.h, I.nDom, nullptr, tab, it.bx,
-                                 it.by, it.bz, sc, P.seed, a.tile);
+        nm_update_body<T, false, true>((const T*)I.U[P.cu], (T*)I.U[1 - P.cu], (const T*)I.K, (const T*)I.P[P.cp],
+                                       I.lab[P.cl], g, (T)a.half_dv, (T)a.dt, I.h * I.h * I.h, I.nDom, nullptr, tab,
+                                       it.bx, it.by, it.bz, sc, P.seed, a.tile, I.nbm);
       }
       break;
     }
@@ -397,6 +405,9 @@ __device__ __forceinline__ void kb_run_item(const BPersist& a, const BPhase& P, 
                         it.bz, a.tile);
       break;
     }
+    case kPhMask:
+      nm_mask_body(I.lab[P.cl], I.nbm, I.g, it.bx);
+      break;
     default:
       break;
   }
@@ -665,6 +676,7 @@ static int build(rq_batch* b) {
     BInst& I = b->hin[q];
     BRC(alloc_fields(b, I, b->f64[q] ? sizeof(double) : sizeof(float)));
     for (int k = 0; k < 2; ++k) BALLOC(I.lab[k], (size_t)I.g.S3 * sizeof(int));
+    BALLOC(I.nbm, (size_t)I.g.S3);
     BALLOC(I.W, (size_t)I.g.S3 * sizeof(float));
     const int lc = I.nlev - 1;
     b->coarse_smem[lc] = std::max(b->coarse_smem[lc], sizeof(double) * 2 * (size_t)I.lg[lc].S3);
@@ -871,6 +883,21 @@ static int b_flush(rq_batch* b) {
 // updates ran since the last normalisation
 static int b_ready(rq_batch* b) { return b->age == 0 ? b_flush(b) : b_normalize(b); }
 
+// the same-label neighbour masks of the current labels, for every active instance
+static int b_mask(rq_batch* b) {
+  for (int p = 0; p < 2; ++p) {
+    const rq_batch::Plan& f = b->pl[p].flat16;
+    if (!f.n) continue;
+    if (b->rec) {
+      b_record(b, kPhMask, p, &f);
+      continue;
+    }
+    kb_mask<<<f.n, 256, 0, b->st>>>(b->din, f.d, b->cl);
+    BL("mask");
+  }
+  return RQ_OK;
+}
+
 static bool any_active(const rq_batch* b) { return b->pl[kF32].march[0].n + b->pl[kF64].march[0].n > 0; }
 
 static int b_step(rq_batch* b, int s) {
@@ -907,12 +934,19 @@ static int b_step(rq_batch* b, int s) {
       b->rec->back().seed_next = sn;
       return RQ_OK;
     }
-    if (norm)
-      kb_update<T, true><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cp, b->cl, (T)hd, (T)dt, b->dnorm,
-                                                             sc, sd, sn, b->tile);
+    double* nrm = norm ? b->dnorm : nullptr;
+    if (norm && sr)
+      kb_update<T, true, true><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cp, b->cl, (T)hd, (T)dt,
+                                                                   nrm, sc, sd, sn, b->tile);
+    else if (norm)
+      kb_update<T, true, false><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cp, b->cl, (T)hd, (T)dt,
+                                                                    nrm, sc, sd, sn, b->tile);
+    else if (sr)
+      kb_update<T, false, true><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cp, b->cl, (T)hd, (T)dt,
+                                                                    nrm, sc, sd, sn, b->tile);
     else
-      kb_update<T, false><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cp, b->cl, (T)hd, (T)dt, nullptr,
-                                                              sc, sd, sn, b->tile);
+      kb_update<T, false, false><<<m.n, nm_march_block(), 0, b->st>>>(b->din, m.d, b->cu, b->cp, b->cl, (T)hd, (T)dt,
+                                                                     nrm, sc, sd, sn, b->tile);
     BL("update");
     return RQ_OK;
   }));
@@ -944,6 +978,7 @@ static int b_step(rq_batch* b, int s) {
       return RQ_OK;
     }));
     b->cl ^= 1;
+    BRC(b_mask(b));
   }
   return RQ_OK;
 }
@@ -969,6 +1004,7 @@ static int b_initialize(rq_batch* b) {
     BCK(launch_fill(I.W, 1.0f, I.g.S3, b->st));
   }
   BRC(b_normalize(b));
+  BRC(b_mask(b));
   for (int v = 0; v < 10; ++v) BRC(each_set([&](auto tag, int p) { return b_vcycle<decltype(tag)>(b, p); }));
   b->steps_done = 0;
   BCK(cudaStreamSynchronize(b->st));
@@ -1110,7 +1146,8 @@ static int b_phase_items(const rq_batch* b, const BPhase& x, int q) {
   if (!b->active[q] || (b->f64[q] ? kF64 : kF32) != x.set) return 0;
   const InstItems& it = b->items[q];
   switch (x.kind) {
-    case kPhApply: return (int)it.flat16.size();
+    case kPhApply:
+    case kPhMask: return (int)it.flat16.size();
     case kPhZeroNorms:
     case kPhScale: return 1;
     case kPhUpdate:

@@ -190,14 +190,44 @@ __device__ __forceinline__ float sr_round(double v, unsigned u24) {
 // scale[label] * update(psi), formed in FP64 and rounded once -- normalise-then-update up to
 // rounding, without a separate pass over psi.  With a non-null `seed` (fp32 fields) the stored
 // value is rounded without bias (sr_round) from its exact FP64 form.
-template <typename T, bool ACC>
+// Same-label neighbour mask of one interior point: bit q set when neighbour q (+i, -i, +j, -j,
+// +k, -k) carries the point's label.  The update reads it in place of the six neighbour labels
+// while the labels do not change (nm_mask_body writes it after every label change).
+constexpr int kNmIp = 1, kNmIm = 2, kNmJp = 4, kNmJm = 8, kNmKp = 16, kNmKm = 32;
+__device__ __forceinline__ unsigned char nm_same_label_mask(const int* __restrict__ label, long long id, long long S,
+                                                            long long S2) {
+  const int l = label[id];
+  return (unsigned char)((label[id + S2] == l ? kNmIp : 0) | (label[id - S2] == l ? kNmIm : 0) |
+                         (label[id + S] == l ? kNmJp : 0) | (label[id - S] == l ? kNmJm : 0) |
+                         (label[id + 1] == l ? kNmKp : 0) | (label[id - 1] == l ? kNmKm : 0));
+}
+
+// The mask of every point of S^3 (0 on the boundary planes), flat: 256 * kNmFlatChunk points from blk.
+__device__ __forceinline__ void nm_mask_body(const int* __restrict__ label, unsigned char* __restrict__ mask,
+                                             const Geo& g, long long blk) {
+  const long long base = blk * blockDim.x * kNmFlatChunk;
+  for (int q = 0; q < kNmFlatChunk; ++q) {
+    const long long id = base + (long long)q * blockDim.x + threadIdx.x;
+    if (id >= g.S3) break;
+    const int i = (int)(id / g.S2), j = (int)((id / g.S) % g.S), k = (int)(id % g.S);
+    const bool interior = i >= 1 && i < g.NN && j >= 1 && j < g.NN && k >= 1 && k < g.NN;
+    mask[id] = interior ? nm_same_label_mask(label, id, g.S, g.S2) : (unsigned char)0;
+  }
+}
+
+// MASK: neighbour-label equality from `mask` (nm_mask_body of the same labels) instead of six label
+// loads; the centre label is then read only where it is used (norm accumulation, pending scale).
+// The arithmetic is the same, so both forms give the same bits.
+// SR: the unbiased rounding of fp32 fields (seed non-null), compiled only where it is asked for
+template <typename T, bool ACC, bool MASK = false, bool SR = false>
 __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __restrict__ Unew, const T* __restrict__ K,
                                                const T* __restrict__ P, const int* __restrict__ label, const Geo& g,
                                                T half_dv, T dt, double h3, int nDom, double* __restrict__ norms,
                                                DomTable<1, 128>& tab, int bx, int by, int bz,
                                                const double* __restrict__ scale = nullptr,
                                                const unsigned* __restrict__ seed = nullptr,
-                                               const NmTile t = kNmTile) {
+                                               const NmTile t = kNmTile,
+                                               const unsigned char* __restrict__ mask = nullptr) {
   using A = Ar<T>;
   RunSum<1> rs;
   rs.reset();
@@ -207,25 +237,39 @@ __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __res
     const int iend = min(i0 + t.march, g.NN);
     const long long S = g.S, S2 = g.S2;
     long long id = (long long)i0 * S2 + j * S + k;
-    const unsigned sd = seed ? __ldg(seed) : 0u;
+    const unsigned sd = (SR && seed) ? __ldg(seed) : 0u;
+    const bool need_l = !MASK || ACC || scale != nullptr;
     T u_m = __ldg(U + id - S2), u_c = __ldg(U + id);
-    int l_m = __ldg(label + id - S2), l_c = __ldg(label + id);
+    int l_m = MASK ? 0 : __ldg(label + id - S2), l_c = need_l ? __ldg(label + id) : 0;
     for (int i = i0; i < iend; ++i, id += S2) {
       const T u_p = __ldg(U + id + S2);
-      const int l_p = __ldg(label + id + S2);
       const T ujp = __ldg(U + id + S), ujm = __ldg(U + id - S), ukp = __ldg(U + id + 1), ukm = __ldg(U + id - 1);
-      const int ljp = __ldg(label + id + S), ljm = __ldg(label + id - S), lkp = __ldg(label + id + 1),
-                lkm = __ldg(label + id - 1);
       const T kv = __ldg(K + id), pv = __ldg(P + id);
-      const T a = (l_p == l_c) ? u_p : u_c;
-      const T b = (l_m == l_c) ? u_m : u_c;
-      const T c = (ljp == l_c) ? ujp : u_c;
-      const T d = (ljm == l_c) ? ujm : u_c;
-      const T e = (lkp == l_c) ? ukp : u_c;
-      const T f = (lkm == l_c) ? ukm : u_c;
+      T a, b, c, d, e, f;
+      int l_p = 0;
+      if (MASK) {
+        const unsigned m = __ldg(mask + id);
+        if (need_l && i + 1 < iend) l_p = __ldg(label + id + S2);
+        a = (m & kNmIp) ? u_p : u_c;
+        b = (m & kNmIm) ? u_m : u_c;
+        c = (m & kNmJp) ? ujp : u_c;
+        d = (m & kNmJm) ? ujm : u_c;
+        e = (m & kNmKp) ? ukp : u_c;
+        f = (m & kNmKm) ? ukm : u_c;
+      } else {
+        l_p = __ldg(label + id + S2);
+        const int ljp = __ldg(label + id + S), ljm = __ldg(label + id - S), lkp = __ldg(label + id + 1),
+                  lkm = __ldg(label + id - 1);
+        a = (l_p == l_c) ? u_p : u_c;
+        b = (l_m == l_c) ? u_m : u_c;
+        c = (ljp == l_c) ? ujp : u_c;
+        d = (ljm == l_c) ? ujm : u_c;
+        e = (lkp == l_c) ? ukp : u_c;
+        f = (lkm == l_c) ? ukm : u_c;
+      }
       const T lap = A::sub(A::add(A::add(A::add(A::add(A::add(a, b), c), d), e), f), A::mul(T(6), u_c));
       T out;
-      if (sizeof(T) == sizeof(float) && seed) {
+      if (SR && sizeof(T) == sizeof(float) && seed) {
         // the same f32 terms, summed exactly in FP64, scaled, then one unbiased rounding
         double v = ((double)u_c + (double)A::mul(half_dv, lap)) + (double)A::mul(A::mul(dt, A::sub(kv, A::mul(T(2), pv))), u_c);
         if (scale) v *= __ldg(scale + min(max(l_c, 0), nDom - 1));

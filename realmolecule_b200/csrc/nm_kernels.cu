@@ -24,19 +24,19 @@ __global__ void __launch_bounds__(256) k_nm_init(T* U, int* label, const float4*
 // seed[0]: the step seed of the unbiased fp32 rounding (null: round to nearest); the next step's
 // seed, seed[0] + 1, goes to seed_next (read and written in different words, so every block reads
 // the same value)
-template <typename T, bool ACC>
+template <typename T, bool ACC, bool SR>
 __global__ void __launch_bounds__(256) k_nm_update(const T* U, T* Unew, const T* K, const T* P, const int* label, Geo g,
                                                    T half_dv, T dt, double h3, int nDom, double* norms, const double* scale,
                                                    const unsigned* seed, unsigned* seed_next) {
   __shared__ DomTable<1, 128> tab;
-  if (seed && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && threadIdx.y == 0)
+  if (SR && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && threadIdx.y == 0)
     *seed_next = *seed + 1u;
   if (ACC) {
     dom_table_init(tab);
     __syncthreads();
   }
-  nm_update_body<T, ACC>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, norms, tab, blockIdx.x, blockIdx.y,
-                         blockIdx.z, scale, seed);
+  nm_update_body<T, ACC, false, SR>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, norms, tab, blockIdx.x, blockIdx.y,
+                                    blockIdx.z, scale, seed);
   if (ACC) {
     __syncthreads();
     dom_table_flush(tab, norms);
@@ -145,12 +145,19 @@ cudaError_t nm_update(const T* U, T* Unew, const T* K, const T* P, const int* la
                       double h3, int nDom, double* norms, cudaStream_t st, const double* scale, const unsigned* seed,
                       unsigned* seed_next) {
   if (g.NN < 2) return cudaSuccess;
-  if (norms)
-    k_nm_update<T, true><<<nm_march_grid(g), nm_march_block(), 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, norms,
-                                                                   scale, seed, seed_next);
+  const dim3 grd = nm_march_grid(g), blk = nm_march_block();
+  if (norms && seed)
+    k_nm_update<T, true, true><<<grd, blk, 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, norms, scale, seed,
+                                                    seed_next);
+  else if (norms)
+    k_nm_update<T, true, false><<<grd, blk, 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, norms, scale, seed,
+                                                     seed_next);
+  else if (seed)
+    k_nm_update<T, false, true><<<grd, blk, 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, nullptr, scale,
+                                                     seed, seed_next);
   else
-    k_nm_update<T, false><<<nm_march_grid(g), nm_march_block(), 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom,
-                                                                    nullptr, scale, seed, seed_next);
+    k_nm_update<T, false, false><<<grd, blk, 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, nullptr, scale,
+                                                      seed, seed_next);
   return cudaGetLastError();
 }
 template <typename T>
