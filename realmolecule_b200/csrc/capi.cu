@@ -133,7 +133,7 @@ static void free_ctx(rq_ctx* c) {
     if (gx) cudaGraphExecDestroy(gx);
   void* ptrs[] = {c->U[0], c->U[1], c->P[0], c->P[1], c->K, c->W, c->bestU, c->rho, c->Pother, c->resid, c->lab[0], c->lab[1],
                   c->Ec[0], c->Ec[1], c->fc, c->atoms5, c->scratch_atoms5, c->sic, c->sic2, c->pdirect, c->lob, c->lob_part, c->lob_scal, c->lock, c->splits, c->bin_start, c->bin_idx, c->bin_far, c->bin_zmax, c->atoms_mj, c->atoms_nm, c->Zdom, c->Zdom64, c->dnorm,
-                  c->dpd, c->dF, c->dsum, c->unorm, c->scale, c->err, c->seeds, c->scale64, c->Kext, c->rseed, c->K64};
+                  c->dpd, c->dF, c->dsum, c->unorm, c->scale, c->err, c->seeds, c->scale64, c->Kext, c->rseed, c->K64, c->nbm};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& L : c->mg) {
@@ -632,6 +632,7 @@ static int upload_labels(rq_ctx* c, const int32_t* label) {
   }
   c->cl ^= 1;
   CK(cudaMemcpyAsync(c->lab[1 - c->cl], c->lab[c->cl], n * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+  if (c->cfg.flavor == RQ_FLAVOR_NEW) return nm_label_mask(c);
   return RQ_OK;
 }
 

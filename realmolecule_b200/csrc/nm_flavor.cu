@@ -31,6 +31,13 @@ double interior(const Geo& g) {
 size_t esize(const rq_ctx* c) { return c->fp64 ? sizeof(double) : sizeof(float); }
 }  // namespace
 
+// the same-label neighbour mask of the current labels (read by the update)
+int nm_label_mask(rq_ctx* c) {
+  if (!c->nbm) return RQ_OK;
+  LAUNCH(RQ_KC_LABELS, 25.0 * c->g.S3, nm_mask(c->lab[c->cl], c->nbm, c->g, c->st));
+  return RQ_OK;
+}
+
 int nm_alloc_levels(rq_ctx* c) {
   // levels: halve NN while it stays even and the next level keeps NN >= 6, or mg_levels if set
   int levels = 1, NN = c->g.NN;
@@ -67,7 +74,8 @@ int nm_alloc_levels(rq_ctx* c) {
   }
   if (cudaMalloc(&c->seeds, sizeof(float4) * c->n_atoms) != cudaSuccess ||
       cudaMalloc(&c->scale64, sizeof(double) * c->n_atoms) != cudaSuccess ||
-      cudaMalloc((void**)&c->rseed, sizeof(unsigned) * 2) != cudaSuccess)
+      cudaMalloc((void**)&c->rseed, sizeof(unsigned) * 2) != cudaSuccess ||
+      cudaMalloc((void**)&c->nbm, (size_t)c->g.S3) != cudaSuccess)
     return rq_cuda(c, cudaErrorMemoryAllocation, "seed table");
   cudaMemsetAsync(c->rseed, 0, sizeof(unsigned) * 2, c->st);
   if (!c->fp64 && cudaMalloc((void**)&c->K64, sizeof(double) * (size_t)c->g.S3) != cudaSuccess)
@@ -169,11 +177,12 @@ static int nm_step_t(rq_ctx* c, int s) {
   if (c->adj.cap > 0 && (rc = nm_adj_record_step(c, s % f.poisson_interval == 0, norm)) != RQ_OK) return rc;
   if (norm) CK(cudaMemsetAsync(c->dnorm, 0, sizeof(double) * c->n_atoms, c->st));
   const bool sr = !c->fp64 && f.fp32_rounding == 1;
-  LAUNCH(RQ_KC_UPDATE, (4.0 * sizeof(T) + 4.0) * interior(c->g),
+  // bytes: psi, K, P read, psi' written, the neighbour mask; the centre label where it is needed
+  LAUNCH(RQ_KC_UPDATE, (4.0 * sizeof(T) + 1.0 + ((norm || c->nm_pending) ? 4.0 : 0.0)) * interior(c->g),
          nm_update<T>((const T*)c->U[c->cu], (T*)c->U[1 - c->cu], (const T*)c->K, (const T*)c->P[c->cp], c->lab[c->cl],
                       c->g, (T)c->half_dv, (T)c->dt, c->h3, c->n_atoms, norm ? c->dnorm : nullptr, c->st,
                       c->nm_pending ? (const double*)c->scale64 : nullptr, sr ? c->rseed + c->cu : nullptr,
-                      sr ? c->rseed + (1 - c->cu) : nullptr));
+                      sr ? c->rseed + (1 - c->cu) : nullptr, c->nbm));
   c->cu ^= 1;
   c->nm_pending = false;  // the update consumed the pending scale
   if (norm) {  // the scale of this step is applied by the next update (or a flush)
@@ -189,6 +198,7 @@ static int nm_step_t(rq_ctx* c, int s) {
            nm_evolve<T>(c->lab[c->cl], c->lab[1 - c->cl], (const T*)c->U[c->cu], c->W, c->g, f.boundary_speed, f.curv_reg,
                         c->st));
     c->cl ^= 1;
+    if ((rc = nm_label_mask(c)) != RQ_OK) return rc;
     if (c->adj.cap > 0) nm_adj_record_label(c);
   }
   return RQ_OK;
@@ -276,6 +286,7 @@ static int nm_init_t(rq_ctx* c) {
   LAUNCH(RQ_KC_OTHER, (sizeof(T) + 4.0) * n,
          nm_init<T>((T*)c->U[0], c->lab[0], (const float4*)c->seeds, (int)seeds.size(), c->g, (float)c->h, c->st));
   CK(cudaMemcpyAsync(c->lab[1], c->lab[0], n * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+  if ((rc = nm_label_mask(c)) != RQ_OK) return rc;
   CK(cudaMemsetAsync(c->U[1], 0, n * sizeof(T), c->st));
   for (int b = 0; b < 2; ++b) CK(cudaMemsetAsync(c->P[b], 0, n * sizeof(T), c->st));
   LAUNCH(RQ_KC_OTHER, 4.0 * n, launch_fill(c->W, 1.0f, c->g.S3, c->st));

@@ -3,6 +3,8 @@
 // stationary-point gradient with respect to the nuclear centres.  The point-wise code lives
 // in nm_bodies.cuh (shared with the batched kernels); here each body gets its block
 // coordinates from blockIdx.  T = float (mixed path) or double (FP64 path).
+#include <type_traits>
+
 #include "nm_bodies.cuh"
 #include "rq_kernels.h"
 
@@ -24,10 +26,16 @@ __global__ void __launch_bounds__(256) k_nm_init(T* U, int* label, const float4*
 // seed[0]: the step seed of the unbiased fp32 rounding (null: round to nearest); the next step's
 // seed, seed[0] + 1, goes to seed_next (read and written in different words, so every block reads
 // the same value)
-template <typename T, bool ACC, bool SR>
+__global__ void __launch_bounds__(256) k_nm_mask(const int* __restrict__ label, unsigned char* __restrict__ mask, Geo g) {
+  nm_mask_body(label, mask, g, blockIdx.x);
+}
+
+// mask: the same-label neighbour mask of `label` (null: the six neighbour labels are read)
+template <typename T, bool ACC, bool SR, bool MASK>
 __global__ void __launch_bounds__(256) k_nm_update(const T* U, T* Unew, const T* K, const T* P, const int* label, Geo g,
                                                    T half_dv, T dt, double h3, int nDom, double* norms, const double* scale,
-                                                   const unsigned* seed, unsigned* seed_next) {
+                                                   const unsigned* seed, unsigned* seed_next,
+                                                   const unsigned char* __restrict__ mask) {
   __shared__ DomTable<1, 128> tab;
   if (SR && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 && threadIdx.y == 0)
     *seed_next = *seed + 1u;
@@ -35,8 +43,8 @@ __global__ void __launch_bounds__(256) k_nm_update(const T* U, T* Unew, const T*
     dom_table_init(tab);
     __syncthreads();
   }
-  nm_update_body<T, ACC, false, SR>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, norms, tab, blockIdx.x, blockIdx.y,
-                                    blockIdx.z, scale, seed);
+  nm_update_body<T, ACC, MASK, SR>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, norms, tab, blockIdx.x, blockIdx.y,
+                                   blockIdx.z, scale, seed, kNmTile, mask);
   if (ACC) {
     __syncthreads();
     dom_table_flush(tab, norms);
@@ -143,21 +151,26 @@ cudaError_t nm_init(T* U, int* label, const float4* seeds, int nSeed, const Geo&
 template <typename T>
 cudaError_t nm_update(const T* U, T* Unew, const T* K, const T* P, const int* label, const Geo& g, T half_dv, T dt,
                       double h3, int nDom, double* norms, cudaStream_t st, const double* scale, const unsigned* seed,
-                      unsigned* seed_next) {
+                      unsigned* seed_next, const unsigned char* mask) {
   if (g.NN < 2) return cudaSuccess;
   const dim3 grd = nm_march_grid(g), blk = nm_march_block();
-  if (norms && seed)
-    k_nm_update<T, true, true><<<grd, blk, 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, norms, scale, seed,
-                                                    seed_next);
-  else if (norms)
-    k_nm_update<T, true, false><<<grd, blk, 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, norms, scale, seed,
-                                                     seed_next);
-  else if (seed)
-    k_nm_update<T, false, true><<<grd, blk, 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, nullptr, scale,
-                                                     seed, seed_next);
-  else
-    k_nm_update<T, false, false><<<grd, blk, 0, st>>>(U, Unew, K, P, label, g, half_dv, dt, h3, nDom, nullptr, scale,
-                                                      seed, seed_next);
+  auto go = [&](auto acc, auto sr, auto msk) {
+    k_nm_update<T, decltype(acc)::value, decltype(sr)::value, decltype(msk)::value><<<grd, blk, 0, st>>>(
+        U, Unew, K, P, label, g, half_dv, dt, h3, nDom, norms, scale, seed, seed_next, mask);
+  };
+  using Y = std::true_type;
+  using N = std::false_type;
+  if (mask) {
+    if (norms) { if (seed) go(Y{}, Y{}, Y{}); else go(Y{}, N{}, Y{}); }
+    else       { if (seed) go(N{}, Y{}, Y{}); else go(N{}, N{}, Y{}); }
+  } else {
+    if (norms) { if (seed) go(Y{}, Y{}, N{}); else go(Y{}, N{}, N{}); }
+    else       { if (seed) go(N{}, Y{}, N{}); else go(N{}, N{}, N{}); }
+  }
+  return cudaGetLastError();
+}
+cudaError_t nm_mask(const int* label, unsigned char* mask, const Geo& g, cudaStream_t st) {
+  k_nm_mask<<<nblk(g.S3, 256 * kNmFlatChunk), 256, 0, st>>>(label, mask, g);
   return cudaGetLastError();
 }
 template <typename T>
@@ -263,7 +276,8 @@ cudaError_t nm_add(T* K, const T* v, long long n, cudaStream_t st) {
   template cudaError_t nm_potential<T>(T*, const double*, int, const Geo&, double, double, cudaStream_t, double*);  \
   template cudaError_t nm_init<T>(T*, int*, const float4*, int, const Geo&, float, cudaStream_t);                   \
   template cudaError_t nm_update<T>(const T*, T*, const T*, const T*, const int*, const Geo&, T, T, double, int,     \
-                                    double*, cudaStream_t, const double*, const unsigned*, unsigned*);               \
+                                    double*, cudaStream_t, const double*, const unsigned*, unsigned*,                \
+                                    const unsigned char*);                                                           \
   template cudaError_t nm_apply<T>(T*, const int*, const double*, int, const Geo&, cudaStream_t);                   \
   template cudaError_t nm_normalize<T>(T*, const int*, const double*, const double*, int, double*, int*, const Geo&, \
                                        cudaStream_t);                                                                \

@@ -123,6 +123,7 @@ struct rq_ctx {
   void* scale64 = nullptr;    // new flavour: per-domain scale (FP64 for both precisions)
   unsigned* rseed = nullptr;  // new flavour, fp32 fields: the step seed of the unbiased rounding (2 words by parity)
   double* K64 = nullptr;      // new flavour, fp32 fields: the FP64 nuclear (+ external) potential the readout uses
+  unsigned char* nbm = nullptr;  // new flavour: same-label neighbour mask of the current labels (read by the update)
   void* Kext = nullptr;       // new flavour: external potential added to K (T), or null
   bool nm_pending = false;    // new flavour: psi awaits scale64 (applied by the next update or a flush)
   int sp_jdone = 0;           // solver.py flavour: the next Poisson step's first sweep is done (in P[1-cp])

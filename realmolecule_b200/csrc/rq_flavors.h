@@ -61,6 +61,7 @@ void nm_adj_record_label(rq_ctx* c);          // a label pass followed the step
 int nm_adjoint(rq_ctx* c, double* F, double* dEdv);
 void nm_adj_free(rq_ctx* c);
 int nm_nuclear_terms(rq_ctx* c, double* E, double* F);
+int nm_label_mask(rq_ctx* c);  // the update's same-label neighbour mask, after a label change
 // nuclear sums (nm_farfield.cu): K (field type, and K64 when given) for the current nuclei, tiled
 // or direct by cfg.nuclear_sum; a force gather over psi (weight rho) or over gw = dE/dK, added
 // into c->dF; the tiles' buffers

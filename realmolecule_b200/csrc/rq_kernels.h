@@ -130,7 +130,10 @@ cudaError_t nm_init(T* U, int* label, const float4* seeds, int nSeed, const Geo&
 template <typename T>
 cudaError_t nm_update(const T* U, T* Unew, const T* K, const T* P, const int* label, const Geo& g, T half_dv, T dt,
                       double h3, int nDom, double* norms, cudaStream_t st, const double* scale = nullptr,
-                      const unsigned* seed = nullptr, unsigned* seed_next = nullptr);
+                      const unsigned* seed = nullptr, unsigned* seed_next = nullptr,
+                      const unsigned char* mask = nullptr);
+// the same-label neighbour mask of `label` (S^3 bytes; bit q: neighbour q has the point's label)
+cudaError_t nm_mask(const int* label, unsigned char* mask, const Geo& g, cudaStream_t st);
 template <typename T>
 cudaError_t nm_apply(T* U, const int* label, const double* scale, int nDom, const Geo& g, cudaStream_t st);
 template <typename T>
