@@ -49,19 +49,21 @@ struct Pt {
   int i, j, k;
   long long id;
 };
-__device__ __forceinline__ Pt interior_pt(const Geo& g, long long q) {
-  const int n = g.NN - 1;
-  Pt p;
-  p.k = 1 + (int)(q % n);
-  p.j = 1 + (int)((q / n) % n);
-  p.i = 1 + (int)(q / ((long long)n * n));
+// Interior point of a 3-D launch (grid3 / kBlk3): x runs along k, y along j, z is the plane i.  No
+// integer division per point, and a block's threads read contiguous rows.
+constexpr int kB3x = 64, kB3y = 4;
+__device__ __forceinline__ bool interior_pt3(const Geo& g, Pt& p) {
+  p.k = 1 + (int)(blockIdx.x * kB3x + threadIdx.x);
+  p.j = 1 + (int)(blockIdx.y * kB3y + threadIdx.y);
+  p.i = 1 + (int)blockIdx.z;
   p.id = (long long)p.i * g.S2 + (long long)p.j * g.S + p.k;
-  return p;
+  return p.k < g.NN && p.j < g.NN && p.i < g.NN;
 }
-__device__ __forceinline__ long long n_interior(const Geo& g) {
-  const long long n = g.NN - 1;
-  return n * n * n;
+inline dim3 grid3(const Geo& g) {
+  const unsigned n = (unsigned)(g.NN - 1);
+  return dim3((n + kB3x - 1) / kB3x, (n + kB3y - 1) / kB3y, n);
 }
+const dim3 kBlk3(kB3x, kB3y, 1);
 
 // dE/dpsi, dE/dP and dE/dK of the readout at psi (nm_energy: E = sum_d w_d Q_d - (h^3 / 2 pi) <P, A P>,
 // Q_d = T_d + V_eK,d + 2 h^3 sum_d P rho, w_d = Z_d / N_d).  wq: per domain (w, Q/N).  T = h/2 sum
@@ -73,9 +75,8 @@ __global__ void __launch_bounds__(256) k_adj_seed(const T* __restrict__ U, const
                                                   double h, int nDom, const double* __restrict__ wq,
                                                   T* __restrict__ lam, T* __restrict__ muP, double* __restrict__ gK,
                                                   const double* __restrict__ K64) {
-  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n_interior(g)) return;
-  const Pt p = interior_pt(g, q);
+  Pt p;
+  if (!interior_pt3(g, p)) return;
   const long long id = p.id, S = g.S, S2 = g.S2;
   const int L = label[id];
   if (L < 0 || L >= nDom) {
@@ -157,9 +158,8 @@ __global__ void __launch_bounds__(256) k_adj_update(const T* __restrict__ in, T*
                                                     const int* __restrict__ label, const T* __restrict__ psi, Geo g,
                                                     double half_dv, double dt, double* __restrict__ gK,
                                                     T* __restrict__ muP) {
-  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n_interior(g)) return;
-  const Pt p = interior_pt(g, q);
+  Pt p;
+  if (!interior_pt3(g, p)) return;
   const long long id = p.id, S = g.S, S2 = g.S2;
   const int L = label[id];
   const double lc = (double)in[id];
@@ -181,9 +181,8 @@ __global__ void __launch_bounds__(256) k_adj_update(const T* __restrict__ in, T*
 template <typename T>
 __global__ void __launch_bounds__(256) k_adj_rbgs(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ muf,
                                                   Geo g, double h2, int color) {
-  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n_interior(g)) return;
-  const Pt p = interior_pt(g, q);
+  Pt p;
+  if (!interior_pt3(g, p)) return;
   const long long id = p.id, S = g.S, S2 = g.S2;
   const double v = (double)in[id];
   if (((p.i + p.j + p.k) & 1) == color) {
@@ -200,9 +199,8 @@ __global__ void __launch_bounds__(256) k_adj_rbgs(const T* __restrict__ in, T* _
 template <typename T>
 __global__ void __launch_bounds__(256) k_adj_residual(const T* __restrict__ mur, T* __restrict__ muP,
                                                       T* __restrict__ muf, Geo g, double inv_h2) {
-  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n_interior(g)) return;
-  const Pt p = interior_pt(g, q);
+  Pt p;
+  if (!interior_pt3(g, p)) return;
   const long long id = p.id, S = g.S, S2 = g.S2;
   const double r = (double)mur[id];
   const double s = (double)mur[id + S2] + (double)mur[id - S2] + (double)mur[id + S] + (double)mur[id - S] +
@@ -214,9 +212,8 @@ __global__ void __launch_bounds__(256) k_adj_residual(const T* __restrict__ mur,
 // full weighting transposed: mur = (1/8) trilinear(mufc) at the fine interior points
 template <typename T>
 __global__ void __launch_bounds__(256) k_adj_restrict(const T* __restrict__ mufc, T* __restrict__ mur, Geo g, Geo gc) {
-  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n_interior(g)) return;
-  const Pt p = interior_pt(g, q);
+  Pt p;
+  if (!interior_pt3(g, p)) return;
   const int oi = p.i & 1, oj = p.j & 1, ok = p.k & 1;
   double v = 0.0;
   for (int a = 0; a <= oi; ++a)
@@ -229,9 +226,8 @@ __global__ void __launch_bounds__(256) k_adj_restrict(const T* __restrict__ mufc
 // trilinear prolongation transposed: muPc = (1/8) sum (8,4,2,1 weights) muP at the coarse interior points
 template <typename T>
 __global__ void __launch_bounds__(256) k_adj_prolong(const T* __restrict__ muP, T* __restrict__ muPc, Geo g, Geo gc) {
-  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n_interior(gc)) return;
-  const Pt p = interior_pt(gc, q);
+  Pt p;
+  if (!interior_pt3(gc, p)) return;
   double v = 0.0;
   for (int a = -1; a <= 1; ++a)
     for (int b = -1; b <= 1; ++b)
@@ -282,9 +278,9 @@ __global__ void __launch_bounds__(1024) k_adj_coarsest(const T* __restrict__ muP
 template <typename T>
 __global__ void __launch_bounds__(256) k_adj_rhs(T* __restrict__ lam, const T* __restrict__ psi, const T* __restrict__ muf,
                                                  Geo g) {
-  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n_interior(g)) return;
-  const long long id = interior_pt(g, q).id;
+  Pt p;
+  if (!interior_pt3(g, p)) return;
+  const long long id = p.id;
   lam[id] = (T)((double)lam[id] + 12.566370614359172 * (double)psi[id] * (double)muf[id]);
 }
 
@@ -473,7 +469,7 @@ int adj_vcycle(rq_ctx* c, int l, int* cur) {
     for (int s = 0; s < sweeps; ++s)
       for (int color = 1; color >= 0; --color) {
         LAUNCH(RQ_KC_MG, 3.5 * sizeof(T) * ni,
-               (k_adj_rbgs<T><<<nblk(ni), 256, 0, c->st>>>(mu[*cur], mu[1 - *cur], muf, L.g, h2, color),
+               (k_adj_rbgs<T><<<grid3(L.g), kBlk3, 0, c->st>>>(mu[*cur], mu[1 - *cur], muf, L.g, h2, color),
                 cudaGetLastError()));
         *cur ^= 1;
       }
@@ -485,14 +481,14 @@ int adj_vcycle(rq_ctx* c, int l, int* cur) {
   const long long nc = (long long)(C.g.NN - 1) * (C.g.NN - 1) * (C.g.NN - 1);
   int ccur = 0;
   LAUNCH(RQ_KC_MG, sizeof(T) * (ni + nc),
-         (k_adj_prolong<T><<<nblk(nc), 256, 0, c->st>>>(mu[*cur], (T*)A.lv[l + 1].mu[0], L.g, C.g), cudaGetLastError()));
+         (k_adj_prolong<T><<<grid3(C.g), kBlk3, 0, c->st>>>(mu[*cur], (T*)A.lv[l + 1].mu[0], L.g, C.g), cudaGetLastError()));
   CK(cudaMemsetAsync(A.lv[l + 1].muf, 0, sizeof(T) * C.g.S3, c->st));
   if ((rc = adj_vcycle<T>(c, l + 1, &ccur)) != RQ_OK) return rc;
   LAUNCH(RQ_KC_MG, sizeof(T) * (ni + nc),
-         (k_adj_restrict<T><<<nblk(ni), 256, 0, c->st>>>((const T*)A.lv[l + 1].muf, (T*)A.lv[l].mur, L.g, C.g),
+         (k_adj_restrict<T><<<grid3(L.g), kBlk3, 0, c->st>>>((const T*)A.lv[l + 1].muf, (T*)A.lv[l].mur, L.g, C.g),
           cudaGetLastError()));
   LAUNCH(RQ_KC_MG, 5.0 * sizeof(T) * ni,
-         (k_adj_residual<T><<<nblk(ni), 256, 0, c->st>>>((const T*)A.lv[l].mur, mu[*cur], muf, L.g, 1.0 / h2),
+         (k_adj_residual<T><<<grid3(L.g), kBlk3, 0, c->st>>>((const T*)A.lv[l].mur, mu[*cur], muf, L.g, 1.0 / h2),
           cudaGetLastError()));
   return smooth(c->cfg.mg_pre);
 }
@@ -529,7 +525,7 @@ int adjoint_t(rq_ctx* c, double* F, double* dEdv) {
   T* lam[2] = {(T*)A.lam[0], (T*)A.lam[1]};
   T* muP[2] = {(T*)A.muP[0], (T*)A.muP[1]};
   LAUNCH(RQ_KC_FORCES, (4.0 * sizeof(T) + 4.0 + 2.0 * sizeof(T) + 8.0) * ni,
-         (k_adj_seed<T><<<nblk(ni), 256, 0, c->st>>>(psi, K, (const T*)c->P[c->cp], lab, g, c->h, n, A.wq, lam[li],
+         (k_adj_seed<T><<<grid3(g), kBlk3, 0, c->st>>>(psi, K, (const T*)c->P[c->cp], lab, g, c->h, n, A.wq, lam[li],
                                                      muP[mi], A.gK, c->K64),
           cudaGetLastError()));
   for (int r = (int)A.rec.size() - 1; r >= 0; --r) {
@@ -541,7 +537,7 @@ int adjoint_t(rq_ctx* c, double* F, double* dEdv) {
       if ((rc = adj_norm<T>(c, psi_s, lam[li], A.scales + (size_t)R.psi_slot * n)) != RQ_OK) return rc;
     }
     LAUNCH(RQ_KC_FORCES, (6.0 * sizeof(T) + 4.0 + 16.0) * ni,
-           (k_adj_update<T><<<nblk(ni), 256, 0, c->st>>>(lam[li], lam[1 - li], K, P_s, lab, psi_prev, g, c->half_dv,
+           (k_adj_update<T><<<grid3(g), kBlk3, 0, c->st>>>(lam[li], lam[1 - li], K, P_s, lab, psi_prev, g, c->half_dv,
                                                          c->dt, A.gK, muP[mi]),
             cudaGetLastError()));
     li ^= 1;
@@ -549,7 +545,7 @@ int adjoint_t(rq_ctx* c, double* F, double* dEdv) {
       CK(cudaMemsetAsync(A.muf, 0, sizeof(T) * S3, c->st));
       if ((rc = adj_vcycle<T>(c, 0, &mi)) != RQ_OK) return rc;
       LAUNCH(RQ_KC_FORCES, 4.0 * sizeof(T) * ni,
-             (k_adj_rhs<T><<<nblk(ni), 256, 0, c->st>>>(lam[li], psi_prev, (const T*)A.muf, g), cudaGetLastError()));
+             (k_adj_rhs<T><<<grid3(g), kBlk3, 0, c->st>>>(lam[li], psi_prev, (const T*)A.muf, g), cudaGetLastError()));
     }
   }
   if (F) {
