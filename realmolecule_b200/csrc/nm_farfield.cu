@@ -99,21 +99,23 @@ __global__ void __launch_bounds__(256) k_ff_lists(const double* __restrict__ nuc
   if (threadIdx.x == 0) near_cnt[t] = cnt;
 }
 
-// Node values: V[t][qa][qb][qc] = sum over the far nuclei of Z / |node - R| in FP64.  Block of
-// 256 threads per tile; thread (qa, qb) owns the 16 nodes along z.  Far nuclei of each chunk of
-// 128 are compacted into shared memory first.
+// Node values: V[t][qa][qb][qc] = sum over the far nuclei of Z / |node - R| in FP64.  Two blocks
+// of 256 threads per tile (blockIdx.x = 2 t + half); thread (qa, qb) owns the 8 nodes qc of its
+// half along z (8 accumulators keep the block at ~3 per SM).  Far nuclei of each chunk of 128 are
+// compacted into shared memory first.
+constexpr int kFfNh = kFfN / 2;
 __global__ void __launch_bounds__(256) k_ff_nodes(const double* __restrict__ nuc, int nNuc, FfGeo f,
                                                   const double* __restrict__ tabs, double* __restrict__ Vn) {
   __shared__ double sf[128 * 4];
   __shared__ int wc[8];
-  const int t = blockIdx.x;
+  const int t = blockIdx.x >> 1, c0 = (blockIdx.x & 1) * kFfNh;
   const FfBox b = ff_box(f, t);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int qa = threadIdx.x >> 4, qb = threadIdx.x & 15;
   const double xa = b.c[0] + b.a[0] * tabs[qa], yb = b.c[1] + b.a[1] * tabs[qb];
-  double zc[kFfN], v[kFfN];
+  double zc[kFfNh], v[kFfNh];
 #pragma unroll
-  for (int q = 0; q < kFfN; ++q) { zc[q] = b.c[2] + b.a[2] * tabs[q]; v[q] = 0.0; }
+  for (int q = 0; q < kFfNh; ++q) { zc[q] = b.c[2] + b.a[2] * tabs[c0 + q]; v[q] = 0.0; }
   for (int base = 0; base < nNuc; base += 128) {
     const int m = base + threadIdx.x;
     const bool far = threadIdx.x < 128 && m < nNuc && !ff_near(b, nuc[m * 4], nuc[m * 4 + 1], nuc[m * 4 + 2]);
@@ -134,16 +136,16 @@ __global__ void __launch_bounds__(256) k_ff_nodes(const double* __restrict__ nuc
       const double dx = xa - sf[q * 4], dy = yb - sf[q * 4 + 1], Z = sf[q * 4 + 2], Zn = sf[q * 4 + 3];
       const double dxy2 = fma(dx, dx, dy * dy);
 #pragma unroll
-      for (int c = 0; c < kFfN; ++c) {
+      for (int c = 0; c < kFfNh; ++c) {
         const double dz = zc[c] - Z;
         v[c] = fma(Zn, rsqrt_refined(fma(dz, dz, dxy2)), v[c]);
       }
     }
     __syncthreads();
   }
-  double* out = Vn + (long long)t * kFfN3 + (qa * kFfN + qb) * kFfN;
+  double* out = Vn + (long long)t * kFfN3 + (qa * kFfN + qb) * kFfN + c0;
 #pragma unroll
-  for (int c = 0; c < kFfN; ++c) out[c] = v[c];
+  for (int c = 0; c < kFfNh; ++c) out[c] = v[c];
 }
 
 // Shared-memory Lagrange tables of one tile: Lx[p][q], Ly[p][q] (row per point) and Lz
@@ -583,7 +585,7 @@ int nm_nuclear_potential(rq_ctx* c, void* K, double* K64) {
   CK(cudaMemsetAsync(Kd, 0, sizeof(double) * g.S3, c->st));  // faces
   if (!c->fp64) CK(cudaMemsetAsync(K, 0, sizeof(float) * g.S3, c->st));
   LAUNCH(RQ_KC_OTHER, 8.0 * kFfN3 * F.nTiles,
-         (k_ff_nodes<<<F.nTiles, 256, 0, c->st>>>(F.nuc, F.nNuc, f, F.tabs, F.nodes), cudaGetLastError()));
+         (k_ff_nodes<<<2 * F.nTiles, 256, 0, c->st>>>(F.nuc, F.nNuc, f, F.tabs, F.nodes), cudaGetLastError()));
   LAUNCH(RQ_KC_OTHER, 8.0 * g.S3,
          (k_ff_interp<<<F.nTiles, 256, kFfInterpSmem, c->st>>>(f, F.tabs, F.nodes, Kd, g), cudaGetLastError()));
   const dim3 grid(F.nTiles, kFfT);
