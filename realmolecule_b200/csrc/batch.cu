@@ -42,7 +42,6 @@ struct BInst {
   int nSeed;
   const double* K64;  // fp32 instances of a mixed batch: the FP64 K of its promotion set, read by the readout
   double* cs;         // FP64 working copy of the coarsest level (P and f) for the persistent launch
-  unsigned char* nbm; // same-label neighbour mask of the current labels (rebuilt after every label change)
 };
 
 struct BItem {
@@ -69,9 +68,9 @@ __global__ void __launch_bounds__(256) kb_update(const BInst* __restrict__ ins, 
     __syncthreads();
   }
   const Geo g = I.g;
-  nm_update_body<T, ACC, true, SR>((const T*)I.U[cu], (T*)I.U[1 - cu], (const T*)I.K, (const T*)I.P[cp], I.lab[cl], g,
-                               half_dv, dt, I.h * I.h * I.h, I.nDom, nrm, tab, it.bx, it.by, it.bz,
-                               scale ? scale + I.dom0 : nullptr, seed, tile, I.nbm);
+  nm_update_body<T, ACC, false, SR>((const T*)I.U[cu], (T*)I.U[1 - cu], (const T*)I.K, (const T*)I.P[cp], I.lab[cl], g,
+                                    half_dv, dt, I.h * I.h * I.h, I.nDom, nrm, tab, it.bx, it.by, it.bz,
+                                    scale ? scale + I.dom0 : nullptr, seed, tile);
   if (ACC) {
     __syncthreads();
     dom_table_flush(tab, nrm);
@@ -186,13 +185,6 @@ __global__ void __launch_bounds__(256) kb_evolve(const BInst* __restrict__ ins, 
   nm_evolve_body<T>(I.lab[cl], I.lab[1 - cl], (const T*)I.U[cu], I.W, g, dt_w, curv, it.bx, it.by, it.bz, tile);
 }
 
-// the same-label neighbour mask of the current labels (flat16 items)
-__global__ void __launch_bounds__(256) kb_mask(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cl) {
-  const BItem it = items[blockIdx.x];
-  const BInst& I = ins[it.inst];
-  nm_mask_body(I.lab[cl], I.nbm, I.g, it.bx);
-}
-
 template <typename T>
 __global__ void __launch_bounds__(256) kb_potential(const BInst* __restrict__ ins, const BItem* __restrict__ items,
                                                     double sigma_scale) {
@@ -277,7 +269,7 @@ __global__ void __launch_bounds__(256) kb_resnorm(const BInst* __restrict__ ins,
 // ---------------------------------------------------------------------------------------
 enum BPhaseKind : int {
   kPhApply, kPhZeroNorms, kPhUpdate, kPhUpdateAcc, kPhScale, kPhRbgs, kPhCoarsest, kPhResidual, kPhRestrict,
-  kPhZero, kPhProlong, kPhEvolve, kPhMask
+  kPhZero, kPhProlong, kPhEvolve
 };
 
 struct BPhase {
@@ -343,15 +335,15 @@ __device__ __forceinline__ void kb_run_item(const BPersist& a, const BPhase& P, 
       if (P.kind == kPhUpdateAcc) {
         dom_table_init(tab);
         __syncthreads();
-        nm_update_body<T, true, true>((const T*)I.U[P.cu], (T*)I.U[1 - P.cu], (const T*)I.K, (const T*)I.P[P.cp],
-                                      I.lab[P.cl], g, (T)a.half_dv, (T)a.dt, I.h * I.h * I.h, I.nDom, a.dnorm + I.dom0,
-                                      tab, it.bx, it.by, it.bz, sc, P.seed, a.tile, I.nbm);
+        nm_update_body<T, true>((const T*)I.U[P.cu], (T*)I.U[1 - P.cu], (const T*)I.K, (const T*)I.P[P.cp], I.lab[P.cl],
+                                g, (T)a.half_dv, (T)a.dt, I.h * I.h * I.h, I.nDom, a.dnorm + I.dom0, tab, it.bx, it.by,
+                                it.bz, sc, P.seed, a.tile);
         __syncthreads();
         dom_table_flush(tab, a.dnorm + I.dom0);
       } else {
-        nm_update_body<T, false, true>((const T*)I.U[P.cu], (T*)I.U[1 - P.cu], (const T*)I.K, (const T*)I.P[P.cp],
-                                       I.lab[P.cl], g, (T)a.half_dv, (T)a.dt, I.h * I.h * I.h, I.nDom, nullptr, tab,
-                                       it.bx, it.by, it.bz, sc, P.seed, a.tile, I.nbm);
+        nm_update_body<T, false>((const T*)I.U[P.cu], (T*)I.U[1 - P.cu], (const T*)I.K, (const T*)I.P[P.cp],
+                                 I.lab[P.cl], g, (T)a.half_dv, (T)a.dt, I.h * I.h * I.h, I.nDom, nullptr, tab, it.bx,
+                                 it.by, it.bz, sc, P.seed, a.tile);
       }
       break;
     }
@@ -405,9 +397,6 @@ __device__ __forceinline__ void kb_run_item(const BPersist& a, const BPhase& P, 
                         it.bz, a.tile);
       break;
     }
-    case kPhMask:
-      nm_mask_body(I.lab[P.cl], I.nbm, I.g, it.bx);
-      break;
     default:
       break;
   }
@@ -676,7 +665,6 @@ static int build(rq_batch* b) {
     BInst& I = b->hin[q];
     BRC(alloc_fields(b, I, b->f64[q] ? sizeof(double) : sizeof(float)));
     for (int k = 0; k < 2; ++k) BALLOC(I.lab[k], (size_t)I.g.S3 * sizeof(int));
-    BALLOC(I.nbm, (size_t)I.g.S3);
     BALLOC(I.W, (size_t)I.g.S3 * sizeof(float));
     const int lc = I.nlev - 1;
     b->coarse_smem[lc] = std::max(b->coarse_smem[lc], sizeof(double) * 2 * (size_t)I.lg[lc].S3);
@@ -883,21 +871,6 @@ static int b_flush(rq_batch* b) {
 // updates ran since the last normalisation
 static int b_ready(rq_batch* b) { return b->age == 0 ? b_flush(b) : b_normalize(b); }
 
-// the same-label neighbour masks of the current labels, for every active instance
-static int b_mask(rq_batch* b) {
-  for (int p = 0; p < 2; ++p) {
-    const rq_batch::Plan& f = b->pl[p].flat16;
-    if (!f.n) continue;
-    if (b->rec) {
-      b_record(b, kPhMask, p, &f);
-      continue;
-    }
-    kb_mask<<<f.n, 256, 0, b->st>>>(b->din, f.d, b->cl);
-    BL("mask");
-  }
-  return RQ_OK;
-}
-
 static bool any_active(const rq_batch* b) { return b->pl[kF32].march[0].n + b->pl[kF64].march[0].n > 0; }
 
 static int b_step(rq_batch* b, int s) {
@@ -978,7 +951,6 @@ static int b_step(rq_batch* b, int s) {
       return RQ_OK;
     }));
     b->cl ^= 1;
-    BRC(b_mask(b));
   }
   return RQ_OK;
 }
@@ -1004,7 +976,6 @@ static int b_initialize(rq_batch* b) {
     BCK(launch_fill(I.W, 1.0f, I.g.S3, b->st));
   }
   BRC(b_normalize(b));
-  BRC(b_mask(b));
   for (int v = 0; v < 10; ++v) BRC(each_set([&](auto tag, int p) { return b_vcycle<decltype(tag)>(b, p); }));
   b->steps_done = 0;
   BCK(cudaStreamSynchronize(b->st));
@@ -1146,8 +1117,7 @@ static int b_phase_items(const rq_batch* b, const BPhase& x, int q) {
   if (!b->active[q] || (b->f64[q] ? kF64 : kF32) != x.set) return 0;
   const InstItems& it = b->items[q];
   switch (x.kind) {
-    case kPhApply:
-    case kPhMask: return (int)it.flat16.size();
+    case kPhApply: return (int)it.flat16.size();
     case kPhZeroNorms:
     case kPhScale: return 1;
     case kPhUpdate:
