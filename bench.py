@@ -422,8 +422,7 @@ def hbm_leg(stream, peak):
 
 def nm_step_bytes(NN, es=4, pi=4, pre=1, post=1):
     """Algorithmic bytes per new-flavour step on one grid (the byte counts of nm_flavor.cu's launches):
-    the update every step (psi, K, P and the 1-byte same-label neighbour mask read, psi written; the
-    centre label too in the update that accumulates the norms, one in pi); every pi steps the materialised
+    the update every step (psi, K, P, label read; psi written); every pi steps the materialised
     normalisation (psi, label read; psi written) and one V(pre, post) cycle (each red-black colour
     2.5 field values per point, the residual 3, full weighting and the coarse zeroing, the
     prolongation 2 fine + 1 coarse, the coarsest level 2 values per point)."""
@@ -438,7 +437,7 @@ def nm_step_bytes(NN, es=4, pi=4, pre=1, post=1):
         v += (pre + post) * 2 * 2.5 * es * n_in[l] + 3 * es * n_in[l] + es * (n_in[l] + n_in[l + 1])
         v += es * s3[l + 1] + es * (2 * n_in[l] + n_in[l + 1])
     v += 2 * es * s3[-1]
-    return (4 * es + 1) * n_in[0] + (4 * n_in[0] + (2 * es + 4) * s3[0] + v) / pi
+    return (4 * es + 4) * n_in[0] + ((2 * es + 4) * s3[0] + v) / pi
 
 
 def batch_leg(stream, peak):
