@@ -120,6 +120,20 @@ __global__ void __launch_bounds__(256) kb_residual(const BInst* __restrict__ ins
   nm_residual_rows_body<T, FINE>(P, f, (T*)I.lr[lev], g, (T)(1.0 / (I.lh[lev] * I.lh[lev])), it.bx, it.by, it.bz);
 }
 
+// residual, full weighting and the zeroed coarse correction of level lev in one pass
+template <typename T, bool FINE>
+__global__ void __launch_bounds__(256) kb_resrestrict(const BInst* __restrict__ ins, const BItem* __restrict__ items,
+                                                      int lev, int cu, int cp) {
+  __shared__ T patch[2][kNmRrPatch];
+  const BItem it = items[blockIdx.x];
+  const BInst& I = ins[it.inst];
+  const T* P = FINE ? (const T*)I.P[cp] : (const T*)I.lP[lev];
+  const T* f = FINE ? (const T*)I.U[cu] : (const T*)I.lf[lev];
+  const Geo g = I.lg[lev], gc = I.lg[lev + 1];
+  nm_resrestrict_body<T, FINE>(P, f, (T*)I.lf[lev + 1], (T*)I.lP[lev + 1], g, gc, (T)(1.0 / (I.lh[lev] * I.lh[lev])),
+                               it.bx, it.by, it.bz, patch);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) kb_restrict(const BInst* __restrict__ ins, const BItem* __restrict__ items,
                                                    int lev) {
@@ -480,7 +494,7 @@ constexpr int kF32 = 0, kF64 = 1;
 
 // Work items of one instance for every list; built once at creation, concatenated by build_plans.
 struct InstItems {
-  std::vector<BItem> march[kMaxLev], rbgs[kMaxLev], restr[kMaxLev], zero[kMaxLev], coarse[kMaxLev];
+  std::vector<BItem> march[kMaxLev], rbgs[kMaxLev], restr[kMaxLev], zero[kMaxLev], coarse[kMaxLev], rr[kMaxLev];
   std::vector<BItem> flat16, flat1, force, one;  // one: a single item (per-instance domain work)
 };
 
@@ -502,7 +516,7 @@ struct rq_batch {
   // work lists, one set per precision
   struct Plan { BItem* d = nullptr; int n = 0, cap = 0; };
   struct Plans {
-    Plan march[kMaxLev], rbgs[kMaxLev], restr[kMaxLev], zero[kMaxLev], coarse[kMaxLev];
+    Plan march[kMaxLev], rbgs[kMaxLev], restr[kMaxLev], zero[kMaxLev], coarse[kMaxLev], rr[kMaxLev];
     Plan flat16, flat1, force, one;
   };
   Plans pl[2];
@@ -593,6 +607,10 @@ static void make_items(const BInst& I, int q, InstItems& it, NmTile tile) {
     const long long nc = (long long)(I.lg[l + 1].NN - 1) * (I.lg[l + 1].NN - 1) * (I.lg[l + 1].NN - 1);
     flat_items(it.restr[l], q, nc, 256);
     flat_items(it.zero[l], q, I.lg[l + 1].S3, 256 * kNmFlatChunk);
+    const int cn = I.lg[l + 1].NN - 1;  // coarse interior of the fused residual + restriction
+    for (int zz = 0; zz < (cn + kNmRrPlanes - 1) / kNmRrPlanes; ++zz)
+      for (int y = 0; y < (cn + kNmRrTJ - 1) / kNmRrTJ; ++y)
+        for (int x = 0; x < (cn + kNmRrTK - 1) / kNmRrTK; ++x) it.rr[l].push_back({q, x, y, zz});
   }
   it.one.push_back({q, 0, 0, 0});
   flat_items(it.flat16, q, I.g.S3, 256 * kNmFlatChunk);
@@ -626,6 +644,7 @@ static int build_plans(rq_batch* b) {
       BRC(gather(P.rbgs[l], [l](const InstItems& it) -> const Items& { return it.rbgs[l]; }));
       BRC(gather(P.restr[l], [l](const InstItems& it) -> const Items& { return it.restr[l]; }));
       BRC(gather(P.zero[l], [l](const InstItems& it) -> const Items& { return it.zero[l]; }));
+      BRC(gather(P.rr[l], [l](const InstItems& it) -> const Items& { return it.rr[l]; }));
       BRC(gather(P.coarse[l], [l](const InstItems& it) -> const Items& { return it.coarse[l]; }));
     }
     BRC(gather(P.flat16, [](const InstItems& it) -> const Items& { return it.flat16; }));
@@ -805,15 +824,12 @@ static int b_vcycle(rq_batch* b, int p) {
       b_record(b, kPhZero, p, &P.zero[l], l + 1);
       continue;
     }
+    // the coarse correction's boundary stays zero from the allocation: only its interior is cleared
     if (l == 0)
-      kb_residual<T, true><<<P.rbgs[l].n, rb, 0, b->st>>>(b->din, P.rbgs[l].d, l, b->cu, b->cp);
+      kb_resrestrict<T, true><<<P.rr[l].n, rb, 0, b->st>>>(b->din, P.rr[l].d, l, b->cu, b->cp);
     else
-      kb_residual<T, false><<<P.rbgs[l].n, rb, 0, b->st>>>(b->din, P.rbgs[l].d, l, b->cu, b->cp);
-    BL("residual");
-    kb_restrict<T><<<P.restr[l].n, 256, 0, b->st>>>(b->din, P.restr[l].d, l);
-    BL("restrict");
-    kb_zero<T><<<P.zero[l].n, 256, 0, b->st>>>(b->din, P.zero[l].d, l + 1);
-    BL("zero");
+      kb_resrestrict<T, false><<<P.rr[l].n, rb, 0, b->st>>>(b->din, P.rr[l].d, l, b->cu, b->cp);
+    BL("resrestrict");
   }
   for (int l = b->maxlev - 2; l >= 0; --l) {
     if (!P.rbgs[l].n) continue;

@@ -357,22 +357,30 @@ __device__ __forceinline__ void nm_rbgs_body(T* __restrict__ P, const T* __restr
   }
 }
 
+// residual f - A P at one interior point from its P values (+i, -i, +j, -j, +k, -k, centre) and
+// its right-hand side
+template <typename T>
+__device__ __forceinline__ T nm_residual_value(T pip, T pim, T pjp, T pjm, T pkp, T pkm, T pc, T rhs, T inv_h2) {
+  using A = Ar<T>;
+  if (sizeof(T) == sizeof(float)) {
+    // fp32 fields: sum_6 P - 6 P cancels most of its digits (P is smooth), so the residual is
+    // formed in FP64 from the fp32 values (each operation rounded to nearest) and rounded once --
+    // this is what lets the fp32 multigrid reach the fp32 resolution of P instead of stalling at
+    // ~1e-4 relative
+    const double sd = __dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn((double)pip, (double)pim), (double)pjp),
+                                                    (double)pjm), (double)pkp), (double)pkm);
+    return (T)__dadd_rn((double)rhs, __dmul_rn(__dsub_rn(sd, __dmul_rn(6.0, (double)pc)), (double)inv_h2));
+  }
+  const T s = A::add(A::add(A::add(A::add(A::add(pip, pim), pjp), pjm), pkp), pkm);
+  return A::add(rhs, A::mul(A::sub(s, A::mul(T(6), pc)), inv_h2));
+}
+
 // residual r = f - A P at one interior point
 template <typename T, bool FINE>
 __device__ __forceinline__ void nm_residual_point(const T* __restrict__ P, const T* __restrict__ f, T* __restrict__ r,
                                                   long long id, long long S, long long S2, T inv_h2) {
-  using A = Ar<T>;
-  if (sizeof(T) == sizeof(float)) {
-    // fp32 fields: sum_6 P - 6 P cancels most of its digits (P is smooth), so the residual is
-    // formed in FP64 from the fp32 values and rounded once -- this is what lets the fp32
-    // multigrid reach the fp32 resolution of P instead of stalling at ~1e-4 relative
-    const double sd = (double)P[id + S2] + (double)P[id - S2] + (double)P[id + S] + (double)P[id - S] +
-                      (double)P[id + 1] + (double)P[id - 1];
-    r[id] = (T)((double)rhs_at<T, FINE>(f, id) + (sd - 6.0 * (double)P[id]) * (double)inv_h2);
-  } else {
-    const T s = A::add(A::add(A::add(A::add(A::add(P[id + S2], P[id - S2]), P[id + S]), P[id - S]), P[id + 1]), P[id - 1]);
-    r[id] = A::add(rhs_at<T, FINE>(f, id), A::mul(A::sub(s, A::mul(T(6), P[id])), inv_h2));
-  }
+  r[id] = nm_residual_value<T>(P[id + S2], P[id - S2], P[id + S], P[id - S], P[id + 1], P[id - 1], P[id],
+                               rhs_at<T, FINE>(f, id), inv_h2);
 }
 
 // Row tiling shared by the residual and the prolongation: block (32, 8) covers 64 points of k
@@ -457,6 +465,89 @@ __device__ __forceinline__ void nm_restrict_body(const T* __restrict__ fine, T* 
         v = A::add(v, A::mul(w, fine[(long long)(2 * I + a) * g.S2 + (long long)(2 * J + b) * g.S + (2 * K2 + c)]));
       }
   coarse[(long long)I * gc.S2 + (long long)J * gc.S + K2] = A::div(v, T(64));
+}
+
+// Residual and full weighting in one pass: fc = R (f - A P) on the coarse interior without storing
+// the fine residual, and the coarse correction Pc (when given) zeroed on the same points.  The
+// block (256 threads, read as 32 x 8) owns the coarse points (K, J) = (K0 + x, J0 + y) of a 32 x 8
+// tile on kNmRrPlanes coarse planes from I0, and walks the fine planes 2 I0 - 1 .. 2 Ilast + 1.
+// On each fine plane it forms the residual on the 65 x 17 fine patch under the tile into shared
+// memory (every thread keeps the P values of its patch points on the planes below and above in
+// registers); after one barrier each coarse point adds the 3 x 3 patch values around it, with
+// their weights, to its running sum.  A fine plane 2I + 1 closes the sum of coarse plane I and
+// opens that of I + 1.  The sums run in the (a, b, c) order of nm_restrict_body and the residual
+// is nm_residual_value, so the result is the one of the residual pass and the restriction.  The
+// patch is double-buffered: one barrier per fine plane.
+constexpr int kNmRrTK = 32, kNmRrTJ = 8, kNmRrPlanes = 8;
+constexpr int kNmRrPK = 2 * kNmRrTK + 1;                      // fine patch row (65 points)
+constexpr int kNmRrPatch = kNmRrPK * (2 * kNmRrTJ + 1);       // 65 x 17 fine points
+constexpr int kNmRrPer = (kNmRrPatch + 255) / 256;            // patch points per thread
+
+template <typename T, bool FINE>
+__device__ __forceinline__ void nm_resrestrict_body(const T* __restrict__ P, const T* __restrict__ f, T* __restrict__ fc,
+                                                    T* __restrict__ Pc, const Geo& g, const Geo& gc, T inv_h2, int bx,
+                                                    int by, int bz, T (*patch)[kNmRrPatch]) {
+  using A = Ar<T>;
+  const int n = gc.NN - 1;  // coarse interior 1..n
+  const int I0 = 1 + bz * kNmRrPlanes;
+  if (I0 > n) return;  // the whole block
+  const int Ilast = min(I0 + kNmRrPlanes - 1, n);
+  const int tx = tile_x<32>(), ty = tile_y<32>(), tid = tx + 32 * ty;
+  const int K0 = 1 + bx * kNmRrTK, J0 = 1 + by * kNmRrTJ;
+  const int K = K0 + tx, J = J0 + ty;
+  const bool own = K <= n && J <= n;
+  const long long S = g.S, S2 = g.S2;
+  const int fi0 = 2 * I0 - 1, fi1 = 2 * Ilast + 1;
+  int col[kNmRrPer];  // fine (j, k) offset of each patch point of this thread, -1 outside the grid
+  T pm[kNmRrPer], pc[kNmRrPer];
+#pragma unroll
+  for (int m = 0; m < kNmRrPer; ++m) {
+    const int p = tid + 256 * m;
+    const int fj = 2 * J0 - 1 + p / kNmRrPK, fk = 2 * K0 - 1 + p % kNmRrPK;
+    col[m] = (p < kNmRrPatch && fj < g.NN && fk < g.NN) ? fj * g.S + fk : -1;
+    pm[m] = pc[m] = T(0);
+    if (col[m] >= 0) {
+      pm[m] = P[(long long)(fi0 - 1) * S2 + col[m]];
+      pc[m] = P[(long long)fi0 * S2 + col[m]];
+    }
+  }
+  T v = T(0);
+  for (int i = fi0; i <= fi1; ++i) {
+    T* buf = patch[i & 1];
+    const long long base = (long long)i * S2;
+#pragma unroll
+    for (int m = 0; m < kNmRrPer; ++m) {
+      if (col[m] < 0) continue;
+      const long long id = base + col[m];
+      const T pp = P[id + S2];
+      buf[tid + 256 * m] =
+          nm_residual_value<T>(pp, pm[m], P[id + S], P[id - S], P[id + 1], P[id - 1], pc[m], rhs_at<T, FINE>(f, id), inv_h2);
+      pm[m] = pc[m];
+      pc[m] = pp;
+    }
+    __syncthreads();
+    if (!own) continue;
+    const T* q = buf + (2 * ty) * kNmRrPK + 2 * tx;  // patch point of fine (2J - 1, 2K - 1)
+    auto add_plane = [&](int wa) {
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          v = A::add(v, A::mul((T)(wa * (b == 1 ? 2 : 1) * (c == 1 ? 2 : 1)), q[b * kNmRrPK + c]));
+    };
+    if (i & 1) {
+      if (i > fi0) {  // a = +1 of coarse plane (i - 1) / 2, whose sum is then complete
+        add_plane(1);
+        const long long cid = (long long)((i - 1) >> 1) * gc.S2 + (long long)J * gc.S + K;
+        fc[cid] = A::div(v, T(64));
+        if (Pc) Pc[cid] = T(0);
+      }
+      v = T(0);
+      if (i < fi1) add_plane(1);  // a = -1 of coarse plane (i + 1) / 2
+    } else {
+      add_plane(2);  // a = 0
+    }
+  }
 }
 
 // coarsest level: `sweeps` red-black sweeps in FP64 by one block; sm: 2*S^3 doubles of smem

@@ -100,10 +100,11 @@ static int vcycle_level(rq_ctx* c, int l) {
   for (int s = 0; s < c->cfg.mg_pre; ++s)
     for (int color = 0; color < 2; ++color)
       LAUNCH(kc, sizeof(T) * 2.5 * ip, nm_rbgs<T>(P, f, fine, L.g, h2, color, c->st));
-  LAUNCH(kc, sizeof(T) * 3.0 * ip, nm_residual<T>(P, f, fine, (T*)L.r, L.g, 1.0 / h2, c->st));
+  // the residual, its full weighting and the cleared coarse correction in one pass (the coarse
+  // boundary stays zero from the allocation)
   rq_mg_level& C = c->mg[l + 1];
-  LAUNCH(RQ_KC_MG, sizeof(T) * (ip + interior(C.g)), nm_restrict<T>((const T*)L.r, (T*)C.f, L.g, C.g, c->st));
-  CK(cudaMemsetAsync(C.P, 0, sizeof(T) * C.g.S3, c->st));
+  LAUNCH(kc, sizeof(T) * (2.0 * ip + 2.0 * interior(C.g)),
+         nm_resrestrict<T>(P, f, fine, (T*)C.f, (T*)C.P, L.g, C.g, 1.0 / h2, c->st));
   int rc = vcycle_level<T>(c, l + 1);
   if (rc != RQ_OK) return rc;
   LAUNCH(RQ_KC_MG, sizeof(T) * (2.0 * ip + interior(C.g)), nm_prolong<T>((const T*)C.P, P, L.g, C.g, c->st));

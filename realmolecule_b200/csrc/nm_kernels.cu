@@ -82,13 +82,9 @@ __global__ void __launch_bounds__(256) k_nm_rbgs(T* P, const T* f, Geo g, T h2, 
 }
 
 template <typename T, bool FINE>
-__global__ void __launch_bounds__(256) k_nm_residual(const T* P, const T* f, T* r, Geo g, T inv_h2) {
-  nm_residual_rows_body<T, FINE>(P, f, r, g, inv_h2, blockIdx.x, blockIdx.y, blockIdx.z);
-}
-
-template <typename T>
-__global__ void __launch_bounds__(256) k_nm_restrict(const T* fine, T* coarse, Geo g, Geo gc) {
-  nm_restrict_body<T>(fine, coarse, g, gc, (long long)blockIdx.x * blockDim.x + threadIdx.x);
+__global__ void __launch_bounds__(256) k_nm_resrestrict(const T* P, const T* f, T* fc, T* Pc, Geo g, Geo gc, T inv_h2) {
+  __shared__ T patch[2][kNmRrPatch];
+  nm_resrestrict_body<T, FINE>(P, f, fc, Pc, g, gc, inv_h2, blockIdx.x, blockIdx.y, blockIdx.z, patch);
 }
 
 template <typename T>
@@ -207,19 +203,15 @@ cudaError_t nm_rbgs(T* P, const T* f, bool fine, const Geo& g, double h2, int co
   return cudaGetLastError();
 }
 template <typename T>
-cudaError_t nm_residual(const T* P, const T* f, bool fine, T* r, const Geo& g, double inv_h2, cudaStream_t st) {
-  const int n = g.NN - 1;
-  const dim3 blk(32, 8), grd((n + 63) / 64, (n + 7) / 8, (n + kNmRowPlanes - 1) / kNmRowPlanes);
+cudaError_t nm_resrestrict(const T* P, const T* f, bool fine, T* fc, T* Pc, const Geo& g, const Geo& gc, double inv_h2,
+                           cudaStream_t st) {
+  const int n = gc.NN - 1;
+  if (n < 1) return cudaSuccess;
+  const dim3 blk(32, 8), grd((n + kNmRrTK - 1) / kNmRrTK, (n + kNmRrTJ - 1) / kNmRrTJ, (n + kNmRrPlanes - 1) / kNmRrPlanes);
   if (fine)
-    k_nm_residual<T, true><<<grd, blk, 0, st>>>(P, f, r, g, (T)inv_h2);
+    k_nm_resrestrict<T, true><<<grd, blk, 0, st>>>(P, f, fc, Pc, g, gc, (T)inv_h2);
   else
-    k_nm_residual<T, false><<<grd, blk, 0, st>>>(P, f, r, g, (T)inv_h2);
-  return cudaGetLastError();
-}
-template <typename T>
-cudaError_t nm_restrict(const T* fine, T* coarse, const Geo& g, const Geo& gc, cudaStream_t st) {
-  const long long n = gc.NN - 1;
-  k_nm_restrict<T><<<nblk(n * n * n), 256, 0, st>>>(fine, coarse, g, gc);
+    k_nm_resrestrict<T, false><<<grd, blk, 0, st>>>(P, f, fc, Pc, g, gc, (T)inv_h2);
   return cudaGetLastError();
 }
 template <typename T>
@@ -284,8 +276,8 @@ cudaError_t nm_add(T* K, const T* v, long long n, cudaStream_t st) {
   template cudaError_t nm_norm_scale<T>(const double*, const double*, int, double*, int*, cudaStream_t);            \
   template cudaError_t nm_norms<T>(const T*, const int*, const Geo&, double, int, double*, cudaStream_t);           \
   template cudaError_t nm_rbgs<T>(T*, const T*, bool, const Geo&, double, int, cudaStream_t);                       \
-  template cudaError_t nm_residual<T>(const T*, const T*, bool, T*, const Geo&, double, cudaStream_t);              \
-  template cudaError_t nm_restrict<T>(const T*, T*, const Geo&, const Geo&, cudaStream_t);                          \
+  template cudaError_t nm_resrestrict<T>(const T*, const T*, bool, T*, T*, const Geo&, const Geo&, double,          \
+                                         cudaStream_t);                                                            \
   template cudaError_t nm_prolong<T>(const T*, T*, const Geo&, const Geo&, cudaStream_t);                           \
   template cudaError_t nm_coarsest<T>(T*, const T*, const Geo&, double, int, cudaStream_t);                         \
   template cudaError_t nm_energy<T>(const T*, const T*, const T*, const int*, const Geo&, double, int, double*,     \
