@@ -138,6 +138,21 @@ struct RunSum {
     const unsigned peers = __match_any_sync(0xffffffffu, label);
     const int lane = lane_id();
     double s[NQ];
+    if (__all_sync(0xffffffffu, peers == 0xffffffffu)) {
+      // one label over the warp (the common case): a butterfly
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        double x = v[q];
+        x += __shfl_xor_sync(0xffffffffu, x, 16);
+        x += __shfl_xor_sync(0xffffffffu, x, 8);
+        x += __shfl_xor_sync(0xffffffffu, x, 4);
+        x += __shfl_xor_sync(0xffffffffu, x, 2);
+        x += __shfl_xor_sync(0xffffffffu, x, 1);
+        s[q] = x;
+      }
+      if (label >= 0 && lane == 0) dom_table_add(t, label, s, global);
+      return;
+    }
 #pragma unroll
     for (int q = 0; q < NQ; ++q) s[q] = 0.0;
     for (int l = 0; l < 32; ++l) {
