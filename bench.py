@@ -424,7 +424,7 @@ def nm_step_bytes(NN, es=4, pi=4, pre=1, post=1):
     """Algorithmic bytes per new-flavour step on one grid (the byte counts of nm_flavor.cu's launches):
     the update every step (psi, K, P, label read; psi written); every pi steps the materialised
     normalisation (psi, label read; psi written) and one V(pre, post) cycle (each red-black colour
-    2.5 field values per point, a whole fine-level sweep in one pass 3, the fused residual + full weighting 2 fine + 2 coarse (the coarse
+    2.5 field values per point, the fused residual + full weighting 2 fine + 2 coarse (the coarse
     right-hand side and the cleared correction), the prolongation 2 fine + 1 coarse, the coarsest
     level 2 values per point)."""
     levels, nn = [NN], NN
@@ -435,9 +435,7 @@ def nm_step_bytes(NN, es=4, pi=4, pre=1, post=1):
     s3 = [(x + 1) ** 3 for x in levels]
     v = 0.0
     for l in range(len(levels) - 1):
-        # the fine level sweeps out of place in one pass (3 values) when pre + post is even
-        per_sweep = 3 if (l == 0 and (pre + post) % 2 == 0) else 2 * 2.5
-        v += (pre + post) * per_sweep * es * n_in[l] + 2 * es * (n_in[l] + n_in[l + 1])
+        v += (pre + post) * 2 * 2.5 * es * n_in[l] + 2 * es * (n_in[l] + n_in[l + 1])
         v += es * (2 * n_in[l] + n_in[l + 1])
     v += 2 * es * s3[-1]
     return (4 * es + 4) * n_in[0] + ((2 * es + 4) * s3[0] + v) / pi

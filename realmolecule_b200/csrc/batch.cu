@@ -120,18 +120,6 @@ __global__ void __launch_bounds__(256) kb_residual(const BInst* __restrict__ ins
   nm_residual_rows_body<T, FINE>(P, f, (T*)I.lr[lev], g, (T)(1.0 / (I.lh[lev] * I.lh[lev])), it.bx, it.by, it.bz);
 }
 
-// one whole red-black sweep of the fine level, out of place: P[src] -> P[1 - src]
-template <typename T>
-__global__ void __launch_bounds__(256) kb_sweep(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cu,
-                                                int src) {
-  __shared__ T buf[4][kNmSwRJ][kNmSwRK];
-  const BItem it = items[blockIdx.x];
-  const BInst& I = ins[it.inst];
-  const Geo g = I.g;
-  nm_sweep_body<T, true>((const T*)I.P[src], (T*)I.P[1 - src], (const T*)I.U[cu], g, (T)(I.lh[0] * I.lh[0]), it.bx,
-                         it.by, it.bz, buf);
-}
-
 // residual, full weighting and the zeroed coarse correction of level lev in one pass
 template <typename T, bool FINE>
 __global__ void __launch_bounds__(256) kb_resrestrict(const BInst* __restrict__ ins, const BItem* __restrict__ items,
@@ -507,7 +495,7 @@ constexpr int kF32 = 0, kF64 = 1;
 // Work items of one instance for every list; built once at creation, concatenated by build_plans.
 struct InstItems {
   std::vector<BItem> march[kMaxLev], rbgs[kMaxLev], restr[kMaxLev], zero[kMaxLev], coarse[kMaxLev], rr[kMaxLev];
-  std::vector<BItem> flat16, flat1, force, one, sw;  // one: a single item (per-instance domain work); sw: fused fine sweeps
+  std::vector<BItem> flat16, flat1, force, one;  // one: a single item (per-instance domain work)
 };
 
 struct rq_batch {
@@ -529,7 +517,7 @@ struct rq_batch {
   struct Plan { BItem* d = nullptr; int n = 0, cap = 0; };
   struct Plans {
     Plan march[kMaxLev], rbgs[kMaxLev], restr[kMaxLev], zero[kMaxLev], coarse[kMaxLev], rr[kMaxLev];
-    Plan flat16, flat1, force, one, sw;
+    Plan flat16, flat1, force, one;
   };
   Plans pl[2];
   size_t coarse_smem[kMaxLev] = {};
@@ -625,10 +613,6 @@ static void make_items(const BInst& I, int q, InstItems& it, NmTile tile) {
         for (int x = 0; x < (cn + kNmRrTK - 1) / kNmRrTK; ++x) it.rr[l].push_back({q, x, y, zz});
   }
   it.one.push_back({q, 0, 0, 0});
-  const int n0 = I.g.NN - 1;
-  for (int zz = 0; zz < (n0 + kNmSwPlanes - 1) / kNmSwPlanes; ++zz)
-    for (int y = 0; y < (n0 + kNmSwTJ - 1) / kNmSwTJ; ++y)
-      for (int x = 0; x < (n0 + kNmSwTK - 1) / kNmSwTK; ++x) it.sw.push_back({q, x, y, zz});
   flat_items(it.flat16, q, I.g.S3, 256 * kNmFlatChunk);
   flat_items(it.flat1, q, I.g.S3, 256);
   const long long n1 = I.g.NN - 1, ntiles = (n1 * n1 * n1 + kNmForceTile - 1) / kNmForceTile;
@@ -665,7 +649,6 @@ static int build_plans(rq_batch* b) {
     }
     BRC(gather(P.flat16, [](const InstItems& it) -> const Items& { return it.flat16; }));
     BRC(gather(P.one, [](const InstItems& it) -> const Items& { return it.one; }));
-    BRC(gather(P.sw, [](const InstItems& it) -> const Items& { return it.sw; }));
     BRC(gather(P.flat1, [](const InstItems& it) -> const Items& { return it.flat1; }));
     BRC(gather(P.force, [](const InstItems& it) -> const Items& { return it.force; }));
   }
@@ -809,17 +792,7 @@ static int b_vcycle(rq_batch* b, int p) {
   const rq_batch::Plans& P = b->pl[p];
   const int pre = b->cfg.mg_pre, post = b->cfg.mg_post;
   const dim3 rb(32, 8);
-  // With an even number of sweeps per cycle the fine level sweeps out of place in one pass each
-  // (kb_sweep), alternating the two P buffers and ending in P[cp]; cur is the current one.
-  const bool fuse = !b->rec && (pre + post) % 2 == 0;
-  int cur = b->cp;
   auto smooth = [&](int l) -> int {
-    if (l == 0 && fuse) {
-      kb_sweep<T><<<P.sw.n, rb, 0, b->st>>>(b->din, P.sw.d, b->cu, cur);
-      BL("sweep");
-      cur ^= 1;
-      return RQ_OK;
-    }
     for (int color = 0; color < 2; ++color) {
       if (b->rec) {
         b_record(b, kPhRbgs, p, &P.rbgs[l], l, color);
@@ -853,7 +826,7 @@ static int b_vcycle(rq_batch* b, int p) {
     }
     // the coarse correction's boundary stays zero from the allocation: only its interior is cleared
     if (l == 0)
-      kb_resrestrict<T, true><<<P.rr[l].n, rb, 0, b->st>>>(b->din, P.rr[l].d, l, b->cu, cur);
+      kb_resrestrict<T, true><<<P.rr[l].n, rb, 0, b->st>>>(b->din, P.rr[l].d, l, b->cu, b->cp);
     else
       kb_resrestrict<T, false><<<P.rr[l].n, rb, 0, b->st>>>(b->din, P.rr[l].d, l, b->cu, b->cp);
     BL("resrestrict");
@@ -863,7 +836,7 @@ static int b_vcycle(rq_batch* b, int p) {
     if (b->rec) {
       b_record(b, kPhProlong, p, &P.rbgs[l], l);
     } else {
-      kb_prolong<T><<<P.rbgs[l].n, rb, 0, b->st>>>(b->din, P.rbgs[l].d, l, cur);
+      kb_prolong<T><<<P.rbgs[l].n, rb, 0, b->st>>>(b->din, P.rbgs[l].d, l, b->cp);
       BL("prolong");
     }
     for (int s = 0; s < post; ++s) BRC(smooth(l));
@@ -1641,8 +1614,7 @@ extern "C" int rq_batch_autotune(rq_batch* b, rq_tune_report* out) {
     b_retile(b, keep);
     b->cfg.batch_persistent = keep_persistent;
   }
-  // 2. smoother sweeps: 3 V-cycles from P = 0 on the current psi, P restored after each from a copy in
-  // the fine residual buffer (which the per-kernel cycle does not use; fused sweeps use both P buffers)
+  // 2. smoother sweeps: 3 V-cycles from P = 0 on the current psi, P restored after each
   if (rc == RQ_OK && !b->dtune) rc = balloc(b, (void**)&b->dtune, sizeof(double));
   if (rc == RQ_OK) rc = b_flush(b);
   const int cand[7][3] = {{1, 1, 16}, {2, 1, 16}, {1, 2, 16}, {2, 2, 16}, {1, 1, 8}, {1, 1, 32}, {2, 2, 32}};
@@ -1657,7 +1629,7 @@ extern "C" int rq_batch_autotune(rq_batch* b, rq_tune_report* out) {
       if (!b->active[q]) continue;
       const BInst& I = b->hin[q];
       const size_t bytes = (b->f64[q] ? sizeof(double) : sizeof(float)) * (size_t)I.g.S3;
-      if (cudaMemcpyAsync(I.lr[0], I.P[b->cp], bytes, cudaMemcpyDeviceToDevice, b->st) != cudaSuccess ||
+      if (cudaMemcpyAsync(I.P[1 - b->cp], I.P[b->cp], bytes, cudaMemcpyDeviceToDevice, b->st) != cudaSuccess ||
           cudaMemsetAsync(I.P[b->cp], 0, bytes, b->st) != cudaSuccess)
         rc = RQ_ECUDA;
     }
@@ -1674,7 +1646,7 @@ extern "C" int rq_batch_autotune(rq_batch* b, rq_tune_report* out) {
       if (!b->active[q]) continue;
       const BInst& I = b->hin[q];
       const size_t bytes = (b->f64[q] ? sizeof(double) : sizeof(float)) * (size_t)I.g.S3;
-      if (cudaMemcpyAsync(I.P[b->cp], I.lr[0], bytes, cudaMemcpyDeviceToDevice, b->st) != cudaSuccess) rc = RQ_ECUDA;
+      if (cudaMemcpyAsync(I.P[b->cp], I.P[1 - b->cp], bytes, cudaMemcpyDeviceToDevice, b->st) != cudaSuccess) rc = RQ_ECUDA;
     }
     if (rc != RQ_OK) break;
     const double rho = r0 > 0 ? std::pow(std::sqrt(r3 / r0), 1.0 / 3.0) : 1.0;

@@ -357,67 +357,6 @@ __device__ __forceinline__ void nm_rbgs_body(T* __restrict__ P, const T* __restr
   }
 }
 
-// One whole red-black sweep (colour 0, the points with i + j + k even, then colour 1) in one pass,
-// out of place: Pn gets what the two in-place colour passes of nm_rbgs_body leave in P, bit for
-// bit.  Colour 0 reads only old colour-1 values, colour 1 only new colour-0 values, so the block
-// marches its planes with colour 1 one plane behind colour 0: at plane i it forms colour 0 on
-// its 64 x 8 tile and a one-point ring around it (the ring redundantly, from the old values) into
-// shared memory, then colour 1 of plane i - 1 from the three planes of colour-0 values there.  The
-// block's chunk of kNmSwPlanes planes also forms colour 0 on the plane below and above the chunk
-// (not stored).  A ring of four plane buffers needs one barrier per plane.  Positions on the
-// boundary hold the boundary value; positions outside the grid are never read.
-constexpr int kNmSwTK = 64, kNmSwTJ = 8, kNmSwPlanes = 16;
-constexpr int kNmSwRK = kNmSwTK + 2, kNmSwRJ = kNmSwTJ + 2;  // tile + ring
-constexpr int kNmSwRow0 = kNmSwRK / 2;                        // colour-0 points per ring row
-constexpr int kNmSwRed = kNmSwRow0 * kNmSwRJ;                 // colour-0 points of the ring region
-
-template <typename T, bool FINE>
-__device__ __forceinline__ void nm_sweep_body(const T* __restrict__ P, T* __restrict__ Pn, const T* __restrict__ f,
-                                              const Geo& g, T h2, int bx, int by, int bz,
-                                              T (*buf)[kNmSwRJ][kNmSwRK]) {
-  using A = Ar<T>;
-  const int NN = g.NN;
-  const int i0 = 1 + bz * kNmSwPlanes;
-  if (i0 > NN - 1) return;  // the whole block
-  const int il = min(i0 + kNmSwPlanes - 1, NN - 1);
-  const int k0 = 1 + bx * kNmSwTK, j0 = 1 + by * kNmSwTJ;
-  const int tx = tile_x<32>(), ty = tile_y<32>(), tid = tx + 32 * ty;
-  const long long S = g.S, S2 = g.S2;
-  for (int i = i0 - 1; i <= il + 1; ++i) {
-    T(*b0)[kNmSwRK] = buf[i & 3];
-    // colour 0 of plane i on the tile and its ring
-    for (int p = tid; p < kNmSwRed; p += 256) {
-      const int r = p / kNmSwRow0, q = p % kNmSwRow0;
-      const int j = j0 - 1 + r;
-      const int k = k0 - 1 + 2 * q + ((i + j + k0 - 1) & 1);
-      if (j > NN || k > NN) continue;  // outside the grid: never read
-      const long long id = (long long)i * S2 + (long long)j * S + k;
-      T v;
-      if (i >= 1 && i < NN && j >= 1 && j < NN && k >= 1 && k < NN) {
-        const T s = A::add(A::add(A::add(A::add(A::add(P[id + S2], P[id - S2]), P[id + S]), P[id - S]), P[id + 1]), P[id - 1]);
-        v = A::div(A::add(s, A::mul(h2, rhs_at<T, FINE>(f, id))), T(6));
-        if (i >= i0 && i <= il && r >= 1 && r <= kNmSwTJ && k >= k0 && k < k0 + kNmSwTK) Pn[id] = v;
-      } else {
-        v = P[id];  // boundary value
-      }
-      b0[r][k - (k0 - 1)] = v;
-    }
-    __syncthreads();
-    // colour 1 of plane i - 1 on the tile: one point per thread
-    const int ib = i - 1;
-    if (ib < i0) continue;
-    const int j = j0 + ty;
-    const int k = k0 + 2 * tx + ((ib + j + k0 + 1) & 1);
-    if (j >= NN || k >= NN) continue;
-    const int r = ty + 1, kk = k - (k0 - 1);
-    const T(*bm)[kNmSwRK] = buf[(i - 1) & 3];
-    const T s = A::add(A::add(A::add(A::add(A::add(b0[r][kk], buf[(i - 2) & 3][r][kk]), bm[r + 1][kk]), bm[r - 1][kk]),
-                              bm[r][kk + 1]), bm[r][kk - 1]);
-    const long long id = (long long)ib * S2 + (long long)j * S + k;
-    Pn[id] = A::div(A::add(s, A::mul(h2, rhs_at<T, FINE>(f, id))), T(6));
-  }
-}
-
 // residual f - A P at one interior point from its P values (+i, -i, +j, -j, +k, -k, centre) and
 // its right-hand side
 template <typename T>

@@ -11,7 +11,6 @@
 // Precision RQ_PREC_MIXED keeps fields in fp32, RQ_PREC_FP64 keeps everything in double.
 #include <cmath>
 #include <cstring>
-#include <utility>
 
 #include "rq_flavors.h"
 #include "rq_kernels.h"
@@ -98,19 +97,9 @@ static int vcycle_level(rq_ctx* c, int l) {
     return RQ_OK;
   }
   const int kc = fine ? RQ_KC_POISSON : RQ_KC_MG;
-  // With an even number of sweeps per cycle the fine level sweeps out of place in one pass each
-  // (nm_sweep), alternating the two P buffers and ending in P[cp]
-  const bool fuse = fine && (c->cfg.mg_pre + c->cfg.mg_post) % 2 == 0;
-  T* Po = fine ? (T*)c->P[1 - c->cp] : nullptr;
-  for (int s = 0; s < c->cfg.mg_pre; ++s) {
-    if (fuse) {
-      LAUNCH(kc, sizeof(T) * 3.0 * ip, nm_sweep<T>(P, Po, f, L.g, h2, c->st));
-      std::swap(P, Po);
-      continue;
-    }
+  for (int s = 0; s < c->cfg.mg_pre; ++s)
     for (int color = 0; color < 2; ++color)
       LAUNCH(kc, sizeof(T) * 2.5 * ip, nm_rbgs<T>(P, f, fine, L.g, h2, color, c->st));
-  }
   // the residual, its full weighting and the cleared coarse correction in one pass (the coarse
   // boundary stays zero from the allocation)
   rq_mg_level& C = c->mg[l + 1];
@@ -119,15 +108,9 @@ static int vcycle_level(rq_ctx* c, int l) {
   int rc = vcycle_level<T>(c, l + 1);
   if (rc != RQ_OK) return rc;
   LAUNCH(RQ_KC_MG, sizeof(T) * (2.0 * ip + interior(C.g)), nm_prolong<T>((const T*)C.P, P, L.g, C.g, c->st));
-  for (int s = 0; s < c->cfg.mg_post; ++s) {
-    if (fuse) {
-      LAUNCH(kc, sizeof(T) * 3.0 * ip, nm_sweep<T>(P, Po, f, L.g, h2, c->st));
-      std::swap(P, Po);
-      continue;
-    }
+  for (int s = 0; s < c->cfg.mg_post; ++s)
     for (int color = 0; color < 2; ++color)
       LAUNCH(kc, sizeof(T) * 2.5 * ip, nm_rbgs<T>(P, f, fine, L.g, h2, color, c->st));
-  }
   return RQ_OK;
 }
 

@@ -81,12 +81,6 @@ __global__ void __launch_bounds__(256) k_nm_rbgs(T* P, const T* f, Geo g, T h2, 
   nm_rbgs_body<T, FINE>(P, f, g, h2, color, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256) k_nm_sweep(const T* P, T* Pn, const T* f, Geo g, T h2) {
-  __shared__ T buf[4][kNmSwRJ][kNmSwRK];
-  nm_sweep_body<T, true>(P, Pn, f, g, h2, blockIdx.x, blockIdx.y, blockIdx.z, buf);
-}
-
 template <typename T, bool FINE>
 __global__ void __launch_bounds__(256) k_nm_resrestrict(const T* P, const T* f, T* fc, T* Pc, Geo g, Geo gc, T inv_h2) {
   __shared__ T patch[2][kNmRrPatch];
@@ -209,14 +203,6 @@ cudaError_t nm_rbgs(T* P, const T* f, bool fine, const Geo& g, double h2, int co
   return cudaGetLastError();
 }
 template <typename T>
-cudaError_t nm_sweep(const T* P, T* Pn, const T* f, const Geo& g, double h2, cudaStream_t st) {
-  const int n = g.NN - 1;
-  if (n < 1) return cudaSuccess;
-  const dim3 blk(32, 8), grd((n + kNmSwTK - 1) / kNmSwTK, (n + kNmSwTJ - 1) / kNmSwTJ, (n + kNmSwPlanes - 1) / kNmSwPlanes);
-  k_nm_sweep<T><<<grd, blk, 0, st>>>(P, Pn, f, g, (T)h2);
-  return cudaGetLastError();
-}
-template <typename T>
 cudaError_t nm_resrestrict(const T* P, const T* f, bool fine, T* fc, T* Pc, const Geo& g, const Geo& gc, double inv_h2,
                            cudaStream_t st) {
   const int n = gc.NN - 1;
@@ -290,7 +276,6 @@ cudaError_t nm_add(T* K, const T* v, long long n, cudaStream_t st) {
   template cudaError_t nm_norm_scale<T>(const double*, const double*, int, double*, int*, cudaStream_t);            \
   template cudaError_t nm_norms<T>(const T*, const int*, const Geo&, double, int, double*, cudaStream_t);           \
   template cudaError_t nm_rbgs<T>(T*, const T*, bool, const Geo&, double, int, cudaStream_t);                       \
-  template cudaError_t nm_sweep<T>(const T*, T*, const T*, const Geo&, double, cudaStream_t);                      \
   template cudaError_t nm_resrestrict<T>(const T*, const T*, bool, T*, T*, const Geo&, const Geo&, double,          \
                                          cudaStream_t);                                                            \
   template cudaError_t nm_prolong<T>(const T*, T*, const Geo&, const Geo&, cudaStream_t);                           \

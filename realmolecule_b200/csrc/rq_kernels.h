@@ -145,9 +145,6 @@ template <typename T>
 cudaError_t nm_norms(const T* U, const int* label, const Geo& g, double h3, int nDom, double* norms, cudaStream_t st);
 template <typename T>
 cudaError_t nm_rbgs(T* P, const T* f, bool fine, const Geo& g, double h2, int color, cudaStream_t st);
-// one whole red-black sweep of the fine level (f = psi), out of place: Pn = what the two colour passes leave
-template <typename T>
-cudaError_t nm_sweep(const T* P, T* Pn, const T* f, const Geo& g, double h2, cudaStream_t st);
 // fc = R (f - A P) (the residual and its full weighting in one pass) and Pc = 0 on the coarse interior
 template <typename T>
 cudaError_t nm_resrestrict(const T* P, const T* f, bool fine, T* fc, T* Pc, const Geo& g, const Geo& gc, double inv_h2,
