@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(256) kb_prolong(const BInst* __restrict__ ins,
   const BInst& I = ins[it.inst];
   T* P = lev == 0 ? (T*)I.P[cp] : (T*)I.lP[lev];
   const Geo g = I.lg[lev], gc = I.lg[lev + 1];
-  nm_prolong_rows_body<T>((const T*)I.lP[lev + 1], P, g, gc, it.bx, it.by, it.bz);
+  nm_prolong_cells_body<T>((const T*)I.lP[lev + 1], P, g, gc, it.bx, it.by, it.bz);
 }
 
 template <typename T>
@@ -494,7 +494,8 @@ constexpr int kF32 = 0, kF64 = 1;
 
 // Work items of one instance for every list; built once at creation, concatenated by build_plans.
 struct InstItems {
-  std::vector<BItem> march[kMaxLev], rbgs[kMaxLev], restr[kMaxLev], zero[kMaxLev], coarse[kMaxLev], rr[kMaxLev];
+  std::vector<BItem> march[kMaxLev], rbgs[kMaxLev], restr[kMaxLev], zero[kMaxLev], coarse[kMaxLev], rr[kMaxLev],
+      pc[kMaxLev];
   std::vector<BItem> flat16, flat1, force, one;  // one: a single item (per-instance domain work)
 };
 
@@ -516,7 +517,7 @@ struct rq_batch {
   // work lists, one set per precision
   struct Plan { BItem* d = nullptr; int n = 0, cap = 0; };
   struct Plans {
-    Plan march[kMaxLev], rbgs[kMaxLev], restr[kMaxLev], zero[kMaxLev], coarse[kMaxLev], rr[kMaxLev];
+    Plan march[kMaxLev], rbgs[kMaxLev], restr[kMaxLev], zero[kMaxLev], coarse[kMaxLev], rr[kMaxLev], pc[kMaxLev];
     Plan flat16, flat1, force, one;
   };
   Plans pl[2];
@@ -611,6 +612,10 @@ static void make_items(const BInst& I, int q, InstItems& it, NmTile tile) {
     for (int zz = 0; zz < (cn + kNmRrPlanes - 1) / kNmRrPlanes; ++zz)
       for (int y = 0; y < (cn + kNmRrTJ - 1) / kNmRrTJ; ++y)
         for (int x = 0; x < (cn + kNmRrTK - 1) / kNmRrTK; ++x) it.rr[l].push_back({q, x, y, zz});
+    const int cc = I.lg[l + 1].NN;  // coarse cells of the prolongation
+    for (int zz = 0; zz < (cc + kNmPrPlanes - 1) / kNmPrPlanes; ++zz)
+      for (int y = 0; y < (cc + kNmPrTJ - 1) / kNmPrTJ; ++y)
+        for (int x = 0; x < (cc + kNmPrTK - 1) / kNmPrTK; ++x) it.pc[l].push_back({q, x, y, zz});
   }
   it.one.push_back({q, 0, 0, 0});
   flat_items(it.flat16, q, I.g.S3, 256 * kNmFlatChunk);
@@ -645,6 +650,7 @@ static int build_plans(rq_batch* b) {
       BRC(gather(P.restr[l], [l](const InstItems& it) -> const Items& { return it.restr[l]; }));
       BRC(gather(P.zero[l], [l](const InstItems& it) -> const Items& { return it.zero[l]; }));
       BRC(gather(P.rr[l], [l](const InstItems& it) -> const Items& { return it.rr[l]; }));
+      BRC(gather(P.pc[l], [l](const InstItems& it) -> const Items& { return it.pc[l]; }));
       BRC(gather(P.coarse[l], [l](const InstItems& it) -> const Items& { return it.coarse[l]; }));
     }
     BRC(gather(P.flat16, [](const InstItems& it) -> const Items& { return it.flat16; }));
@@ -836,7 +842,7 @@ static int b_vcycle(rq_batch* b, int p) {
     if (b->rec) {
       b_record(b, kPhProlong, p, &P.rbgs[l], l);
     } else {
-      kb_prolong<T><<<P.rbgs[l].n, rb, 0, b->st>>>(b->din, P.rbgs[l].d, l, b->cp);
+      kb_prolong<T><<<P.pc[l].n, rb, 0, b->st>>>(b->din, P.pc[l].d, l, b->cp);
       BL("prolong");
     }
     for (int s = 0; s < post; ++s) BRC(smooth(l));

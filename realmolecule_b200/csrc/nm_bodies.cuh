@@ -449,6 +449,74 @@ __device__ __forceinline__ void nm_prolong_rows_body(const T* __restrict__ Ec, T
 }
 #undef NM_ROWS_PROLOGUE
 
+// The same prolongation by coarse cells: thread (x, y) of a block of 256 owns the cells (I, J, K) =
+// (I0 + t, by * 8 + y, bx * 32 + x) for kNmPrPlanes values of t and updates the 2 x 2 x 2 fine
+// points (2I + a, 2J + b, 2K + c) of each that are interior.  A fine point with offsets (a, b, c)
+// averages the coarse values (I + da, J + db, K + dc) with da <= a, db <= b, dc <= c, added in
+// the (da, db, dc) order of nm_prolong_rows_body and scaled by the exact reciprocal of their
+// count, so the result is the row body's bit for bit.  Every load is unconditional (no branch
+// on parities) and each coarse plane is loaded once per march: 4 coarse and 8 fine loads and 8
+// fine stores per cell.
+constexpr int kNmPrTK = 32, kNmPrTJ = 8, kNmPrPlanes = 4;
+template <typename T>
+__device__ __forceinline__ void nm_prolong_cells_body(const T* __restrict__ Ec, T* __restrict__ P, const Geo& g,
+                                                      const Geo& gc, int bx, int by, int bz) {
+  using A = Ar<T>;
+  const int nc = gc.NN;  // coarse cells 0..nc-1 along each axis cover the fine interior 1..NN-1
+  const int K = bx * kNmPrTK + tile_x<32>(), J = by * kNmPrTJ + tile_y<32>();
+  if (K >= nc || J >= nc) return;
+  const int I0 = bz * kNmPrPlanes;
+  const int Iend = min(I0 + kNmPrPlanes, nc);
+  const long long S = g.S, S2 = g.S2, Sc = gc.S, Sc2 = gc.S2;
+  T c0[2][2], c1[2][2];  // coarse values of planes I and I + 1: [db][dc]
+#pragma unroll
+  for (int db = 0; db < 2; ++db)
+#pragma unroll
+    for (int dc = 0; dc < 2; ++dc) c0[db][dc] = Ec[(long long)I0 * Sc2 + (long long)(J + db) * Sc + K + dc];
+  for (int I = I0; I < Iend; ++I) {
+#pragma unroll
+    for (int db = 0; db < 2; ++db)
+#pragma unroll
+      for (int dc = 0; dc < 2; ++dc) c1[db][dc] = Ec[(long long)(I + 1) * Sc2 + (long long)(J + db) * Sc + K + dc];
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+      const int i = 2 * I + a;
+      if (i < 1) continue;  // the fine boundary plane
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        const int j = 2 * J + b;
+        if (j < 1) continue;
+        const long long row = (long long)i * S2 + (long long)j * S;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const int k = 2 * K + c;
+          if (k < 1) continue;
+          T v = A::add(T(0), c0[0][0]);
+          if (c) v = A::add(v, c0[0][1]);
+          if (b) {
+            v = A::add(v, c0[1][0]);
+            if (c) v = A::add(v, c0[1][1]);
+          }
+          if (a) {
+            v = A::add(v, c1[0][0]);
+            if (c) v = A::add(v, c1[0][1]);
+            if (b) {
+              v = A::add(v, c1[1][0]);
+              if (c) v = A::add(v, c1[1][1]);
+            }
+          }
+          v = A::mul(v, (T)(1.0 / ((1 + a) * (1 + b) * (1 + c))));
+          P[row + k] = A::add(P[row + k], v);
+        }
+      }
+    }
+#pragma unroll
+    for (int db = 0; db < 2; ++db)
+#pragma unroll
+      for (int dc = 0; dc < 2; ++dc) c0[db][dc] = c1[db][dc];
+  }
+}
+
 // full weighting (1/64)(8,4,2,1) at coarse interior point number q; loop order a, b, c
 template <typename T>
 __device__ __forceinline__ void nm_restrict_body(const T* __restrict__ fine, T* __restrict__ coarse, const Geo& g,

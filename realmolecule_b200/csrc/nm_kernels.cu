@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(256) k_nm_resrestrict(const T* P, const T* f, 
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_nm_prolong(const T* Ec, T* P, Geo g, Geo gc) {
-  nm_prolong_rows_body<T>(Ec, P, g, gc, blockIdx.x, blockIdx.y, blockIdx.z);
+  nm_prolong_cells_body<T>(Ec, P, g, gc, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 template <typename T>
@@ -216,8 +216,8 @@ cudaError_t nm_resrestrict(const T* P, const T* f, bool fine, T* fc, T* Pc, cons
 }
 template <typename T>
 cudaError_t nm_prolong(const T* Ec, T* P, const Geo& g, const Geo& gc, cudaStream_t st) {
-  const int n = g.NN - 1;
-  const dim3 blk(32, 8), grd((n + 63) / 64, (n + 7) / 8, (n + kNmRowPlanes - 1) / kNmRowPlanes);
+  const int nc = gc.NN;  // coarse cells per axis
+  const dim3 blk(32, 8), grd((nc + kNmPrTK - 1) / kNmPrTK, (nc + kNmPrTJ - 1) / kNmPrTJ, (nc + kNmPrPlanes - 1) / kNmPrPlanes);
   k_nm_prolong<T><<<grd, blk, 0, st>>>(Ec, P, g, gc);
   return cudaGetLastError();
 }
