@@ -290,18 +290,50 @@ __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __res
 }
 
 // U *= scale[label] (FP64 product, rounded once) for labels in [0, nDom) over kNmFlatChunk*256
-// points from blk
+// points from blk.  With 16-byte aligned fields each thread moves 16-byte vectors of psi (and the
+// matching int4 / int2 of labels), kNmFlatChunk points in all; the block covers the same points
+// as the scalar walk and every point gets the same product.
+template <typename T>
+__device__ __forceinline__ void nm_apply_scale_point(T& u, int l, const double* __restrict__ scale, int nDom) {
+  if (l >= 0 && l < nDom) u = (T)((double)u * scale[l]);
+}
+
 template <typename T>
 __device__ __forceinline__ void nm_apply_scale_body(T* __restrict__ U, const int* __restrict__ label,
                                                     const double* __restrict__ scale, long long S3, int nDom,
                                                     long long blk) {
   const long long base = blk * blockDim.x * kNmFlatChunk;
+  if ((((unsigned long long)U | (unsigned long long)label) & 15) == 0) {
+    constexpr int W = 16 / (int)sizeof(T);  // points per vector
+#pragma unroll
+    for (int q = 0; q < kNmFlatChunk / W; ++q) {
+      const long long e0 = base + ((long long)q * blockDim.x + threadIdx.x) * W;
+      if (e0 + W <= S3) {
+        if constexpr (sizeof(T) == sizeof(float)) {
+          float4 u = *reinterpret_cast<const float4*>(U + e0);
+          const int4 l = *reinterpret_cast<const int4*>(label + e0);
+          nm_apply_scale_point(u.x, l.x, scale, nDom);
+          nm_apply_scale_point(u.y, l.y, scale, nDom);
+          nm_apply_scale_point(u.z, l.z, scale, nDom);
+          nm_apply_scale_point(u.w, l.w, scale, nDom);
+          *reinterpret_cast<float4*>(U + e0) = u;
+        } else {
+          double2 u = *reinterpret_cast<const double2*>(U + e0);
+          const int2 l = *reinterpret_cast<const int2*>(label + e0);
+          nm_apply_scale_point(u.x, l.x, scale, nDom);
+          nm_apply_scale_point(u.y, l.y, scale, nDom);
+          *reinterpret_cast<double2*>(U + e0) = u;
+        }
+      } else {
+        for (long long e = e0; e < S3; ++e) nm_apply_scale_point(U[e], label[e], scale, nDom);
+      }
+    }
+    return;
+  }
   for (int q = 0; q < kNmFlatChunk; ++q) {
     const long long id = base + (long long)q * blockDim.x + threadIdx.x;
     if (id >= S3) break;
-    const int l = label[id];
-    if (l < 0 || l >= nDom) continue;
-    U[id] = (T)((double)U[id] * scale[l]);
+    nm_apply_scale_point(U[id], label[id], scale, nDom);
   }
 }
 
