@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(256) kb_residual(const BInst* __restrict__ ins
 // residual, full weighting and the zeroed coarse correction of level lev in one pass
 template <typename T, bool FINE>
 __global__ void __launch_bounds__(256) kb_resrestrict(const BInst* __restrict__ ins, const BItem* __restrict__ items,
-                                                      int lev, int cu, int cp) {
+                                                      int lev, int cu, int cp, int planes) {
   __shared__ T patch[2][kNmRrPatch];
   const BItem it = items[blockIdx.x];
   const BInst& I = ins[it.inst];
@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(256) kb_resrestrict(const BInst* __restrict__ 
   const T* f = FINE ? (const T*)I.U[cu] : (const T*)I.lf[lev];
   const Geo g = I.lg[lev], gc = I.lg[lev + 1];
   nm_resrestrict_body<T, FINE>(P, f, (T*)I.lf[lev + 1], (T*)I.lP[lev + 1], g, gc, (T)(1.0 / (I.lh[lev] * I.lh[lev])),
-                               it.bx, it.by, it.bz, patch);
+                               it.bx, it.by, it.bz, planes, patch);
 }
 
 template <typename T>
@@ -158,12 +158,12 @@ __global__ void __launch_bounds__(256) kb_zero(const BInst* __restrict__ ins, co
 
 template <typename T>
 __global__ void __launch_bounds__(256) kb_prolong(const BInst* __restrict__ ins, const BItem* __restrict__ items, int lev,
-                                                  int cp) {
+                                                  int cp, int planes) {
   const BItem it = items[blockIdx.x];
   const BInst& I = ins[it.inst];
   T* P = lev == 0 ? (T*)I.P[cp] : (T*)I.lP[lev];
   const Geo g = I.lg[lev], gc = I.lg[lev + 1];
-  nm_prolong_cells_body<T>((const T*)I.lP[lev + 1], P, g, gc, it.bx, it.by, it.bz);
+  nm_prolong_cells_body<T>((const T*)I.lP[lev + 1], P, g, gc, it.bx, it.by, it.bz, planes);
 }
 
 template <typename T>
@@ -514,6 +514,7 @@ struct rq_batch {
   unsigned* rseed = nullptr;      // the step seed of the fp32 set's unbiased rounding (2 words by parity)
   float4* seeds_all = nullptr;
   int maxlev = 0;
+  int rr_pl[kMaxLev] = {}, pr_pl[kMaxLev] = {};  // coarse planes per block of the level's residual-restriction / prolongation
   // work lists, one set per precision
   struct Plan { BItem* d = nullptr; int n = 0, cap = 0; };
   struct Plans {
@@ -593,7 +594,7 @@ static void flat_items(std::vector<BItem>& v, int inst, long long npts, long lon
   for (long long x = 0; x < (npts + per_block - 1) / per_block; ++x) v.push_back({inst, (int)x, 0, 0});
 }
 
-static void make_items(const BInst& I, int q, InstItems& it, NmTile tile) {
+static void make_items(const BInst& I, int q, InstItems& it, NmTile tile, const int* rr_pl, const int* pr_pl) {
   it = InstItems{};
   for (int l = 0; l < I.nlev; ++l) {
     march_items(it.march[l], q, I.lg[l], tile);
@@ -609,11 +610,11 @@ static void make_items(const BInst& I, int q, InstItems& it, NmTile tile) {
     flat_items(it.restr[l], q, nc, 256);
     flat_items(it.zero[l], q, I.lg[l + 1].S3, 256 * kNmFlatChunk);
     const int cn = I.lg[l + 1].NN - 1;  // coarse interior of the fused residual + restriction
-    for (int zz = 0; zz < (cn + kNmRrPlanes - 1) / kNmRrPlanes; ++zz)
+    for (int zz = 0; zz < (cn + rr_pl[l] - 1) / rr_pl[l]; ++zz)
       for (int y = 0; y < (cn + kNmRrTJ - 1) / kNmRrTJ; ++y)
         for (int x = 0; x < (cn + kNmRrTK - 1) / kNmRrTK; ++x) it.rr[l].push_back({q, x, y, zz});
     const int cc = I.lg[l + 1].NN;  // coarse cells of the prolongation
-    for (int zz = 0; zz < (cc + kNmPrPlanes - 1) / kNmPrPlanes; ++zz)
+    for (int zz = 0; zz < (cc + pr_pl[l] - 1) / pr_pl[l]; ++zz)
       for (int y = 0; y < (cc + kNmPrTJ - 1) / kNmPrTJ; ++y)
         for (int x = 0; x < (cc + kNmPrTK - 1) / kNmPrTK; ++x) it.pc[l].push_back({q, x, y, zz});
   }
@@ -684,6 +685,28 @@ static int alloc_fields(rq_batch* b, BInst& I, size_t es) {
   return RQ_OK;
 }
 
+// Coarse planes per block of each level's residual-restriction and prolongation over all
+// instances: 8, halved while the level's launch would have fewer than 8 blocks per SM.
+static void b_mg_planes(rq_batch* b) {
+  for (int l = 0; l + 1 < b->maxlev; ++l) {
+    auto blocks = [&](int planes, bool rr) {
+      long long tot = 0;
+      for (const BInst& I : b->hin) {
+        if (l + 1 >= I.nlev) continue;
+        const int n = rr ? I.lg[l + 1].NN - 1 : I.lg[l + 1].NN;
+        const int tk = rr ? kNmRrTK : kNmPrTK, tj = rr ? kNmRrTJ : kNmPrTJ;
+        tot += (long long)((n + tk - 1) / tk) * ((n + tj - 1) / tj) * ((n + planes - 1) / planes);
+      }
+      return tot;
+    };
+    for (int r = 0; r < 2; ++r) {
+      int planes = 8;
+      while (planes > 1 && blocks(planes, r == 0) < 8LL * 148) planes /= 2;
+      (r == 0 ? b->rr_pl : b->pr_pl)[l] = planes;
+    }
+  }
+}
+
 static int build(rq_batch* b) {
   const int n = b->n;
   for (int q = 0; q < n; ++q) {
@@ -747,7 +770,8 @@ static int build(rq_batch* b) {
     BCK(cudaMemcpyAsync(b->din, b->hin.data(), sizeof(BInst) * n, cudaMemcpyHostToDevice, b->st));
   }
   b->items.resize(n);
-  for (int q = 0; q < n; ++q) make_items(b->hin[q], q, b->items[q], b->tile);
+  b_mg_planes(b);
+  for (int q = 0; q < n; ++q) make_items(b->hin[q], q, b->items[q], b->tile, b->rr_pl, b->pr_pl);
   BRC(build_plans(b));
   size_t smax = 0;
   for (int l = 0; l < b->maxlev; ++l) smax = std::max(smax, b->coarse_smem[l]);
@@ -832,9 +856,9 @@ static int b_vcycle(rq_batch* b, int p) {
     }
     // the coarse correction's boundary stays zero from the allocation: only its interior is cleared
     if (l == 0)
-      kb_resrestrict<T, true><<<P.rr[l].n, rb, 0, b->st>>>(b->din, P.rr[l].d, l, b->cu, b->cp);
+      kb_resrestrict<T, true><<<P.rr[l].n, rb, 0, b->st>>>(b->din, P.rr[l].d, l, b->cu, b->cp, b->rr_pl[l]);
     else
-      kb_resrestrict<T, false><<<P.rr[l].n, rb, 0, b->st>>>(b->din, P.rr[l].d, l, b->cu, b->cp);
+      kb_resrestrict<T, false><<<P.rr[l].n, rb, 0, b->st>>>(b->din, P.rr[l].d, l, b->cu, b->cp, b->rr_pl[l]);
     BL("resrestrict");
   }
   for (int l = b->maxlev - 2; l >= 0; --l) {
@@ -842,7 +866,7 @@ static int b_vcycle(rq_batch* b, int p) {
     if (b->rec) {
       b_record(b, kPhProlong, p, &P.rbgs[l], l);
     } else {
-      kb_prolong<T><<<P.pc[l].n, rb, 0, b->st>>>(b->din, P.pc[l].d, l, b->cp);
+      kb_prolong<T><<<P.pc[l].n, rb, 0, b->st>>>(b->din, P.pc[l].d, l, b->cp, b->pr_pl[l]);
       BL("prolong");
     }
     for (int s = 0; s < post; ++s) BRC(smooth(l));
@@ -1548,7 +1572,7 @@ static void b_drop_graphs(rq_batch* b) {
 static int b_retile(rq_batch* b, NmTile t) {
   b->tile = t;
   b->cfg.batch_tile = t.lgk | (t.march << 8);
-  for (int q = 0; q < b->n; ++q) make_items(b->hin[q], q, b->items[q], t);
+  for (int q = 0; q < b->n; ++q) make_items(b->hin[q], q, b->items[q], t, b->rr_pl, b->pr_pl);
   return build_plans(b);
 }
 

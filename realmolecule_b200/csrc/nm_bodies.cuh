@@ -482,23 +482,23 @@ __device__ __forceinline__ void nm_prolong_rows_body(const T* __restrict__ Ec, T
 #undef NM_ROWS_PROLOGUE
 
 // The same prolongation by coarse cells: thread (x, y) of a block of 256 owns the cells (I, J, K) =
-// (I0 + t, by * 8 + y, bx * 32 + x) for kNmPrPlanes values of t and updates the 2 x 2 x 2 fine
+// (I0 + t, by * 8 + y, bx * 32 + x) for `planes` values of t and updates the 2 x 2 x 2 fine
 // points (2I + a, 2J + b, 2K + c) of each that are interior.  A fine point with offsets (a, b, c)
 // averages the coarse values (I + da, J + db, K + dc) with da <= a, db <= b, dc <= c, added in
 // the (da, db, dc) order of nm_prolong_rows_body and scaled by the exact reciprocal of their
 // count, so the result is the row body's bit for bit.  Every load is unconditional (no branch
 // on parities) and each coarse plane is loaded once per march: 4 coarse and 8 fine loads and 8
 // fine stores per cell.
-constexpr int kNmPrTK = 32, kNmPrTJ = 8, kNmPrPlanes = 4;
+constexpr int kNmPrTK = 32, kNmPrTJ = 8;
 template <typename T>
 __device__ __forceinline__ void nm_prolong_cells_body(const T* __restrict__ Ec, T* __restrict__ P, const Geo& g,
-                                                      const Geo& gc, int bx, int by, int bz) {
+                                                      const Geo& gc, int bx, int by, int bz, int planes) {
   using A = Ar<T>;
   const int nc = gc.NN;  // coarse cells 0..nc-1 along each axis cover the fine interior 1..NN-1
   const int K = bx * kNmPrTK + tile_x<32>(), J = by * kNmPrTJ + tile_y<32>();
   if (K >= nc || J >= nc) return;
-  const int I0 = bz * kNmPrPlanes;
-  const int Iend = min(I0 + kNmPrPlanes, nc);
+  const int I0 = bz * planes;
+  const int Iend = min(I0 + planes, nc);
   const long long S = g.S, S2 = g.S2, Sc = gc.S, Sc2 = gc.S2;
   T c0[2][2], c1[2][2];  // coarse values of planes I and I + 1: [db][dc]
 #pragma unroll
@@ -570,7 +570,7 @@ __device__ __forceinline__ void nm_restrict_body(const T* __restrict__ fine, T* 
 // Residual and full weighting in one pass: fc = R (f - A P) on the coarse interior without storing
 // the fine residual, and the coarse correction Pc (when given) zeroed on the same points.  The
 // block (256 threads, read as 32 x 8) owns the coarse points (K, J) = (K0 + x, J0 + y) of a 32 x 8
-// tile on kNmRrPlanes coarse planes from I0, and walks the fine planes 2 I0 - 1 .. 2 Ilast + 1.
+// tile on `planes` coarse planes from I0, and walks the fine planes 2 I0 - 1 .. 2 Ilast + 1.
 // On each fine plane it forms the residual on the 65 x 17 fine patch under the tile into shared
 // memory (every thread keeps the P values of its patch points on the planes below and above in
 // registers); after one barrier each coarse point adds the 3 x 3 patch values around it, with
@@ -578,7 +578,17 @@ __device__ __forceinline__ void nm_restrict_body(const T* __restrict__ fine, T* 
 // opens that of I + 1.  The sums run in the (a, b, c) order of nm_restrict_body and the residual
 // is nm_residual_value, so the result is the one of the residual pass and the restriction.  The
 // patch is double-buffered: one barrier per fine plane.
-constexpr int kNmRrTK = 32, kNmRrTJ = 8, kNmRrPlanes = 8;
+constexpr int kNmRrTK = 32, kNmRrTJ = 8;
+
+// Coarse planes per block of the residual-restriction and prolongation kernels for a launch of
+// `blocks_per_plane` blocks on each of n coarse planes: 8, halved while the launch would have
+// fewer than 8 blocks per SM (small levels and single grids favour more blocks over the extra
+// fine plane a block forms at its chunk's ends).
+inline int nm_mg_planes(long long blocks_per_plane, int n) {
+  int planes = 8;
+  while (planes > 1 && blocks_per_plane * ((n + planes - 1) / planes) < 8LL * 148) planes /= 2;
+  return planes;
+}
 constexpr int kNmRrPK = 2 * kNmRrTK + 1;                      // fine patch row (65 points)
 constexpr int kNmRrPatch = kNmRrPK * (2 * kNmRrTJ + 1);       // 65 x 17 fine points
 constexpr int kNmRrPer = (kNmRrPatch + 255) / 256;            // patch points per thread
@@ -586,12 +596,13 @@ constexpr int kNmRrPer = (kNmRrPatch + 255) / 256;            // patch points pe
 template <typename T, bool FINE>
 __device__ __forceinline__ void nm_resrestrict_body(const T* __restrict__ P, const T* __restrict__ f, T* __restrict__ fc,
                                                     T* __restrict__ Pc, const Geo& g, const Geo& gc, T inv_h2, int bx,
-                                                    int by, int bz, T (*patch)[kNmRrPatch]) {
+                                                    int by, int bz, int planes,
+                                                    T (*patch)[kNmRrPatch]) {
   using A = Ar<T>;
   const int n = gc.NN - 1;  // coarse interior 1..n
-  const int I0 = 1 + bz * kNmRrPlanes;
+  const int I0 = 1 + bz * planes;
   if (I0 > n) return;  // the whole block
-  const int Ilast = min(I0 + kNmRrPlanes - 1, n);
+  const int Ilast = min(I0 + planes - 1, n);
   const int tx = tile_x<32>(), ty = tile_y<32>(), tid = tx + 32 * ty;
   const int K0 = 1 + bx * kNmRrTK, J0 = 1 + by * kNmRrTJ;
   const int K = K0 + tx, J = J0 + ty;

@@ -82,14 +82,15 @@ __global__ void __launch_bounds__(256) k_nm_rbgs(T* P, const T* f, Geo g, T h2, 
 }
 
 template <typename T, bool FINE>
-__global__ void __launch_bounds__(256) k_nm_resrestrict(const T* P, const T* f, T* fc, T* Pc, Geo g, Geo gc, T inv_h2) {
+__global__ void __launch_bounds__(256) k_nm_resrestrict(const T* P, const T* f, T* fc, T* Pc, Geo g, Geo gc, T inv_h2,
+                                                        int planes) {
   __shared__ T patch[2][kNmRrPatch];
-  nm_resrestrict_body<T, FINE>(P, f, fc, Pc, g, gc, inv_h2, blockIdx.x, blockIdx.y, blockIdx.z, patch);
+  nm_resrestrict_body<T, FINE>(P, f, fc, Pc, g, gc, inv_h2, blockIdx.x, blockIdx.y, blockIdx.z, planes, patch);
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_nm_prolong(const T* Ec, T* P, Geo g, Geo gc) {
-  nm_prolong_cells_body<T>(Ec, P, g, gc, blockIdx.x, blockIdx.y, blockIdx.z);
+__global__ void __launch_bounds__(256) k_nm_prolong(const T* Ec, T* P, Geo g, Geo gc, int planes) {
+  nm_prolong_cells_body<T>(Ec, P, g, gc, blockIdx.x, blockIdx.y, blockIdx.z, planes);
 }
 
 template <typename T>
@@ -207,18 +208,22 @@ cudaError_t nm_resrestrict(const T* P, const T* f, bool fine, T* fc, T* Pc, cons
                            cudaStream_t st) {
   const int n = gc.NN - 1;
   if (n < 1) return cudaSuccess;
-  const dim3 blk(32, 8), grd((n + kNmRrTK - 1) / kNmRrTK, (n + kNmRrTJ - 1) / kNmRrTJ, (n + kNmRrPlanes - 1) / kNmRrPlanes);
+  const long long tiles = (long long)((n + kNmRrTK - 1) / kNmRrTK) * ((n + kNmRrTJ - 1) / kNmRrTJ);
+  const int planes = nm_mg_planes(tiles, n);
+  const dim3 blk(32, 8), grd((n + kNmRrTK - 1) / kNmRrTK, (n + kNmRrTJ - 1) / kNmRrTJ, (n + planes - 1) / planes);
   if (fine)
-    k_nm_resrestrict<T, true><<<grd, blk, 0, st>>>(P, f, fc, Pc, g, gc, (T)inv_h2);
+    k_nm_resrestrict<T, true><<<grd, blk, 0, st>>>(P, f, fc, Pc, g, gc, (T)inv_h2, planes);
   else
-    k_nm_resrestrict<T, false><<<grd, blk, 0, st>>>(P, f, fc, Pc, g, gc, (T)inv_h2);
+    k_nm_resrestrict<T, false><<<grd, blk, 0, st>>>(P, f, fc, Pc, g, gc, (T)inv_h2, planes);
   return cudaGetLastError();
 }
 template <typename T>
 cudaError_t nm_prolong(const T* Ec, T* P, const Geo& g, const Geo& gc, cudaStream_t st) {
   const int nc = gc.NN;  // coarse cells per axis
-  const dim3 blk(32, 8), grd((nc + kNmPrTK - 1) / kNmPrTK, (nc + kNmPrTJ - 1) / kNmPrTJ, (nc + kNmPrPlanes - 1) / kNmPrPlanes);
-  k_nm_prolong<T><<<grd, blk, 0, st>>>(Ec, P, g, gc);
+  const long long tiles = (long long)((nc + kNmPrTK - 1) / kNmPrTK) * ((nc + kNmPrTJ - 1) / kNmPrTJ);
+  const int planes = nm_mg_planes(tiles, nc);
+  const dim3 blk(32, 8), grd((nc + kNmPrTK - 1) / kNmPrTK, (nc + kNmPrTJ - 1) / kNmPrTJ, (nc + planes - 1) / planes);
+  k_nm_prolong<T><<<grd, blk, 0, st>>>(Ec, P, g, gc, planes);
   return cudaGetLastError();
 }
 template <typename T>
