@@ -609,48 +609,33 @@ __device__ __forceinline__ void nm_resrestrict_body(const T* __restrict__ P, con
   const bool own = K <= n && J <= n;
   const long long S = g.S, S2 = g.S2;
   const int fi0 = 2 * I0 - 1, fi1 = 2 * Ilast + 1;
-  // fine (j, k) offset of each patch point of this thread; points outside the grid use the offset
-  // of (1, 1) (in bounds, never stored)
-  int col[kNmRrPer];
-  bool in[kNmRrPer];
+  int col[kNmRrPer];  // fine (j, k) offset of each patch point of this thread, -1 outside the grid
   T pm[kNmRrPer], pc[kNmRrPer];
-  T nx[kNmRrPer][2];  // P(+i) and f of each patch point on the current plane (the loads that reach DRAM)
-  auto load_plane = [&](int i) {
-    const long long base = (long long)i * S2;
-#pragma unroll
-    for (int m = 0; m < kNmRrPer; ++m) {
-      nx[m][0] = P[base + S2 + col[m]];
-      nx[m][1] = f[base + col[m]];
-    }
-  };
 #pragma unroll
   for (int m = 0; m < kNmRrPer; ++m) {
     const int p = tid + 256 * m;
     const int fj = 2 * J0 - 1 + p / kNmRrPK, fk = 2 * K0 - 1 + p % kNmRrPK;
-    in[m] = p < kNmRrPatch && fj < g.NN && fk < g.NN;
-    col[m] = in[m] ? fj * g.S + fk : g.S + 1;
-    pm[m] = P[(long long)(fi0 - 1) * S2 + col[m]];
-    pc[m] = P[(long long)fi0 * S2 + col[m]];
+    col[m] = (p < kNmRrPatch && fj < g.NN && fk < g.NN) ? fj * g.S + fk : -1;
+    pm[m] = pc[m] = T(0);
+    if (col[m] >= 0) {
+      pm[m] = P[(long long)(fi0 - 1) * S2 + col[m]];
+      pc[m] = P[(long long)fi0 * S2 + col[m]];
+    }
   }
-  load_plane(fi0);
   T v = T(0);
   for (int i = fi0; i <= fi1; ++i) {
     T* buf = patch[i & 1];
     const long long base = (long long)i * S2;
-    T r[kNmRrPer];
 #pragma unroll
     for (int m = 0; m < kNmRrPer; ++m) {
-      // the in-plane neighbours were the previous plane's P(+i) loads of neighbouring threads (L1)
+      if (col[m] < 0) continue;
       const long long id = base + col[m];
-      const T rhs = FINE ? A::mul(A::mul((T)6.283185307179586, nx[m][1]), nx[m][1]) : nx[m][1];
-      r[m] = nm_residual_value<T>(nx[m][0], pm[m], P[id + S], P[id - S], P[id + 1], P[id - 1], pc[m], rhs, inv_h2);
+      const T pp = P[id + S2];
+      buf[tid + 256 * m] =
+          nm_residual_value<T>(pp, pm[m], P[id + S], P[id - S], P[id + 1], P[id - 1], pc[m], rhs_at<T, FINE>(f, id), inv_h2);
       pm[m] = pc[m];
-      pc[m] = nx[m][0];
+      pc[m] = pp;
     }
-    if (i < fi1) load_plane(i + 1);  // in flight through the barrier and the weighting below
-#pragma unroll
-    for (int m = 0; m < kNmRrPer; ++m)
-      if (in[m]) buf[tid + 256 * m] = r[m];
     __syncthreads();
     if (!own) continue;
     const T* q = buf + (2 * ty) * kNmRrPK + 2 * tx;  // patch point of fine (2J - 1, 2K - 1)
