@@ -241,8 +241,6 @@ __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __res
     const bool need_l = !MASK || ACC || scale != nullptr;
     T u_m = __ldg(U + id - S2), u_c = __ldg(U + id);
     int l_m = MASK ? 0 : __ldg(label + id - S2), l_c = need_l ? __ldg(label + id) : 0;
-    // two planes per trip: the second plane's loads can issue before the first plane's store
-#pragma unroll 2
     for (int i = i0; i < iend; ++i, id += S2) {
       const T u_p = __ldg(U + id + S2);
       const T ujp = __ldg(U + id + S), ujm = __ldg(U + id - S), ukp = __ldg(U + id + 1), ukm = __ldg(U + id - 1);
@@ -369,10 +367,7 @@ __device__ __forceinline__ T rhs_at(const T* __restrict__ f, long long id) {
 
 // one colour of a red-black sweep for A P = f, A P = (6P - sum_6 P)/h^2; block (32, 8): each
 // thread owns the pair (k0, k0+1) of row j on the kNmRowPlanes planes i from 1 + bz*kNmRowPlanes,
-// and on each plane updates the one of the pair that has the colour.  The point it updates on
-// plane i + 1 is the other of the pair, whose -i neighbour (the pair partner on plane i) and
-// k neighbour (the +i neighbour of plane i's point) it already loaded on plane i: neither has
-// this colour, so this pass does not change them, and the sum keeps its order.
+// and on each plane updates the one of the pair that has the colour
 template <typename T, bool FINE>
 __device__ __forceinline__ void nm_rbgs_body(T* __restrict__ P, const T* __restrict__ f, const Geo& g, T h2, int color,
                                              int bx, int by, int bz) {
@@ -383,27 +378,14 @@ __device__ __forceinline__ void nm_rbgs_body(T* __restrict__ P, const T* __restr
   if (j >= g.NN || k0 >= g.NN) return;
   const int iend = min(i0 + kNmRowPlanes, g.NN);
   const long long S = g.S, S2 = g.S2;
-  bool have = false;          // the previous plane's point was updated
-  T part = T(0), up = T(0);   // its pair partner's value, and its +i neighbour
 #pragma unroll
   for (int q = 0; q < kNmRowPlanes; ++q) {
     const int i = i0 + q;
     const int k = k0 + ((i + j + k0 + color) & 1);
-    if (i >= iend || k >= g.NN) {
-      have = false;
-      continue;
-    }
+    if (i >= iend || k >= g.NN) continue;
     const long long id = (long long)i * S2 + (long long)j * S + k;
-    const T pip = P[id + S2];
-    const T pim = have ? part : P[id - S2];
-    // k == k0 + 1: the -k neighbour is (i, j, k0), plane i - 1's +i neighbour; else the +k one
-    const T pkp = (have && k == k0) ? up : P[id + 1];
-    const T pkm = (have && k != k0) ? up : P[id - 1];
-    const T s = A::add(A::add(A::add(A::add(A::add(pip, pim), P[id + S]), P[id - S]), pkp), pkm);
+    const T s = A::add(A::add(A::add(A::add(A::add(P[id + S2], P[id - S2]), P[id + S]), P[id - S]), P[id + 1]), P[id - 1]);
     P[id] = A::div(A::add(s, A::mul(h2, rhs_at<T, FINE>(f, id))), T(6));
-    have = true;
-    part = k == k0 ? pkp : pkm;  // (i, j, partner): the next plane's -i neighbour
-    up = pip;                    // (i + 1, j, k): the next plane's k neighbour
   }
 }
 
