@@ -367,7 +367,10 @@ __device__ __forceinline__ T rhs_at(const T* __restrict__ f, long long id) {
 
 // one colour of a red-black sweep for A P = f, A P = (6P - sum_6 P)/h^2; block (32, 8): each
 // thread owns the pair (k0, k0+1) of row j on the kNmRowPlanes planes i from 1 + bz*kNmRowPlanes,
-// and on each plane updates the one of the pair that has the colour
+// and on each plane updates the one of the pair that has the colour.  The pass is in place, so
+// the compiler may not move a plane's loads above the previous plane's store; they only read
+// points of the other colour, which the pass does not change, so all planes' loads are issued
+// first (explicitly) and the updates follow.
 template <typename T, bool FINE>
 __device__ __forceinline__ void nm_rbgs_body(T* __restrict__ P, const T* __restrict__ f, const Geo& g, T h2, int color,
                                              int bx, int by, int bz) {
@@ -378,15 +381,20 @@ __device__ __forceinline__ void nm_rbgs_body(T* __restrict__ P, const T* __restr
   if (j >= g.NN || k0 >= g.NN) return;
   const int iend = min(i0 + kNmRowPlanes, g.NN);
   const long long S = g.S, S2 = g.S2;
+  T s[kNmRowPlanes], rhs[kNmRowPlanes];
+  long long ids[kNmRowPlanes];
 #pragma unroll
   for (int q = 0; q < kNmRowPlanes; ++q) {
     const int i = i0 + q;
     const int k = k0 + ((i + j + k0 + color) & 1);
-    if (i >= iend || k >= g.NN) continue;
-    const long long id = (long long)i * S2 + (long long)j * S + k;
-    const T s = A::add(A::add(A::add(A::add(A::add(P[id + S2], P[id - S2]), P[id + S]), P[id - S]), P[id + 1]), P[id - 1]);
-    P[id] = A::div(A::add(s, A::mul(h2, rhs_at<T, FINE>(f, id))), T(6));
+    ids[q] = (i < iend && k < g.NN) ? (long long)i * S2 + (long long)j * S + k : -1;
+    const long long id = ids[q] >= 0 ? ids[q] : S2 + S + 1;  // an interior point: in bounds, not stored
+    s[q] = A::add(A::add(A::add(A::add(A::add(P[id + S2], P[id - S2]), P[id + S]), P[id - S]), P[id + 1]), P[id - 1]);
+    rhs[q] = rhs_at<T, FINE>(f, id);
   }
+#pragma unroll
+  for (int q = 0; q < kNmRowPlanes; ++q)
+    if (ids[q] >= 0) P[ids[q]] = A::div(A::add(s[q], A::mul(h2, rhs[q])), T(6));
 }
 
 // residual f - A P at one interior point from its P values (+i, -i, +j, -j, +k, -k, centre) and
