@@ -122,9 +122,9 @@ __global__ void __launch_bounds__(256) kb_residual(const BInst* __restrict__ ins
 
 // residual, full weighting and the zeroed coarse correction of level lev in one pass
 template <typename T, bool FINE>
-__global__ void __launch_bounds__(256) kb_resrestrict(const BInst* __restrict__ ins, const BItem* __restrict__ items,
+__global__ void __launch_bounds__(256, 4) kb_resrestrict(const BInst* __restrict__ ins, const BItem* __restrict__ items,
                                                       int lev, int cu, int cp, int planes) {
-  __shared__ T patch[2][kNmRrPatch];
+  __shared__ T patch[kNmRrBuf][kNmRrPatch];
   const BItem it = items[blockIdx.x];
   const BInst& I = ins[it.inst];
   const T* P = FINE ? (const T*)I.P[cp] : (const T*)I.lP[lev];

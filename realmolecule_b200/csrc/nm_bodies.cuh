@@ -581,11 +581,12 @@ __device__ __forceinline__ void nm_restrict_body(const T* __restrict__ fine, T* 
 // tile on `planes` coarse planes from I0, and walks the fine planes 2 I0 - 1 .. 2 Ilast + 1.
 // On each fine plane it forms the residual on the 65 x 17 fine patch under the tile into shared
 // memory (every thread keeps the P values of its patch points on the planes below and above in
-// registers); after one barrier each coarse point adds the 3 x 3 patch values around it, with
-// their weights, to its running sum.  A fine plane 2I + 1 closes the sum of coarse plane I and
-// opens that of I + 1.  The sums run in the (a, b, c) order of nm_restrict_body and the residual
-// is nm_residual_value, so the result is the one of the residual pass and the restriction.  The
-// patch is double-buffered: one barrier per fine plane.
+// registers).  One step per coarse plane I forms the fine planes 2I and 2I + 1 and, after one
+// barrier, adds the 3 x 3 patch values of the fine planes 2I - 1, 2I and 2I + 1 around each coarse
+// point with their weights.  The sums run in the (a, b, c) order of nm_restrict_body and the
+// residual is nm_residual_value, so the result is the one of the residual pass and the
+// restriction.  A ring of kNmRrBuf patch planes lets the next step's planes be written while
+// slower threads still read this step's three: one barrier per coarse plane.
 constexpr int kNmRrTK = 32, kNmRrTJ = 8;
 
 // Coarse planes per block of the residual-restriction and prolongation kernels for a launch of
@@ -600,12 +601,12 @@ inline int nm_mg_planes(long long blocks_per_plane, int n) {
 constexpr int kNmRrPK = 2 * kNmRrTK + 1;                      // fine patch row (65 points)
 constexpr int kNmRrPatch = kNmRrPK * (2 * kNmRrTJ + 1);       // 65 x 17 fine points
 constexpr int kNmRrPer = (kNmRrPatch + 255) / 256;            // patch points per thread
+constexpr int kNmRrBuf = 6;                                   // patch planes in the ring
 
 template <typename T, bool FINE>
 __device__ __forceinline__ void nm_resrestrict_body(const T* __restrict__ P, const T* __restrict__ f, T* __restrict__ fc,
                                                     T* __restrict__ Pc, const Geo& g, const Geo& gc, T inv_h2, int bx,
-                                                    int by, int bz, int planes,
-                                                    T (*patch)[kNmRrPatch]) {
+                                                    int by, int bz, int planes, T (*patch)[kNmRrPatch]) {
   using A = Ar<T>;
   const int n = gc.NN - 1;  // coarse interior 1..n
   const int I0 = 1 + bz * planes;
@@ -616,56 +617,54 @@ __device__ __forceinline__ void nm_resrestrict_body(const T* __restrict__ P, con
   const int K = K0 + tx, J = J0 + ty;
   const bool own = K <= n && J <= n;
   const long long S = g.S, S2 = g.S2;
-  const int fi0 = 2 * I0 - 1, fi1 = 2 * Ilast + 1;
-  int col[kNmRrPer];  // fine (j, k) offset of each patch point of this thread, -1 outside the grid
-  T pm[kNmRrPer], pc[kNmRrPer];
+  const int fi0 = 2 * I0 - 1;
+  // fine (j, k) offset of each patch point of this thread; points outside the grid use the
+  // offset of (1, 1) (in bounds, their residuals are not stored)
+  int col[kNmRrPer];
+  bool in[kNmRrPer];
+  T pm[kNmRrPer], pc[kNmRrPer];  // P of each patch point on the planes below and at the next residual plane
 #pragma unroll
   for (int m = 0; m < kNmRrPer; ++m) {
     const int p = tid + 256 * m;
     const int fj = 2 * J0 - 1 + p / kNmRrPK, fk = 2 * K0 - 1 + p % kNmRrPK;
-    col[m] = (p < kNmRrPatch && fj < g.NN && fk < g.NN) ? fj * g.S + fk : -1;
-    pm[m] = pc[m] = T(0);
-    if (col[m] >= 0) {
-      pm[m] = P[(long long)(fi0 - 1) * S2 + col[m]];
-      pc[m] = P[(long long)fi0 * S2 + col[m]];
-    }
+    in[m] = p < kNmRrPatch && fj < g.NN && fk < g.NN;
+    col[m] = in[m] ? fj * g.S + fk : g.S + 1;
+    pm[m] = P[(long long)(fi0 - 1) * S2 + col[m]];
+    pc[m] = P[(long long)fi0 * S2 + col[m]];
   }
-  T v = T(0);
-  for (int i = fi0; i <= fi1; ++i) {
-    T* buf = patch[i & 1];
+  auto residual_plane = [&](int i) {  // the residuals of fine plane i into its ring slot
+    T* buf = patch[i % kNmRrBuf];
     const long long base = (long long)i * S2;
 #pragma unroll
     for (int m = 0; m < kNmRrPer; ++m) {
-      if (col[m] < 0) continue;
       const long long id = base + col[m];
       const T pp = P[id + S2];
-      buf[tid + 256 * m] =
-          nm_residual_value<T>(pp, pm[m], P[id + S], P[id - S], P[id + 1], P[id - 1], pc[m], rhs_at<T, FINE>(f, id), inv_h2);
+      const T r = nm_residual_value<T>(pp, pm[m], P[id + S], P[id - S], P[id + 1], P[id - 1], pc[m],
+                                       rhs_at<T, FINE>(f, id), inv_h2);
+      if (in[m]) buf[tid + 256 * m] = r;
       pm[m] = pc[m];
       pc[m] = pp;
     }
+  };
+  residual_plane(fi0);
+  for (int I = I0; I <= Ilast; ++I) {
+    residual_plane(2 * I);
+    residual_plane(2 * I + 1);
     __syncthreads();
     if (!own) continue;
-    const T* q = buf + (2 * ty) * kNmRrPK + 2 * tx;  // patch point of fine (2J - 1, 2K - 1)
-    auto add_plane = [&](int wa) {
+    T v = T(0);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const T* q = patch[(2 * I - 1 + a) % kNmRrBuf] + (2 * ty) * kNmRrPK + 2 * tx;  // fine (2J - 1, 2K - 1)
 #pragma unroll
       for (int b = 0; b < 3; ++b)
 #pragma unroll
         for (int c = 0; c < 3; ++c)
-          v = A::add(v, A::mul((T)(wa * (b == 1 ? 2 : 1) * (c == 1 ? 2 : 1)), q[b * kNmRrPK + c]));
-    };
-    if (i & 1) {
-      if (i > fi0) {  // a = +1 of coarse plane (i - 1) / 2, whose sum is then complete
-        add_plane(1);
-        const long long cid = (long long)((i - 1) >> 1) * gc.S2 + (long long)J * gc.S + K;
-        fc[cid] = A::div(v, T(64));
-        if (Pc) Pc[cid] = T(0);
-      }
-      v = T(0);
-      if (i < fi1) add_plane(1);  // a = -1 of coarse plane (i + 1) / 2
-    } else {
-      add_plane(2);  // a = 0
+          v = A::add(v, A::mul((T)((a == 1 ? 2 : 1) * (b == 1 ? 2 : 1) * (c == 1 ? 2 : 1)), q[b * kNmRrPK + c]));
     }
+    const long long cid = (long long)I * gc.S2 + (long long)J * gc.S + K;
+    fc[cid] = A::div(v, T(64));
+    if (Pc) Pc[cid] = T(0);
   }
 }
 

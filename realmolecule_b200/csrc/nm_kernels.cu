@@ -82,9 +82,9 @@ __global__ void __launch_bounds__(256) k_nm_rbgs(T* P, const T* f, Geo g, T h2, 
 }
 
 template <typename T, bool FINE>
-__global__ void __launch_bounds__(256) k_nm_resrestrict(const T* P, const T* f, T* fc, T* Pc, Geo g, Geo gc, T inv_h2,
+__global__ void __launch_bounds__(256, 4) k_nm_resrestrict(const T* P, const T* f, T* fc, T* Pc, Geo g, Geo gc, T inv_h2,
                                                         int planes) {
-  __shared__ T patch[2][kNmRrPatch];
+  __shared__ T patch[kNmRrBuf][kNmRrPatch];
   nm_resrestrict_body<T, FINE>(P, f, fc, Pc, g, gc, inv_h2, blockIdx.x, blockIdx.y, blockIdx.z, planes, patch);
 }
 
