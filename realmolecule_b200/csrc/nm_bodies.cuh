@@ -585,7 +585,7 @@ __device__ __forceinline__ void nm_restrict_body(const T* __restrict__ fine, T* 
 // barrier, adds the 3 x 3 patch values of the fine planes 2I - 1, 2I and 2I + 1 around each coarse
 // point with their weights.  The sums run in the (a, b, c) order of nm_restrict_body and the
 // residual is nm_residual_value, so the result is the one of the residual pass and the
-// restriction.  A ring of kNmRrBuf patch planes lets the next step's planes be written while
+// restriction.  A ring of kNmRrBuf (5) patch planes lets the next step's planes be written while
 // slower threads still read this step's three: one barrier per coarse plane.
 constexpr int kNmRrTK = 32, kNmRrTJ = 8;
 
@@ -601,7 +601,7 @@ inline int nm_mg_planes(long long blocks_per_plane, int n) {
 constexpr int kNmRrPK = 2 * kNmRrTK + 1;                      // fine patch row (65 points)
 constexpr int kNmRrPatch = kNmRrPK * (2 * kNmRrTJ + 1);       // 65 x 17 fine points
 constexpr int kNmRrPer = (kNmRrPatch + 255) / 256;            // patch points per thread
-constexpr int kNmRrBuf = 6;                                   // patch planes in the ring
+constexpr int kNmRrBuf = 5;                                   // patch planes in the ring
 
 template <typename T, bool FINE>
 __device__ __forceinline__ void nm_resrestrict_body(const T* __restrict__ P, const T* __restrict__ f, T* __restrict__ fc,
