@@ -53,12 +53,11 @@ struct BItem {
 // registers first: through a reference into the instance table the compiler would re-read it
 // after every store, as it cannot prove the field pointers do not alias the table.
 // ---------------------------------------------------------------------------------------
-// The plain fp32 update fits 32 registers (8 blocks of 256 per SM); the others keep their own.
 template <typename T, bool ACC, bool SR>
-__global__ void __launch_bounds__(256, (sizeof(T) == sizeof(float) && !ACC && !SR) ? 8 : (ACC && SR ? 4 : 5))
-    kb_update(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cu, int cp, int cl, T half_dv, T dt,
-              double* __restrict__ norms, const double* __restrict__ scale, const unsigned* __restrict__ seed,
-              unsigned* __restrict__ seed_next, NmTile tile) {
+__global__ void __launch_bounds__(256) kb_update(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cu,
+                                                 int cp, int cl, T half_dv, T dt, double* __restrict__ norms,
+                                                 const double* __restrict__ scale, const unsigned* __restrict__ seed,
+                                                 unsigned* __restrict__ seed_next, NmTile tile) {
   __shared__ DomTable<1, 128> tab;
   if (SR && blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) *seed_next = *seed + 1u;
   const BItem it = items[blockIdx.x];
