@@ -233,10 +233,7 @@ __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __res
   rs.reset();
   int k, j, i0;
   nm_tile_origin(t, bx, by, bz, k, j, i0);
-  const bool inside = k < g.NN && j < g.NN && i0 < g.NN;
-  // the lanes that march (every lane of the block calls this body; their trip counts agree)
-  const unsigned act = ACC ? __ballot_sync(0xffffffffu, inside) : 0u;
-  if (inside) {
+  if (k < g.NN && j < g.NN && i0 < g.NN) {
     const int iend = min(i0 + t.march, g.NN);
     const long long S = g.S, S2 = g.S2;
     long long id = (long long)i0 * S2 + j * S + k;
@@ -284,7 +281,7 @@ __device__ __forceinline__ void nm_update_body(const T* __restrict__ U, T* __res
       Unew[id] = out;
       if (ACC) {
         const double r = (double)out * (double)out * h3;
-        rs.add_warp(min(max(l_c, 0), nDom - 1), &r, tab, norms, act);
+        rs.add(min(max(l_c, 0), nDom - 1), &r, tab, norms);
       }
       u_m = u_c; u_c = u_p; l_m = l_c; l_c = l_p;
     }

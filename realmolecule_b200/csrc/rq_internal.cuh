@@ -126,38 +126,6 @@ struct RunSum {
       for (int q = 0; q < NQ; ++q) v[q] += x[q];
     }
   }
-  // Same as add, called together by the lanes `act` of the warp (the same lanes at every call):
-  // the lanes whose label changes combine their sums per label with shuffles first, so one lane
-  // per distinct label touches the shared table.  A warp usually crosses a domain boundary with
-  // all its lanes on the same plane; one by one, their atomics on one slot would serialise.
-  template <int NSLOT>
-  __device__ __forceinline__ void add_warp(int l, const double* x, DomTable<NQ, NSLOT>& t, double* global,
-                                           unsigned act) {
-    const bool flush = l != label && label >= 0;
-    const unsigned fm = __ballot_sync(act, flush);
-    if (flush) {
-      const unsigned peers = __match_any_sync(fm, label);
-      double s[NQ];
-#pragma unroll
-      for (int q = 0; q < NQ; ++q) s[q] = 0.0;
-      for (int src = 0; src < 32; ++src) {  // the same 32 shuffles on every flushing lane
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) {
-          const double y = __shfl_sync(fm, v[q], src);
-          if ((peers >> src) & 1u) s[q] += y;
-        }
-      }
-      if (lane_id() == __ffs(peers) - 1) dom_table_add(t, label, s, global);
-    }
-    if (l != label) {
-      label = l;
-#pragma unroll
-      for (int q = 0; q < NQ; ++q) v[q] = x[q];
-    } else {
-#pragma unroll
-      for (int q = 0; q < NQ; ++q) v[q] += x[q];
-    }
-  }
   template <int NSLOT>
   __device__ __forceinline__ void finish(DomTable<NQ, NSLOT>& t, double* global) {
     if (label >= 0) dom_table_add(t, label, v, global);
