@@ -139,7 +139,6 @@ static void free_ctx(rq_ctx* c) {
   for (auto& L : c->mg) {
     if (L.P) cudaFree(L.P);
     if (L.f) cudaFree(L.f);
-    if (L.r) cudaFree(L.r);
   }
   if (c->own_st) cudaStreamDestroy(c->own_st);
 }

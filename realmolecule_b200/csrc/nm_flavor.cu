@@ -65,10 +65,6 @@ int nm_alloc_levels(rq_ctx* c) {
       cudaMemsetAsync(L.P, 0, n, c->st);
       cudaMemsetAsync(L.f, 0, n, c->st);
     }
-    if (l < levels - 1) {
-      if (cudaMalloc(&L.r, n) != cudaSuccess) return rq_cuda(c, cudaErrorMemoryAllocation, "multigrid residual");
-      cudaMemsetAsync(L.r, 0, n, c->st);
-    }
     h *= 2;
     nn /= 2;
   }
@@ -323,7 +319,7 @@ int nm_promote(rq_ctx* c) {
   // graphs still valid).
   void* nb[6] = {};  // U0, U1, P0, P1, K, Kext
   void* old[6] = {c->U[0], c->U[1], c->P[0], c->P[1], c->K, c->Kext};
-  std::vector<void*> lv;  // new multigrid buffers, in the order of the (L.P, L.f, L.r) walk below
+  std::vector<void*> lv;  // new multigrid buffers, in the order of the (L.P, L.f) walk below
   auto undo = [&]() {
     for (void* p : nb)
       if (p) cudaFree(p);
@@ -336,7 +332,7 @@ int nm_promote(rq_ctx* c) {
       return rq_cuda(c, cudaErrorMemoryAllocation, "promotion to FP64");
     }
   for (const rq_mg_level& L : c->mg)
-    for (void* p : {L.P, L.f, L.r}) {
+    for (void* p : {L.P, L.f}) {
       if (!p) continue;
       void* q = nullptr;
       if (cudaMalloc(&q, sizeof(double) * (size_t)L.g.S3) != cudaSuccess) {
@@ -358,7 +354,7 @@ int nm_promote(rq_ctx* c) {
     }
   size_t li = 0;
   for (const rq_mg_level& L : c->mg)
-    for (void* p : {L.P, L.f, L.r})
+    for (void* p : {L.P, L.f})
       if (p) cudaMemsetAsync(lv[li++], 0, sizeof(double) * (size_t)L.g.S3, c->st);
   if (cudaStreamSynchronize(c->st) != cudaSuccess) {
     const cudaError_t e = cudaGetLastError();
@@ -371,7 +367,7 @@ int nm_promote(rq_ctx* c) {
   c->U[0] = nb[0]; c->U[1] = nb[1]; c->P[0] = nb[2]; c->P[1] = nb[3]; c->K = nb[4]; c->Kext = nb[5];
   li = 0;
   for (rq_mg_level& L : c->mg)
-    for (void** p : {&L.P, &L.f, &L.r})
+    for (void** p : {&L.P, &L.f})
       if (*p) {
         cudaFree(*p);
         *p = lv[li++];

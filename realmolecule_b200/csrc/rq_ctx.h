@@ -14,8 +14,7 @@ struct rq_mg_level {  // one level of the new flavour's multigrid hierarchy
   rq::Geo g;
   double h;
   void* P = nullptr;  // solution / correction (T)
-  void* f = nullptr;  // right-hand side (T)
-  void* r = nullptr;  // residual (T)
+  void* f = nullptr;  // right-hand side (T); the residual is never stored (fused into the restriction)
 };
 
 // Recording window of the new flavour's adjoint: the state each recorded step started from, so
