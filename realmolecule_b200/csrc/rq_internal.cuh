@@ -54,15 +54,10 @@ inline dim3 march_block() { return dim3(kThreadsK, kThreadsJ, 1); }
 // global per-domain array with one FP64 atomic per quantity.  A label that finds no free
 // slot goes straight to global memory, so the result is exact for any label count.
 // ---------------------------------------------------------------------------------------
-// Single-quantity tables keep kCopies sums per slot, picked by lane: the lanes of a warp that
-// cross a domain boundary together flush into one slot, and FP64 adds to one shared word
-// serialise; spread over the copies they serialise four times less.  The flush adds the copies
-// in order.
 template <int NQ, int NSLOT = 128>
 struct DomTable {
-  static constexpr int kCopies = NQ == 1 ? 4 : 1;
   int keys[NSLOT];
-  double vals[NSLOT * NQ * kCopies];
+  double vals[NSLOT * NQ];
 };
 
 template <int NQ, int NSLOT>
@@ -70,22 +65,17 @@ __device__ __forceinline__ void dom_table_init(DomTable<NQ, NSLOT>& t) {
   const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
   const int nt = blockDim.x * blockDim.y * blockDim.z;
   for (int s = tid; s < NSLOT; s += nt) t.keys[s] = -1;
-  for (int s = tid; s < NSLOT * NQ * DomTable<NQ, NSLOT>::kCopies; s += nt) t.vals[s] = 0.0;
+  for (int s = tid; s < NSLOT * NQ; s += nt) t.vals[s] = 0.0;
 }
 
 template <int NQ, int NSLOT>
 __device__ __forceinline__ void dom_table_add(DomTable<NQ, NSLOT>& t, int label, const double* v, double* global) {
-  constexpr int C = DomTable<NQ, NSLOT>::kCopies;
-  const int copy = (int)((threadIdx.x + blockDim.x * threadIdx.y) & (C - 1));
   unsigned slot = ((unsigned)label * 2654435761u) & (NSLOT - 1);
   for (int p = 0; p < NSLOT; ++p) {
-    // a slot, once claimed, keeps its label for the block's lifetime: a plain read that finds it
-    // saves the compare-and-swap
-    const int seen = *(volatile int*)&t.keys[slot];
-    const int old = seen == label ? label : atomicCAS(&t.keys[slot], -1, label);
+    int old = atomicCAS(&t.keys[slot], -1, label);
     if (old == -1 || old == label) {
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) atomicAdd(&t.vals[(slot * C + copy) * NQ + q], v[q]);
+      for (int q = 0; q < NQ; ++q) atomicAdd(&t.vals[slot * NQ + q], v[q]);
       return;
     }
     slot = (slot + 1) & (NSLOT - 1);
@@ -96,19 +86,13 @@ __device__ __forceinline__ void dom_table_add(DomTable<NQ, NSLOT>& t, int label,
 
 template <int NQ, int NSLOT>
 __device__ __forceinline__ void dom_table_flush(DomTable<NQ, NSLOT>& t, double* global) {
-  constexpr int C = DomTable<NQ, NSLOT>::kCopies;
   const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
   const int nt = blockDim.x * blockDim.y * blockDim.z;
   for (int s = tid; s < NSLOT; s += nt) {
     int k = t.keys[s];
     if (k >= 0) {
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) {
-        double x = t.vals[(s * C) * NQ + q];
-#pragma unroll
-        for (int c = 1; c < C; ++c) x += t.vals[(s * C + c) * NQ + q];
-        atomicAdd(&global[(long long)k * NQ + q], x);
-      }
+      for (int q = 0; q < NQ; ++q) atomicAdd(&global[(long long)k * NQ + q], t.vals[s * NQ + q]);
     }
   }
 }
