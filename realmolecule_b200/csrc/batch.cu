@@ -109,17 +109,6 @@ __global__ void __launch_bounds__(256) kb_rbgs(const BInst* __restrict__ ins, co
   nm_rbgs_body<T, FINE>(P, f, g, (T)(I.lh[lev] * I.lh[lev]), color, it.bx, it.by, it.bz);
 }
 
-template <typename T, bool FINE>
-__global__ void __launch_bounds__(256) kb_residual(const BInst* __restrict__ ins, const BItem* __restrict__ items, int lev,
-                                                   int cu, int cp) {
-  const BItem it = items[blockIdx.x];
-  const BInst& I = ins[it.inst];
-  const T* P = FINE ? (const T*)I.P[cp] : (const T*)I.lP[lev];
-  const T* f = FINE ? (const T*)I.U[cu] : (const T*)I.lf[lev];
-  const Geo g = I.lg[lev];
-  nm_residual_rows_body<T, FINE>(P, f, (T*)I.lr[lev], g, (T)(1.0 / (I.lh[lev] * I.lh[lev])), it.bx, it.by, it.bz);
-}
-
 // residual, full weighting and the zeroed coarse correction of level lev in one pass
 template <typename T, bool FINE>
 __global__ void __launch_bounds__(256, 4) kb_resrestrict(const BInst* __restrict__ ins, const BItem* __restrict__ items,
@@ -132,28 +121,6 @@ __global__ void __launch_bounds__(256, 4) kb_resrestrict(const BInst* __restrict
   const Geo g = I.lg[lev], gc = I.lg[lev + 1];
   nm_resrestrict_body<T, FINE>(P, f, (T*)I.lf[lev + 1], (T*)I.lP[lev + 1], g, gc, (T)(1.0 / (I.lh[lev] * I.lh[lev])),
                                it.bx, it.by, it.bz, planes, patch);
-}
-
-template <typename T>
-__global__ void __launch_bounds__(256) kb_restrict(const BInst* __restrict__ ins, const BItem* __restrict__ items,
-                                                   int lev) {
-  const BItem it = items[blockIdx.x];
-  const BInst& I = ins[it.inst];
-  const Geo g = I.lg[lev], gc = I.lg[lev + 1];
-  nm_restrict_body<T>((const T*)I.lr[lev], (T*)I.lf[lev + 1], g, gc, (long long)it.bx * blockDim.x + threadIdx.x);
-}
-
-// zero the correction of level lev (flat blocks of 256 * kNmFlatChunk points)
-template <typename T>
-__global__ void __launch_bounds__(256) kb_zero(const BInst* __restrict__ ins, const BItem* __restrict__ items, int lev) {
-  const BItem it = items[blockIdx.x];
-  const BInst& I = ins[it.inst];
-  const long long S3 = I.lg[lev].S3, base = (long long)it.bx * blockDim.x * kNmFlatChunk;
-  T* p = (T*)I.lP[lev];
-  for (int q = 0; q < kNmFlatChunk; ++q) {
-    const long long id = base + (long long)q * blockDim.x + threadIdx.x;
-    if (id < S3) p[id] = T(0);
-  }
 }
 
 template <typename T>
@@ -230,7 +197,7 @@ __global__ void __launch_bounds__(256) kb_force(const BInst* __restrict__ ins, c
 }
 
 // Sum over the fine interior of the squared residual 2 pi psi^2 - A P (FP64), added into *out:
-// the autotuner's multigrid convergence measure.  Row tiling of kb_residual.
+// the autotuner's multigrid convergence measure.  Row tiling (nm_residual_rows_body's).
 template <typename T>
 __global__ void __launch_bounds__(256) kb_resnorm(const BInst* __restrict__ ins, const BItem* __restrict__ items, int cu,
                                                   int cp, double* __restrict__ out) {
